@@ -1,0 +1,1472 @@
+// C ABI of the B200 solve phase (include/s2l_gpu.h): setup upload, schedules, apply, Krylov.
+//
+// Host code.  Setup converts the caller's arrays once into the device layout of
+// s2l_internal.cuh (factors in level order, index maps, tiles of the coarse basis, E^-1); the
+// solve phase is a sequence of kernel launches on the setup's stream.  Krylov scalars
+// (Givens rotations, the small least-squares solve, BiCGStab coefficients) run on the host in
+// FP64 from device reductions read back once per orthogonalization step.
+#include "s2l_internal.cuh"
+#include "../../include/s2l_gpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace s2l;
+
+struct s2l_ctx {
+    int device = 0;
+    size_t budget = 0;
+    size_t used = 0;
+    std::string err;
+    std::mutex mu;
+};
+
+namespace {
+
+enum { PC_SPMV = 0, PC_SOLVE, PC_COARSE, PC_COMBINE, PC_VEC, PC_N };
+const char* kProfNames[PC_N] = {"spmv", "local_solve", "coarse", "combine", "krylov_vec"};
+
+struct HostCsr {
+    std::vector<int64_t> rp;
+    std::vector<int32_t> ci;
+    std::vector<double> v;  // values widened to double on the host
+};
+
+struct HostSub {
+    bool set = false;
+    int64_t begin = 0;
+    int n_owned = 0, n_ghost = 0;
+    std::vector<int64_t> ghosts;
+    std::vector<double> D;
+    int kind = S2L_FACTOR_LU;
+    std::vector<int32_t> pin, pout;
+    HostCsr L, U;
+    std::vector<double> d;
+    int m = 0;
+    std::vector<double> V;  // column-major n_local x m
+    int n_local() const { return n_owned + n_ghost; }
+};
+
+// one triangular factor of one subdomain in solve order
+struct Sched {
+    std::vector<int32_t> rows;
+    std::vector<int64_t> ptr;  // relative to the subdomain's first entry
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    std::vector<double> dinv;
+    std::vector<int32_t> lvl;
+    std::vector<int8_t> mode;
+};
+
+}  // namespace
+
+struct s2l_setup {
+    s2l_ctx* ctx = nullptr;
+    int64_t n = 0;
+    int nsub = 0;
+    int one_level = 0, coarse = 0, pou = 0;
+    int real = -1;
+    bool ended = false;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+
+    // host staging
+    HostCsr A;
+    bool have_A = false;
+    std::vector<HostSub> hs;
+    int64_t n0 = 0;
+    std::vector<int64_t> coff;
+    std::vector<double> E;
+    bool have_coarse = false;
+
+    // device memory
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    int32_t *d_rp = nullptr, *d_ci = nullptr;
+    double* d_av = nullptr;
+    int64_t nnz = 0;
+    int tpr = 8;
+    std::vector<DevSub> h_subs;
+    DevSub* d_subs = nullptr;
+    int64_t nloc = 0;
+    int32_t* d_rows[2] = {nullptr, nullptr};
+    int64_t* d_ptr[2] = {nullptr, nullptr};
+    int32_t* d_col[2] = {nullptr, nullptr};
+    void* d_val[2] = {nullptr, nullptr};
+    void* d_dinv[2] = {nullptr, nullptr};
+    int32_t* d_lvl = nullptr;
+    int8_t* d_mode = nullptr;
+    int32_t *d_gin = nullptr, *d_pin = nullptr, *d_gout = nullptr, *d_l2g = nullptr;
+    double* d_D = nullptr;
+    int64_t* d_cp_ptr = nullptr;
+    int32_t* d_cp_pos = nullptr;
+    double* d_cp_w = nullptr;
+    bool need_copies = false;
+    // coarse
+    double* d_V = nullptr;
+    int32_t *d_t_sub = nullptr, *d_t_row0 = nullptr, *d_t_nrow = nullptr, *d_t_first = nullptr;
+    int ntiles = 0, mmax = 0;
+    double* d_Einv = nullptr;
+    double* d_cpart = nullptr;
+    double *d_c = nullptr, *d_y = nullptr;
+    // work vectors
+    double *d_ylocal = nullptr, *d_x0 = nullptr, *d_w = nullptr, *d_in = nullptr, *d_out = nullptr;
+    double* d_plocal = nullptr;
+    void* d_xscratch = nullptr;
+    double* d_part = nullptr;
+    double* d_red = nullptr;
+    double* h_red = nullptr;
+    size_t smem_bytes = 0;
+    double solve_bytes = 0.0;
+    // Krylov work (lazy)
+    int kr_m = -1;
+    bool kr_flex = false;
+    double *d_V_kr = nullptr, *d_Z_kr = nullptr, *d_r = nullptr, *d_z = nullptr, *d_kw = nullptr, *d_b = nullptr,
+           *d_xk = nullptr, *d_u = nullptr;
+    double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
+    double* d_coef = nullptr;
+    // profiling
+    bool prof = false;
+    struct Ev {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Ev> evs;
+    std::vector<cudaEvent_t> pool;
+    double acc_ms[PC_N] = {0, 0, 0, 0, 0};
+    long acc_n[PC_N] = {0, 0, 0, 0, 0};
+
+    int fail(int code, const std::string& msg)
+    {
+        if (ctx) {
+            std::lock_guard<std::mutex> g(ctx->mu);
+            ctx->err = msg;
+        }
+        return code;
+    }
+};
+
+#define CUDA_OK(s, call)                                                                                             \
+    do {                                                                                                             \
+        cudaError_t _e = (call);                                                                                     \
+        if (_e != cudaSuccess) return (s)->fail(S2L_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));  \
+    } while (0)
+
+#define RET_IF(x)         \
+    do {                  \
+        int _r = (x);     \
+        if (_r) return _r; \
+    } while (0)
+
+namespace {
+
+int dev_alloc(s2l_setup* s, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    {
+        std::lock_guard<std::mutex> g(s->ctx->mu);
+        if (s->ctx->budget && s->ctx->used + bytes > s->ctx->budget) {
+            s->ctx->err = "HBM budget exceeded: need " + std::to_string(s->ctx->used + bytes) + " of " +
+                          std::to_string(s->ctx->budget) + " bytes";
+            return S2L_ERR_OOM;
+        }
+        s->ctx->used += bytes;
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(s->ctx->mu);
+        s->ctx->used -= bytes;
+        s->ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return S2L_ERR_OOM;
+    }
+    s->allocs.push_back(*p);
+    s->bytes += bytes;
+    return S2L_OK;
+}
+
+template <typename T>
+int upload(s2l_setup* s, T** dst, const T* src, size_t count)
+{
+    RET_IF(dev_alloc(s, reinterpret_cast<void**>(dst), count * sizeof(T)));
+    if (count) CUDA_OK(s, cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+    return S2L_OK;
+}
+
+template <typename T>
+int upload(s2l_setup* s, T** dst, const std::vector<T>& v)
+{
+    return upload(s, dst, v.data(), v.size());
+}
+
+int alloc_doubles(s2l_setup* s, double** p, size_t count)
+{
+    return dev_alloc(s, reinterpret_cast<void**>(p), count * sizeof(double));
+}
+
+// level schedule of a triangular CSR (lower: forward; upper: backward)
+void build_sched(const HostCsr& M, int n, bool lower, bool unit_diag, Sched& out, std::string& err)
+{
+    std::vector<int32_t> level(n, 0);
+    std::vector<double> diag(n, 1.0);
+    std::vector<int64_t> offcnt(n, 0);
+    auto visit = [&](int r) {
+        int lv = 0;
+        for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
+            const int c = M.ci[e];
+            if (c == r) {
+                diag[r] = M.v[e];
+                continue;
+            }
+            if (lower ? (c > r) : (c < r)) continue;  // wrong triangle: ignored (checked by caller)
+            lv = std::max(lv, level[c] + 1);
+            ++offcnt[r];
+        }
+        level[r] = lv;
+    };
+    if (lower)
+        for (int r = 0; r < n; ++r) visit(r);
+    else
+        for (int r = n - 1; r >= 0; --r) visit(r);
+    int nlev = 0;
+    for (int r = 0; r < n; ++r) nlev = std::max(nlev, level[r] + 1);
+    if (n == 0) nlev = 0;
+    std::vector<int32_t> cnt(nlev + 1, 0);
+    for (int r = 0; r < n; ++r) ++cnt[level[r] + 1];
+    for (int l = 0; l < nlev; ++l) cnt[l + 1] += cnt[l];
+    out.lvl.assign(cnt.begin(), cnt.end());
+    std::vector<int32_t> next(cnt.begin(), cnt.end() - 1);
+    out.rows.assign(n, 0);
+    if (lower) {
+        for (int r = 0; r < n; ++r) out.rows[next[level[r]]++] = r;
+    } else {
+        for (int r = n - 1; r >= 0; --r) out.rows[next[level[r]]++] = r;
+    }
+    out.ptr.assign(n + 1, 0);
+    for (int p = 0; p < n; ++p) out.ptr[p + 1] = out.ptr[p] + offcnt[out.rows[p]];
+    out.col.resize(out.ptr[n]);
+    out.val.resize(out.ptr[n]);
+    out.dinv.resize(n);
+    for (int p = 0; p < n; ++p) {
+        const int r = out.rows[p];
+        int64_t q = out.ptr[p];
+        for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
+            const int c = M.ci[e];
+            if (c == r || (lower ? (c > r) : (c < r))) continue;
+            out.col[q] = c;
+            out.val[q] = M.v[e];
+            ++q;
+        }
+        const double dg = unit_diag ? 1.0 : diag[r];
+        if (dg == 0.0 || !std::isfinite(dg)) {
+            err = "zero or non-finite diagonal in a triangular factor";
+            return;
+        }
+        out.dinv[p] = 1.0 / dg;
+    }
+    // group width per level
+    out.mode.assign(nlev + 1, 1);
+    for (int l = 0; l < nlev; ++l) {
+        const int a = out.lvl[l], b = out.lvl[l + 1];
+        const int64_t nz = out.ptr[b] - out.ptr[a];
+        const int rows = b - a;
+        const double avg = rows ? (double)nz / rows : 0.0;
+        int G = 1;
+        while (G < 32 && G < avg) G <<= 1;
+        if (rows * 32 <= S2L_BS_SOLVE / 2 && avg >= 128.0) G = S2L_MODE_CTA;
+        out.mode[l] = (int8_t)G;
+    }
+}
+
+// transpose of a lower CSR (values scaled by rowscale[c] of the result rows if given)
+HostCsr transpose_lower(const HostCsr& L, int n, const std::vector<double>* rowscale)
+{
+    HostCsr U;
+    U.rp.assign(n + 1, 0);
+    for (int r = 0; r < n; ++r)
+        for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e) ++U.rp[L.ci[e] + 1];
+    for (int i = 0; i < n; ++i) U.rp[i + 1] += U.rp[i];
+    U.ci.resize(U.rp[n]);
+    U.v.resize(U.rp[n]);
+    std::vector<int64_t> nx(U.rp.begin(), U.rp.end() - 1);
+    for (int r = 0; r < n; ++r)
+        for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e) {
+            const int c = L.ci[e];
+            const int64_t q = nx[c]++;
+            U.ci[q] = r;
+            U.v[q] = L.v[e] * (rowscale ? (*rowscale)[c] : 1.0);
+        }
+    return U;
+}
+
+// dense inverse by LU with partial pivoting (FP64); false if singular
+bool dense_inverse(std::vector<double>& A, int n, std::vector<double>& Ainv)
+{
+    std::vector<int> piv(n);
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        double best = std::fabs(A[(size_t)k * n + k]);
+        for (int i = k + 1; i < n; ++i) {
+            const double v = std::fabs(A[(size_t)i * n + k]);
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (best == 0.0 || !std::isfinite(best)) return false;
+        piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < n; ++j) std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
+        const double inv = 1.0 / A[(size_t)k * n + k];
+        for (int i = k + 1; i < n; ++i) {
+            double& lik = A[(size_t)i * n + k];
+            lik *= inv;
+            if (lik != 0.0) {
+                const double* rk = &A[(size_t)k * n];
+                double* ri = &A[(size_t)i * n];
+                for (int j = k + 1; j < n; ++j) ri[j] -= lik * rk[j];
+            }
+        }
+    }
+    Ainv.assign((size_t)n * n, 0.0);
+    std::vector<double> col(n);
+    for (int j = 0; j < n; ++j) {
+        std::fill(col.begin(), col.end(), 0.0);
+        col[j] = 1.0;
+        // apply the row interchanges
+        for (int k = 0; k < n; ++k) std::swap(col[k], col[piv[k]]);
+        for (int i = 0; i < n; ++i) {
+            double s = col[i];
+            for (int k = 0; k < i; ++k) s -= A[(size_t)i * n + k] * col[k];
+            col[i] = s;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double s = col[i];
+            for (int k = i + 1; k < n; ++k) s -= A[(size_t)i * n + k] * col[k];
+            col[i] = s / A[(size_t)i * n + i];
+        }
+        for (int i = 0; i < n; ++i) Ainv[(size_t)i * n + j] = col[i];
+    }
+    return true;
+}
+
+template <typename Real>
+int upload_real(s2l_setup* s, void** dst, const std::vector<double>& v)
+{
+    std::vector<Real> t(v.begin(), v.end());
+    Real* p = nullptr;
+    RET_IF(upload(s, &p, t));
+    *dst = p;
+    return S2L_OK;
+}
+
+// ------------------------------------------------------------------------------ profiling
+void prof_begin(s2l_setup* s, int cls, cudaEvent_t* a)
+{
+    if (!s->prof) return;
+    if (s->pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->pool.push_back(e);
+    }
+    *a = s->pool.back();
+    s->pool.pop_back();
+    cudaEventRecord(*a, s->stream);
+    (void)cls;
+}
+
+void prof_end(s2l_setup* s, int cls, cudaEvent_t a)
+{
+    if (!s->prof) return;
+    if (s->pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->pool.push_back(e);
+    }
+    cudaEvent_t b = s->pool.back();
+    s->pool.pop_back();
+    cudaEventRecord(b, s->stream);
+    s->evs.push_back({cls, a, b});
+}
+
+void prof_drain(s2l_setup* s)
+{
+    if (s->evs.empty()) return;
+    cudaStreamSynchronize(s->stream);
+    for (auto& e : s->evs) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+            s->acc_ms[e.cls] += ms;
+            s->acc_n[e.cls] += 1;
+        }
+        s->pool.push_back(e.a);
+        s->pool.push_back(e.b);
+    }
+    s->evs.clear();
+}
+
+struct Prof {
+    s2l_setup* s;
+    int cls;
+    cudaEvent_t a{};
+    Prof(s2l_setup* s_, int c) : s(s_), cls(c) { prof_begin(s, cls, &a); }
+    ~Prof() { prof_end(s, cls, a); }
+};
+
+// ------------------------------------------------------------------------------ solve-phase pieces
+int run_local_solve(s2l_setup* s, const double* in, const double* base, double* out, int mode, int only_sub,
+                    const double* local_in)
+{
+    Prof pr(s, PC_SOLVE);
+    const int nb = only_sub >= 0 ? 1 : s->nsub;
+    int32_t* sub_list = nullptr;
+    if (only_sub >= 0) sub_list = reinterpret_cast<int32_t*>(s->d_red + 500);  // scratch slot for one index
+    if (only_sub >= 0) {
+        int32_t v = only_sub;
+        CUDA_OK(s, cudaMemcpyAsync(sub_list, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+    }
+    cudaError_t e;
+    if (s->real == S2L_REAL_F32) {
+        SolveArgs<float> a{};
+        a.subs = s->d_subs;
+        a.sub_list = sub_list;
+        for (int f = 0; f < 2; ++f)
+            a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const float*)s->d_val[f], (const float*)s->d_dinv[f]};
+        a.lvl_pos = s->d_lvl;
+        a.lvl_mode = s->d_mode;
+        a.gin = s->d_gin;
+        a.pin = s->d_pin;
+        a.gout = s->d_gout;
+        a.in = mode == 2 ? local_in : in;
+        a.base = base;
+        a.out = out;
+        a.ylocal = s->d_ylocal;
+        a.xscratch = (float*)s->d_xscratch;
+        a.mode = mode;
+        e = launch_local_solve<float>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
+    } else {
+        SolveArgs<double> a{};
+        a.subs = s->d_subs;
+        a.sub_list = sub_list;
+        for (int f = 0; f < 2; ++f)
+            a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const double*)s->d_val[f],
+                      (const double*)s->d_dinv[f]};
+        a.lvl_pos = s->d_lvl;
+        a.lvl_mode = s->d_mode;
+        a.gin = s->d_gin;
+        a.pin = s->d_pin;
+        a.gout = s->d_gout;
+        a.in = mode == 2 ? local_in : in;
+        a.base = base;
+        a.out = out;
+        a.ylocal = s->d_ylocal;
+        a.xscratch = (double*)s->d_xscratch;
+        a.mode = mode;
+        e = launch_local_solve<double>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
+    }
+    if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
+    return S2L_OK;
+}
+
+// z = M1^-1 in (+ base), M1 = RAS or ASM
+int one_level(s2l_setup* s, const double* in, const double* base, double* out)
+{
+    if (s->pou == S2L_POU_BOOLEAN && s->one_level == S2L_ONE_LEVEL_RAS) return run_local_solve(s, in, base, out, 0, -1, nullptr);
+    RET_IF(run_local_solve(s, in, nullptr, nullptr, 1, -1, nullptr));
+    Prof pr(s, PC_COMBINE);
+    launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, s->one_level == S2L_ONE_LEVEL_RAS ? s->d_cp_w : nullptr,
+                   s->d_ylocal, base, out);
+    return S2L_OK;
+}
+
+// x0 = R0^T E^-1 R0 r
+int coarse_apply(s2l_setup* s, const double* r, double* x0)
+{
+    Prof pr(s, PC_COARSE);
+    const int boolean = s->pou == S2L_POU_BOOLEAN;
+    launch_coarse_restrict(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+                           boolean, r, s->mmax, s->d_cpart);
+    launch_coarse_reduce(s->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, s->d_cpart, s->d_c);
+    launch_dense_gemv(s->stream, (int)s->n0, s->d_Einv, s->d_c, s->d_y);
+    launch_coarse_prolong(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
+                          s->d_y, x0, s->d_plocal);
+    if (!boolean) launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, s->d_plocal, nullptr, x0);
+    return S2L_OK;
+}
+
+int spmv_dev(s2l_setup* s, const double* x, double* y, const double* b, bool with_norm)
+{
+    Prof pr(s, PC_SPMV);
+    launch_spmv(s->stream, s->n, s->d_rp, s->d_ci, s->d_av, x, y, b, with_norm ? s->d_part : nullptr,
+                s->d_red + 256, s->tpr);
+    return S2L_OK;
+}
+
+// z = M^-1 r (two-level Schwarz, src/preconditioner/two_level_schwarz.cpp:134-163); r and z distinct
+int apply_dev(s2l_setup* s, const double* r, double* z)
+{
+    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return one_level(s, r, nullptr, z);
+    RET_IF(coarse_apply(s, r, s->d_x0));
+    if (s->coarse == S2L_COARSE_ADDITIVE) return one_level(s, r, s->d_x0, z);
+    RET_IF(spmv_dev(s, s->d_x0, s->d_w, r, false));  // w = r - A x0
+    return one_level(s, s->d_w, s->d_x0, z);
+}
+
+int check_ready(s2l_setup* s)
+{
+    if (!s) return S2L_ERR_BADARG;
+    if (!s->ended) return s->fail(S2L_ERR_STATE, "setup_end() was not called");
+    return S2L_OK;
+}
+
+// host/device staging of a global vector argument
+int stage_in(s2l_setup* s, const double* p, int kind, int64_t count, double* tmp, const double** dev)
+{
+    if (kind == S2L_PTR_DEVICE) {
+        *dev = p;
+        return S2L_OK;
+    }
+    if (kind != S2L_PTR_HOST) return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    CUDA_OK(s, cudaMemcpyAsync(tmp, p, count * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    *dev = tmp;
+    return S2L_OK;
+}
+
+int finish_out(s2l_setup* s, double* dst, const double* dev, int kind, int64_t count)
+{
+    if (kind == S2L_PTR_HOST)
+        CUDA_OK(s, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    else if (dst != dev)
+        CUDA_OK(s, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    CUDA_OK(s, cudaGetLastError());
+    return S2L_OK;
+}
+
+int ensure_krylov(s2l_setup* s, int m, bool flexible)
+{
+    if (s->kr_m >= m && (!flexible || s->kr_flex)) return S2L_OK;
+    if (m + 1 > S2L_MAX_RED_COLS - 1) return s->fail(S2L_ERR_BADARG, "restart too large (max 120)");
+    const size_t n = (size_t)s->n;
+    RET_IF(alloc_doubles(s, &s->d_V_kr, n * (m + 1)));
+    if (flexible) RET_IF(alloc_doubles(s, &s->d_Z_kr, n * m));
+    if (s->kr_m < 0) {
+        RET_IF(alloc_doubles(s, &s->d_r, n));
+        RET_IF(alloc_doubles(s, &s->d_z, n));
+        RET_IF(alloc_doubles(s, &s->d_kw, n));
+        RET_IF(alloc_doubles(s, &s->d_b, n));
+        RET_IF(alloc_doubles(s, &s->d_xk, n));
+        RET_IF(alloc_doubles(s, &s->d_u, n));
+        RET_IF(alloc_doubles(s, &s->d_coef, S2L_MAX_RED_COLS));
+    }
+    s->kr_m = m;
+    s->kr_flex = s->kr_flex || flexible;
+    return S2L_OK;
+}
+
+int read_red(s2l_setup* s, int off, int count)
+{
+    CUDA_OK(s, cudaMemcpyAsync(s->h_red + off, s->d_red + off, count * sizeof(double), cudaMemcpyDeviceToHost,
+                               s->stream));
+    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    return S2L_OK;
+}
+
+int norm2_dev(s2l_setup* s, const double* x, double* out_host)
+{
+    {
+        Prof pr(s, PC_VEC);
+        launch_dot2(s->stream, s->n, x, x, nullptr, s->d_part, s->d_red + 256);
+    }
+    RET_IF(read_red(s, 256, 1));
+    *out_host = std::sqrt(s->h_red[256]);
+    return S2L_OK;
+}
+
+}  // namespace
+
+// ================================================================================= C ABI
+extern "C" {
+
+int s2l_gpu_create(int device, size_t hbm_budget_bytes, s2l_ctx** ctx)
+{
+    if (!ctx) return S2L_ERR_BADARG;
+    *ctx = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return S2L_ERR_CUDA;
+    if (device < 0 || device >= count) return S2L_ERR_BADARG;
+    if (cudaSetDevice(device) != cudaSuccess) return S2L_ERR_CUDA;
+    auto* c = new s2l_ctx;
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    *ctx = c;
+    return S2L_OK;
+}
+
+int s2l_gpu_destroy(s2l_ctx* ctx)
+{
+    delete ctx;
+    return S2L_OK;
+}
+
+const char* s2l_gpu_last_error(const s2l_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int s2l_gpu_setup_begin(s2l_ctx* ctx, int64_t n, int nsub, int one_level, int coarse, int pou, s2l_setup** out)
+{
+    if (!ctx || !out) return S2L_ERR_BADARG;
+    *out = nullptr;
+    auto bad = [&](const char* m) {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        ctx->err = m;
+        return S2L_ERR_BADARG;
+    };
+    if (n <= 0 || n >= (int64_t)INT32_MAX) return bad("n must be in [1, 2^31)");
+    if (nsub <= 0) return bad("nsub must be positive");
+    if (one_level != S2L_ONE_LEVEL_RAS && one_level != S2L_ONE_LEVEL_ASM) return bad("unknown one-level variant");
+    if (coarse < S2L_COARSE_NONE || coarse > S2L_COARSE_DEFLATED) return bad("unknown coarse correction");
+    if (pou != S2L_POU_BOOLEAN && pou != S2L_POU_MULTIPLICITY) return bad("unknown partition of unity");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return S2L_ERR_CUDA;
+    auto* s = new s2l_setup;
+    s->ctx = ctx;
+    s->n = n;
+    s->nsub = nsub;
+    s->one_level = one_level;
+    s->coarse = coarse;
+    s->pou = pou;
+    s->hs.resize(nsub);
+    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return S2L_ERR_CUDA;
+    }
+    s->stream = s->own_stream;
+    *out = s;
+    return S2L_OK;
+}
+
+int s2l_gpu_set_matrix(s2l_setup* s, const int64_t* rowptr, const int64_t* col, const double* val)
+{
+    if (!s || !rowptr || !col || !val) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "set_matrix after setup_end");
+    const int64_t n = s->n;
+    if (rowptr[0] != 0) return s->fail(S2L_ERR_BADARG, "rowptr[0] must be 0");
+    const int64_t nnz = rowptr[n];
+    if (nnz < 0 || nnz >= (int64_t)INT32_MAX) return s->fail(S2L_ERR_BADARG, "nnz must be in [0, 2^31)");
+    s->A.rp.assign(rowptr, rowptr + n + 1);
+    s->A.ci.resize(nnz);
+    for (int64_t r = 0; r < n; ++r) {
+        if (rowptr[r + 1] < rowptr[r]) return s->fail(S2L_ERR_BADARG, "rowptr not monotone");
+        for (int64_t e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+            if (col[e] < 0 || col[e] >= n) return s->fail(S2L_ERR_BADARG, "column index out of range");
+            s->A.ci[e] = (int32_t)col[e];
+        }
+    }
+    s->A.v.assign(val, val + nnz);
+    s->have_A = true;
+    return S2L_OK;
+}
+
+int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t* ghosts,
+                          const double* D, int factor_kind, int real_type, const int32_t* perm_in,
+                          const int32_t* perm_out, const int64_t* L_rowptr, const int32_t* L_col, const void* L_val,
+                          const int64_t* U_rowptr, const int32_t* U_col, const void* U_val, const void* ldlt_d,
+                          int m, const double* V)
+{
+    if (!s) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "add_subdomain after setup_end");
+    if (i < 0 || i >= s->nsub) return s->fail(S2L_ERR_BADARG, "subdomain index out of range");
+    if (n_owned <= 0 || n_ghost < 0) return s->fail(S2L_ERR_BADARG, "n_owned must be > 0 and n_ghost >= 0");
+    if (begin < 0 || begin + n_owned > s->n) return s->fail(S2L_ERR_BADARG, "owned range outside [0, n)");
+    if (real_type != S2L_REAL_F64 && real_type != S2L_REAL_F32) return s->fail(S2L_ERR_BADARG, "unknown real type");
+    if (s->real >= 0 && s->real != real_type)
+        return s->fail(S2L_ERR_BADARG, "all subdomains must store their factors in the same precision");
+    if (factor_kind < S2L_FACTOR_LU || factor_kind > S2L_FACTOR_LDLT) return s->fail(S2L_ERR_BADARG, "unknown factor kind");
+    if (!D || !perm_in || !perm_out || !L_rowptr || !L_col || !L_val || (n_ghost && !ghosts))
+        return s->fail(S2L_ERR_BADARG, "null array");
+    if (factor_kind == S2L_FACTOR_LU && (!U_rowptr || !U_col || !U_val)) return s->fail(S2L_ERR_BADARG, "LU needs U");
+    if (factor_kind == S2L_FACTOR_LDLT && !ldlt_d) return s->fail(S2L_ERR_BADARG, "LDLT needs d");
+    if (m < 0 || m > S2L_MAX_RED_COLS || (m > 0 && !V)) return s->fail(S2L_ERR_BADARG, "bad coarse basis (m <= 128)");
+    s->real = real_type;
+    HostSub& h = s->hs[i];
+    h = HostSub();
+    const int nl = n_owned + n_ghost;
+    h.begin = begin;
+    h.n_owned = n_owned;
+    h.n_ghost = n_ghost;
+    h.ghosts.assign(ghosts, ghosts + n_ghost);
+    for (int k = 0; k < n_ghost; ++k) {
+        if (ghosts[k] < 0 || ghosts[k] >= s->n) return s->fail(S2L_ERR_BADARG, "ghost id out of range");
+        if (ghosts[k] >= begin && ghosts[k] < begin + n_owned) return s->fail(S2L_ERR_BADARG, "ghost is an owned row");
+        if (k && ghosts[k] <= ghosts[k - 1]) return s->fail(S2L_ERR_BADARG, "ghosts must be sorted and unique");
+    }
+    h.D.assign(D, D + nl);
+    h.kind = factor_kind;
+    h.pin.assign(perm_in, perm_in + nl);
+    h.pout.assign(perm_out, perm_out + nl);
+    {
+        std::vector<char> seen(nl, 0), seen2(nl, 0);
+        for (int k = 0; k < nl; ++k) {
+            if (perm_in[k] < 0 || perm_in[k] >= nl || seen[perm_in[k]]) return s->fail(S2L_ERR_BADARG, "perm_in is not a permutation");
+            if (perm_out[k] < 0 || perm_out[k] >= nl || seen2[perm_out[k]]) return s->fail(S2L_ERR_BADARG, "perm_out is not a permutation");
+            seen[perm_in[k]] = seen2[perm_out[k]] = 1;
+        }
+    }
+    auto copy_csr = [&](HostCsr& dst, const int64_t* rp, const int32_t* ci, const void* v, bool lower) -> int {
+        if (rp[0] != 0) return s->fail(S2L_ERR_BADARG, "factor rowptr[0] must be 0");
+        dst.rp.assign(rp, rp + nl + 1);
+        const int64_t nz = rp[nl];
+        dst.ci.assign(ci, ci + nz);
+        dst.v.resize(nz);
+        if (real_type == S2L_REAL_F64)
+            std::copy((const double*)v, (const double*)v + nz, dst.v.begin());
+        else
+            std::copy((const float*)v, (const float*)v + nz, dst.v.begin());
+        for (int r = 0; r < nl; ++r) {
+            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "factor rowptr not monotone");
+            for (int64_t e = rp[r]; e < rp[r + 1]; ++e) {
+                const int c = ci[e];
+                if (c < 0 || c >= nl) return s->fail(S2L_ERR_BADARG, "factor column out of range");
+                if (lower ? c > r : c < r) return s->fail(S2L_ERR_BADARG, lower ? "L has an entry above the diagonal" : "U has an entry below the diagonal");
+            }
+        }
+        return S2L_OK;
+    };
+    RET_IF(copy_csr(h.L, L_rowptr, L_col, L_val, true));
+    if (factor_kind == S2L_FACTOR_LU) RET_IF(copy_csr(h.U, U_rowptr, U_col, U_val, false));
+    if (factor_kind == S2L_FACTOR_LDLT) {
+        h.d.resize(nl);
+        for (int k = 0; k < nl; ++k)
+            h.d[k] = real_type == S2L_REAL_F64 ? ((const double*)ldlt_d)[k] : ((const float*)ldlt_d)[k];
+    }
+    h.m = m;
+    if (m) h.V.assign(V, V + (size_t)nl * m);
+    h.set = true;
+    return S2L_OK;
+}
+
+int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E)
+{
+    if (!s) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "set_coarse after setup_end");
+    if (n0 < 0 || (n0 > 0 && (!offsets || !E))) return s->fail(S2L_ERR_BADARG, "bad coarse arguments");
+    if (n0 > 65536) return s->fail(S2L_ERR_BADARG, "coarse dimension too large for the dense inverse (max 65536)");
+    s->n0 = n0;
+    s->coff.assign(offsets, offsets + s->nsub + 1);
+    s->E.assign(E, E + (size_t)n0 * n0);
+    s->have_coarse = true;
+    return S2L_OK;
+}
+
+int s2l_gpu_setup_end(s2l_setup* s)
+{
+    if (!s) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "setup_end called twice");
+    if (!s->have_A) return s->fail(S2L_ERR_STATE, "set_matrix was not called");
+    if (cudaSetDevice(s->ctx->device) != cudaSuccess) return S2L_ERR_CUDA;
+    const int nsub = s->nsub;
+    // ---- ownership checks: contiguous ranges covering [0, n)
+    {
+        int64_t next = 0;
+        for (int i = 0; i < nsub; ++i) {
+            if (!s->hs[i].set) return s->fail(S2L_ERR_STATE, "subdomain " + std::to_string(i) + " was not added");
+            if (s->hs[i].begin != next) return s->fail(S2L_ERR_BADARG, "owned ranges must be contiguous in subdomain order");
+            next += s->hs[i].n_owned;
+        }
+        if (next != s->n) return s->fail(S2L_ERR_BADARG, "owned ranges do not cover [0, n)");
+    }
+    if (s->coarse != S2L_COARSE_NONE) {
+        if (!s->have_coarse) return s->fail(S2L_ERR_STATE, "set_coarse was not called");
+        if (s->coff[0] != 0 || s->coff[nsub] != s->n0) return s->fail(S2L_ERR_BADARG, "coarse offsets inconsistent with n0");
+        for (int i = 0; i < nsub; ++i)
+            if (s->coff[i + 1] - s->coff[i] != s->hs[i].m)
+                return s->fail(S2L_ERR_BADARG, "coarse offsets do not match the basis sizes");
+    }
+    const bool boolean = s->pou == S2L_POU_BOOLEAN;
+    s->need_copies = !(boolean && s->one_level == S2L_ONE_LEVEL_RAS);
+
+    // ---- global matrix
+    {
+        std::vector<int32_t> rp(s->n + 1);
+        for (int64_t r = 0; r <= s->n; ++r) rp[r] = (int32_t)s->A.rp[r];
+        s->nnz = s->A.rp[s->n];
+        RET_IF(upload(s, &s->d_rp, rp));
+        RET_IF(upload(s, &s->d_ci, s->A.ci));
+        RET_IF(upload(s, &s->d_av, s->A.v));
+        const double avg = (double)s->nnz / (double)s->n;
+        s->tpr = avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32));
+    }
+
+    // ---- per-subdomain schedules and index maps
+    s->h_subs.resize(nsub);
+    int64_t loc = 0, ent[2] = {0, 0}, lvl_total = 0;
+    std::vector<Sched> sch[2];
+    sch[0].resize(nsub);
+    sch[1].resize(nsub);
+    std::vector<int32_t> gin, pin, gout, l2g;
+    std::vector<double> Dall;
+    int max_nl = 0;
+    for (int i = 0; i < nsub; ++i) {
+        HostSub& h = s->hs[i];
+        const int nl = h.n_local();
+        max_nl = std::max(max_nl, nl);
+        std::string err;
+        const bool unit = h.kind != S2L_FACTOR_LLT;
+        build_sched(h.L, nl, true, unit, sch[0][i], err);
+        if (err.empty()) {
+            if (h.kind == S2L_FACTOR_LU) {
+                build_sched(h.U, nl, false, false, sch[1][i], err);
+            } else {
+                HostCsr U = transpose_lower(h.L, nl, nullptr);
+                if (h.kind == S2L_FACTOR_LDLT) {
+                    // U = diag(d) L^T: scale row r by d[r]; the unit diagonal of L becomes d[r]
+                    for (int r = 0; r < nl; ++r)
+                        for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) U.v[e] = (U.ci[e] == r) ? h.d[r] : U.v[e] * h.d[r];
+                    bool has_diag_missing = false;
+                    for (int r = 0; r < nl && !has_diag_missing; ++r) {
+                        bool f = false;
+                        for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) f = f || U.ci[e] == r;
+                        has_diag_missing = !f;
+                    }
+                    if (has_diag_missing) err = "LDLT: L must store its unit diagonal";
+                }
+                if (err.empty()) build_sched(U, nl, false, false, sch[1][i], err);
+            }
+        }
+        if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
+        DevSub d{};
+        d.begin = h.begin;
+        d.loc_off = loc;
+        d.n_owned = h.n_owned;
+        d.n_local = nl;
+        for (int f = 0; f < 2; ++f) {
+            d.lvl_off[f] = lvl_total;
+            d.nlev[f] = (int)sch[f][i].lvl.size() - 1;
+            lvl_total += sch[f][i].lvl.size();
+        }
+        d.m = h.m;
+        d.v_rows = boolean ? h.n_owned : nl;
+        d.c_off = s->coarse != S2L_COARSE_NONE ? s->coff[i] : 0;
+        s->h_subs[i] = d;
+        for (int j = 0; j < nl; ++j) {
+            const int64_t g = j < h.n_owned ? h.begin + j : h.ghosts[j - h.n_owned];
+            l2g.push_back((int32_t)g);
+        }
+        for (int k = 0; k < nl; ++k) {
+            gin.push_back(l2g[loc + h.pin[k]]);
+            pin.push_back(h.pin[k]);
+            gout.push_back(h.pout[k]);
+        }
+        Dall.insert(Dall.end(), h.D.begin(), h.D.end());
+        loc += nl;
+        ent[0] += sch[0][i].col.size();
+        ent[1] += sch[1][i].col.size();
+    }
+    s->nloc = loc;
+    // concatenate the schedules
+    double bytes = 0.0;
+    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    for (int f = 0; f < 2; ++f) {
+        std::vector<int32_t> rows, col;
+        std::vector<int64_t> ptr;
+        std::vector<double> val, dinv;
+        rows.reserve(loc);
+        ptr.reserve(loc + 1);
+        col.reserve(ent[f]);
+        val.reserve(ent[f]);
+        dinv.reserve(loc);
+        int64_t e0 = 0;
+        for (int i = 0; i < nsub; ++i) {
+            const Sched& q = sch[f][i];
+            rows.insert(rows.end(), q.rows.begin(), q.rows.end());
+            for (size_t p = 0; p + 1 < q.ptr.size(); ++p) ptr.push_back(e0 + q.ptr[p]);
+            col.insert(col.end(), q.col.begin(), q.col.end());
+            val.insert(val.end(), q.val.begin(), q.val.end());
+            dinv.insert(dinv.end(), q.dinv.begin(), q.dinv.end());
+            e0 += q.col.size();
+            bytes += (double)q.col.size() * (rs + 4) + (double)q.rows.size() * (4 + 8 + rs);
+        }
+        ptr.push_back(e0);
+        RET_IF(upload(s, &s->d_rows[f], rows));
+        RET_IF(upload(s, &s->d_ptr[f], ptr));
+        RET_IF(upload(s, &s->d_col[f], col));
+        if (s->real == S2L_REAL_F32) {
+            RET_IF(upload_real<float>(s, &s->d_val[f], val));
+            RET_IF(upload_real<float>(s, &s->d_dinv[f], dinv));
+        } else {
+            RET_IF(upload_real<double>(s, &s->d_val[f], val));
+            RET_IF(upload_real<double>(s, &s->d_dinv[f], dinv));
+        }
+    }
+    {
+        std::vector<int32_t> lvl;
+        std::vector<int8_t> mode;
+        lvl.reserve(lvl_total);
+        mode.reserve(lvl_total);
+        for (int i = 0; i < nsub; ++i)
+            for (int f = 0; f < 2; ++f) {
+                // lvl_off[f] of subdomain i was assigned in (i, f) order
+                lvl.insert(lvl.end(), sch[f][i].lvl.begin(), sch[f][i].lvl.end());
+                mode.insert(mode.end(), sch[f][i].mode.begin(), sch[f][i].mode.end());
+            }
+        // re-assign offsets in the (i, f) order used just above
+        int64_t off = 0;
+        for (int i = 0; i < nsub; ++i)
+            for (int f = 0; f < 2; ++f) {
+                s->h_subs[i].lvl_off[f] = off;
+                off += sch[f][i].lvl.size();
+            }
+        RET_IF(upload(s, &s->d_lvl, lvl));
+        RET_IF(upload(s, &s->d_mode, mode));
+    }
+    // gather, output and owned traffic of one launch
+    for (int i = 0; i < nsub; ++i) {
+        const HostSub& h = s->hs[i];
+        bytes += (double)h.n_local() * (4 + 8) + (double)h.n_owned * (4 + 8 + 8);
+    }
+    s->solve_bytes = bytes;
+    RET_IF(upload(s, &s->d_gin, gin));
+    RET_IF(upload(s, &s->d_pin, pin));
+    RET_IF(upload(s, &s->d_gout, gout));
+    RET_IF(upload(s, &s->d_l2g, l2g));
+    RET_IF(upload(s, &s->d_D, Dall));
+
+    // ---- copies of every global row in the local space (owner first, then ghosts by subdomain)
+    if (s->need_copies) {
+        std::vector<int64_t> cnt(s->n + 1, 0);
+        for (int64_t p = 0; p < loc; ++p) ++cnt[l2g[p] + 1];
+        for (int64_t g = 0; g < s->n; ++g) cnt[g + 1] += cnt[g];
+        std::vector<int32_t> pos(loc);
+        std::vector<double> w(loc);
+        std::vector<int64_t> nx(cnt.begin(), cnt.end() - 1);
+        for (int i = 0; i < nsub; ++i) {  // owned copies first
+            const DevSub& d = s->h_subs[i];
+            for (int j = 0; j < d.n_owned; ++j) {
+                const int64_t q = nx[d.begin + j]++;
+                pos[q] = (int32_t)(d.loc_off + j);
+                w[q] = Dall[d.loc_off + j];
+            }
+        }
+        for (int i = 0; i < nsub; ++i) {
+            const DevSub& d = s->h_subs[i];
+            for (int j = d.n_owned; j < d.n_local; ++j) {
+                const int64_t g = l2g[d.loc_off + j];
+                const int64_t q = nx[g]++;
+                pos[q] = (int32_t)(d.loc_off + j);
+                w[q] = Dall[d.loc_off + j];
+            }
+        }
+        RET_IF(upload(s, &s->d_cp_ptr, cnt));
+        RET_IF(upload(s, &s->d_cp_pos, pos));
+        RET_IF(upload(s, &s->d_cp_w, w));
+    }
+
+    // ---- coarse basis (row-major, owned rows for the boolean PoU) and E^-1
+    if (s->coarse != S2L_COARSE_NONE && s->n0 > 0) {
+        std::vector<double> Vr;
+        std::vector<int32_t> tsub, trow0, tnrow, tfirst(nsub + 1, 0);
+        int64_t voff = 0;
+        int mmax = 0;
+        for (int i = 0; i < nsub; ++i) {
+            HostSub& h = s->hs[i];
+            DevSub& d = s->h_subs[i];
+            const int nl = h.n_local();
+            d.v_off = voff;
+            mmax = std::max(mmax, h.m);
+            for (int l = 0; l < d.v_rows; ++l)
+                for (int c = 0; c < h.m; ++c) Vr.push_back(h.V[(size_t)c * nl + l]);
+            voff += (int64_t)d.v_rows * h.m;
+            tfirst[i] = (int32_t)tsub.size();
+            if (h.m > 0)
+                for (int r0 = 0; r0 < d.v_rows; r0 += S2L_TILE_ROWS) {
+                    tsub.push_back(i);
+                    trow0.push_back(r0);
+                    tnrow.push_back(std::min(S2L_TILE_ROWS, d.v_rows - r0));
+                }
+        }
+        tfirst[nsub] = (int32_t)tsub.size();
+        // subdomains with m = 0 contribute no tile; prolong must still zero their rows: add zero tiles
+        for (int i = 0; i < nsub; ++i) {
+            if (s->hs[i].m > 0) continue;
+            for (int r0 = 0; r0 < s->h_subs[i].v_rows; r0 += S2L_TILE_ROWS) {
+                tsub.push_back(i);
+                trow0.push_back(r0);
+                tnrow.push_back(std::min(S2L_TILE_ROWS, s->h_subs[i].v_rows - r0));
+            }
+        }
+        s->ntiles = (int)tsub.size();
+        s->mmax = std::max(mmax, 1);
+        RET_IF(upload(s, &s->d_V, Vr));
+        RET_IF(upload(s, &s->d_t_sub, tsub));
+        RET_IF(upload(s, &s->d_t_row0, trow0));
+        RET_IF(upload(s, &s->d_t_nrow, tnrow));
+        RET_IF(upload(s, &s->d_t_first, tfirst));
+        std::vector<double> Ecopy = s->E, Einv;
+        if (!dense_inverse(Ecopy, (int)s->n0, Einv)) return s->fail(S2L_ERR_NUMERIC, "coarse matrix E is singular");
+        RET_IF(upload(s, &s->d_Einv, Einv));
+        RET_IF(alloc_doubles(s, &s->d_cpart, (size_t)s->ntiles * s->mmax));
+        RET_IF(alloc_doubles(s, &s->d_c, s->n0));
+        RET_IF(alloc_doubles(s, &s->d_y, s->n0));
+    }
+    RET_IF(upload(s, &s->d_subs, s->h_subs));
+
+    // ---- work vectors
+    RET_IF(alloc_doubles(s, &s->d_ylocal, loc));
+    RET_IF(alloc_doubles(s, &s->d_plocal, loc));
+    RET_IF(alloc_doubles(s, &s->d_x0, s->n));
+    RET_IF(alloc_doubles(s, &s->d_w, s->n));
+    RET_IF(alloc_doubles(s, &s->d_in, std::max<int64_t>(s->n, max_nl)));
+    RET_IF(alloc_doubles(s, &s->d_out, std::max<int64_t>(s->n, max_nl)));
+    RET_IF(alloc_doubles(s, &s->d_part, (size_t)S2L_NB_RED * S2L_MAX_RED_COLS));
+    RET_IF(alloc_doubles(s, &s->d_red, 512));
+    CUDA_OK(s, cudaMallocHost(&s->h_red, 512 * sizeof(double)));
+    const size_t smem = (size_t)max_nl * rs;
+    const size_t smem_cap = 227 * 1024 - 1024;
+    if (smem <= smem_cap) {
+        s->smem_bytes = smem;
+    } else {
+        s->smem_bytes = 0;
+        RET_IF(dev_alloc(s, &s->d_xscratch, (size_t)loc * rs));
+    }
+    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    // host staging no longer needed
+    s->A = HostCsr();
+    for (auto& h : s->hs) {
+        h.L = HostCsr();
+        h.U = HostCsr();
+        h.V.clear();
+        h.V.shrink_to_fit();
+    }
+    s->ended = true;
+    return S2L_OK;
+}
+
+int s2l_gpu_setup_destroy(s2l_setup* s)
+{
+    if (!s) return S2L_OK;
+    cudaSetDevice(s->ctx->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    prof_drain(s);
+    for (void* p : s->allocs) cudaFree(p);
+    {
+        std::lock_guard<std::mutex> g(s->ctx->mu);
+        s->ctx->used -= std::min(s->ctx->used, s->bytes);
+    }
+    if (s->h_red) cudaFreeHost(s->h_red);
+    for (auto e : s->pool) cudaEventDestroy(e);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+    return S2L_OK;
+}
+
+int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
+{
+    if (!s || !bytes) return S2L_ERR_BADARG;
+    *bytes = s->bytes;
+    return S2L_OK;
+}
+
+int s2l_gpu_set_stream(s2l_setup* s, void* stream)
+{
+    if (!s) return S2L_ERR_BADARG;
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return S2L_OK;
+}
+
+int s2l_gpu_profile_enable(s2l_setup* s, int on)
+{
+    if (!s) return S2L_ERR_BADARG;
+    prof_drain(s);
+    for (int c = 0; c < PC_N; ++c) {
+        s->acc_ms[c] = 0.0;
+        s->acc_n[c] = 0;
+    }
+    s->prof = on != 0;
+    return S2L_OK;
+}
+
+int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launches)
+{
+    if (!s || !name || !ms || !launches) return S2L_ERR_BADARG;
+    prof_drain(s);
+    if (std::strcmp(name, "all") == 0) {
+        *ms = 0;
+        *launches = 0;
+        for (int c = 0; c < PC_N; ++c) {
+            *ms += s->acc_ms[c];
+            *launches += s->acc_n[c];
+        }
+        return S2L_OK;
+    }
+    for (int c = 0; c < PC_N; ++c)
+        if (std::strcmp(name, kProfNames[c]) == 0) {
+            *ms = s->acc_ms[c];
+            *launches = s->acc_n[c];
+            return S2L_OK;
+        }
+    return s->fail(S2L_ERR_BADARG, std::string("unknown profile class ") + name);
+}
+
+int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes)
+{
+    if (!s || !bytes) return S2L_ERR_BADARG;
+    *bytes = s->solve_bytes;
+    return S2L_OK;
+}
+
+// ------------------------------------------------------------------------------ solve-phase calls
+int s2l_gpu_spmv(s2l_setup* s, const double* x, double* y, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!x || !y) return s->fail(S2L_ERR_BADARG, "null vector");
+    const double* dx;
+    RET_IF(stage_in(s, x, ptr_kind, s->n, s->d_in, &dx));
+    double* dy = ptr_kind == S2L_PTR_DEVICE ? y : s->d_out;
+    RET_IF(spmv_dev(s, dx, dy, nullptr, false));
+    return finish_out(s, y, dy, ptr_kind, s->n);
+}
+
+int s2l_gpu_local_solve(s2l_setup* s, int i, const double* b_local, double* x_local, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (i < 0 || i >= s->nsub) return s->fail(S2L_ERR_BADARG, "subdomain index out of range");
+    if (!b_local || !x_local) return s->fail(S2L_ERR_BADARG, "null vector");
+    const int nl = s->h_subs[i].n_local;
+    const double* db;
+    RET_IF(stage_in(s, b_local, ptr_kind, nl, s->d_in, &db));
+    double* dx = ptr_kind == S2L_PTR_DEVICE ? x_local : s->d_out;
+    RET_IF(run_local_solve(s, nullptr, nullptr, dx, 2, i, db));
+    return finish_out(s, x_local, dx, ptr_kind, nl);
+}
+
+int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!r || !x0) return s->fail(S2L_ERR_BADARG, "null vector");
+    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return s->fail(S2L_ERR_STATE, "no coarse space");
+    const double* dr;
+    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
+    double* dx = ptr_kind == S2L_PTR_DEVICE ? x0 : s->d_out;
+    RET_IF(coarse_apply(s, dr, dx));
+    return finish_out(s, x0, dx, ptr_kind, s->n);
+}
+
+int s2l_gpu_one_level_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!r || !z) return s->fail(S2L_ERR_BADARG, "null vector");
+    if (r == z) return s->fail(S2L_ERR_BADARG, "r and z must not alias");
+    const double* dr;
+    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
+    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : s->d_out;
+    RET_IF(one_level(s, dr, nullptr, dz));
+    return finish_out(s, z, dz, ptr_kind, s->n);
+}
+
+int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!r || !z) return s->fail(S2L_ERR_BADARG, "null vector");
+    if (r == z) return s->fail(S2L_ERR_BADARG, "r and z must not alias");
+    const double* dr;
+    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
+    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : s->d_out;
+    RET_IF(apply_dev(s, dr, dz));
+    return finish_out(s, z, dz, ptr_kind, s->n);
+}
+
+// Restarted right-preconditioned GMRES(m) with CGS2 (src/solver/gmres.cpp:18-161); flexible variant
+// keeps Z_j = M^-1 v_j and updates x += Z y instead of x += M^-1 (V y).
+int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                  s2l_result* res)
+{
+    RET_IF(check_ready(s));
+    if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
+    if (o->restart < 1 || o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
+    const int m = o->restart;
+    const bool flex = o->flexible != 0;
+    RET_IF(ensure_krylov(s, m, flex));
+    const int64_t n = s->n;
+    cudaStream_t st = s->stream;
+    double* V = s->d_V_kr;
+    double* Z = s->d_Z_kr;
+    const double* db;
+    if (ptr_kind == S2L_PTR_HOST) {
+        CUDA_OK(s, cudaMemcpyAsync(s->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        db = s->d_b;
+    } else if (ptr_kind == S2L_PTR_DEVICE) {
+        db = b;
+        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+        return s->fail(S2L_ERR_BADARG, "bad ptr_kind");
+    }
+    double* dx = s->d_xk;
+    res->converged = 0;
+    res->breakdown = 0;
+    res->iterations = 0;
+    res->restarts = 0;
+    res->history_len = 0;
+    auto hist = [&](double v) {
+        if (res->history && res->history_len < o->history_cap) res->history[res->history_len] = v;
+        if (res->history_len < o->history_cap) ++res->history_len;
+    };
+    double bnorm = 0.0;
+    RET_IF(norm2_dev(s, db, &bnorm));
+    if (bnorm == 0.0) {
+        CUDA_OK(s, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
+        res->converged = 1;
+        hist(0.0);
+        res->rel_residual = res->true_rel_residual = 0.0;
+        return finish_out(s, x, dx, ptr_kind, n);
+    }
+    if (!std::isfinite(bnorm)) return s->fail(S2L_ERR_NUMERIC, "non-finite right-hand side");
+    double* r = s->d_r;
+    double* z = s->d_z;
+    double* w = s->d_kw;
+    RET_IF(spmv_dev(s, dx, r, db, true));
+    RET_IF(read_red(s, 256, 1));
+    double beta = std::sqrt(s->h_red[256]);
+    hist(beta / bnorm);
+    res->rel_residual = beta / bnorm;
+    bool converged = beta <= o->rtol * bnorm;
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (m + 1) + i]; };
+    while (!converged && res->iterations < o->maxit) {
+        if (!std::isfinite(beta)) return s->fail(S2L_ERR_NUMERIC, "non-finite residual");
+        {
+            Prof pr(s, PC_VEC);
+            launch_axpby(st, n, 1.0 / beta, r, 0.0, V);
+        }
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        std::fill(H.begin(), H.end(), 0.0);
+        int k = 0;
+        bool breakdown = false;
+        for (int j = 0; j < m && res->iterations < o->maxit; ++j) {
+            double* zj = flex ? Z + (size_t)j * n : z;
+            RET_IF(apply_dev(s, V + (size_t)j * n, zj));
+            RET_IF(spmv_dev(s, zj, w, nullptr, false));
+            {
+                Prof pr(s, PC_VEC);
+                launch_mdot(st, n, V, n, j + 1, w, s->d_part, s->d_red);
+                launch_gemv_update(st, n, V, n, j + 1, s->d_red, -1.0, w, nullptr);
+                launch_mdot(st, n, V, n, j + 1, w, s->d_part, s->d_red + 128);
+                launch_gemv_update(st, n, V, n, j + 1, s->d_red + 128, -1.0, w, s->d_part);
+                launch_reduce(st, s->d_part, S2L_NB_RED, 1, s->d_red + 256);
+            }
+            CUDA_OK(s, cudaMemcpyAsync(s->h_red, s->d_red, 257 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CUDA_OK(s, cudaStreamSynchronize(st));
+            const double hn = std::sqrt(s->h_red[256]);
+            for (int i = 0; i <= j; ++i) Hc(i, j) = s->h_red[i] + s->h_red[128 + i];
+            Hc(j + 1, j) = hn;
+            if (hn > 0.0) {
+                Prof pr(s, PC_VEC);
+                launch_axpby(st, n, 1.0 / hn, w, 0.0, V + (size_t)(j + 1) * n);
+            }
+            for (int i = 0; i < j; ++i) {
+                const double t = cs[i] * Hc(i, j) + sn[i] * Hc(i + 1, j);
+                Hc(i + 1, j) = -sn[i] * Hc(i, j) + cs[i] * Hc(i + 1, j);
+                Hc(i, j) = t;
+            }
+            const double den = std::hypot(Hc(j, j), Hc(j + 1, j));
+            cs[j] = den > 0.0 ? Hc(j, j) / den : 1.0;
+            sn[j] = den > 0.0 ? Hc(j + 1, j) / den : 0.0;
+            Hc(j, j) = den;
+            Hc(j + 1, j) = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            ++k;
+            ++res->iterations;
+            res->rel_residual = std::fabs(g[j + 1]) / bnorm;
+            hist(res->rel_residual);
+            if (!std::isfinite(res->rel_residual)) return s->fail(S2L_ERR_NUMERIC, "non-finite GMRES residual");
+            if (res->rel_residual <= o->rtol) {
+                converged = true;
+                break;
+            }
+            if (hn == 0.0) {
+                breakdown = true;
+                break;
+            }
+        }
+        // y = H_k^-1 g_k (upper triangular), x += M^-1 V_k y (or Z_k y)
+        for (int i = k - 1; i >= 0; --i) {
+            double t = g[i];
+            for (int c = i + 1; c < k; ++c) t -= Hc(i, c) * y[c];
+            y[i] = t / Hc(i, i);
+        }
+        CUDA_OK(s, cudaMemcpyAsync(s->d_coef, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+        {
+            Prof pr(s, PC_VEC);
+            launch_gemv(st, n, flex ? Z : V, n, k, s->d_coef, s->d_u);
+        }
+        if (flex) {
+            Prof pr(s, PC_VEC);
+            launch_axpby(st, n, 1.0, s->d_u, 1.0, dx);
+        } else {
+            RET_IF(apply_dev(s, s->d_u, z));
+            Prof pr(s, PC_VEC);
+            launch_axpby(st, n, 1.0, z, 1.0, dx);
+        }
+        RET_IF(spmv_dev(s, dx, r, db, true));
+        RET_IF(read_red(s, 256, 1));
+        beta = std::sqrt(s->h_red[256]);
+        const bool within = beta <= o->rtol * bnorm;
+        const bool within_slack = beta <= (o->strict_true_residual ? 1.0 : 1.1) * o->rtol * bnorm;
+        if (breakdown) converged = within || converged;
+        if (converged && !within_slack) converged = false;
+        if (beta == 0.0) converged = true;
+        if (!converged) ++res->restarts;
+    }
+    res->converged = converged ? 1 : 0;
+    res->true_rel_residual = beta / bnorm;
+    return finish_out(s, x, dx, ptr_kind, n);
+}
+
+// Right-preconditioned BiCGStab, L2 stopping test (src/solver/bicgstab.cpp:15-154).
+int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                     s2l_result* res)
+{
+    RET_IF(check_ready(s));
+    if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
+    if (o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
+    RET_IF(ensure_krylov(s, 1, false));
+    const int64_t n = s->n;
+    cudaStream_t st = s->stream;
+    if (!s->d_rh) {
+        RET_IF(alloc_doubles(s, &s->d_rh, n));
+        RET_IF(alloc_doubles(s, &s->d_p, n));
+        RET_IF(alloc_doubles(s, &s->d_v, n));
+        RET_IF(alloc_doubles(s, &s->d_s, n));
+        RET_IF(alloc_doubles(s, &s->d_t, n));
+        RET_IF(alloc_doubles(s, &s->d_yb, n));
+    }
+    const double* db;
+    if (ptr_kind == S2L_PTR_HOST) {
+        CUDA_OK(s, cudaMemcpyAsync(s->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        db = s->d_b;
+    } else if (ptr_kind == S2L_PTR_DEVICE) {
+        db = b;
+        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+        return s->fail(S2L_ERR_BADARG, "bad ptr_kind");
+    }
+    double* dx = s->d_xk;
+    double *r = s->d_r, *rh = s->d_rh, *p = s->d_p, *v = s->d_v, *y = s->d_yb, *sv = s->d_s, *zv = s->d_z,
+           *t = s->d_t;
+    res->converged = 0;
+    res->breakdown = 0;
+    res->iterations = 0;
+    res->restarts = 0;
+    res->history_len = 0;
+    auto hist = [&](double val) {
+        if (res->history && res->history_len < o->history_cap) res->history[res->history_len] = val;
+        if (res->history_len < o->history_cap) ++res->history_len;
+    };
+    double bnorm = 0.0;
+    RET_IF(norm2_dev(s, db, &bnorm));
+    if (bnorm == 0.0) {
+        CUDA_OK(s, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
+        res->converged = 1;
+        hist(0.0);
+        res->rel_residual = res->true_rel_residual = 0.0;
+        return finish_out(s, x, dx, ptr_kind, n);
+    }
+    RET_IF(spmv_dev(s, dx, r, db, true));
+    RET_IF(read_red(s, 256, 1));
+    double rn = std::sqrt(s->h_red[256]);
+    hist(rn / bnorm);
+    res->rel_residual = rn / bnorm;
+    auto satisfied = [&](double slack) { return rn <= slack * o->rtol * bnorm; };
+    for (;;) {
+        if (satisfied(1.0)) {
+            res->converged = 1;
+            break;
+        }
+        if (res->iterations >= o->maxit) break;
+        CUDA_OK(s, cudaMemcpyAsync(rh, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        const double rhn = rn;
+        double rho = rn * rn, rho_old = 1.0, alpha = 1.0, omega = 1.0;
+        bool first = true, candidate = false;
+        while (res->iterations < o->maxit) {
+            {
+                Prof pr(s, PC_VEC);
+                launch_bicg_p(st, n, r, v, first ? 0.0 : (rho / rho_old) * (alpha / omega), omega, p, first ? 1 : 0);
+            }
+            first = false;
+            RET_IF(apply_dev(s, p, y));
+            RET_IF(spmv_dev(s, y, v, nullptr, false));
+            ++res->iterations;
+            {
+                Prof pr(s, PC_VEC);
+                launch_dot2(st, n, rh, v, nullptr, s->d_part, s->d_red + 256);
+            }
+            RET_IF(read_red(s, 256, 1));
+            const double rhv = s->h_red[256];
+            if (rhv == 0.0 || !std::isfinite(rhv)) {
+                res->breakdown = 1;
+                break;
+            }
+            alpha = rho / rhv;
+            {
+                Prof pr(s, PC_VEC);
+                launch_bicg_s(st, n, r, v, alpha, sv, nullptr, s->d_part, s->d_red + 256);
+            }
+            RET_IF(read_red(s, 256, 1));
+            rn = std::sqrt(s->h_red[256]);
+            res->rel_residual = rn / bnorm;
+            hist(res->rel_residual);
+            if (satisfied(1.0) || res->iterations >= o->maxit) {
+                Prof pr(s, PC_VEC);
+                launch_axpby(st, n, alpha, y, 1.0, dx);
+                CUDA_OK(s, cudaMemcpyAsync(r, sv, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                candidate = satisfied(1.0);
+                break;
+            }
+            RET_IF(apply_dev(s, sv, zv));
+            RET_IF(spmv_dev(s, zv, t, nullptr, false));
+            ++res->iterations;
+            {
+                Prof pr(s, PC_VEC);
+                launch_dot2(st, n, t, t, sv, s->d_part, s->d_red + 256);
+            }
+            RET_IF(read_red(s, 256, 2));
+            const double tt = s->h_red[256], ts = s->h_red[257];
+            omega = tt > 0.0 ? ts / tt : 0.0;
+            {
+                Prof pr(s, PC_VEC);
+                launch_bicg_x(st, n, dx, y, zv, alpha, omega, r, sv, t, rh, s->d_part, s->d_red + 256);
+            }
+            RET_IF(read_red(s, 256, 2));
+            rho_old = rho;
+            rn = std::sqrt(s->h_red[256]);
+            rho = s->h_red[257];
+            res->rel_residual = rn / bnorm;
+            hist(res->rel_residual);
+            if (satisfied(1.0)) {
+                candidate = true;
+                break;
+            }
+            if (omega == 0.0 || std::fabs(rho) < 1e-14 * rhn * rn) break;
+        }
+        RET_IF(spmv_dev(s, dx, r, db, true));
+        RET_IF(read_red(s, 256, 1));
+        rn = std::sqrt(s->h_red[256]);
+        if (res->breakdown) break;
+        if (candidate && satisfied(o->strict_true_residual ? 1.0 : 1.1)) {
+            res->converged = 1;
+            break;
+        }
+        if (res->iterations >= o->maxit) break;
+        ++res->restarts;
+    }
+    res->true_rel_residual = rn / bnorm;
+    return finish_out(s, x, dx, ptr_kind, n);
+}
+
+}  // extern "C"

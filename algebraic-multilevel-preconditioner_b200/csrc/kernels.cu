@@ -1,0 +1,577 @@
+// sm_100a kernels of the solve phase.
+//
+// All reductions are deterministic: every reduction-producing kernel runs on a fixed grid of
+// S2L_NB_RED blocks, writes one partial per block and column, and reduce_kernel sums them in a
+// fixed order.  The same input therefore gives bitwise-identical results, alone or in a batch.
+#include "s2l_internal.cuh"
+
+namespace s2l {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over the CTA; the result is valid in thread 0.  sh holds one value per warp.
+template <int BS>
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = (l < BS / 32) ? sh[l] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// ------------------------------------------------------------------------------ SpMV (K1, K10)
+// y = A x, or y = b - A x when b != nullptr; with partials, also sum(y^2) per block.
+// TPR threads per row (sub-warp groups), grid-stride over rows; the loop is warp-uniform so
+// the group shuffles always see the full warp.
+template <int TPR>
+__global__ void __launch_bounds__(S2L_BS_VEC) spmv_kernel(int64_t n, const int32_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ ci,
+                                                          const double* __restrict__ v,
+                                                          const double* __restrict__ x, double* __restrict__ y,
+                                                          const double* __restrict__ b, double* __restrict__ partials)
+{
+    __shared__ double sh[S2L_BS_VEC / 32];
+    const int lane = threadIdx.x % TPR;
+    const int64_t g0 = ((int64_t)blockIdx.x * S2L_BS_VEC + threadIdx.x) / TPR;
+    const int64_t stride = (int64_t)gridDim.x * (S2L_BS_VEC / TPR);
+    double acc = 0.0;
+    for (int64_t row = g0; __any_sync(0xffffffffu, row < n); row += stride) {
+        double s = 0.0;
+        if (row < n) {
+            const int e1 = rp[row + 1];
+            for (int e = rp[row] + lane; e < e1; e += TPR) s += v[e] * __ldg(x + ci[e]);
+        }
+#pragma unroll
+        for (int o = TPR / 2; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && row < n) {
+            const double yv = b ? b[row] - s : s;
+            y[row] = yv;
+            acc += yv * yv;
+        }
+    }
+    if (partials) {
+        const double t = block_sum<S2L_BS_VEC>(acc, sh);
+        if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    }
+}
+
+// out[c] = sum over blocks of partials[b * ncols + c]; one warp per column, fixed order.
+__global__ void __launch_bounds__(256) reduce_kernel(const double* __restrict__ partials, int nblocks, int ncols,
+                                                     double* __restrict__ out)
+{
+    const int col = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (col >= ncols) return;
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += partials[(int64_t)b * ncols + col];
+    s = warp_sum(s);
+    if (lane == 0) out[col] = s;
+}
+
+// ------------------------------------------------------------------------------ CGS2 (K7)
+// h = V(:, 0:k)^T w.  A CTA takes 1024-row tiles (w staged in shared memory), each warp owns the
+// columns warp + 8q; partials[b * k + c].
+__global__ void __launch_bounds__(256) mdot_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int k,
+                                                   const double* __restrict__ w, double* __restrict__ partials)
+{
+    __shared__ double ws[1024];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+    for (int64_t t0 = (int64_t)blockIdx.x * 1024; t0 < n; t0 += (int64_t)gridDim.x * 1024) {
+        const int cnt = (int)((n - t0) < 1024 ? (n - t0) : 1024);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += 256) ws[i] = w[t0 + i];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = warp + 8 * q;
+            if (c < k) {
+                const double* vc = V + (int64_t)c * ldv + t0;
+                double s0 = 0.0, s1 = 0.0;
+                int i = lane;
+                for (; i + 32 < cnt; i += 64) {
+                    s0 += vc[i] * ws[i];
+                    s1 += vc[i + 32] * ws[i + 32];
+                }
+                if (i < cnt) s0 += vc[i] * ws[i];
+                acc[q] += s0 + s1;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int c = warp + 8 * q;
+        if (c < k) {
+            const double s = warp_sum(acc[q]);
+            if (lane == 0) partials[(int64_t)blockIdx.x * k + c] = s;
+        }
+    }
+}
+
+// w += alpha * V(:, 0:k) h (h on the device); with partials, also sum(w^2) of the new w.
+__global__ void __launch_bounds__(256) gemv_update_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int k,
+                                                          const double* __restrict__ h, double alpha,
+                                                          double* __restrict__ w, double* __restrict__ partials)
+{
+    __shared__ double hs[S2L_MAX_RED_COLS];
+    __shared__ double sh[8];
+    for (int c = threadIdx.x; c < k; c += 256) hs[c] = h[c];
+    __syncthreads();
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        double s = 0.0;
+        for (int c = 0; c < k; ++c) s += V[i + (int64_t)c * ldv] * hs[c];
+        const double wn = w[i] + alpha * s;
+        w[i] = wn;
+        acc += wn * wn;
+    }
+    if (partials) {
+        const double t = block_sum<256>(acc, sh);
+        if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    }
+}
+
+// u = V(:, 0:k) y (y on the device)
+__global__ void __launch_bounds__(256) gemv_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int k,
+                                                   const double* __restrict__ y, double* __restrict__ u)
+{
+    __shared__ double ys[S2L_MAX_RED_COLS];
+    for (int c = threadIdx.x; c < k; c += 256) ys[c] = y[c];
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        double s = 0.0;
+        for (int c = 0; c < k; ++c) s += V[i + (int64_t)c * ldv] * ys[c];
+        u[i] = s;
+    }
+}
+
+__global__ void axpby_kernel(int64_t n, double a, const double* __restrict__ x, double b, double* __restrict__ y)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = (b == 0.0) ? a * x[i] : a * x[i] + b * y[i];
+}
+
+// y = x / s_dev[0]
+__global__ void scale_copy_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ s,
+                                  double* __restrict__ y)
+{
+    const double inv = 1.0 / s[0];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = x[i] * inv;
+}
+
+// partials of x.y and (z != nullptr) x.z
+__global__ void __launch_bounds__(256) dot2_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                                   const double* __restrict__ z, double* __restrict__ partials)
+{
+    __shared__ double sh[8];
+    double a = 0.0, b = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        a += x[i] * y[i];
+        if (z) b += x[i] * z[i];
+    }
+    const double ta = block_sum<256>(a, sh);
+    const double tb = block_sum<256>(b, sh);
+    if (threadIdx.x == 0) {
+        partials[(int64_t)blockIdx.x * 2] = ta;
+        partials[(int64_t)blockIdx.x * 2 + 1] = tb;
+    }
+}
+
+// ------------------------------------------------------------------------------ BiCGStab (K9)
+__global__ void bicg_p_kernel(int64_t n, const double* __restrict__ r, const double* __restrict__ v, double beta,
+                              double omega, double* __restrict__ p, int first)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = first ? r[i] : r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// s = r - alpha v; partials: s.s
+__global__ void __launch_bounds__(256) bicg_s_kernel(int64_t n, const double* __restrict__ r,
+                                                     const double* __restrict__ v, double alpha,
+                                                     double* __restrict__ s, double* __restrict__ partials)
+{
+    __shared__ double sh[8];
+    double a = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        const double si = r[i] - alpha * v[i];
+        s[i] = si;
+        a += si * si;
+    }
+    const double t = block_sum<256>(a, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// x += alpha y + omega z; r = s - omega t; partials: r.r, rh.r
+__global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restrict__ x, const double* __restrict__ y,
+                                                     const double* __restrict__ z, double alpha, double omega,
+                                                     double* __restrict__ r, const double* __restrict__ s,
+                                                     const double* __restrict__ t, const double* __restrict__ rh,
+                                                     double* __restrict__ partials)
+{
+    __shared__ double sh[8];
+    double a = 0.0, b = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        x[i] += alpha * y[i] + omega * z[i];
+        const double ri = s[i] - omega * t[i];
+        r[i] = ri;
+        a += ri * ri;
+        b += rh[i] * ri;
+    }
+    const double ta = block_sum<256>(a, sh);
+    const double tb = block_sum<256>(b, sh);
+    if (threadIdx.x == 0) {
+        partials[(int64_t)blockIdx.x * 2] = ta;
+        partials[(int64_t)blockIdx.x * 2 + 1] = tb;
+    }
+}
+
+// ------------------------------------------------------------------------------ local solves (K2, K3)
+template <typename Real>
+__device__ __forceinline__ Real group_sum(Real s, int G)
+{
+    for (int o = G >> 1; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
+    return s;
+}
+
+// One triangular solve, level by level, in place on x (shared or global memory).
+// Levels of width G: groups of G threads per row, shuffle-reduced.  S2L_MODE_CTA levels: the whole
+// CTA reduces each row.  Every level ends with a CTA barrier.
+template <typename Real>
+__device__ __forceinline__ void solve_pass(Real* __restrict__ x, const DevFactor<Real>& F, int64_t slot0,
+                                           const int32_t* __restrict__ lvl, const int8_t* __restrict__ mode, int nlev,
+                                           double* red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int lv = 0; lv < nlev; ++lv) {
+        const int a = lvl[lv], b = lvl[lv + 1];
+        const int G = mode[lv];
+        if (G > 0) {
+            const int ng = S2L_BS_SOLVE / G;
+            const int gid = tid / G, gl = tid - gid * G;
+            for (int p0 = a; p0 < b; p0 += ng) {
+                const int p = p0 + gid;
+                Real s = Real(0);
+                const bool act = p < b;
+                int r = 0;
+                if (act) {
+                    const int64_t slot = slot0 + p;
+                    r = F.rows[slot];
+                    const int64_t e1 = F.ptr[slot + 1];
+                    for (int64_t e = F.ptr[slot] + gl; e < e1; e += G) s += F.val[e] * x[F.col[e]];
+                }
+                s = group_sum(s, G);
+                if (act && gl == 0) x[r] = (x[r] - s) * F.dinv[slot0 + p];
+            }
+        } else {
+            for (int p = a; p < b; ++p) {
+                const int64_t slot = slot0 + p;
+                const int r = F.rows[slot];
+                Real s = Real(0);
+                const int64_t e1 = F.ptr[slot + 1];
+                for (int64_t e = F.ptr[slot] + tid; e < e1; e += S2L_BS_SOLVE) s += F.val[e] * x[F.col[e]];
+                s = warp_sum(s);
+                if (lane == 0) red[warp] = (double)s;
+                __syncthreads();
+                if (warp == 0) {
+                    Real t = (lane < S2L_BS_SOLVE / 32) ? (Real)red[lane] : Real(0);
+                    t = warp_sum(t);
+                    if (lane == 0) x[r] = (x[r] - t) * F.dinv[slot];
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One CTA per subdomain: gather the rhs (permuted), forward solve with L, backward solve with U,
+// then the epilogue: direct owned write (boolean RAS, + base), local-space write, or local output.
+template <typename Real, bool SMEM>
+__global__ void __launch_bounds__(S2L_BS_SOLVE) local_solve_kernel(const SolveArgs<Real> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[S2L_BS_SOLVE / 32];
+    const int sid = a.sub_list ? a.sub_list[blockIdx.x] : (int)blockIdx.x;
+    const DevSub sd = a.subs[sid];
+    const int64_t lo = sd.loc_off;
+    const int n = sd.n_local;
+    Real* x = SMEM ? reinterpret_cast<Real*>(smem_raw) : a.xscratch + lo;
+    if (a.mode == 2) {
+        for (int k = threadIdx.x; k < n; k += S2L_BS_SOLVE) x[k] = (Real)a.in[a.pin[lo + k]];
+    } else {
+        for (int k = threadIdx.x; k < n; k += S2L_BS_SOLVE) x[k] = (Real)a.in[a.gin[lo + k]];
+    }
+    __syncthreads();
+    solve_pass<Real>(x, a.f[0], lo, a.lvl_pos + sd.lvl_off[0], a.lvl_mode + sd.lvl_off[0], sd.nlev[0], red);
+    solve_pass<Real>(x, a.f[1], lo, a.lvl_pos + sd.lvl_off[1], a.lvl_mode + sd.lvl_off[1], sd.nlev[1], red);
+    if (a.mode == 0) {
+        for (int j = threadIdx.x; j < sd.n_owned; j += S2L_BS_SOLVE) {
+            double v = (double)x[a.gout[lo + j]];
+            if (a.base) v += a.base[sd.begin + j];
+            a.out[sd.begin + j] = v;
+        }
+    } else if (a.mode == 1) {
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SOLVE) a.ylocal[lo + j] = (double)x[a.gout[lo + j]];
+    } else {
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SOLVE) a.out[j] = (double)x[a.gout[lo + j]];
+    }
+}
+
+// out[g] = base[g] + sum over the copies c of g of w_c * ylocal[pos_c] (w = 1 when cp_w is null)
+__global__ void combine_kernel(int64_t n, const int64_t* __restrict__ cp_ptr, const int32_t* __restrict__ cp_pos,
+                               const double* __restrict__ cp_w, const double* __restrict__ ylocal,
+                               const double* __restrict__ base, double* __restrict__ out)
+{
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int64_t e = cp_ptr[g]; e < cp_ptr[g + 1]; ++e) s += (cp_w ? cp_w[e] : 1.0) * ylocal[cp_pos[e]];
+        out[g] = base ? base[g] + s : s;
+    }
+}
+
+// ------------------------------------------------------------------------------ coarse space (K4-K6)
+// c_i = V_i^T r per 256-row tile of one subdomain: partials[tile * mmax + c].
+__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_kernel(const int32_t* __restrict__ t_sub,
+                                                                        const int32_t* __restrict__ t_row0,
+                                                                        const int32_t* __restrict__ t_nrow,
+                                                                        const DevSub* __restrict__ subs,
+                                                                        const double* __restrict__ V,
+                                                                        const int32_t* __restrict__ l2g,
+                                                                        int boolean_pou, const double* __restrict__ r,
+                                                                        int mmax, double* __restrict__ partials)
+{
+    __shared__ double red[S2L_TILE_ROWS / 32][S2L_MAX_RED_COLS];
+    const int tile = blockIdx.x;
+    const DevSub sd = subs[t_sub[tile]];
+    const int m = sd.m, nr = t_nrow[tile];
+    const int l = t_row0[tile] + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool act = threadIdx.x < nr;
+    double rv = 0.0;
+    const double* vr = V;
+    if (act) {
+        rv = boolean_pou ? r[sd.begin + l] : r[l2g[sd.loc_off + l]];
+        vr = V + sd.v_off + (int64_t)l * m;
+    }
+    for (int c = 0; c < m; ++c) {
+        const double p = warp_sum(act ? rv * vr[c] : 0.0);
+        if (lane == 0) red[warp][c] = p;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < m; c += S2L_TILE_ROWS) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) s += red[w][c];
+        partials[(int64_t)tile * mmax + c] = s;
+    }
+}
+
+__global__ void coarse_reduce_kernel(const DevSub* __restrict__ subs, const int32_t* __restrict__ t_first, int mmax,
+                                     const double* __restrict__ partials, double* __restrict__ cvec)
+{
+    const int i = blockIdx.x;
+    const DevSub sd = subs[i];
+    for (int c = threadIdx.x; c < sd.m; c += blockDim.x) {
+        double s = 0.0;
+        for (int t = t_first[i]; t < t_first[i + 1]; ++t) s += partials[(int64_t)t * mmax + c];
+        cvec[sd.c_off + c] = s;
+    }
+}
+
+// y = M x, M dense row-major n0 x n0, one warp per row
+__global__ void __launch_bounds__(256) dense_gemv_kernel(int n0, const double* __restrict__ M,
+                                                         const double* __restrict__ x, double* __restrict__ y)
+{
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n0) return;
+    const double* mr = M + (int64_t)row * n0;
+    double s = 0.0;
+    for (int c = lane; c < n0; c += 32) s += mr[c] * x[c];
+    s = warp_sum(s);
+    if (lane == 0) y[row] = s;
+}
+
+// x0 = V_i y_i on the owned rows (boolean PoU: direct global write) or on Omega_i (plocal, summed
+// over the copies afterwards).
+__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_prolong_kernel(const int32_t* __restrict__ t_sub,
+                                                                       const int32_t* __restrict__ t_row0,
+                                                                       const int32_t* __restrict__ t_nrow,
+                                                                       const DevSub* __restrict__ subs,
+                                                                       const double* __restrict__ V, int boolean_pou,
+                                                                       const double* __restrict__ y,
+                                                                       double* __restrict__ out,
+                                                                       double* __restrict__ plocal)
+{
+    const int tile = blockIdx.x;
+    if ((int)threadIdx.x >= t_nrow[tile]) return;
+    const DevSub sd = subs[t_sub[tile]];
+    const int l = t_row0[tile] + threadIdx.x;
+    const double* vr = V + sd.v_off + (int64_t)l * sd.m;
+    const double* yc = y + sd.c_off;
+    double s = 0.0;
+    for (int c = 0; c < sd.m; ++c) s += vr[c] * yc[c];
+    if (boolean_pou)
+        out[sd.begin + l] = s;
+    else
+        plocal[sd.loc_off + l] = s;
+}
+
+inline int grid_for(int64_t n, int bs, int cap)
+{
+    const int64_t g = (n + bs - 1) / bs;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ launch wrappers
+void launch_spmv(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* x,
+                 double* y, const double* b, double* partials, double* red_out, int tpr)
+{
+    const int grid = S2L_NB_RED;
+    switch (tpr) {
+    case 4: spmv_kernel<4><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
+    case 16: spmv_kernel<16><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
+    case 32: spmv_kernel<32><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
+    default: spmv_kernel<8><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
+    }
+    if (partials) reduce_kernel<<<1, 256, 0, st>>>(partials, grid, 1, red_out);
+}
+
+void launch_reduce(cudaStream_t st, const double* partials, int nblocks, int ncols, double* out)
+{
+    reduce_kernel<<<(ncols + 7) / 8, 256, 0, st>>>(partials, nblocks, ncols, out);
+}
+
+void launch_mdot(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* w, double* partials,
+                 double* out)
+{
+    mdot_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, V, ldv, k, w, partials);
+    reduce_kernel<<<(k + 7) / 8, 256, 0, st>>>(partials, S2L_NB_RED, k, out);
+}
+
+void launch_gemv_update(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* h, double alpha,
+                        double* w, double* partials)
+{
+    gemv_update_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, V, ldv, k, h, alpha, w, partials);
+}
+
+void launch_gemv(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* y, double* u)
+{
+    gemv_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, V, ldv, k, y, u);
+}
+
+void launch_axpby(cudaStream_t st, int64_t n, double a, const double* x, double b, double* y)
+{
+    axpby_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, a, x, b, y);
+}
+
+void launch_scale_copy(cudaStream_t st, int64_t n, const double* x, const double* s_dev, double* y)
+{
+    scale_copy_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, x, s_dev, y);
+}
+
+void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, const double* z, double* partials,
+                 double* out)
+{
+    dot2_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, x, y, z, partials);
+    reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
+}
+
+void launch_bicg_p(cudaStream_t st, int64_t n, const double* r, const double* v, double beta, double omega, double* p,
+                   int first)
+{
+    bicg_p_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, r, v, beta, omega, p, first);
+}
+
+void launch_bicg_s(cudaStream_t st, int64_t n, const double* r, const double* v, double alpha, double* s,
+                   const double* /*rh*/, double* partials, double* out)
+{
+    bicg_s_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, r, v, alpha, s, partials);
+    reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 1, out);
+}
+
+void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const double* z, double alpha,
+                   double omega, double* r, const double* s, const double* t, const double* rh, double* partials,
+                   double* out)
+{
+    bicg_x_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, x, y, z, alpha, omega, r, s, t, rh, partials);
+    reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
+}
+
+template <typename Real>
+cudaError_t launch_local_solve(cudaStream_t st, const SolveArgs<Real>& a, int nblocks, size_t smem_bytes)
+{
+    if (smem_bytes > 0) {
+        cudaError_t e = cudaFuncSetAttribute(local_solve_kernel<Real, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+        if (e != cudaSuccess) return e;
+        local_solve_kernel<Real, true><<<nblocks, S2L_BS_SOLVE, smem_bytes, st>>>(a);
+    } else {
+        local_solve_kernel<Real, false><<<nblocks, S2L_BS_SOLVE, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_local_solve<double>(cudaStream_t, const SolveArgs<double>&, int, size_t);
+template cudaError_t launch_local_solve<float>(cudaStream_t, const SolveArgs<float>&, int, size_t);
+
+void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int32_t* cp_pos, const double* cp_w,
+                    const double* ylocal, const double* base, double* out)
+{
+    combine_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, cp_ptr, cp_pos, cp_w, ylocal, base, out);
+}
+
+void launch_coarse_restrict(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                            const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                            int boolean_pou, const double* r, int mmax, double* partials)
+{
+    coarse_restrict_kernel<<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, r,
+                                                             mmax, partials);
+}
+
+void launch_coarse_reduce(cudaStream_t st, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,
+                          const double* partials, double* c)
+{
+    coarse_reduce_kernel<<<nsub, 64, 0, st>>>(subs, t_first, mmax, partials, c);
+}
+
+void launch_dense_gemv(cudaStream_t st, int n0, const double* M, const double* x, double* y)
+{
+    dense_gemv_kernel<<<(n0 + 7) / 8, 256, 0, st>>>(n0, M, x, y);
+}
+
+void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                           const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
+                           const double* y, double* out, double* plocal)
+{
+    coarse_prolong_kernel<<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V, boolean_pou, y, out,
+                                                            plocal);
+}
+
+}  // namespace s2l

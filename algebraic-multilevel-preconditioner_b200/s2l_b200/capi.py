@@ -1,0 +1,298 @@
+"""ctypes binding of the C ABI in include/s2l_gpu.h (the library is libs2l_gpu.so, built in-tree).
+
+``GpuSetup`` uploads a host ``Setup`` (setup_phase) once and exposes the solve-phase calls.
+There is no CPU fallback: if the library or a CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .setup_phase import Setup
+
+HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(HERE, "lib", "libs2l_gpu.so")
+
+S2L_OK = 0
+ERRORS = {1: "BADARG", 2: "OOM", 3: "CUDA", 4: "NUMERIC", 5: "TIMEOUT", 6: "BREAKDOWN", 7: "STATE"}
+ONE_LEVEL = {"ras": 0, "asm": 1}
+COARSE = {"none": 0, "additive": 1, "deflated": 2}
+POU = {"boolean": 0, "multiplicity": 1}
+FACTOR = {"lu": 0, "llt": 1, "ldlt": 2}
+PTR_HOST, PTR_DEVICE = 0, 1
+
+# every symbol include/s2l_gpu.h declares
+EXPORTED = [
+    "s2l_gpu_create", "s2l_gpu_destroy", "s2l_gpu_last_error", "s2l_gpu_setup_begin", "s2l_gpu_set_matrix",
+    "s2l_gpu_add_subdomain", "s2l_gpu_set_coarse", "s2l_gpu_setup_end", "s2l_gpu_setup_destroy",
+    "s2l_gpu_setup_bytes", "s2l_gpu_spmv", "s2l_gpu_local_solve", "s2l_gpu_coarse_apply",
+    "s2l_gpu_one_level_apply", "s2l_gpu_apply", "s2l_gpu_gmres", "s2l_gpu_bicgstab", "s2l_gpu_set_stream",
+    "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes",
+]
+
+
+class KrylovOpts(C.Structure):
+    _fields_ = [("restart", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int), ("flexible", C.c_int),
+                ("strict_true_residual", C.c_int), ("history_cap", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("converged", C.c_int), ("breakdown", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
+                ("rel_residual", C.c_double), ("true_rel_residual", C.c_double), ("history_len", C.c_int),
+                ("history", C.POINTER(C.c_double))]
+
+
+class S2LError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"s2l_gpu error {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libs2l_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run algebraic-multilevel-preconditioner_b200/build.py")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    i64p = C.POINTER(C.c_int64)
+    i32p = C.POINTER(C.c_int32)
+    dp = C.POINTER(C.c_double)
+    sig = {
+        "s2l_gpu_create": ([C.c_int, C.c_size_t, C.POINTER(vp)], C.c_int),
+        "s2l_gpu_destroy": ([vp], C.c_int),
+        "s2l_gpu_last_error": ([vp], C.c_char_p),
+        "s2l_gpu_setup_begin": ([vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+        "s2l_gpu_set_matrix": ([vp, i64p, i64p, dp], C.c_int),
+        "s2l_gpu_add_subdomain": ([vp, C.c_int, C.c_int64, C.c_int, C.c_int, i64p, dp, C.c_int, C.c_int, i32p,
+                                   i32p, i64p, i32p, vp, i64p, i32p, vp, vp, C.c_int, dp], C.c_int),
+        "s2l_gpu_set_coarse": ([vp, C.c_int64, i64p, dp], C.c_int),
+        "s2l_gpu_setup_end": ([vp], C.c_int),
+        "s2l_gpu_setup_destroy": ([vp], C.c_int),
+        "s2l_gpu_setup_bytes": ([vp, C.POINTER(C.c_size_t)], C.c_int),
+        "s2l_gpu_spmv": ([vp, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_local_solve": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_coarse_apply": ([vp, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_one_level_apply": ([vp, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_apply": ([vp, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_gmres": ([vp, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
+        "s2l_gpu_bicgstab": ([vp, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
+        "s2l_gpu_set_stream": ([vp, vp], C.c_int),
+        "s2l_gpu_profile_enable": ([vp, C.c_int], C.c_int),
+        "s2l_gpu_profile_get": ([vp, C.c_char_p, dp, C.POINTER(C.c_long)], C.c_int),
+        "s2l_gpu_local_solve_bytes": ([vp, dp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _vp(a):
+    """void* of a numpy array or a device pointer (int)."""
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    return C.c_void_p(a.ctypes.data)
+
+
+class Context:
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.s2l_gpu_create(device, hbm_budget, C.byref(h))
+        if rc != S2L_OK:
+            raise S2LError(rc, "s2l_gpu_create failed (no CUDA device?)")
+        self.h = h
+
+    def error(self) -> str:
+        return self.lib.s2l_gpu_last_error(self.h).decode()
+
+    def check(self, rc):
+        if rc != S2L_OK:
+            raise S2LError(rc, self.error())
+
+    def close(self):
+        if self.h:
+            self.lib.s2l_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuSetup:
+    """One matrix's setup on the GPU (the drop-in for the reference's TwoLevelSchwarz + Krylov)."""
+
+    def __init__(self, ctx: Context, st: Setup, one_level=None, coarse=None, pou=None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.n = st.n
+        self.nsub = st.nsub
+        opts = st.opts
+        h = C.c_void_p()
+        ctx.check(self.lib.s2l_gpu_setup_begin(ctx.h, st.n, st.nsub, ONE_LEVEL[one_level or opts.one_level],
+                                                COARSE[coarse or opts.coarse], POU[pou or opts.pou], C.byref(h)))
+        self.h = h
+        try:
+            self._upload(st, coarse or opts.coarse)
+        except Exception:
+            self.close()
+            raise
+
+    def _upload(self, st: Setup, coarse: str):
+        lib, ctx = self.lib, self.ctx
+        A = st.A
+        rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        ci = np.ascontiguousarray(A.indices, dtype=np.int64)
+        av = np.ascontiguousarray(A.data, dtype=np.float64)
+        ctx.check(lib.s2l_gpu_set_matrix(self.h, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(av, C.c_double)))
+        self.local_sizes = []
+        for i, s in enumerate(st.subdomains):
+            f = s.factor
+            real = 1 if f.L.dtype == np.float32 else 0
+            vt = np.float32 if real else np.float64
+            Lrp = np.ascontiguousarray(f.L.indptr, dtype=np.int64)
+            Lci = np.ascontiguousarray(f.L.indices, dtype=np.int32)
+            Lv = np.ascontiguousarray(f.L.data, dtype=vt)
+            if f.kind == "lu":
+                Urp = np.ascontiguousarray(f.U.indptr, dtype=np.int64)
+                Uci = np.ascontiguousarray(f.U.indices, dtype=np.int32)
+                Uv = np.ascontiguousarray(f.U.data, dtype=vt)
+                up = (_p(Urp, C.c_int64), _p(Uci, C.c_int32), _vp(Uv))
+            else:
+                up = (None, None, None)
+            d = np.ascontiguousarray(f.d, dtype=vt) if f.kind == "ldlt" else None
+            gh = np.ascontiguousarray(s.ghosts, dtype=np.int64)
+            D = np.ascontiguousarray(s.D, dtype=np.float64)
+            pin = np.ascontiguousarray(f.perm_in, dtype=np.int32)
+            pout = np.ascontiguousarray(f.perm_out, dtype=np.int32)
+            m = s.V.shape[1] if coarse != "none" else 0
+            V = np.asfortranarray(s.V, dtype=np.float64) if m else np.zeros(1)
+            rc = lib.s2l_gpu_add_subdomain(self.h, i, int(s.begin), int(s.n_owned), int(gh.size), _p(gh, C.c_int64),
+                                           _p(D, C.c_double), FACTOR[f.kind], real, _p(pin, C.c_int32),
+                                           _p(pout, C.c_int32), _p(Lrp, C.c_int64), _p(Lci, C.c_int32), _vp(Lv),
+                                           *up, _vp(d) if d is not None else None, m, _p(V, C.c_double))
+            ctx.check(rc)
+            self.local_sizes.append(s.n_local)
+        if coarse != "none":
+            off = np.ascontiguousarray(st.offsets, dtype=np.int64)
+            E = np.ascontiguousarray(st.E, dtype=np.float64)
+            if E.size == 0:
+                E = np.zeros(1)
+            ctx.check(lib.s2l_gpu_set_coarse(self.h, int(st.n0), _p(off, C.c_int64), _p(E, C.c_double)))
+        ctx.check(lib.s2l_gpu_setup_end(self.h))
+
+    # ---- helpers
+    def _vec(self, x, n):
+        if isinstance(x, int):
+            return x, PTR_DEVICE
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != n:
+            raise ValueError(f"vector of size {x.size}, expected {n}")
+        return x, PTR_HOST
+
+    def _call2(self, fn, x, n_in, n_out, out=None):
+        xv, kind = self._vec(x, n_in)
+        if kind == PTR_DEVICE:
+            if out is None or not isinstance(out, int):
+                raise ValueError("device input needs a device output pointer")
+            self.ctx.check(fn(self.h, C.c_void_p(xv), C.c_void_p(out), PTR_DEVICE))
+            return out
+        y = np.empty(n_out) if out is None else out
+        self.ctx.check(fn(self.h, _vp(xv), _vp(y), PTR_HOST))
+        return y
+
+    # ---- solve phase
+    def spmv(self, x, out=None):
+        return self._call2(self.lib.s2l_gpu_spmv, x, self.n, self.n, out)
+
+    def apply(self, r, out=None):
+        return self._call2(self.lib.s2l_gpu_apply, r, self.n, self.n, out)
+
+    def coarse_apply(self, r, out=None):
+        return self._call2(self.lib.s2l_gpu_coarse_apply, r, self.n, self.n, out)
+
+    def one_level_apply(self, r, out=None):
+        return self._call2(self.lib.s2l_gpu_one_level_apply, r, self.n, self.n, out)
+
+    def local_solve(self, i, b):
+        n = self.local_sizes[i] if 0 <= i < len(self.local_sizes) else max(1, np.size(b))
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(n)
+        self.ctx.check(self.lib.s2l_gpu_local_solve(self.h, i, _vp(b), _vp(x), PTR_HOST))
+        return x
+
+    def _krylov(self, fn, b, x0, restart, rtol, maxit, flexible, strict, history_cap, device_out=None):
+        o = KrylovOpts(restart, rtol, maxit, 1 if flexible else 0, 1 if strict else 0, history_cap)
+        hist = np.zeros(max(history_cap, 1))
+        res = Result()
+        res.history = _p(hist, C.c_double)
+        if isinstance(b, int):
+            self.ctx.check(fn(self.h, C.c_void_p(b), C.c_void_p(device_out), PTR_DEVICE, C.byref(o), C.byref(res)))
+            x = device_out
+        else:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+            self.ctx.check(fn(self.h, _vp(b), _vp(x), PTR_HOST, C.byref(o), C.byref(res)))
+        out = {"converged": bool(res.converged), "breakdown": bool(res.breakdown), "iterations": res.iterations,
+               "restarts": res.restarts, "rel_residual": res.rel_residual,
+               "true_rel_residual": res.true_rel_residual, "history": hist[:res.history_len].copy()}
+        return x, out
+
+    def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False, history_cap=4096,
+              device_out=None):
+        return self._krylov(self.lib.s2l_gpu_gmres, b, x0, restart, rtol, maxit, flexible, strict, history_cap,
+                            device_out)
+
+    def bicgstab(self, b, x0=None, rtol=1e-8, maxit=1000, strict=False, history_cap=4096, device_out=None):
+        return self._krylov(self.lib.s2l_gpu_bicgstab, b, x0, 1, rtol, maxit, False, strict, history_cap,
+                            device_out)
+
+    def set_stream(self, stream_ptr: int | None):
+        self.ctx.check(self.lib.s2l_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def profile(self, on=True):
+        self.ctx.check(self.lib.s2l_gpu_profile_enable(self.h, 1 if on else 0))
+
+    def profile_get(self, name):
+        ms = C.c_double()
+        n = C.c_long()
+        self.ctx.check(self.lib.s2l_gpu_profile_get(self.h, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def local_solve_bytes(self) -> float:
+        b = C.c_double()
+        self.ctx.check(self.lib.s2l_gpu_local_solve_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        self.ctx.check(self.lib.s2l_gpu_setup_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.s2l_gpu_setup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,157 @@
+/*
+ * s2l_gpu.h - C ABI of the B200 solve phase of the two-level Schwarz preconditioner.
+ *
+ * One GPU holds every subdomain of a matrix.  The host (the reference's setup, or any caller)
+ * uploads once per matrix: the renumbered global CSR, and per subdomain its ghost list, partition
+ * of unity, local triangular factors and coarse basis, then the coarse matrix.  After that the
+ * solve phase runs on the device: preconditioner applications and whole Krylov solves.
+ *
+ * Conventions (kept from the reference's interfaces):
+ *  - vectors are in the renumbered ordering, subdomain i owning rows [begin_i, begin_i + n_I,i);
+ *  - local numbering of subdomain i is [owned rows | ghosts in increasing global id];
+ *  - every call returns S2L_OK (0) or an S2L_ERR_* code; s2l_gpu_last_error() gives the message.
+ *    The reference reports the same failures with exceptions (std::invalid_argument for bad
+ *    arguments, std::runtime_error for numerical failures, std::logic_error for misuse);
+ *  - calls on different setups are independent; calls on one setup are serialised by the caller
+ *    (the reference's apply() is not re-entrant either, include/preconditioner/two_level_schwarz.hpp:220);
+ *  - pointer arguments of the solve-phase calls are host or device memory, as `ptr_kind` says.
+ *    Host pointers are copied in and out on the setup's stream inside the call.
+ *
+ * Entry points and the reference interface each one replaces:
+ *  s2l_gpu_create/destroy           no reference counterpart (device context)
+ *  s2l_gpu_setup_begin .. _end      the state built by TwoLevelSchwarz's constructor
+ *                                   (src/preconditioner/two_level_schwarz.cpp:20-28), uploaded
+ *  s2l_gpu_spmv                     DistributedMatrix::apply (include/linalg/distributed_matrix.hpp:33-38)
+ *  s2l_gpu_local_solve              LocalSolver::solve (include/linalg/local_solver.hpp:95)
+ *  s2l_gpu_coarse_apply             CoarseSpace::apply (src/preconditioner/coarse_space.cpp:234-246)
+ *  s2l_gpu_one_level_apply          OneLevelSchwarz::apply (src/preconditioner/one_level_schwarz.cpp:80-99)
+ *  s2l_gpu_apply                    Preconditioner::apply / TwoLevelSchwarz::apply
+ *                                   (include/preconditioner/preconditioner.hpp:73,
+ *                                    src/preconditioner/two_level_schwarz.cpp:134-163)
+ *  s2l_gpu_gmres                    Gmres::solve (include/solver/gmres.hpp:53-54, src/solver/gmres.cpp:18-161)
+ *  s2l_gpu_bicgstab                 BiCgStab::solve (src/solver/bicgstab.cpp:15-154)
+ */
+#ifndef S2L_GPU_H
+#define S2L_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct s2l_ctx s2l_ctx;
+typedef struct s2l_setup s2l_setup;
+
+/* status codes */
+enum {
+    S2L_OK = 0,
+    S2L_ERR_BADARG = 1,    /* invalid argument (reference: std::invalid_argument) */
+    S2L_ERR_OOM = 2,       /* device memory or the HBM budget exhausted */
+    S2L_ERR_CUDA = 3,      /* a CUDA call failed */
+    S2L_ERR_NUMERIC = 4,   /* singular coarse matrix, non-finite values (reference: std::runtime_error) */
+    S2L_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+    S2L_ERR_BREAKDOWN = 6, /* Krylov breakdown */
+    S2L_ERR_STATE = 7      /* call out of order (reference: std::logic_error) */
+};
+
+/* preconditioner variants (include/core/config.hpp:61-64) */
+enum { S2L_ONE_LEVEL_RAS = 0, S2L_ONE_LEVEL_ASM = 1 };
+enum { S2L_COARSE_NONE = 0, S2L_COARSE_ADDITIVE = 1, S2L_COARSE_DEFLATED = 2 };
+enum { S2L_POU_BOOLEAN = 0, S2L_POU_MULTIPLICITY = 1 };
+
+/* local factor kinds (include/linalg/local_solver.hpp:51-52) and storage precision */
+enum { S2L_FACTOR_LU = 0, S2L_FACTOR_LLT = 1, S2L_FACTOR_LDLT = 2 };
+enum { S2L_REAL_F64 = 0, S2L_REAL_F32 = 1 };
+
+/* where a vector argument lives */
+enum { S2L_PTR_HOST = 0, S2L_PTR_DEVICE = 1 };
+
+/* Krylov methods and options (include/core/config.hpp:94-103) */
+enum { S2L_KRYLOV_GMRES = 0, S2L_KRYLOV_BICGSTAB = 1 };
+
+typedef struct {
+    int restart;        /* GMRES restart length m */
+    double rtol;        /* ||b - A x||_2 <= rtol ||b||_2 */
+    int maxit;          /* maximum applications of the preconditioner */
+    int flexible;       /* 1: flexible GMRES (stores Z_j = M^-1 v_j); 0: the reference's GMRES */
+    int strict_true_residual; /* 1: converged only if the recomputed true residual is <= rtol;
+                                 0: the reference's 10% slack (src/solver/gmres.cpp:148-156) */
+    int history_cap;    /* capacity of result->history (0: no history) */
+} s2l_krylov_opts;
+
+typedef struct {
+    int converged;
+    int breakdown;
+    int iterations;           /* applications of M^-1 inside the iteration (include/solver/krylov.hpp:46) */
+    int restarts;
+    double rel_residual;      /* last Krylov residual estimate / ||b|| */
+    double true_rel_residual; /* ||b - A x|| / ||b|| recomputed in FP64 at the end */
+    int history_len;
+    double* history;          /* caller-owned, history_cap entries: ||r||/||b|| after every M^-1 */
+} s2l_result;
+
+/* ---- context ---------------------------------------------------------------------------- */
+int s2l_gpu_create(int device, size_t hbm_budget_bytes, s2l_ctx** ctx);
+int s2l_gpu_destroy(s2l_ctx* ctx);
+const char* s2l_gpu_last_error(const s2l_ctx* ctx);
+
+/* ---- setup upload (once per matrix) ---------------------------------------------------- */
+int s2l_gpu_setup_begin(s2l_ctx* ctx, int64_t n, int nsub, int one_level, int coarse, int pou, s2l_setup** setup);
+
+/* Renumbered global matrix, CSR with sorted columns (rowptr has n+1 entries). */
+int s2l_gpu_set_matrix(s2l_setup* s, const int64_t* rowptr, const int64_t* col, const double* val);
+
+/*
+ * Subdomain i.  ghosts: n_ghost sorted global ids.  D: partition of unity (n_local = n_owned + n_ghost).
+ * The local factor solves A_ii x = b as: t[k] = b[perm_in[k]]; L u = t; U v = u; x[j] = v[perm_out[j]].
+ *   S2L_FACTOR_LU  : L unit lower (diagonal entries may be present; they are ignored), U upper with diagonal.
+ *   S2L_FACTOR_LLT : L lower with diagonal, U = L^T (U_* arguments ignored).
+ *   S2L_FACTOR_LDLT: L unit lower, U = diag(ldlt_d) L^T (U_* ignored).
+ * L/U are CSR over the n_local rows with sorted columns; values are double or float (real_type).
+ * V: coarse basis, n_local x m, column-major (m may be 0).
+ */
+int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t* ghosts,
+                          const double* D, int factor_kind, int real_type, const int32_t* perm_in,
+                          const int32_t* perm_out, const int64_t* L_rowptr, const int32_t* L_col, const void* L_val,
+                          const int64_t* U_rowptr, const int32_t* U_col, const void* U_val, const void* ldlt_d,
+                          int m, const double* V);
+
+/* Coarse matrix E = R0 A R0^T (n0 x n0, row-major) and coarse offsets (nsub+1 entries). */
+int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E);
+
+int s2l_gpu_setup_end(s2l_setup* s);
+int s2l_gpu_setup_destroy(s2l_setup* s);
+
+/* Device bytes held by the setup (matrix, factors, basis, schedules, work vectors). */
+int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
+
+/* ---- solve phase ---------------------------------------------------------------------- */
+int s2l_gpu_spmv(s2l_setup* s, const double* x, double* y, int ptr_kind);
+int s2l_gpu_local_solve(s2l_setup* s, int i, const double* b_local, double* x_local, int ptr_kind);
+int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind);
+int s2l_gpu_one_level_apply(s2l_setup* s, const double* r, double* z, int ptr_kind);
+int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind);
+
+int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
+                  s2l_result* result);
+int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
+                     s2l_result* result);
+
+/* ---- streams and measurement -------------------------------------------------------------- */
+/* Launch on this CUDA stream (cudaStream_t passed as a pointer; NULL = the setup's own stream). */
+int s2l_gpu_set_stream(s2l_setup* s, void* stream);
+/* 1: time every kernel class with CUDA events on the launching stream. */
+int s2l_gpu_profile_enable(s2l_setup* s, int on);
+/* Accumulated event time [ms] and launch count of one kernel class; names: "spmv", "local_solve",
+   "coarse", "combine", "krylov_vec", "all".  Resets with s2l_gpu_profile_enable(s, 1). */
+int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launches);
+/* Algorithmic bytes read+written by one local_solve launch (the roofline numerator). */
+int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* S2L_GPU_H */

@@ -1,0 +1,567 @@
+/*
+ * s2l_oracle.c - CPU restatement of the reference's solve phase.  TEST INFRASTRUCTURE ONLY.
+ *
+ * This file is the oracle the GPU path is checked against: only tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg may load it, and only as the checker or the timed CPU baseline.
+ * It is never part of the product path.
+ *
+ * It restates, in plain sequential C, the algorithm of the reference (fraBuffoli/
+ * Algebraic-Multilevel-Preconditioner) on one process holding every subdomain:
+ *   - DistributedMatrix::apply          include/linalg/distributed_matrix.hpp:33-38
+ *   - HaloExchange::forward/reverseAdd   src/linalg/halo_exchange.cpp:34-53, 86-107
+ *   - LocalSolver::solve                src/linalg/local_solver.cpp:119-126 (Eigen triangular solves)
+ *   - OneLevelSchwarz::apply            src/preconditioner/one_level_schwarz.cpp:80-99
+ *   - CoarseSpace::restrict/prolong     src/preconditioner/coarse_space.cpp:208-230
+ *   - CoarseSolver::solve (root)        src/preconditioner/coarse_solver.cpp:166-179 (direct solve of E)
+ *   - TwoLevelSchwarz::apply            src/preconditioner/two_level_schwarz.cpp:134-163
+ *   - Gmres::solve                      src/solver/gmres.cpp:18-161 (L2 stopping test)
+ *   - BiCgStab::solve                   src/solver/bicgstab.cpp:15-154 (L2 stopping test)
+ * The factors, coarse basis and coarse matrix are inputs (the setup phase produces them), in the
+ * same conventions as include/s2l_gpu.h.  Parity of this restatement with the reference itself is
+ * pinned by the golden fixtures under tests/golden/ (generated by running the reference).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    int64_t begin;
+    int n_owned, n_local;
+    int64_t *l2g;       /* local -> global */
+    double *D;
+    int kind;           /* 0 LU, 1 LLT, 2 LDLT */
+    int32_t *pin, *pout;
+    int64_t *Lp, *Up;
+    int32_t *Li, *Ui;
+    double *Lx, *Ux, *d; /* values widened to double (float factors are exact in double) */
+    int single;          /* 1: the solve runs in float, as the reference's float factors do */
+    int m;
+    double *V;           /* n_local x m column-major */
+    double *rloc, *yloc; /* work */
+} OSub;
+
+typedef struct {
+    int64_t n;
+    int nsub, one_level, coarse, pou;
+    int64_t *Ap, *Ai;
+    double *Ax;
+    OSub *sub;
+    int64_t n0;
+    int64_t *coff;
+    double *ELU;   /* LU of E (row-major, partial pivoting) */
+    int *piv;
+    double *c, *y, *x0, *w, *z1, *tmp;
+} OSetup;
+
+/* ---------------------------------------------------------------------------------------- */
+OSetup *oracle_setup_create(int64_t n, int nsub, int one_level, int coarse, int pou)
+{
+    OSetup *s = (OSetup *)calloc(1, sizeof(OSetup));
+    s->n = n;
+    s->nsub = nsub;
+    s->one_level = one_level;
+    s->coarse = coarse;
+    s->pou = pou;
+    s->sub = (OSub *)calloc((size_t)nsub, sizeof(OSub));
+    s->x0 = (double *)calloc((size_t)n, sizeof(double));
+    s->w = (double *)calloc((size_t)n, sizeof(double));
+    s->z1 = (double *)calloc((size_t)n, sizeof(double));
+    s->tmp = (double *)calloc((size_t)n, sizeof(double));
+    return s;
+}
+
+void oracle_setup_destroy(OSetup *s)
+{
+    if (!s) return;
+    for (int i = 0; i < s->nsub; ++i) {
+        OSub *q = &s->sub[i];
+        free(q->l2g); free(q->D); free(q->pin); free(q->pout); free(q->Lp); free(q->Up); free(q->Li);
+        free(q->Ui); free(q->Lx); free(q->Ux); free(q->d); free(q->V); free(q->rloc); free(q->yloc);
+    }
+    free(s->sub); free(s->Ap); free(s->Ai); free(s->Ax); free(s->coff); free(s->ELU); free(s->piv);
+    free(s->c); free(s->y); free(s->x0); free(s->w); free(s->z1); free(s->tmp);
+    free(s);
+}
+
+void oracle_set_matrix(OSetup *s, const int64_t *rp, const int64_t *ci, const double *v)
+{
+    int64_t nnz = rp[s->n];
+    s->Ap = (int64_t *)malloc((size_t)(s->n + 1) * sizeof(int64_t));
+    s->Ai = (int64_t *)malloc((size_t)(nnz ? nnz : 1) * sizeof(int64_t));
+    s->Ax = (double *)malloc((size_t)(nnz ? nnz : 1) * sizeof(double));
+    memcpy(s->Ap, rp, (size_t)(s->n + 1) * sizeof(int64_t));
+    memcpy(s->Ai, ci, (size_t)nnz * sizeof(int64_t));
+    memcpy(s->Ax, v, (size_t)nnz * sizeof(double));
+}
+
+static double *dup_vals(const void *v, int64_t count, int single)
+{
+    double *o = (double *)malloc((size_t)(count ? count : 1) * sizeof(double));
+    for (int64_t k = 0; k < count; ++k) o[k] = single ? (double)((const float *)v)[k] : ((const double *)v)[k];
+    return o;
+}
+
+void oracle_add_subdomain(OSetup *s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t *ghosts,
+                          const double *D, int kind, int single, const int32_t *pin, const int32_t *pout,
+                          const int64_t *Lp, const int32_t *Li, const void *Lx, const int64_t *Up, const int32_t *Ui,
+                          const void *Ux, const void *d, int m, const double *V)
+{
+    OSub *q = &s->sub[i];
+    int nl = n_owned + n_ghost;
+    q->begin = begin;
+    q->n_owned = n_owned;
+    q->n_local = nl;
+    q->l2g = (int64_t *)malloc((size_t)nl * sizeof(int64_t));
+    for (int j = 0; j < n_owned; ++j) q->l2g[j] = begin + j;
+    for (int j = 0; j < n_ghost; ++j) q->l2g[n_owned + j] = ghosts[j];
+    q->D = (double *)malloc((size_t)nl * sizeof(double));
+    memcpy(q->D, D, (size_t)nl * sizeof(double));
+    q->kind = kind;
+    q->single = single;
+    q->pin = (int32_t *)malloc((size_t)nl * sizeof(int32_t));
+    q->pout = (int32_t *)malloc((size_t)nl * sizeof(int32_t));
+    memcpy(q->pin, pin, (size_t)nl * sizeof(int32_t));
+    memcpy(q->pout, pout, (size_t)nl * sizeof(int32_t));
+    q->Lp = (int64_t *)malloc((size_t)(nl + 1) * sizeof(int64_t));
+    memcpy(q->Lp, Lp, (size_t)(nl + 1) * sizeof(int64_t));
+    q->Li = (int32_t *)malloc((size_t)(Lp[nl] ? Lp[nl] : 1) * sizeof(int32_t));
+    memcpy(q->Li, Li, (size_t)Lp[nl] * sizeof(int32_t));
+    q->Lx = dup_vals(Lx, Lp[nl], single);
+    if (kind == 0) {
+        q->Up = (int64_t *)malloc((size_t)(nl + 1) * sizeof(int64_t));
+        memcpy(q->Up, Up, (size_t)(nl + 1) * sizeof(int64_t));
+        q->Ui = (int32_t *)malloc((size_t)(Up[nl] ? Up[nl] : 1) * sizeof(int32_t));
+        memcpy(q->Ui, Ui, (size_t)Up[nl] * sizeof(int32_t));
+        q->Ux = dup_vals(Ux, Up[nl], single);
+    }
+    if (kind == 2) q->d = dup_vals(d, nl, single);
+    q->m = m;
+    if (m) {
+        q->V = (double *)malloc((size_t)nl * m * sizeof(double));
+        memcpy(q->V, V, (size_t)nl * m * sizeof(double));
+    }
+    q->rloc = (double *)calloc((size_t)nl, sizeof(double));
+    q->yloc = (double *)calloc((size_t)nl, sizeof(double));
+}
+
+/* LU with partial pivoting of the coarse matrix (the root solver factorizes E once,
+   src/preconditioner/coarse_solver.cpp:113-139).  Returns 0 if E is singular. */
+int oracle_set_coarse(OSetup *s, int64_t n0, const int64_t *offsets, const double *E)
+{
+    int n = (int)n0;
+    s->n0 = n0;
+    s->coff = (int64_t *)malloc((size_t)(s->nsub + 1) * sizeof(int64_t));
+    memcpy(s->coff, offsets, (size_t)(s->nsub + 1) * sizeof(int64_t));
+    s->ELU = (double *)malloc((size_t)(n ? n : 1) * (n ? n : 1) * sizeof(double));
+    memcpy(s->ELU, E, (size_t)n * n * sizeof(double));
+    s->piv = (int *)malloc((size_t)(n ? n : 1) * sizeof(int));
+    s->c = (double *)calloc((size_t)(n ? n : 1), sizeof(double));
+    s->y = (double *)calloc((size_t)(n ? n : 1), sizeof(double));
+    double *A = s->ELU;
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        double best = fabs(A[(size_t)k * n + k]);
+        for (int i = k + 1; i < n; ++i)
+            if (fabs(A[(size_t)i * n + k]) > best) { best = fabs(A[(size_t)i * n + k]); p = i; }
+        if (best == 0.0) return 0;
+        s->piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < n; ++j) { double t = A[(size_t)k * n + j]; A[(size_t)k * n + j] = A[(size_t)p * n + j]; A[(size_t)p * n + j] = t; }
+        for (int i = k + 1; i < n; ++i) {
+            double l = A[(size_t)i * n + k] / A[(size_t)k * n + k];
+            A[(size_t)i * n + k] = l;
+            for (int j = k + 1; j < n; ++j) A[(size_t)i * n + j] -= l * A[(size_t)k * n + j];
+        }
+    }
+    return 1;
+}
+
+/* ------------------------------------------------------------------------ building blocks */
+/* y = A x (or y = b - A x) */
+void oracle_spmv(const OSetup *s, const double *x, double *y)
+{
+    for (int64_t r = 0; r < s->n; ++r) {
+        double t = 0.0;
+        for (int64_t e = s->Ap[r]; e < s->Ap[r + 1]; ++e) t += s->Ax[e] * x[s->Ai[e]];
+        y[r] = t;
+    }
+}
+
+/* A_ii x = b with the factors: t = b[perm_in]; L u = t; U v = u; x = v[perm_out] */
+static void local_solve_d(const OSub *q, const double *b, double *x, double *t)
+{
+    int n = q->n_local;
+    for (int k = 0; k < n; ++k) t[k] = b[q->pin[k]];
+    /* forward: L lower (unit for LU/LDLT) */
+    for (int r = 0; r < n; ++r) {
+        double acc = t[r], dg = 1.0;
+        for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e) {
+            int c = q->Li[e];
+            if (c < r) acc -= q->Lx[e] * t[c];
+            else if (c == r) dg = q->Lx[e];
+        }
+        t[r] = (q->kind == 1) ? acc / dg : acc;
+    }
+    if (q->kind == 0) { /* U upper */
+        for (int r = n - 1; r >= 0; --r) {
+            double acc = t[r], dg = 1.0;
+            for (int64_t e = q->Up[r]; e < q->Up[r + 1]; ++e) {
+                int c = q->Ui[e];
+                if (c > r) acc -= q->Ux[e] * t[c];
+                else if (c == r) dg = q->Ux[e];
+            }
+            t[r] = acc / dg;
+        }
+    } else { /* U = L^T (LLT) or diag(d) L^T (LDLT): column sweep over the rows of L */
+        if (q->kind == 2)
+            for (int r = 0; r < n; ++r) t[r] /= q->d[r];
+        for (int r = n - 1; r >= 0; --r) {
+            double dg = 1.0;
+            if (q->kind == 1)
+                for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e)
+                    if (q->Li[e] == r) dg = q->Lx[e];
+            t[r] /= dg;
+            for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e) {
+                int c = q->Li[e];
+                if (c < r) t[c] -= q->Lx[e] * t[r];
+            }
+        }
+    }
+    for (int j = 0; j < n; ++j) x[j] = t[q->pout[j]];
+}
+
+/* the same solve with float arithmetic (factors stored in float, rhs rounded to float,
+   src/linalg/local_solver.cpp:76-84) */
+static void local_solve_f(const OSub *q, const double *b, double *x, float *t)
+{
+    int n = q->n_local;
+    for (int k = 0; k < n; ++k) t[k] = (float)b[q->pin[k]];
+    for (int r = 0; r < n; ++r) {
+        float acc = t[r], dg = 1.0f;
+        for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e) {
+            int c = q->Li[e];
+            if (c < r) acc -= (float)q->Lx[e] * t[c];
+            else if (c == r) dg = (float)q->Lx[e];
+        }
+        t[r] = (q->kind == 1) ? acc / dg : acc;
+    }
+    if (q->kind == 0) {
+        for (int r = n - 1; r >= 0; --r) {
+            float acc = t[r], dg = 1.0f;
+            for (int64_t e = q->Up[r]; e < q->Up[r + 1]; ++e) {
+                int c = q->Ui[e];
+                if (c > r) acc -= (float)q->Ux[e] * t[c];
+                else if (c == r) dg = (float)q->Ux[e];
+            }
+            t[r] = acc / dg;
+        }
+    } else {
+        if (q->kind == 2)
+            for (int r = 0; r < n; ++r) t[r] /= (float)q->d[r];
+        for (int r = n - 1; r >= 0; --r) {
+            float dg = 1.0f;
+            if (q->kind == 1)
+                for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e)
+                    if (q->Li[e] == r) dg = (float)q->Lx[e];
+            t[r] /= dg;
+            for (int64_t e = q->Lp[r]; e < q->Lp[r + 1]; ++e) {
+                int c = q->Li[e];
+                if (c < r) t[c] -= (float)q->Lx[e] * t[r];
+            }
+        }
+    }
+    for (int j = 0; j < n; ++j) x[j] = (double)t[q->pout[j]];
+}
+
+void oracle_local_solve(const OSetup *s, int i, const double *b, double *x)
+{
+    const OSub *q = &s->sub[i];
+    if (q->single) {
+        float *t = (float *)malloc((size_t)q->n_local * sizeof(float));
+        local_solve_f(q, b, x, t);
+        free(t);
+    } else {
+        double *t = (double *)malloc((size_t)q->n_local * sizeof(double));
+        local_solve_d(q, b, x, t);
+        free(t);
+    }
+}
+
+/* z = M1^-1 r: halo forward, A_ii^-1, D (RAS), reverse accumulation (one_level_schwarz.cpp:80-99) */
+void oracle_one_level(OSetup *s, const double *r, double *z)
+{
+    int boolean = s->pou == 0, ras = s->one_level == 0;
+    for (int64_t g = 0; g < s->n; ++g) z[g] = 0.0;
+    for (int i = 0; i < s->nsub; ++i) {
+        OSub *q = &s->sub[i];
+        for (int j = 0; j < q->n_local; ++j) q->rloc[j] = r[q->l2g[j]]; /* R_i r (owned + forward) */
+        oracle_local_solve(s, i, q->rloc, q->yloc);
+        if (ras)
+            for (int j = 0; j < q->n_local; ++j) q->yloc[j] *= q->D[j];
+    }
+    /* z = sum_i R_i^T y_i: own rows, then the ghost copies of the other subdomains in order */
+    for (int i = 0; i < s->nsub; ++i) {
+        OSub *q = &s->sub[i];
+        for (int j = 0; j < q->n_owned; ++j) z[q->begin + j] += q->yloc[j];
+    }
+    if (!(ras && boolean))
+        for (int i = 0; i < s->nsub; ++i) {
+            OSub *q = &s->sub[i];
+            for (int j = q->n_owned; j < q->n_local; ++j) z[q->l2g[j]] += q->yloc[j];
+        }
+}
+
+/* x0 = R0^T E^-1 R0 r (coarse_space.cpp:208-246) */
+void oracle_coarse_apply(OSetup *s, const double *r, double *x0)
+{
+    int n0 = (int)s->n0;
+    for (int i = 0; i < s->nsub; ++i) { /* restrict: c_i = V_i^T R_i r */
+        OSub *q = &s->sub[i];
+        for (int a = 0; a < q->m; ++a) {
+            double t = 0.0;
+            for (int j = 0; j < q->n_local; ++j) t += q->V[(size_t)a * q->n_local + j] * r[q->l2g[j]];
+            s->c[s->coff[i] + a] = t;
+        }
+    }
+    /* solve E y = c with the LU */
+    for (int k = 0; k < n0; ++k) s->y[k] = s->c[k];
+    for (int k = 0; k < n0; ++k) { double t = s->y[k]; s->y[k] = s->y[s->piv[k]]; s->y[s->piv[k]] = t; }
+    for (int i = 0; i < n0; ++i) {
+        double t = s->y[i];
+        for (int k = 0; k < i; ++k) t -= s->ELU[(size_t)i * n0 + k] * s->y[k];
+        s->y[i] = t;
+    }
+    for (int i = n0 - 1; i >= 0; --i) {
+        double t = s->y[i];
+        for (int k = i + 1; k < n0; ++k) t -= s->ELU[(size_t)i * n0 + k] * s->y[k];
+        s->y[i] = t / s->ELU[(size_t)i * n0 + i];
+    }
+    /* prolong: x = sum_j R_j^T V_j y_j */
+    for (int64_t g = 0; g < s->n; ++g) x0[g] = 0.0;
+    for (int i = 0; i < s->nsub; ++i) {
+        OSub *q = &s->sub[i];
+        for (int j = 0; j < q->n_local; ++j) {
+            double t = 0.0;
+            for (int a = 0; a < q->m; ++a) t += q->V[(size_t)a * q->n_local + j] * s->y[s->coff[i] + a];
+            if (j < q->n_owned || s->pou != 0) x0[q->l2g[j]] += t;
+        }
+    }
+}
+
+/* two_level_schwarz.cpp:134-163 */
+void oracle_apply(OSetup *s, const double *r, double *z)
+{
+    if (s->coarse == 0 || s->n0 == 0) { oracle_one_level(s, r, z); return; }
+    oracle_coarse_apply(s, r, s->x0);
+    if (s->coarse == 1) {
+        oracle_one_level(s, r, z);
+        for (int64_t g = 0; g < s->n; ++g) z[g] += s->x0[g];
+    } else {
+        oracle_spmv(s, s->x0, s->w);
+        for (int64_t g = 0; g < s->n; ++g) s->w[g] = r[g] - s->w[g];
+        oracle_one_level(s, s->w, s->z1);
+        for (int64_t g = 0; g < s->n; ++g) z[g] = s->x0[g] + s->z1[g];
+    }
+}
+
+/* ------------------------------------------------------------------------ Krylov */
+typedef struct {
+    int converged, breakdown, iterations, restarts;
+    double rel_residual, true_rel_residual;
+    int history_len;
+    double *history;
+} OResult;
+
+static double dotv(int64_t n, const double *a, const double *b)
+{
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) t += a[i] * b[i];
+    return t;
+}
+
+static void hpush(OResult *res, int cap, double v)
+{
+    if (res->history && res->history_len < cap) res->history[res->history_len] = v;
+    if (res->history_len < cap) res->history_len++;
+}
+
+/* gmres.cpp:18-161; flexible = 1 keeps Z_j (not in the reference), strict = 1 accepts only a true
+   residual <= rtol (the reference accepts 1.1 rtol, gmres.cpp:148-156) */
+int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int maxit, int flexible, int strict,
+                 int hist_cap, OResult *res)
+{
+    int64_t n = s->n;
+    memset(res, 0, sizeof(*res) - sizeof(double *));
+    res->history_len = 0;
+    double bnorm = sqrt(dotv(n, b, b));
+    if (bnorm == 0.0) {
+        memset(x, 0, (size_t)n * sizeof(double));
+        res->converged = 1;
+        hpush(res, hist_cap, 0.0);
+        return 0;
+    }
+    double *V = (double *)malloc((size_t)n * (m + 1) * sizeof(double));
+    double *Z = flexible ? (double *)malloc((size_t)n * m * sizeof(double)) : NULL;
+    double *H = (double *)calloc((size_t)(m + 1) * m, sizeof(double));
+    double *cs = (double *)calloc((size_t)m, sizeof(double)), *sn = (double *)calloc((size_t)m, sizeof(double));
+    double *g = (double *)calloc((size_t)m + 1, sizeof(double)), *h = (double *)calloc((size_t)m + 1, sizeof(double));
+    double *h2 = (double *)calloc((size_t)m + 1, sizeof(double)), *yv = (double *)calloc((size_t)m + 1, sizeof(double));
+    double *r = (double *)malloc((size_t)n * sizeof(double)), *w = (double *)malloc((size_t)n * sizeof(double));
+    double *zz = (double *)malloc((size_t)n * sizeof(double)), *u = (double *)malloc((size_t)n * sizeof(double));
+#define HH(i, j) H[(size_t)(j) * (m + 1) + (i)]
+    oracle_spmv(s, x, r);
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
+    double beta = sqrt(dotv(n, r, r));
+    hpush(res, hist_cap, beta / bnorm);
+    res->rel_residual = beta / bnorm;
+    int converged = beta <= rtol * bnorm;
+    while (!converged && res->iterations < maxit) {
+        for (int64_t i = 0; i < n; ++i) V[i] = r[i] / beta;
+        memset(g, 0, (size_t)(m + 1) * sizeof(double));
+        g[0] = beta;
+        memset(H, 0, (size_t)(m + 1) * m * sizeof(double));
+        int k = 0, breakdown = 0;
+        for (int j = 0; j < m && res->iterations < maxit; ++j) {
+            double *zj = flexible ? Z + (size_t)j * n : zz;
+            oracle_apply(s, V + (size_t)j * n, zj);
+            oracle_spmv(s, zj, w);
+            for (int i = 0; i <= j; ++i) h[i] = dotv(n, V + (size_t)i * n, w);
+            for (int i = 0; i <= j; ++i) { double c = h[i]; const double *vi = V + (size_t)i * n; for (int64_t t = 0; t < n; ++t) w[t] -= c * vi[t]; }
+            for (int i = 0; i <= j; ++i) h2[i] = dotv(n, V + (size_t)i * n, w);
+            for (int i = 0; i <= j; ++i) { double c = h2[i]; const double *vi = V + (size_t)i * n; for (int64_t t = 0; t < n; ++t) w[t] -= c * vi[t]; }
+            double hn = sqrt(dotv(n, w, w));
+            for (int i = 0; i <= j; ++i) HH(i, j) = h[i] + h2[i];
+            HH(j + 1, j) = hn;
+            if (hn > 0.0)
+                for (int64_t t = 0; t < n; ++t) V[(size_t)(j + 1) * n + t] = w[t] / hn;
+            for (int i = 0; i < j; ++i) {
+                double t = cs[i] * HH(i, j) + sn[i] * HH(i + 1, j);
+                HH(i + 1, j) = -sn[i] * HH(i, j) + cs[i] * HH(i + 1, j);
+                HH(i, j) = t;
+            }
+            double den = hypot(HH(j, j), HH(j + 1, j));
+            cs[j] = den > 0.0 ? HH(j, j) / den : 1.0;
+            sn[j] = den > 0.0 ? HH(j + 1, j) / den : 0.0;
+            HH(j, j) = den;
+            HH(j + 1, j) = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            ++k;
+            ++res->iterations;
+            res->rel_residual = fabs(g[j + 1]) / bnorm;
+            hpush(res, hist_cap, res->rel_residual);
+            if (res->rel_residual <= rtol) { converged = 1; break; }
+            if (hn == 0.0) { breakdown = 1; break; }
+        }
+        for (int i = k - 1; i >= 0; --i) {
+            double t = g[i];
+            for (int c = i + 1; c < k; ++c) t -= HH(i, c) * yv[c];
+            yv[i] = t / HH(i, i);
+        }
+        const double *B = flexible ? Z : V;
+        for (int64_t t = 0; t < n; ++t) {
+            double acc = 0.0;
+            for (int c = 0; c < k; ++c) acc += B[(size_t)c * n + t] * yv[c];
+            u[t] = acc;
+        }
+        if (flexible) {
+            for (int64_t t = 0; t < n; ++t) x[t] += u[t];
+        } else {
+            oracle_apply(s, u, zz);
+            for (int64_t t = 0; t < n; ++t) x[t] += zz[t];
+        }
+        oracle_spmv(s, x, r);
+        for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
+        beta = sqrt(dotv(n, r, r));
+        int within = beta <= rtol * bnorm;
+        int within_slack = beta <= (strict ? 1.0 : 1.1) * rtol * bnorm;
+        if (breakdown) converged = within || converged;
+        if (converged && !within_slack) converged = 0;
+        if (beta == 0.0) converged = 1;
+        if (!converged) res->restarts++;
+    }
+#undef HH
+    res->converged = converged;
+    res->true_rel_residual = beta / bnorm;
+    free(V); free(Z); free(H); free(cs); free(sn); free(g); free(h); free(h2); free(yv); free(r); free(w); free(zz); free(u);
+    return 0;
+}
+
+/* bicgstab.cpp:15-154 (L2 test) */
+int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxit, int strict, int hist_cap,
+                    OResult *res)
+{
+    int64_t n = s->n;
+    memset(res, 0, sizeof(*res) - sizeof(double *));
+    double bnorm = sqrt(dotv(n, b, b));
+    if (bnorm == 0.0) {
+        memset(x, 0, (size_t)n * sizeof(double));
+        res->converged = 1;
+        hpush(res, hist_cap, 0.0);
+        return 0;
+    }
+    size_t sz = (size_t)n * sizeof(double);
+    double *r = (double *)malloc(sz), *rh = (double *)malloc(sz), *p = (double *)calloc((size_t)n, sizeof(double));
+    double *v = (double *)calloc((size_t)n, sizeof(double)), *y = (double *)malloc(sz), *sv = (double *)malloc(sz);
+    double *z = (double *)malloc(sz), *t = (double *)malloc(sz);
+    oracle_spmv(s, x, r);
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
+    double rn = sqrt(dotv(n, r, r));
+    hpush(res, hist_cap, rn / bnorm);
+    res->rel_residual = rn / bnorm;
+    for (;;) {
+        if (rn <= rtol * bnorm) { res->converged = 1; break; }
+        if (res->iterations >= maxit) break;
+        memcpy(rh, r, sz);
+        double rhn = rn, rho = rn * rn, rho_old = 1.0, alpha = 1.0, omega = 1.0;
+        int first = 1, candidate = 0;
+        while (res->iterations < maxit) {
+            if (first) memcpy(p, r, sz);
+            else {
+                double beta = (rho / rho_old) * (alpha / omega);
+                for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+            }
+            first = 0;
+            oracle_apply(s, p, y);
+            oracle_spmv(s, y, v);
+            ++res->iterations;
+            double rhv = dotv(n, rh, v);
+            if (rhv == 0.0 || !isfinite(rhv)) { res->breakdown = 1; break; }
+            alpha = rho / rhv;
+            for (int64_t i = 0; i < n; ++i) sv[i] = r[i] - alpha * v[i];
+            rn = sqrt(dotv(n, sv, sv));
+            res->rel_residual = rn / bnorm;
+            hpush(res, hist_cap, res->rel_residual);
+            if (rn <= rtol * bnorm || res->iterations >= maxit) {
+                for (int64_t i = 0; i < n; ++i) x[i] += alpha * y[i];
+                memcpy(r, sv, sz);
+                candidate = rn <= rtol * bnorm;
+                break;
+            }
+            oracle_apply(s, sv, z);
+            oracle_spmv(s, z, t);
+            ++res->iterations;
+            double tt = dotv(n, t, t), ts = dotv(n, t, sv);
+            omega = tt > 0.0 ? ts / tt : 0.0;
+            for (int64_t i = 0; i < n; ++i) { x[i] += alpha * y[i] + omega * z[i]; r[i] = sv[i] - omega * t[i]; }
+            rho_old = rho;
+            rn = sqrt(dotv(n, r, r));
+            rho = dotv(n, rh, r);
+            res->rel_residual = rn / bnorm;
+            hpush(res, hist_cap, res->rel_residual);
+            if (rn <= rtol * bnorm) { candidate = 1; break; }
+            if (omega == 0.0 || fabs(rho) < 1e-14 * rhn * rn) break;
+        }
+        oracle_spmv(s, x, t);
+        for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
+        rn = sqrt(dotv(n, r, r));
+        if (res->breakdown) break;
+        if (candidate && rn <= (strict ? 1.0 : 1.1) * rtol * bnorm) { res->converged = 1; break; }
+        if (res->iterations >= maxit) break;
+        res->restarts++;
+    }
+    res->true_rel_residual = rn / bnorm;
+    free(r); free(rh); free(p); free(v); free(y); free(sv); free(z); free(t);
+    return 0;
+}

@@ -1,0 +1,165 @@
+"""GPU solve phase against the CPU oracle, through the C ABI (libs2l_gpu.so).
+
+Tolerances (FP64 path): SpMV 1e-14 relative (same products, different summation grouping);
+local solves, coarse correction, one-level and two-level apply 1e-12 relative; Krylov iteration
+counts within +-1 of the oracle and the recomputed FP64 true residual <= rtol (1.1 rtol for the
+reference's slack rule).  FP32-factor path: within 1e-5 of the oracle's float solve.
+"""
+import numpy as np
+import pytest
+
+from conftest import small_setup
+from oracle.oracle import OracleSetup
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [(ol, co, pou) for ol in ("ras", "asm") for co in ("additive", "deflated", "none")
+            for pou in ("boolean", "multiplicity")]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from s2l_b200 import capi
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_spmv_matches(ctx, rng):
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st)
+    x = rng.standard_normal(st.n)
+    assert rel(g.spmv(x), st.A @ x) <= 1e-14
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["poisson2d", "bubbles3d", "convdiff3d"])
+def test_local_solves_match(ctx, rng, name):
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup(name)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    for i, s in enumerate(st.subdomains):
+        b = rng.standard_normal(s.n_local)
+        assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-12
+    g.close()
+
+
+@pytest.mark.parametrize("one_level,coarse,pou", VARIANTS)
+def test_apply_matches_oracle(ctx, rng, one_level, coarse, pou):
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup("poisson2d", nx=24, nsub=4, pou=pou, one_level=one_level, coarse=coarse)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    for _ in range(2):
+        r = rng.standard_normal(st.n)
+        assert rel(g.one_level_apply(r), o.one_level_apply(r)) <= 1e-12
+        if coarse != "none":
+            assert rel(g.coarse_apply(r), o.coarse_apply(r)) <= 1e-12
+        assert rel(g.apply(r), o.apply(r)) <= 1e-12
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["bubbles3d", "convdiff3d"])
+def test_apply_3d_matches_oracle(ctx, rng, name):
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup(name)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    r = rng.standard_normal(st.n)
+    assert rel(g.apply(r), o.apply(r)) <= 1e-12
+    # the same input twice gives bitwise-identical output (fixed-order kernels)
+    assert np.array_equal(g.apply(r), g.apply(r))
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["poisson2d", "bubbles3d", "convdiff3d"])
+def test_gmres_matches_oracle(ctx, name):
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup(name)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    x, res = g.gmres(st.b, restart=w.restart, rtol=1e-8)
+    xo, reso = o.gmres(st.b, restart=w.restart, rtol=1e-8)
+    assert res["converged"] and reso["converged"]
+    assert abs(res["iterations"] - reso["iterations"]) <= 1
+    true = np.linalg.norm(st.b - st.A @ x) / np.linalg.norm(st.b)
+    assert true <= 1.1e-8 and abs(true - res["true_rel_residual"]) <= 1e-10
+    n = min(res["history"].size, reso["history"].size)
+    assert np.allclose(res["history"][:n], reso["history"][:n], rtol=1e-6, atol=1e-13)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["poisson2d", "bubbles3d"])
+def test_bicgstab_matches_oracle(ctx, name):
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup(name)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    x, res = g.bicgstab(st.b, rtol=1e-8)
+    xo, reso = o.bicgstab(st.b, rtol=1e-8)
+    assert res["converged"] and reso["converged"]
+    assert abs(res["iterations"] - reso["iterations"]) <= 2
+    assert np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+    g.close()
+
+
+def test_single_precision_factors(ctx, rng):
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("convdiff3d", precision="single")
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    for i, s in enumerate(st.subdomains[:3]):
+        b = rng.standard_normal(s.n_local)
+        assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-5
+    x, res = g.gmres(st.b, restart=w.restart, rtol=1e-8, flexible=True, strict=True)
+    xo, reso = o.gmres(st.b, restart=w.restart, rtol=1e-8, flexible=True, strict=True)
+    assert res["converged"]
+    assert abs(res["iterations"] - reso["iterations"]) <= 2
+    assert np.linalg.norm(st.b - st.A @ x) <= 1e-8 * np.linalg.norm(st.b)
+    g.close()
+
+
+def test_device_pointers(ctx, rng):
+    import torch
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st)
+    r = rng.standard_normal(st.n)
+    rd = torch.tensor(r, device="cuda", dtype=torch.float64)
+    zd = torch.empty_like(rd)
+    torch.cuda.synchronize()
+    g.apply(rd.data_ptr(), out=zd.data_ptr())
+    assert rel(zd.cpu().numpy(), g.apply(r)) == 0.0
+    bd = torch.tensor(st.b, device="cuda", dtype=torch.float64)
+    xd = torch.zeros_like(bd)
+    _, res = g.gmres(bd.data_ptr(), restart=w.restart, device_out=xd.data_ptr())
+    x = xd.cpu().numpy()
+    assert res["converged"] and np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+    g.close()
+
+
+def test_bad_arguments_fail_loudly(ctx):
+    from s2l_b200 import capi
+    _, st = small_setup("poisson2d")
+    g = capi.GpuSetup(ctx, st)
+    with pytest.raises(ValueError):
+        g.apply(np.zeros(st.n + 1))
+    with pytest.raises(capi.S2LError):
+        g.local_solve(st.nsub + 3, np.zeros(4))
+    g.close()
+
+
+def test_hbm_budget_refusal():
+    from s2l_b200 import capi
+    _, st = small_setup("poisson2d")
+    c = capi.Context(0, hbm_budget=1 << 16)
+    with pytest.raises(capi.S2LError) as e:
+        capi.GpuSetup(c, st)
+    assert e.value.code == 2
+    c.close()

@@ -1,0 +1,94 @@
+"""The CPU oracle against dense sequential references of the same operators.
+
+Mirrors the reference's own test pattern (test/test_preconditioner.cpp:104-192): the two-level
+apply on the same partition is compared with a dense matrix assembled from the global matrix, the
+subdomain index sets, D_i and V_i, at 1e-9 there; the oracle must do far better (1e-12).
+"""
+import numpy as np
+import pytest
+
+from conftest import small_setup
+from oracle.oracle import OracleSetup
+
+VARIANTS = [(ol, co, pou) for ol in ("ras", "asm") for co in ("additive", "deflated", "none")
+            for pou in ("boolean", "multiplicity")]
+
+
+def dense_apply_operator(st, one_level, coarse):
+    n = st.n
+    Ad = st.A.toarray()
+    M1 = np.zeros((n, n))
+    R0 = np.zeros((st.n0, n))
+    for i, s in enumerate(st.subdomains):
+        l2g = s.l2g()
+        inv = np.linalg.inv(Ad[np.ix_(l2g, l2g)])
+        M1[np.ix_(l2g, l2g)] += (np.diag(s.D) @ inv) if one_level == "ras" else inv
+        if st.n0:
+            R0[st.offsets[i]:st.offsets[i + 1], l2g] = s.V.T
+    if coarse == "none" or st.n0 == 0:
+        return M1
+    Q = R0.T @ np.linalg.solve(R0 @ Ad @ R0.T, R0)
+    if coarse == "additive":
+        return Q + M1
+    return Q + M1 @ (np.eye(n) - Ad @ Q)
+
+
+@pytest.mark.parametrize("one_level,coarse,pou", VARIANTS)
+def test_apply_matches_dense_reference(one_level, coarse, pou, rng):
+    _, st = small_setup("poisson2d", nx=24, nsub=4, pou=pou, one_level=one_level, coarse=coarse)
+    o = OracleSetup(st)
+    M = dense_apply_operator(st, one_level, coarse)
+    for _ in range(2):
+        r = rng.standard_normal(st.n)
+        z = o.apply(r)
+        zr = M @ r
+        assert np.linalg.norm(z - zr) <= 1e-12 * np.linalg.norm(zr)
+
+
+@pytest.mark.parametrize("name", ["bubbles3d", "convdiff3d"])
+def test_apply_3d_matches_dense(name, rng):
+    _, st = small_setup(name, nx=10, nsub=4, nbubbles=3) if name == "bubbles3d" else small_setup(name, nx=10, nsub=4)
+    o = OracleSetup(st)
+    M = dense_apply_operator(st, st.opts.one_level, st.opts.coarse)
+    r = rng.standard_normal(st.n)
+    zr = M @ r
+    assert np.linalg.norm(o.apply(r) - zr) <= 1e-12 * np.linalg.norm(zr)
+
+
+def test_local_solve_and_spmv(rng):
+    _, st = small_setup("bubbles3d", nx=12, nsub=4, nbubbles=4)
+    o = OracleSetup(st)
+    x = rng.standard_normal(st.n)
+    assert np.array_equal(o.spmv(x), st.A @ x) or np.allclose(o.spmv(x), st.A @ x, rtol=1e-15, atol=1e-15)
+    for i, s in enumerate(st.subdomains):
+        b = rng.standard_normal(s.n_local)
+        y = o.local_solve(i, b)
+        assert np.linalg.norm(s.Aii @ y - b) <= 1e-12 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name", ["poisson2d", "bubbles3d", "convdiff3d"])
+def test_krylov_converges(name):
+    w, st = small_setup(name)
+    o = OracleSetup(st)
+    x, res = o.gmres(st.b, restart=w.restart, rtol=1e-8)
+    assert res["converged"]
+    assert np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+    assert res["history"].size == res["iterations"] + 1 + 0 * res["restarts"] or res["restarts"] > 0
+    x2, res2 = o.bicgstab(st.b, rtol=1e-8)
+    assert res2["converged"]
+    assert np.linalg.norm(st.b - st.A @ x2) <= 1.1e-8 * np.linalg.norm(st.b)
+
+
+def test_gmres_zero_rhs():
+    _, st = small_setup("poisson2d")
+    o = OracleSetup(st)
+    x, res = o.gmres(np.zeros(st.n))
+    assert res["converged"] and res["iterations"] == 0 and not np.any(x)
+
+
+def test_single_precision_factors_flexible_gmres():
+    w, st = small_setup("convdiff3d", precision="single")
+    o = OracleSetup(st)
+    x, res = o.gmres(st.b, restart=w.restart, rtol=1e-8, flexible=True, strict=True)
+    assert res["converged"]
+    assert np.linalg.norm(st.b - st.A @ x) <= 1e-8 * np.linalg.norm(st.b)
