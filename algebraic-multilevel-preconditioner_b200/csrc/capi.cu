@@ -131,7 +131,8 @@ struct s2l_setup {
     double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
     double* d_coef = nullptr;
     // profiling
-    bool prof = false;
+    unsigned prof = 0;  // bit c: time kernel class c
+    long launches = 0;  // kernel launches issued by this setup
     struct Ev {
         int cls;
         cudaEvent_t a, b;
@@ -368,7 +369,7 @@ int upload_real(s2l_setup* s, void** dst, const std::vector<double>& v)
 // ------------------------------------------------------------------------------ profiling
 void prof_begin(s2l_setup* s, int cls, cudaEvent_t* a)
 {
-    if (!s->prof) return;
+    if (!(s->prof & (1u << cls))) return;
     if (s->pool.empty()) {
         cudaEvent_t e;
         cudaEventCreate(&e);
@@ -382,7 +383,7 @@ void prof_begin(s2l_setup* s, int cls, cudaEvent_t* a)
 
 void prof_end(s2l_setup* s, int cls, cudaEvent_t a)
 {
-    if (!s->prof) return;
+    if (!(s->prof & (1u << cls))) return;
     if (s->pool.empty()) {
         cudaEvent_t e;
         cudaEventCreate(&e);
@@ -449,6 +450,7 @@ int run_local_solve(s2l_setup* s, const double* in, const double* base, double* 
         a.xscratch = (float*)s->d_xscratch;
         a.mode = mode;
         e = launch_local_solve<float>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
+        s->launches += 1;
     } else {
         SolveArgs<double> a{};
         a.subs = s->d_subs;
@@ -468,6 +470,7 @@ int run_local_solve(s2l_setup* s, const double* in, const double* base, double* 
         a.xscratch = (double*)s->d_xscratch;
         a.mode = mode;
         e = launch_local_solve<double>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
+        s->launches += 1;
     }
     if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
     return S2L_OK;
@@ -481,6 +484,7 @@ int one_level(s2l_setup* s, const double* in, const double* base, double* out)
     Prof pr(s, PC_COMBINE);
     launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, s->one_level == S2L_ONE_LEVEL_RAS ? s->d_cp_w : nullptr,
                    s->d_ylocal, base, out);
+    s->launches += 1;
     return S2L_OK;
 }
 
@@ -496,6 +500,7 @@ int coarse_apply(s2l_setup* s, const double* r, double* x0)
     launch_coarse_prolong(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
                           s->d_y, x0, s->d_plocal);
     if (!boolean) launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, s->d_plocal, nullptr, x0);
+    s->launches += boolean ? 4 : 5;
     return S2L_OK;
 }
 
@@ -504,6 +509,7 @@ int spmv_dev(s2l_setup* s, const double* x, double* y, const double* b, bool wit
     Prof pr(s, PC_SPMV);
     launch_spmv(s->stream, s->n, s->d_rp, s->d_ci, s->d_av, x, y, b, with_norm ? s->d_part : nullptr,
                 s->d_red + 256, s->tpr);
+    s->launches += with_norm ? 2 : 1;
     return S2L_OK;
 }
 
@@ -582,6 +588,7 @@ int norm2_dev(s2l_setup* s, const double* x, double* out_host)
     {
         Prof pr(s, PC_VEC);
         launch_dot2(s->stream, s->n, x, x, nullptr, s->d_part, s->d_red + 256);
+        s->launches += 2;
     }
     RET_IF(read_red(s, 256, 1));
     *out_host = std::sqrt(s->h_red[256]);
@@ -1084,7 +1091,8 @@ int s2l_gpu_profile_enable(s2l_setup* s, int on)
         s->acc_ms[c] = 0.0;
         s->acc_n[c] = 0;
     }
-    s->prof = on != 0;
+    s->prof = (unsigned)on & 0x1Fu;
+    s->launches = 0;
     return S2L_OK;
 }
 
@@ -1092,6 +1100,11 @@ int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launch
 {
     if (!s || !name || !ms || !launches) return S2L_ERR_BADARG;
     prof_drain(s);
+    if (std::strcmp(name, "launches") == 0) {
+        *ms = 0.0;
+        *launches = s->launches;
+        return S2L_OK;
+    }
     if (std::strcmp(name, "all") == 0) {
         *ms = 0;
         *launches = 0;
@@ -1240,6 +1253,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         {
             Prof pr(s, PC_VEC);
             launch_axpby(st, n, 1.0 / beta, r, 0.0, V);
+            s->launches += 1;
         }
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
@@ -1257,6 +1271,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
                 launch_mdot(st, n, V, n, j + 1, w, s->d_part, s->d_red + 128);
                 launch_gemv_update(st, n, V, n, j + 1, s->d_red + 128, -1.0, w, s->d_part);
                 launch_reduce(st, s->d_part, S2L_NB_RED, 1, s->d_red + 256);
+                s->launches += 7;
             }
             CUDA_OK(s, cudaMemcpyAsync(s->h_red, s->d_red, 257 * sizeof(double), cudaMemcpyDeviceToHost, st));
             CUDA_OK(s, cudaStreamSynchronize(st));
@@ -1266,6 +1281,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
             if (hn > 0.0) {
                 Prof pr(s, PC_VEC);
                 launch_axpby(st, n, 1.0 / hn, w, 0.0, V + (size_t)(j + 1) * n);
+                s->launches += 1;
             }
             for (int i = 0; i < j; ++i) {
                 const double t = cs[i] * Hc(i, j) + sn[i] * Hc(i + 1, j);
@@ -1303,14 +1319,17 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         {
             Prof pr(s, PC_VEC);
             launch_gemv(st, n, flex ? Z : V, n, k, s->d_coef, s->d_u);
+            s->launches += 1;
         }
         if (flex) {
             Prof pr(s, PC_VEC);
             launch_axpby(st, n, 1.0, s->d_u, 1.0, dx);
+            s->launches += 1;
         } else {
             RET_IF(apply_dev(s, s->d_u, z));
             Prof pr(s, PC_VEC);
             launch_axpby(st, n, 1.0, z, 1.0, dx);
+            s->launches += 1;
         }
         RET_IF(spmv_dev(s, dx, r, db, true));
         RET_IF(read_red(s, 256, 1));
@@ -1397,6 +1416,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             {
                 Prof pr(s, PC_VEC);
                 launch_bicg_p(st, n, r, v, first ? 0.0 : (rho / rho_old) * (alpha / omega), omega, p, first ? 1 : 0);
+                s->launches += 1;
             }
             first = false;
             RET_IF(apply_dev(s, p, y));
@@ -1405,6 +1425,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             {
                 Prof pr(s, PC_VEC);
                 launch_dot2(st, n, rh, v, nullptr, s->d_part, s->d_red + 256);
+                s->launches += 2;
             }
             RET_IF(read_red(s, 256, 1));
             const double rhv = s->h_red[256];
@@ -1416,6 +1437,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             {
                 Prof pr(s, PC_VEC);
                 launch_bicg_s(st, n, r, v, alpha, sv, nullptr, s->d_part, s->d_red + 256);
+                s->launches += 2;
             }
             RET_IF(read_red(s, 256, 1));
             rn = std::sqrt(s->h_red[256]);
@@ -1424,6 +1446,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             if (satisfied(1.0) || res->iterations >= o->maxit) {
                 Prof pr(s, PC_VEC);
                 launch_axpby(st, n, alpha, y, 1.0, dx);
+                s->launches += 1;
                 CUDA_OK(s, cudaMemcpyAsync(r, sv, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
                 candidate = satisfied(1.0);
                 break;
@@ -1434,6 +1457,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             {
                 Prof pr(s, PC_VEC);
                 launch_dot2(st, n, t, t, sv, s->d_part, s->d_red + 256);
+                s->launches += 2;
             }
             RET_IF(read_red(s, 256, 2));
             const double tt = s->h_red[256], ts = s->h_red[257];
@@ -1441,6 +1465,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             {
                 Prof pr(s, PC_VEC);
                 launch_bicg_x(st, n, dx, y, zv, alpha, omega, r, sv, t, rh, s->d_part, s->d_red + 256);
+                s->launches += 2;
             }
             RET_IF(read_red(s, 256, 2));
             rho_old = rho;

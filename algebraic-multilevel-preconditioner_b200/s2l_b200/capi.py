@@ -248,7 +248,12 @@ class GpuSetup:
             x = device_out
         else:
             b = np.ascontiguousarray(b, dtype=np.float64)
-            x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+            if x0 is None:
+                x = np.zeros(self.n)
+            elif isinstance(x0, np.ndarray) and x0.dtype == np.float64 and x0.flags.c_contiguous and x0.size == self.n:
+                x = x0  # used in place (keeps a pinned buffer pinned)
+            else:
+                x = np.array(x0, dtype=np.float64)
             self.ctx.check(fn(self.h, _vp(b), _vp(x), PTR_HOST, C.byref(o), C.byref(res)))
         out = {"converged": bool(res.converged), "breakdown": bool(res.breakdown), "iterations": res.iterations,
                "restarts": res.restarts, "rel_residual": res.rel_residual,
@@ -267,8 +272,17 @@ class GpuSetup:
     def set_stream(self, stream_ptr: int | None):
         self.ctx.check(self.lib.s2l_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
 
-    def profile(self, on=True):
-        self.ctx.check(self.lib.s2l_gpu_profile_enable(self.h, 1 if on else 0))
+    PROF = {"spmv": 1, "local_solve": 2, "coarse": 4, "combine": 8, "krylov_vec": 16, "all": 31}
+
+    def profile(self, classes=("all",)):
+        """Time the given kernel classes with CUDA events (empty: off); resets counters."""
+        mask = 0
+        for c in classes:
+            mask |= self.PROF[c]
+        self.ctx.check(self.lib.s2l_gpu_profile_enable(self.h, mask))
+
+    def launches(self) -> int:
+        return self.profile_get("launches")[1]
 
     def profile_get(self, name):
         ms = C.c_double()

@@ -498,3 +498,27 @@ def cached(key: dict, make):
             pickle.dump(st, f, protocol=pickle.HIGHEST_PROTOCOL)
         os.replace(tmp, path)
     return st
+
+
+def with_factor_precision(st: Setup, precision: str) -> Setup:
+    """Shallow copy of a setup whose local factors are stored in ``precision`` ('single'/'double').
+
+    The factors are rounded from the FP64 factorization (the reference factorizes in float when
+    ``--local-precision single``, ``src/linalg/local_solver.cpp:66-84``; rounding an FP64 factor
+    is the mixed-precision form used here); everything else is shared.
+    """
+    import copy
+    dt = np.float32 if precision == "single" else np.float64
+    out = copy.copy(st)
+    out.opts = copy.copy(st.opts)
+    out.opts.local_precision = precision
+    subs = []
+    for s in st.subdomains:
+        f = s.factor
+        nf = LocalFactor(f.kind, f.L.astype(dt), f.U.astype(dt) if f.U is not None else None, f.perm_in, f.perm_out,
+                         f.d.astype(dt) if f.d is not None else None)
+        ns = copy.copy(s)
+        ns.factor = nf
+        subs.append(ns)
+    out.subdomains = subs
+    return out

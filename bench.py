@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 solve phase: solves to a true FP64 residual of 1e-8.
+
+Workload (default): 3D 7-point variable-coefficient pressure Poisson 100^3 (n = 1.0M),
+beta = 1/rho with rho = 1e-3 in 200 seeded spheres of radius 3-8 cells, 64 subdomains (recursive
+coordinate bisection), overlap 2, nev 20, deflated two-level RAS, local L L^T, GMRES(50),
+rtol 1e-8, U[-1,1] right-hand side (seed 12345).  Two forms are timed:
+  plain_fp64  : FP64 factors, the reference's GMRES (true-residual restart rule),
+  mixed       : the same factors stored in FP32 + flexible GMRES(50) in FP64, converged only when
+                the recomputed FP64 true residual is <= rtol.
+A step is one full solve from x0 = 0.  `value` = solves/s of the mixed form with b resident in
+HBM; `e2e` = the same through the C ABI with host buffers (copies inside the timed region).
+
+--impl reference times the reference itself (built from its sources into oracle/_ref/ with an
+in-process thread-rank MPI) on the host cores, same problem and partition.
+With torchrun (N > 1) every rank solves its own replica (the solve phase has no cross-GPU step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "algebraic-multilevel-preconditioner_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "solve time to FP64 residual 1e-8 (mixed/batched vs plain FP64 GPU); p50/p99 latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=100)
+    ap.add_argument("--nsub", type=int, default=64)
+    ap.add_argument("--nbubbles", type=int, default=200)
+    ap.add_argument("--overlap", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-threads", type=int, default=0, help="reference arm: host threads (0 = all)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+# ------------------------------------------------------------------------------------ our arm
+def run_ours(a):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    os.environ.setdefault("S2L_CACHE_DIR", os.path.join(REPO, "_cache"))
+    from s2l_b200 import workloads as W
+    from s2l_b200.setup_phase import with_factor_precision
+
+    wl = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=900))
+        # rank 0 fills the setup cache first; the replicas then load it (setup is outside the timing)
+        if rank == 0:
+            st = W.build(wl)
+        dist.barrier()
+        if rank != 0:
+            st = W.build(wl)
+    else:
+        t0 = time.time()
+        st = W.build(wl)
+        setup_s = time.time() - t0
+    # ---- device (no CUDA call before the setup's process pool is done)
+    import numpy as np
+    import torch
+    from s2l_b200 import capi
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = capi.Context(local)
+    st32 = with_factor_precision(st, "single")
+    g64 = capi.GpuSetup(ctx, st)
+    g32 = capi.GpuSetup(ctx, st32)
+    stream = torch.cuda.current_stream(dev)
+    for g in (g64, g32):
+        g.set_stream(stream.cuda_stream)
+    n = st.n
+    b_dev = torch.tensor(st.b, device=dev, dtype=torch.float64)
+    x_dev = torch.zeros(n, device=dev, dtype=torch.float64)
+    forms = {
+        "plain_fp64": (g64, dict(restart=wl.restart, rtol=wl.rtol, flexible=False, strict=False)),
+        "mixed": (g32, dict(restart=wl.restart, rtol=wl.rtol, flexible=True, strict=True)),
+    }
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    peak, peak_src = measured_peaks()
+    sampler = None
+    for name, (g, kw) in forms.items():
+        for _ in range(a.warmup):
+            x_dev.zero_()
+            g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
+        headline = name == "mixed"
+        g.profile(("local_solve",))
+        if headline:
+            sampler = ClockSampler(local)
+            sampler.start()
+        barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        its = []
+        conv = []
+        true_res = []
+        for k in range(a.steps):
+            ev[k][0].record(stream)
+            x_dev.zero_()
+            _, res = g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
+            ev[k][1].record(stream)
+            its.append(res["iterations"])
+            conv.append(res["converged"])
+            true_res.append(res["true_rel_residual"])
+        barrier()
+        per = [s.elapsed_time(e) for s, e in ev]
+        total_ms = max_over_ranks(sum(per))
+        clocks = sampler.stop() if headline else None
+        ls_ms, ls_n = g.profile_get("local_solve")
+        launches = g.launches()
+        g.profile(())
+        # independent FP64 check of the last solution
+        x = x_dev.cpu().numpy()
+        true_chk = float(np.linalg.norm(st.b - st.A @ x) / np.linalg.norm(st.b))
+        results[name] = {
+            "ms_per_solve": total_ms / a.steps, "per_solve_ms": per, "iterations": its, "converged": all(conv),
+            "true_rel_residual": max(true_res), "true_rel_residual_host_check": true_chk,
+            "local_solve_ms_total": ls_ms, "local_solve_launches": ls_n, "launches": launches,
+            "local_solve_bytes": g.local_solve_bytes(), "clocks": clocks,
+            "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+        }
+    # ---- end to end through the C ABI with pinned host buffers (headline form)
+    g, kw = forms["mixed"]
+    b_pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    b_pin.numpy()[:] = st.b
+    x_pin = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+    barrier()
+    e2e = []
+    for k in range(a.steps):
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x_pin.zero_()
+        s_ev.record(stream)
+        g.gmres(b_pin.numpy(), x0=x_pin.numpy(), history_cap=0, **kw)
+        e_ev.record(stream)
+        e_ev.synchronize()
+        e2e.append(s_ev.elapsed_time(e_ev))
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e))
+
+    head = results["mixed"]
+    plain = results["plain_fp64"]
+    ls_avg_ms = head["local_solve_ms_total"] / max(head["local_solve_launches"], 1)
+    achieved = head["local_solve_bytes"] / (ls_avg_ms * 1e-3) / 1e9 if ls_avg_ms > 0 else 0.0
+    ls_avg_ms64 = plain["local_solve_ms_total"] / max(plain["local_solve_launches"], 1)
+    achieved64 = plain["local_solve_bytes"] / (ls_avg_ms64 * 1e-3) / 1e9 if ls_avg_ms64 > 0 else 0.0
+    out = {
+        "metric": METRIC,
+        "value": world * a.steps / (sum([head["ms_per_solve"] * a.steps]) * 1e-3),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": head["ms_per_solve"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (FP32 local factors, FP64 Krylov/coarse/true residual)",
+        "data": "synthetic (seeded generator, U[-1,1] rhs)",
+        "config": {
+            "workload": f"bubbles3d {a.nx}^3 pressure Poisson, {a.nsub} subdomains, overlap {a.overlap}, nev 20, "
+                        f"deflated RAS, LL^T factors, GMRES(50), rtol 1e-8",
+            "n": st.n, "nnz": int(st.A.nnz), "n0": st.n0, "nnz_factors": st.stats.get("nnz_factors"),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU, all subdomains resident",
+            "l2": "inputs larger than L2 (local factors %.1f GB per form)" % (head["local_solve_bytes"] / 1e9),
+            "setup_s": round(setup_s, 1) if world == 1 else None,
+        },
+        "forms": {
+            "mixed": {k: head[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
+                                            "true_rel_residual_host_check", "p50_ms", "p99_ms")},
+            "plain_fp64": {k: plain[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
+                                                  "true_rel_residual_host_check", "p50_ms", "p99_ms")},
+            "speedup_mixed_vs_plain": plain["ms_per_solve"] / head["ms_per_solve"],
+            "iteration_delta_mixed_vs_plain": head["iterations"][0] - plain["iterations"][0],
+        },
+        "p50_ms": head["p50_ms"],
+        "p99_ms": head["p99_ms"],
+        "e2e": {"value": world * a.steps / (e2e_total * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n,
+                "ms_per_solve": e2e_total / a.steps},
+        "roofline": {"bound": "hbm", "kernel": "local_solve (fused gather + L/U triangular solves + PoU write)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": None,
+                     "bytes_per_launch": head["local_solve_bytes"], "avg_launch_ms": ls_avg_ms,
+                     "fp64_form": {"achieved": achieved64, "frac": achieved64 / peak, "avg_launch_ms": ls_avg_ms64,
+                                   "bytes_per_launch": plain["local_solve_bytes"]}},
+        "gpu_launches": head["launches"],
+        "clocks": head["clocks"],
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(st, plain["iterations"][0], wl.restart)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    g64.close()
+    g32.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(st, iterations: int, restart: int) -> dict:
+    """The oracle (sequential C restatement) on a bounded sample: 3 GMRES iterations of the same solve."""
+    from oracle.oracle import OracleSetup
+    o = OracleSetup(st)
+    t0 = time.perf_counter()
+    _, res = o.gmres(st.b, restart=restart, rtol=1e-8, maxit=3)
+    dt = time.perf_counter() - t0
+    o.close()
+    per_it = dt / max(res["iterations"], 1)
+    est = per_it * iterations
+    return {"value": 1.0 / est, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": f"{res['iterations']} GMRES iterations of the same FP64 solve ({dt:.1f} s, "
+                      f"{per_it * 1e3:.0f} ms/iteration), scaled to the GPU's {iterations} iterations"}
+
+
+# ------------------------------------------------------------------------------------ reference arm
+def run_reference(a):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    binary = os.path.join(REPO, "oracle", "_ref", "s2l_ref_bench")
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/s2l_ref_bench was not built "
+                                                             "(the reference compiles only where its sources are)"}))
+        return
+    import numpy as np
+    from s2l_b200 import workloads as W
+    from s2l_b200.rng import random_rhs  # noqa: F401  (the reference draws the same rhs itself)
+
+    wl = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap)
+    prob = W.make_problem(wl)
+    part = W.make_partition(wl, prob).astype(np.int32)
+    threads = a.ref_threads or os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        mtx = os.path.join(td, "A.mtx")
+        write_mtx(mtx, prob.A)
+        pf = os.path.join(td, "part.bin")
+        part.tofile(pf)
+        env = dict(os.environ, S2L_NP=str(a.nsub), S2L_PART_FILE=pf, OMP_NUM_THREADS="1",
+                   S2L_REF_THREADS=str(threads))
+        cmd = [binary, "--matrix", mtx, "--rhs", "random", "--seed", str(wl.seed), "--pou", "boolean",
+               "--one-level", "ras", "--coarse", "deflated", "--nev", "20", "--local-solver", "sparselu",
+               "--local-factorization", "cholesky", "--coarse-solver", "root", "--krylov", "gmres",
+               "--restart", str(wl.restart), "--rtol", str(wl.rtol), "--verbose", "0",
+               "--bench-steps", str(a.steps), "--bench-warmup", str(a.warmup)]
+        r = subprocess.run(cmd, env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed ({r.returncode}): "
+                                                              f"{r.stderr.strip().splitlines()[-1:]}"}))
+        return
+    rec = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    per = rec["solve_s"]
+    ms = 1e3 * sum(per) / len(per)
+    value = 1e3 / ms
+    out = {
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "solves/s", "n_gpus": a.gpus,
+        "steps": len(per), "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (same generator, partition and rhs)",
+        "config": {"workload": f"bubbles3d {a.nx}^3 pressure Poisson, {a.nsub} subdomains, overlap 1 (the "
+                               f"reference has no overlap 2), nev 20, deflated RAS, Eigen LL^T, root coarse "
+                               f"solver, GMRES(50), rtol 1e-8",
+                   "n": int(prob.n), "iterations": rec.get("iterations"), "setup_s": rec.get("setup_s"),
+                   "true_rel_residual": rec.get("true_rel_residual")},
+        "p50_ms": float(np.percentile(np.array(per) * 1e3, 50)), "p99_ms": float(np.percentile(np.array(per) * 1e3, 99)),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
+                         "sample": f"{len(per)} full solves, {a.nsub} thread-ranks on {threads} host threads"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def write_mtx(path, A):
+    """Matrix Market coordinate file (1-based), full precision."""
+    import numpy as np
+    A = A.tocoo()
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{A.shape[0]} {A.shape[1]} {A.nnz}\n")
+        data = np.column_stack([A.row + 1, A.col + 1, A.data])
+        np.savetxt(f, data, fmt=["%d", "%d", "%.17g"])
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)

@@ -142,10 +142,14 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
 /* ---- streams and measurement -------------------------------------------------------------- */
 /* Launch on this CUDA stream (cudaStream_t passed as a pointer; NULL = the setup's own stream). */
 int s2l_gpu_set_stream(s2l_setup* s, void* stream);
-/* 1: time every kernel class with CUDA events on the launching stream. */
-int s2l_gpu_profile_enable(s2l_setup* s, int on);
+/* Kernel classes timed with CUDA events on the launching stream (bit mask; 0 = off). */
+enum { S2L_PROF_SPMV = 1, S2L_PROF_LOCAL_SOLVE = 2, S2L_PROF_COARSE = 4, S2L_PROF_COMBINE = 8,
+       S2L_PROF_KRYLOV_VEC = 16, S2L_PROF_ALL = 31 };
+/* Enables the classes of `mask` and resets the accumulators and the launch counter. */
+int s2l_gpu_profile_enable(s2l_setup* s, int mask);
 /* Accumulated event time [ms] and launch count of one kernel class; names: "spmv", "local_solve",
-   "coarse", "combine", "krylov_vec", "all".  Resets with s2l_gpu_profile_enable(s, 1). */
+   "coarse", "combine", "krylov_vec", "all"; "launches" gives every kernel launch of the setup since
+   the last s2l_gpu_profile_enable (timed or not) in *launches. */
 int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launches);
 /* Algorithmic bytes read+written by one local_solve launch (the roofline numerator). */
 int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes);
