@@ -8,6 +8,8 @@
 #include "s2l_internal.cuh"
 #include "../../include/s2l_gpu.h"
 
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -99,8 +101,23 @@ struct s2l_setup {
     int32_t* d_col[2] = {nullptr, nullptr};
     void* d_val[2] = {nullptr, nullptr};
     void* d_dinv[2] = {nullptr, nullptr};
-    int32_t* d_lvl = nullptr;
-    int8_t* d_mode = nullptr;
+    int32_t *d_tr_sub = nullptr, *d_tr_i = nullptr, *d_lts_col = nullptr;
+    int64_t* d_lts_ptr = nullptr;
+    void* d_lts_val = nullptr;
+    int32_t *d_us_sub = nullptr, *d_us_r = nullptr, *d_ust_col = nullptr;
+    int64_t* d_ust_ptr = nullptr;
+    void* d_ust_val = nullptr;
+    void *d_linv = nullptr, *d_uinv = nullptr;
+    void *d_ybuf = nullptr, *d_xbuf = nullptr;
+    uint8_t* d_gflags = nullptr;
+    int* d_err = nullptr;
+    std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
+    int sweep_group = 32;
+    // options (s2l_gpu_setup_option)
+    int opt_tail_min = 96, opt_tail_max = 4096, opt_group = 0;
+    double opt_tail_density = 0.25;
+    // statistics
+    int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
     int32_t *d_gin = nullptr, *d_pin = nullptr, *d_gout = nullptr, *d_l2g = nullptr;
     double* d_D = nullptr;
     int64_t* d_cp_ptr = nullptr;
@@ -117,7 +134,6 @@ struct s2l_setup {
     // work vectors
     double *d_ylocal = nullptr, *d_x0 = nullptr, *d_w = nullptr, *d_in = nullptr, *d_out = nullptr;
     double* d_plocal = nullptr;
-    void* d_xscratch = nullptr;
     double* d_part = nullptr;
     double* d_red = nullptr;
     double* h_red = nullptr;
@@ -166,6 +182,8 @@ struct s2l_setup {
 
 namespace {
 
+int check_err(s2l_setup* s);
+
 int dev_alloc(s2l_setup* s, void** p, size_t bytes)
 {
     *p = nullptr;
@@ -210,12 +228,14 @@ int alloc_doubles(s2l_setup* s, double** p, size_t count)
     return dev_alloc(s, reinterpret_cast<void**>(p), count * sizeof(double));
 }
 
-// level schedule of a triangular CSR (lower: forward; upper: backward)
-void build_sched(const HostCsr& M, int n, bool lower, bool unit_diag, Sched& out, std::string& err)
+// Sweep schedule of the sparse part of a triangular factor: rows [0, T), off-diagonal entries
+// with a column < T, rows sorted by dependency level (lower: forward, upper: backward), which is a
+// topological order of the rows with independent rows next to each other.
+void build_sweep(const HostCsr& M, int n, int T, bool lower, bool unit_diag, Sched& out, std::string& err)
 {
-    std::vector<int32_t> level(n, 0);
-    std::vector<double> diag(n, 1.0);
-    std::vector<int64_t> offcnt(n, 0);
+    std::vector<int32_t> level(T, 0);
+    std::vector<double> diag(T, 1.0);
+    std::vector<int64_t> offcnt(T, 0);
     auto visit = [&](int r) {
         int lv = 0;
         for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
@@ -224,41 +244,40 @@ void build_sched(const HostCsr& M, int n, bool lower, bool unit_diag, Sched& out
                 diag[r] = M.v[e];
                 continue;
             }
-            if (lower ? (c > r) : (c < r)) continue;  // wrong triangle: ignored (checked by caller)
+            if (lower ? (c > r) : (c < r || c >= T)) continue;
             lv = std::max(lv, level[c] + 1);
             ++offcnt[r];
         }
         level[r] = lv;
     };
     if (lower)
-        for (int r = 0; r < n; ++r) visit(r);
+        for (int r = 0; r < T; ++r) visit(r);
     else
-        for (int r = n - 1; r >= 0; --r) visit(r);
+        for (int r = T - 1; r >= 0; --r) visit(r);
     int nlev = 0;
-    for (int r = 0; r < n; ++r) nlev = std::max(nlev, level[r] + 1);
-    if (n == 0) nlev = 0;
+    for (int r = 0; r < T; ++r) nlev = std::max(nlev, level[r] + 1);
     std::vector<int32_t> cnt(nlev + 1, 0);
-    for (int r = 0; r < n; ++r) ++cnt[level[r] + 1];
+    for (int r = 0; r < T; ++r) ++cnt[level[r] + 1];
     for (int l = 0; l < nlev; ++l) cnt[l + 1] += cnt[l];
     out.lvl.assign(cnt.begin(), cnt.end());
     std::vector<int32_t> next(cnt.begin(), cnt.end() - 1);
-    out.rows.assign(n, 0);
+    out.rows.assign(T, 0);
     if (lower) {
-        for (int r = 0; r < n; ++r) out.rows[next[level[r]]++] = r;
+        for (int r = 0; r < T; ++r) out.rows[next[level[r]]++] = r;
     } else {
-        for (int r = n - 1; r >= 0; --r) out.rows[next[level[r]]++] = r;
+        for (int r = T - 1; r >= 0; --r) out.rows[next[level[r]]++] = r;
     }
-    out.ptr.assign(n + 1, 0);
-    for (int p = 0; p < n; ++p) out.ptr[p + 1] = out.ptr[p] + offcnt[out.rows[p]];
-    out.col.resize(out.ptr[n]);
-    out.val.resize(out.ptr[n]);
-    out.dinv.resize(n);
-    for (int p = 0; p < n; ++p) {
+    out.ptr.assign(T + 1, 0);
+    for (int p = 0; p < T; ++p) out.ptr[p + 1] = out.ptr[p] + offcnt[out.rows[p]];
+    out.col.resize(out.ptr[T]);
+    out.val.resize(out.ptr[T]);
+    out.dinv.resize(T);
+    for (int p = 0; p < T; ++p) {
         const int r = out.rows[p];
         int64_t q = out.ptr[p];
         for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
             const int c = M.ci[e];
-            if (c == r || (lower ? (c > r) : (c < r))) continue;
+            if (c == r || (lower ? (c > r) : (c < r || c >= T))) continue;
             out.col[q] = c;
             out.val[q] = M.v[e];
             ++q;
@@ -270,18 +289,27 @@ void build_sched(const HostCsr& M, int n, bool lower, bool unit_diag, Sched& out
         }
         out.dinv[p] = 1.0 / dg;
     }
-    // group width per level
-    out.mode.assign(nlev + 1, 1);
-    for (int l = 0; l < nlev; ++l) {
-        const int a = out.lvl[l], b = out.lvl[l + 1];
-        const int64_t nz = out.ptr[b] - out.ptr[a];
-        const int rows = b - a;
-        const double avg = rows ? (double)nz / rows : 0.0;
-        int G = 1;
-        while (G < 32 && G < avg) G <<= 1;
-        if (rows * 32 <= S2L_BS_SOLVE / 2 && avg >= 128.0) G = S2L_MODE_CTA;
-        out.mode[l] = (int8_t)G;
+    (void)n;
+}
+
+// Tail split: the largest trailing block [T, n) of L whose strictly-lower part is at least
+// `density` full, with tail_min <= n - T <= tail_max (T = n: no dense tail).
+int choose_tail(const HostCsr& L, int n, int tail_min, int tail_max, double density)
+{
+    if (n < tail_min || tail_min <= 0) return n;
+    std::vector<int64_t> colcnt(n + 1, 0);
+    for (int r = 0; r < n; ++r)
+        for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e)
+            if (L.ci[e] < r) ++colcnt[L.ci[e]];
+    // suffix sums: entries (r, c) with c >= T lie inside the trailing block
+    std::vector<int64_t> suf(n + 1, 0);
+    for (int c = n - 1; c >= 0; --c) suf[c] = suf[c + 1] + colcnt[c];
+    for (int sz = std::min(tail_max, n); sz >= tail_min; --sz) {
+        const int T = n - sz;
+        const double full = 0.5 * (double)sz * (double)(sz - 1);
+        if ((double)suf[T] >= density * full) return T;
     }
+    return n;
 }
 
 // transpose of a lower CSR (values scaled by rowscale[c] of the result rows if given)
@@ -420,58 +448,75 @@ struct Prof {
 };
 
 // ------------------------------------------------------------------------------ solve-phase pieces
+template <typename Real>
+LocalSolveArgs<Real> solve_args(s2l_setup* s)
+{
+    LocalSolveArgs<Real> a{};
+    a.subs = s->d_subs;
+    for (int f = 0; f < 2; ++f)
+        a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const Real*)s->d_val[f], (const Real*)s->d_dinv[f]};
+    a.tr_sub = s->d_tr_sub;
+    a.tr_i = s->d_tr_i;
+    a.lts_ptr = s->d_lts_ptr;
+    a.lts_col = s->d_lts_col;
+    a.lts_val = (const Real*)s->d_lts_val;
+    a.us_sub = s->d_us_sub;
+    a.us_r = s->d_us_r;
+    a.ust_ptr = s->d_ust_ptr;
+    a.ust_col = s->d_ust_col;
+    a.ust_val = (const Real*)s->d_ust_val;
+    a.linv = (const Real*)s->d_linv;
+    a.uinv = (const Real*)s->d_uinv;
+    a.gout = s->d_gout;
+    a.ylocal = s->d_ylocal;
+    a.ybuf = (Real*)s->d_ybuf;
+    a.xbuf = (Real*)s->d_xbuf;
+    a.gflags = s->d_gflags;
+    a.err = s->d_err;
+    return a;
+}
+
+// Local solves of every subdomain (only_sub < 0) or of one: in -> (mode 0) out[owned] (+ base),
+// (mode 1) ylocal, (mode 2: local input/output of subdomain only_sub) out.
 int run_local_solve(s2l_setup* s, const double* in, const double* base, double* out, int mode, int only_sub,
                     const double* local_in)
 {
     Prof pr(s, PC_SOLVE);
     const int nb = only_sub >= 0 ? 1 : s->nsub;
     int32_t* sub_list = nullptr;
-    if (only_sub >= 0) sub_list = reinterpret_cast<int32_t*>(s->d_red + 500);  // scratch slot for one index
+    int tr0 = 0, trn = s->tr_first_h[s->nsub], us0 = 0, usn = s->us_first_h[s->nsub];
     if (only_sub >= 0) {
+        sub_list = reinterpret_cast<int32_t*>(s->d_red + 500);  // scratch slot for one index
         int32_t v = only_sub;
         CUDA_OK(s, cudaMemcpyAsync(sub_list, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+        tr0 = s->tr_first_h[only_sub];
+        trn = s->tr_first_h[only_sub + 1] - tr0;
+        us0 = s->us_first_h[only_sub];
+        usn = s->us_first_h[only_sub + 1] - us0;
     }
     cudaError_t e;
+    int launched = 0;
+    const size_t smem = s->d_gflags ? 0 : s->smem_bytes;
     if (s->real == S2L_REAL_F32) {
-        SolveArgs<float> a{};
-        a.subs = s->d_subs;
+        LocalSolveArgs<float> a = solve_args<float>(s);
         a.sub_list = sub_list;
-        for (int f = 0; f < 2; ++f)
-            a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const float*)s->d_val[f], (const float*)s->d_dinv[f]};
-        a.lvl_pos = s->d_lvl;
-        a.lvl_mode = s->d_mode;
-        a.gin = s->d_gin;
-        a.pin = s->d_pin;
-        a.gout = s->d_gout;
+        a.gather = mode == 2 ? s->d_pin : s->d_gin;
         a.in = mode == 2 ? local_in : in;
         a.base = base;
         a.out = out;
-        a.ylocal = s->d_ylocal;
-        a.xscratch = (float*)s->d_xscratch;
         a.mode = mode;
-        e = launch_local_solve<float>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
-        s->launches += 1;
+        e = launch_local_solve<float>(s->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
     } else {
-        SolveArgs<double> a{};
-        a.subs = s->d_subs;
+        LocalSolveArgs<double> a = solve_args<double>(s);
         a.sub_list = sub_list;
-        for (int f = 0; f < 2; ++f)
-            a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const double*)s->d_val[f],
-                      (const double*)s->d_dinv[f]};
-        a.lvl_pos = s->d_lvl;
-        a.lvl_mode = s->d_mode;
-        a.gin = s->d_gin;
-        a.pin = s->d_pin;
-        a.gout = s->d_gout;
+        a.gather = mode == 2 ? s->d_pin : s->d_gin;
         a.in = mode == 2 ? local_in : in;
         a.base = base;
         a.out = out;
-        a.ylocal = s->d_ylocal;
-        a.xscratch = (double*)s->d_xscratch;
         a.mode = mode;
-        e = launch_local_solve<double>(s->stream, a, nb, s->d_xscratch ? 0 : s->smem_bytes);
-        s->launches += 1;
+        e = launch_local_solve<double>(s->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
     }
+    s->launches += launched;
     if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
     return S2L_OK;
 }
@@ -551,7 +596,7 @@ int finish_out(s2l_setup* s, double* dst, const double* dev, int kind, int64_t c
         CUDA_OK(s, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
     CUDA_OK(s, cudaStreamSynchronize(s->stream));
     CUDA_OK(s, cudaGetLastError());
-    return S2L_OK;
+    return check_err(s);
 }
 
 int ensure_krylov(s2l_setup* s, int m, bool flexible)
@@ -579,8 +624,7 @@ int read_red(s2l_setup* s, int off, int count)
 {
     CUDA_OK(s, cudaMemcpyAsync(s->h_red + off, s->d_red + off, count * sizeof(double), cudaMemcpyDeviceToHost,
                                s->stream));
-    CUDA_OK(s, cudaStreamSynchronize(s->stream));
-    return S2L_OK;
+    return check_err(s);
 }
 
 int norm2_dev(s2l_setup* s, const double* x, double* out_host)
@@ -592,6 +636,77 @@ int norm2_dev(s2l_setup* s, const double* x, double* out_host)
     }
     RET_IF(read_red(s, 256, 1));
     *out_host = std::sqrt(s->h_red[256]);
+    return S2L_OK;
+}
+
+// Inverses of the dense tails: X = L_tt^-1 and Y = U_tt^-1, row-major, through cuBLAS DTRSM on
+// the identity.  A row-major triangle is the column-major transpose, so solving with the
+// transposed triangle leaves the row-major inverse in place.
+int invert_tails(s2l_setup* s, const std::vector<std::vector<double>>& Ltt, const std::vector<std::vector<double>>& Utt,
+                 const std::vector<int64_t>& d_off)
+{
+    int max_sz = 0;
+    for (size_t i = 0; i < Ltt.size(); ++i)
+        if (!Ltt[i].empty()) max_sz = std::max(max_sz, (int)std::lround(std::sqrt((double)Ltt[i].size())));
+    if (max_sz == 0) return S2L_OK;
+    double *dA = nullptr, *dB = nullptr;
+    const size_t mb = (size_t)max_sz * max_sz * sizeof(double);
+    if (cudaMalloc(&dA, mb) != cudaSuccess || cudaMalloc(&dB, mb) != cudaSuccess) {
+        cudaFree(dA);
+        return s->fail(S2L_ERR_OOM, "no device memory for the tail inversion");
+    }
+    cublasHandle_t hb = nullptr;
+    int rc = S2L_OK;
+    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) rc = s->fail(S2L_ERR_CUDA, "cublasCreate failed");
+    if (rc == S2L_OK) cublasSetStream(hb, s->stream);
+    std::vector<double> eye;
+    for (size_t i = 0; i < Ltt.size() && rc == S2L_OK; ++i) {
+        if (Ltt[i].empty()) continue;
+        const int sz = (int)std::lround(std::sqrt((double)Ltt[i].size()));
+        eye.assign((size_t)sz * sz, 0.0);
+        for (int k = 0; k < sz; ++k) eye[(size_t)k * sz + k] = 1.0;
+        const double one = 1.0;
+        for (int f = 0; f < 2 && rc == S2L_OK; ++f) {
+            const std::vector<double>& M = f == 0 ? Ltt[i] : Utt[i];
+            if (cudaMemcpyAsync(dA, M.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+                cudaMemcpyAsync(dB, eye.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+                rc = s->fail(S2L_ERR_CUDA, "tail upload failed");
+                break;
+            }
+            // row-major lower L = column-major upper L^T (and row-major upper U = column-major lower U^T)
+            const cublasFillMode_t fill = f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER;
+            if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, fill, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, sz, sz, &one, dA, sz, dB, sz) !=
+                CUBLAS_STATUS_SUCCESS) {
+                rc = s->fail(S2L_ERR_CUDA, "cublasDtrsm failed");
+                break;
+            }
+            void* dst = f == 0 ? s->d_linv : s->d_uinv;
+            if (s->real == S2L_REAL_F32) {
+                launch_to_float(s->stream, dB, (float*)dst + d_off[i], (int64_t)sz * sz);
+            } else if (cudaMemcpyAsync((double*)dst + d_off[i], dB, (size_t)sz * sz * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
+                rc = s->fail(S2L_ERR_CUDA, "tail copy failed");
+            }
+            // the host copies of M and eye are reused: finish before the next upload
+            if (cudaStreamSynchronize(s->stream) != cudaSuccess) rc = s->fail(S2L_ERR_CUDA, "tail inversion failed");
+        }
+    }
+    if (hb) cublasDestroy(hb);
+    cudaFree(dA);
+    cudaFree(dB);
+    return rc;
+}
+
+// error word of the sweeps: a bounded wait gave up
+int check_err(s2l_setup* s)
+{
+    int e = 0;
+    CUDA_OK(s, cudaMemcpyAsync(&e, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    if (e) {
+        CUDA_OK(s, cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+        return s->fail(S2L_ERR_TIMEOUT, "a sparse sweep gave up waiting for a row (bounded wait exceeded)");
+    }
     return S2L_OK;
 }
 
@@ -807,53 +922,138 @@ int s2l_gpu_setup_end(s2l_setup* s)
         s->tpr = avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32));
     }
 
-    // ---- per-subdomain schedules and index maps
+    // ---- per-subdomain factor split, schedules and index maps
     s->h_subs.resize(nsub);
-    int64_t loc = 0, ent[2] = {0, 0}, lvl_total = 0;
-    std::vector<Sched> sch[2];
-    sch[0].resize(nsub);
-    sch[1].resize(nsub);
+    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    int64_t loc = 0;
     std::vector<int32_t> gin, pin, gout, l2g;
     std::vector<double> Dall;
-    int max_nl = 0;
+    // concatenated sweep data (f = 0: L forward, 1: U backward)
+    std::vector<int32_t> sw_rows[2], sw_col[2];
+    std::vector<int64_t> sw_ptr[2];
+    std::vector<double> sw_val[2], sw_dinv[2];
+    // tail rows (L coupling) and sparse rows with U coupling
+    std::vector<int32_t> tr_sub, tr_i, lts_col, us_sub, us_r, ust_col;
+    std::vector<int64_t> lts_ptr(1, 0), ust_ptr(1, 0);
+    std::vector<double> lts_val, ust_val;
+    // dense tails (row-major), inverted on the device below
+    std::vector<std::vector<double>> Ltt(nsub), Utt(nsub);
+    std::vector<int64_t> d_off(nsub + 1, 0);
+    s->tr_first_h.assign(nsub + 1, 0);
+    s->us_first_h.assign(nsub + 1, 0);
+    double bytes = 0.0;
+    int max_T = 0, max_nl = 0;
+    int64_t sparse_nnz = 0;
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
         const int nl = h.n_local();
         max_nl = std::max(max_nl, nl);
-        std::string err;
-        const bool unit = h.kind != S2L_FACTOR_LLT;
-        build_sched(h.L, nl, true, unit, sch[0][i], err);
-        if (err.empty()) {
-            if (h.kind == S2L_FACTOR_LU) {
-                build_sched(h.U, nl, false, false, sch[1][i], err);
-            } else {
-                HostCsr U = transpose_lower(h.L, nl, nullptr);
-                if (h.kind == S2L_FACTOR_LDLT) {
-                    // U = diag(d) L^T: scale row r by d[r]; the unit diagonal of L becomes d[r]
-                    for (int r = 0; r < nl; ++r)
-                        for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) U.v[e] = (U.ci[e] == r) ? h.d[r] : U.v[e] * h.d[r];
-                    bool has_diag_missing = false;
-                    for (int r = 0; r < nl && !has_diag_missing; ++r) {
-                        bool f = false;
-                        for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) f = f || U.ci[e] == r;
-                        has_diag_missing = !f;
+        const bool unitL = h.kind != S2L_FACTOR_LLT;
+        HostCsr U;
+        if (h.kind == S2L_FACTOR_LU) {
+            U = std::move(h.U);
+        } else {
+            U = transpose_lower(h.L, nl, nullptr);
+            if (h.kind == S2L_FACTOR_LDLT) {
+                bool missing = false;
+                for (int r = 0; r < nl; ++r) {
+                    bool f = false;
+                    for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
+                        if (U.ci[e] == r) {
+                            U.v[e] = h.d[r];
+                            f = true;
+                        } else {
+                            U.v[e] *= h.d[r];
+                        }
                     }
-                    if (has_diag_missing) err = "LDLT: L must store its unit diagonal";
+                    missing = missing || !f;
                 }
-                if (err.empty()) build_sched(U, nl, false, false, sch[1][i], err);
+                if (missing) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
             }
         }
+        const int T = choose_tail(h.L, nl, s->opt_tail_min, s->opt_tail_max, s->opt_tail_density);
+        const int sz = nl - T;
+        max_T = std::max(max_T, T);
+        std::string err;
+        Sched sl, su;
+        build_sweep(h.L, nl, T, true, unitL, sl, err);
+        if (err.empty()) build_sweep(U, nl, T, false, false, su, err);
         if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
+        for (int f = 0; f < 2; ++f) {
+            const Sched& q = f == 0 ? sl : su;
+            const int64_t e0 = sw_col[f].size();
+            sw_rows[f].insert(sw_rows[f].end(), q.rows.begin(), q.rows.end());
+            for (int p = 0; p < T; ++p) sw_ptr[f].push_back(e0 + q.ptr[p]);
+            // slots [T, n) of the subdomain are unused by the sweeps: empty rows keep the layout flat
+            for (int p = T; p < nl; ++p) {
+                sw_ptr[f].push_back(e0 + q.ptr[T]);
+                sw_rows[f].push_back(p);
+            }
+            sw_col[f].insert(sw_col[f].end(), q.col.begin(), q.col.end());
+            sw_val[f].insert(sw_val[f].end(), q.val.begin(), q.val.end());
+            sw_dinv[f].insert(sw_dinv[f].end(), q.dinv.begin(), q.dinv.end());
+            sw_dinv[f].resize(sw_dinv[f].size() + sz, 1.0);
+            sparse_nnz += (int64_t)q.col.size();
+            bytes += (double)q.col.size() * (rs + 4) + (double)T * (4 + 8 + rs);
+        }
+        // L coupling of the tail rows and the dense lower tail
+        s->tr_first_h[i] = (int)tr_sub.size();
+        if (sz > 0) {
+            Ltt[i].assign((size_t)sz * sz, 0.0);
+            for (int k = T; k < nl; ++k) {
+                tr_sub.push_back(i);
+                tr_i.push_back(k - T);
+                for (int64_t e = h.L.rp[k]; e < h.L.rp[k + 1]; ++e) {
+                    const int c = h.L.ci[e];
+                    if (c < T) {
+                        lts_col.push_back(c);
+                        lts_val.push_back(h.L.v[e]);
+                    } else if (c < k) {
+                        Ltt[i][(size_t)(k - T) * sz + (c - T)] = h.L.v[e];
+                    } else if (c == k) {
+                        Ltt[i][(size_t)(k - T) * sz + (c - T)] = unitL ? 1.0 : h.L.v[e];
+                    }
+                }
+                if (unitL) Ltt[i][(size_t)(k - T) * sz + (k - T)] = 1.0;
+                lts_ptr.push_back((int64_t)lts_col.size());
+            }
+            Utt[i].assign((size_t)sz * sz, 0.0);
+            for (int k = T; k < nl; ++k)
+                for (int64_t e = U.rp[k]; e < U.rp[k + 1]; ++e) {
+                    const int c = U.ci[e];
+                    if (c >= k) Utt[i][(size_t)(k - T) * sz + (c - T)] = U.v[e];
+                }
+            for (int k = 0; k < sz; ++k)
+                if (Utt[i][(size_t)k * sz + k] == 0.0 || Ltt[i][(size_t)k * sz + k] == 0.0)
+                    return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": zero pivot in the dense tail");
+        }
+        // U coupling of the sparse rows
+        s->us_first_h[i] = (int)us_sub.size();
+        if (sz > 0)
+            for (int r = 0; r < T; ++r) {
+                bool any = false;
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e)
+                    if (U.ci[e] >= T) {
+                        ust_col.push_back(U.ci[e]);
+                        ust_val.push_back(U.v[e]);
+                        any = true;
+                    }
+                if (any) {
+                    us_sub.push_back(i);
+                    us_r.push_back(r);
+                    ust_ptr.push_back((int64_t)ust_col.size());
+                }
+            }
+        d_off[i + 1] = d_off[i] + (int64_t)sz * sz;
         DevSub d{};
         d.begin = h.begin;
         d.loc_off = loc;
         d.n_owned = h.n_owned;
         d.n_local = nl;
-        for (int f = 0; f < 2; ++f) {
-            d.lvl_off[f] = lvl_total;
-            d.nlev[f] = (int)sch[f][i].lvl.size() - 1;
-            lvl_total += sch[f][i].lvl.size();
-        }
+        d.T = T;
+        d.tr_first = s->tr_first_h[i];
+        d.us_first = s->us_first_h[i];
+        d.d_off = d_off[i];
         d.m = h.m;
         d.v_rows = boolean ? h.n_owned : nl;
         d.c_off = s->coarse != S2L_COARSE_NONE ? s->coff[i] : 0;
@@ -868,73 +1068,65 @@ int s2l_gpu_setup_end(s2l_setup* s)
             gout.push_back(h.pout[k]);
         }
         Dall.insert(Dall.end(), h.D.begin(), h.D.end());
+        // dense tails: the triangles of L^-1 and U^-1 are read once each
+        bytes += (double)sz * (sz + 1) * rs;
         loc += nl;
-        ent[0] += sch[0][i].col.size();
-        ent[1] += sch[1][i].col.size();
+        h.L = HostCsr();
     }
+    s->tr_first_h[nsub] = (int)tr_sub.size();
+    s->us_first_h[nsub] = (int)us_sub.size();
     s->nloc = loc;
-    // concatenate the schedules
-    double bytes = 0.0;
-    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    s->st_sparse_nnz = sparse_nnz;
+    s->st_coupling_nnz = (int64_t)lts_col.size() + (int64_t)ust_col.size();
+    s->st_dense_entries = d_off[nsub];
+    s->st_tail_rows = (int64_t)tr_sub.size();
+    bytes += (double)s->st_coupling_nnz * (rs + 4) + (double)(tr_sub.size() + us_sub.size()) * (8 + 8 + rs);
     for (int f = 0; f < 2; ++f) {
-        std::vector<int32_t> rows, col;
-        std::vector<int64_t> ptr;
-        std::vector<double> val, dinv;
-        rows.reserve(loc);
-        ptr.reserve(loc + 1);
-        col.reserve(ent[f]);
-        val.reserve(ent[f]);
-        dinv.reserve(loc);
-        int64_t e0 = 0;
-        for (int i = 0; i < nsub; ++i) {
-            const Sched& q = sch[f][i];
-            rows.insert(rows.end(), q.rows.begin(), q.rows.end());
-            for (size_t p = 0; p + 1 < q.ptr.size(); ++p) ptr.push_back(e0 + q.ptr[p]);
-            col.insert(col.end(), q.col.begin(), q.col.end());
-            val.insert(val.end(), q.val.begin(), q.val.end());
-            dinv.insert(dinv.end(), q.dinv.begin(), q.dinv.end());
-            e0 += q.col.size();
-            bytes += (double)q.col.size() * (rs + 4) + (double)q.rows.size() * (4 + 8 + rs);
-        }
-        ptr.push_back(e0);
-        RET_IF(upload(s, &s->d_rows[f], rows));
-        RET_IF(upload(s, &s->d_ptr[f], ptr));
-        RET_IF(upload(s, &s->d_col[f], col));
+        sw_ptr[f].push_back((int64_t)sw_col[f].size());
+        RET_IF(upload(s, &s->d_rows[f], sw_rows[f]));
+        RET_IF(upload(s, &s->d_ptr[f], sw_ptr[f]));
+        RET_IF(upload(s, &s->d_col[f], sw_col[f]));
         if (s->real == S2L_REAL_F32) {
-            RET_IF(upload_real<float>(s, &s->d_val[f], val));
-            RET_IF(upload_real<float>(s, &s->d_dinv[f], dinv));
+            RET_IF(upload_real<float>(s, &s->d_val[f], sw_val[f]));
+            RET_IF(upload_real<float>(s, &s->d_dinv[f], sw_dinv[f]));
         } else {
-            RET_IF(upload_real<double>(s, &s->d_val[f], val));
-            RET_IF(upload_real<double>(s, &s->d_dinv[f], dinv));
+            RET_IF(upload_real<double>(s, &s->d_val[f], sw_val[f]));
+            RET_IF(upload_real<double>(s, &s->d_dinv[f], sw_dinv[f]));
         }
+        sw_rows[f] = {};
+        sw_col[f] = {};
+        sw_val[f] = {};
     }
-    {
-        std::vector<int32_t> lvl;
-        std::vector<int8_t> mode;
-        lvl.reserve(lvl_total);
-        mode.reserve(lvl_total);
-        for (int i = 0; i < nsub; ++i)
-            for (int f = 0; f < 2; ++f) {
-                // lvl_off[f] of subdomain i was assigned in (i, f) order
-                lvl.insert(lvl.end(), sch[f][i].lvl.begin(), sch[f][i].lvl.end());
-                mode.insert(mode.end(), sch[f][i].mode.begin(), sch[f][i].mode.end());
-            }
-        // re-assign offsets in the (i, f) order used just above
-        int64_t off = 0;
-        for (int i = 0; i < nsub; ++i)
-            for (int f = 0; f < 2; ++f) {
-                s->h_subs[i].lvl_off[f] = off;
-                off += sch[f][i].lvl.size();
-            }
-        RET_IF(upload(s, &s->d_lvl, lvl));
-        RET_IF(upload(s, &s->d_mode, mode));
+    RET_IF(upload(s, &s->d_tr_sub, tr_sub));
+    RET_IF(upload(s, &s->d_tr_i, tr_i));
+    RET_IF(upload(s, &s->d_lts_ptr, lts_ptr));
+    RET_IF(upload(s, &s->d_lts_col, lts_col));
+    RET_IF(upload(s, &s->d_us_sub, us_sub));
+    RET_IF(upload(s, &s->d_us_r, us_r));
+    RET_IF(upload(s, &s->d_ust_ptr, ust_ptr));
+    RET_IF(upload(s, &s->d_ust_col, ust_col));
+    if (s->real == S2L_REAL_F32) {
+        RET_IF(upload_real<float>(s, &s->d_lts_val, lts_val));
+        RET_IF(upload_real<float>(s, &s->d_ust_val, ust_val));
+    } else {
+        RET_IF(upload_real<double>(s, &s->d_lts_val, lts_val));
+        RET_IF(upload_real<double>(s, &s->d_ust_val, ust_val));
     }
-    // gather, output and owned traffic of one launch
+    // ---- dense tail inverses on the device (FP64 triangular solves with the identity)
+    RET_IF(dev_alloc(s, &s->d_linv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
+    RET_IF(dev_alloc(s, &s->d_uinv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
+    RET_IF(invert_tails(s, Ltt, Utt, d_off));
+    // input gather and owned output of one local solve
     for (int i = 0; i < nsub; ++i) {
         const HostSub& h = s->hs[i];
         bytes += (double)h.n_local() * (4 + 8) + (double)h.n_owned * (4 + 8 + 8);
     }
     s->solve_bytes = bytes;
+    {
+        // sweep group width from the mean row length of the sparse parts
+        const double avg = loc ? (double)sparse_nnz / (2.0 * (double)loc) : 0.0;
+        s->sweep_group = s->opt_group ? s->opt_group : (avg <= 6.0 ? 8 : (avg <= 14.0 ? 16 : 32));
+    }
     RET_IF(upload(s, &s->d_gin, gin));
     RET_IF(upload(s, &s->d_pin, pin));
     RET_IF(upload(s, &s->d_gout, gout));
@@ -1030,13 +1222,18 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(alloc_doubles(s, &s->d_part, (size_t)S2L_NB_RED * S2L_MAX_RED_COLS));
     RET_IF(alloc_doubles(s, &s->d_red, 512));
     CUDA_OK(s, cudaMallocHost(&s->h_red, 512 * sizeof(double)));
-    const size_t smem = (size_t)max_nl * rs;
-    const size_t smem_cap = 227 * 1024 - 1024;
+    RET_IF(dev_alloc(s, &s->d_ybuf, (size_t)std::max<int64_t>(loc, 1) * rs));
+    RET_IF(dev_alloc(s, &s->d_xbuf, (size_t)std::max<int64_t>(loc, 1) * rs));
+    RET_IF(dev_alloc(s, reinterpret_cast<void**>(&s->d_err), 16));
+    CUDA_OK(s, cudaMemsetAsync(s->d_err, 0, 16, s->stream));
+    // sweep shared memory: x (T values) + one ready byte per row
+    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15);
+    const size_t smem_cap = 227 * 1024 - 64;
     if (smem <= smem_cap) {
         s->smem_bytes = smem;
     } else {
         s->smem_bytes = 0;
-        RET_IF(dev_alloc(s, &s->d_xscratch, (size_t)loc * rs));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&s->d_gflags), (size_t)std::max<int64_t>(loc, 1)));
     }
     CUDA_OK(s, cudaStreamSynchronize(s->stream));
     // host staging no longer needed
@@ -1073,6 +1270,36 @@ int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
 {
     if (!s || !bytes) return S2L_ERR_BADARG;
     *bytes = s->bytes;
+    return S2L_OK;
+}
+
+int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
+{
+    if (!s || !name) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "setup_option after setup_end");
+    const std::string n(name);
+    if (n == "tail_min") s->opt_tail_min = (int)value;
+    else if (n == "tail_max") s->opt_tail_max = (int)value;
+    else if (n == "tail_density") s->opt_tail_density = value;
+    else if (n == "sweep_group") {
+        const int g = (int)value;
+        if (g != 0 && g != 8 && g != 16 && g != 32) return s->fail(S2L_ERR_BADARG, "sweep_group must be 0, 8, 16 or 32");
+        s->opt_group = g;
+    } else return s->fail(S2L_ERR_BADARG, "unknown setup option " + n);
+    return S2L_OK;
+}
+
+int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
+{
+    if (!s || !name || !value) return S2L_ERR_BADARG;
+    const std::string n(name);
+    if (n == "sparse_nnz") *value = (double)s->st_sparse_nnz;
+    else if (n == "coupling_nnz") *value = (double)s->st_coupling_nnz;
+    else if (n == "dense_entries") *value = (double)s->st_dense_entries;
+    else if (n == "tail_rows") *value = (double)s->st_tail_rows;
+    else if (n == "sweep_group") *value = (double)s->sweep_group;
+    else if (n == "smem_bytes") *value = (double)s->smem_bytes;
+    else return S2L_ERR_BADARG;
     return S2L_OK;
 }
 
@@ -1274,7 +1501,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
                 s->launches += 7;
             }
             CUDA_OK(s, cudaMemcpyAsync(s->h_red, s->d_red, 257 * sizeof(double), cudaMemcpyDeviceToHost, st));
-            CUDA_OK(s, cudaStreamSynchronize(st));
+            RET_IF(check_err(s));
             const double hn = std::sqrt(s->h_red[256]);
             for (int i = 0; i <= j; ++i) Hc(i, j) = s->h_red[i] + s->h_red[128 + i];
             Hc(j + 1, j) = hn;
@@ -1436,7 +1663,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             alpha = rho / rhv;
             {
                 Prof pr(s, PC_VEC);
-                launch_bicg_s(st, n, r, v, alpha, sv, nullptr, s->d_part, s->d_red + 256);
+                launch_bicg_s(st, n, r, v, alpha, sv, s->d_part, s->d_red + 256);
                 s->launches += 2;
             }
             RET_IF(read_red(s, 256, 1));

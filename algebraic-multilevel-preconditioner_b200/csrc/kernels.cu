@@ -174,15 +174,6 @@ __global__ void axpby_kernel(int64_t n, double a, const double* __restrict__ x, 
         y[i] = (b == 0.0) ? a * x[i] : a * x[i] + b * y[i];
 }
 
-// y = x / s_dev[0]
-__global__ void scale_copy_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ s,
-                                  double* __restrict__ y)
-{
-    const double inv = 1.0 / s[0];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        y[i] = x[i] * inv;
-}
-
 // partials of x.y and (z != nullptr) x.z
 __global__ void __launch_bounds__(256) dot2_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
                                                    const double* __restrict__ z, double* __restrict__ partials)
@@ -250,95 +241,233 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 }
 
 // ------------------------------------------------------------------------------ local solves (K2, K3)
-template <typename Real>
-__device__ __forceinline__ Real group_sum(Real s, int G)
+// Sparse sweep of one factor, one CTA per subdomain, x in shared memory (or, when it does not
+// fit, in the local-space buffer with global ready flags).
+//
+// Rows are taken in solve order (a topological order: every dependency of slot p sits in a slot
+// < p).  Group g (G lanes) owns slots g, g + NG, g + 2 NG, ...; it waits, entry by entry, until
+// the ready flag of each column it reads is set, then writes its row and sets the row's flag.  A
+// group only ever waits for slots owned by groups that are at most one slot behind it, so the
+// sweep cannot deadlock.  Every wait is bounded: after S2L_SPIN_LIMIT polls the CTA raises *err
+// and all groups leave.  While a group works on one row its next S2L_PREFETCH rows are already in
+// flight (row id, entry range, 1/diag and the first G entries), so the latency of the factor
+// stream overlaps the dependency chain instead of adding to it.
+template <typename Real, int G>
+__device__ __forceinline__ Real group_reduce(Real v)
 {
-    for (int o = G >> 1; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
-    return s;
-}
-
-// One triangular solve, level by level, in place on x (shared or global memory).
-// Levels of width G: groups of G threads per row, shuffle-reduced.  S2L_MODE_CTA levels: the whole
-// CTA reduces each row.  Every level ends with a CTA barrier.
-template <typename Real>
-__device__ __forceinline__ void solve_pass(Real* __restrict__ x, const DevFactor<Real>& F, int64_t slot0,
-                                           const int32_t* __restrict__ lvl, const int8_t* __restrict__ mode, int nlev,
-                                           double* red)
-{
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int lv = 0; lv < nlev; ++lv) {
-        const int a = lvl[lv], b = lvl[lv + 1];
-        const int G = mode[lv];
-        if (G > 0) {
-            const int ng = S2L_BS_SOLVE / G;
-            const int gid = tid / G, gl = tid - gid * G;
-            for (int p0 = a; p0 < b; p0 += ng) {
-                const int p = p0 + gid;
-                Real s = Real(0);
-                const bool act = p < b;
-                int r = 0;
-                if (act) {
-                    const int64_t slot = slot0 + p;
-                    r = F.rows[slot];
-                    const int64_t e1 = F.ptr[slot + 1];
-                    for (int64_t e = F.ptr[slot] + gl; e < e1; e += G) s += F.val[e] * x[F.col[e]];
-                }
-                s = group_sum(s, G);
-                if (act && gl == 0) x[r] = (x[r] - s) * F.dinv[slot0 + p];
-            }
-        } else {
-            for (int p = a; p < b; ++p) {
-                const int64_t slot = slot0 + p;
-                const int r = F.rows[slot];
-                Real s = Real(0);
-                const int64_t e1 = F.ptr[slot + 1];
-                for (int64_t e = F.ptr[slot] + tid; e < e1; e += S2L_BS_SOLVE) s += F.val[e] * x[F.col[e]];
-                s = warp_sum(s);
-                if (lane == 0) red[warp] = (double)s;
-                __syncthreads();
-                if (warp == 0) {
-                    Real t = (lane < S2L_BS_SOLVE / 32) ? (Real)red[lane] : Real(0);
-                    t = warp_sum(t);
-                    if (lane == 0) x[r] = (x[r] - t) * F.dinv[slot];
-                }
-                __syncthreads();
-            }
-        }
-        __syncthreads();
+#pragma unroll
+    for (int o = G >> 1; o; o >>= 1) {
+        const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+        v += __shfl_down_sync(mask, v, o, G);
     }
+    return v;
 }
 
-// One CTA per subdomain: gather the rhs (permuted), forward solve with L, backward solve with U,
-// then the epilogue: direct owned write (boolean RAS, + base), local-space write, or local output.
-template <typename Real, bool SMEM>
-__global__ void __launch_bounds__(S2L_BS_SOLVE) local_solve_kernel(const SolveArgs<Real> a)
+template <typename Real, int G, bool SMEM, bool FWD>
+__global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red[S2L_BS_SOLVE / 32];
+    __shared__ int abort_word;
+    volatile int& abort_flag = abort_word;
     const int sid = a.sub_list ? a.sub_list[blockIdx.x] : (int)blockIdx.x;
     const DevSub sd = a.subs[sid];
     const int64_t lo = sd.loc_off;
-    const int n = sd.n_local;
-    Real* x = SMEM ? reinterpret_cast<Real*>(smem_raw) : a.xscratch + lo;
-    if (a.mode == 2) {
-        for (int k = threadIdx.x; k < n; k += S2L_BS_SOLVE) x[k] = (Real)a.in[a.pin[lo + k]];
+    const int T = sd.T;
+    const SweepFactor<Real> F = a.f[FWD ? 0 : 1];
+    Real* xs = SMEM ? reinterpret_cast<Real*>(smem_raw) : a.ybuf + lo;
+    volatile Real* x = xs;
+    volatile uint8_t* flag;
+    if (SMEM) {
+        const size_t off = (((size_t)T * sizeof(Real)) + 15) & ~(size_t)15;
+        flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off);
     } else {
-        for (int k = threadIdx.x; k < n; k += S2L_BS_SOLVE) x[k] = (Real)a.in[a.gin[lo + k]];
+        flag = a.gflags + lo;
+    }
+    if (threadIdx.x == 0) abort_flag = 0;
+    for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) {
+        if (FWD)
+            xs[k] = (Real)a.in[a.gather[lo + k]];
+        else if (SMEM)
+            xs[k] = a.ybuf[lo + k];
+        flag[k] = 0;
     }
     __syncthreads();
-    solve_pass<Real>(x, a.f[0], lo, a.lvl_pos + sd.lvl_off[0], a.lvl_mode + sd.lvl_off[0], sd.nlev[0], red);
-    solve_pass<Real>(x, a.f[1], lo, a.lvl_pos + sd.lvl_off[1], a.lvl_mode + sd.lvl_off[1], sd.nlev[1], red);
+    constexpr int NG = S2L_BS_SWEEP / G;
+    constexpr int D = S2L_PREFETCH;
+    const int g = threadIdx.x / G, l = threadIdx.x % G;
+    int pr_row[D];
+    int64_t pr_e0[D], pr_e1[D];
+    Real pr_dinv[D], pr_val[D];
+    int pr_col[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const int p = g + d * NG;
+        pr_e0[d] = pr_e1[d] = 0;
+        pr_row[d] = 0;
+        pr_dinv[d] = Real(1);
+        pr_col[d] = 0;
+        pr_val[d] = Real(0);
+        if (p < T) {
+            const int64_t slot = lo + p;
+            pr_row[d] = F.rows[slot];
+            pr_e0[d] = F.ptr[slot];
+            pr_e1[d] = F.ptr[slot + 1];
+            pr_dinv[d] = F.dinv[slot];
+            if (pr_e0[d] + l < pr_e1[d]) {
+                pr_col[d] = F.col[pr_e0[d] + l];
+                pr_val[d] = F.val[pr_e0[d] + l];
+            }
+        }
+    }
+    bool dead = false;
+    for (int p0 = g; p0 < T && !dead; p0 += D * NG) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const int p = p0 + d * NG;
+            if (p < T && !dead) {
+                Real acc = Real(0);
+                int64_t e = pr_e0[d] + l;
+                const int64_t e1 = pr_e1[d];
+                if (e < e1) {
+                    const int c = pr_col[d];
+                    int spin = 0;
+                    while (flag[c] == 0) {
+                        if (abort_flag) { dead = true; break; }
+                        if (++spin > S2L_SPIN_LIMIT) {
+                            abort_flag = 1;
+                            atomicExch(a.err, 1);
+                            dead = true;
+                            break;
+                        }
+                    }
+                    acc += pr_val[d] * x[c];
+                }
+                for (e += G; e < e1 && !dead; e += G) {
+                    const int c = F.col[e];
+                    const Real v = F.val[e];
+                    int spin = 0;
+                    while (flag[c] == 0) {
+                        if (abort_flag) { dead = true; break; }
+                        if (++spin > S2L_SPIN_LIMIT) {
+                            abort_flag = 1;
+                            atomicExch(a.err, 1);
+                            dead = true;
+                            break;
+                        }
+                    }
+                    acc += v * x[c];
+                }
+                {
+                    const unsigned gmask =
+                        (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+                    dead = __any_sync(gmask, dead);  // one decision per group before its shuffles
+                }
+                acc = group_reduce<Real, G>(acc);
+                if (l == 0 && !dead) {
+                    const int r = pr_row[d];
+                    x[r] = (x[r] - acc) * pr_dinv[d];
+                    __threadfence_block();
+                    flag[r] = 1;
+                }
+                // refill this prefetch slot with the group's slot D rows ahead
+                const int q = p + D * NG;
+                if (q < T) {
+                    const int64_t slot = lo + q;
+                    pr_row[d] = F.rows[slot];
+                    pr_e0[d] = F.ptr[slot];
+                    pr_e1[d] = F.ptr[slot + 1];
+                    pr_dinv[d] = F.dinv[slot];
+                    if (pr_e0[d] + l < pr_e1[d]) {
+                        pr_col[d] = F.col[pr_e0[d] + l];
+                        pr_val[d] = F.val[pr_e0[d] + l];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (FWD) {
+        if (SMEM)
+            for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) a.ybuf[lo + k] = xs[k];
+        return;
+    }
+    // epilogue of the backward sweep: x_local[j] = x[perm_out[j]] (tail values from the buffer)
+    const int n = sd.n_local;
+    auto val_at = [&](int q) -> double { return q < T ? (double)xs[q] : (double)a.ybuf[lo + q]; };
     if (a.mode == 0) {
-        for (int j = threadIdx.x; j < sd.n_owned; j += S2L_BS_SOLVE) {
-            double v = (double)x[a.gout[lo + j]];
+        for (int j = threadIdx.x; j < sd.n_owned; j += S2L_BS_SWEEP) {
+            double v = val_at(a.gout[lo + j]);
             if (a.base) v += a.base[sd.begin + j];
             a.out[sd.begin + j] = v;
         }
     } else if (a.mode == 1) {
-        for (int j = threadIdx.x; j < n; j += S2L_BS_SOLVE) a.ylocal[lo + j] = (double)x[a.gout[lo + j]];
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) a.ylocal[lo + j] = val_at(a.gout[lo + j]);
     } else {
-        for (int j = threadIdx.x; j < n; j += S2L_BS_SOLVE) a.out[j] = (double)x[a.gout[lo + j]];
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) a.out[j] = val_at(a.gout[lo + j]);
     }
+}
+
+// Tail right-hand side: t(T+i) = b(T+i) - L(T+i, 0:T) y(0:T), one warp per tail row.
+template <typename Real>
+__global__ void __launch_bounds__(256) tail_rhs_kernel(const LocalSolveArgs<Real> a, int q0, int count)
+{
+    const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= q0 + count) return;
+    const DevSub sd = a.subs[a.tr_sub[q]];
+    const int64_t lo = sd.loc_off;
+    const int k = sd.T + a.tr_i[q];
+    Real acc = Real(0);
+    for (int64_t e = a.lts_ptr[q] + lane; e < a.lts_ptr[q + 1]; e += 32) acc += a.lts_val[e] * a.ybuf[lo + a.lts_col[e]];
+    acc = warp_sum(acc);
+    if (lane == 0) a.ybuf[lo + k] = (Real)a.in[a.gather[lo + k]] - acc;
+}
+
+// Dense tail: out(T+i) = sum_j Minv(i, j) in(T+j), j <= i (lower) or j >= i (upper); warp per row.
+template <typename Real, bool LOWER>
+__global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Real> a, const Real* __restrict__ Minv,
+                                                        const Real* __restrict__ vin, Real* __restrict__ vout,
+                                                        int q0, int count)
+{
+    const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= q0 + count) return;
+    const DevSub sd = a.subs[a.tr_sub[q]];
+    const int s = sd.n_local - sd.T;
+    const int i = a.tr_i[q];
+    const int64_t base = sd.loc_off + sd.T;
+    const Real* row = Minv + sd.d_off + (int64_t)i * s;
+    const int j0 = LOWER ? 0 : i, j1 = LOWER ? i + 1 : s;
+    Real acc0 = Real(0), acc1 = Real(0);
+    int j = j0 + lane;
+    for (; j + 32 < j1; j += 64) {
+        acc0 += row[j] * vin[base + j];
+        acc1 += row[j + 32] * vin[base + j + 32];
+    }
+    if (j < j1) acc0 += row[j] * vin[base + j];
+    const Real acc = warp_sum(acc0 + acc1);
+    if (lane == 0) vout[base + i] = acc;
+}
+
+// Backward coupling: y(r) -= U(r, T:n) x(T:n) for the sparse rows that have tail columns.
+template <typename Real>
+__global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveArgs<Real> a, int q0, int count)
+{
+    const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= q0 + count) return;
+    const DevSub sd = a.subs[a.us_sub[q]];
+    const int64_t lo = sd.loc_off;
+    Real acc = Real(0);
+    for (int64_t e = a.ust_ptr[q] + lane; e < a.ust_ptr[q + 1]; e += 32) acc += a.ust_val[e] * a.ybuf[lo + a.ust_col[e]];
+    acc = warp_sum(acc);
+    if (lane == 0) a.ybuf[lo + a.us_r[q]] -= acc;
+}
+
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
 }
 
 // out[g] = base[g] + sum over the copies c of g of w_c * ylocal[pos_c] (w = 1 when cp_w is null)
@@ -491,11 +620,6 @@ void launch_axpby(cudaStream_t st, int64_t n, double a, const double* x, double 
     axpby_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, a, x, b, y);
 }
 
-void launch_scale_copy(cudaStream_t st, int64_t n, const double* x, const double* s_dev, double* y)
-{
-    scale_copy_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, x, s_dev, y);
-}
-
 void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, const double* z, double* partials,
                  double* out)
 {
@@ -510,7 +634,7 @@ void launch_bicg_p(cudaStream_t st, int64_t n, const double* r, const double* v,
 }
 
 void launch_bicg_s(cudaStream_t st, int64_t n, const double* r, const double* v, double alpha, double* s,
-                   const double* /*rh*/, double* partials, double* out)
+                   double* partials, double* out)
 {
     bicg_s_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, r, v, alpha, s, partials);
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 1, out);
@@ -524,22 +648,60 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
 }
 
-template <typename Real>
-cudaError_t launch_local_solve(cudaStream_t st, const SolveArgs<Real>& a, int nblocks, size_t smem_bytes)
+template <typename Real, int G>
+cudaError_t launch_sweeps_g(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
+                            int tr_count, int us_first, int us_count, int* launches)
 {
-    if (smem_bytes > 0) {
-        cudaError_t e = cudaFuncSetAttribute(local_solve_kernel<Real, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    cudaError_t e;
+    if (smem > 0) {
+        e = cudaFuncSetAttribute(sweep_kernel<Real, G, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        local_solve_kernel<Real, true><<<nblocks, S2L_BS_SOLVE, smem_bytes, st>>>(a);
+        e = cudaFuncSetAttribute(sweep_kernel<Real, G, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        sweep_kernel<Real, G, true, true><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
     } else {
-        local_solve_kernel<Real, false><<<nblocks, S2L_BS_SOLVE, 0, st>>>(a);
+        sweep_kernel<Real, G, false, true><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
     }
+    int nl = 1;
+    if (tr_count > 0) {
+        const int grid = (tr_count + 7) / 8;
+        tail_rhs_kernel<Real><<<grid, 256, 0, st>>>(a, tr_first, tr_count);
+        tail_gemv_kernel<Real, true><<<grid, 256, 0, st>>>(a, a.linv, a.ybuf, a.xbuf, tr_first, tr_count);
+        tail_gemv_kernel<Real, false><<<grid, 256, 0, st>>>(a, a.uinv, a.xbuf, a.ybuf, tr_first, tr_count);
+        nl += 3;
+    }
+    if (us_count > 0) {
+        sparse_coupling_kernel<Real><<<(us_count + 7) / 8, 256, 0, st>>>(a, us_first, us_count);
+        nl += 1;
+    }
+    if (smem > 0)
+        sweep_kernel<Real, G, true, false><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
+    else
+        sweep_kernel<Real, G, false, false><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
+    *launches = nl + 1;
     return cudaGetLastError();
 }
 
-template cudaError_t launch_local_solve<double>(cudaStream_t, const SolveArgs<double>&, int, size_t);
-template cudaError_t launch_local_solve<float>(cudaStream_t, const SolveArgs<float>&, int, size_t);
+template <typename Real>
+cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem_bytes,
+                               int group, int tr_first, int tr_count, int us_first, int us_count, int* launches)
+{
+    switch (group) {
+    case 8: return launch_sweeps_g<Real, 8>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
+    case 16: return launch_sweeps_g<Real, 16>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
+    default: return launch_sweeps_g<Real, 32>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
+    }
+}
+
+template cudaError_t launch_local_solve<double>(cudaStream_t, const LocalSolveArgs<double>&, int, size_t, int, int, int,
+                                                int, int, int*);
+template cudaError_t launch_local_solve<float>(cudaStream_t, const LocalSolveArgs<float>&, int, size_t, int, int, int,
+                                               int, int, int*);
+
+void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n)
+{
+    to_float_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(in, out, n);
+}
 
 void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int32_t* cp_pos, const double* cp_w,
                     const double* ylocal, const double* base, double* out)

@@ -2,10 +2,14 @@
 //
 // Everything of one matrix lives in HBM for the whole solve phase:
 //  * the renumbered global CSR (int32 indices, FP64 values);
-//  * the "local space": the concatenation of every subdomain's local vector
-//    [owned | ghosts], subdomain i at [loc_off_i, loc_off_i + n_i);
-//  * per subdomain, the two triangular factors stored row-wise IN SOLVE ORDER (level by level),
-//    diagonal split off as its inverse, columns in the factor's permuted numbering;
+//  * the "local space": the concatenation of every subdomain's local vector, subdomain i at
+//    [loc_off_i, loc_off_i + n_i), in the factor's permuted numbering;
+//  * per subdomain, each triangular factor split at a tail index T_i:
+//      sparse part  rows [0, T) : stored row-wise IN SOLVE ORDER (a topological order of the rows),
+//                                 off-diagonal entries only, inverse diagonal apart;
+//      coupling     L(T:n, 0:T) rows of the tail / U(0:T, T:n) rows of the sparse part: CSR;
+//      dense tail   the inverse of the trailing triangle L(T:n, T:n) / U(T:n, T:n), row-major s x s
+//                   (s = n - T), computed once at setup, so the tail solve is a dense GEMV;
 //  * the coarse basis row-major (n_rows_i x m_i), the dense inverse of E (n0 x n0, row-major);
 //  * a "copies" CSR mapping each global row to its copies in the local space (used when the
 //    one-level result or the prolongation must be summed over subdomains).
@@ -14,21 +18,24 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define S2L_BS_SOLVE 512      // threads of the local-solve CTA (one CTA per subdomain)
+#define S2L_BS_SWEEP 1024     // threads of a sparse-sweep CTA (one CTA per subdomain)
 #define S2L_BS_VEC 256        // threads of the vector / SpMV kernels
 #define S2L_NB_RED 592        // blocks of every kernel that produces reduction partials (4 x 148 SMs)
 #define S2L_MAX_RED_COLS 128  // columns of the reduction buffer
 #define S2L_TILE_ROWS 256     // rows of one coarse restrict/prolong tile
-#define S2L_MODE_CTA 0        // level mode: the whole CTA works on each row of the level
+#define S2L_PREFETCH 4        // rows prefetched per group in a sparse sweep
+#define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {
     int64_t begin;      // first owned global row
     int64_t loc_off;    // offset of the subdomain in the local space
     int n_owned;
     int n_local;
-    // forward (L) and backward (U) schedules
-    int64_t lvl_off[2];  // offset into lvl_pos / lvl_mode (nlev+1 entries of lvl_pos per factor)
-    int nlev[2];
+    int T;              // rows [0, T) sparse, [T, n_local) dense tail
+    int tr_first;       // first entry of the subdomain in the tail-row list
+    int us_first;       // first entry of the subdomain in the sparse-row coupling list
+    int pad;
+    int64_t d_off;      // offset of the subdomain's s x s inverse tails
     // coarse basis
     int m;
     int v_rows;         // rows stored: n_owned (boolean PoU) or n_local
@@ -36,11 +43,10 @@ struct DevSub {
     int64_t c_off;      // coarse offset of the subdomain (first coarse unknown)
 };
 
-// One triangular factor of every subdomain, in solve order.  Row slot p of subdomain i is
-// global slot loc_off_i + p; its row id (permuted numbering) is rows[slot], entries
-// ptr[slot]..ptr[slot+1] (off-diagonal only), inverse diagonal dinv[slot].
+// Sparse part of one factor of every subdomain, in solve order: slot p (p < T_i) of subdomain i
+// is global slot loc_off_i + p; its row id rows[slot], entries ptr[slot]..ptr[slot+1], 1/diag dinv[slot].
 template <typename Real>
-struct DevFactor {
+struct SweepFactor {
     const int32_t* rows;
     const int64_t* ptr;
     const int32_t* col;
@@ -49,20 +55,34 @@ struct DevFactor {
 };
 
 template <typename Real>
-struct SolveArgs {
+struct LocalSolveArgs {
     const DevSub* subs;
-    const int32_t* sub_list;   // CTA b solves subdomain sub_list[b] (nullptr: b itself)
-    DevFactor<Real> f[2];      // 0 = L (forward), 1 = U (backward)
-    const int32_t* lvl_pos;    // level boundaries (slot offsets relative to the subdomain)
-    const int8_t* lvl_mode;    // group width of each level (1..32) or S2L_MODE_CTA
-    const int32_t* gin;        // gather index of slot k: global row of local perm_in[k]
-    const int32_t* pin;        // perm_in itself (local-input mode)
+    const int32_t* sub_list;   // CTA b of a sweep works on subdomain sub_list[b] (nullptr: b)
+    SweepFactor<Real> f[2];    // 0 = L (forward), 1 = U (backward)
+    // tail rows of every subdomain: (sub, i) pairs, L(T+i, 0:T) coupling CSR
+    const int32_t* tr_sub;
+    const int32_t* tr_i;
+    const int64_t* lts_ptr;
+    const int32_t* lts_col;
+    const Real* lts_val;
+    // sparse rows with U(r, T:n) coupling: (sub, r) pairs and CSR
+    const int32_t* us_sub;
+    const int32_t* us_r;
+    const int64_t* ust_ptr;
+    const int32_t* ust_col;
+    const Real* ust_val;
+    const Real* linv;          // inverse tails, row-major per subdomain
+    const Real* uinv;
+    const int32_t* gather;     // slot k -> index into `in` (global gather, or perm_in for a local input)
     const int32_t* gout;       // perm_out: local j -> slot
-    const double* in;          // input vector (global, or local in local-input mode)
+    const double* in;
     const double* base;        // added to the owned output (x0 of the coarse correction), may be null
-    double* out;               // global output (direct mode) or local output
-    double* ylocal;            // local space output (sum mode)
-    Real* xscratch;            // local space scratch when the vector does not fit shared memory
+    double* out;               // global output (direct mode) or local output (mode 2)
+    double* ylocal;            // local-space output (mode 1)
+    Real* ybuf;                // local-space work vectors
+    Real* xbuf;
+    uint8_t* gflags;           // ready flags when a sweep does not fit shared memory
+    int* err;                  // device error word (1: a sweep wait gave up)
     int mode;                  // 0 direct owned write, 1 local-space write, 2 local input/output
 };
 
@@ -78,19 +98,22 @@ void launch_gemv_update(cudaStream_t st, int64_t n, const double* V, int64_t ldv
                         double* w, double* partials);
 void launch_gemv(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* y, double* u);
 void launch_axpby(cudaStream_t st, int64_t n, double a, const double* x, double b, double* y);
-void launch_scale_copy(cudaStream_t st, int64_t n, const double* x, const double* s_dev, double* y);
 void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, const double* z, double* partials,
                  double* out);
 void launch_bicg_p(cudaStream_t st, int64_t n, const double* r, const double* v, double beta, double omega, double* p,
                    int first);
 void launch_bicg_s(cudaStream_t st, int64_t n, const double* r, const double* v, double alpha, double* s,
-                   const double* rh, double* partials, double* out);
+                   double* partials, double* out);
 void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const double* z, double alpha,
                    double omega, double* r, const double* s, const double* t, const double* rh, double* partials,
                    double* out);
 
+// The local solve of every subdomain (or one): forward sweep, tail coupling, two dense tail GEMVs,
+// backward coupling, backward sweep + epilogue.  `tr_range`/`us_range` restrict the row-list
+// kernels (first, count); `launches` receives the number of kernels issued.
 template <typename Real>
-cudaError_t launch_local_solve(cudaStream_t st, const SolveArgs<Real>& a, int nblocks, size_t smem_bytes);
+cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem_bytes,
+                               int group, int tr_first, int tr_count, int us_first, int us_count, int* launches);
 
 void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int32_t* cp_pos, const double* cp_w,
                     const double* ylocal, const double* base, double* out);
@@ -103,5 +126,6 @@ void launch_dense_gemv(cudaStream_t st, int n0, const double* M, const double* x
 void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
                            const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
                            const double* y, double* out, double* plocal);
+void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 
 }  // namespace s2l

@@ -29,7 +29,8 @@ EXPORTED = [
     "s2l_gpu_add_subdomain", "s2l_gpu_set_coarse", "s2l_gpu_setup_end", "s2l_gpu_setup_destroy",
     "s2l_gpu_setup_bytes", "s2l_gpu_spmv", "s2l_gpu_local_solve", "s2l_gpu_coarse_apply",
     "s2l_gpu_one_level_apply", "s2l_gpu_apply", "s2l_gpu_gmres", "s2l_gpu_bicgstab", "s2l_gpu_set_stream",
-    "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes",
+    "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes", "s2l_gpu_setup_option",
+    "s2l_gpu_setup_stat",
 ]
 
 
@@ -88,6 +89,8 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_profile_enable": ([vp, C.c_int], C.c_int),
         "s2l_gpu_profile_get": ([vp, C.c_char_p, dp, C.POINTER(C.c_long)], C.c_int),
         "s2l_gpu_local_solve_bytes": ([vp, dp], C.c_int),
+        "s2l_gpu_setup_option": ([vp, C.c_char_p, C.c_double], C.c_int),
+        "s2l_gpu_setup_stat": ([vp, C.c_char_p, dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -139,7 +142,7 @@ class Context:
 class GpuSetup:
     """One matrix's setup on the GPU (the drop-in for the reference's TwoLevelSchwarz + Krylov)."""
 
-    def __init__(self, ctx: Context, st: Setup, one_level=None, coarse=None, pou=None):
+    def __init__(self, ctx: Context, st: Setup, one_level=None, coarse=None, pou=None, options=None):
         self.ctx = ctx
         self.lib = ctx.lib
         self.n = st.n
@@ -150,6 +153,8 @@ class GpuSetup:
                                                 COARSE[coarse or opts.coarse], POU[pou or opts.pou], C.byref(h)))
         self.h = h
         try:
+            for k, v in (options or {}).items():
+                ctx.check(self.lib.s2l_gpu_setup_option(h, k.encode(), float(v)))
             self._upload(st, coarse or opts.coarse)
         except Exception:
             self.close()
@@ -294,6 +299,11 @@ class GpuSetup:
         b = C.c_double()
         self.ctx.check(self.lib.s2l_gpu_local_solve_bytes(self.h, C.byref(b)))
         return b.value
+
+    def stat(self, name: str) -> float:
+        v = C.c_double()
+        self.ctx.check(self.lib.s2l_gpu_setup_stat(self.h, name.encode(), C.byref(v)))
+        return v.value
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

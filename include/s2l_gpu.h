@@ -121,11 +121,23 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
 /* Coarse matrix E = R0 A R0^T (n0 x n0, row-major) and coarse offsets (nsub+1 entries). */
 int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E);
 
+/*
+ * Layout options, before s2l_gpu_setup_end (no reference counterpart: they only choose how the
+ * same factors are laid out on the device).  "tail_min"/"tail_max" (rows, default 96/4096) and
+ * "tail_density" (default 0.25): the trailing block [T, n) of each factor whose strictly-lower
+ * part is at least that full is solved through its dense inverse; "sweep_group" (0 = automatic,
+ * 8, 16 or 32): threads per row in the sparse sweeps.
+ */
+int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
+
 int s2l_gpu_setup_end(s2l_setup* s);
 int s2l_gpu_setup_destroy(s2l_setup* s);
 
 /* Device bytes held by the setup (matrix, factors, basis, schedules, work vectors). */
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
+/* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
+   "sweep_group", "smem_bytes". */
+int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 
 /* ---- solve phase ---------------------------------------------------------------------- */
 int s2l_gpu_spmv(s2l_setup* s, const double* x, double* y, int ptr_kind);

@@ -27,13 +27,14 @@ def ctx():
     c.close()
 
 
+@pytest.mark.parametrize("layout", [{}, {"tail_min": 8, "tail_density": 0.05}])
 @pytest.mark.parametrize("case", CASES)
-def test_gpu_reproduces_reference(ctx, case):
+def test_gpu_reproduces_reference(ctx, case, layout):
     from s2l_b200.capi import GpuSetup
     st, applies, kr, local = G.load(case)
     single = st.opts.local_precision == "single"
     tol = 1e-5 if single else 1e-12
-    g = GpuSetup(ctx, st)
+    g = GpuSetup(ctx, st, options=layout)
     for i, (b, x) in enumerate(local):
         assert rel(g.local_solve(i, b), x) <= tol
     for a in applies:

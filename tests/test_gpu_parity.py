@@ -163,3 +163,46 @@ def test_hbm_budget_refusal():
         capi.GpuSetup(c, st)
     assert e.value.code == 2
     c.close()
+
+
+LAYOUTS = [
+    {},
+    {"tail_min": 8, "tail_density": 0.05},   # force dense tails on small subdomains
+    {"tail_min": 1_000_000},                 # no dense tail: the sweeps do all rows
+    {"sweep_group": 8, "tail_min": 16, "tail_density": 0.1},
+    {"sweep_group": 16},
+]
+
+
+@pytest.mark.parametrize("layout", range(len(LAYOUTS)))
+@pytest.mark.parametrize("name", ["poisson2d", "bubbles3d", "convdiff3d"])
+def test_layouts_agree_with_oracle(ctx, rng, name, layout):
+    """Every device layout of the same factors (dense tail split, sweep group width) gives the
+    oracle's local solves and two-level apply to 1e-12."""
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup(name)
+    opts = LAYOUTS[layout]
+    g = GpuSetup(ctx, st, options=opts)
+    if "tail_density" in opts:
+        assert g.stat("tail_rows") > 0
+    if opts.get("tail_min") == 1_000_000:
+        assert g.stat("tail_rows") == 0
+    o = OracleSetup(st)
+    for i, s in enumerate(st.subdomains):
+        b = rng.standard_normal(s.n_local)
+        assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-12
+    r = rng.standard_normal(st.n)
+    assert rel(g.apply(r), o.apply(r)) <= 1e-12
+    g.close()
+
+
+def test_forced_tail_single_precision(ctx, rng):
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("convdiff3d", precision="single")
+    g = GpuSetup(ctx, st, options={"tail_min": 8, "tail_density": 0.05})
+    assert g.stat("tail_rows") > 0
+    o = OracleSetup(st)
+    for i, s in enumerate(st.subdomains):
+        b = rng.standard_normal(s.n_local)
+        assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-5
+    g.close()
