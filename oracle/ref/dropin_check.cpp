@@ -1,0 +1,98 @@
+// Checks the C++ drop-in (algebraic-multilevel-preconditioner_b200/host/s2l_dropin.*) against the
+// reference itself.  TEST INFRASTRUCTURE ONLY (run by tests/test_gpu_dropin.py on the GPU host).
+//
+// With the reference's flags it builds, on S2L_NP thread-ranks, the reference's own
+// preconditioner and Krylov solver and the drop-in GpuTwoLevelSchwarz / GpuKrylov from the same
+// set-up objects, then compares: Preconditioner::apply of seeded vectors (relative difference), and
+// KrylovSolver::solve (iterations, convergence, true residual, solution).  Rank 0 prints one JSON
+// line; the exit code is 0 when every comparison is within tolerance.
+#include "s2l_dropin.hpp"
+
+#include "domain_decomposer.hpp"
+#include "mpi_utils.hpp"
+
+#include <cmath>
+#include <iomanip>
+#include <iostream>
+#include <random>
+#include <sstream>
+
+using namespace schwarz2lvl;
+
+int main(int argc, char** argv)
+{
+    MPI_Init(&argc, &argv);
+    MPI_Comm comm = MPI_COMM_WORLD;
+    const int rank = core::mpiRank(comm);
+    int code = 0;
+    try {
+        const core::SolverConfig cfg = core::SolverConfig::fromCommandLine(argc, argv);
+        part::DecompositionInfo info;
+        core::LocalSystem sys = part::DomainDecomposer::decompose(cfg, comm, info);
+        part::Subdomain sd(sys, cfg.pou);
+        linalg::DistributedMatrix A(sd);
+        std::unique_ptr<prec::Preconditioner> M;
+        const prec::OneLevelSchwarz* one = nullptr;
+        const prec::TwoLevelSchwarz* two = nullptr;
+        if (cfg.coarse == "none") {
+            auto p = std::make_unique<prec::OneLevelSchwarz>(
+                sd, cfg.one_level == "asm" ? prec::OneLevelSchwarz::Variant::ASM : prec::OneLevelSchwarz::Variant::RAS,
+                prec::localSolverSpec(cfg, sys.symmetric));
+            one = p.get();
+            M = std::move(p);
+        } else {
+            auto p = std::make_unique<prec::TwoLevelSchwarz>(sd, A, cfg);
+            two = p.get();
+            one = &p->oneLevel();
+            M = std::move(p);
+        }
+        auto phase = std::make_shared<s2l::dropin::GpuSolvePhase>(sd, *one, two, cfg, 0, 0);
+        s2l::dropin::GpuTwoLevelSchwarz G(phase, M->name());
+        // apply parity on seeded vectors (U[-1,1], owned part of a global renumbered vector)
+        double worst = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            std::mt19937_64 g(4242 + k);
+            std::uniform_real_distribution<double> u(-1.0, 1.0);
+            std::vector<double> rg((size_t)sys.n_global);
+            for (auto& v : rg) v = u(g);
+            core::Vec r(sys.nOwned()), z1, z2;
+            for (int i = 0; i < sys.nOwned(); ++i) r[i] = rg[(size_t)(sys.rowBegin() + i)];
+            M->apply(r, z1);
+            G.apply(r, z2);
+            double num = (z1 - z2).squaredNorm(), den = z1.squaredNorm();
+            double gn = 0.0, gd = 0.0;
+            MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
+            MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
+            worst = std::max(worst, std::sqrt(gn / gd));
+        }
+        // solves: the reference's Krylov solver with its preconditioner, the GPU's with the drop-in
+        const core::Vec b = Eigen::Map<const core::Vec>(sys.rhs.data(), (Eigen::Index)sys.rhs.size());
+        core::Vec x1 = core::Vec::Zero(b.size()), x2 = core::Vec::Zero(b.size());
+        const solv::KrylovResult r1 = solv::makeKrylovSolver(cfg)->solve(A, *M, b, x1);
+        auto gk = s2l::dropin::makeGpuKrylovSolver(cfg);
+        const solv::KrylovResult r2 = gk->solve(A, G, b, x2);
+        double num = (x1 - x2).squaredNorm(), den = x1.squaredNorm(), gn = 0, gd = 0;
+        MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
+        MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
+        const double xdiff = std::sqrt(gn / gd);
+        const bool single = cfg.local_precision == "single";
+        const double tol = single ? 1e-5 : 1e-12;
+        const bool ok = worst <= tol && r2.converged && r2.true_rel_residual <= 1.1 * cfg.rtol &&
+                        std::abs(r1.iterations - r2.iterations) <= (single ? 3 : 1);
+        if (rank == 0) {
+            std::ostringstream s;
+            s << std::setprecision(6) << "{\"apply_rel_diff\": " << worst << ", \"ref_iterations\": " << r1.iterations
+              << ", \"gpu_iterations\": " << r2.iterations << ", \"gpu_converged\": " << (r2.converged ? "true" : "false")
+              << ", \"gpu_true_rel_residual\": " << r2.true_rel_residual << ", \"ref_true_rel_residual\": "
+              << r1.true_rel_residual << ", \"x_rel_diff\": " << xdiff << ", \"gpu_solver\": \"" << gk->name()
+              << "\", \"ok\": " << (ok ? "true" : "false") << "}";
+            std::cout << s.str() << std::endl;
+        }
+        code = ok ? 0 : 1;
+    } catch (const std::exception& e) {
+        std::cerr << "[rank " << rank << "] error: " << e.what() << std::endl;
+        code = 2;
+    }
+    MPI_Finalize();
+    return code;
+}

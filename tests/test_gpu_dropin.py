@@ -1,0 +1,43 @@
+"""The C++ drop-in (host/s2l_dropin.*) inside the reference itself, on the GPU.
+
+oracle/_ref/dropin_check builds, on thread-ranks, the reference's own preconditioner and Krylov
+solver and the drop-in GpuTwoLevelSchwarz / GpuKrylov from the same set-up objects, and compares
+Preconditioner::apply (1e-12 FP64, 1e-5 FP32 factors) and KrylovSolver::solve (iterations within
++-1, GPU true residual <= 1.1 rtol).  The binary is built where the reference sources are
+(oracle/ref/Makefile) and travels with the repository copy.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+from conftest import REPO
+
+pytestmark = pytest.mark.gpu
+BIN = os.path.join(REPO, "oracle", "_ref", "dropin_check")
+COMMON = ["--local-solver", "sparselu", "--coarse-solver", "root", "--verbose", "0", "--rhs", "random"]
+CASES = {
+    "laplace2d_ras_additive_lu": (4, ["--generate", "laplace2d", "--nx", "32", "--nev", "8", "--coarse", "additive",
+                                      "--local-factorization", "lu"]),
+    "bubbles3d_ras_deflated_llt": (8, ["--generate", "bubbles3d", "--nx", "16", "--nbubbles", "8", "--radius",
+                                       "0.12", "--nev", "10", "--coarse", "deflated", "--local-factorization",
+                                       "cholesky", "--restart", "50"]),
+    "convdiff3d_single_lu": (4, ["--generate", "convdiff3d", "--nx", "12", "--nev", "8", "--coarse", "deflated",
+                                 "--local-factorization", "lu", "--local-precision", "single", "--restart", "40"]),
+    "laplace2d_asm_mult_bicgstab": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--pou",
+                                        "multiplicity", "--one-level", "asm", "--krylov", "bicgstab"]),
+}
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="oracle/_ref/dropin_check is built only where the reference sources are")
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_dropin_matches_reference(case):
+    np_, args = CASES[case]
+    env = dict(os.environ, S2L_NP=str(np_), OMP_NUM_THREADS="1")
+    r = subprocess.run([BIN, *COMMON, *args], env=env, capture_output=True, text=True, timeout=600)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert lines, f"no result (rc={r.returncode}): {r.stderr[-2000:]}"
+    res = json.loads(lines[-1])
+    assert res["ok"], res
+    assert r.returncode == 0
