@@ -31,6 +31,17 @@ struct s2l_ctx {
 namespace {
 
 enum { PC_SPMV = 0, PC_SOLVE, PC_COARSE, PC_COMBINE, PC_VEC, PC_N };
+
+struct s2l_tail_model {
+    int force_rows = 0;      // > 0: every subdomain gets a tail of this many rows
+    int tail_min = 64;       // smallest tail considered (0 rows is always allowed)
+    int tail_max = 4096;
+    double hop_s = 0.25e-6;  // time of one dependency level of a sweep
+    double bw = 6.0e12;      // bytes/s shared by all subdomains
+    double nsub = 1.0;
+    double real_bytes = 8.0;
+    double smem_cap = 227.0 * 1024.0 - 1024.0;
+};
 const char* kProfNames[PC_N] = {"spmv", "local_solve", "coarse", "combine", "krylov_vec"};
 
 struct HostCsr {
@@ -54,15 +65,16 @@ struct HostSub {
     int n_local() const { return n_owned + n_ghost; }
 };
 
-// one triangular factor of one subdomain in solve order
-struct Sched {
-    std::vector<int32_t> rows;
-    std::vector<int64_t> ptr;  // relative to the subdomain's first entry
-    std::vector<int32_t> col;
+// sparse part of one triangular factor of one subdomain, renumbered in solve order
+struct Sweep {
+    std::vector<int32_t> order;   // slot -> row
+    std::vector<int32_t> pos;     // row -> slot
+    std::vector<uint16_t> len;    // entries per slot
+    std::vector<double> dinv;     // per slot
+    std::vector<int32_t> col;     // column slots, group-contiguous
     std::vector<double> val;
-    std::vector<double> dinv;
-    std::vector<int32_t> lvl;
-    std::vector<int8_t> mode;
+    std::vector<int64_t> gstart;  // per group, relative to the subdomain's first entry
+    int nlev = 0;
 };
 
 }  // namespace
@@ -96,9 +108,10 @@ struct s2l_setup {
     std::vector<DevSub> h_subs;
     DevSub* d_subs = nullptr;
     int64_t nloc = 0;
-    int32_t* d_rows[2] = {nullptr, nullptr};
-    int64_t* d_ptr[2] = {nullptr, nullptr};
+    uint16_t* d_len[2] = {nullptr, nullptr};
+    int64_t* d_gstart[2] = {nullptr, nullptr};
     int32_t* d_col[2] = {nullptr, nullptr};
+    int32_t* d_u2l = nullptr;
     void* d_val[2] = {nullptr, nullptr};
     void* d_dinv[2] = {nullptr, nullptr};
     int32_t *d_tr_sub = nullptr, *d_tr_i = nullptr, *d_lts_col = nullptr;
@@ -114,8 +127,8 @@ struct s2l_setup {
     std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
-    int opt_tail_min = 96, opt_tail_max = 4096, opt_group = 0;
-    double opt_tail_density = 0.25;
+    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0;
+    double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
     int32_t *d_gin = nullptr, *d_pin = nullptr, *d_gout = nullptr, *d_l2g = nullptr;
@@ -228,25 +241,17 @@ int alloc_doubles(s2l_setup* s, double** p, size_t count)
     return dev_alloc(s, reinterpret_cast<void**>(p), count * sizeof(double));
 }
 
-// Sweep schedule of the sparse part of a triangular factor: rows [0, T), off-diagonal entries
-// with a column < T, rows sorted by dependency level (lower: forward, upper: backward), which is a
-// topological order of the rows with independent rows next to each other.
-void build_sweep(const HostCsr& M, int n, int T, bool lower, bool unit_diag, Sched& out, std::string& err)
+// Dependency levels of the rows [0, T) of a triangular factor (lower: forward, entries c < r;
+// upper: backward, entries r < c < T).  Returns the number of levels.
+int sweep_levels(const HostCsr& M, int T, bool lower, std::vector<int32_t>& level)
 {
-    std::vector<int32_t> level(T, 0);
-    std::vector<double> diag(T, 1.0);
-    std::vector<int64_t> offcnt(T, 0);
+    level.assign(T, 0);
     auto visit = [&](int r) {
         int lv = 0;
         for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
             const int c = M.ci[e];
-            if (c == r) {
-                diag[r] = M.v[e];
-                continue;
-            }
-            if (lower ? (c > r) : (c < r || c >= T)) continue;
+            if (c == r || (lower ? (c > r) : (c < r || c >= T))) continue;
             lv = std::max(lv, level[c] + 1);
-            ++offcnt[r];
         }
         level[r] = lv;
     };
@@ -256,60 +261,120 @@ void build_sweep(const HostCsr& M, int n, int T, bool lower, bool unit_diag, Sch
         for (int r = T - 1; r >= 0; --r) visit(r);
     int nlev = 0;
     for (int r = 0; r < T; ++r) nlev = std::max(nlev, level[r] + 1);
-    std::vector<int32_t> cnt(nlev + 1, 0);
+    return nlev;
+}
+
+// Sweep layout of the sparse part (rows [0, T)): slots in level order, columns as slots, the rows
+// of group g (slots g, g + ng, ...) stored back to back.
+void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int ng, Sweep& out, std::string& err)
+{
+    std::vector<int32_t> level;
+    out.nlev = sweep_levels(M, T, lower, level);
+    std::vector<int32_t> cnt(out.nlev + 1, 0);
     for (int r = 0; r < T; ++r) ++cnt[level[r] + 1];
-    for (int l = 0; l < nlev; ++l) cnt[l + 1] += cnt[l];
-    out.lvl.assign(cnt.begin(), cnt.end());
-    std::vector<int32_t> next(cnt.begin(), cnt.end() - 1);
-    out.rows.assign(T, 0);
-    if (lower) {
-        for (int r = 0; r < T; ++r) out.rows[next[level[r]]++] = r;
-    } else {
-        for (int r = T - 1; r >= 0; --r) out.rows[next[level[r]]++] = r;
+    for (int l = 0; l < out.nlev; ++l) cnt[l + 1] += cnt[l];
+    out.order.assign(T, 0);
+    out.pos.assign(T, 0);
+    {
+        std::vector<int32_t> next(cnt.begin(), cnt.end() - 1);
+        if (lower)
+            for (int r = 0; r < T; ++r) out.order[next[level[r]]++] = r;
+        else
+            for (int r = T - 1; r >= 0; --r) out.order[next[level[r]]++] = r;
     }
-    out.ptr.assign(T + 1, 0);
-    for (int p = 0; p < T; ++p) out.ptr[p + 1] = out.ptr[p] + offcnt[out.rows[p]];
-    out.col.resize(out.ptr[T]);
-    out.val.resize(out.ptr[T]);
-    out.dinv.resize(T);
+    for (int p = 0; p < T; ++p) out.pos[out.order[p]] = p;
+    out.len.assign(T, 0);
+    out.dinv.assign(T, 1.0);
+    std::vector<std::vector<std::pair<int32_t, double>>> rows(T);
     for (int p = 0; p < T; ++p) {
-        const int r = out.rows[p];
-        int64_t q = out.ptr[p];
+        const int r = out.order[p];
+        double dg = 1.0;
         for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
             const int c = M.ci[e];
-            if (c == r || (lower ? (c > r) : (c < r || c >= T))) continue;
-            out.col[q] = c;
-            out.val[q] = M.v[e];
-            ++q;
+            if (c == r) {
+                dg = M.v[e];
+                continue;
+            }
+            if (lower ? (c > r) : (c < r || c >= T)) continue;
+            rows[p].emplace_back(out.pos[c], M.v[e]);
         }
-        const double dg = unit_diag ? 1.0 : diag[r];
+        if (rows[p].size() >= 65535) {
+            err = "a sparse row has 65535 or more entries";
+            return;
+        }
+        out.len[p] = (uint16_t)rows[p].size();
+        if (unit_diag) dg = 1.0;
         if (dg == 0.0 || !std::isfinite(dg)) {
             err = "zero or non-finite diagonal in a triangular factor";
             return;
         }
         out.dinv[p] = 1.0 / dg;
     }
-    (void)n;
+    out.gstart.assign(ng, 0);
+    out.col.clear();
+    out.val.clear();
+    for (int g = 0; g < ng; ++g) {
+        out.gstart[g] = (int64_t)out.col.size();
+        for (int p = g; p < T; p += ng)
+            for (const auto& cv : rows[p]) {
+                out.col.push_back(cv.first);
+                out.val.push_back(cv.second);
+            }
+    }
 }
 
-// Tail split: the largest trailing block [T, n) of L whose strictly-lower part is at least
-// `density` full, with tail_min <= n - T <= tail_max (T = n: no dense tail).
-int choose_tail(const HostCsr& L, int n, int tail_min, int tail_max, double density)
+// Tail split of one subdomain: T minimising  2 hop levels(T) + bytes(T) nsub / bw, where levels is
+// the dependency depth of the sparse rows < T (forward levels of L, a row's level depends on
+// smaller rows only) and bytes what one local solve reads for this split: sparse entries of L and
+// U, coupling entries L(T:n, 0:T) and U(0:T, T:n), and the two dense triangles of the tail.  The
+// tail is at most tail_max rows; the sweep's shared memory must hold T rows.
+int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model& tm)
 {
-    if (n < tail_min || tail_min <= 0) return n;
-    std::vector<int64_t> colcnt(n + 1, 0);
-    for (int r = 0; r < n; ++r)
-        for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e)
-            if (L.ci[e] < r) ++colcnt[L.ci[e]];
-    // suffix sums: entries (r, c) with c >= T lie inside the trailing block
-    std::vector<int64_t> suf(n + 1, 0);
-    for (int c = n - 1; c >= 0; --c) suf[c] = suf[c + 1] + colcnt[c];
-    for (int sz = std::min(tail_max, n); sz >= tail_min; --sz) {
-        const int T = n - sz;
-        const double full = 0.5 * (double)sz * (double)(sz - 1);
-        if ((double)suf[T] >= density * full) return T;
+    if (tm.force_rows > 0) return std::max(1, n - std::min(tm.force_rows, n - 1));
+    std::vector<int32_t> level;
+    sweep_levels(L, n, true, level);
+    std::vector<int32_t> maxlev(n + 1, 0);  // levels of rows [0, T)
+    for (int r = 0; r < n; ++r) maxlev[r + 1] = std::max(maxlev[r], level[r] + 1);
+    // entry counts as functions of T (difference arrays)
+    std::vector<double> sp(n + 2, 0.0), cp(n + 2, 0.0);
+    auto account = [&](const HostCsr& M, bool lower) {
+        for (int r = 0; r < n; ++r)
+            for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
+                const int c = M.ci[e];
+                if (c == r || (lower ? c > r : c < r)) continue;
+                const int lo = std::min(r, c), hi = std::max(r, c);
+                // sparse-part entry iff hi < T  ->  T in [hi + 1, n]
+                sp[hi + 1] += 1.0;
+                // coupling entry iff lo < T <= hi  ->  T in [lo + 1, hi]
+                cp[lo + 1] += 1.0;
+                cp[hi + 1] -= 1.0;
+            }
+    };
+    account(L, true);
+    account(U, false);
+    const double rs = tm.real_bytes, idx = 4.0;
+    double best = 1e300;
+    int bestT = n;
+    double spc = 0.0, cpc = 0.0;
+    std::vector<double> spT(n + 1, 0.0), cpT(n + 1, 0.0);
+    for (int T = 0; T <= n; ++T) {
+        spc += sp[T];
+        cpc += cp[T];
+        spT[T] = spc;
+        cpT[T] = cpc;
     }
-    return n;
+    for (int T = n; T >= std::max(1, n - tm.tail_max); --T) {
+        const double sz = n - T;
+        if (sz > 0 && sz < tm.tail_min) continue;
+        if ((double)T * (rs + 3.0) + 64.0 > tm.smem_cap) continue;
+        const double bytes = (spT[T] + cpT[T]) * (rs + idx) + sz * (sz + 1.0) * rs + 2.0 * T * (rs + 2.0);
+        const double cost = 2.0 * tm.hop_s * maxlev[T] + bytes * tm.nsub / tm.bw;
+        if (cost < best) {
+            best = cost;
+            bestT = T;
+        }
+    }
+    return bestT;
 }
 
 // transpose of a lower CSR (values scaled by rowscale[c] of the result rows if given)
@@ -454,7 +519,8 @@ LocalSolveArgs<Real> solve_args(s2l_setup* s)
     LocalSolveArgs<Real> a{};
     a.subs = s->d_subs;
     for (int f = 0; f < 2; ++f)
-        a.f[f] = {s->d_rows[f], s->d_ptr[f], s->d_col[f], (const Real*)s->d_val[f], (const Real*)s->d_dinv[f]};
+        a.f[f] = {s->d_col[f], (const Real*)s->d_val[f], (const Real*)s->d_dinv[f], s->d_len[f], s->d_gstart[f]};
+    a.u2l = s->d_u2l;
     a.tr_sub = s->d_tr_sub;
     a.tr_i = s->d_tr_i;
     a.lts_ptr = s->d_lts_ptr;
@@ -922,21 +988,66 @@ int s2l_gpu_setup_end(s2l_setup* s)
         s->tpr = avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32));
     }
 
-    // ---- per-subdomain factor split, schedules and index maps
+    // ---- per-subdomain factor split, sweep layouts and index maps
     s->h_subs.resize(nsub);
     const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    // pass 1: full U of every subdomain and its tail split
+    std::vector<HostCsr> Us(nsub);
+    std::vector<int> Ts(nsub);
+    s2l_tail_model tm;
+    tm.force_rows = s->opt_tail_rows;
+    tm.tail_min = s->opt_tail_min;
+    tm.tail_max = s->opt_tail_max;
+    tm.hop_s = s->opt_hop_us * 1e-6;
+    tm.bw = s->opt_bw_gbs * 1e9;
+    tm.nsub = nsub;
+    tm.real_bytes = (double)rs;
+    double sp_nnz_total = 0.0, sp_rows_total = 0.0;
+    for (int i = 0; i < nsub; ++i) {
+        HostSub& h = s->hs[i];
+        const int nl = h.n_local();
+        if (h.kind == S2L_FACTOR_LU) {
+            Us[i] = std::move(h.U);
+        } else {
+            Us[i] = transpose_lower(h.L, nl, nullptr);
+            if (h.kind == S2L_FACTOR_LDLT) {
+                bool missing = false;
+                for (int r = 0; r < nl; ++r) {
+                    bool f = false;
+                    for (int64_t e = Us[i].rp[r]; e < Us[i].rp[r + 1]; ++e) {
+                        if (Us[i].ci[e] == r) {
+                            Us[i].v[e] = h.d[r];
+                            f = true;
+                        } else {
+                            Us[i].v[e] *= h.d[r];
+                        }
+                    }
+                    missing = missing || !f;
+                }
+                if (missing) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
+            }
+        }
+        Ts[i] = choose_tail(h.L, Us[i], nl, tm);
+        for (int r = 0; r < Ts[i]; ++r)
+            for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) sp_nnz_total += h.L.ci[e] < r ? 1.0 : 0.0;
+        sp_rows_total += Ts[i];
+    }
+    {
+        const double avg = sp_rows_total > 0 ? sp_nnz_total / sp_rows_total : 0.0;
+        s->sweep_group = s->opt_group ? s->opt_group : (avg <= 10.0 ? 8 : (avg <= 24.0 ? 16 : 32));
+    }
+    const int ng = S2L_BS_SWEEP / s->sweep_group;
+    // pass 2: layouts
     int64_t loc = 0;
-    std::vector<int32_t> gin, pin, gout, l2g;
+    std::vector<int32_t> gin, pin, gout, l2g, u2l;
     std::vector<double> Dall;
-    // concatenated sweep data (f = 0: L forward, 1: U backward)
-    std::vector<int32_t> sw_rows[2], sw_col[2];
-    std::vector<int64_t> sw_ptr[2];
+    std::vector<int32_t> sw_col[2];
     std::vector<double> sw_val[2], sw_dinv[2];
-    // tail rows (L coupling) and sparse rows with U coupling
+    std::vector<uint16_t> sw_len[2];
+    std::vector<int64_t> sw_gstart[2];
     std::vector<int32_t> tr_sub, tr_i, lts_col, us_sub, us_r, ust_col;
     std::vector<int64_t> lts_ptr(1, 0), ust_ptr(1, 0);
     std::vector<double> lts_val, ust_val;
-    // dense tails (row-major), inverted on the device below
     std::vector<std::vector<double>> Ltt(nsub), Utt(nsub);
     std::vector<int64_t> d_off(nsub + 1, 0);
     s->tr_first_h.assign(nsub + 1, 0);
@@ -946,57 +1057,35 @@ int s2l_gpu_setup_end(s2l_setup* s)
     int64_t sparse_nnz = 0;
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
+        const HostCsr& U = Us[i];
         const int nl = h.n_local();
         max_nl = std::max(max_nl, nl);
         const bool unitL = h.kind != S2L_FACTOR_LLT;
-        HostCsr U;
-        if (h.kind == S2L_FACTOR_LU) {
-            U = std::move(h.U);
-        } else {
-            U = transpose_lower(h.L, nl, nullptr);
-            if (h.kind == S2L_FACTOR_LDLT) {
-                bool missing = false;
-                for (int r = 0; r < nl; ++r) {
-                    bool f = false;
-                    for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
-                        if (U.ci[e] == r) {
-                            U.v[e] = h.d[r];
-                            f = true;
-                        } else {
-                            U.v[e] *= h.d[r];
-                        }
-                    }
-                    missing = missing || !f;
-                }
-                if (missing) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
-            }
-        }
-        const int T = choose_tail(h.L, nl, s->opt_tail_min, s->opt_tail_max, s->opt_tail_density);
+        const int T = Ts[i];
         const int sz = nl - T;
         max_T = std::max(max_T, T);
         std::string err;
-        Sched sl, su;
-        build_sweep(h.L, nl, T, true, unitL, sl, err);
-        if (err.empty()) build_sweep(U, nl, T, false, false, su, err);
+        Sweep sl, su;
+        build_sweep(h.L, T, true, unitL, ng, sl, err);
+        if (err.empty()) build_sweep(U, T, false, false, ng, su, err);
         if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
         for (int f = 0; f < 2; ++f) {
-            const Sched& q = f == 0 ? sl : su;
+            const Sweep& q = f == 0 ? sl : su;
             const int64_t e0 = sw_col[f].size();
-            sw_rows[f].insert(sw_rows[f].end(), q.rows.begin(), q.rows.end());
-            for (int p = 0; p < T; ++p) sw_ptr[f].push_back(e0 + q.ptr[p]);
-            // slots [T, n) of the subdomain are unused by the sweeps: empty rows keep the layout flat
-            for (int p = T; p < nl; ++p) {
-                sw_ptr[f].push_back(e0 + q.ptr[T]);
-                sw_rows[f].push_back(p);
-            }
+            for (int g = 0; g < ng; ++g) sw_gstart[f].push_back(e0 + q.gstart[g]);
             sw_col[f].insert(sw_col[f].end(), q.col.begin(), q.col.end());
             sw_val[f].insert(sw_val[f].end(), q.val.begin(), q.val.end());
             sw_dinv[f].insert(sw_dinv[f].end(), q.dinv.begin(), q.dinv.end());
             sw_dinv[f].resize(sw_dinv[f].size() + sz, 1.0);
+            sw_len[f].insert(sw_len[f].end(), q.len.begin(), q.len.end());
+            sw_len[f].resize(sw_len[f].size() + sz, 0);
             sparse_nnz += (int64_t)q.col.size();
-            bytes += (double)q.col.size() * (rs + 4) + (double)T * (4 + 8 + rs);
+            bytes += (double)q.col.size() * (rs + 4) + (double)T * (2 + rs);
         }
-        // L coupling of the tail rows and the dense lower tail
+        // backward slot -> forward slot
+        for (int u = 0; u < T; ++u) u2l.push_back(sl.pos[su.order[u]]);
+        u2l.resize(u2l.size() + sz, 0);
+        // L coupling of the tail rows (columns as forward slots) and the dense lower tail
         s->tr_first_h[i] = (int)tr_sub.size();
         if (sz > 0) {
             Ltt[i].assign((size_t)sz * sz, 0.0);
@@ -1006,7 +1095,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 for (int64_t e = h.L.rp[k]; e < h.L.rp[k + 1]; ++e) {
                     const int c = h.L.ci[e];
                     if (c < T) {
-                        lts_col.push_back(c);
+                        lts_col.push_back(sl.pos[c]);
                         lts_val.push_back(h.L.v[e]);
                     } else if (c < k) {
                         Ltt[i][(size_t)(k - T) * sz + (c - T)] = h.L.v[e];
@@ -1027,7 +1116,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 if (Utt[i][(size_t)k * sz + k] == 0.0 || Ltt[i][(size_t)k * sz + k] == 0.0)
                     return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": zero pivot in the dense tail");
         }
-        // U coupling of the sparse rows
+        // U coupling of the sparse rows: the target is the row's forward slot (ybuf keeps forward order)
         s->us_first_h[i] = (int)us_sub.size();
         if (sz > 0)
             for (int r = 0; r < T; ++r) {
@@ -1040,7 +1129,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     }
                 if (any) {
                     us_sub.push_back(i);
-                    us_r.push_back(r);
+                    us_r.push_back(sl.pos[r]);
                     ust_ptr.push_back((int64_t)ust_col.size());
                 }
             }
@@ -1062,16 +1151,21 @@ int s2l_gpu_setup_end(s2l_setup* s)
             const int64_t g = j < h.n_owned ? h.begin + j : h.ghosts[j - h.n_owned];
             l2g.push_back((int32_t)g);
         }
+        // forward gather per slot (< T) or tail row (>= T); backward output position per local j
         for (int k = 0; k < nl; ++k) {
-            gin.push_back(l2g[loc + h.pin[k]]);
-            pin.push_back(h.pin[k]);
-            gout.push_back(h.pout[k]);
+            const int prow = k < T ? sl.order[k] : k;
+            gin.push_back(l2g[loc + h.pin[prow]]);
+            pin.push_back(h.pin[prow]);
+        }
+        for (int j = 0; j < nl; ++j) {
+            const int q = h.pout[j];
+            gout.push_back(q < T ? su.pos[q] : q);
         }
         Dall.insert(Dall.end(), h.D.begin(), h.D.end());
-        // dense tails: the triangles of L^-1 and U^-1 are read once each
         bytes += (double)sz * (sz + 1) * rs;
         loc += nl;
         h.L = HostCsr();
+        Us[i] = HostCsr();
     }
     s->tr_first_h[nsub] = (int)tr_sub.size();
     s->us_first_h[nsub] = (int)us_sub.size();
@@ -1082,10 +1176,9 @@ int s2l_gpu_setup_end(s2l_setup* s)
     s->st_tail_rows = (int64_t)tr_sub.size();
     bytes += (double)s->st_coupling_nnz * (rs + 4) + (double)(tr_sub.size() + us_sub.size()) * (8 + 8 + rs);
     for (int f = 0; f < 2; ++f) {
-        sw_ptr[f].push_back((int64_t)sw_col[f].size());
-        RET_IF(upload(s, &s->d_rows[f], sw_rows[f]));
-        RET_IF(upload(s, &s->d_ptr[f], sw_ptr[f]));
         RET_IF(upload(s, &s->d_col[f], sw_col[f]));
+        RET_IF(upload(s, &s->d_len[f], sw_len[f]));
+        RET_IF(upload(s, &s->d_gstart[f], sw_gstart[f]));
         if (s->real == S2L_REAL_F32) {
             RET_IF(upload_real<float>(s, &s->d_val[f], sw_val[f]));
             RET_IF(upload_real<float>(s, &s->d_dinv[f], sw_dinv[f]));
@@ -1093,10 +1186,10 @@ int s2l_gpu_setup_end(s2l_setup* s)
             RET_IF(upload_real<double>(s, &s->d_val[f], sw_val[f]));
             RET_IF(upload_real<double>(s, &s->d_dinv[f], sw_dinv[f]));
         }
-        sw_rows[f] = {};
         sw_col[f] = {};
         sw_val[f] = {};
     }
+    RET_IF(upload(s, &s->d_u2l, u2l));
     RET_IF(upload(s, &s->d_tr_sub, tr_sub));
     RET_IF(upload(s, &s->d_tr_i, tr_i));
     RET_IF(upload(s, &s->d_lts_ptr, lts_ptr));
@@ -1122,11 +1215,6 @@ int s2l_gpu_setup_end(s2l_setup* s)
         bytes += (double)h.n_local() * (4 + 8) + (double)h.n_owned * (4 + 8 + 8);
     }
     s->solve_bytes = bytes;
-    {
-        // sweep group width from the mean row length of the sparse parts
-        const double avg = loc ? (double)sparse_nnz / (2.0 * (double)loc) : 0.0;
-        s->sweep_group = s->opt_group ? s->opt_group : (avg <= 6.0 ? 8 : (avg <= 14.0 ? 16 : 32));
-    }
     RET_IF(upload(s, &s->d_gin, gin));
     RET_IF(upload(s, &s->d_pin, pin));
     RET_IF(upload(s, &s->d_gout, gout));
@@ -1227,7 +1315,8 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(dev_alloc(s, reinterpret_cast<void**>(&s->d_err), 16));
     CUDA_OK(s, cudaMemsetAsync(s->d_err, 0, 16, s->stream));
     // sweep shared memory: x (T values) + one ready byte per row
-    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15);
+    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15) +
+                        ((((size_t)max_T * 2) + 15) & ~(size_t)15);
     const size_t smem_cap = 227 * 1024 - 64;
     if (smem <= smem_cap) {
         s->smem_bytes = smem;
@@ -1280,7 +1369,9 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
     const std::string n(name);
     if (n == "tail_min") s->opt_tail_min = (int)value;
     else if (n == "tail_max") s->opt_tail_max = (int)value;
-    else if (n == "tail_density") s->opt_tail_density = value;
+    else if (n == "tail_rows") s->opt_tail_rows = (int)value;
+    else if (n == "hop_us") s->opt_hop_us = value;
+    else if (n == "bw_gbs") s->opt_bw_gbs = value;
     else if (n == "sweep_group") {
         const int g = (int)value;
         if (g != 0 && g != 8 && g != 16 && g != 32) return s->fail(S2L_ERR_BADARG, "sweep_group must be 0, 8, 16 or 32");

@@ -242,16 +242,18 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 
 // ------------------------------------------------------------------------------ local solves (K2, K3)
 // Sparse sweep of one factor, one CTA per subdomain, x in shared memory (or, when it does not
-// fit, in the local-space buffer with global ready flags).
+// fit, in the local-space buffers with global ready flags and lengths).
 //
-// Rows are taken in solve order (a topological order: every dependency of slot p sits in a slot
-// < p).  Group g (G lanes) owns slots g, g + NG, g + 2 NG, ...; it waits, entry by entry, until
-// the ready flag of each column it reads is set, then writes its row and sets the row's flag.  A
-// group only ever waits for slots owned by groups that are at most one slot behind it, so the
-// sweep cannot deadlock.  Every wait is bounded: after S2L_SPIN_LIMIT polls the CTA raises *err
-// and all groups leave.  While a group works on one row its next S2L_PREFETCH rows are already in
-// flight (row id, entry range, 1/diag and the first G entries), so the latency of the factor
-// stream overlaps the dependency chain instead of adding to it.
+// Rows are slots in solve order (every dependency of slot p is a slot < p).  Group g (G lanes)
+// owns the slots g, g + NG, g + 2 NG, ... and their entries are stored back to back, so the group
+// knows where its next rows start from the row lengths alone (kept in shared memory).  For each
+// entry it waits until the ready flag of the column is set, then writes its row and sets its own
+// flag; no CTA barrier is taken per level.  A group only waits for smaller slots, and the smallest
+// unfinished slot always has its inputs ready, so the sweep cannot deadlock.  Every wait is
+// bounded: after S2L_SPIN_LIMIT polls the CTA raises *err and all groups leave.  While a group works
+// on one row, its next S2L_PREFETCH rows (1/diag and the first S2L_PREFETCH_CHUNKS*G entries) are
+// already in flight, with addresses that depend on no load, so the factor stream overlaps the
+// dependency chain instead of adding to it.
 template <typename Real, int G>
 __device__ __forceinline__ Real group_reduce(Real v)
 {
@@ -269,54 +271,66 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_word;
     volatile int& abort_flag = abort_word;
+    constexpr int NG = S2L_BS_SWEEP / G;
+    constexpr int D = S2L_PREFETCH;
+    constexpr int P = S2L_PREFETCH_CHUNKS;
     const int sid = a.sub_list ? a.sub_list[blockIdx.x] : (int)blockIdx.x;
     const DevSub sd = a.subs[sid];
     const int64_t lo = sd.loc_off;
     const int T = sd.T;
     const SweepFactor<Real> F = a.f[FWD ? 0 : 1];
-    Real* xs = SMEM ? reinterpret_cast<Real*>(smem_raw) : a.ybuf + lo;
-    volatile Real* x = xs;
+    Real* xs;
     volatile uint8_t* flag;
+    const uint16_t* lens;
     if (SMEM) {
-        const size_t off = (((size_t)T * sizeof(Real)) + 15) & ~(size_t)15;
-        flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off);
+        const size_t off1 = (((size_t)T * sizeof(Real)) + 15) & ~(size_t)15;
+        const size_t off2 = off1 + ((((size_t)T) + 15) & ~(size_t)15);
+        xs = reinterpret_cast<Real*>(smem_raw);
+        flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off1);
+        uint16_t* ls = reinterpret_cast<uint16_t*>(smem_raw + off2);
+        for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) ls[k] = F.len[lo + k];
+        lens = ls;
     } else {
+        xs = (FWD ? a.ybuf : a.xbuf) + lo;
         flag = a.gflags + lo;
+        lens = F.len + lo;
     }
+    volatile Real* x = xs;
     if (threadIdx.x == 0) abort_flag = 0;
     for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) {
-        if (FWD)
-            xs[k] = (Real)a.in[a.gather[lo + k]];
-        else if (SMEM)
-            xs[k] = a.ybuf[lo + k];
+        xs[k] = FWD ? (Real)a.in[a.gather[lo + k]] : a.ybuf[lo + a.u2l[lo + k]];
         flag[k] = 0;
     }
     __syncthreads();
-    constexpr int NG = S2L_BS_SWEEP / G;
-    constexpr int D = S2L_PREFETCH;
     const int g = threadIdx.x / G, l = threadIdx.x % G;
-    int pr_row[D];
-    int64_t pr_e0[D], pr_e1[D];
-    Real pr_dinv[D], pr_val[D];
-    int pr_col[D];
+    int64_t nst = F.gstart[(int64_t)sid * NG + g];  // start of the next row to prefetch
+    int pr_len[D];
+    int64_t pr_st[D];
+    Real pr_dinv[D];
+    int pr_col[D][P];
+    Real pr_val[D][P];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         const int p = g + d * NG;
-        pr_e0[d] = pr_e1[d] = 0;
-        pr_row[d] = 0;
+        pr_len[d] = 0;
+        pr_st[d] = nst;
         pr_dinv[d] = Real(1);
-        pr_col[d] = 0;
-        pr_val[d] = Real(0);
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            pr_col[d][k] = 0;
+            pr_val[d][k] = Real(0);
+        }
         if (p < T) {
-            const int64_t slot = lo + p;
-            pr_row[d] = F.rows[slot];
-            pr_e0[d] = F.ptr[slot];
-            pr_e1[d] = F.ptr[slot + 1];
-            pr_dinv[d] = F.dinv[slot];
-            if (pr_e0[d] + l < pr_e1[d]) {
-                pr_col[d] = F.col[pr_e0[d] + l];
-                pr_val[d] = F.val[pr_e0[d] + l];
-            }
+            const int L = lens[p];
+            pr_len[d] = L;
+            pr_dinv[d] = F.dinv[lo + p];
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                if (l + k * G < L) {
+                    pr_col[d][k] = F.col[nst + l + k * G];
+                    pr_val[d][k] = F.val[nst + l + k * G];
+                }
+            nst += L;
         }
     }
     bool dead = false;
@@ -326,25 +340,27 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
             const int p = p0 + d * NG;
             if (p < T && !dead) {
                 Real acc = Real(0);
-                int64_t e = pr_e0[d] + l;
-                const int64_t e1 = pr_e1[d];
-                if (e < e1) {
-                    const int c = pr_col[d];
-                    int spin = 0;
-                    while (flag[c] == 0) {
-                        if (abort_flag) { dead = true; break; }
-                        if (++spin > S2L_SPIN_LIMIT) {
-                            abort_flag = 1;
-                            atomicExch(a.err, 1);
-                            dead = true;
-                            break;
+                const int L = pr_len[d];
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    if (l + k * G < L && !dead) {
+                        const int c = pr_col[d][k];
+                        int spin = 0;
+                        while (flag[c] == 0) {
+                            if (abort_flag) { dead = true; break; }
+                            if (++spin > S2L_SPIN_LIMIT) {
+                                abort_flag = 1;
+                                atomicExch(a.err, 1);
+                                dead = true;
+                                break;
+                            }
                         }
+                        acc += pr_val[d][k] * x[c];
                     }
-                    acc += pr_val[d] * x[c];
                 }
-                for (e += G; e < e1 && !dead; e += G) {
-                    const int c = F.col[e];
-                    const Real v = F.val[e];
+                for (int e = l + P * G; e < L && !dead; e += G) {
+                    const int c = F.col[pr_st[d] + e];
+                    const Real v = F.val[pr_st[d] + e];
                     int spin = 0;
                     while (flag[c] == 0) {
                         if (abort_flag) { dead = true; break; }
@@ -364,23 +380,24 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
                 }
                 acc = group_reduce<Real, G>(acc);
                 if (l == 0 && !dead) {
-                    const int r = pr_row[d];
-                    x[r] = (x[r] - acc) * pr_dinv[d];
+                    x[p] = (x[p] - acc) * pr_dinv[d];
                     __threadfence_block();
-                    flag[r] = 1;
+                    flag[p] = 1;
                 }
-                // refill this prefetch slot with the group's slot D rows ahead
+                // refill this prefetch slot with the group's row D rows ahead
                 const int q = p + D * NG;
                 if (q < T) {
-                    const int64_t slot = lo + q;
-                    pr_row[d] = F.rows[slot];
-                    pr_e0[d] = F.ptr[slot];
-                    pr_e1[d] = F.ptr[slot + 1];
-                    pr_dinv[d] = F.dinv[slot];
-                    if (pr_e0[d] + l < pr_e1[d]) {
-                        pr_col[d] = F.col[pr_e0[d] + l];
-                        pr_val[d] = F.val[pr_e0[d] + l];
-                    }
+                    const int Lq = lens[q];
+                    pr_len[d] = Lq;
+                    pr_st[d] = nst;
+                    pr_dinv[d] = F.dinv[lo + q];
+#pragma unroll
+                    for (int k = 0; k < P; ++k)
+                        if (l + k * G < Lq) {
+                            pr_col[d][k] = F.col[nst + l + k * G];
+                            pr_val[d][k] = F.val[nst + l + k * G];
+                        }
+                    nst += Lq;
                 }
             }
         }
@@ -391,7 +408,7 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
             for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) a.ybuf[lo + k] = xs[k];
         return;
     }
-    // epilogue of the backward sweep: x_local[j] = x[perm_out[j]] (tail values from the buffer)
+    // epilogue of the backward sweep: x_local[j] from its backward slot (< T) or tail row (>= T)
     const int n = sd.n_local;
     auto val_at = [&](int q) -> double { return q < T ? (double)xs[q] : (double)a.ybuf[lo + q]; };
     if (a.mode == 0) {

@@ -18,12 +18,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define S2L_BS_SWEEP 1024     // threads of a sparse-sweep CTA (one CTA per subdomain)
+#define S2L_BS_SWEEP 512      // threads of a sparse-sweep CTA (one CTA per subdomain)
 #define S2L_BS_VEC 256        // threads of the vector / SpMV kernels
 #define S2L_NB_RED 592        // blocks of every kernel that produces reduction partials (4 x 148 SMs)
 #define S2L_MAX_RED_COLS 128  // columns of the reduction buffer
 #define S2L_TILE_ROWS 256     // rows of one coarse restrict/prolong tile
 #define S2L_PREFETCH 4        // rows prefetched per group in a sparse sweep
+#define S2L_PREFETCH_CHUNKS 2 // entries prefetched per lane and row (chunks of G)
 #define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {
@@ -43,15 +44,18 @@ struct DevSub {
     int64_t c_off;      // coarse offset of the subdomain (first coarse unknown)
 };
 
-// Sparse part of one factor of every subdomain, in solve order: slot p (p < T_i) of subdomain i
-// is global slot loc_off_i + p; its row id rows[slot], entries ptr[slot]..ptr[slot+1], 1/diag dinv[slot].
+// Sparse part of one factor of every subdomain.  Its rows are renumbered in solve order (slot =
+// row: a topological order, rows of one dependency level next to each other), and so are the
+// columns, so a sweep needs no row-index array.  Slot p belongs to group p % NG; the entries of a
+// group's rows are stored one row after the other, so a group finds the start of its next row by
+// adding the lengths of its previous rows, without a load from memory.
 template <typename Real>
 struct SweepFactor {
-    const int32_t* rows;
-    const int64_t* ptr;
-    const int32_t* col;
+    const int32_t* col;        // column slots, group-contiguous
     const Real* val;
-    const Real* dinv;
+    const Real* dinv;          // per slot (local space layout)
+    const uint16_t* len;       // row length per slot (local space layout)
+    const int64_t* gstart;     // first entry of group g of subdomain i: gstart[i * NG + g]
 };
 
 template <typename Real>
@@ -74,7 +78,8 @@ struct LocalSolveArgs {
     const Real* linv;          // inverse tails, row-major per subdomain
     const Real* uinv;
     const int32_t* gather;     // slot k -> index into `in` (global gather, or perm_in for a local input)
-    const int32_t* gout;       // perm_out: local j -> slot
+    const int32_t* gout;       // local j -> x position: backward slot (< T) or tail row (>= T)
+    const int32_t* u2l;        // backward slot -> forward slot (the hand-off between the two sweeps)
     const double* in;
     const double* base;        // added to the owned output (x0 of the coarse correction), may be null
     double* out;               // global output (direct mode) or local output (mode 2)

@@ -309,9 +309,9 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    binary = os.path.join(REPO, "oracle", "_ref", "s2l_ref_bench")
+    binary = os.path.join(REPO, "oracle", "_ref", "s2l_ref")
     if not os.path.exists(binary):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/s2l_ref_bench was not built "
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/s2l_ref was not built "
                                                              "(the reference compiles only where its sources are)"}))
         return
     import numpy as np

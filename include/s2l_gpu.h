@@ -123,10 +123,13 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
 
 /*
  * Layout options, before s2l_gpu_setup_end (no reference counterpart: they only choose how the
- * same factors are laid out on the device).  "tail_min"/"tail_max" (rows, default 96/4096) and
- * "tail_density" (default 0.25): the trailing block [T, n) of each factor whose strictly-lower
- * part is at least that full is solved through its dense inverse; "sweep_group" (0 = automatic,
- * 8, 16 or 32): threads per row in the sparse sweeps.
+ * same factors are laid out on the device).  Each factor is split at a tail index T: rows [0, T)
+ * are solved by the sparse sweeps, the trailing triangle [T, n) through its dense inverse.  T is
+ * chosen per subdomain to minimise 2 * hop_us * (sparse dependency levels) + bytes * nsub / bw_gbs.
+ *   "tail_min" (rows, default 64), "tail_max" (default 4096): bounds of a non-empty tail;
+ *   "tail_rows" (default 0 = cost model): force every subdomain's tail to this many rows;
+ *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
+ *   "sweep_group" (0 = automatic, 8, 16 or 32): threads per row in the sparse sweeps.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 

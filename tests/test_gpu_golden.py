@@ -27,7 +27,7 @@ def ctx():
     c.close()
 
 
-@pytest.mark.parametrize("layout", [{}, {"tail_min": 8, "tail_density": 0.05}])
+@pytest.mark.parametrize("layout", [{}, {"tail_rows": 24}, {"tail_max": 0, "sweep_group": 8}])
 @pytest.mark.parametrize("case", CASES)
 def test_gpu_reproduces_reference(ctx, case, layout):
     from s2l_b200.capi import GpuSetup

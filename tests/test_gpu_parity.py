@@ -167,10 +167,11 @@ def test_hbm_budget_refusal():
 
 LAYOUTS = [
     {},
-    {"tail_min": 8, "tail_density": 0.05},   # force dense tails on small subdomains
-    {"tail_min": 1_000_000},                 # no dense tail: the sweeps do all rows
-    {"sweep_group": 8, "tail_min": 16, "tail_density": 0.1},
+    {"tail_rows": 40},                       # force dense tails on small subdomains
+    {"tail_max": 0},                         # no dense tail: the sweeps do all rows
+    {"sweep_group": 8, "tail_rows": 17},
     {"sweep_group": 16},
+    {"sweep_group": 32, "tail_rows": 3},
 ]
 
 
@@ -183,9 +184,9 @@ def test_layouts_agree_with_oracle(ctx, rng, name, layout):
     _, st = small_setup(name)
     opts = LAYOUTS[layout]
     g = GpuSetup(ctx, st, options=opts)
-    if "tail_density" in opts:
-        assert g.stat("tail_rows") > 0
-    if opts.get("tail_min") == 1_000_000:
+    if opts.get("tail_rows"):
+        assert g.stat("tail_rows") == opts["tail_rows"] * st.nsub
+    if opts.get("tail_max") == 0:
         assert g.stat("tail_rows") == 0
     o = OracleSetup(st)
     for i, s in enumerate(st.subdomains):
@@ -199,7 +200,7 @@ def test_layouts_agree_with_oracle(ctx, rng, name, layout):
 def test_forced_tail_single_precision(ctx, rng):
     from s2l_b200.capi import GpuSetup
     w, st = small_setup("convdiff3d", precision="single")
-    g = GpuSetup(ctx, st, options={"tail_min": 8, "tail_density": 0.05})
+    g = GpuSetup(ctx, st, options={"tail_rows": 50})
     assert g.stat("tail_rows") > 0
     o = OracleSetup(st)
     for i, s in enumerate(st.subdomains):
