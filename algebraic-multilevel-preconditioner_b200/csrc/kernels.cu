@@ -266,7 +266,7 @@ __device__ __forceinline__ Real group_reduce(Real v)
 }
 
 template <typename Real, int G, bool SMEM, bool FWD>
-__global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArgs<Real> a)
+__global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolveArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_word;
@@ -358,7 +358,39 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
                         acc += pr_val[d][k] * x[c];
                     }
                 }
-                for (int e = l + P * G; e < L && !dead; e += G) {
+                // entries beyond the prefetched chunks: the next Q chunks are loaded together (their
+                // lines were hinted into L2 when the row was queued), the rest one chunk at a time
+                constexpr int Q = S2L_LATE_CHUNKS;
+                int lc[Q];
+                Real lv[Q];
+#pragma unroll
+                for (int k = 0; k < Q; ++k) {
+                    lc[k] = 0;
+                    lv[k] = Real(0);
+                    const int e = l + (P + k) * G;
+                    if (e < L) {
+                        lc[k] = F.col[pr_st[d] + e];
+                        lv[k] = F.val[pr_st[d] + e];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < Q; ++k) {
+                    if (l + (P + k) * G < L && !dead) {
+                        const int c = lc[k];
+                        int spin = 0;
+                        while (flag[c] == 0) {
+                            if (abort_flag) { dead = true; break; }
+                            if (++spin > S2L_SPIN_LIMIT) {
+                                abort_flag = 1;
+                                atomicExch(a.err, 1);
+                                dead = true;
+                                break;
+                            }
+                        }
+                        acc += lv[k] * x[c];
+                    }
+                }
+                for (int e = l + (P + Q) * G; e < L && !dead; e += G) {
                     const int c = F.col[pr_st[d] + e];
                     const Real v = F.val[pr_st[d] + e];
                     int spin = 0;
@@ -397,6 +429,12 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP) sweep_kernel(const LocalSolveArg
                             pr_col[d][k] = F.col[nst + l + k * G];
                             pr_val[d][k] = F.val[nst + l + k * G];
                         }
+                    // hint the row's later chunks into L2 (one lane per chunk, lines of 128 bytes)
+                    for (int k = P; l == 0 && k * G < Lq && k < P + S2L_LATE_CHUNKS; ++k) {
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.col + nst + k * G));
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + nst + k * G));
+                        if (sizeof(Real) * G > 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + nst + k * G + 16));
+                    }
                     nst += Lq;
                 }
             }

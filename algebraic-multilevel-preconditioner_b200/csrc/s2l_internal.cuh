@@ -25,6 +25,7 @@
 #define S2L_TILE_ROWS 256     // rows of one coarse restrict/prolong tile
 #define S2L_PREFETCH 4        // rows prefetched per group in a sparse sweep
 #define S2L_PREFETCH_CHUNKS 2 // entries prefetched per lane and row (chunks of G)
+#define S2L_LATE_CHUNKS 6     // further chunks of a row loaded together when the row is processed
 #define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {

@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--overlap", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-threads", type=int, default=0, help="reference arm: host threads (0 = all)")
+    ap.add_argument("--opt", action="append", default=[], help="device layout option key=value (s2l_gpu_setup_option)")
     return ap.parse_args()
 
 
@@ -144,8 +145,9 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     ctx = capi.Context(local)
     st32 = with_factor_precision(st, "single")
-    g64 = capi.GpuSetup(ctx, st)
-    g32 = capi.GpuSetup(ctx, st32)
+    layout = {kv.split("=")[0]: float(kv.split("=")[1]) for kv in a.opt}
+    g64 = capi.GpuSetup(ctx, st, options=layout)
+    g32 = capi.GpuSetup(ctx, st32, options=layout)
     stream = torch.cuda.current_stream(dev)
     for g in (g64, g32):
         g.set_stream(stream.cuda_stream)
@@ -255,6 +257,9 @@ def run_ours(a):
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU, all subdomains resident",
             "l2": "inputs larger than L2 (local factors %.1f GB per form)" % (head["local_solve_bytes"] / 1e9),
             "setup_s": round(setup_s, 1) if world == 1 else None,
+            "layout": {"options": layout, "tail_rows": g64.stat("tail_rows"), "sparse_nnz": g64.stat("sparse_nnz"),
+                       "coupling_nnz": g64.stat("coupling_nnz"), "dense_entries": g64.stat("dense_entries"),
+                       "sweep_group": g64.stat("sweep_group")},
         },
         "forms": {
             "mixed": {k: head[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
