@@ -1485,6 +1485,67 @@ int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind
     return finish_out(s, x0, dx, ptr_kind, s->n);
 }
 
+}  // extern "C"
+
+// Scratch of s2l_gpu_coarse_apply_noalloc: one static array per device, never allocated.  Host
+// code reaches it only through the device address looked up once per device below.
+static __device__ __align__(256) double s2l_noalloc_scratch[S2L_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+std::mutex g_noalloc_mu;
+std::vector<double*> g_noalloc_addr;  // per device, filled on the first call
+
+int noalloc_scratch(s2l_setup* s, double** out)
+{
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    const int dev = s->ctx->device;
+    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
+    if (!g_noalloc_addr[dev]) {
+        int prev = 0;
+        CUDA_OK(s, cudaGetDevice(&prev));
+        CUDA_OK(s, cudaSetDevice(dev));
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, s2l_noalloc_scratch);
+        cudaSetDevice(prev);
+        if (e != cudaSuccess)
+            return s->fail(S2L_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return S2L_OK;
+}
+}  // namespace
+
+extern "C" int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, double* x0)
+{
+    RET_IF(check_ready(s));
+    if (!r || !x0) return s->fail(S2L_ERR_BADARG, "null vector");
+    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return s->fail(S2L_ERR_STATE, "no coarse space");
+    const int boolean = s->pou == S2L_POU_BOOLEAN;
+    const int64_t need = (int64_t)s->ntiles * s->mmax + 2 * s->n0 + (boolean ? 0 : s->nloc);
+    if (need > S2L_NOALLOC_SCRATCH_DOUBLES)
+        return s->fail(S2L_ERR_BADARG, "coarse_apply_noalloc: this setup needs " + std::to_string(need) +
+                                           " doubles of scratch; the static no-alloc scratch holds " +
+                                           std::to_string(S2L_NOALLOC_SCRATCH_DOUBLES));
+    double* scr = nullptr;
+    RET_IF(noalloc_scratch(s, &scr));
+    double* part = scr;
+    double* c = part + (int64_t)s->ntiles * s->mmax;
+    double* y = c + s->n0;
+    double* plocal = y + s->n0;
+    launch_coarse_restrict(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+                           boolean, r, s->mmax, part);
+    launch_coarse_reduce(s->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
+    launch_dense_gemv(s->stream, (int)s->n0, s->d_Einv, c, y);
+    launch_coarse_prolong(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
+                          plocal);
+    if (!boolean) launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
+    CUDA_OK(s, cudaGetLastError());
+    return S2L_OK;
+}
+
+extern "C" {
+
 int s2l_gpu_one_level_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
 {
     RET_IF(check_ready(s));

@@ -30,7 +30,7 @@ EXPORTED = [
     "s2l_gpu_setup_bytes", "s2l_gpu_spmv", "s2l_gpu_local_solve", "s2l_gpu_coarse_apply",
     "s2l_gpu_one_level_apply", "s2l_gpu_apply", "s2l_gpu_gmres", "s2l_gpu_bicgstab", "s2l_gpu_set_stream",
     "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes", "s2l_gpu_setup_option",
-    "s2l_gpu_setup_stat",
+    "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc",
 ]
 
 
@@ -91,6 +91,7 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_local_solve_bytes": ([vp, dp], C.c_int),
         "s2l_gpu_setup_option": ([vp, C.c_char_p, C.c_double], C.c_int),
         "s2l_gpu_setup_stat": ([vp, C.c_char_p, dp], C.c_int),
+        "s2l_gpu_coarse_apply_noalloc": ([vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -232,6 +233,11 @@ class GpuSetup:
 
     def coarse_apply(self, r, out=None):
         return self._call2(self.lib.s2l_gpu_coarse_apply, r, self.n, self.n, out)
+
+    def coarse_apply_noalloc(self, r_dev: int, x0_dev: int):
+        """x0 = R0^T E^-1 R0 r with the library's static scratch (device pointers, enqueued on the
+        setup's stream; the caller synchronizes)."""
+        self.ctx.check(self.lib.s2l_gpu_coarse_apply_noalloc(self.h, C.c_void_p(r_dev), C.c_void_p(x0_dev)))
 
     def one_level_apply(self, r, out=None):
         return self._call2(self.lib.s2l_gpu_one_level_apply, r, self.n, self.n, out)

@@ -149,6 +149,29 @@ int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind
 int s2l_gpu_one_level_apply(s2l_setup* s, const double* r, double* z, int ptr_kind);
 int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind);
 
+/*
+ * The coarse correction x0 = R0^T E^-1 R0 r of s2l_gpu_coarse_apply, for callers that cannot
+ * allocate device memory when they call it: code that hands all device memory to its own pool
+ * or allocator (a framework's caching allocator, a memory-capped serving process), or that must
+ * not allocate once its solve loop runs.  No counterpart in the reference (it has no device).
+ *
+ * It allocates nothing and uses none of the setup's scratch buffers: the restriction partials and
+ * the two coarse vectors live in one static device array of S2L_NOALLOC_SCRATCH_DOUBLES doubles
+ * (2 MiB), which every GPU that loads this library holds until the process exits.  A setup needs
+ * (coarse tiles x largest m) + 2 n0 doubles of it, plus the local-space size for the multiplicity
+ * partition of unity; a setup that needs more is rejected with S2L_ERR_BADARG before any launch.
+ * r and x0 are device pointers (n doubles each).  The kernels are enqueued on the setup's stream
+ * and the call returns; x0 is ready once that stream is synchronized.
+ *
+ * The first call on a device looks up the device address of the static array (with that device
+ * current): make that first call before any stream capture on the device.  Every call shares the
+ * one array and leaves its contents behind; every scratch element a call reads is written earlier
+ * in the same call, so nothing needs clearing, but calls that overlap on the GPU (other streams,
+ * other setups on the same device) race on it.
+ */
+#define S2L_NOALLOC_SCRATCH_DOUBLES 262144
+int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, double* x0);
+
 int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
                   s2l_result* result);
 int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
