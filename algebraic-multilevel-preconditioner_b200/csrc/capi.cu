@@ -79,6 +79,8 @@ struct Sweep {
 
 }  // namespace
 
+struct s2l_work;
+
 struct s2l_setup {
     s2l_ctx* ctx = nullptr;
     int64_t n = 0;
@@ -86,8 +88,7 @@ struct s2l_setup {
     int one_level = 0, coarse = 0, pou = 0;
     int real = -1;
     bool ended = false;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t setup_stream = nullptr;  // uploads and the tail inversion
 
     // host staging
     HostCsr A;
@@ -98,7 +99,7 @@ struct s2l_setup {
     std::vector<double> E;
     bool have_coarse = false;
 
-    // device memory
+    // device memory (read-only after setup_end)
     std::vector<void*> allocs;
     size_t bytes = 0;
     int32_t *d_rp = nullptr, *d_ci = nullptr;
@@ -108,6 +109,7 @@ struct s2l_setup {
     std::vector<DevSub> h_subs;
     DevSub* d_subs = nullptr;
     int64_t nloc = 0;
+    int max_nl = 0;
     uint16_t* d_len[2] = {nullptr, nullptr};
     int64_t* d_gstart[2] = {nullptr, nullptr};
     int32_t* d_col[2] = {nullptr, nullptr};
@@ -121,9 +123,7 @@ struct s2l_setup {
     int64_t* d_ust_ptr = nullptr;
     void* d_ust_val = nullptr;
     void *d_linv = nullptr, *d_uinv = nullptr;
-    void *d_ybuf = nullptr, *d_xbuf = nullptr;
-    uint8_t* d_gflags = nullptr;
-    int* d_err = nullptr;
+    bool need_gflags = false;
     std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
@@ -142,34 +142,14 @@ struct s2l_setup {
     int32_t *d_t_sub = nullptr, *d_t_row0 = nullptr, *d_t_nrow = nullptr, *d_t_first = nullptr;
     int ntiles = 0, mmax = 0;
     double* d_Einv = nullptr;
-    double* d_cpart = nullptr;
-    double *d_c = nullptr, *d_y = nullptr;
-    // work vectors
-    double *d_ylocal = nullptr, *d_x0 = nullptr, *d_w = nullptr, *d_in = nullptr, *d_out = nullptr;
-    double* d_plocal = nullptr;
-    double* d_part = nullptr;
-    double* d_red = nullptr;
-    double* h_red = nullptr;
     size_t smem_bytes = 0;
     double solve_bytes = 0.0;
-    // Krylov work (lazy)
-    int kr_m = -1;
-    bool kr_flex = false;
-    double *d_V_kr = nullptr, *d_Z_kr = nullptr, *d_r = nullptr, *d_z = nullptr, *d_kw = nullptr, *d_b = nullptr,
-           *d_xk = nullptr, *d_u = nullptr;
-    double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
-    double* d_coef = nullptr;
-    // profiling
-    unsigned prof = 0;  // bit c: time kernel class c
-    long launches = 0;  // kernel launches issued by this setup
-    struct Ev {
-        int cls;
-        cudaEvent_t a, b;
-    };
-    std::vector<Ev> evs;
-    std::vector<cudaEvent_t> pool;
-    double acc_ms[PC_N] = {0, 0, 0, 0, 0};
-    long acc_n[PC_N] = {0, 0, 0, 0, 0};
+    // workspaces: one per concurrent solve-phase call (workspace 0 is the caller's default)
+    mutable std::mutex wmu;
+    std::vector<s2l_work*> works;
+    std::vector<char> busy;
+    cudaStream_t user_stream = nullptr;  // s2l_gpu_set_stream: used by workspace 0
+    unsigned prof_mask = 0;              // s2l_gpu_profile_enable: inherited by new workspaces
 
     int fail(int code, const std::string& msg)
     {
@@ -179,6 +159,47 @@ struct s2l_setup {
         }
         return code;
     }
+};
+
+// Work state of one solve-phase call: its stream, work vectors, Krylov basis, reduction buffers,
+// error word and kernel timers.  The setup's data is only read.
+struct s2l_work {
+    s2l_setup* s = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;  // orders this workspace's stream after the caller's stream
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    void *d_ybuf = nullptr, *d_xbuf = nullptr;
+    uint8_t* d_gflags = nullptr;
+    int* d_err = nullptr;
+    double* d_cpart = nullptr;
+    double *d_c = nullptr, *d_y = nullptr;
+    double *d_ylocal = nullptr, *d_x0 = nullptr, *d_w = nullptr, *d_in = nullptr, *d_out = nullptr;
+    double* d_plocal = nullptr;
+    double* d_part = nullptr;
+    double* d_red = nullptr;
+    double* h_red = nullptr;
+    // Krylov work (lazy)
+    int kr_m = -1;
+    bool kr_flex = false;
+    double *d_V_kr = nullptr, *d_Z_kr = nullptr, *d_r = nullptr, *d_z = nullptr, *d_kw = nullptr, *d_b = nullptr,
+           *d_xk = nullptr, *d_u = nullptr;
+    double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
+    double* d_coef = nullptr;
+    // profiling
+    unsigned prof = 0;  // bit c: time kernel class c
+    long launches = 0;  // kernel launches issued through this workspace
+    struct Ev {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Ev> evs;
+    std::vector<cudaEvent_t> pool;
+    double acc_ms[PC_N] = {0, 0, 0, 0, 0};
+    long acc_n[PC_N] = {0, 0, 0, 0, 0};
+
+    int fail(int code, const std::string& msg) { return s->fail(code, msg); }
 };
 
 #define CUDA_OK(s, call)                                                                                             \
@@ -195,7 +216,7 @@ struct s2l_setup {
 
 namespace {
 
-int check_err(s2l_setup* s);
+int check_err(s2l_work* w);
 
 int dev_alloc(s2l_setup* s, void** p, size_t bytes)
 {
@@ -226,7 +247,7 @@ template <typename T>
 int upload(s2l_setup* s, T** dst, const T* src, size_t count)
 {
     RET_IF(dev_alloc(s, reinterpret_cast<void**>(dst), count * sizeof(T)));
-    if (count) CUDA_OK(s, cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+    if (count) CUDA_OK(s, cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s->setup_stream));
     return S2L_OK;
 }
 
@@ -234,11 +255,6 @@ template <typename T>
 int upload(s2l_setup* s, T** dst, const std::vector<T>& v)
 {
     return upload(s, dst, v.data(), v.size());
-}
-
-int alloc_doubles(s2l_setup* s, double** p, size_t count)
-{
-    return dev_alloc(s, reinterpret_cast<void**>(p), count * sizeof(double));
 }
 
 // Dependency levels of the rows [0, T) of a triangular factor (lower: forward, entries c < r;
@@ -460,62 +476,106 @@ int upload_real(s2l_setup* s, void** dst, const std::vector<double>& v)
 }
 
 // ------------------------------------------------------------------------------ profiling
-void prof_begin(s2l_setup* s, int cls, cudaEvent_t* a)
+int check_ready(s2l_setup* s)
 {
-    if (!(s->prof & (1u << cls))) return;
-    if (s->pool.empty()) {
+    if (!s) return S2L_ERR_BADARG;
+    if (!s->ended) return s->fail(S2L_ERR_STATE, "setup_end() was not called");
+    return S2L_OK;
+}
+
+int work_alloc(s2l_work* w, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    s2l_ctx* c = w->s->ctx;
+    {
+        std::lock_guard<std::mutex> g(c->mu);
+        if (c->budget && c->used + bytes > c->budget) {
+            c->err = "HBM budget exceeded: need " + std::to_string(c->used + bytes) + " of " + std::to_string(c->budget) +
+                     " bytes";
+            return S2L_ERR_OOM;
+        }
+        c->used += bytes;
+    }
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(c->mu);
+        c->used -= bytes;
+        c->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return S2L_ERR_OOM;
+    }
+    w->allocs.push_back(*p);
+    w->bytes += bytes;
+    return S2L_OK;
+}
+
+int work_doubles(s2l_work* w, double** p, size_t count)
+{
+    return work_alloc(w, reinterpret_cast<void**>(p), count * sizeof(double));
+}
+
+void prof_begin(s2l_work* w, int cls, cudaEvent_t* a)
+{
+    if (!(w->prof & (1u << cls))) return;
+    if (w->pool.empty()) {
         cudaEvent_t e;
         cudaEventCreate(&e);
-        s->pool.push_back(e);
+        w->pool.push_back(e);
     }
-    *a = s->pool.back();
-    s->pool.pop_back();
-    cudaEventRecord(*a, s->stream);
+    *a = w->pool.back();
+    w->pool.pop_back();
+    cudaEventRecord(*a, w->stream);
     (void)cls;
 }
 
-void prof_end(s2l_setup* s, int cls, cudaEvent_t a)
+void prof_end(s2l_work* w, int cls, cudaEvent_t a)
 {
-    if (!(s->prof & (1u << cls))) return;
-    if (s->pool.empty()) {
+    s2l_setup* s = w->s;
+    (void)s;
+    if (!(w->prof & (1u << cls))) return;
+    if (w->pool.empty()) {
         cudaEvent_t e;
         cudaEventCreate(&e);
-        s->pool.push_back(e);
+        w->pool.push_back(e);
     }
-    cudaEvent_t b = s->pool.back();
-    s->pool.pop_back();
-    cudaEventRecord(b, s->stream);
-    s->evs.push_back({cls, a, b});
+    cudaEvent_t b = w->pool.back();
+    w->pool.pop_back();
+    cudaEventRecord(b, w->stream);
+    w->evs.push_back({cls, a, b});
 }
 
-void prof_drain(s2l_setup* s)
+void prof_drain(s2l_work* w)
 {
-    if (s->evs.empty()) return;
-    cudaStreamSynchronize(s->stream);
-    for (auto& e : s->evs) {
+    s2l_setup* s = w->s;
+    (void)s;
+    if (w->evs.empty()) return;
+    cudaStreamSynchronize(w->stream);
+    for (auto& e : w->evs) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
-            s->acc_ms[e.cls] += ms;
-            s->acc_n[e.cls] += 1;
+            w->acc_ms[e.cls] += ms;
+            w->acc_n[e.cls] += 1;
         }
-        s->pool.push_back(e.a);
-        s->pool.push_back(e.b);
+        w->pool.push_back(e.a);
+        w->pool.push_back(e.b);
     }
-    s->evs.clear();
+    w->evs.clear();
 }
 
 struct Prof {
-    s2l_setup* s;
+    s2l_work* w;
     int cls;
     cudaEvent_t a{};
-    Prof(s2l_setup* s_, int c) : s(s_), cls(c) { prof_begin(s, cls, &a); }
-    ~Prof() { prof_end(s, cls, a); }
+    Prof(s2l_work* w_, int c) : w(w_), cls(c) { prof_begin(w, cls, &a); }
+    ~Prof() { prof_end(w, cls, a); }
 };
 
 // ------------------------------------------------------------------------------ solve-phase pieces
 template <typename Real>
-LocalSolveArgs<Real> solve_args(s2l_setup* s)
+LocalSolveArgs<Real> solve_args(s2l_work* w)
 {
+    s2l_setup* s = w->s;
+    (void)s;
     LocalSolveArgs<Real> a{};
     a.subs = s->d_subs;
     for (int f = 0; f < 2; ++f)
@@ -534,27 +594,29 @@ LocalSolveArgs<Real> solve_args(s2l_setup* s)
     a.linv = (const Real*)s->d_linv;
     a.uinv = (const Real*)s->d_uinv;
     a.gout = s->d_gout;
-    a.ylocal = s->d_ylocal;
-    a.ybuf = (Real*)s->d_ybuf;
-    a.xbuf = (Real*)s->d_xbuf;
-    a.gflags = s->d_gflags;
-    a.err = s->d_err;
+    a.ylocal = w->d_ylocal;
+    a.ybuf = (Real*)w->d_ybuf;
+    a.xbuf = (Real*)w->d_xbuf;
+    a.gflags = w->d_gflags;
+    a.err = w->d_err;
     return a;
 }
 
 // Local solves of every subdomain (only_sub < 0) or of one: in -> (mode 0) out[owned] (+ base),
 // (mode 1) ylocal, (mode 2: local input/output of subdomain only_sub) out.
-int run_local_solve(s2l_setup* s, const double* in, const double* base, double* out, int mode, int only_sub,
+int run_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
                     const double* local_in)
 {
-    Prof pr(s, PC_SOLVE);
+    s2l_setup* s = w->s;
+    (void)s;
+    Prof pr(w, PC_SOLVE);
     const int nb = only_sub >= 0 ? 1 : s->nsub;
     int32_t* sub_list = nullptr;
     int tr0 = 0, trn = s->tr_first_h[s->nsub], us0 = 0, usn = s->us_first_h[s->nsub];
     if (only_sub >= 0) {
-        sub_list = reinterpret_cast<int32_t*>(s->d_red + 500);  // scratch slot for one index
+        sub_list = reinterpret_cast<int32_t*>(w->d_red + 500);  // scratch slot for one index
         int32_t v = only_sub;
-        CUDA_OK(s, cudaMemcpyAsync(sub_list, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+        CUDA_OK(w, cudaMemcpyAsync(sub_list, &v, sizeof(v), cudaMemcpyHostToDevice, w->stream));
         tr0 = s->tr_first_h[only_sub];
         trn = s->tr_first_h[only_sub + 1] - tr0;
         us0 = s->us_first_h[only_sub];
@@ -562,146 +624,157 @@ int run_local_solve(s2l_setup* s, const double* in, const double* base, double* 
     }
     cudaError_t e;
     int launched = 0;
-    const size_t smem = s->d_gflags ? 0 : s->smem_bytes;
+    const size_t smem = w->d_gflags ? 0 : s->smem_bytes;
     if (s->real == S2L_REAL_F32) {
-        LocalSolveArgs<float> a = solve_args<float>(s);
+        LocalSolveArgs<float> a = solve_args<float>(w);
         a.sub_list = sub_list;
         a.gather = mode == 2 ? s->d_pin : s->d_gin;
         a.in = mode == 2 ? local_in : in;
         a.base = base;
         a.out = out;
         a.mode = mode;
-        e = launch_local_solve<float>(s->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
+        e = launch_local_solve<float>(w->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
     } else {
-        LocalSolveArgs<double> a = solve_args<double>(s);
+        LocalSolveArgs<double> a = solve_args<double>(w);
         a.sub_list = sub_list;
         a.gather = mode == 2 ? s->d_pin : s->d_gin;
         a.in = mode == 2 ? local_in : in;
         a.base = base;
         a.out = out;
         a.mode = mode;
-        e = launch_local_solve<double>(s->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
+        e = launch_local_solve<double>(w->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
     }
-    s->launches += launched;
-    if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
+    w->launches += launched;
+    if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
     return S2L_OK;
 }
 
 // z = M1^-1 in (+ base), M1 = RAS or ASM
-int one_level(s2l_setup* s, const double* in, const double* base, double* out)
+int one_level(s2l_work* w, const double* in, const double* base, double* out)
 {
-    if (s->pou == S2L_POU_BOOLEAN && s->one_level == S2L_ONE_LEVEL_RAS) return run_local_solve(s, in, base, out, 0, -1, nullptr);
-    RET_IF(run_local_solve(s, in, nullptr, nullptr, 1, -1, nullptr));
-    Prof pr(s, PC_COMBINE);
-    launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, s->one_level == S2L_ONE_LEVEL_RAS ? s->d_cp_w : nullptr,
-                   s->d_ylocal, base, out);
-    s->launches += 1;
+    s2l_setup* s = w->s;
+    (void)s;
+    if (s->pou == S2L_POU_BOOLEAN && s->one_level == S2L_ONE_LEVEL_RAS) return run_local_solve(w, in, base, out, 0, -1, nullptr);
+    RET_IF(run_local_solve(w, in, nullptr, nullptr, 1, -1, nullptr));
+    Prof pr(w, PC_COMBINE);
+    launch_combine(w->stream, s->n, s->d_cp_ptr, s->d_cp_pos, s->one_level == S2L_ONE_LEVEL_RAS ? s->d_cp_w : nullptr,
+                   w->d_ylocal, base, out);
+    w->launches += 1;
     return S2L_OK;
 }
 
 // x0 = R0^T E^-1 R0 r
-int coarse_apply(s2l_setup* s, const double* r, double* x0)
+int coarse_apply(s2l_work* w, const double* r, double* x0)
 {
-    Prof pr(s, PC_COARSE);
+    s2l_setup* s = w->s;
+    (void)s;
+    Prof pr(w, PC_COARSE);
     const int boolean = s->pou == S2L_POU_BOOLEAN;
-    launch_coarse_restrict(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
-                           boolean, r, s->mmax, s->d_cpart);
-    launch_coarse_reduce(s->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, s->d_cpart, s->d_c);
-    launch_dense_gemv(s->stream, (int)s->n0, s->d_Einv, s->d_c, s->d_y);
-    launch_coarse_prolong(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
-                          s->d_y, x0, s->d_plocal);
-    if (!boolean) launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, s->d_plocal, nullptr, x0);
-    s->launches += boolean ? 4 : 5;
+    launch_coarse_restrict(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+                           boolean, r, s->mmax, w->d_cpart);
+    launch_coarse_reduce(w->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, w->d_cpart, w->d_c);
+    launch_dense_gemv(w->stream, (int)s->n0, s->d_Einv, w->d_c, w->d_y);
+    launch_coarse_prolong(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
+                          w->d_y, x0, w->d_plocal);
+    if (!boolean) launch_combine(w->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, w->d_plocal, nullptr, x0);
+    w->launches += boolean ? 4 : 5;
     return S2L_OK;
 }
 
-int spmv_dev(s2l_setup* s, const double* x, double* y, const double* b, bool with_norm)
+int spmv_dev(s2l_work* w, const double* x, double* y, const double* b, bool with_norm)
 {
-    Prof pr(s, PC_SPMV);
-    launch_spmv(s->stream, s->n, s->d_rp, s->d_ci, s->d_av, x, y, b, with_norm ? s->d_part : nullptr,
-                s->d_red + 256, s->tpr);
-    s->launches += with_norm ? 2 : 1;
+    s2l_setup* s = w->s;
+    (void)s;
+    Prof pr(w, PC_SPMV);
+    launch_spmv(w->stream, s->n, s->d_rp, s->d_ci, s->d_av, x, y, b, with_norm ? w->d_part : nullptr,
+                w->d_red + 256, s->tpr);
+    w->launches += with_norm ? 2 : 1;
     return S2L_OK;
 }
 
 // z = M^-1 r (two-level Schwarz, src/preconditioner/two_level_schwarz.cpp:134-163); r and z distinct
-int apply_dev(s2l_setup* s, const double* r, double* z)
+int apply_dev(s2l_work* w, const double* r, double* z)
 {
-    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return one_level(s, r, nullptr, z);
-    RET_IF(coarse_apply(s, r, s->d_x0));
-    if (s->coarse == S2L_COARSE_ADDITIVE) return one_level(s, r, s->d_x0, z);
-    RET_IF(spmv_dev(s, s->d_x0, s->d_w, r, false));  // w = r - A x0
-    return one_level(s, s->d_w, s->d_x0, z);
+    s2l_setup* s = w->s;
+    (void)s;
+    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return one_level(w, r, nullptr, z);
+    RET_IF(coarse_apply(w, r, w->d_x0));
+    if (s->coarse == S2L_COARSE_ADDITIVE) return one_level(w, r, w->d_x0, z);
+    RET_IF(spmv_dev(w, w->d_x0, w->d_w, r, false));  // w = r - A x0
+    return one_level(w, w->d_w, w->d_x0, z);
 }
 
-int check_ready(s2l_setup* s)
-{
-    if (!s) return S2L_ERR_BADARG;
-    if (!s->ended) return s->fail(S2L_ERR_STATE, "setup_end() was not called");
-    return S2L_OK;
-}
 
 // host/device staging of a global vector argument
-int stage_in(s2l_setup* s, const double* p, int kind, int64_t count, double* tmp, const double** dev)
+int stage_in(s2l_work* w, const double* p, int kind, int64_t count, double* tmp, const double** dev)
 {
+    s2l_setup* s = w->s;
+    (void)s;
     if (kind == S2L_PTR_DEVICE) {
         *dev = p;
         return S2L_OK;
     }
-    if (kind != S2L_PTR_HOST) return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
-    CUDA_OK(s, cudaMemcpyAsync(tmp, p, count * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    if (kind != S2L_PTR_HOST) return w->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    CUDA_OK(w, cudaMemcpyAsync(tmp, p, count * sizeof(double), cudaMemcpyHostToDevice, w->stream));
     *dev = tmp;
     return S2L_OK;
 }
 
-int finish_out(s2l_setup* s, double* dst, const double* dev, int kind, int64_t count)
+int finish_out(s2l_work* w, double* dst, const double* dev, int kind, int64_t count)
 {
+    s2l_setup* s = w->s;
+    (void)s;
     if (kind == S2L_PTR_HOST)
-        CUDA_OK(s, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_OK(w, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
     else if (dst != dev)
-        CUDA_OK(s, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-    CUDA_OK(s, cudaStreamSynchronize(s->stream));
-    CUDA_OK(s, cudaGetLastError());
-    return check_err(s);
+        CUDA_OK(w, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_OK(w, cudaStreamSynchronize(w->stream));
+    CUDA_OK(w, cudaGetLastError());
+    return check_err(w);
 }
 
-int ensure_krylov(s2l_setup* s, int m, bool flexible)
+int ensure_krylov(s2l_work* w, int m, bool flexible)
 {
-    if (s->kr_m >= m && (!flexible || s->kr_flex)) return S2L_OK;
-    if (m + 1 > S2L_MAX_RED_COLS - 1) return s->fail(S2L_ERR_BADARG, "restart too large (max 120)");
+    s2l_setup* s = w->s;
+    (void)s;
+    if (w->kr_m >= m && (!flexible || w->kr_flex)) return S2L_OK;
+    if (m + 1 > S2L_MAX_RED_COLS - 1) return w->fail(S2L_ERR_BADARG, "restart too large (max 120)");
     const size_t n = (size_t)s->n;
-    RET_IF(alloc_doubles(s, &s->d_V_kr, n * (m + 1)));
-    if (flexible) RET_IF(alloc_doubles(s, &s->d_Z_kr, n * m));
-    if (s->kr_m < 0) {
-        RET_IF(alloc_doubles(s, &s->d_r, n));
-        RET_IF(alloc_doubles(s, &s->d_z, n));
-        RET_IF(alloc_doubles(s, &s->d_kw, n));
-        RET_IF(alloc_doubles(s, &s->d_b, n));
-        RET_IF(alloc_doubles(s, &s->d_xk, n));
-        RET_IF(alloc_doubles(s, &s->d_u, n));
-        RET_IF(alloc_doubles(s, &s->d_coef, S2L_MAX_RED_COLS));
+    RET_IF(work_doubles(w, &w->d_V_kr, n * (m + 1)));
+    if (flexible) RET_IF(work_doubles(w, &w->d_Z_kr, n * m));
+    if (w->kr_m < 0) {
+        RET_IF(work_doubles(w, &w->d_r, n));
+        RET_IF(work_doubles(w, &w->d_z, n));
+        RET_IF(work_doubles(w, &w->d_kw, n));
+        RET_IF(work_doubles(w, &w->d_b, n));
+        RET_IF(work_doubles(w, &w->d_xk, n));
+        RET_IF(work_doubles(w, &w->d_u, n));
+        RET_IF(work_doubles(w, &w->d_coef, S2L_MAX_RED_COLS));
     }
-    s->kr_m = m;
-    s->kr_flex = s->kr_flex || flexible;
+    w->kr_m = m;
+    w->kr_flex = w->kr_flex || flexible;
     return S2L_OK;
 }
 
-int read_red(s2l_setup* s, int off, int count)
+int read_red(s2l_work* w, int off, int count)
 {
-    CUDA_OK(s, cudaMemcpyAsync(s->h_red + off, s->d_red + off, count * sizeof(double), cudaMemcpyDeviceToHost,
-                               s->stream));
-    return check_err(s);
+    s2l_setup* s = w->s;
+    (void)s;
+    CUDA_OK(w, cudaMemcpyAsync(w->h_red + off, w->d_red + off, count * sizeof(double), cudaMemcpyDeviceToHost,
+                               w->stream));
+    return check_err(w);
 }
 
-int norm2_dev(s2l_setup* s, const double* x, double* out_host)
+int norm2_dev(s2l_work* w, const double* x, double* out_host)
 {
+    s2l_setup* s = w->s;
     {
-        Prof pr(s, PC_VEC);
-        launch_dot2(s->stream, s->n, x, x, nullptr, s->d_part, s->d_red + 256);
-        s->launches += 2;
+        Prof pr(w, PC_VEC);
+        launch_dot2(w->stream, s->n, x, x, nullptr, w->d_part, w->d_red + 256);
+        w->launches += 2;
     }
-    RET_IF(read_red(s, 256, 1));
-    *out_host = std::sqrt(s->h_red[256]);
+    RET_IF(read_red(w, 256, 1));
+    *out_host = std::sqrt(w->h_red[256]);
     return S2L_OK;
 }
 
@@ -724,7 +797,7 @@ int invert_tails(s2l_setup* s, const std::vector<std::vector<double>>& Ltt, cons
     cublasHandle_t hb = nullptr;
     int rc = S2L_OK;
     if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) rc = s->fail(S2L_ERR_CUDA, "cublasCreate failed");
-    if (rc == S2L_OK) cublasSetStream(hb, s->stream);
+    if (rc == S2L_OK) cublasSetStream(hb, s->setup_stream);
     std::vector<double> eye;
     for (size_t i = 0; i < Ltt.size() && rc == S2L_OK; ++i) {
         if (Ltt[i].empty()) continue;
@@ -734,8 +807,8 @@ int invert_tails(s2l_setup* s, const std::vector<std::vector<double>>& Ltt, cons
         const double one = 1.0;
         for (int f = 0; f < 2 && rc == S2L_OK; ++f) {
             const std::vector<double>& M = f == 0 ? Ltt[i] : Utt[i];
-            if (cudaMemcpyAsync(dA, M.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
-                cudaMemcpyAsync(dB, eye.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+            if (cudaMemcpyAsync(dA, M.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->setup_stream) != cudaSuccess ||
+                cudaMemcpyAsync(dB, eye.data(), (size_t)sz * sz * sizeof(double), cudaMemcpyHostToDevice, s->setup_stream) != cudaSuccess) {
                 rc = s->fail(S2L_ERR_CUDA, "tail upload failed");
                 break;
             }
@@ -748,13 +821,13 @@ int invert_tails(s2l_setup* s, const std::vector<std::vector<double>>& Ltt, cons
             }
             void* dst = f == 0 ? s->d_linv : s->d_uinv;
             if (s->real == S2L_REAL_F32) {
-                launch_to_float(s->stream, dB, (float*)dst + d_off[i], (int64_t)sz * sz);
+                launch_to_float(s->setup_stream, dB, (float*)dst + d_off[i], (int64_t)sz * sz);
             } else if (cudaMemcpyAsync((double*)dst + d_off[i], dB, (size_t)sz * sz * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess) {
+                                       cudaMemcpyDeviceToDevice, s->setup_stream) != cudaSuccess) {
                 rc = s->fail(S2L_ERR_CUDA, "tail copy failed");
             }
             // the host copies of M and eye are reused: finish before the next upload
-            if (cudaStreamSynchronize(s->stream) != cudaSuccess) rc = s->fail(S2L_ERR_CUDA, "tail inversion failed");
+            if (cudaStreamSynchronize(s->setup_stream) != cudaSuccess) rc = s->fail(S2L_ERR_CUDA, "tail inversion failed");
         }
     }
     if (hb) cublasDestroy(hb);
@@ -764,17 +837,140 @@ int invert_tails(s2l_setup* s, const std::vector<std::vector<double>>& Ltt, cons
 }
 
 // error word of the sweeps: a bounded wait gave up
-int check_err(s2l_setup* s)
+int check_err(s2l_work* w)
 {
     int e = 0;
-    CUDA_OK(s, cudaMemcpyAsync(&e, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    CUDA_OK(w, cudaMemcpyAsync(&e, w->d_err, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+    CUDA_OK(w, cudaStreamSynchronize(w->stream));
     if (e) {
-        CUDA_OK(s, cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
-        return s->fail(S2L_ERR_TIMEOUT, "a sparse sweep gave up waiting for a row (bounded wait exceeded)");
+        CUDA_OK(w, cudaMemsetAsync(w->d_err, 0, sizeof(int), w->stream));
+        return w->fail(S2L_ERR_TIMEOUT, "a sparse sweep gave up waiting for a row (bounded wait exceeded)");
     }
     return S2L_OK;
 }
+
+// ------------------------------------------------------------------------------ workspaces
+int work_create(s2l_setup* s, s2l_work** out)
+{
+    *out = nullptr;
+    auto* w = new s2l_work;
+    w->s = s;
+    if (cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete w;
+        return s->fail(S2L_ERR_CUDA, "cannot create a stream");
+    }
+    w->stream = w->own_stream;
+    w->prof = s->prof_mask;
+    if (cudaEventCreateWithFlags(&w->join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(w->own_stream);
+        delete w;
+        return s->fail(S2L_ERR_CUDA, "cannot create an event");
+    }
+    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    const int64_t loc = std::max<int64_t>(s->nloc, 1);
+    int rc = S2L_OK;
+    auto A = [&](void** p, size_t b) {
+        if (rc == S2L_OK) rc = work_alloc(w, p, b);
+    };
+    A(&w->d_ybuf, (size_t)loc * rs);
+    A(&w->d_xbuf, (size_t)loc * rs);
+    A(reinterpret_cast<void**>(&w->d_err), 16);
+    if (s->need_gflags) A(reinterpret_cast<void**>(&w->d_gflags), (size_t)loc);
+    if (s->ntiles > 0) {
+        A(reinterpret_cast<void**>(&w->d_cpart), (size_t)s->ntiles * s->mmax * sizeof(double));
+        A(reinterpret_cast<void**>(&w->d_c), (size_t)std::max<int64_t>(s->n0, 1) * sizeof(double));
+        A(reinterpret_cast<void**>(&w->d_y), (size_t)std::max<int64_t>(s->n0, 1) * sizeof(double));
+    }
+    A(reinterpret_cast<void**>(&w->d_ylocal), (size_t)loc * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_plocal), (size_t)loc * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_x0), (size_t)s->n * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_w), (size_t)s->n * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_in), (size_t)std::max<int64_t>(s->n, s->max_nl) * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_out), (size_t)std::max<int64_t>(s->n, s->max_nl) * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_part), (size_t)S2L_NB_RED * S2L_MAX_RED_COLS * sizeof(double));
+    A(reinterpret_cast<void**>(&w->d_red), 512 * sizeof(double));
+    if (rc == S2L_OK && cudaMallocHost(&w->h_red, 512 * sizeof(double)) != cudaSuccess)
+        rc = s->fail(S2L_ERR_OOM, "cannot allocate pinned host memory");
+    if (rc == S2L_OK && cudaMemsetAsync(w->d_err, 0, 16, w->stream) != cudaSuccess) rc = S2L_ERR_CUDA;
+    if (rc == S2L_OK && cudaStreamSynchronize(w->stream) != cudaSuccess) rc = S2L_ERR_CUDA;
+    if (rc != S2L_OK) {
+        for (void* p : w->allocs) cudaFree(p);
+        {
+            std::lock_guard<std::mutex> g(s->ctx->mu);
+            s->ctx->used -= std::min(s->ctx->used, w->bytes);
+        }
+        if (w->h_red) cudaFreeHost(w->h_red);
+        cudaEventDestroy(w->join);
+        cudaStreamDestroy(w->own_stream);
+        delete w;
+        return rc;
+    }
+    *out = w;
+    return S2L_OK;
+}
+
+void work_destroy(s2l_work* w)
+{
+    if (!w) return;
+    cudaStreamSynchronize(w->stream);
+    cudaStreamSynchronize(w->own_stream);
+    prof_drain(w);
+    for (void* p : w->allocs) cudaFree(p);
+    {
+        std::lock_guard<std::mutex> g(w->s->ctx->mu);
+        w->s->ctx->used -= std::min(w->s->ctx->used, w->bytes);
+    }
+    if (w->h_red) cudaFreeHost(w->h_red);
+    for (auto e : w->pool) cudaEventDestroy(e);
+    cudaEventDestroy(w->join);
+    cudaStreamDestroy(w->own_stream);
+    delete w;
+}
+
+// A free workspace for one solve-phase call: workspace 0 when it is free (it carries the caller's
+// stream and timers), another free one, or a new one when every workspace is busy (concurrent
+// calls on one setup from several threads).
+struct Lease {
+    s2l_setup* s;
+    s2l_work* w = nullptr;
+    int idx = -1;
+    int rc = S2L_OK;
+    explicit Lease(s2l_setup* s_) : s(s_)
+    {
+        std::lock_guard<std::mutex> g(s->wmu);
+        for (size_t i = 0; i < s->works.size(); ++i)
+            if (!s->busy[i]) {
+                idx = (int)i;
+                break;
+            }
+        if (idx < 0) {
+            s2l_work* nw = nullptr;
+            rc = work_create(s, &nw);
+            if (rc != S2L_OK) return;
+            s->works.push_back(nw);
+            s->busy.push_back(0);
+            idx = (int)s->works.size() - 1;
+        }
+        s->busy[idx] = 1;
+        w = s->works[idx];
+        if (cudaSetDevice(s->ctx->device) != cudaSuccess) {
+            rc = s->fail(S2L_ERR_CUDA, "cudaSetDevice failed");
+            return;
+        }
+        // another workspace's stream starts after the work already queued on the caller's stream
+        if (idx != 0 && s->user_stream) {
+            if (cudaEventRecord(w->join, s->user_stream) != cudaSuccess ||
+                cudaStreamWaitEvent(w->stream, w->join, 0) != cudaSuccess)
+                rc = s->fail(S2L_ERR_CUDA, "cannot order a workspace after the caller's stream");
+        }
+    }
+    ~Lease()
+    {
+        if (idx < 0) return;
+        std::lock_guard<std::mutex> g(s->wmu);
+        s->busy[idx] = 0;
+    }
+};
 
 }  // namespace
 
@@ -827,11 +1023,10 @@ int s2l_gpu_setup_begin(s2l_ctx* ctx, int64_t n, int nsub, int one_level, int co
     s->coarse = coarse;
     s->pou = pou;
     s->hs.resize(nsub);
-    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&s->setup_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete s;
         return S2L_ERR_CUDA;
     }
-    s->stream = s->own_stream;
     *out = s;
     return S2L_OK;
 }
@@ -1294,26 +1489,9 @@ int s2l_gpu_setup_end(s2l_setup* s)
         std::vector<double> Ecopy = s->E, Einv;
         if (!dense_inverse(Ecopy, (int)s->n0, Einv)) return s->fail(S2L_ERR_NUMERIC, "coarse matrix E is singular");
         RET_IF(upload(s, &s->d_Einv, Einv));
-        RET_IF(alloc_doubles(s, &s->d_cpart, (size_t)s->ntiles * s->mmax));
-        RET_IF(alloc_doubles(s, &s->d_c, s->n0));
-        RET_IF(alloc_doubles(s, &s->d_y, s->n0));
     }
     RET_IF(upload(s, &s->d_subs, s->h_subs));
 
-    // ---- work vectors
-    RET_IF(alloc_doubles(s, &s->d_ylocal, loc));
-    RET_IF(alloc_doubles(s, &s->d_plocal, loc));
-    RET_IF(alloc_doubles(s, &s->d_x0, s->n));
-    RET_IF(alloc_doubles(s, &s->d_w, s->n));
-    RET_IF(alloc_doubles(s, &s->d_in, std::max<int64_t>(s->n, max_nl)));
-    RET_IF(alloc_doubles(s, &s->d_out, std::max<int64_t>(s->n, max_nl)));
-    RET_IF(alloc_doubles(s, &s->d_part, (size_t)S2L_NB_RED * S2L_MAX_RED_COLS));
-    RET_IF(alloc_doubles(s, &s->d_red, 512));
-    CUDA_OK(s, cudaMallocHost(&s->h_red, 512 * sizeof(double)));
-    RET_IF(dev_alloc(s, &s->d_ybuf, (size_t)std::max<int64_t>(loc, 1) * rs));
-    RET_IF(dev_alloc(s, &s->d_xbuf, (size_t)std::max<int64_t>(loc, 1) * rs));
-    RET_IF(dev_alloc(s, reinterpret_cast<void**>(&s->d_err), 16));
-    CUDA_OK(s, cudaMemsetAsync(s->d_err, 0, 16, s->stream));
     // sweep shared memory: x (T values) + one ready byte per row
     const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15) +
                         ((((size_t)max_T * 2) + 15) & ~(size_t)15);
@@ -1322,9 +1500,10 @@ int s2l_gpu_setup_end(s2l_setup* s)
         s->smem_bytes = smem;
     } else {
         s->smem_bytes = 0;
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&s->d_gflags), (size_t)std::max<int64_t>(loc, 1)));
+        s->need_gflags = true;
     }
-    CUDA_OK(s, cudaStreamSynchronize(s->stream));
+    s->max_nl = max_nl;
+    CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
     // host staging no longer needed
     s->A = HostCsr();
     for (auto& h : s->hs) {
@@ -1333,6 +1512,11 @@ int s2l_gpu_setup_end(s2l_setup* s)
         h.V.clear();
         h.V.shrink_to_fit();
     }
+    s2l_work* w0 = nullptr;
+    RET_IF(work_create(s, &w0));
+    if (s->user_stream) w0->stream = s->user_stream;
+    s->works.push_back(w0);
+    s->busy.push_back(0);
     s->ended = true;
     return S2L_OK;
 }
@@ -1341,16 +1525,14 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
 {
     if (!s) return S2L_OK;
     cudaSetDevice(s->ctx->device);
-    if (s->stream) cudaStreamSynchronize(s->stream);
-    prof_drain(s);
+    for (s2l_work* w : s->works) work_destroy(w);
+    if (s->setup_stream) cudaStreamSynchronize(s->setup_stream);
     for (void* p : s->allocs) cudaFree(p);
     {
         std::lock_guard<std::mutex> g(s->ctx->mu);
         s->ctx->used -= std::min(s->ctx->used, s->bytes);
     }
-    if (s->h_red) cudaFreeHost(s->h_red);
-    for (auto e : s->pool) cudaEventDestroy(e);
-    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (s->setup_stream) cudaStreamDestroy(s->setup_stream);
     delete s;
     return S2L_OK;
 }
@@ -1358,7 +1540,10 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
 {
     if (!s || !bytes) return S2L_ERR_BADARG;
-    *bytes = s->bytes;
+    std::lock_guard<std::mutex> g(s->wmu);
+    size_t b = s->bytes;
+    for (const s2l_work* w : s->works) b += w->bytes;
+    *bytes = b;
     return S2L_OK;
 }
 
@@ -1397,48 +1582,57 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
 int s2l_gpu_set_stream(s2l_setup* s, void* stream)
 {
     if (!s) return S2L_ERR_BADARG;
-    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    std::lock_guard<std::mutex> g(s->wmu);
+    s->user_stream = (cudaStream_t)stream;
+    if (!s->works.empty()) s->works[0]->stream = stream ? (cudaStream_t)stream : s->works[0]->own_stream;
     return S2L_OK;
 }
 
 int s2l_gpu_profile_enable(s2l_setup* s, int on)
 {
     if (!s) return S2L_ERR_BADARG;
-    prof_drain(s);
-    for (int c = 0; c < PC_N; ++c) {
-        s->acc_ms[c] = 0.0;
-        s->acc_n[c] = 0;
+    std::lock_guard<std::mutex> g(s->wmu);
+    s->prof_mask = (unsigned)on & 0x1Fu;
+    for (s2l_work* w : s->works) {
+        prof_drain(w);
+        for (int c = 0; c < PC_N; ++c) {
+            w->acc_ms[c] = 0.0;
+            w->acc_n[c] = 0;
+        }
+        w->prof = s->prof_mask;
+        w->launches = 0;
     }
-    s->prof = (unsigned)on & 0x1Fu;
-    s->launches = 0;
     return S2L_OK;
 }
 
 int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launches)
 {
     if (!s || !name || !ms || !launches) return S2L_ERR_BADARG;
-    prof_drain(s);
-    if (std::strcmp(name, "launches") == 0) {
-        *ms = 0.0;
-        *launches = s->launches;
-        return S2L_OK;
+    int cls = -2;  // -2 launches, -1 all classes, else one class
+    if (std::strcmp(name, "launches") == 0) cls = -2;
+    else if (std::strcmp(name, "all") == 0) cls = -1;
+    else {
+        cls = PC_N;
+        for (int c = 0; c < PC_N; ++c)
+            if (std::strcmp(name, kProfNames[c]) == 0) cls = c;
+        if (cls == PC_N) return s->fail(S2L_ERR_BADARG, std::string("unknown profile class ") + name);
     }
-    if (std::strcmp(name, "all") == 0) {
-        *ms = 0;
-        *launches = 0;
-        for (int c = 0; c < PC_N; ++c) {
-            *ms += s->acc_ms[c];
-            *launches += s->acc_n[c];
+    std::lock_guard<std::mutex> g(s->wmu);
+    *ms = 0.0;
+    *launches = 0;
+    for (s2l_work* w : s->works) {  // summed over the workspaces of concurrent calls
+        prof_drain(w);
+        if (cls == -2) {
+            *launches += w->launches;
+            continue;
         }
-        return S2L_OK;
+        for (int c = 0; c < PC_N; ++c)
+            if (cls == -1 || cls == c) {
+                *ms += w->acc_ms[c];
+                *launches += w->acc_n[c];
+            }
     }
-    for (int c = 0; c < PC_N; ++c)
-        if (std::strcmp(name, kProfNames[c]) == 0) {
-            *ms = s->acc_ms[c];
-            *launches = s->acc_n[c];
-            return S2L_OK;
-        }
-    return s->fail(S2L_ERR_BADARG, std::string("unknown profile class ") + name);
+    return S2L_OK;
 }
 
 int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes)
@@ -1452,37 +1646,46 @@ int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes)
 int s2l_gpu_spmv(s2l_setup* s, const double* x, double* y, int ptr_kind)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!x || !y) return s->fail(S2L_ERR_BADARG, "null vector");
     const double* dx;
-    RET_IF(stage_in(s, x, ptr_kind, s->n, s->d_in, &dx));
-    double* dy = ptr_kind == S2L_PTR_DEVICE ? y : s->d_out;
-    RET_IF(spmv_dev(s, dx, dy, nullptr, false));
-    return finish_out(s, y, dy, ptr_kind, s->n);
+    RET_IF(stage_in(w, x, ptr_kind, s->n, w->d_in, &dx));
+    double* dy = ptr_kind == S2L_PTR_DEVICE ? y : w->d_out;
+    RET_IF(spmv_dev(w, dx, dy, nullptr, false));
+    return finish_out(w, y, dy, ptr_kind, s->n);
 }
 
 int s2l_gpu_local_solve(s2l_setup* s, int i, const double* b_local, double* x_local, int ptr_kind)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (i < 0 || i >= s->nsub) return s->fail(S2L_ERR_BADARG, "subdomain index out of range");
     if (!b_local || !x_local) return s->fail(S2L_ERR_BADARG, "null vector");
     const int nl = s->h_subs[i].n_local;
     const double* db;
-    RET_IF(stage_in(s, b_local, ptr_kind, nl, s->d_in, &db));
-    double* dx = ptr_kind == S2L_PTR_DEVICE ? x_local : s->d_out;
-    RET_IF(run_local_solve(s, nullptr, nullptr, dx, 2, i, db));
-    return finish_out(s, x_local, dx, ptr_kind, nl);
+    RET_IF(stage_in(w, b_local, ptr_kind, nl, w->d_in, &db));
+    double* dx = ptr_kind == S2L_PTR_DEVICE ? x_local : w->d_out;
+    RET_IF(run_local_solve(w, nullptr, nullptr, dx, 2, i, db));
+    return finish_out(w, x_local, dx, ptr_kind, nl);
 }
 
 int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!r || !x0) return s->fail(S2L_ERR_BADARG, "null vector");
     if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return s->fail(S2L_ERR_STATE, "no coarse space");
     const double* dr;
-    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
-    double* dx = ptr_kind == S2L_PTR_DEVICE ? x0 : s->d_out;
-    RET_IF(coarse_apply(s, dr, dx));
-    return finish_out(s, x0, dx, ptr_kind, s->n);
+    RET_IF(stage_in(w, r, ptr_kind, s->n, w->d_in, &dr));
+    double* dx = ptr_kind == S2L_PTR_DEVICE ? x0 : w->d_out;
+    RET_IF(coarse_apply(w, dr, dx));
+    return finish_out(w, x0, dx, ptr_kind, s->n);
 }
 
 }  // extern "C"
@@ -1529,18 +1732,20 @@ extern "C" int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, doubl
                                            std::to_string(S2L_NOALLOC_SCRATCH_DOUBLES));
     double* scr = nullptr;
     RET_IF(noalloc_scratch(s, &scr));
+    // launched on the stream of workspace 0 (the caller's stream from s2l_gpu_set_stream)
+    s2l_work* w = s->works[0];
     double* part = scr;
     double* c = part + (int64_t)s->ntiles * s->mmax;
     double* y = c + s->n0;
     double* plocal = y + s->n0;
-    launch_coarse_restrict(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+    launch_coarse_restrict(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
                            boolean, r, s->mmax, part);
-    launch_coarse_reduce(s->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
-    launch_dense_gemv(s->stream, (int)s->n0, s->d_Einv, c, y);
-    launch_coarse_prolong(s->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
+    launch_coarse_reduce(w->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
+    launch_dense_gemv(w->stream, (int)s->n0, s->d_Einv, c, y);
+    launch_coarse_prolong(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
                           plocal);
-    if (!boolean) launch_combine(s->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
-    CUDA_OK(s, cudaGetLastError());
+    if (!boolean) launch_combine(w->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
+    CUDA_OK(w, cudaGetLastError());
     return S2L_OK;
 }
 
@@ -1549,25 +1754,31 @@ extern "C" {
 int s2l_gpu_one_level_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!r || !z) return s->fail(S2L_ERR_BADARG, "null vector");
     if (r == z) return s->fail(S2L_ERR_BADARG, "r and z must not alias");
     const double* dr;
-    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
-    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : s->d_out;
-    RET_IF(one_level(s, dr, nullptr, dz));
-    return finish_out(s, z, dz, ptr_kind, s->n);
+    RET_IF(stage_in(w, r, ptr_kind, s->n, w->d_in, &dr));
+    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : w->d_out;
+    RET_IF(one_level(w, dr, nullptr, dz));
+    return finish_out(w, z, dz, ptr_kind, s->n);
 }
 
 int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!r || !z) return s->fail(S2L_ERR_BADARG, "null vector");
     if (r == z) return s->fail(S2L_ERR_BADARG, "r and z must not alias");
     const double* dr;
-    RET_IF(stage_in(s, r, ptr_kind, s->n, s->d_in, &dr));
-    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : s->d_out;
-    RET_IF(apply_dev(s, dr, dz));
-    return finish_out(s, z, dz, ptr_kind, s->n);
+    RET_IF(stage_in(w, r, ptr_kind, s->n, w->d_in, &dr));
+    double* dz = ptr_kind == S2L_PTR_DEVICE ? z : w->d_out;
+    RET_IF(apply_dev(w, dr, dz));
+    return finish_out(w, z, dz, ptr_kind, s->n);
 }
 
 // Restarted right-preconditioned GMRES(m) with CGS2 (src/solver/gmres.cpp:18-161); flexible variant
@@ -1576,27 +1787,30 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
                   s2l_result* res)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->restart < 1 || o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
     const int m = o->restart;
     const bool flex = o->flexible != 0;
-    RET_IF(ensure_krylov(s, m, flex));
+    RET_IF(ensure_krylov(w, m, flex));
     const int64_t n = s->n;
-    cudaStream_t st = s->stream;
-    double* V = s->d_V_kr;
-    double* Z = s->d_Z_kr;
+    cudaStream_t st = w->stream;
+    double* V = w->d_V_kr;
+    double* Z = w->d_Z_kr;
     const double* db;
     if (ptr_kind == S2L_PTR_HOST) {
-        CUDA_OK(s, cudaMemcpyAsync(s->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        db = s->d_b;
+        CUDA_OK(w, cudaMemcpyAsync(w->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(w->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        db = w->d_b;
     } else if (ptr_kind == S2L_PTR_DEVICE) {
         db = b;
-        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(w->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     } else {
         return s->fail(S2L_ERR_BADARG, "bad ptr_kind");
     }
-    double* dx = s->d_xk;
+    double* dx = w->d_xk;
     res->converged = 0;
     res->breakdown = 0;
     res->iterations = 0;
@@ -1607,21 +1821,21 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         if (res->history_len < o->history_cap) ++res->history_len;
     };
     double bnorm = 0.0;
-    RET_IF(norm2_dev(s, db, &bnorm));
+    RET_IF(norm2_dev(w, db, &bnorm));
     if (bnorm == 0.0) {
-        CUDA_OK(s, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
+        CUDA_OK(w, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
         res->converged = 1;
         hist(0.0);
         res->rel_residual = res->true_rel_residual = 0.0;
-        return finish_out(s, x, dx, ptr_kind, n);
+        return finish_out(w, x, dx, ptr_kind, n);
     }
     if (!std::isfinite(bnorm)) return s->fail(S2L_ERR_NUMERIC, "non-finite right-hand side");
-    double* r = s->d_r;
-    double* z = s->d_z;
-    double* w = s->d_kw;
-    RET_IF(spmv_dev(s, dx, r, db, true));
-    RET_IF(read_red(s, 256, 1));
-    double beta = std::sqrt(s->h_red[256]);
+    double* r = w->d_r;
+    double* z = w->d_z;
+    double* wv = w->d_kw;
+    RET_IF(spmv_dev(w, dx, r, db, true));
+    RET_IF(read_red(w, 256, 1));
+    double beta = std::sqrt(w->h_red[256]);
     hist(beta / bnorm);
     res->rel_residual = beta / bnorm;
     bool converged = beta <= o->rtol * bnorm;
@@ -1630,9 +1844,9 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     while (!converged && res->iterations < o->maxit) {
         if (!std::isfinite(beta)) return s->fail(S2L_ERR_NUMERIC, "non-finite residual");
         {
-            Prof pr(s, PC_VEC);
+            Prof pr(w, PC_VEC);
             launch_axpby(st, n, 1.0 / beta, r, 0.0, V);
-            s->launches += 1;
+            w->launches += 1;
         }
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
@@ -1641,26 +1855,26 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         bool breakdown = false;
         for (int j = 0; j < m && res->iterations < o->maxit; ++j) {
             double* zj = flex ? Z + (size_t)j * n : z;
-            RET_IF(apply_dev(s, V + (size_t)j * n, zj));
-            RET_IF(spmv_dev(s, zj, w, nullptr, false));
+            RET_IF(apply_dev(w, V + (size_t)j * n, zj));
+            RET_IF(spmv_dev(w, zj, wv, nullptr, false));
             {
-                Prof pr(s, PC_VEC);
-                launch_mdot(st, n, V, n, j + 1, w, s->d_part, s->d_red);
-                launch_gemv_update(st, n, V, n, j + 1, s->d_red, -1.0, w, nullptr);
-                launch_mdot(st, n, V, n, j + 1, w, s->d_part, s->d_red + 128);
-                launch_gemv_update(st, n, V, n, j + 1, s->d_red + 128, -1.0, w, s->d_part);
-                launch_reduce(st, s->d_part, S2L_NB_RED, 1, s->d_red + 256);
-                s->launches += 7;
+                Prof pr(w, PC_VEC);
+                launch_mdot(st, n, V, n, j + 1, wv, w->d_part, w->d_red);
+                launch_gemv_update(st, n, V, n, j + 1, w->d_red, -1.0, wv, nullptr);
+                launch_mdot(st, n, V, n, j + 1, wv, w->d_part, w->d_red + 128);
+                launch_gemv_update(st, n, V, n, j + 1, w->d_red + 128, -1.0, wv, w->d_part);
+                launch_reduce(st, w->d_part, S2L_NB_RED, 1, w->d_red + 256);
+                w->launches += 7;
             }
-            CUDA_OK(s, cudaMemcpyAsync(s->h_red, s->d_red, 257 * sizeof(double), cudaMemcpyDeviceToHost, st));
-            RET_IF(check_err(s));
-            const double hn = std::sqrt(s->h_red[256]);
-            for (int i = 0; i <= j; ++i) Hc(i, j) = s->h_red[i] + s->h_red[128 + i];
+            CUDA_OK(w, cudaMemcpyAsync(w->h_red, w->d_red, 257 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            RET_IF(check_err(w));
+            const double hn = std::sqrt(w->h_red[256]);
+            for (int i = 0; i <= j; ++i) Hc(i, j) = w->h_red[i] + w->h_red[128 + i];
             Hc(j + 1, j) = hn;
             if (hn > 0.0) {
-                Prof pr(s, PC_VEC);
-                launch_axpby(st, n, 1.0 / hn, w, 0.0, V + (size_t)(j + 1) * n);
-                s->launches += 1;
+                Prof pr(w, PC_VEC);
+                launch_axpby(st, n, 1.0 / hn, wv, 0.0, V + (size_t)(j + 1) * n);
+                w->launches += 1;
             }
             for (int i = 0; i < j; ++i) {
                 const double t = cs[i] * Hc(i, j) + sn[i] * Hc(i + 1, j);
@@ -1694,25 +1908,25 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
             for (int c = i + 1; c < k; ++c) t -= Hc(i, c) * y[c];
             y[i] = t / Hc(i, i);
         }
-        CUDA_OK(s, cudaMemcpyAsync(s->d_coef, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(w->d_coef, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
         {
-            Prof pr(s, PC_VEC);
-            launch_gemv(st, n, flex ? Z : V, n, k, s->d_coef, s->d_u);
-            s->launches += 1;
+            Prof pr(w, PC_VEC);
+            launch_gemv(st, n, flex ? Z : V, n, k, w->d_coef, w->d_u);
+            w->launches += 1;
         }
         if (flex) {
-            Prof pr(s, PC_VEC);
-            launch_axpby(st, n, 1.0, s->d_u, 1.0, dx);
-            s->launches += 1;
+            Prof pr(w, PC_VEC);
+            launch_axpby(st, n, 1.0, w->d_u, 1.0, dx);
+            w->launches += 1;
         } else {
-            RET_IF(apply_dev(s, s->d_u, z));
-            Prof pr(s, PC_VEC);
+            RET_IF(apply_dev(w, w->d_u, z));
+            Prof pr(w, PC_VEC);
             launch_axpby(st, n, 1.0, z, 1.0, dx);
-            s->launches += 1;
+            w->launches += 1;
         }
-        RET_IF(spmv_dev(s, dx, r, db, true));
-        RET_IF(read_red(s, 256, 1));
-        beta = std::sqrt(s->h_red[256]);
+        RET_IF(spmv_dev(w, dx, r, db, true));
+        RET_IF(read_red(w, 256, 1));
+        beta = std::sqrt(w->h_red[256]);
         const bool within = beta <= o->rtol * bnorm;
         const bool within_slack = beta <= (o->strict_true_residual ? 1.0 : 1.1) * o->rtol * bnorm;
         if (breakdown) converged = within || converged;
@@ -1722,7 +1936,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     }
     res->converged = converged ? 1 : 0;
     res->true_rel_residual = beta / bnorm;
-    return finish_out(s, x, dx, ptr_kind, n);
+    return finish_out(w, x, dx, ptr_kind, n);
 }
 
 // Right-preconditioned BiCGStab, L2 stopping test (src/solver/bicgstab.cpp:15-154).
@@ -1730,33 +1944,36 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
                      s2l_result* res)
 {
     RET_IF(check_ready(s));
+    Lease lease(s);
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
-    RET_IF(ensure_krylov(s, 1, false));
+    RET_IF(ensure_krylov(w, 1, false));
     const int64_t n = s->n;
-    cudaStream_t st = s->stream;
-    if (!s->d_rh) {
-        RET_IF(alloc_doubles(s, &s->d_rh, n));
-        RET_IF(alloc_doubles(s, &s->d_p, n));
-        RET_IF(alloc_doubles(s, &s->d_v, n));
-        RET_IF(alloc_doubles(s, &s->d_s, n));
-        RET_IF(alloc_doubles(s, &s->d_t, n));
-        RET_IF(alloc_doubles(s, &s->d_yb, n));
+    cudaStream_t st = w->stream;
+    if (!w->d_rh) {
+        RET_IF(work_doubles(w, &w->d_rh, n));
+        RET_IF(work_doubles(w, &w->d_p, n));
+        RET_IF(work_doubles(w, &w->d_v, n));
+        RET_IF(work_doubles(w, &w->d_s, n));
+        RET_IF(work_doubles(w, &w->d_t, n));
+        RET_IF(work_doubles(w, &w->d_yb, n));
     }
     const double* db;
     if (ptr_kind == S2L_PTR_HOST) {
-        CUDA_OK(s, cudaMemcpyAsync(s->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        db = s->d_b;
+        CUDA_OK(w, cudaMemcpyAsync(w->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(w->d_xk, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        db = w->d_b;
     } else if (ptr_kind == S2L_PTR_DEVICE) {
         db = b;
-        CUDA_OK(s, cudaMemcpyAsync(s->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(w->d_xk, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     } else {
         return s->fail(S2L_ERR_BADARG, "bad ptr_kind");
     }
-    double* dx = s->d_xk;
-    double *r = s->d_r, *rh = s->d_rh, *p = s->d_p, *v = s->d_v, *y = s->d_yb, *sv = s->d_s, *zv = s->d_z,
-           *t = s->d_t;
+    double* dx = w->d_xk;
+    double *r = w->d_r, *rh = w->d_rh, *p = w->d_p, *v = w->d_v, *y = w->d_yb, *sv = w->d_s, *zv = w->d_z,
+           *t = w->d_t;
     res->converged = 0;
     res->breakdown = 0;
     res->iterations = 0;
@@ -1767,17 +1984,17 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         if (res->history_len < o->history_cap) ++res->history_len;
     };
     double bnorm = 0.0;
-    RET_IF(norm2_dev(s, db, &bnorm));
+    RET_IF(norm2_dev(w, db, &bnorm));
     if (bnorm == 0.0) {
-        CUDA_OK(s, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
+        CUDA_OK(w, cudaMemsetAsync(dx, 0, n * sizeof(double), st));
         res->converged = 1;
         hist(0.0);
         res->rel_residual = res->true_rel_residual = 0.0;
-        return finish_out(s, x, dx, ptr_kind, n);
+        return finish_out(w, x, dx, ptr_kind, n);
     }
-    RET_IF(spmv_dev(s, dx, r, db, true));
-    RET_IF(read_red(s, 256, 1));
-    double rn = std::sqrt(s->h_red[256]);
+    RET_IF(spmv_dev(w, dx, r, db, true));
+    RET_IF(read_red(w, 256, 1));
+    double rn = std::sqrt(w->h_red[256]);
     hist(rn / bnorm);
     res->rel_residual = rn / bnorm;
     auto satisfied = [&](double slack) { return rn <= slack * o->rtol * bnorm; };
@@ -1787,69 +2004,69 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             break;
         }
         if (res->iterations >= o->maxit) break;
-        CUDA_OK(s, cudaMemcpyAsync(rh, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(w, cudaMemcpyAsync(rh, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         const double rhn = rn;
         double rho = rn * rn, rho_old = 1.0, alpha = 1.0, omega = 1.0;
         bool first = true, candidate = false;
         while (res->iterations < o->maxit) {
             {
-                Prof pr(s, PC_VEC);
+                Prof pr(w, PC_VEC);
                 launch_bicg_p(st, n, r, v, first ? 0.0 : (rho / rho_old) * (alpha / omega), omega, p, first ? 1 : 0);
-                s->launches += 1;
+                w->launches += 1;
             }
             first = false;
-            RET_IF(apply_dev(s, p, y));
-            RET_IF(spmv_dev(s, y, v, nullptr, false));
+            RET_IF(apply_dev(w, p, y));
+            RET_IF(spmv_dev(w, y, v, nullptr, false));
             ++res->iterations;
             {
-                Prof pr(s, PC_VEC);
-                launch_dot2(st, n, rh, v, nullptr, s->d_part, s->d_red + 256);
-                s->launches += 2;
+                Prof pr(w, PC_VEC);
+                launch_dot2(st, n, rh, v, nullptr, w->d_part, w->d_red + 256);
+                w->launches += 2;
             }
-            RET_IF(read_red(s, 256, 1));
-            const double rhv = s->h_red[256];
+            RET_IF(read_red(w, 256, 1));
+            const double rhv = w->h_red[256];
             if (rhv == 0.0 || !std::isfinite(rhv)) {
                 res->breakdown = 1;
                 break;
             }
             alpha = rho / rhv;
             {
-                Prof pr(s, PC_VEC);
-                launch_bicg_s(st, n, r, v, alpha, sv, s->d_part, s->d_red + 256);
-                s->launches += 2;
+                Prof pr(w, PC_VEC);
+                launch_bicg_s(st, n, r, v, alpha, sv, w->d_part, w->d_red + 256);
+                w->launches += 2;
             }
-            RET_IF(read_red(s, 256, 1));
-            rn = std::sqrt(s->h_red[256]);
+            RET_IF(read_red(w, 256, 1));
+            rn = std::sqrt(w->h_red[256]);
             res->rel_residual = rn / bnorm;
             hist(res->rel_residual);
             if (satisfied(1.0) || res->iterations >= o->maxit) {
-                Prof pr(s, PC_VEC);
+                Prof pr(w, PC_VEC);
                 launch_axpby(st, n, alpha, y, 1.0, dx);
-                s->launches += 1;
-                CUDA_OK(s, cudaMemcpyAsync(r, sv, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                w->launches += 1;
+                CUDA_OK(w, cudaMemcpyAsync(r, sv, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
                 candidate = satisfied(1.0);
                 break;
             }
-            RET_IF(apply_dev(s, sv, zv));
-            RET_IF(spmv_dev(s, zv, t, nullptr, false));
+            RET_IF(apply_dev(w, sv, zv));
+            RET_IF(spmv_dev(w, zv, t, nullptr, false));
             ++res->iterations;
             {
-                Prof pr(s, PC_VEC);
-                launch_dot2(st, n, t, t, sv, s->d_part, s->d_red + 256);
-                s->launches += 2;
+                Prof pr(w, PC_VEC);
+                launch_dot2(st, n, t, t, sv, w->d_part, w->d_red + 256);
+                w->launches += 2;
             }
-            RET_IF(read_red(s, 256, 2));
-            const double tt = s->h_red[256], ts = s->h_red[257];
+            RET_IF(read_red(w, 256, 2));
+            const double tt = w->h_red[256], ts = w->h_red[257];
             omega = tt > 0.0 ? ts / tt : 0.0;
             {
-                Prof pr(s, PC_VEC);
-                launch_bicg_x(st, n, dx, y, zv, alpha, omega, r, sv, t, rh, s->d_part, s->d_red + 256);
-                s->launches += 2;
+                Prof pr(w, PC_VEC);
+                launch_bicg_x(st, n, dx, y, zv, alpha, omega, r, sv, t, rh, w->d_part, w->d_red + 256);
+                w->launches += 2;
             }
-            RET_IF(read_red(s, 256, 2));
+            RET_IF(read_red(w, 256, 2));
             rho_old = rho;
-            rn = std::sqrt(s->h_red[256]);
-            rho = s->h_red[257];
+            rn = std::sqrt(w->h_red[256]);
+            rho = w->h_red[257];
             res->rel_residual = rn / bnorm;
             hist(res->rel_residual);
             if (satisfied(1.0)) {
@@ -1858,9 +2075,9 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             }
             if (omega == 0.0 || std::fabs(rho) < 1e-14 * rhn * rn) break;
         }
-        RET_IF(spmv_dev(s, dx, r, db, true));
-        RET_IF(read_red(s, 256, 1));
-        rn = std::sqrt(s->h_red[256]);
+        RET_IF(spmv_dev(w, dx, r, db, true));
+        RET_IF(read_red(w, 256, 1));
+        rn = std::sqrt(w->h_red[256]);
         if (res->breakdown) break;
         if (candidate && satisfied(o->strict_true_residual ? 1.0 : 1.1)) {
             res->converged = 1;
@@ -1870,7 +2087,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         ++res->restarts;
     }
     res->true_rel_residual = rn / bnorm;
-    return finish_out(s, x, dx, ptr_kind, n);
+    return finish_out(w, x, dx, ptr_kind, n);
 }
 
 }  // extern "C"

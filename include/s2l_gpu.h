@@ -136,13 +136,21 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 int s2l_gpu_setup_end(s2l_setup* s);
 int s2l_gpu_setup_destroy(s2l_setup* s);
 
-/* Device bytes held by the setup (matrix, factors, basis, schedules, work vectors). */
+/* Device bytes held by the setup (matrix, factors, basis, schedules) and its workspaces. */
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
 /* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
    "sweep_group", "smem_bytes". */
 int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 
-/* ---- solve phase ---------------------------------------------------------------------- */
+/* ---- solve phase ----------------------------------------------------------------------
+ * Every call below returns when its results are complete (host or device pointers alike).
+ * Calls on one setup may come from several host threads at once.  Each call holds a workspace
+ * (stream, work vectors, Krylov basis, error word) for its duration.  Workspace 0 runs on the
+ * stream of s2l_gpu_set_stream and is taken when free.  A call that finds every workspace busy
+ * creates one more, with its own stream ordered after the work already queued on the
+ * s2l_gpu_set_stream stream, and the setup keeps it until s2l_gpu_setup_destroy.  The factors,
+ * matrix and coarse data are shared and only read.  s2l_gpu_set_stream, s2l_gpu_profile_* and
+ * s2l_gpu_setup_destroy must not overlap solve-phase calls. */
 int s2l_gpu_spmv(s2l_setup* s, const double* x, double* y, int ptr_kind);
 int s2l_gpu_local_solve(s2l_setup* s, int i, const double* b_local, double* x_local, int ptr_kind);
 int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind);
@@ -185,9 +193,9 @@ enum { S2L_PROF_SPMV = 1, S2L_PROF_LOCAL_SOLVE = 2, S2L_PROF_COARSE = 4, S2L_PRO
        S2L_PROF_KRYLOV_VEC = 16, S2L_PROF_ALL = 31 };
 /* Enables the classes of `mask` and resets the accumulators and the launch counter. */
 int s2l_gpu_profile_enable(s2l_setup* s, int mask);
-/* Accumulated event time [ms] and launch count of one kernel class; names: "spmv", "local_solve",
-   "coarse", "combine", "krylov_vec", "all"; "launches" gives every kernel launch of the setup since
-   the last s2l_gpu_profile_enable (timed or not) in *launches. */
+/* Accumulated event time [ms] and launch count of one kernel class, summed over the workspaces;
+   names: "spmv", "local_solve", "coarse", "combine", "krylov_vec", "all"; "launches" gives every
+   kernel launch of the setup since the last s2l_gpu_profile_enable (timed or not) in *launches. */
 int s2l_gpu_profile_get(s2l_setup* s, const char* name, double* ms, long* launches);
 /* Algorithmic bytes read+written by one local_solve launch (the roofline numerator). */
 int s2l_gpu_local_solve_bytes(const s2l_setup* s, double* bytes);
