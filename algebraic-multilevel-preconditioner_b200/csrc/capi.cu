@@ -11,14 +11,30 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <mutex>
+#include <thread>
 #include <numeric>
 #include <string>
 #include <vector>
 
 using namespace s2l;
+
+struct s2l_ticket;
+
+// Worker threads of the asynchronous solves (s2l_gpu_serve_start / s2l_gpu_submit)
+struct s2l_serve {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<s2l_ticket*> queue;
+    std::vector<std::thread> workers;
+    bool stop = false;
+};
 
 struct s2l_ctx {
     int device = 0;
@@ -26,7 +42,13 @@ struct s2l_ctx {
     size_t used = 0;
     std::string err;
     std::mutex mu;
+    s2l_serve* serve = nullptr;
 };
+
+namespace {
+thread_local std::string t_last_error;  // message of this thread's last failure (tickets read it)
+void serve_stop(s2l_ctx* ctx);
+}
 
 namespace {
 
@@ -40,7 +62,8 @@ struct s2l_tail_model {
     double bw = 6.0e12;      // bytes/s shared by all subdomains
     double nsub = 1.0;
     double real_bytes = 8.0;
-    double smem_cap = 227.0 * 1024.0 - 1024.0;
+    double smem_cap = (double)S2L_SWEEP_SMEM_CAP;
+    int chain = S2L_CHAIN_DEFAULT;  // chain block rows (1 = no blocking)
 };
 const char* kProfNames[PC_N] = {"spmv", "local_solve", "coarse", "combine", "krylov_vec"};
 
@@ -71,10 +94,18 @@ struct Sweep {
     std::vector<int32_t> pos;     // row -> slot
     std::vector<uint16_t> len;    // entries per slot
     std::vector<double> dinv;     // per slot
-    std::vector<int32_t> col;     // column slots, group-contiguous
-    std::vector<double> val;
-    std::vector<int64_t> gstart;  // per group, relative to the subdomain's first entry
+    std::vector<int32_t> col;     // column slots (-1: padding), per warp, per task lane-interleaved
+    std::vector<double> val;      // values times 1/diag of their row
+    std::vector<uint32_t> thdr;   // per task: chunks C (bits 0-15), log2 G (16-18), rows R - 1 (19-23)
+    std::vector<int32_t> tslot;   // per task: its R slots
+    std::vector<int64_t> wtask, wslot, went;  // per warp (nw + 1): first task, slot and entry
+    int64_t pad = 0, ntask = 0;
     int nlev = 0;
+    // chain blocks (>= 2 rows): block b holds the slots blk_slot[blk_off[b] .. blk_off[b + 1]) in
+    // solve order and the packed lower triangle of W^-1 at blk_inv[blk_ioff[b] ...]
+    std::vector<int64_t> blk_off{0}, blk_ioff{0};
+    std::vector<int32_t> blk_slot;
+    std::vector<double> blk_inv;
 };
 
 }  // namespace
@@ -104,14 +135,20 @@ struct s2l_setup {
     size_t bytes = 0;
     int32_t *d_rp = nullptr, *d_ci = nullptr;
     double* d_av = nullptr;
+    double* d_rowsum = nullptr;  // A 1 (OpenFOAM normalisation factor)
     int64_t nnz = 0;
     int tpr = 8;
     std::vector<DevSub> h_subs;
     DevSub* d_subs = nullptr;
     int64_t nloc = 0;
     int max_nl = 0;
-    uint16_t* d_len[2] = {nullptr, nullptr};
-    int64_t* d_gstart[2] = {nullptr, nullptr};
+    int64_t *d_wtask[2] = {nullptr, nullptr}, *d_wslot[2] = {nullptr, nullptr}, *d_went[2] = {nullptr, nullptr};
+    uint32_t* d_thdr[2] = {nullptr, nullptr};
+    int32_t* d_tslot[2] = {nullptr, nullptr};
+    int32_t* d_bfirst[2] = {nullptr, nullptr};
+    int64_t *d_boff[2] = {nullptr, nullptr}, *d_bioff[2] = {nullptr, nullptr};
+    int32_t* d_bslot[2] = {nullptr, nullptr};
+    void* d_binv[2] = {nullptr, nullptr};
     int32_t* d_col[2] = {nullptr, nullptr};
     int32_t* d_u2l = nullptr;
     void* d_val[2] = {nullptr, nullptr};
@@ -127,10 +164,13 @@ struct s2l_setup {
     std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
-    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0;
+    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
+    int64_t st_levels_max = 0, st_levels_sum = 0;  // sweep dependency levels (both factors)
+    int64_t st_blocks = 0;                         // chain blocks (both factors)
+    int64_t st_tasks = 0, st_pad = 0;              // sweep tasks and padding entries (both factors)
     int32_t *d_gin = nullptr, *d_pin = nullptr, *d_gout = nullptr, *d_l2g = nullptr;
     double* d_D = nullptr;
     int64_t* d_cp_ptr = nullptr;
@@ -151,8 +191,11 @@ struct s2l_setup {
     cudaStream_t user_stream = nullptr;  // s2l_gpu_set_stream: used by workspace 0
     unsigned prof_mask = 0;              // s2l_gpu_profile_enable: inherited by new workspaces
 
+    std::atomic<int> pending{0};  // asynchronous solves queued or running on this setup
+
     int fail(int code, const std::string& msg)
     {
+        t_last_error = msg;
         if (ctx) {
             std::lock_guard<std::mutex> g(ctx->mu);
             ctx->err = msg;
@@ -257,35 +300,148 @@ int upload(s2l_setup* s, T** dst, const std::vector<T>& v)
     return upload(s, dst, v.data(), v.size());
 }
 
-// Dependency levels of the rows [0, T) of a triangular factor (lower: forward, entries c < r;
-// upper: backward, entries r < c < T).  Returns the number of levels.
-int sweep_levels(const HostCsr& M, int T, bool lower, std::vector<int32_t>& level)
+// Chain blocks of the sparse part, in solve order (lower: rows 0, 1, ..; upper: T-1, T-2, ..): a
+// block grows while its next row depends on the row solved just before it, up to `chain` rows.
+// Returns, per block, the rows in solve order.
+std::vector<std::vector<int32_t>> chain_blocks(const HostCsr& M, int T, bool lower, int chain)
 {
-    level.assign(T, 0);
-    auto visit = [&](int r) {
-        int lv = 0;
-        for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
-            const int c = M.ci[e];
-            if (c == r || (lower ? (c > r) : (c < r || c >= T))) continue;
-            lv = std::max(lv, level[c] + 1);
-        }
-        level[r] = lv;
+    std::vector<std::vector<int32_t>> blocks;
+    auto seq = [&](int t) { return lower ? t : T - 1 - t; };
+    auto has = [&](int r, int c) {  // entry (r, c) present (sorted columns)
+        const int32_t* b = M.ci.data() + M.rp[r];
+        const int32_t* e = M.ci.data() + M.rp[r + 1];
+        const int32_t* it = std::lower_bound(b, e, c);
+        return it != e && *it == c;
     };
-    if (lower)
-        for (int r = 0; r < T; ++r) visit(r);
-    else
-        for (int r = T - 1; r >= 0; --r) visit(r);
-    int nlev = 0;
-    for (int r = 0; r < T; ++r) nlev = std::max(nlev, level[r] + 1);
-    return nlev;
+    for (int t = 0; t < T;) {
+        std::vector<int32_t> blk{(int32_t)seq(t)};
+        while (t + (int)blk.size() < T && (int)blk.size() < chain && has(seq(t + (int)blk.size()), blk.back()))
+            blk.push_back((int32_t)seq(t + (int)blk.size()));
+        t += (int)blk.size();
+        blocks.push_back(std::move(blk));
+    }
+    return blocks;
 }
 
 // Sweep layout of the sparse part (rows [0, T)): slots in level order, columns as slots, the rows
-// of group g (slots g, g + ng, ...) stored back to back.
-void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int ng, Sweep& out, std::string& err)
+// of each level packed into tasks of the nw warps of a sweep CTA (below).
+//
+// Chain blocks: for a block B of k rows solved one after another (row a depends on row a - 1),
+// W = M(B, B) (k x k, lower in solve order).  The block's rows are replaced by W^-1 M(B, outside),
+// which depend only on rows solved before the block, and the right-hand side of the block by
+// W^-1 b(B) (the sweep's prologue): the k-step chain becomes one level.  The replaced rows hold
+// the union of the block rows' patterns; a block stops before a row that would reach 65535 entries.
+void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, int gmax, int chain, Sweep& out,
+                 std::string& err)
 {
-    std::vector<int32_t> level;
-    out.nlev = sweep_levels(M, T, lower, level);
+    // rows of the sparse part, original numbering: (column, value) outside the diagonal, and diagonal
+    std::vector<std::vector<std::pair<int32_t, double>>> rows(T);
+    std::vector<double> diag(T, 1.0);
+    for (int r = 0; r < T; ++r) {
+        double dg = 1.0;
+        for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
+            const int c = M.ci[e];
+            if (c == r) {
+                dg = M.v[e];
+                continue;
+            }
+            if (lower ? (c > r) : (c < r || c >= T)) continue;
+            rows[r].emplace_back(c, M.v[e]);
+        }
+        if (unit_diag) dg = 1.0;
+        if (dg == 0.0 || !std::isfinite(dg)) {
+            err = "zero or non-finite diagonal in a triangular factor";
+            return;
+        }
+        diag[r] = dg;
+    }
+    // chain blocks: rewrite their rows
+    std::vector<std::vector<int32_t>> blocks = chain_blocks(M, T, lower, std::max(chain, 1));
+    std::vector<char> inblk(T, 0);
+    std::vector<double> acc(T, 0.0);
+    std::vector<int32_t> mark(T, -1), touched;
+    std::vector<std::vector<double>> winv_of;  // per block, packed lower W^-1
+    std::vector<int> blk_ids;                  // blocks of >= 2 rows, in solve order
+    for (int bi = 0; bi < (int)blocks.size(); ++bi) {
+        std::vector<int32_t>& B = blocks[bi];
+        int k = (int)B.size();
+        if (k < 2) continue;
+        for (int32_t r : B) inblk[r] = 1;
+        // W (k x k, lower in solve order) and its inverse by forward substitution, column by column
+        std::vector<double> W((size_t)k * k, 0.0);
+        for (int a2 = 0; a2 < k; ++a2) {
+            W[(size_t)a2 * k + a2] = diag[B[a2]];
+            for (const auto& cv : rows[B[a2]])
+                for (int b2 = 0; b2 < a2; ++b2)
+                    if (cv.first == B[b2]) W[(size_t)a2 * k + b2] = cv.second;
+        }
+        std::vector<double> Wi((size_t)k * k, 0.0);
+        for (int j = 0; j < k; ++j)
+            for (int i = j; i < k; ++i) {
+                double v = i == j ? 1.0 : 0.0;
+                for (int q = j; q < i; ++q) v -= W[(size_t)i * k + q] * Wi[(size_t)q * k + j];
+                Wi[(size_t)i * k + j] = v / W[(size_t)i * k + i];
+            }
+        // new row a = sum_{b <= a} W^-1(a, b) M(B[b], outside the block)
+        std::vector<std::vector<std::pair<int32_t, double>>> nrows(k);
+        int kept = k;
+        for (int a2 = 0; a2 < k; ++a2) {
+            touched.clear();
+            for (int b2 = 0; b2 <= a2; ++b2) {
+                const double w = Wi[(size_t)a2 * k + b2];
+                for (const auto& cv : rows[B[b2]]) {
+                    if (inblk[cv.first]) continue;
+                    if (mark[cv.first] != a2 + 1 + bi * 64) {
+                        mark[cv.first] = a2 + 1 + bi * 64;
+                        acc[cv.first] = 0.0;
+                        touched.push_back(cv.first);
+                    }
+                    acc[cv.first] += w * cv.second;
+                }
+            }
+            if (touched.size() >= 65535) {
+                kept = a2;
+                break;
+            }
+            std::sort(touched.begin(), touched.end());
+            for (int32_t c : touched) nrows[a2].emplace_back(c, acc[c]);
+        }
+        if (kept < 2) {  // too long to block: leave the rows as they are
+            for (int32_t r : B) inblk[r] = 0;
+            continue;
+        }
+        if (kept < k) {
+            // shorten the block: W^-1 of the leading rows is the leading part of W^-1, and the rows
+            // already rewritten never reference the dropped rows (those are solved after them)
+            for (int a2 = kept; a2 < k; ++a2) inblk[B[a2]] = 0;
+            B.resize(kept);
+            std::vector<double> Wk((size_t)kept * kept);
+            for (int i = 0; i < kept; ++i)
+                for (int j = 0; j < kept; ++j) Wk[(size_t)i * kept + j] = Wi[(size_t)i * k + j];
+            Wi.swap(Wk);
+            k = kept;
+        }
+        for (int a2 = 0; a2 < k; ++a2) {
+            rows[B[a2]].swap(nrows[a2]);
+            diag[B[a2]] = 1.0;
+            inblk[B[a2]] = 0;  // the marker covers the block being rewritten only
+        }
+        std::vector<double> packed;
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j <= i; ++j) packed.push_back(Wi[(size_t)i * k + j]);
+        winv_of.push_back(std::move(packed));
+        blk_ids.push_back(bi);
+    }
+    // dependency levels of the rewritten rows, in solve order
+    std::vector<int32_t> level(T, 0);
+    out.nlev = 0;
+    for (int t = 0; t < T; ++t) {
+        const int r = lower ? t : T - 1 - t;
+        int lv = 0;
+        for (const auto& cv : rows[r]) lv = std::max(lv, level[cv.first] + 1);
+        level[r] = lv;
+        out.nlev = std::max(out.nlev, lv + 1);
+    }
     std::vector<int32_t> cnt(out.nlev + 1, 0);
     for (int r = 0; r < T; ++r) ++cnt[level[r] + 1];
     for (int l = 0; l < out.nlev; ++l) cnt[l + 1] += cnt[l];
@@ -301,41 +457,109 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int ng, Sw
     for (int p = 0; p < T; ++p) out.pos[out.order[p]] = p;
     out.len.assign(T, 0);
     out.dinv.assign(T, 1.0);
-    std::vector<std::vector<std::pair<int32_t, double>>> rows(T);
     for (int p = 0; p < T; ++p) {
         const int r = out.order[p];
-        double dg = 1.0;
-        for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
-            const int c = M.ci[e];
-            if (c == r) {
-                dg = M.v[e];
-                continue;
-            }
-            if (lower ? (c > r) : (c < r || c >= T)) continue;
-            rows[p].emplace_back(out.pos[c], M.v[e]);
-        }
-        if (rows[p].size() >= 65535) {
+        if (rows[r].size() >= 65535) {
             err = "a sparse row has 65535 or more entries";
             return;
         }
-        out.len[p] = (uint16_t)rows[p].size();
-        if (unit_diag) dg = 1.0;
-        if (dg == 0.0 || !std::isfinite(dg)) {
-            err = "zero or non-finite diagonal in a triangular factor";
-            return;
-        }
-        out.dinv[p] = 1.0 / dg;
+        out.len[p] = (uint16_t)rows[r].size();
+        out.dinv[p] = 1.0 / diag[r];
     }
-    out.gstart.assign(ng, 0);
+    // Tasks: the rows of one level, R = 32 / G of them with G lanes each (G from the row length,
+    // about four entries per lane, at most gmax), sorted by width and length so a task's rows
+    // are alike.  Each task goes to the warp with the least work so far; a warp's tasks stay in
+    // level order.  Entries are stored lane-interleaved: chunk c of a task holds, for lane
+    // k * G + j, entry c * G + j of its row k (column -1 and value 0 past the row's end), with
+    // 1/diag folded into the values (the sweep scales the right-hand side by 1/diag too).
+    auto width = [&](int len) {
+        int g = 1;
+        while (g < gmax && g * 4 < len) g <<= 1;
+        return g;
+    };
+    struct WarpOut {
+        std::vector<uint32_t> hdr;
+        std::vector<int32_t> slot, col;
+        std::vector<double> val;
+        double cost = 0.0;
+    };
+    std::vector<WarpOut> wo(nw);
+    out.pad = 0;
+    out.ntask = 0;
+    std::vector<std::pair<int, int>> items;  // (width, slot)
+    for (int l = 0; l < out.nlev; ++l) {
+        items.clear();
+        for (int p = cnt[l]; p < cnt[l + 1]; ++p) items.emplace_back(width(out.len[p]), p);
+        std::sort(items.begin(), items.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+            if (a.first != b.first) return a.first < b.first;
+            if (out.len[a.second] != out.len[b.second]) return out.len[a.second] < out.len[b.second];
+            return a.second < b.second;
+        });
+        for (size_t i0 = 0; i0 < items.size();) {
+            const int G = items[i0].first;
+            size_t i1 = i0;
+            while (i1 < items.size() && items[i1].first == G && (int)(i1 - i0) < 32 / G) ++i1;
+            const int R = (int)(i1 - i0);
+            int C = 0;
+            for (size_t i = i0; i < i1; ++i) C = std::max(C, (out.len[items[i].second] + G - 1) / G);
+            int wbest = 0;
+            for (int w = 1; w < nw; ++w)
+                if (wo[w].cost < wo[wbest].cost) wbest = w;
+            WarpOut& W = wo[wbest];
+            W.cost += C + 3.0;
+            int gl2 = 0;
+            while ((1 << gl2) < G) ++gl2;
+            W.hdr.push_back((uint32_t)C | ((uint32_t)gl2 << 16) | ((uint32_t)(R - 1) << 19));
+            for (size_t i = i0; i < i1; ++i) W.slot.push_back(items[i].second);
+            for (int c = 0; c < C; ++c)
+                for (int lane = 0; lane < 32; ++lane) {
+                    const int k = lane / G, j = lane % G, e = c * G + j;
+                    int32_t colv = -1;
+                    double v = 0.0;
+                    if (k < R) {
+                        const int p = items[i0 + k].second;
+                        const auto& row = rows[out.order[p]];
+                        if (e < (int)row.size()) {
+                            colv = out.pos[row[e].first];
+                            v = row[e].second * out.dinv[p];
+                        }
+                    }
+                    if (colv < 0) ++out.pad;
+                    W.col.push_back(colv);
+                    W.val.push_back(v);
+                }
+            ++out.ntask;
+            i0 = i1;
+        }
+    }
+    out.wtask.assign(nw + 1, 0);
+    out.wslot.assign(nw + 1, 0);
+    out.went.assign(nw + 1, 0);
+    out.thdr.clear();
+    out.tslot.clear();
     out.col.clear();
     out.val.clear();
-    for (int g = 0; g < ng; ++g) {
-        out.gstart[g] = (int64_t)out.col.size();
-        for (int p = g; p < T; p += ng)
-            for (const auto& cv : rows[p]) {
-                out.col.push_back(cv.first);
-                out.val.push_back(cv.second);
-            }
+    for (int w = 0; w < nw; ++w) {
+        out.wtask[w] = (int64_t)out.thdr.size();
+        out.wslot[w] = (int64_t)out.tslot.size();
+        out.went[w] = (int64_t)out.col.size();
+        out.thdr.insert(out.thdr.end(), wo[w].hdr.begin(), wo[w].hdr.end());
+        out.tslot.insert(out.tslot.end(), wo[w].slot.begin(), wo[w].slot.end());
+        out.col.insert(out.col.end(), wo[w].col.begin(), wo[w].col.end());
+        out.val.insert(out.val.end(), wo[w].val.begin(), wo[w].val.end());
+    }
+    out.wtask[nw] = (int64_t)out.thdr.size();
+    out.wslot[nw] = (int64_t)out.tslot.size();
+    out.went[nw] = (int64_t)out.col.size();
+    out.blk_off.assign(1, 0);
+    out.blk_ioff.assign(1, 0);
+    out.blk_slot.clear();
+    out.blk_inv.clear();
+    for (size_t q = 0; q < blk_ids.size(); ++q) {
+        for (int32_t r : blocks[blk_ids[q]]) out.blk_slot.push_back(out.pos[r]);
+        out.blk_off.push_back((int64_t)out.blk_slot.size());
+        out.blk_inv.insert(out.blk_inv.end(), winv_of[q].begin(), winv_of[q].end());
+        out.blk_ioff.push_back((int64_t)out.blk_inv.size());
     }
 }
 
@@ -347,8 +571,33 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int ng, Sw
 int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model& tm)
 {
     if (tm.force_rows > 0) return std::max(1, n - std::min(tm.force_rows, n - 1));
-    std::vector<int32_t> level;
-    sweep_levels(L, n, true, level);
+    // forward levels of L after chain blocking, and the entries blocking adds to each row
+    std::vector<int32_t> level(n, 0), extra(n, 0);
+    {
+        std::vector<int32_t> mark(n, -1);
+        int stamp = 0;
+        for (const auto& B : chain_blocks(L, n, true, std::max(tm.chain, 1))) {
+            const int r0 = B.front();
+            int lv = 0, uni = 0;
+            ++stamp;
+            for (int32_t r : B) {
+                int raw = 0;
+                for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e) {
+                    const int c = L.ci[e];
+                    if (c >= r) continue;
+                    ++raw;
+                    if (c >= r0) continue;  // inside the block
+                    lv = std::max(lv, level[c] + 1);
+                    if (mark[c] != stamp) {
+                        mark[c] = stamp;
+                        ++uni;
+                    }
+                }
+                level[r] = lv;
+                if (B.size() > 1) extra[r] = uni - raw;
+            }
+        }
+    }
     std::vector<int32_t> maxlev(n + 1, 0);  // levels of rows [0, T)
     for (int r = 0; r < n; ++r) maxlev[r + 1] = std::max(maxlev[r], level[r] + 1);
     // entry counts as functions of T (difference arrays)
@@ -368,6 +617,7 @@ int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model&
     };
     account(L, true);
     account(U, false);
+    for (int r = 0; r < n; ++r) sp[r + 1] += 2.0 * extra[r];  // fill of the blocked rows (L and U alike)
     const double rs = tm.real_bytes, idx = 4.0;
     double best = 1e300;
     int bestT = n;
@@ -382,7 +632,7 @@ int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model&
     for (int T = n; T >= std::max(1, n - tm.tail_max); --T) {
         const double sz = n - T;
         if (sz > 0 && sz < tm.tail_min) continue;
-        if ((double)T * (rs + 3.0) + 64.0 > tm.smem_cap) continue;
+        if ((double)T * (rs + 1.0) + 64.0 > tm.smem_cap) continue;
         const double bytes = (spT[T] + cpT[T]) * (rs + idx) + sz * (sz + 1.0) * rs + 2.0 * T * (rs + 2.0);
         const double cost = 2.0 * tm.hop_s * maxlev[T] + bytes * tm.nsub / tm.bw;
         if (cost < best) {
@@ -530,8 +780,6 @@ void prof_begin(s2l_work* w, int cls, cudaEvent_t* a)
 
 void prof_end(s2l_work* w, int cls, cudaEvent_t a)
 {
-    s2l_setup* s = w->s;
-    (void)s;
     if (!(w->prof & (1u << cls))) return;
     if (w->pool.empty()) {
         cudaEvent_t e;
@@ -546,8 +794,6 @@ void prof_end(s2l_work* w, int cls, cudaEvent_t a)
 
 void prof_drain(s2l_work* w)
 {
-    s2l_setup* s = w->s;
-    (void)s;
     if (w->evs.empty()) return;
     cudaStreamSynchronize(w->stream);
     for (auto& e : w->evs) {
@@ -575,11 +821,13 @@ template <typename Real>
 LocalSolveArgs<Real> solve_args(s2l_work* w)
 {
     s2l_setup* s = w->s;
-    (void)s;
     LocalSolveArgs<Real> a{};
     a.subs = s->d_subs;
     for (int f = 0; f < 2; ++f)
-        a.f[f] = {s->d_col[f], (const Real*)s->d_val[f], (const Real*)s->d_dinv[f], s->d_len[f], s->d_gstart[f]};
+        a.f[f] = {s->d_col[f],   (const Real*)s->d_val[f], (const Real*)s->d_dinv[f], s->d_thdr[f],
+                  s->d_tslot[f], s->d_wtask[f],            s->d_wslot[f],             s->d_went[f],
+                  s->d_bfirst[f], s->d_boff[f],            s->d_bioff[f],             s->d_bslot[f],
+                  (const Real*)s->d_binv[f]};
     a.u2l = s->d_u2l;
     a.tr_sub = s->d_tr_sub;
     a.tr_i = s->d_tr_i;
@@ -608,7 +856,6 @@ int run_local_solve(s2l_work* w, const double* in, const double* base, double* o
                     const double* local_in)
 {
     s2l_setup* s = w->s;
-    (void)s;
     Prof pr(w, PC_SOLVE);
     const int nb = only_sub >= 0 ? 1 : s->nsub;
     int32_t* sub_list = nullptr;
@@ -633,7 +880,7 @@ int run_local_solve(s2l_work* w, const double* in, const double* base, double* o
         a.base = base;
         a.out = out;
         a.mode = mode;
-        e = launch_local_solve<float>(w->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
+        e = launch_local_solve<float>(w->stream, a, nb, smem, tr0, trn, us0, usn, &launched);
     } else {
         LocalSolveArgs<double> a = solve_args<double>(w);
         a.sub_list = sub_list;
@@ -642,7 +889,7 @@ int run_local_solve(s2l_work* w, const double* in, const double* base, double* o
         a.base = base;
         a.out = out;
         a.mode = mode;
-        e = launch_local_solve<double>(w->stream, a, nb, smem, s->sweep_group, tr0, trn, us0, usn, &launched);
+        e = launch_local_solve<double>(w->stream, a, nb, smem, tr0, trn, us0, usn, &launched);
     }
     w->launches += launched;
     if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("local_solve launch: ") + cudaGetErrorString(e));
@@ -653,7 +900,6 @@ int run_local_solve(s2l_work* w, const double* in, const double* base, double* o
 int one_level(s2l_work* w, const double* in, const double* base, double* out)
 {
     s2l_setup* s = w->s;
-    (void)s;
     if (s->pou == S2L_POU_BOOLEAN && s->one_level == S2L_ONE_LEVEL_RAS) return run_local_solve(w, in, base, out, 0, -1, nullptr);
     RET_IF(run_local_solve(w, in, nullptr, nullptr, 1, -1, nullptr));
     Prof pr(w, PC_COMBINE);
@@ -667,7 +913,6 @@ int one_level(s2l_work* w, const double* in, const double* base, double* out)
 int coarse_apply(s2l_work* w, const double* r, double* x0)
 {
     s2l_setup* s = w->s;
-    (void)s;
     Prof pr(w, PC_COARSE);
     const int boolean = s->pou == S2L_POU_BOOLEAN;
     launch_coarse_restrict(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
@@ -684,7 +929,6 @@ int coarse_apply(s2l_work* w, const double* r, double* x0)
 int spmv_dev(s2l_work* w, const double* x, double* y, const double* b, bool with_norm)
 {
     s2l_setup* s = w->s;
-    (void)s;
     Prof pr(w, PC_SPMV);
     launch_spmv(w->stream, s->n, s->d_rp, s->d_ci, s->d_av, x, y, b, with_norm ? w->d_part : nullptr,
                 w->d_red + 256, s->tpr);
@@ -696,7 +940,6 @@ int spmv_dev(s2l_work* w, const double* x, double* y, const double* b, bool with
 int apply_dev(s2l_work* w, const double* r, double* z)
 {
     s2l_setup* s = w->s;
-    (void)s;
     if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return one_level(w, r, nullptr, z);
     RET_IF(coarse_apply(w, r, w->d_x0));
     if (s->coarse == S2L_COARSE_ADDITIVE) return one_level(w, r, w->d_x0, z);
@@ -708,8 +951,6 @@ int apply_dev(s2l_work* w, const double* r, double* z)
 // host/device staging of a global vector argument
 int stage_in(s2l_work* w, const double* p, int kind, int64_t count, double* tmp, const double** dev)
 {
-    s2l_setup* s = w->s;
-    (void)s;
     if (kind == S2L_PTR_DEVICE) {
         *dev = p;
         return S2L_OK;
@@ -722,8 +963,6 @@ int stage_in(s2l_work* w, const double* p, int kind, int64_t count, double* tmp,
 
 int finish_out(s2l_work* w, double* dst, const double* dev, int kind, int64_t count)
 {
-    s2l_setup* s = w->s;
-    (void)s;
     if (kind == S2L_PTR_HOST)
         CUDA_OK(w, cudaMemcpyAsync(dst, dev, count * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
     else if (dst != dev)
@@ -736,7 +975,6 @@ int finish_out(s2l_work* w, double* dst, const double* dev, int kind, int64_t co
 int ensure_krylov(s2l_work* w, int m, bool flexible)
 {
     s2l_setup* s = w->s;
-    (void)s;
     if (w->kr_m >= m && (!flexible || w->kr_flex)) return S2L_OK;
     if (m + 1 > S2L_MAX_RED_COLS - 1) return w->fail(S2L_ERR_BADARG, "restart too large (max 120)");
     const size_t n = (size_t)s->n;
@@ -749,7 +987,7 @@ int ensure_krylov(s2l_work* w, int m, bool flexible)
         RET_IF(work_doubles(w, &w->d_b, n));
         RET_IF(work_doubles(w, &w->d_xk, n));
         RET_IF(work_doubles(w, &w->d_u, n));
-        RET_IF(work_doubles(w, &w->d_coef, S2L_MAX_RED_COLS));
+        RET_IF(work_doubles(w, &w->d_coef, 2 * S2L_MAX_RED_COLS));
     }
     w->kr_m = m;
     w->kr_flex = w->kr_flex || flexible;
@@ -758,8 +996,6 @@ int ensure_krylov(s2l_work* w, int m, bool flexible)
 
 int read_red(s2l_work* w, int off, int count)
 {
-    s2l_setup* s = w->s;
-    (void)s;
     CUDA_OK(w, cudaMemcpyAsync(w->h_red + off, w->d_red + off, count * sizeof(double), cudaMemcpyDeviceToHost,
                                w->stream));
     return check_err(w);
@@ -775,6 +1011,46 @@ int norm2_dev(s2l_work* w, const double* x, double* out_host)
     }
     RET_IF(read_red(w, 256, 1));
     *out_host = std::sqrt(w->h_red[256]);
+    return S2L_OK;
+}
+
+// sum|a - alpha c| (c may be nullptr) and sum a
+int l1_dev(s2l_work* w, const double* a, double alpha, const double* c, double* l1, double* sum)
+{
+    s2l_setup* s = w->s;
+    {
+        Prof pr(w, PC_VEC);
+        launch_l1(w->stream, s->n, a, alpha, c, w->d_part, w->d_red + 300);
+        w->launches += 2;
+    }
+    RET_IF(read_red(w, 300, 2));
+    *l1 = w->h_red[300];
+    if (sum) *sum = w->h_red[301];
+    return S2L_OK;
+}
+
+// OpenFOAM normalisation factor of x0 (src/solver/krylov.cpp:48-58), Ax0 = A x0:
+// F = sum|A x0 - xm A 1| + sum|b - xm A 1| + 1e-20, xm the mean of x0 (A 1 not needed when xm = 0)
+int of_norm_factor(s2l_work* w, const double* b, const double* x0, const double* Ax0, double* F)
+{
+    s2l_setup* s = w->s;
+    double unused = 0.0, sx = 0.0, a1 = 0.0, a2 = 0.0;
+    RET_IF(l1_dev(w, x0, 0.0, nullptr, &unused, &sx));
+    const double xm = s->n > 0 ? sx / (double)s->n : 0.0;
+    RET_IF(l1_dev(w, Ax0, xm, xm == 0.0 ? nullptr : s->d_rowsum, &a1, nullptr));
+    RET_IF(l1_dev(w, b, xm, xm == 0.0 ? nullptr : s->d_rowsum, &a2, nullptr));
+    *F = a1 + a2 + 1e-20;
+    return S2L_OK;
+}
+
+// checks of the stopping-norm options (src/solver/krylov.cpp:14-33)
+int check_stop(s2l_setup* s, const s2l_krylov_opts* o)
+{
+    if (o->stop_norm != S2L_STOP_L2 && o->stop_norm != S2L_STOP_OPENFOAM)
+        return s->fail(S2L_ERR_BADARG, "unknown stopping norm (S2L_STOP_L2 | S2L_STOP_OPENFOAM)");
+    if (!(o->atol >= 0.0)) return s->fail(S2L_ERR_BADARG, "atol must be >= 0");
+    if (o->atol > 0.0 && o->stop_norm != S2L_STOP_OPENFOAM)
+        return s->fail(S2L_ERR_BADARG, "an absolute tolerance needs the OpenFOAM stopping norm");
     return S2L_OK;
 }
 
@@ -994,6 +1270,8 @@ int s2l_gpu_create(int device, size_t hbm_budget_bytes, s2l_ctx** ctx)
 
 int s2l_gpu_destroy(s2l_ctx* ctx)
 {
+    if (!ctx) return S2L_OK;
+    serve_stop(ctx);
     delete ctx;
     return S2L_OK;
 }
@@ -1179,6 +1457,10 @@ int s2l_gpu_setup_end(s2l_setup* s)
         RET_IF(upload(s, &s->d_rp, rp));
         RET_IF(upload(s, &s->d_ci, s->A.ci));
         RET_IF(upload(s, &s->d_av, s->A.v));
+        std::vector<double> rowsum(s->n, 0.0);  // A 1, summed in row order as a CSR product does
+        for (int64_t r = 0; r < s->n; ++r)
+            for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) rowsum[r] += s->A.v[e];
+        RET_IF(upload(s, &s->d_rowsum, rowsum));
         const double avg = (double)s->nnz / (double)s->n;
         s->tpr = avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32));
     }
@@ -1197,6 +1479,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
     tm.bw = s->opt_bw_gbs * 1e9;
     tm.nsub = nsub;
     tm.real_bytes = (double)rs;
+    tm.chain = s->opt_chain;
     double sp_nnz_total = 0.0, sp_rows_total = 0.0;
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
@@ -1227,19 +1510,21 @@ int s2l_gpu_setup_end(s2l_setup* s)
             for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) sp_nnz_total += h.L.ci[e] < r ? 1.0 : 0.0;
         sp_rows_total += Ts[i];
     }
-    {
-        const double avg = sp_rows_total > 0 ? sp_nnz_total / sp_rows_total : 0.0;
-        s->sweep_group = s->opt_group ? s->opt_group : (avg <= 10.0 ? 8 : (avg <= 24.0 ? 16 : 32));
-    }
-    const int ng = S2L_BS_SWEEP / s->sweep_group;
+    (void)sp_nnz_total;
+    (void)sp_rows_total;
+    s->sweep_group = s->opt_group ? s->opt_group : 32;  // widest lane group of a sweep row
+    const int nw = S2L_BS_SWEEP / 32;
     // pass 2: layouts
     int64_t loc = 0;
     std::vector<int32_t> gin, pin, gout, l2g, u2l;
     std::vector<double> Dall;
-    std::vector<int32_t> sw_col[2];
+    std::vector<int32_t> sw_col[2], sw_tslot[2];
     std::vector<double> sw_val[2], sw_dinv[2];
-    std::vector<uint16_t> sw_len[2];
-    std::vector<int64_t> sw_gstart[2];
+    std::vector<uint32_t> sw_thdr[2];
+    std::vector<int64_t> sw_wtask[2], sw_wslot[2], sw_went[2];
+    std::vector<int32_t> sw_bfirst[2], sw_bslot[2];
+    std::vector<int64_t> sw_boff[2] = {{0}, {0}}, sw_bioff[2] = {{0}, {0}};
+    std::vector<double> sw_binv[2];
     std::vector<int32_t> tr_sub, tr_i, lts_col, us_sub, us_r, ust_col;
     std::vector<int64_t> lts_ptr(1, 0), ust_ptr(1, 0);
     std::vector<double> lts_val, ust_val;
@@ -1261,21 +1546,41 @@ int s2l_gpu_setup_end(s2l_setup* s)
         max_T = std::max(max_T, T);
         std::string err;
         Sweep sl, su;
-        build_sweep(h.L, T, true, unitL, ng, sl, err);
-        if (err.empty()) build_sweep(U, T, false, false, ng, su, err);
+        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, sl, err);
+        if (err.empty()) build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, su, err);
         if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
+        s->st_levels_max = std::max<int64_t>(s->st_levels_max, std::max(sl.nlev, su.nlev));
+        s->st_levels_sum += sl.nlev + su.nlev;
         for (int f = 0; f < 2; ++f) {
             const Sweep& q = f == 0 ? sl : su;
-            const int64_t e0 = sw_col[f].size();
-            for (int g = 0; g < ng; ++g) sw_gstart[f].push_back(e0 + q.gstart[g]);
+            const int64_t e0 = sw_col[f].size(), t0 = sw_thdr[f].size(), s0 = sw_tslot[f].size();
+            for (int w = 0; w < nw; ++w) {
+                sw_wtask[f].push_back(t0 + q.wtask[w]);
+                sw_wslot[f].push_back(s0 + q.wslot[w]);
+                sw_went[f].push_back(e0 + q.went[w]);
+            }
             sw_col[f].insert(sw_col[f].end(), q.col.begin(), q.col.end());
             sw_val[f].insert(sw_val[f].end(), q.val.begin(), q.val.end());
+            sw_thdr[f].insert(sw_thdr[f].end(), q.thdr.begin(), q.thdr.end());
+            sw_tslot[f].insert(sw_tslot[f].end(), q.tslot.begin(), q.tslot.end());
             sw_dinv[f].insert(sw_dinv[f].end(), q.dinv.begin(), q.dinv.end());
             sw_dinv[f].resize(sw_dinv[f].size() + sz, 1.0);
-            sw_len[f].insert(sw_len[f].end(), q.len.begin(), q.len.end());
-            sw_len[f].resize(sw_len[f].size() + sz, 0);
-            sparse_nnz += (int64_t)q.col.size();
-            bytes += (double)q.col.size() * (rs + 4) + (double)T * (2 + rs);
+            const int64_t real = (int64_t)q.col.size() - q.pad;
+            sparse_nnz += real;
+            s->st_pad += q.pad;
+            s->st_tasks += q.ntask;
+            // algorithmic bytes: the real entries, 1/diag and the task slots and headers
+            bytes += (double)real * (rs + 4) + (double)T * (rs + 4) + (double)q.ntask * 4;
+            // chain blocks (slots stay subdomain-relative)
+            sw_bfirst[f].push_back((int32_t)(sw_boff[f].size() - 1));
+            const int64_t so = (int64_t)sw_bslot[f].size(), io = (int64_t)sw_binv[f].size();
+            sw_bslot[f].insert(sw_bslot[f].end(), q.blk_slot.begin(), q.blk_slot.end());
+            sw_binv[f].insert(sw_binv[f].end(), q.blk_inv.begin(), q.blk_inv.end());
+            for (size_t b = 1; b < q.blk_off.size(); ++b) {
+                sw_boff[f].push_back(so + q.blk_off[b]);
+                sw_bioff[f].push_back(io + q.blk_ioff[b]);
+            }
+            bytes += (double)q.blk_inv.size() * rs + (double)q.blk_slot.size() * 4 + (double)(q.blk_off.size() - 1) * 16;
         }
         // backward slot -> forward slot
         for (int u = 0; u < T; ++u) u2l.push_back(sl.pos[su.order[u]]);
@@ -1371,9 +1676,25 @@ int s2l_gpu_setup_end(s2l_setup* s)
     s->st_tail_rows = (int64_t)tr_sub.size();
     bytes += (double)s->st_coupling_nnz * (rs + 4) + (double)(tr_sub.size() + us_sub.size()) * (8 + 8 + rs);
     for (int f = 0; f < 2; ++f) {
+        sw_wtask[f].push_back((int64_t)sw_thdr[f].size());
+        sw_wslot[f].push_back((int64_t)sw_tslot[f].size());
+        sw_went[f].push_back((int64_t)sw_col[f].size());
+        RET_IF(upload(s, &s->d_wtask[f], sw_wtask[f]));
+        RET_IF(upload(s, &s->d_wslot[f], sw_wslot[f]));
+        RET_IF(upload(s, &s->d_went[f], sw_went[f]));
+        RET_IF(upload(s, &s->d_thdr[f], sw_thdr[f]));
+        RET_IF(upload(s, &s->d_tslot[f], sw_tslot[f]));
+        sw_thdr[f] = {};
+        sw_tslot[f] = {};
+        sw_bfirst[f].push_back((int32_t)(sw_boff[f].size() - 1));
+        RET_IF(upload(s, &s->d_bfirst[f], sw_bfirst[f]));
+        RET_IF(upload(s, &s->d_boff[f], sw_boff[f]));
+        RET_IF(upload(s, &s->d_bioff[f], sw_bioff[f]));
+        RET_IF(upload(s, &s->d_bslot[f], sw_bslot[f]));
+        if (s->real == S2L_REAL_F32) RET_IF(upload_real<float>(s, &s->d_binv[f], sw_binv[f]));
+        else RET_IF(upload_real<double>(s, &s->d_binv[f], sw_binv[f]));
+        s->st_blocks += (int64_t)sw_boff[f].size() - 1;
         RET_IF(upload(s, &s->d_col[f], sw_col[f]));
-        RET_IF(upload(s, &s->d_len[f], sw_len[f]));
-        RET_IF(upload(s, &s->d_gstart[f], sw_gstart[f]));
         if (s->real == S2L_REAL_F32) {
             RET_IF(upload_real<float>(s, &s->d_val[f], sw_val[f]));
             RET_IF(upload_real<float>(s, &s->d_dinv[f], sw_dinv[f]));
@@ -1493,9 +1814,8 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(upload(s, &s->d_subs, s->h_subs));
 
     // sweep shared memory: x (T values) + one ready byte per row
-    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15) +
-                        ((((size_t)max_T * 2) + 15) & ~(size_t)15);
-    const size_t smem_cap = 227 * 1024 - 64;
+    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15);
+    const size_t smem_cap = S2L_SWEEP_SMEM_CAP;
     if (smem <= smem_cap) {
         s->smem_bytes = smem;
     } else {
@@ -1524,6 +1844,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
 int s2l_gpu_setup_destroy(s2l_setup* s)
 {
     if (!s) return S2L_OK;
+    if (s->pending.load() > 0) return s->fail(S2L_ERR_STATE, "asynchronous solves are queued or running on this setup");
     cudaSetDevice(s->ctx->device);
     for (s2l_work* w : s->works) work_destroy(w);
     if (s->setup_stream) cudaStreamSynchronize(s->setup_stream);
@@ -1561,6 +1882,10 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         const int g = (int)value;
         if (g != 0 && g != 8 && g != 16 && g != 32) return s->fail(S2L_ERR_BADARG, "sweep_group must be 0, 8, 16 or 32");
         s->opt_group = g;
+    } else if (n == "chain_block") {
+        const int c = (int)value;
+        if (c < 1 || c > S2L_CHAIN_MAX) return s->fail(S2L_ERR_BADARG, "chain_block must be in [1, 16]");
+        s->opt_chain = c;
     } else return s->fail(S2L_ERR_BADARG, "unknown setup option " + n);
     return S2L_OK;
 }
@@ -1575,6 +1900,11 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "tail_rows") *value = (double)s->st_tail_rows;
     else if (n == "sweep_group") *value = (double)s->sweep_group;
     else if (n == "smem_bytes") *value = (double)s->smem_bytes;
+    else if (n == "levels_max") *value = (double)s->st_levels_max;
+    else if (n == "chain_blocks") *value = (double)s->st_blocks;
+    else if (n == "sweep_tasks") *value = (double)s->st_tasks;
+    else if (n == "sweep_padding") *value = (double)s->st_pad;
+    else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;
     else return S2L_ERR_BADARG;
     return S2L_OK;
 }
@@ -1783,8 +2113,8 @@ int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind)
 
 // Restarted right-preconditioned GMRES(m) with CGS2 (src/solver/gmres.cpp:18-161); flexible variant
 // keeps Z_j = M^-1 v_j and updates x += Z y instead of x += M^-1 (V y).
-int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
-                  s2l_result* res)
+static int gmres_run(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                     s2l_result* res, const std::atomic<int>* cancel)
 {
     RET_IF(check_ready(s));
     Lease lease(s);
@@ -1792,6 +2122,8 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->restart < 1 || o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
+    RET_IF(check_stop(s, o));
+    const bool of = o->stop_norm == S2L_STOP_OPENFOAM;
     const int m = o->restart;
     const bool flex = o->flexible != 0;
     RET_IF(ensure_krylov(w, m, flex));
@@ -1816,6 +2148,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     res->iterations = 0;
     res->restarts = 0;
     res->history_len = 0;
+    res->initial_residual_of = res->final_residual_of = 0.0;
     auto hist = [&](double v) {
         if (res->history && res->history_len < o->history_cap) res->history[res->history_len] = v;
         if (res->history_len < o->history_cap) ++res->history_len;
@@ -1833,12 +2166,26 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     double* r = w->d_r;
     double* z = w->d_z;
     double* wv = w->d_kw;
+    // OpenFOAM test: sum|r| <= thr = max(rtol sum|r0|, atol F) (src/solver/gmres.cpp:41-56)
+    double normF = 1.0, l1 = 0.0, thr = 0.0;
+    if (of) {
+        RET_IF(spmv_dev(w, dx, w->d_u, nullptr, false));
+        RET_IF(of_norm_factor(w, db, dx, w->d_u, &normF));
+    }
     RET_IF(spmv_dev(w, dx, r, db, true));
     RET_IF(read_red(w, 256, 1));
     double beta = std::sqrt(w->h_red[256]);
     hist(beta / bnorm);
     res->rel_residual = beta / bnorm;
-    bool converged = beta <= o->rtol * bnorm;
+    bool converged = false;
+    if (of) {
+        RET_IF(l1_dev(w, r, 0.0, nullptr, &l1, nullptr));
+        res->initial_residual_of = l1 / normF;
+        thr = std::max(o->rtol * l1, o->atol * normF);
+        converged = l1 <= thr;  // x0 already satisfies the test: no iteration
+    } else {
+        converged = beta <= o->rtol * bnorm;
+    }
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (m + 1) + i]; };
     while (!converged && res->iterations < o->maxit) {
@@ -1854,6 +2201,7 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         int k = 0;
         bool breakdown = false;
         for (int j = 0; j < m && res->iterations < o->maxit; ++j) {
+            if (cancel && cancel->load(std::memory_order_relaxed)) return s->fail(S2L_ERR_CANCELED, "solve canceled");
             double* zj = flex ? Z + (size_t)j * n : z;
             RET_IF(apply_dev(w, V + (size_t)j * n, zj));
             RET_IF(spmv_dev(w, zj, wv, nullptr, false));
@@ -1893,7 +2241,34 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
             res->rel_residual = std::fabs(g[j + 1]) / bnorm;
             hist(res->rel_residual);
             if (!std::isfinite(res->rel_residual)) return s->fail(S2L_ERR_NUMERIC, "non-finite GMRES residual");
-            if (res->rel_residual <= o->rtol) {
+            bool done = false;
+            if (of) {
+                // GMRES residual r_j = g_{j+1} V_{j+2} Q^T e_{j+1} (src/solver/gmres.cpp:106-123)
+                if (hn == 0.0 || g[j + 1] == 0.0) {
+                    l1 = 0.0;
+                } else {
+                    std::vector<double> q(j + 2, 0.0);
+                    q[j + 1] = 1.0;
+                    for (int i = j; i >= 0; --i) {
+                        const double qa = q[i], qc = q[i + 1];
+                        q[i] = cs[i] * qa - sn[i] * qc;
+                        q[i + 1] = sn[i] * qa + cs[i] * qc;
+                    }
+                    double* dq = w->d_coef + S2L_MAX_RED_COLS;
+                    CUDA_OK(w, cudaMemcpyAsync(dq, q.data(), (j + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+                    {
+                        Prof pr(w, PC_VEC);
+                        launch_gemv_l1(st, n, V, n, j + 2, dq, w->d_part, w->d_red + 300);
+                        w->launches += 2;
+                    }
+                    RET_IF(read_red(w, 300, 1));
+                    l1 = std::fabs(g[j + 1]) * w->h_red[300];
+                }
+                done = l1 <= thr;
+            } else {
+                done = res->rel_residual <= o->rtol;
+            }
+            if (done) {
                 converged = true;
                 break;
             }
@@ -1927,8 +2302,10 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
         RET_IF(spmv_dev(w, dx, r, db, true));
         RET_IF(read_red(w, 256, 1));
         beta = std::sqrt(w->h_red[256]);
-        const bool within = beta <= o->rtol * bnorm;
-        const bool within_slack = beta <= (o->strict_true_residual ? 1.0 : 1.1) * o->rtol * bnorm;
+        if (of) RET_IF(l1_dev(w, r, 0.0, nullptr, &l1, nullptr));
+        const double slack = o->strict_true_residual ? 1.0 : 1.1;
+        const bool within = of ? l1 <= thr : beta <= o->rtol * bnorm;
+        const bool within_slack = of ? l1 <= slack * thr : beta <= slack * o->rtol * bnorm;
         if (breakdown) converged = within || converged;
         if (converged && !within_slack) converged = false;
         if (beta == 0.0) converged = true;
@@ -1936,12 +2313,13 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
     }
     res->converged = converged ? 1 : 0;
     res->true_rel_residual = beta / bnorm;
+    if (of) res->final_residual_of = l1 / normF;
     return finish_out(w, x, dx, ptr_kind, n);
 }
 
-// Right-preconditioned BiCGStab, L2 stopping test (src/solver/bicgstab.cpp:15-154).
-int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
-                     s2l_result* res)
+// Right-preconditioned BiCGStab, L2 or OpenFOAM stopping test (src/solver/bicgstab.cpp:15-154).
+static int bicgstab_run(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                        s2l_result* res, const std::atomic<int>* cancel)
 {
     RET_IF(check_ready(s));
     Lease lease(s);
@@ -1949,6 +2327,8 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
     s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
+    RET_IF(check_stop(s, o));
+    const bool of = o->stop_norm == S2L_STOP_OPENFOAM;
     RET_IF(ensure_krylov(w, 1, false));
     const int64_t n = s->n;
     cudaStream_t st = w->stream;
@@ -1979,6 +2359,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
     res->iterations = 0;
     res->restarts = 0;
     res->history_len = 0;
+    res->initial_residual_of = res->final_residual_of = 0.0;
     auto hist = [&](double val) {
         if (res->history && res->history_len < o->history_cap) res->history[res->history_len] = val;
         if (res->history_len < o->history_cap) ++res->history_len;
@@ -1992,12 +2373,23 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         res->rel_residual = res->true_rel_residual = 0.0;
         return finish_out(w, x, dx, ptr_kind, n);
     }
+    // OpenFOAM test: sum|r| <= thr = max(rtol sum|r0|, atol F) (src/solver/bicgstab.cpp:33-66)
+    double normF = 1.0, l1 = 0.0, thr = 0.0;
+    if (of) {
+        RET_IF(spmv_dev(w, dx, w->d_u, nullptr, false));
+        RET_IF(of_norm_factor(w, db, dx, w->d_u, &normF));
+    }
     RET_IF(spmv_dev(w, dx, r, db, true));
     RET_IF(read_red(w, 256, 1));
     double rn = std::sqrt(w->h_red[256]);
+    if (of) {
+        RET_IF(l1_dev(w, r, 0.0, nullptr, &l1, nullptr));
+        res->initial_residual_of = l1 / normF;
+        thr = std::max(o->rtol * l1, o->atol * normF);
+    }
     hist(rn / bnorm);
     res->rel_residual = rn / bnorm;
-    auto satisfied = [&](double slack) { return rn <= slack * o->rtol * bnorm; };
+    auto satisfied = [&](double slack) { return of ? l1 <= slack * thr : rn <= slack * o->rtol * bnorm; };
     for (;;) {
         if (satisfied(1.0)) {
             res->converged = 1;
@@ -2009,6 +2401,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         double rho = rn * rn, rho_old = 1.0, alpha = 1.0, omega = 1.0;
         bool first = true, candidate = false;
         while (res->iterations < o->maxit) {
+            if (cancel && cancel->load(std::memory_order_relaxed)) return s->fail(S2L_ERR_CANCELED, "solve canceled");
             {
                 Prof pr(w, PC_VEC);
                 launch_bicg_p(st, n, r, v, first ? 0.0 : (rho / rho_old) * (alpha / omega), omega, p, first ? 1 : 0);
@@ -2037,6 +2430,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             }
             RET_IF(read_red(w, 256, 1));
             rn = std::sqrt(w->h_red[256]);
+            if (of) RET_IF(l1_dev(w, sv, 0.0, nullptr, &l1, nullptr));
             res->rel_residual = rn / bnorm;
             hist(res->rel_residual);
             if (satisfied(1.0) || res->iterations >= o->maxit) {
@@ -2067,6 +2461,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
             rho_old = rho;
             rn = std::sqrt(w->h_red[256]);
             rho = w->h_red[257];
+            if (of) RET_IF(l1_dev(w, r, 0.0, nullptr, &l1, nullptr));
             res->rel_residual = rn / bnorm;
             hist(res->rel_residual);
             if (satisfied(1.0)) {
@@ -2078,6 +2473,7 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         RET_IF(spmv_dev(w, dx, r, db, true));
         RET_IF(read_red(w, 256, 1));
         rn = std::sqrt(w->h_red[256]);
+        if (of) RET_IF(l1_dev(w, r, 0.0, nullptr, &l1, nullptr));
         if (res->breakdown) break;
         if (candidate && satisfied(o->strict_true_residual ? 1.0 : 1.1)) {
             res->converged = 1;
@@ -2087,7 +2483,229 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
         ++res->restarts;
     }
     res->true_rel_residual = rn / bnorm;
+    if (of) res->final_residual_of = l1 / normF;
     return finish_out(w, x, dx, ptr_kind, n);
+}
+
+int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                  s2l_result* res)
+{
+    return gmres_run(s, b, x, ptr_kind, o, res, nullptr);
+}
+
+int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                     s2l_result* res)
+{
+    return bicgstab_run(s, b, x, ptr_kind, o, res, nullptr);
+}
+
+// ------------------------------------------------------------------------------ batched solves
+int s2l_gpu_solve_batch(s2l_setup* s, int method, int k, const double* const* b, double* const* x, int ptr_kind,
+                        const s2l_krylov_opts* opts, s2l_result* results, int* status)
+{
+    RET_IF(check_ready(s));
+    if (k < 1 || !b || !x || !opts || !results || !status) return s->fail(S2L_ERR_BADARG, "bad batch arguments");
+    if (method != S2L_KRYLOV_GMRES && method != S2L_KRYLOV_BICGSTAB)
+        return s->fail(S2L_ERR_BADARG, "unknown Krylov method");
+    auto one = [&](int j) {
+        status[j] = method == S2L_KRYLOV_GMRES ? gmres_run(s, b[j], x[j], ptr_kind, opts, &results[j], nullptr)
+                                               : bicgstab_run(s, b[j], x[j], ptr_kind, opts, &results[j], nullptr);
+    };
+    std::vector<std::thread> th;
+    th.reserve(k - 1);
+    for (int j = 1; j < k; ++j) th.emplace_back(one, j);
+    one(0);
+    for (auto& t : th) t.join();
+    for (int j = 0; j < k; ++j)
+        if (status[j] != S2L_OK) return status[j];
+    return S2L_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------ asynchronous solves
+struct s2l_ticket {
+    s2l_setup* s = nullptr;
+    int method = S2L_KRYLOV_GMRES;
+    const double* b = nullptr;
+    double* x = nullptr;
+    int ptr_kind = S2L_PTR_HOST;
+    s2l_krylov_opts opts{};
+    s2l_result* res = nullptr;
+    std::atomic<int> state{S2L_JOB_QUEUED};
+    std::atomic<int> cancel{0};
+    int status = S2L_OK;
+    std::string err;
+    std::chrono::steady_clock::time_point t_submit, t_start, t_end;
+    std::mutex mu;
+    std::condition_variable cv;
+};
+
+namespace {
+
+void ticket_finish(s2l_ticket* t, int state, int status)
+{
+    {
+        std::lock_guard<std::mutex> g(t->mu);
+        t->status = status;
+        t->t_end = std::chrono::steady_clock::now();
+        t->state.store(state);
+    }
+    t->s->pending.fetch_sub(1);
+    t->cv.notify_all();
+}
+
+void serve_worker(s2l_ctx* ctx)
+{
+    s2l_serve* sv = ctx->serve;
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        s2l_ticket* t = nullptr;
+        {
+            std::unique_lock<std::mutex> g(sv->mu);
+            sv->cv.wait(g, [&] { return sv->stop || !sv->queue.empty(); });
+            if (sv->queue.empty()) return;  // stop requested and nothing left
+            t = sv->queue.front();
+            sv->queue.pop_front();
+        }
+        if (t->cancel.load()) {
+            t->err = "solve canceled before it started";
+            ticket_finish(t, S2L_JOB_CANCELED, S2L_ERR_CANCELED);
+            continue;
+        }
+        t->t_start = std::chrono::steady_clock::now();
+        t->state.store(S2L_JOB_RUNNING);
+        t_last_error.clear();
+        const int rc = t->method == S2L_KRYLOV_GMRES
+                           ? gmres_run(t->s, t->b, t->x, t->ptr_kind, &t->opts, t->res, &t->cancel)
+                           : bicgstab_run(t->s, t->b, t->x, t->ptr_kind, &t->opts, t->res, &t->cancel);
+        if (rc != S2L_OK) t->err = t_last_error;
+        ticket_finish(t, rc == S2L_ERR_CANCELED ? S2L_JOB_CANCELED : S2L_JOB_DONE, rc);
+    }
+}
+
+void serve_stop(s2l_ctx* ctx)
+{
+    s2l_serve* sv = ctx->serve;
+    if (!sv) return;
+    std::deque<s2l_ticket*> left;
+    {
+        std::lock_guard<std::mutex> g(sv->mu);
+        sv->stop = true;
+        left.swap(sv->queue);
+    }
+    for (s2l_ticket* t : left) {
+        t->err = "context destroyed before the solve started";
+        ticket_finish(t, S2L_JOB_CANCELED, S2L_ERR_CANCELED);
+    }
+    sv->cv.notify_all();
+    for (auto& w : sv->workers) w.join();
+    delete sv;
+    ctx->serve = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int s2l_gpu_serve_start(s2l_ctx* ctx, int workers)
+{
+    if (!ctx || workers < 1 || workers > 256) return S2L_ERR_BADARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->serve) {
+        ctx->err = "the worker threads are already running";
+        return S2L_ERR_STATE;
+    }
+    ctx->serve = new s2l_serve;
+    for (int i = 0; i < workers; ++i) ctx->serve->workers.emplace_back(serve_worker, ctx);
+    return S2L_OK;
+}
+
+int s2l_gpu_submit(s2l_setup* s, int method, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
+                   s2l_result* result, s2l_ticket** ticket)
+{
+    RET_IF(check_ready(s));
+    if (!ticket) return s->fail(S2L_ERR_BADARG, "null ticket");
+    *ticket = nullptr;
+    if (!b || !x || !opts || !result) return s->fail(S2L_ERR_BADARG, "null argument");
+    if (method != S2L_KRYLOV_GMRES && method != S2L_KRYLOV_BICGSTAB)
+        return s->fail(S2L_ERR_BADARG, "unknown Krylov method");
+    s2l_serve* sv = s->ctx->serve;
+    if (!sv) return s->fail(S2L_ERR_STATE, "s2l_gpu_serve_start was not called on this context");
+    auto* t = new s2l_ticket;
+    t->s = s;
+    t->method = method;
+    t->b = b;
+    t->x = x;
+    t->ptr_kind = ptr_kind;
+    t->opts = *opts;
+    t->res = result;
+    t->t_submit = std::chrono::steady_clock::now();
+    s->pending.fetch_add(1);
+    {
+        std::lock_guard<std::mutex> g(sv->mu);
+        if (sv->stop) {
+            s->pending.fetch_sub(1);
+            delete t;
+            return s->fail(S2L_ERR_STATE, "the worker threads are stopping");
+        }
+        sv->queue.push_back(t);
+    }
+    sv->cv.notify_one();
+    *ticket = t;
+    return S2L_OK;
+}
+
+int s2l_gpu_poll(s2l_ticket* t, int* state)
+{
+    if (!t || !state) return S2L_ERR_BADARG;
+    *state = t->state.load();
+    return S2L_OK;
+}
+
+int s2l_gpu_wait(s2l_ticket* t, double timeout_s, int* status)
+{
+    if (!t) return S2L_ERR_BADARG;
+    std::unique_lock<std::mutex> g(t->mu);
+    auto finished = [&] { return t->state.load() >= S2L_JOB_DONE; };
+    if (timeout_s < 0.0) {
+        t->cv.wait(g, finished);
+    } else if (!t->cv.wait_for(g, std::chrono::duration<double>(timeout_s), finished)) {
+        return S2L_ERR_TIMEOUT;
+    }
+    if (status) *status = t->status;
+    return S2L_OK;
+}
+
+int s2l_gpu_cancel(s2l_ticket* t)
+{
+    if (!t) return S2L_ERR_BADARG;
+    t->cancel.store(1);
+    return S2L_OK;
+}
+
+int s2l_gpu_ticket_info(s2l_ticket* t, double* queue_ms, double* run_ms, const char** error)
+{
+    if (!t) return S2L_ERR_BADARG;
+    std::lock_guard<std::mutex> g(t->mu);
+    const int st = t->state.load();
+    using ms = std::chrono::duration<double, std::milli>;
+    if (queue_ms)
+        *queue_ms = st >= S2L_JOB_RUNNING && t->t_start.time_since_epoch().count()
+                        ? ms(t->t_start - t->t_submit).count()
+                        : (st >= S2L_JOB_DONE ? ms(t->t_end - t->t_submit).count() : 0.0);
+    if (run_ms)
+        *run_ms = st >= S2L_JOB_DONE && t->t_start.time_since_epoch().count() ? ms(t->t_end - t->t_start).count() : 0.0;
+    if (error) *error = t->err.c_str();
+    return S2L_OK;
+}
+
+int s2l_gpu_ticket_free(s2l_ticket* t)
+{
+    if (!t) return S2L_OK;
+    if (t->state.load() < S2L_JOB_DONE) return S2L_ERR_STATE;
+    delete t;
+    return S2L_OK;
 }
 
 }  // extern "C"

@@ -192,6 +192,45 @@ __global__ void __launch_bounds__(256) dot2_kernel(int64_t n, const double* __re
     }
 }
 
+// ------------------------------------------------------------------------------ OpenFOAM stopping norm
+// partials[b * 2 + 0] = sum |a_i - alpha c_i| (c may be nullptr), partials[b * 2 + 1] = sum a_i
+__global__ void __launch_bounds__(256) l1_kernel(int64_t n, const double* __restrict__ a, double alpha,
+                                                 const double* __restrict__ c, double* __restrict__ partials)
+{
+    __shared__ double sh[8];
+    double s1 = 0.0, s0 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        const double ai = a[i];
+        s1 += fabs(c ? ai - alpha * c[i] : ai);
+        s0 += ai;
+    }
+    const double t1 = block_sum<256>(s1, sh);
+    const double t0 = block_sum<256>(s0, sh);
+    if (threadIdx.x == 0) {
+        partials[(int64_t)blockIdx.x * 2] = t1;
+        partials[(int64_t)blockIdx.x * 2 + 1] = t0;
+    }
+}
+
+// partials[b] = sum_i |(V(:, 0:k) q)_i| (q on the device): the 1-norm of a combination of the
+// Krylov basis without writing it
+__global__ void __launch_bounds__(256) gemv_l1_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int k,
+                                                      const double* __restrict__ q, double* __restrict__ partials)
+{
+    __shared__ double qs[S2L_MAX_RED_COLS];
+    __shared__ double sh[8];
+    for (int c = threadIdx.x; c < k; c += 256) qs[c] = q[c];
+    __syncthreads();
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        double s = 0.0;
+        for (int c = 0; c < k; ++c) s += V[i + (int64_t)c * ldv] * qs[c];
+        acc += fabs(s);
+    }
+    const double t = block_sum<256>(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
 // ------------------------------------------------------------------------------ BiCGStab (K9)
 __global__ void bicg_p_kernel(int64_t n, const double* __restrict__ r, const double* __restrict__ v, double beta,
                               double omega, double* __restrict__ p, int first)
@@ -242,38 +281,26 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 
 // ------------------------------------------------------------------------------ local solves (K2, K3)
 // Sparse sweep of one factor, one CTA per subdomain, x in shared memory (or, when it does not
-// fit, in the local-space buffers with global ready flags and lengths).
+// fit, in the local-space buffers with global ready flags).
 //
-// Rows are slots in solve order (every dependency of slot p is a slot < p).  Group g (G lanes)
-// owns the slots g, g + NG, g + 2 NG, ... and their entries are stored back to back, so the group
-// knows where its next rows start from the row lengths alone (kept in shared memory).  For each
-// entry it waits until the ready flag of the column is set, then writes its row and sets its own
-// flag; no CTA barrier is taken per level.  A group only waits for smaller slots, and the smallest
-// unfinished slot always has its inputs ready, so the sweep cannot deadlock.  Every wait is
-// bounded: after S2L_SPIN_LIMIT polls the CTA raises *err and all groups leave.  While a group works
-// on one row, its next S2L_PREFETCH rows (1/diag and the first S2L_PREFETCH_CHUNKS*G entries) are
-// already in flight, with addresses that depend on no load, so the factor stream overlaps the
-// dependency chain instead of adding to it.
-template <typename Real, int G>
-__device__ __forceinline__ Real group_reduce(Real v)
-{
-#pragma unroll
-    for (int o = G >> 1; o; o >>= 1) {
-        const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-        v += __shfl_down_sync(mask, v, o, G);
-    }
-    return v;
-}
-
-template <typename Real, int G, bool SMEM, bool FWD>
+// Rows are slots in solve order (every dependency of slot p is a slot of a lower level).  The rows
+// of each level are packed into tasks: a task is R rows of one level with G = 32 / R lanes each
+// (G follows the row length), and each warp runs its own list of tasks in level order.  Rows of
+// one task never depend on each other, a warp only waits for rows of lower levels, and the lowest
+// unfinished level always has its inputs ready, so the sweep cannot deadlock.  A task's entries
+// are stored lane-interleaved, so every load is coalesced and its address depends on no loaded
+// value; the chunks of a task are loaded in batches (all loads of a batch issued before the first
+// wait on a ready flag) and the next batch is hinted into L2.  For each entry a lane waits until
+// the ready flag of the column is set; 1/diag is folded into the values and the right-hand side,
+// so a row ends with x = b - sum, one write and its flag.  Every wait is bounded: after
+// S2L_SPIN_LIMIT polls the CTA raises *err and all warps leave.
+template <typename Real, bool SMEM, bool FWD>
 __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolveArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_word;
     volatile int& abort_flag = abort_word;
-    constexpr int NG = S2L_BS_SWEEP / G;
-    constexpr int D = S2L_PREFETCH;
-    constexpr int P = S2L_PREFETCH_CHUNKS;
+    constexpr int Q = S2L_BATCH_CHUNKS;
     const int sid = a.sub_list ? a.sub_list[blockIdx.x] : (int)blockIdx.x;
     const DevSub sd = a.subs[sid];
     const int64_t lo = sd.loc_off;
@@ -281,118 +308,75 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     const SweepFactor<Real> F = a.f[FWD ? 0 : 1];
     Real* xs;
     volatile uint8_t* flag;
-    const uint16_t* lens;
     if (SMEM) {
         const size_t off1 = (((size_t)T * sizeof(Real)) + 15) & ~(size_t)15;
-        const size_t off2 = off1 + ((((size_t)T) + 15) & ~(size_t)15);
         xs = reinterpret_cast<Real*>(smem_raw);
         flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off1);
-        uint16_t* ls = reinterpret_cast<uint16_t*>(smem_raw + off2);
-        for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) ls[k] = F.len[lo + k];
-        lens = ls;
     } else {
         xs = (FWD ? a.ybuf : a.xbuf) + lo;
         flag = a.gflags + lo;
-        lens = F.len + lo;
     }
     volatile Real* x = xs;
     if (threadIdx.x == 0) abort_flag = 0;
     for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) {
-        xs[k] = FWD ? (Real)a.in[a.gather[lo + k]] : a.ybuf[lo + a.u2l[lo + k]];
+        const Real b = FWD ? (Real)a.in[a.gather[lo + k]] : a.ybuf[lo + a.u2l[lo + k]];
+        xs[k] = b * F.dinv[lo + k];
         flag[k] = 0;
     }
     __syncthreads();
-    const int g = threadIdx.x / G, l = threadIdx.x % G;
-    int64_t nst = F.gstart[(int64_t)sid * NG + g];  // start of the next row to prefetch
-    int pr_len[D];
-    int64_t pr_st[D];
-    Real pr_dinv[D];
-    int pr_col[D][P];
-    Real pr_val[D][P];
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-        const int p = g + d * NG;
-        pr_len[d] = 0;
-        pr_st[d] = nst;
-        pr_dinv[d] = Real(1);
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            pr_col[d][k] = 0;
-            pr_val[d][k] = Real(0);
+    // chain blocks: right-hand side of block B becomes W^-1 b(B) (W^-1 packed lower, solve order);
+    // row i of the block only needs b(0..i), so the rows are overwritten from the last one down
+    {
+        const int b1 = F.blk_first[sid + 1];
+        for (int b = F.blk_first[sid] + threadIdx.x; b < b1; b += S2L_BS_SWEEP) {
+            const int64_t o = F.blk_off[b];
+            const int k = (int)(F.blk_off[b + 1] - o);
+            const Real* W = F.blk_inv + F.blk_ioff[b];
+            for (int i = k - 1; i >= 0; --i) {
+                const Real* Wi = W + i * (i + 1) / 2;
+                Real v = Real(0);
+                for (int j = 0; j <= i; ++j) v += Wi[j] * xs[F.blk_slot[o + j]];
+                xs[F.blk_slot[o + i]] = v;
+            }
         }
-        if (p < T) {
-            const int L = lens[p];
-            pr_len[d] = L;
-            pr_dinv[d] = F.dinv[lo + p];
-#pragma unroll
-            for (int k = 0; k < P; ++k)
-                if (l + k * G < L) {
-                    pr_col[d][k] = F.col[nst + l + k * G];
-                    pr_val[d][k] = F.val[nst + l + k * G];
-                }
-            nst += L;
-        }
+        __syncthreads();
     }
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t wi = (int64_t)sid * S2L_SWEEP_WARPS + wid;
+    const int64_t t1 = F.wtask[wi + 1];
+    int64_t so = F.wslot[wi], eo = F.went[wi];
     bool dead = false;
-    for (int p0 = g; p0 < T && !dead; p0 += D * NG) {
+    for (int64_t t = F.wtask[wi]; t < t1; ++t) {
+        const uint32_t h = F.thdr[t];
+        const int C = (int)(h & 0xFFFFu), gl2 = (int)((h >> 16) & 7u), R = (int)((h >> 19) & 31u) + 1;
+        const int k = lane >> gl2;
+        const int slot = k < R ? F.tslot[so + k] : -1;
+        so += R;
+        Real acc = Real(0);
+        for (int c0 = 0; c0 < C; c0 += Q) {  // C is the same for the whole warp
+            int lc[Q];
+            Real lv[Q];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-            const int p = p0 + d * NG;
-            if (p < T && !dead) {
-                Real acc = Real(0);
-                const int L = pr_len[d];
-#pragma unroll
-                for (int k = 0; k < P; ++k) {
-                    if (l + k * G < L && !dead) {
-                        const int c = pr_col[d][k];
-                        int spin = 0;
-                        while (flag[c] == 0) {
-                            if (abort_flag) { dead = true; break; }
-                            if (++spin > S2L_SPIN_LIMIT) {
-                                abort_flag = 1;
-                                atomicExch(a.err, 1);
-                                dead = true;
-                                break;
-                            }
-                        }
-                        acc += pr_val[d][k] * x[c];
-                    }
+            for (int q = 0; q < Q; ++q) {
+                lc[q] = -1;
+                lv[q] = Real(0);
+                if (c0 + q < C) {
+                    const int64_t e = eo + (int64_t)(c0 + q) * 32 + lane;
+                    lc[q] = F.col[e];
+                    lv[q] = F.val[e];
                 }
-                // entries beyond the prefetched chunks: the next Q chunks are loaded together (their
-                // lines were hinted into L2 when the row was queued), the rest one chunk at a time
-                constexpr int Q = S2L_LATE_CHUNKS;
-                int lc[Q];
-                Real lv[Q];
+            }
+            // hint the next batch into L2: lane q < Q takes chunk q of it (lines of 128 bytes)
+            if (lane < Q && c0 + Q + lane < C) {
+                const int64_t e = eo + (int64_t)(c0 + Q + lane) * 32;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F.col + e));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e));
+                if (sizeof(Real) == 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e + 16));
+            }
 #pragma unroll
-                for (int k = 0; k < Q; ++k) {
-                    lc[k] = 0;
-                    lv[k] = Real(0);
-                    const int e = l + (P + k) * G;
-                    if (e < L) {
-                        lc[k] = F.col[pr_st[d] + e];
-                        lv[k] = F.val[pr_st[d] + e];
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < Q; ++k) {
-                    if (l + (P + k) * G < L && !dead) {
-                        const int c = lc[k];
-                        int spin = 0;
-                        while (flag[c] == 0) {
-                            if (abort_flag) { dead = true; break; }
-                            if (++spin > S2L_SPIN_LIMIT) {
-                                abort_flag = 1;
-                                atomicExch(a.err, 1);
-                                dead = true;
-                                break;
-                            }
-                        }
-                        acc += lv[k] * x[c];
-                    }
-                }
-                for (int e = l + (P + Q) * G; e < L && !dead; e += G) {
-                    const int c = F.col[pr_st[d] + e];
-                    const Real v = F.val[pr_st[d] + e];
+            for (int q = 0; q < Q; ++q) {
+                const int c = lc[q];
+                if (c >= 0 && !dead) {
                     int spin = 0;
                     while (flag[c] == 0) {
                         if (abort_flag) { dead = true; break; }
@@ -403,41 +387,18 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                             break;
                         }
                     }
-                    acc += v * x[c];
-                }
-                {
-                    const unsigned gmask =
-                        (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-                    dead = __any_sync(gmask, dead);  // one decision per group before its shuffles
-                }
-                acc = group_reduce<Real, G>(acc);
-                if (l == 0 && !dead) {
-                    x[p] = (x[p] - acc) * pr_dinv[d];
-                    __threadfence_block();
-                    flag[p] = 1;
-                }
-                // refill this prefetch slot with the group's row D rows ahead
-                const int q = p + D * NG;
-                if (q < T) {
-                    const int Lq = lens[q];
-                    pr_len[d] = Lq;
-                    pr_st[d] = nst;
-                    pr_dinv[d] = F.dinv[lo + q];
-#pragma unroll
-                    for (int k = 0; k < P; ++k)
-                        if (l + k * G < Lq) {
-                            pr_col[d][k] = F.col[nst + l + k * G];
-                            pr_val[d][k] = F.val[nst + l + k * G];
-                        }
-                    // hint the row's later chunks into L2 (one lane per chunk, lines of 128 bytes)
-                    for (int k = P; l == 0 && k * G < Lq && k < P + S2L_LATE_CHUNKS; ++k) {
-                        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.col + nst + k * G));
-                        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + nst + k * G));
-                        if (sizeof(Real) * G > 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + nst + k * G + 16));
-                    }
-                    nst += Lq;
+                    acc += lv[q] * x[c];
                 }
             }
+        }
+        eo += (int64_t)C * 32;
+        dead = __any_sync(0xffffffffu, dead);  // one decision per warp before its shuffles
+        if (dead) break;
+        for (int o = (1 << gl2) >> 1; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, 1 << gl2);
+        if ((lane & ((1 << gl2) - 1)) == 0 && slot >= 0) {
+            x[slot] = x[slot] - acc;
+            __threadfence_block();
+            flag[slot] = 1;
         }
     }
     __syncthreads();
@@ -682,6 +643,20 @@ void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, c
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
 }
 
+void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
+               double* out)
+{
+    l1_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, a, alpha, c, partials);
+    reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
+}
+
+void launch_gemv_l1(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* q, double* partials,
+                    double* out)
+{
+    gemv_l1_kernel<<<S2L_NB_RED, 256, 0, st>>>(n, V, ldv, k, q, partials);
+    reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 1, out);
+}
+
 void launch_bicg_p(cudaStream_t st, int64_t n, const double* r, const double* v, double beta, double omega, double* p,
                    int first)
 {
@@ -703,19 +678,24 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
 }
 
-template <typename Real, int G>
-cudaError_t launch_sweeps_g(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
-                            int tr_count, int us_first, int us_count, int* launches)
+template <typename Real>
+cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
+                               int tr_count, int us_first, int us_count, int* launches)
 {
     cudaError_t e;
     if (smem > 0) {
-        e = cudaFuncSetAttribute(sweep_kernel<Real, G, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        // the limit is a process-wide attribute of the kernel: always the same cap, so launches of
+        // setups with different shared-memory sizes from several threads cannot undercut each other
+        if (smem > S2L_SWEEP_SMEM_CAP) return cudaErrorInvalidValue;
+        e = cudaFuncSetAttribute(sweep_kernel<Real, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 S2L_SWEEP_SMEM_CAP);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(sweep_kernel<Real, G, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(sweep_kernel<Real, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 S2L_SWEEP_SMEM_CAP);
         if (e != cudaSuccess) return e;
-        sweep_kernel<Real, G, true, true><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
+        sweep_kernel<Real, true, true><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
     } else {
-        sweep_kernel<Real, G, false, true><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
+        sweep_kernel<Real, false, true><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
     }
     int nl = 1;
     if (tr_count > 0) {
@@ -730,28 +710,17 @@ cudaError_t launch_sweeps_g(cudaStream_t st, const LocalSolveArgs<Real>& a, int 
         nl += 1;
     }
     if (smem > 0)
-        sweep_kernel<Real, G, true, false><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
+        sweep_kernel<Real, true, false><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
     else
-        sweep_kernel<Real, G, false, false><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
+        sweep_kernel<Real, false, false><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
     *launches = nl + 1;
     return cudaGetLastError();
 }
 
-template <typename Real>
-cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem_bytes,
-                               int group, int tr_first, int tr_count, int us_first, int us_count, int* launches)
-{
-    switch (group) {
-    case 8: return launch_sweeps_g<Real, 8>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
-    case 16: return launch_sweeps_g<Real, 16>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
-    default: return launch_sweeps_g<Real, 32>(st, a, nblocks, smem_bytes, tr_first, tr_count, us_first, us_count, launches);
-    }
-}
-
 template cudaError_t launch_local_solve<double>(cudaStream_t, const LocalSolveArgs<double>&, int, size_t, int, int, int,
-                                                int, int, int*);
+                                                int, int*);
 template cudaError_t launch_local_solve<float>(cudaStream_t, const LocalSolveArgs<float>&, int, size_t, int, int, int,
-                                               int, int, int*);
+                                                int, int*);
 
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n)
 {

@@ -18,14 +18,16 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define S2L_BS_SWEEP 512      // threads of a sparse-sweep CTA (one CTA per subdomain)
+#define S2L_BS_SWEEP 1024    // threads of a sweep CTA (one CTA per subdomain)
 #define S2L_BS_VEC 256        // threads of the vector / SpMV kernels
 #define S2L_NB_RED 592        // blocks of every kernel that produces reduction partials (4 x 148 SMs)
 #define S2L_MAX_RED_COLS 128  // columns of the reduction buffer
 #define S2L_TILE_ROWS 256     // rows of one coarse restrict/prolong tile
-#define S2L_PREFETCH 4        // rows prefetched per group in a sparse sweep
-#define S2L_PREFETCH_CHUNKS 2 // entries prefetched per lane and row (chunks of G)
-#define S2L_LATE_CHUNKS 6     // further chunks of a row loaded together when the row is processed
+#define S2L_SWEEP_WARPS (S2L_BS_SWEEP / 32)
+#define S2L_BATCH_CHUNKS 8    // chunks of a task loaded together (all loads issued before the first wait)
+#define S2L_CHAIN_DEFAULT 8   // rows of a chain block (setup option "chain_block")
+#define S2L_CHAIN_MAX 16
+#define S2L_SWEEP_SMEM_CAP (227 * 1024 - 64)  // dynamic shared memory of a sweep CTA, at most
 #define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {
@@ -52,11 +54,21 @@ struct DevSub {
 // adding the lengths of its previous rows, without a load from memory.
 template <typename Real>
 struct SweepFactor {
-    const int32_t* col;        // column slots, group-contiguous
-    const Real* val;
-    const Real* dinv;          // per slot (local space layout)
-    const uint16_t* len;       // row length per slot (local space layout)
-    const int64_t* gstart;     // first entry of group g of subdomain i: gstart[i * NG + g]
+    const int32_t* col;        // column slots (-1: padding), per warp, each task lane-interleaved
+    const Real* val;           // values times 1/diag of their row
+    const Real* dinv;          // per slot (local space layout); the right-hand side is scaled by it
+    const uint32_t* thdr;      // per task: chunks C (bits 0-15), log2 G (16-18), rows R - 1 (19-23)
+    const int32_t* tslot;      // per task: its R slots
+    const int64_t* wtask;      // per (subdomain, warp), plus one: first task
+    const int64_t* wslot;      //   first entry of the slot lists
+    const int64_t* went;       //   first entry of col / val
+    // chain blocks: blocks blk_first[i] .. blk_first[i + 1] of subdomain i; block b has the slots
+    // blk_slot[blk_off[b] .. blk_off[b + 1]) (solve order) and W^-1 packed at blk_inv + blk_ioff[b]
+    const int32_t* blk_first;
+    const int64_t* blk_off;
+    const int64_t* blk_ioff;
+    const int32_t* blk_slot;
+    const Real* blk_inv;
 };
 
 template <typename Real>
@@ -106,6 +118,12 @@ void launch_gemv(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k
 void launch_axpby(cudaStream_t st, int64_t n, double a, const double* x, double b, double* y);
 void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, const double* z, double* partials,
                  double* out);
+// out[0] = sum |a - alpha c| (c may be nullptr), out[1] = sum a
+void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
+               double* out);
+// out[0] = sum |V(:, 0:k) q|
+void launch_gemv_l1(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k, const double* q, double* partials,
+                    double* out);
 void launch_bicg_p(cudaStream_t st, int64_t n, const double* r, const double* v, double beta, double omega, double* p,
                    int first);
 void launch_bicg_s(cudaStream_t st, int64_t n, const double* r, const double* v, double alpha, double* s,
@@ -119,7 +137,7 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
 // kernels (first, count); `launches` receives the number of kernels issued.
 template <typename Real>
 cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem_bytes,
-                               int group, int tr_first, int tr_count, int us_first, int us_count, int* launches);
+                               int tr_first, int tr_count, int us_first, int us_count, int* launches);
 
 void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int32_t* cp_pos, const double* cp_w,
                     const double* ylocal, const double* base, double* out);

@@ -200,7 +200,6 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
         displs_[p] = (int)sys.ownership[p];
     }
     if (cfg.local_approx != "none") throw std::invalid_argument("the GPU solve phase needs exact local factors (--local-approx none)");
-    if (cfg.stop_norm != "l2") throw std::invalid_argument("the GPU solve phase implements the L2 stopping test only");
 
     // ---- this rank's part
     Blob blob;
@@ -395,10 +394,11 @@ solv::KrylovResult GpuKrylov::solve(const linalg::DistributedMatrix&, const prec
     ph.gather(x, xg);
     s2l_result res{};
     std::vector<double> hist((size_t)maxit_ + 8);
-    double meta[6] = {0, 0, 0, 0, 0, 0};
+    double meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int st = S2L_OK;
     if (ph.rank() == 0) {
-        s2l_krylov_opts o{restart_, rtol_, maxit_, flexible_ ? 1 : 0, strict_ ? 1 : 0, (int)hist.size()};
+        s2l_krylov_opts o{restart_, rtol_, maxit_, flexible_ ? 1 : 0, strict_ ? 1 : 0, (int)hist.size(),
+                          stop_ == solv::StopNorm::OpenFOAM ? S2L_STOP_OPENFOAM : S2L_STOP_L2, atol_};
         res.history = hist.data();
         st = method_ == "bicgstab" ? s2l_gpu_bicgstab(ph.setup(), bg.data(), xg.data(), S2L_PTR_HOST, &o, &res)
                                    : s2l_gpu_gmres(ph.setup(), bg.data(), xg.data(), S2L_PTR_HOST, &o, &res);
@@ -408,10 +408,12 @@ solv::KrylovResult GpuKrylov::solve(const linalg::DistributedMatrix&, const prec
         meta[3] = res.restarts;
         meta[4] = res.rel_residual;
         meta[5] = res.true_rel_residual;
+        meta[6] = res.initial_residual_of;
+        meta[7] = res.final_residual_of;
     }
     ph.check(st, "GPU Krylov solve");
     int hl = res.history_len;
-    MPI_Bcast(meta, 6, MPI_DOUBLE, 0, ph.comm());
+    MPI_Bcast(meta, 8, MPI_DOUBLE, 0, ph.comm());
     MPI_Bcast(&hl, 1, MPI_INT, 0, ph.comm());
     MPI_Bcast(hist.data(), hl, MPI_DOUBLE, 0, ph.comm());
     ph.scatter(xg, x);
@@ -422,6 +424,8 @@ solv::KrylovResult GpuKrylov::solve(const linalg::DistributedMatrix&, const prec
     out.restarts = (int)meta[3];
     out.rel_residual = meta[4];
     out.true_rel_residual = meta[5];
+    out.initial_residual_of = meta[6];
+    out.final_residual_of = meta[7];
     out.history.assign(hist.begin(), hist.begin() + hl);
     return out;
 }
@@ -432,12 +436,20 @@ std::string GpuKrylov::name() const
     return (flexible_ ? "FGMRES(" : "GMRES(") + std::to_string(restart_) + ") (B200)";
 }
 
-std::unique_ptr<solv::KrylovSolver> makeGpuKrylovSolver(const core::SolverConfig& cfg)
+std::unique_ptr<solv::KrylovSolver> makeGpuKrylovSolver(const core::SolverConfig& cfg, double rtol, double atol)
 {
-    if (cfg.stop_norm != "l2" || cfg.atol > 0.0) throw std::invalid_argument("the GPU solvers implement the L2 test only");
+    const solv::StopNorm stop = solv::parseStopNorm(cfg.stop_norm);
+    if (atol > 0.0 && stop != solv::StopNorm::OpenFOAM)
+        throw std::invalid_argument("an absolute tolerance needs the OpenFOAM stopping norm");
     if (cfg.krylov != "gmres" && cfg.krylov != "bicgstab") throw std::invalid_argument("unknown Krylov solver " + cfg.krylov);
     const bool single = cfg.local_precision == "single";
-    return std::make_unique<GpuKrylov>(cfg.krylov, cfg.restart, cfg.rtol, cfg.maxit, single && cfg.krylov == "gmres", single);
+    return std::make_unique<GpuKrylov>(cfg.krylov, cfg.restart, rtol, cfg.maxit, single && cfg.krylov == "gmres", single,
+                                       stop, atol);
+}
+
+std::unique_ptr<solv::KrylovSolver> makeGpuKrylovSolver(const core::SolverConfig& cfg)
+{
+    return makeGpuKrylovSolver(cfg, cfg.rtol, cfg.atol);
 }
 
 }  // namespace s2l::dropin

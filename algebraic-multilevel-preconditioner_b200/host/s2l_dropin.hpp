@@ -91,9 +91,10 @@ private:
 /// @brief Right-preconditioned GMRES(m) or BiCGStab with every step on the GPU.
 class GpuKrylov final : public schwarz2lvl::solv::KrylovSolver {
 public:
-    GpuKrylov(std::string method, int restart, double rtol, int maxit, bool flexible, bool strict)
+    GpuKrylov(std::string method, int restart, double rtol, int maxit, bool flexible, bool strict,
+              schwarz2lvl::solv::StopNorm stop = schwarz2lvl::solv::StopNorm::L2, double atol = 0.0)
         : method_(std::move(method)), restart_(restart), rtol_(rtol), maxit_(maxit), flexible_(flexible),
-          strict_(strict) {}
+          strict_(strict), stop_(stop), atol_(atol) {}
     /// @brief M must be a GpuTwoLevelSchwarz (std::invalid_argument otherwise).
     schwarz2lvl::solv::KrylovResult solve(const schwarz2lvl::linalg::DistributedMatrix& A,
                                           const schwarz2lvl::prec::Preconditioner& M,
@@ -106,12 +107,19 @@ private:
     double rtol_;
     int maxit_;
     bool flexible_, strict_;
+    schwarz2lvl::solv::StopNorm stop_;
+    double atol_;
 };
 
-/// @brief The GPU counterpart of solv::makeKrylovSolver(cfg): --krylov gmres|bicgstab, --restart,
-///        --rtol, --maxit; FP32 local factors (--local-precision single) select flexible GMRES with
-///        an FP64 true-residual acceptance.  Only the L2 stopping norm is available on the GPU.
+/// @brief The GPU counterpart of solv::makeKrylovSolver(cfg) (src/solver/krylov.cpp:23-36):
+///        --krylov gmres|bicgstab, --restart, --rtol, --atol, --maxit, --stop-norm l2|openfoam; FP32
+///        local factors (--local-precision single) select flexible GMRES with an FP64 true-residual
+///        acceptance.
 std::unique_ptr<schwarz2lvl::solv::KrylovSolver> makeGpuKrylovSolver(const schwarz2lvl::core::SolverConfig& cfg);
+/// @brief Same, with the tolerances @p rtol and @p atol instead of those of @p cfg (e.g. the last
+///        corrector), as solv::makeKrylovSolver(cfg, rtol, atol).
+std::unique_ptr<schwarz2lvl::solv::KrylovSolver> makeGpuKrylovSolver(const schwarz2lvl::core::SolverConfig& cfg,
+                                                                     double rtol, double atol);
 
 }  // namespace s2l::dropin
 

@@ -30,19 +30,25 @@ EXPORTED = [
     "s2l_gpu_setup_bytes", "s2l_gpu_spmv", "s2l_gpu_local_solve", "s2l_gpu_coarse_apply",
     "s2l_gpu_one_level_apply", "s2l_gpu_apply", "s2l_gpu_gmres", "s2l_gpu_bicgstab", "s2l_gpu_set_stream",
     "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes", "s2l_gpu_setup_option",
-    "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc",
+    "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
+    "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
+    "s2l_gpu_ticket_free",
 ]
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
+ERR_TIMEOUT, ERR_CANCELED = 5, 8
 
 
 class KrylovOpts(C.Structure):
     _fields_ = [("restart", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int), ("flexible", C.c_int),
-                ("strict_true_residual", C.c_int), ("history_cap", C.c_int)]
+                ("strict_true_residual", C.c_int), ("history_cap", C.c_int), ("stop_norm", C.c_int),
+                ("atol", C.c_double)]
 
 
 class Result(C.Structure):
     _fields_ = [("converged", C.c_int), ("breakdown", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
                 ("rel_residual", C.c_double), ("true_rel_residual", C.c_double), ("history_len", C.c_int),
-                ("history", C.POINTER(C.c_double))]
+                ("history", C.POINTER(C.c_double)), ("initial_residual_of", C.c_double),
+                ("final_residual_of", C.c_double)]
 
 
 class S2LError(RuntimeError):
@@ -92,6 +98,16 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_setup_option": ([vp, C.c_char_p, C.c_double], C.c_int),
         "s2l_gpu_setup_stat": ([vp, C.c_char_p, dp], C.c_int),
         "s2l_gpu_coarse_apply_noalloc": ([vp, vp, vp], C.c_int),
+        "s2l_gpu_solve_batch": ([vp, C.c_int, C.c_int, C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(KrylovOpts),
+                                 C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
+        "s2l_gpu_serve_start": ([vp, C.c_int], C.c_int),
+        "s2l_gpu_submit": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result), C.POINTER(vp)],
+                           C.c_int),
+        "s2l_gpu_poll": ([vp, C.POINTER(C.c_int)], C.c_int),
+        "s2l_gpu_wait": ([vp, C.c_double, C.POINTER(C.c_int)], C.c_int),
+        "s2l_gpu_cancel": ([vp], C.c_int),
+        "s2l_gpu_ticket_info": ([vp, dp, dp, C.POINTER(C.c_char_p)], C.c_int),
+        "s2l_gpu_ticket_free": ([vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -128,6 +144,10 @@ class Context:
         if rc != S2L_OK:
             raise S2LError(rc, self.error())
 
+    def serve_start(self, workers: int = 4):
+        """Start the native worker threads of the asynchronous solves (GpuSetup.submit)."""
+        self.check(self.lib.s2l_gpu_serve_start(self.h, workers))
+
     def close(self):
         if self.h:
             self.lib.s2l_gpu_destroy(self.h)
@@ -136,6 +156,56 @@ class Context:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+def _result_dict(res: "Result", hist: np.ndarray) -> dict:
+    return {"converged": bool(res.converged), "breakdown": bool(res.breakdown), "iterations": res.iterations,
+            "restarts": res.restarts, "rel_residual": res.rel_residual, "true_rel_residual": res.true_rel_residual,
+            "history": hist[:res.history_len].copy(), "initial_residual_of": res.initial_residual_of,
+            "final_residual_of": res.final_residual_of}
+
+
+class Ticket:
+    """An asynchronous solve (s2l_gpu_submit); keeps b, x and the result buffers alive until freed."""
+
+    def __init__(self, setup: "GpuSetup", h, keep):
+        self.setup, self.lib, self.h, self._keep = setup, setup.lib, h, keep
+
+    def state(self) -> int:
+        v = C.c_int()
+        self.setup.ctx.check(self.lib.s2l_gpu_poll(self.h, C.byref(v)))
+        return v.value
+
+    def cancel(self):
+        self.lib.s2l_gpu_cancel(self.h)
+
+    def wait(self, timeout: float = -1.0):
+        """(x, result dict, status) once finished; raises TimeoutError if not finished in time."""
+        st = C.c_int()
+        rc = self.lib.s2l_gpu_wait(self.h, timeout, C.byref(st))
+        if rc == ERR_TIMEOUT:
+            raise TimeoutError("solve not finished")
+        self.setup.ctx.check(rc)
+        x, res, hist = self._keep["x"], self._keep["res"], self._keep["hist"]
+        return x, _result_dict(res, hist), st.value
+
+    def info(self) -> dict:
+        q, r, e = C.c_double(), C.c_double(), C.c_char_p()
+        self.setup.ctx.check(self.lib.s2l_gpu_ticket_info(self.h, C.byref(q), C.byref(r), C.byref(e)))
+        return {"queue_ms": q.value, "run_ms": r.value, "error": (e.value or b"").decode()}
+
+    def free(self):
+        if self.h is not None and self.lib.s2l_gpu_ticket_free(self.h) == S2L_OK:
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h is not None:
+                self.cancel()
+                self.lib.s2l_gpu_wait(self.h, -1.0, None)
+                self.free()
         except Exception:
             pass
 
@@ -249,8 +319,12 @@ class GpuSetup:
         self.ctx.check(self.lib.s2l_gpu_local_solve(self.h, i, _vp(b), _vp(x), PTR_HOST))
         return x
 
-    def _krylov(self, fn, b, x0, restart, rtol, maxit, flexible, strict, history_cap, device_out=None):
-        o = KrylovOpts(restart, rtol, maxit, 1 if flexible else 0, 1 if strict else 0, history_cap)
+    STOP = {"l2": 0, "openfoam": 1}
+
+    def _krylov(self, fn, b, x0, restart, rtol, maxit, flexible, strict, history_cap, device_out=None,
+                stop_norm="l2", atol=0.0):
+        o = KrylovOpts(restart, rtol, maxit, 1 if flexible else 0, 1 if strict else 0, history_cap,
+                       self.STOP[stop_norm], atol)
         hist = np.zeros(max(history_cap, 1))
         res = Result()
         res.history = _p(hist, C.c_double)
@@ -268,17 +342,58 @@ class GpuSetup:
             self.ctx.check(fn(self.h, _vp(b), _vp(x), PTR_HOST, C.byref(o), C.byref(res)))
         out = {"converged": bool(res.converged), "breakdown": bool(res.breakdown), "iterations": res.iterations,
                "restarts": res.restarts, "rel_residual": res.rel_residual,
-               "true_rel_residual": res.true_rel_residual, "history": hist[:res.history_len].copy()}
+               "true_rel_residual": res.true_rel_residual, "history": hist[:res.history_len].copy(),
+               "initial_residual_of": res.initial_residual_of, "final_residual_of": res.final_residual_of}
         return x, out
 
     def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False, history_cap=4096,
-              device_out=None):
+              device_out=None, stop_norm="l2", atol=0.0):
         return self._krylov(self.lib.s2l_gpu_gmres, b, x0, restart, rtol, maxit, flexible, strict, history_cap,
-                            device_out)
+                            device_out, stop_norm, atol)
 
-    def bicgstab(self, b, x0=None, rtol=1e-8, maxit=1000, strict=False, history_cap=4096, device_out=None):
+    def bicgstab(self, b, x0=None, rtol=1e-8, maxit=1000, strict=False, history_cap=4096, device_out=None,
+                 stop_norm="l2", atol=0.0):
         return self._krylov(self.lib.s2l_gpu_bicgstab, b, x0, 1, rtol, maxit, False, strict, history_cap,
-                            device_out)
+                            device_out, stop_norm, atol)
+
+    METHOD = {"gmres": 0, "bicgstab": 1}
+
+    def _opts(self, restart, rtol, maxit, flexible, strict, history_cap, stop_norm, atol):
+        return KrylovOpts(restart, rtol, maxit, 1 if flexible else 0, 1 if strict else 0, history_cap,
+                          self.STOP[stop_norm], atol)
+
+    def solve_batch(self, bs, method="gmres", restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False,
+                    history_cap=4096, stop_norm="l2", atol=0.0, x0s=None):
+        """k solves at once (s2l_gpu_solve_batch) from host vectors: list of (x, result dict, status)."""
+        k = len(bs)
+        bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+        xs = [np.zeros(self.n) if x0s is None else np.array(x0s[j], dtype=np.float64) for j in range(k)]
+        o = self._opts(restart, rtol, maxit, flexible, strict, history_cap, stop_norm, atol)
+        res = (Result * k)()
+        hists = [np.zeros(max(history_cap, 1)) for _ in range(k)]
+        for j in range(k):
+            res[j].history = _p(hists[j], C.c_double)
+        pb = (C.c_void_p * k)(*[b.ctypes.data for b in bs])
+        px = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
+        st = (C.c_int * k)()
+        rc = self.lib.s2l_gpu_solve_batch(self.h, self.METHOD[method], k, pb, px, PTR_HOST, C.byref(o), res, st)
+        if rc != S2L_OK and all(v == S2L_OK for v in st):
+            self.ctx.check(rc)
+        return [(xs[j], _result_dict(res[j], hists[j]), st[j]) for j in range(k)]
+
+    def submit(self, b, x0=None, method="gmres", restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False,
+               history_cap=4096, stop_norm="l2", atol=0.0) -> Ticket:
+        """Queue one solve on the context's worker threads (Context.serve_start) and return at once."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        o = self._opts(restart, rtol, maxit, flexible, strict, history_cap, stop_norm, atol)
+        hist = np.zeros(max(history_cap, 1))
+        res = Result()
+        res.history = _p(hist, C.c_double)
+        t = C.c_void_p()
+        self.ctx.check(self.lib.s2l_gpu_submit(self.h, self.METHOD[method], _vp(b), _vp(x), PTR_HOST, C.byref(o),
+                                               C.byref(res), C.byref(t)))
+        return Ticket(self, t, {"b": b, "x": x, "res": res, "hist": hist, "opts": o})
 
     def set_stream(self, stream_ptr: int | None):
         self.ctx.check(self.lib.s2l_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))

@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-threads", type=int, default=0, help="reference arm: host threads (0 = all)")
     ap.add_argument("--opt", action="append", default=[], help="device layout option key=value (s2l_gpu_setup_option)")
+    ap.add_argument("--batch", default="2,4,8", help="batched form: right-hand sides solved at once (comma list)")
     return ap.parse_args()
 
 
@@ -213,6 +214,58 @@ def run_ours(a):
             "local_solve_bytes": g.local_solve_bytes(), "clocks": clocks,
             "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
         }
+    # ---- batched form: k right-hand sides solved at once on one setup (k host threads, each call on
+    # its own workspace and stream); a step is one batch, timed from the first call to the last return
+    import threading
+    g, kw = forms["mixed"]
+    batched = {}
+    for k in [int(v) for v in str(a.batch).split(",") if v.strip() and int(v) > 1]:
+        rng = np.random.default_rng(4321)
+        bs = [b_dev] + [torch.tensor(rng.uniform(-1.0, 1.0, n), device=dev) for _ in range(k - 1)]
+        xs = [torch.zeros(n, device=dev, dtype=torch.float64) for _ in range(k)]
+        its_k = [None] * k
+        conv_k = [None] * k
+
+        def one_batch():
+            errs = []
+
+            def body(j):
+                try:
+                    _, r = g.gmres(bs[j].data_ptr(), device_out=xs[j].data_ptr(), **kw)
+                    its_k[j] = r["iterations"]
+                    conv_k[j] = r["converged"] and r["true_rel_residual"] <= wl.rtol
+                except Exception as e:  # re-raised below
+                    errs.append(e)
+
+            for x in xs:
+                x.zero_()
+            torch.cuda.synchronize()
+            ts = [threading.Thread(target=body, args=(j,)) for j in range(k)]
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+            if errs:
+                raise errs[0]
+
+        for _ in range(a.warmup):
+            one_batch()
+        barrier()
+        per_b = []
+        for _ in range(a.steps):
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            one_batch()
+            e_ev.record(stream)  # every call of the batch has returned with its work complete
+            e_ev.synchronize()
+            per_b.append(s_ev.elapsed_time(e_ev))
+        barrier()
+        tot = max_over_ranks(sum(per_b))
+        batched[str(k)] = {"rhs": k, "ms_per_batch": tot / a.steps, "solves_per_s": world * k * a.steps / (tot * 1e-3),
+                           "iterations": list(its_k), "converged": all(conv_k),
+                           "p50_batch_ms": float(np.percentile(per_b, 50)),
+                           "p99_batch_ms": float(np.percentile(per_b, 99))}
+        del bs, xs
     # ---- end to end through the C ABI with pinned host buffers (headline form)
     g, kw = forms["mixed"]
     b_pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -259,13 +312,17 @@ def run_ours(a):
             "setup_s": round(setup_s, 1) if world == 1 else None,
             "layout": {"options": layout, "tail_rows": g64.stat("tail_rows"), "sparse_nnz": g64.stat("sparse_nnz"),
                        "coupling_nnz": g64.stat("coupling_nnz"), "dense_entries": g64.stat("dense_entries"),
-                       "sweep_group": g64.stat("sweep_group")},
+                       "sweep_group": g64.stat("sweep_group"), "levels_max": g64.stat("levels_max"),
+                       "chain_blocks": g64.stat("chain_blocks"), "sweep_tasks": g64.stat("sweep_tasks"),
+                       "sweep_padding": g64.stat("sweep_padding"),
+                       "levels_mean": round(g64.stat("levels_mean"), 1)},
         },
         "forms": {
             "mixed": {k: head[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
                                             "true_rel_residual_host_check", "p50_ms", "p99_ms")},
             "plain_fp64": {k: plain[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
                                                   "true_rel_residual_host_check", "p50_ms", "p99_ms")},
+            "batched_mixed": batched,
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / head["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": head["iterations"][0] - plain["iterations"][0],
         },

@@ -12,8 +12,9 @@
  *  - every call returns S2L_OK (0) or an S2L_ERR_* code; s2l_gpu_last_error() gives the message.
  *    The reference reports the same failures with exceptions (std::invalid_argument for bad
  *    arguments, std::runtime_error for numerical failures, std::logic_error for misuse);
- *  - calls on different setups are independent; calls on one setup are serialised by the caller
- *    (the reference's apply() is not re-entrant either, include/preconditioner/two_level_schwarz.hpp:220);
+ *  - calls on different setups are independent; solve-phase calls on one setup may overlap from
+ *    several host threads, each on a workspace of its own (the reference's apply() is not
+ *    re-entrant, include/preconditioner/two_level_schwarz.hpp:220; this one is);
  *  - pointer arguments of the solve-phase calls are host or device memory, as `ptr_kind` says.
  *    Host pointers are copied in and out on the setup's stream inside the call.
  *
@@ -53,7 +54,8 @@ enum {
     S2L_ERR_NUMERIC = 4,   /* singular coarse matrix, non-finite values (reference: std::runtime_error) */
     S2L_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
     S2L_ERR_BREAKDOWN = 6, /* Krylov breakdown */
-    S2L_ERR_STATE = 7      /* call out of order (reference: std::logic_error) */
+    S2L_ERR_STATE = 7,     /* call out of order (reference: std::logic_error) */
+    S2L_ERR_CANCELED = 8   /* an asynchronous solve was canceled (s2l_gpu_cancel) */
 };
 
 /* preconditioner variants (include/core/config.hpp:61-64) */
@@ -70,6 +72,12 @@ enum { S2L_PTR_HOST = 0, S2L_PTR_DEVICE = 1 };
 
 /* Krylov methods and options (include/core/config.hpp:94-103) */
 enum { S2L_KRYLOV_GMRES = 0, S2L_KRYLOV_BICGSTAB = 1 };
+/* stopping norms (include/solver/krylov.hpp:21-35):
+ *  S2L_STOP_L2:       ||b - A x||_2 <= rtol ||b||_2;
+ *  S2L_STOP_OPENFOAM: sum|b - A x| <= max(rtol sum|b - A x0|, atol F), F the OpenFOAM normalisation
+ *                     factor of x0 (sum|A x0 - xm A 1| + sum|b - xm A 1| + 1e-20, xm = mean of x0);
+ *                     no iteration when x0 already satisfies it. */
+enum { S2L_STOP_L2 = 0, S2L_STOP_OPENFOAM = 1 };
 
 typedef struct {
     int restart;        /* GMRES restart length m */
@@ -79,6 +87,8 @@ typedef struct {
     int strict_true_residual; /* 1: converged only if the recomputed true residual is <= rtol;
                                  0: the reference's 10% slack (src/solver/gmres.cpp:148-156) */
     int history_cap;    /* capacity of result->history (0: no history) */
+    int stop_norm;      /* S2L_STOP_L2 (0) or S2L_STOP_OPENFOAM */
+    double atol;        /* absolute tolerance of the OpenFOAM test (0: none; needs S2L_STOP_OPENFOAM) */
 } s2l_krylov_opts;
 
 typedef struct {
@@ -90,6 +100,8 @@ typedef struct {
     double true_rel_residual; /* ||b - A x|| / ||b|| recomputed in FP64 at the end */
     int history_len;
     double* history;          /* caller-owned, history_cap entries: ||r||/||b|| after every M^-1 */
+    double initial_residual_of; /* OpenFOAM normalised residual of x0 (S2L_STOP_OPENFOAM only) */
+    double final_residual_of;   /* OpenFOAM normalised residual of x, recomputed (S2L_STOP_OPENFOAM only) */
 } s2l_result;
 
 /* ---- context ---------------------------------------------------------------------------- */
@@ -129,7 +141,12 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "tail_min" (rows, default 64), "tail_max" (default 4096): bounds of a non-empty tail;
  *   "tail_rows" (default 0 = cost model): force every subdomain's tail to this many rows;
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
- *   "sweep_group" (0 = automatic, 8, 16 or 32): threads per row in the sparse sweeps.
+ *   "sweep_group" (0 = 32, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
+ *   entries get G lanes, 32 / G rows of one dependency level share a warp);
+ *   "chain_block" (1..16, default 8; 1 = off): rows of a chain block.  Runs of sparse rows where
+ *   each row depends on the one solved just before it (the rows of a supernode) are cut into
+ *   blocks of up to this many rows; a block's rows are stored multiplied by the inverse of its
+ *   diagonal block, so the block is one dependency level of the sweep instead of one per row.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 
@@ -139,7 +156,9 @@ int s2l_gpu_setup_destroy(s2l_setup* s);
 /* Device bytes held by the setup (matrix, factors, basis, schedules) and its workspaces. */
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
 /* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
-   "sweep_group", "smem_bytes". */
+   "sweep_group", "smem_bytes", "levels_max" / "levels_mean" (dependency levels of a sparse sweep,
+   largest and mean over subdomains and both factors), "chain_blocks", "sweep_tasks" and
+   "sweep_padding" (padding entries of the lane-interleaved task layout), both factors. */
 int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 
 /* ---- solve phase ----------------------------------------------------------------------
@@ -184,6 +203,42 @@ int s2l_gpu_gmres(s2l_setup* s, const double* b, double* x, int ptr_kind, const 
                   s2l_result* result);
 int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
                      s2l_result* result);
+
+/* ---- batched and asynchronous solves ------------------------------------------------------
+ * No counterpart in the reference (it solves one right-hand side at a time per process); these
+ * serve several right-hand sides of one matrix, or requests over several matrices, from one GPU.
+ */
+/* k solves of A x_j = b_j on one setup at once, each on its own workspace and stream (k - 1 extra
+ * host threads); returns when all are done.  method: S2L_KRYLOV_GMRES or S2L_KRYLOV_BICGSTAB.
+ * b[j], x[j]: host or device vectors as ptr_kind says; results[j], status[j] per solve; the
+ * return value is the first failing status (or S2L_OK). */
+int s2l_gpu_solve_batch(s2l_setup* s, int method, int k, const double* const* b, double* const* x, int ptr_kind,
+                        const s2l_krylov_opts* opts, s2l_result* results, int* status);
+
+/* Asynchronous solves: s2l_gpu_serve_start starts `workers` native threads on the context; each
+ * s2l_gpu_submit queues one solve (first in, first out) and returns a ticket at once.  b, x,
+ * result (and result->history) stay owned by the caller and must stay valid until the ticket is
+ * finished; opts is copied.  Solves on different setups of the context, and on one setup, run
+ * concurrently up to the number of workers (each holds a workspace of its setup).
+ * s2l_gpu_cancel drops a queued solve, or stops a running one before its next iteration (status
+ * S2L_ERR_CANCELED; x is then unspecified).  s2l_gpu_setup_destroy refuses (S2L_ERR_STATE) while
+ * solves are queued or running on the setup; s2l_gpu_destroy cancels queued solves, waits for
+ * running ones and joins the workers.  A finished ticket is released with s2l_gpu_ticket_free. */
+typedef struct s2l_ticket s2l_ticket;
+enum { S2L_JOB_QUEUED = 0, S2L_JOB_RUNNING = 1, S2L_JOB_DONE = 2, S2L_JOB_CANCELED = 3 };
+int s2l_gpu_serve_start(s2l_ctx* ctx, int workers);
+int s2l_gpu_submit(s2l_setup* s, int method, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
+                   s2l_result* result, s2l_ticket** ticket);
+/* state: S2L_JOB_* */
+int s2l_gpu_poll(s2l_ticket* t, int* state);
+/* Waits until the ticket is finished (timeout_s < 0: no limit); returns S2L_ERR_TIMEOUT if it is
+ * not finished in time, else S2L_OK with the solve's status in *status. */
+int s2l_gpu_wait(s2l_ticket* t, double timeout_s, int* status);
+int s2l_gpu_cancel(s2l_ticket* t);
+/* Time in the queue and running [ms] (host clock, submit to start to finish) and the message of a
+ * failed solve (valid until the ticket is freed). */
+int s2l_gpu_ticket_info(s2l_ticket* t, double* queue_ms, double* run_ms, const char** error);
+int s2l_gpu_ticket_free(s2l_ticket* t);
 
 /* ---- streams and measurement -------------------------------------------------------------- */
 /* Launch on this CUDA stream (cudaStream_t passed as a pointer; NULL = the setup's own stream). */

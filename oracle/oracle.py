@@ -20,7 +20,8 @@ _lib = None
 
 class OResult(C.Structure):
     _fields_ = [("converged", C.c_int), ("breakdown", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
-                ("rel_residual", C.c_double), ("true_rel_residual", C.c_double), ("history_len", C.c_int),
+                ("rel_residual", C.c_double), ("true_rel_residual", C.c_double),
+                ("initial_residual_of", C.c_double), ("final_residual_of", C.c_double), ("history_len", C.c_int),
                 ("history", C.POINTER(C.c_double))]
 
 
@@ -48,9 +49,10 @@ def load():
     for f in ("oracle_spmv", "oracle_one_level", "oracle_coarse_apply", "oracle_apply"):
         getattr(lib, f).argtypes = [vp, vp, vp]
     lib.oracle_local_solve.argtypes = [vp, C.c_int, vp, vp]
-    lib.oracle_gmres.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
-                                 C.POINTER(OResult)]
-    lib.oracle_bicgstab.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(OResult)]
+    lib.oracle_gmres.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_double, C.POINTER(OResult)]
+    lib.oracle_bicgstab.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                    C.POINTER(OResult)]
     _lib = lib
     return lib
 
@@ -134,25 +136,30 @@ class OracleSetup:
     def _res(self, res, hist):
         return {"converged": bool(res.converged), "breakdown": bool(res.breakdown), "iterations": res.iterations,
                 "restarts": res.restarts, "rel_residual": res.rel_residual,
-                "true_rel_residual": res.true_rel_residual, "history": hist[:res.history_len].copy()}
+                "true_rel_residual": res.true_rel_residual, "history": hist[:res.history_len].copy(),
+                "initial_residual_of": res.initial_residual_of, "final_residual_of": res.final_residual_of}
 
-    def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False, history_cap=4096):
+    STOP = {"l2": 0, "openfoam": 1}
+
+    def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False, history_cap=4096,
+              stop_norm="l2", atol=0.0):
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
         hist = np.zeros(history_cap)
         res = OResult()
         res.history = hist.ctypes.data_as(C.POINTER(C.c_double))
         self.lib.oracle_gmres(self.h, _a(b), _a(x), restart, rtol, maxit, int(flexible), int(strict), history_cap,
-                              C.byref(res))
+                              self.STOP[stop_norm], atol, C.byref(res))
         return x, self._res(res, hist)
 
-    def bicgstab(self, b, x0=None, rtol=1e-8, maxit=1000, strict=False, history_cap=4096):
+    def bicgstab(self, b, x0=None, rtol=1e-8, maxit=1000, strict=False, history_cap=4096, stop_norm="l2", atol=0.0):
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
         hist = np.zeros(history_cap)
         res = OResult()
         res.history = hist.ctypes.data_as(C.POINTER(C.c_double))
-        self.lib.oracle_bicgstab(self.h, _a(b), _a(x), rtol, maxit, int(strict), history_cap, C.byref(res))
+        self.lib.oracle_bicgstab(self.h, _a(b), _a(x), rtol, maxit, int(strict), history_cap, self.STOP[stop_norm],
+                                 atol, C.byref(res))
         return x, self._res(res, hist)
 
     def close(self):

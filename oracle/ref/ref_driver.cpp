@@ -480,8 +480,9 @@ int main(int argc, char** argv)
         if (rank == 0) {
             w.vec("krylov_x", gx);
             w.vec("krylov_history", res.history);
-            std::vector<double> meta = {(double)res.iterations, res.converged ? 1.0 : 0.0, res.rel_residual,
-                                        res.true_rel_residual, (double)res.restarts, res.breakdown ? 1.0 : 0.0};
+            std::vector<double> meta = {(double)res.iterations,  res.converged ? 1.0 : 0.0, res.rel_residual,
+                                        res.true_rel_residual,   (double)res.restarts,   res.breakdown ? 1.0 : 0.0,
+                                        res.initial_residual_of, res.final_residual_of};
             w.vec("krylov_meta", meta);
         }
     } catch (const std::exception& e) {

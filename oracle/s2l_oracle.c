@@ -14,8 +14,9 @@
  *   - CoarseSpace::restrict/prolong     src/preconditioner/coarse_space.cpp:208-230
  *   - CoarseSolver::solve (root)        src/preconditioner/coarse_solver.cpp:166-179 (direct solve of E)
  *   - TwoLevelSchwarz::apply            src/preconditioner/two_level_schwarz.cpp:134-163
- *   - Gmres::solve                      src/solver/gmres.cpp:18-161 (L2 stopping test)
- *   - BiCgStab::solve                   src/solver/bicgstab.cpp:15-154 (L2 stopping test)
+ *   - Gmres::solve                      src/solver/gmres.cpp:18-161 (L2 and OpenFOAM stopping tests)
+ *   - BiCgStab::solve                   src/solver/bicgstab.cpp:15-154 (L2 and OpenFOAM stopping tests)
+ *   - detail::openfoamNormFactor        src/solver/krylov.cpp:48-58
  * The factors, coarse basis and coarse matrix are inputs (the setup phase produces them), in the
  * same conventions as include/s2l_gpu.h.  Parity of this restatement with the reference itself is
  * pinned by the golden fixtures under tests/golden/ (generated by running the reference).
@@ -369,6 +370,7 @@ void oracle_apply(OSetup *s, const double *r, double *z)
 typedef struct {
     int converged, breakdown, iterations, restarts;
     double rel_residual, true_rel_residual;
+    double initial_residual_of, final_residual_of; /* OpenFOAM test only (include/solver/krylov.hpp:51-52) */
     int history_len;
     double *history;
 } OResult;
@@ -380,6 +382,38 @@ static double dotv(int64_t n, const double *a, const double *b)
     return t;
 }
 
+static double norm1v(int64_t n, const double *a)
+{
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) t += fabs(a[i]);
+    return t;
+}
+
+/* sum |a - alpha c| */
+static double norm1_diff(int64_t n, const double *a, double alpha, const double *c)
+{
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) t += fabs(a[i] - alpha * c[i]);
+    return t;
+}
+
+/* OpenFOAM normalisation factor of x0 (krylov.cpp:48-58), Ax0 = A x0 */
+static double of_norm_factor(OSetup *s, const double *b, const double *x0, const double *Ax0)
+{
+    int64_t n = s->n;
+    double sum = 0.0;
+    for (int64_t i = 0; i < n; ++i) sum += x0[i];
+    double xm = n > 0 ? sum / (double)n : 0.0;
+    if (xm == 0.0) return norm1v(n, Ax0) + norm1v(n, b) + 1e-20;
+    double *ones = (double *)malloc((size_t)n * sizeof(double)), *rs = (double *)malloc((size_t)n * sizeof(double));
+    for (int64_t i = 0; i < n; ++i) ones[i] = 1.0;
+    oracle_spmv(s, ones, rs);
+    double F = norm1_diff(n, Ax0, xm, rs) + norm1_diff(n, b, xm, rs) + 1e-20;
+    free(ones);
+    free(rs);
+    return F;
+}
+
 static void hpush(OResult *res, int cap, double v)
 {
     if (res->history && res->history_len < cap) res->history[res->history_len] = v;
@@ -387,10 +421,12 @@ static void hpush(OResult *res, int cap, double v)
 }
 
 /* gmres.cpp:18-161; flexible = 1 keeps Z_j (not in the reference), strict = 1 accepts only a true
-   residual <= rtol (the reference accepts 1.1 rtol, gmres.cpp:148-156) */
+   residual <= rtol (the reference accepts 1.1 rtol, gmres.cpp:148-156); stop_norm 1 = OpenFOAM test
+   with absolute tolerance atol (gmres.cpp:41-56, 106-123, 145-150) */
 int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int maxit, int flexible, int strict,
-                 int hist_cap, OResult *res)
+                 int hist_cap, int stop_norm, double atol, OResult *res)
 {
+    const int of = stop_norm == 1;
     int64_t n = s->n;
     memset(res, 0, sizeof(*res) - sizeof(double *));
     res->history_len = 0;
@@ -411,11 +447,21 @@ int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int 
     double *zz = (double *)malloc((size_t)n * sizeof(double)), *u = (double *)malloc((size_t)n * sizeof(double));
 #define HH(i, j) H[(size_t)(j) * (m + 1) + (i)]
     oracle_spmv(s, x, r);
+    double normF = 1.0, l1 = 0.0, thr = 0.0;
+    if (of) normF = of_norm_factor(s, b, x, r);
     for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
     double beta = sqrt(dotv(n, r, r));
     hpush(res, hist_cap, beta / bnorm);
     res->rel_residual = beta / bnorm;
-    int converged = beta <= rtol * bnorm;
+    int converged;
+    if (of) {
+        l1 = norm1v(n, r);
+        res->initial_residual_of = l1 / normF;
+        thr = fmax(rtol * l1, atol * normF);
+        converged = l1 <= thr;
+    } else {
+        converged = beta <= rtol * bnorm;
+    }
     while (!converged && res->iterations < maxit) {
         for (int64_t i = 0; i < n; ++i) V[i] = r[i] / beta;
         memset(g, 0, (size_t)(m + 1) * sizeof(double));
@@ -451,7 +497,33 @@ int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int 
             ++res->iterations;
             res->rel_residual = fabs(g[j + 1]) / bnorm;
             hpush(res, hist_cap, res->rel_residual);
-            if (res->rel_residual <= rtol) { converged = 1; break; }
+            int done;
+            if (of) {
+                /* r_j = g_{j+1} V_{j+2} Q^T e_{j+1} (gmres.cpp:106-123) */
+                if (hn == 0.0 || g[j + 1] == 0.0) {
+                    l1 = 0.0;
+                } else {
+                    double *q = (double *)calloc((size_t)j + 2, sizeof(double));
+                    q[j + 1] = 1.0;
+                    for (int i = j; i >= 0; --i) {
+                        double qa = q[i], qc = q[i + 1];
+                        q[i] = cs[i] * qa - sn[i] * qc;
+                        q[i + 1] = sn[i] * qa + cs[i] * qc;
+                    }
+                    double acc1 = 0.0;
+                    for (int64_t t = 0; t < n; ++t) {
+                        double v = 0.0;
+                        for (int c = 0; c < j + 2; ++c) v += V[(size_t)c * n + t] * q[c];
+                        acc1 += fabs(v);
+                    }
+                    l1 = fabs(g[j + 1]) * acc1;
+                    free(q);
+                }
+                done = l1 <= thr;
+            } else {
+                done = res->rel_residual <= rtol;
+            }
+            if (done) { converged = 1; break; }
             if (hn == 0.0) { breakdown = 1; break; }
         }
         for (int i = k - 1; i >= 0; --i) {
@@ -474,8 +546,10 @@ int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int 
         oracle_spmv(s, x, r);
         for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
         beta = sqrt(dotv(n, r, r));
-        int within = beta <= rtol * bnorm;
-        int within_slack = beta <= (strict ? 1.0 : 1.1) * rtol * bnorm;
+        if (of) l1 = norm1v(n, r);
+        double slack = strict ? 1.0 : 1.1;
+        int within = of ? l1 <= thr : beta <= rtol * bnorm;
+        int within_slack = of ? l1 <= slack * thr : beta <= slack * rtol * bnorm;
         if (breakdown) converged = within || converged;
         if (converged && !within_slack) converged = 0;
         if (beta == 0.0) converged = 1;
@@ -484,14 +558,16 @@ int oracle_gmres(OSetup *s, const double *b, double *x, int m, double rtol, int 
 #undef HH
     res->converged = converged;
     res->true_rel_residual = beta / bnorm;
+    if (of) res->final_residual_of = l1 / normF;
     free(V); free(Z); free(H); free(cs); free(sn); free(g); free(h); free(h2); free(yv); free(r); free(w); free(zz); free(u);
     return 0;
 }
 
-/* bicgstab.cpp:15-154 (L2 test) */
+/* bicgstab.cpp:15-154; stop_norm 1 = OpenFOAM test with absolute tolerance atol (bicgstab.cpp:33-66) */
 int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxit, int strict, int hist_cap,
-                    OResult *res)
+                    int stop_norm, double atol, OResult *res)
 {
+    const int of = stop_norm == 1;
     int64_t n = s->n;
     memset(res, 0, sizeof(*res) - sizeof(double *));
     double bnorm = sqrt(dotv(n, b, b));
@@ -506,12 +582,20 @@ int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxi
     double *v = (double *)calloc((size_t)n, sizeof(double)), *y = (double *)malloc(sz), *sv = (double *)malloc(sz);
     double *z = (double *)malloc(sz), *t = (double *)malloc(sz);
     oracle_spmv(s, x, r);
+    double normF = 1.0, l1 = 0.0, thr = 0.0;
+    if (of) normF = of_norm_factor(s, b, x, r);
     for (int64_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
     double rn = sqrt(dotv(n, r, r));
+    if (of) {
+        l1 = norm1v(n, r);
+        res->initial_residual_of = l1 / normF;
+        thr = fmax(rtol * l1, atol * normF);
+    }
+#define SATISFIED(slack) (of ? l1 <= (slack) * thr : rn <= (slack) * rtol * bnorm)
     hpush(res, hist_cap, rn / bnorm);
     res->rel_residual = rn / bnorm;
     for (;;) {
-        if (rn <= rtol * bnorm) { res->converged = 1; break; }
+        if (SATISFIED(1.0)) { res->converged = 1; break; }
         if (res->iterations >= maxit) break;
         memcpy(rh, r, sz);
         double rhn = rn, rho = rn * rn, rho_old = 1.0, alpha = 1.0, omega = 1.0;
@@ -531,12 +615,13 @@ int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxi
             alpha = rho / rhv;
             for (int64_t i = 0; i < n; ++i) sv[i] = r[i] - alpha * v[i];
             rn = sqrt(dotv(n, sv, sv));
+            if (of) l1 = norm1v(n, sv);
             res->rel_residual = rn / bnorm;
             hpush(res, hist_cap, res->rel_residual);
-            if (rn <= rtol * bnorm || res->iterations >= maxit) {
+            if (SATISFIED(1.0) || res->iterations >= maxit) {
                 for (int64_t i = 0; i < n; ++i) x[i] += alpha * y[i];
                 memcpy(r, sv, sz);
-                candidate = rn <= rtol * bnorm;
+                candidate = SATISFIED(1.0);
                 break;
             }
             oracle_apply(s, sv, z);
@@ -548,20 +633,24 @@ int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxi
             rho_old = rho;
             rn = sqrt(dotv(n, r, r));
             rho = dotv(n, rh, r);
+            if (of) l1 = norm1v(n, r);
             res->rel_residual = rn / bnorm;
             hpush(res, hist_cap, res->rel_residual);
-            if (rn <= rtol * bnorm) { candidate = 1; break; }
+            if (SATISFIED(1.0)) { candidate = 1; break; }
             if (omega == 0.0 || fabs(rho) < 1e-14 * rhn * rn) break;
         }
         oracle_spmv(s, x, t);
         for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
         rn = sqrt(dotv(n, r, r));
+        if (of) l1 = norm1v(n, r);
         if (res->breakdown) break;
-        if (candidate && rn <= (strict ? 1.0 : 1.1) * rtol * bnorm) { res->converged = 1; break; }
+        if (candidate && SATISFIED(strict ? 1.0 : 1.1)) { res->converged = 1; break; }
         if (res->iterations >= maxit) break;
         res->restarts++;
     }
+#undef SATISFIED
     res->true_rel_residual = rn / bnorm;
+    if (of) res->final_residual_of = l1 / normF;
     free(r); free(rh); free(p); free(v); free(y); free(sv); free(z); free(t);
     return 0;
 }

@@ -13,7 +13,8 @@ case below it runs in dump mode and the outputs are packed into <case>.npz:
               DistributedMatrix::apply, OneLevelSchwarz::apply, CoarseSpace::apply and
               Preconditioner::apply of it
   krylov_*    the reference's Krylov solve of A x = b from x0 = 0: x, residual history, and
-              [iterations, converged, rel_residual, true_rel_residual, restarts, breakdown]
+              [iterations, converged, rel_residual, true_rel_residual, restarts, breakdown,
+               initial_residual_of, final_residual_of] (the last two for --stop-norm openfoam)
 
 Run here (where the reference sources are): python tests/golden/make_golden.py
 """
@@ -60,6 +61,16 @@ CASES = {
     "laplace2d_ras_deflated_ldlt": (2, ["--generate", "laplace2d", "--nx", "16", "--pou", "boolean",
                                         "--one-level", "ras", "--coarse", "deflated", "--nev", "6",
                                         "--local-factorization", "ldlt", "--restart", "30"]),
+    # OpenFOAM stopping norm (relTol semantics), GMRES on the bubbly-pressure family
+    "bubbles3d_gmres_openfoam": (4, ["--generate", "bubbles3d", "--nx", "12", "--nbubbles", "6", "--radius", "0.15",
+                                     "--rho-ratio", "1000", "--pou", "boolean", "--one-level", "ras", "--coarse",
+                                     "deflated", "--nev", "10", "--local-factorization", "cholesky", "--restart",
+                                     "20", "--stop-norm", "openfoam", "--rtol", "1e-6"]),
+    # OpenFOAM norm with an absolute tolerance only (relTol 0), BiCGStab, two-level additive
+    "laplace2d_bicgstab_openfoam_atol": (3, ["--generate", "laplace2d", "--nx", "20", "--pou", "boolean",
+                                             "--one-level", "ras", "--coarse", "additive", "--nev", "6",
+                                             "--local-factorization", "lu", "--krylov", "bicgstab", "--stop-norm",
+                                             "openfoam", "--rtol", "0", "--atol", "1e-9"]),
 }
 
 

@@ -19,7 +19,9 @@ def cases():
 
 
 def _flag(cmd: list, name: str, default: str) -> str:
-    return cmd[cmd.index(name) + 1] if name in cmd else default
+    """Value of the last occurrence of a flag (the reference's parser keeps the last one)."""
+    idx = [i for i, a in enumerate(cmd) if a == name]
+    return cmd[idx[-1] + 1] if idx else default
 
 
 def load(name: str):
@@ -53,7 +55,11 @@ def load(name: str):
     krylov = {"method": _flag(cmd, "--krylov", "gmres"), "restart": int(_flag(cmd, "--restart", "30")),
               "rtol": float(_flag(cmd, "--rtol", "1e-8")), "x": d["krylov_x"], "history": d["krylov_history"],
               "iterations": int(d["krylov_meta"][0]), "converged": bool(d["krylov_meta"][1]),
-              "true_rel_residual": float(d["krylov_meta"][3])}
+              "true_rel_residual": float(d["krylov_meta"][3]),
+              "stop_norm": _flag(cmd, "--stop-norm", "l2"), "atol": float(_flag(cmd, "--atol", "0"))}
+    if d["krylov_meta"].size >= 8:  # OpenFOAM normalised residuals (include/solver/krylov.hpp:51-52)
+        krylov["initial_residual_of"] = float(d["krylov_meta"][6])
+        krylov["final_residual_of"] = float(d["krylov_meta"][7])
     applies = []
     k = 0
     while f"apply{k}_r" in d:

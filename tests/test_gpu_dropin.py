@@ -3,7 +3,8 @@
 oracle/_ref/dropin_check builds, on thread-ranks, the reference's own preconditioner and Krylov
 solver and the drop-in GpuTwoLevelSchwarz / GpuKrylov from the same set-up objects, and compares
 Preconditioner::apply (1e-12 FP64, 1e-5 FP32 factors) and KrylovSolver::solve (iterations within
-+-1, GPU true residual <= 1.1 rtol).  The binary is built where the reference sources are
++-1; GPU true residual <= 1.1 rtol, or with --stop-norm openfoam the normalised residual <= 1.1
+max(rtol x initial, atol) and the initial one equal to the reference's).  The binary is built where the reference sources are
 (oracle/ref/Makefile) and travels with the repository copy.
 """
 import json
@@ -27,6 +28,12 @@ CASES = {
                                  "--local-factorization", "lu", "--local-precision", "single", "--restart", "40"]),
     "laplace2d_asm_mult_bicgstab": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--pou",
                                         "multiplicity", "--one-level", "asm", "--krylov", "bicgstab"]),
+    "bubbles3d_gmres_openfoam": (4, ["--generate", "bubbles3d", "--nx", "14", "--nbubbles", "6", "--radius",
+                                     "0.12", "--nev", "10", "--coarse", "deflated", "--local-factorization",
+                                     "cholesky", "--restart", "30", "--stop-norm", "openfoam", "--rtol", "1e-6"]),
+    "laplace2d_bicgstab_openfoam_atol": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--coarse",
+                                             "additive", "--local-factorization", "lu", "--krylov", "bicgstab",
+                                             "--stop-norm", "openfoam", "--rtol", "0", "--atol", "1e-9"]),
 }
 
 

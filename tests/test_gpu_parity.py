@@ -109,6 +109,75 @@ def test_bicgstab_matches_oracle(ctx, name):
     g.close()
 
 
+def _of_residual(st, x, F):
+    """OpenFOAM normalised residual sum|b - A x| / F (include/solver/krylov.hpp:24-34)."""
+    return np.abs(st.b - st.A @ x).sum() / F
+
+
+def _of_factor(st, x0):
+    """OpenFOAM normalisation factor of x0 (src/solver/krylov.cpp:48-58), in numpy."""
+    xm = x0.mean()
+    Ax0 = st.A @ x0
+    if xm == 0.0:
+        return np.abs(Ax0).sum() + np.abs(st.b).sum() + 1e-20
+    rs = st.A @ np.ones(st.n)
+    return np.abs(Ax0 - xm * rs).sum() + np.abs(st.b - xm * rs).sum() + 1e-20
+
+
+@pytest.mark.parametrize("method", ["gmres", "bicgstab"])
+@pytest.mark.parametrize("warm", [False, True])
+@pytest.mark.parametrize("rtol,atol", [(1e-6, 0.0), (0.0, 1e-9), (1e-3, 1e-7)])
+def test_openfoam_stopping_norm_matches_oracle(ctx, method, warm, rtol, atol):
+    """The OpenFOAM test sum|b - A x| <= max(rtol sum|b - A x0|, atol F): GPU and oracle take the
+    same number of iterations and report the same normalised residuals; a warm start x0 != 0
+    exercises the mean-shifted factor F."""
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    x0 = np.random.default_rng(3).uniform(0.0, 0.2, st.n) if warm else np.zeros(st.n)
+    kw = dict(rtol=rtol, stop_norm="openfoam", atol=atol)
+    if method == "gmres":
+        x, res = g.gmres(st.b, x0=x0.copy(), restart=w.restart, **kw)
+        xo, reso = o.gmres(st.b, x0=x0.copy(), restart=w.restart, **kw)
+    else:
+        x, res = g.bicgstab(st.b, x0=x0.copy(), **kw)
+        xo, reso = o.bicgstab(st.b, x0=x0.copy(), **kw)
+    assert res["converged"] and reso["converged"]
+    assert res["iterations"] == reso["iterations"]
+    F = _of_factor(st, x0)
+    assert abs(res["initial_residual_of"] - _of_residual(st, x0, F)) <= 1e-10 * res["initial_residual_of"]
+    assert abs(res["initial_residual_of"] - reso["initial_residual_of"]) <= 1e-12 * reso["initial_residual_of"]
+    fin = _of_residual(st, x, F)
+    # the residual sums of the GPU and of numpy differ by rounding (~1e-16 of sum|A x| / F)
+    assert abs(res["final_residual_of"] - fin) <= 1e-6 * fin + 1e-14
+    assert fin <= 1.1 * max(rtol * res["initial_residual_of"], atol)
+    assert rel(x, xo) <= 1e-8
+    g.close()
+
+
+def test_openfoam_x0_already_converged(ctx):
+    """No iteration when x0 already satisfies the OpenFOAM test (src/solver/gmres.cpp:52)."""
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st)
+    x1, r1 = g.gmres(st.b, restart=w.restart, rtol=1e-10)
+    x2, r2 = g.gmres(st.b, x0=x1.copy(), restart=w.restart, rtol=0.0, stop_norm="openfoam", atol=1e-6)
+    assert r2["converged"] and r2["iterations"] == 0
+    assert np.array_equal(x1, x2)
+    g.close()
+
+
+def test_stop_norm_option_errors(ctx):
+    from s2l_b200.capi import GpuSetup, S2LError
+    w, st = small_setup("poisson2d")
+    g = GpuSetup(ctx, st)
+    with pytest.raises(S2LError) as e:
+        g.gmres(st.b, atol=1e-6)  # an absolute tolerance needs the OpenFOAM norm
+    assert e.value.code == 1 and "OpenFOAM" in str(e.value)
+    g.close()
+
+
 def test_single_precision_factors(ctx, rng):
     from s2l_b200.capi import GpuSetup
     w, st = small_setup("convdiff3d", precision="single")
@@ -172,14 +241,18 @@ LAYOUTS = [
     {"sweep_group": 8, "tail_rows": 17},
     {"sweep_group": 16},
     {"sweep_group": 32, "tail_rows": 3},
+    {"chain_block": 1},                      # no chain blocks
+    {"chain_block": 2, "sweep_group": 8},
+    {"chain_block": 16, "tail_max": 0},      # long chain blocks over the whole factor
+    {"chain_block": 16, "tail_rows": 5, "sweep_group": 16},
 ]
 
 
 @pytest.mark.parametrize("layout", range(len(LAYOUTS)))
 @pytest.mark.parametrize("name", ["poisson2d", "bubbles3d", "convdiff3d"])
 def test_layouts_agree_with_oracle(ctx, rng, name, layout):
-    """Every device layout of the same factors (dense tail split, sweep group width) gives the
-    oracle's local solves and two-level apply to 1e-12."""
+    """Every device layout of the same factors (dense tail split, sweep group width, chain blocks)
+    gives the oracle's local solves and two-level apply to 1e-12."""
     from s2l_b200.capi import GpuSetup
     _, st = small_setup(name)
     opts = LAYOUTS[layout]
@@ -188,6 +261,8 @@ def test_layouts_agree_with_oracle(ctx, rng, name, layout):
         assert g.stat("tail_rows") == opts["tail_rows"] * st.nsub
     if opts.get("tail_max") == 0:
         assert g.stat("tail_rows") == 0
+    if opts.get("chain_block") == 1:
+        assert g.stat("chain_blocks") == 0
     o = OracleSetup(st)
     for i, s in enumerate(st.subdomains):
         b = rng.standard_normal(s.n_local)

@@ -1,0 +1,111 @@
+"""Batched and asynchronous solves (s2l_gpu_solve_batch, s2l_gpu_submit / poll / wait / cancel).
+
+Every solve runs on a workspace of its own, so a solve gives the same bits alone, in a batch and
+through the worker threads; cancellation stops a queued solve before it starts and a running one
+before its next iteration; a setup with queued or running solves refuses to be destroyed.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import small_setup
+
+pytestmark = pytest.mark.gpu
+
+
+def _rhs(n, k, seed=11):
+    rng = np.random.default_rng(seed)
+    return [rng.uniform(-1.0, 1.0, n) for _ in range(k)]
+
+
+@pytest.mark.parametrize("method", ["gmres", "bicgstab"])
+def test_batch_same_bits_as_single_solves(method):
+    from s2l_b200 import capi
+    ctx = capi.Context(0)
+    w, st = small_setup("bubbles3d")
+    g = capi.GpuSetup(ctx, st)
+    bs = _rhs(st.n, 3)
+    kw = dict(rtol=1e-9) if method == "bicgstab" else dict(restart=w.restart, rtol=1e-9)
+    single = [(g.gmres(b, **kw) if method == "gmres" else g.bicgstab(b, **kw)) for b in bs]
+    out = g.solve_batch(bs, method=method, **kw)
+    for (xs, rs), (xb, rb, status) in zip(single, out):
+        assert status == 0 and rb["converged"]
+        assert rb["iterations"] == rs["iterations"]
+        assert np.array_equal(xs, xb)
+    g.close()
+    ctx.close()
+
+
+def test_submit_across_setups_same_bits():
+    from s2l_b200 import capi
+    ctx = capi.Context(0)
+    ctx.serve_start(3)
+    w1, st1 = small_setup("bubbles3d")
+    w2, st2 = small_setup("poisson2d")
+    g1, g2 = capi.GpuSetup(ctx, st1), capi.GpuSetup(ctx, st2)
+    jobs = [(g1, b, "gmres") for b in _rhs(st1.n, 3)] + [(g2, b, "bicgstab") for b in _rhs(st2.n, 2, 12)]
+    alone = [(g.gmres(b, rtol=1e-9) if m == "gmres" else g.bicgstab(b, rtol=1e-9)) for g, b, m in jobs]
+    tickets = [g.submit(b, method=m, rtol=1e-9) for g, b, m in jobs]
+    for t, (xa, ra) in zip(tickets, alone):
+        x, r, status = t.wait(120.0)
+        assert status == 0 and t.state() == capi.JOB_DONE, t.info()["error"]
+        assert r["iterations"] == ra["iterations"] and np.array_equal(x, xa)
+        info = t.info()
+        assert info["queue_ms"] >= 0.0 and info["run_ms"] > 0.0 and info["error"] == ""
+        t.free()
+    g1.close()
+    g2.close()
+    ctx.close()
+
+
+def test_cancel_queued_and_running():
+    from s2l_b200 import capi
+    ctx = capi.Context(0)
+    ctx.serve_start(1)
+    w, st = small_setup("bubbles3d")
+    g = capi.GpuSetup(ctx, st)
+    b = _rhs(st.n, 1)[0]
+    # rtol 0 with the L2 test never converges: the first solve runs until it is canceled
+    long = g.submit(b, restart=w.restart, rtol=0.0, maxit=10**7, history_cap=0)
+    queued = g.submit(b, restart=w.restart, rtol=1e-8)
+    queued.cancel()
+    deadline = time.time() + 30.0
+    while long.state() != capi.JOB_RUNNING and time.time() < deadline:
+        time.sleep(0.01)
+    assert long.state() == capi.JOB_RUNNING
+    with pytest.raises(TimeoutError):
+        long.wait(0.05)
+    # the setup refuses to be destroyed while a solve is queued or running
+    assert g.lib.s2l_gpu_setup_destroy(g.h) == 7
+    long.cancel()
+    _, _, st_long = long.wait(60.0)
+    _, _, st_queued = queued.wait(60.0)
+    assert st_long == capi.ERR_CANCELED and long.state() == capi.JOB_CANCELED
+    assert st_queued == capi.ERR_CANCELED and queued.state() == capi.JOB_CANCELED
+    assert "canceled" in long.info()["error"] and queued.info()["run_ms"] == 0.0
+    # the worker and the setup stay usable
+    x, r, status = g.submit(b, restart=w.restart, rtol=1e-8).wait(60.0)
+    assert status == 0 and r["converged"]
+    assert np.linalg.norm(st.b - st.A @ x) >= 0.0
+    long.free()
+    queued.free()
+    g.close()
+    ctx.close()
+
+
+def test_submit_needs_workers_and_reports_errors():
+    from s2l_b200 import capi
+    ctx = capi.Context(0)
+    w, st = small_setup("poisson2d")
+    g = capi.GpuSetup(ctx, st)
+    with pytest.raises(capi.S2LError) as e:
+        g.submit(st.b)
+    assert e.value.code == 7
+    ctx.serve_start(2)
+    t = g.submit(st.b, atol=1e-6)  # an absolute tolerance needs the OpenFOAM norm: fails in the worker
+    _, _, status = t.wait(60.0)
+    assert status == 1 and "OpenFOAM" in t.info()["error"]
+    t.free()
+    g.close()
+    ctx.close()

@@ -92,3 +92,23 @@ def test_single_precision_factors_flexible_gmres():
     x, res = o.gmres(st.b, restart=w.restart, rtol=1e-8, flexible=True, strict=True)
     assert res["converged"]
     assert np.linalg.norm(st.b - st.A @ x) <= 1e-8 * np.linalg.norm(st.b)
+
+
+@pytest.mark.parametrize("method", ["gmres", "bicgstab"])
+def test_openfoam_norm_warm_start(method):
+    """OpenFOAM test from x0 != 0: the oracle's normalisation factor is the mean-shifted one of
+    src/solver/krylov.cpp:48-58 (the golden fixtures cover x0 = 0), and the final normalised residual
+    meets sum|b - A x| <= rtol sum|b - A x0| (include/solver/krylov.hpp:24-34)."""
+    w, st = small_setup("bubbles3d")
+    o = OracleSetup(st)
+    x0 = np.random.default_rng(3).uniform(0.0, 0.2, st.n)
+    rs = st.A @ np.ones(st.n)
+    xm = x0.mean()
+    F = np.abs(st.A @ x0 - xm * rs).sum() + np.abs(st.b - xm * rs).sum() + 1e-20
+    kw = dict(rtol=1e-6, stop_norm="openfoam")
+    x, res = o.gmres(st.b, x0=x0, restart=w.restart, **kw) if method == "gmres" else o.bicgstab(st.b, x0=x0, **kw)
+    r0 = np.abs(st.b - st.A @ x0).sum()
+    assert abs(res["initial_residual_of"] - r0 / F) <= 1e-12 * r0 / F
+    r1 = np.abs(st.b - st.A @ x).sum()
+    assert res["converged"] and r1 <= 1.1e-6 * r0
+    assert abs(res["final_residual_of"] - r1 / F) <= 1e-9 * r1 / F
