@@ -17,6 +17,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <numeric>
@@ -184,8 +185,11 @@ struct s2l_setup {
     double* d_Einv = nullptr;
     size_t smem_bytes = 0;
     double solve_bytes = 0.0;
+    int max_T = 0;   // largest sparse part of a subdomain (rows)
+    int kc_max = 1;  // right-hand sides a sweep CTA can hold in shared memory (1, 2 or 4)
     // workspaces: one per concurrent solve-phase call (workspace 0 is the caller's default)
     mutable std::mutex wmu;
+    std::condition_variable wcv;  // a workspace came free
     std::vector<s2l_work*> works;
     std::vector<char> busy;
     cudaStream_t user_stream = nullptr;  // s2l_gpu_set_stream: used by workspace 0
@@ -212,6 +216,7 @@ struct s2l_work {
     cudaStream_t stream = nullptr;
     cudaEvent_t join = nullptr;  // orders this workspace's stream after the caller's stream
     std::vector<void*> allocs;
+    std::vector<size_t> alloc_bytes;  // size of each of allocs
     size_t bytes = 0;
     void *d_ybuf = nullptr, *d_xbuf = nullptr;
     uint8_t* d_gflags = nullptr;
@@ -230,6 +235,18 @@ struct s2l_work {
            *d_xk = nullptr, *d_u = nullptr;
     double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
     double* d_coef = nullptr;
+    // block solves (K interleaved right-hand sides), allocated on first use
+    struct Block {
+        int K = 0, m = -1;
+        bool flex = false;
+        void *ybuf = nullptr, *xbuf = nullptr;
+        uint8_t* gflags = nullptr;
+        double *ylocal = nullptr, *plocal = nullptr, *x0 = nullptr, *wv = nullptr, *cpart = nullptr, *c = nullptr,
+               *y = nullptr;
+        double *V = nullptr, *Z = nullptr, *r = nullptr, *z = nullptr, *kw = nullptr, *b = nullptr, *xk = nullptr,
+               *u = nullptr, *coef = nullptr, *scal = nullptr, *part = nullptr, *red = nullptr, *h_red = nullptr;
+        std::vector<void*> allocs;
+    } blk;
     // profiling
     unsigned prof = 0;  // bit c: time kernel class c
     long launches = 0;  // kernel launches issued through this workspace
@@ -755,6 +772,7 @@ int work_alloc(s2l_work* w, void** p, size_t bytes)
         return S2L_ERR_OOM;
     }
     w->allocs.push_back(*p);
+    w->alloc_bytes.push_back(bytes);
     w->bytes += bytes;
     return S2L_OK;
 }
@@ -762,6 +780,21 @@ int work_alloc(s2l_work* w, void** p, size_t bytes)
 int work_doubles(s2l_work* w, double** p, size_t count)
 {
     return work_alloc(w, reinterpret_cast<void**>(p), count * sizeof(double));
+}
+
+void work_free(s2l_work* w, void* p)
+{
+    for (size_t i = 0; i < w->allocs.size(); ++i)
+        if (w->allocs[i] == p) {
+            const size_t bytes = w->alloc_bytes[i];
+            cudaFree(p);
+            w->allocs.erase(w->allocs.begin() + (long)i);
+            w->alloc_bytes.erase(w->alloc_bytes.begin() + (long)i);
+            w->bytes -= bytes;
+            std::lock_guard<std::mutex> g(w->s->ctx->mu);
+            w->s->ctx->used -= std::min(w->s->ctx->used, bytes);
+            return;
+        }
 }
 
 void prof_begin(s2l_work* w, int cls, cudaEvent_t* a)
@@ -847,6 +880,9 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
     a.xbuf = (Real*)w->d_xbuf;
     a.gflags = w->d_gflags;
     a.err = w->d_err;
+    a.K = 1;
+    a.KC = 1;
+    a.nloc = s->nloc;
     return a;
 }
 
@@ -948,6 +984,155 @@ int apply_dev(s2l_work* w, const double* r, double* z)
 }
 
 
+// ------------------------------------------------------------------------------ block solve pieces
+// Block vectors: n x K, entry i of column r at i * K + r.
+
+// Buffers of a block solve with K columns and restart m (reallocated when a call needs others).
+int ensure_block(s2l_work* w, int K, int m, bool flex)
+{
+    s2l_setup* s = w->s;
+    s2l_work::Block& B = w->blk;
+    if (B.K == K && B.m >= m && (!flex || B.flex)) return S2L_OK;
+    CUDA_OK(w, cudaStreamSynchronize(w->stream));
+    for (void* p : B.allocs) work_free(w, p);
+    if (B.h_red) cudaFreeHost(B.h_red);
+    B = s2l_work::Block{};
+    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    const int64_t loc = std::max<int64_t>(s->nloc, 1), n = s->n;
+    int rc = S2L_OK;
+    auto A = [&](void** p, size_t bytes) {
+        if (rc == S2L_OK) {
+            rc = work_alloc(w, p, bytes);
+            if (rc == S2L_OK) B.allocs.push_back(*p);
+        }
+    };
+    auto D = [&](double** p, size_t count) { A(reinterpret_cast<void**>(p), count * sizeof(double)); };
+    A(&B.ybuf, (size_t)loc * K * rs);
+    A(&B.xbuf, (size_t)loc * K * rs);
+    if (s->need_gflags) A(reinterpret_cast<void**>(&B.gflags), (size_t)loc * K);
+    D(&B.ylocal, (size_t)loc * K);
+    D(&B.plocal, (size_t)loc * K);
+    D(&B.x0, (size_t)n * K);
+    D(&B.wv, (size_t)n * K);
+    if (s->ntiles > 0) {
+        D(&B.cpart, (size_t)s->ntiles * s->mmax * K);
+        D(&B.c, (size_t)std::max<int64_t>(s->n0, 1) * K);
+        D(&B.y, (size_t)std::max<int64_t>(s->n0, 1) * K);
+    }
+    D(&B.V, (size_t)n * K * (m + 1));
+    if (flex) D(&B.Z, (size_t)n * K * m);
+    D(&B.r, (size_t)n * K);
+    D(&B.z, (size_t)n * K);
+    D(&B.kw, (size_t)n * K);
+    D(&B.b, (size_t)n * K);
+    D(&B.xk, (size_t)n * K);
+    D(&B.u, (size_t)n * K);
+    D(&B.coef, S2L_MAX_BLOCK_COLS);
+    D(&B.scal, 4 * S2L_MAX_RHS);
+    D(&B.part, (size_t)S2L_NB_RED * S2L_MAX_BLOCK_COLS);
+    D(&B.red, 3 * S2L_MAX_BLOCK_COLS);
+    if (rc == S2L_OK && cudaMallocHost(&B.h_red, 3 * S2L_MAX_BLOCK_COLS * sizeof(double)) != cudaSuccess)
+        rc = w->fail(S2L_ERR_OOM, "cannot allocate pinned host memory");
+    if (rc != S2L_OK) {
+        for (void* p : B.allocs) work_free(w, p);
+        B = s2l_work::Block{};
+        return rc;
+    }
+    B.K = K;
+    B.m = m;
+    B.flex = flex;
+    return S2L_OK;
+}
+
+size_t sweep_smem(const s2l_setup* s, int kc)
+{
+    const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
+    return ((((size_t)s->max_T * kc * rs) + 15) & ~(size_t)15) + (((size_t)s->max_T + 15) & ~(size_t)15);
+}
+
+// local solves of every subdomain for K columns: (mode 0) out[owned] (+ base), (mode 1) ylocal
+template <typename Real>
+int local_solve_block_t(s2l_work* w, int K, const double* in, const double* base, double* out, int mode)
+{
+    s2l_setup* s = w->s;
+    s2l_work::Block& B = w->blk;
+    LocalSolveArgs<Real> a = solve_args<Real>(w);
+    a.gather = s->d_gin;
+    a.in = in;
+    a.base = base;
+    a.out = out;
+    a.mode = mode;
+    a.ylocal = B.ylocal;
+    a.ybuf = (Real*)B.ybuf;
+    a.xbuf = (Real*)B.xbuf;
+    a.gflags = B.gflags;
+    a.K = K;
+    a.KC = B.gflags ? 1 : std::min(K, s->kc_max);
+    const size_t smem = B.gflags ? 0 : sweep_smem(s, a.KC);
+    int launched = 0;
+    const cudaError_t e = launch_local_solve<Real>(w->stream, a, s->nsub, smem, 0, s->tr_first_h[s->nsub], 0,
+                                                   s->us_first_h[s->nsub], &launched);
+    w->launches += launched;
+    if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("block local_solve launch: ") + cudaGetErrorString(e));
+    return S2L_OK;
+}
+
+int one_level_block(s2l_work* w, int K, const double* in, const double* base, double* out)
+{
+    s2l_setup* s = w->s;
+    const bool direct = s->pou == S2L_POU_BOOLEAN && s->one_level == S2L_ONE_LEVEL_RAS;
+    {
+        Prof pr(w, PC_SOLVE);
+        if (s->real == S2L_REAL_F32) RET_IF(local_solve_block_t<float>(w, K, in, base, out, direct ? 0 : 1));
+        else RET_IF(local_solve_block_t<double>(w, K, in, base, out, direct ? 0 : 1));
+    }
+    if (direct) return S2L_OK;
+    Prof pr(w, PC_COMBINE);
+    launch_combine_block(w->stream, s->n, K, s->d_cp_ptr, s->d_cp_pos,
+                         s->one_level == S2L_ONE_LEVEL_RAS ? s->d_cp_w : nullptr, w->blk.ylocal, base, out);
+    w->launches += 1;
+    return S2L_OK;
+}
+
+int coarse_block(s2l_work* w, int K, const double* r, double* x0)
+{
+    s2l_setup* s = w->s;
+    s2l_work::Block& B = w->blk;
+    Prof pr(w, PC_COARSE);
+    const int boolean = s->pou == S2L_POU_BOOLEAN;
+    launch_coarse_restrict_block(w->stream, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V,
+                                 s->d_l2g, boolean, r, s->mmax, B.cpart);
+    launch_coarse_reduce_block(w->stream, K, s->nsub, s->d_subs, s->d_t_first, s->mmax, B.cpart, B.c);
+    launch_dense_gemm(w->stream, K, (int)s->n0, s->d_Einv, B.c, B.y);
+    launch_coarse_prolong_block(w->stream, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V,
+                                boolean, B.y, x0, B.plocal);
+    if (!boolean) launch_combine_block(w->stream, s->n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, B.plocal, nullptr, x0);
+    w->launches += boolean ? 4 : 5;
+    return S2L_OK;
+}
+
+int spmv_block(s2l_work* w, int K, const double* X, double* Y, const double* Bv, bool with_norm)
+{
+    s2l_setup* s = w->s;
+    Prof pr(w, PC_SPMV);
+    launch_spmv_block(w->stream, s->n, K, s->d_rp, s->d_ci, s->d_av, X, Y, Bv, with_norm ? w->blk.part : nullptr,
+                      w->blk.red + 2 * S2L_MAX_BLOCK_COLS, s->tpr);
+    w->launches += with_norm ? 2 : 1;
+    return S2L_OK;
+}
+
+// Z = M^-1 R for K columns (two-level Schwarz); R and Z distinct
+int apply_block(s2l_work* w, int K, const double* R, double* Z)
+{
+    s2l_setup* s = w->s;
+    s2l_work::Block& B = w->blk;
+    if (s->coarse == S2L_COARSE_NONE || s->n0 == 0) return one_level_block(w, K, R, nullptr, Z);
+    RET_IF(coarse_block(w, K, R, B.x0));
+    if (s->coarse == S2L_COARSE_ADDITIVE) return one_level_block(w, K, R, B.x0, Z);
+    RET_IF(spmv_block(w, K, B.x0, B.wv, R, false));  // W = R - A X0
+    return one_level_block(w, K, B.wv, B.x0, Z);
+}
+
 // host/device staging of a global vector argument
 int stage_in(s2l_work* w, const double* p, int kind, int64_t count, double* tmp, const double** dev)
 {
@@ -978,16 +1163,44 @@ int ensure_krylov(s2l_work* w, int m, bool flexible)
     if (w->kr_m >= m && (!flexible || w->kr_flex)) return S2L_OK;
     if (m + 1 > S2L_MAX_RED_COLS - 1) return w->fail(S2L_ERR_BADARG, "restart too large (max 120)");
     const size_t n = (size_t)s->n;
-    RET_IF(work_doubles(w, &w->d_V_kr, n * (m + 1)));
-    if (flexible) RET_IF(work_doubles(w, &w->d_Z_kr, n * m));
+    std::vector<double*> fresh;  // undone if a later allocation fails (admission retries it)
+    int rc = S2L_OK;
+    auto D = [&](double** p, size_t count) {
+        double* q = nullptr;
+        if (rc == S2L_OK) rc = work_doubles(w, &q, count);
+        if (rc == S2L_OK) fresh.push_back(q);
+        return q;
+    };
+    double* V = D(nullptr, n * (m + 1));
+    double* Z = flexible ? D(nullptr, n * m) : nullptr;
+    double *r = nullptr, *z = nullptr, *kw = nullptr, *b = nullptr, *xk = nullptr, *u = nullptr, *coef = nullptr;
     if (w->kr_m < 0) {
-        RET_IF(work_doubles(w, &w->d_r, n));
-        RET_IF(work_doubles(w, &w->d_z, n));
-        RET_IF(work_doubles(w, &w->d_kw, n));
-        RET_IF(work_doubles(w, &w->d_b, n));
-        RET_IF(work_doubles(w, &w->d_xk, n));
-        RET_IF(work_doubles(w, &w->d_u, n));
-        RET_IF(work_doubles(w, &w->d_coef, 2 * S2L_MAX_RED_COLS));
+        r = D(nullptr, n);
+        z = D(nullptr, n);
+        kw = D(nullptr, n);
+        b = D(nullptr, n);
+        xk = D(nullptr, n);
+        u = D(nullptr, n);
+        coef = D(nullptr, 2 * S2L_MAX_RED_COLS);
+    }
+    if (rc != S2L_OK) {
+        for (double* q : fresh) work_free(w, q);
+        return rc;
+    }
+    if (w->d_V_kr) work_free(w, w->d_V_kr);
+    w->d_V_kr = V;
+    if (flexible) {
+        if (w->d_Z_kr) work_free(w, w->d_Z_kr);
+        w->d_Z_kr = Z;
+    }
+    if (w->kr_m < 0) {
+        w->d_r = r;
+        w->d_z = z;
+        w->d_kw = kw;
+        w->d_b = b;
+        w->d_xk = xk;
+        w->d_u = u;
+        w->d_coef = coef;
     }
     w->kr_m = m;
     w->kr_flex = w->kr_flex || flexible;
@@ -1197,6 +1410,7 @@ void work_destroy(s2l_work* w)
         w->s->ctx->used -= std::min(w->s->ctx->used, w->bytes);
     }
     if (w->h_red) cudaFreeHost(w->h_red);
+    if (w->blk.h_red) cudaFreeHost(w->blk.h_red);
     for (auto e : w->pool) cudaEventDestroy(e);
     cudaEventDestroy(w->join);
     cudaStreamDestroy(w->own_stream);
@@ -1206,33 +1420,71 @@ void work_destroy(s2l_work* w)
 // A free workspace for one solve-phase call: workspace 0 when it is free (it carries the caller's
 // stream and timers), another free one, or a new one when every workspace is busy (concurrent
 // calls on one setup from several threads).
+// A workspace for one solve-phase call: workspace 0 when it is free (it carries the caller's
+// stream and timers), another free one, or a new one when every workspace is busy (concurrent
+// calls on one setup from several threads).  `prepare` allocates what the call needs on the
+// workspace (Krylov basis, block buffers).
+//
+// Admission by HBM footprint: when those allocations do not fit the context's budget, the call
+// waits for a busy workspace of this setup to come free (it usually has them already) and tries
+// again; it fails with S2L_ERR_OOM only when no workspace is busy or after S2L_ADMIT_WAIT_S seconds.
 struct Lease {
     s2l_setup* s;
     s2l_work* w = nullptr;
     int idx = -1;
     int rc = S2L_OK;
-    explicit Lease(s2l_setup* s_) : s(s_)
+    explicit Lease(s2l_setup* s_, const std::function<int(s2l_work*)>& prepare = {}) : s(s_)
     {
-        std::lock_guard<std::mutex> g(s->wmu);
-        for (size_t i = 0; i < s->works.size(); ++i)
-            if (!s->busy[i]) {
-                idx = (int)i;
-                break;
-            }
-        if (idx < 0) {
-            s2l_work* nw = nullptr;
-            rc = work_create(s, &nw);
-            if (rc != S2L_OK) return;
-            s->works.push_back(nw);
-            s->busy.push_back(0);
-            idx = (int)s->works.size() - 1;
-        }
-        s->busy[idx] = 1;
-        w = s->works[idx];
         if (cudaSetDevice(s->ctx->device) != cudaSuccess) {
             rc = s->fail(S2L_ERR_CUDA, "cudaSetDevice failed");
             return;
         }
+        std::unique_lock<std::mutex> g(s->wmu);
+        const auto deadline = std::chrono::steady_clock::now() + std::chrono::seconds(S2L_ADMIT_WAIT_S);
+        auto take = [&](size_t i) -> int {  // reserve workspace i and prepare it (lock released meanwhile)
+            s->busy[i] = 1;
+            s2l_work* cand = s->works[i];
+            g.unlock();
+            const int r = prepare ? prepare(cand) : S2L_OK;
+            g.lock();
+            if (r != S2L_OK) s->busy[i] = 0;
+            return r;
+        };
+        for (;;) {
+            for (size_t i = 0; i < s->works.size() && idx < 0; ++i) {
+                if (s->busy[i]) continue;
+                const int r = take(i);
+                if (r == S2L_OK) idx = (int)i;
+                else if (r != S2L_ERR_OOM) {
+                    rc = r;
+                    return;
+                }
+            }
+            if (idx >= 0) break;
+            s2l_work* nw = nullptr;
+            int r = work_create(s, &nw);
+            if (r == S2L_OK) {
+                s->works.push_back(nw);
+                s->busy.push_back(0);
+                const size_t i = s->works.size() - 1;
+                r = take(i);
+                if (r == S2L_OK) {
+                    idx = (int)i;
+                    break;
+                }
+            }
+            if (r != S2L_ERR_OOM) {
+                rc = r;
+                return;
+            }
+            bool anybusy = false;
+            for (char b : s->busy) anybusy = anybusy || b;
+            if (!anybusy || s->wcv.wait_until(g, deadline) == std::cv_status::timeout) {
+                rc = S2L_ERR_OOM;  // the message of the failed allocation stays in last_error
+                return;
+            }
+        }
+        w = s->works[idx];
         // another workspace's stream starts after the work already queued on the caller's stream
         if (idx != 0 && s->user_stream) {
             if (cudaEventRecord(w->join, s->user_stream) != cudaSuccess ||
@@ -1243,8 +1495,11 @@ struct Lease {
     ~Lease()
     {
         if (idx < 0) return;
-        std::lock_guard<std::mutex> g(s->wmu);
-        s->busy[idx] = 0;
+        {
+            std::lock_guard<std::mutex> g(s->wmu);
+            s->busy[idx] = 0;
+        }
+        s->wcv.notify_all();
     }
 };
 
@@ -1823,6 +2078,12 @@ int s2l_gpu_setup_end(s2l_setup* s)
         s->need_gflags = true;
     }
     s->max_nl = max_nl;
+    s->max_T = max_T;
+    s->kc_max = 1;
+    if (s->smem_bytes > 0)
+        for (int kc = 2; kc <= 4; kc *= 2)
+            if (((((size_t)max_T * kc * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15) <= smem_cap)
+                s->kc_max = kc;
     CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
     // host staging no longer needed
     s->A = HostCsr();
@@ -2117,16 +2378,15 @@ static int gmres_run(s2l_setup* s, const double* b, double* x, int ptr_kind, con
                      s2l_result* res, const std::atomic<int>* cancel)
 {
     RET_IF(check_ready(s));
-    Lease lease(s);
-    RET_IF(lease.rc);
-    s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->restart < 1 || o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
     RET_IF(check_stop(s, o));
     const bool of = o->stop_norm == S2L_STOP_OPENFOAM;
     const int m = o->restart;
     const bool flex = o->flexible != 0;
-    RET_IF(ensure_krylov(w, m, flex));
+    Lease lease(s, [&](s2l_work* lw) { return ensure_krylov(lw, m, flex); });
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     const int64_t n = s->n;
     cudaStream_t st = w->stream;
     double* V = w->d_V_kr;
@@ -2322,24 +2582,33 @@ static int bicgstab_run(s2l_setup* s, const double* b, double* x, int ptr_kind, 
                         s2l_result* res, const std::atomic<int>* cancel)
 {
     RET_IF(check_ready(s));
-    Lease lease(s);
-    RET_IF(lease.rc);
-    s2l_work* w = lease.w;
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
     RET_IF(check_stop(s, o));
     const bool of = o->stop_norm == S2L_STOP_OPENFOAM;
-    RET_IF(ensure_krylov(w, 1, false));
+    Lease lease(s, [&](s2l_work* lw) -> int {
+        RET_IF(ensure_krylov(lw, 1, false));
+        if (lw->d_rh) return S2L_OK;
+        double* q[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        for (int i = 0; i < 6; ++i) {
+            const int r = work_doubles(lw, &q[i], (size_t)s->n);
+            if (r != S2L_OK) {
+                for (int j = 0; j < i; ++j) work_free(lw, q[j]);
+                return r;
+            }
+        }
+        lw->d_rh = q[0];
+        lw->d_p = q[1];
+        lw->d_v = q[2];
+        lw->d_s = q[3];
+        lw->d_t = q[4];
+        lw->d_yb = q[5];
+        return S2L_OK;
+    });
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
     const int64_t n = s->n;
     cudaStream_t st = w->stream;
-    if (!w->d_rh) {
-        RET_IF(work_doubles(w, &w->d_rh, n));
-        RET_IF(work_doubles(w, &w->d_p, n));
-        RET_IF(work_doubles(w, &w->d_v, n));
-        RET_IF(work_doubles(w, &w->d_s, n));
-        RET_IF(work_doubles(w, &w->d_t, n));
-        RET_IF(work_doubles(w, &w->d_yb, n));
-    }
     const double* db;
     if (ptr_kind == S2L_PTR_HOST) {
         CUDA_OK(w, cudaMemcpyAsync(w->d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -2497,6 +2766,287 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
                      s2l_result* res)
 {
     return bicgstab_run(s, b, x, ptr_kind, o, res, nullptr);
+}
+
+// ------------------------------------------------------------------------------ block solves
+// Stage k column-major vectors (host or device) into a block vector of K interleaved columns.
+static int block_in(s2l_work* w, int K, int k, const double* src, int ptr_kind, double* dst)
+{
+    s2l_setup* s = w->s;
+    const double* d = src;
+    if (ptr_kind == S2L_PTR_HOST) {
+        CUDA_OK(w, cudaMemcpyAsync(w->blk.u, src, (size_t)s->n * k * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+        d = w->blk.u;
+    } else if (ptr_kind != S2L_PTR_DEVICE) {
+        return w->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    }
+    launch_interleave(w->stream, s->n, K, k, d, dst);
+    w->launches += 1;
+    return S2L_OK;
+}
+
+static int block_out(s2l_work* w, int K, int k, const double* src, int ptr_kind, double* dst)
+{
+    s2l_setup* s = w->s;
+    if (ptr_kind == S2L_PTR_HOST) {
+        launch_deinterleave(w->stream, s->n, K, k, src, w->blk.u);
+        CUDA_OK(w, cudaMemcpyAsync(dst, w->blk.u, (size_t)s->n * k * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+    } else {
+        launch_deinterleave(w->stream, s->n, K, k, src, dst);
+    }
+    w->launches += 1;
+    CUDA_OK(w, cudaStreamSynchronize(w->stream));
+    CUDA_OK(w, cudaGetLastError());
+    return check_err(w);
+}
+
+static int block_width(s2l_setup* s, int k, int* K)
+{
+    if (k < 1 || k > S2L_MAX_RHS) return s->fail(S2L_ERR_BADARG, "a block holds 1 to 16 right-hand sides");
+    *K = 1;
+    while (*K < k) *K <<= 1;
+    return S2L_OK;
+}
+
+int s2l_gpu_apply_block(s2l_setup* s, int k, const double* r, double* z, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!r || !z) return s->fail(S2L_ERR_BADARG, "null vector");
+    int K = 1;
+    RET_IF(block_width(s, k, &K));
+    Lease lease(s, [&](s2l_work* lw) { return ensure_block(lw, K, std::max(lw->blk.m, 1), lw->blk.flex); });
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
+    RET_IF(block_in(w, K, k, r, ptr_kind, w->blk.r));
+    RET_IF(apply_block(w, K, w->blk.r, w->blk.z));
+    return block_out(w, K, k, w->blk.z, ptr_kind, z);
+}
+
+// k right-hand sides solved together: the GMRES of s2l_gpu_gmres (src/solver/gmres.cpp:18-161) run
+// in lockstep, each column with its own Hessenberg matrix, rotations, restarts and convergence;
+// the preconditioner, the products with A and the orthogonalization act on all columns at once.
+// A column that has converged, broken down or used maxit gets a zero basis vector, so the shared
+// steps leave it unchanged.  L2 stopping test only.
+static int gmres_block_run(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                           s2l_result* res)
+{
+    RET_IF(check_ready(s));
+    if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
+    if (o->restart < 1 || o->maxit < 0 || !(o->rtol >= 0.0)) return s->fail(S2L_ERR_BADARG, "bad Krylov options");
+    RET_IF(check_stop(s, o));
+    if (o->stop_norm != S2L_STOP_L2) return s->fail(S2L_ERR_BADARG, "block solves implement the L2 stopping test");
+    int K = 1;
+    RET_IF(block_width(s, k, &K));
+    const int m = o->restart;
+    if ((m + 1) * K > S2L_MAX_BLOCK_COLS) return s->fail(S2L_ERR_BADARG, "restart x right-hand sides too large");
+    const bool flex = o->flexible != 0;
+    Lease lease(s, [&](s2l_work* lw) { return ensure_block(lw, K, m, flex); });
+    RET_IF(lease.rc);
+    s2l_work* w = lease.w;
+    s2l_work::Block& B = w->blk;
+    const int64_t n = s->n, nK = n * K;
+    cudaStream_t st = w->stream;
+    RET_IF(block_in(w, K, k, b, ptr_kind, B.b));
+    RET_IF(block_in(w, K, k, x, ptr_kind, B.xk));
+    const int MC = S2L_MAX_BLOCK_COLS;
+    auto read = [&](int off, int count) -> int {
+        CUDA_OK(w, cudaMemcpyAsync(B.h_red + off, B.red + off, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+        return check_err(w);
+    };
+    auto upload = [&](double* dst, const double* src, int count) -> int {
+        CUDA_OK(w, cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, st));
+        return S2L_OK;
+    };
+    for (int r = 0; r < k; ++r) {
+        res[r].converged = res[r].breakdown = res[r].iterations = res[r].restarts = 0;
+        res[r].history_len = 0;
+        res[r].rel_residual = res[r].true_rel_residual = 0.0;
+        res[r].initial_residual_of = res[r].final_residual_of = 0.0;
+    }
+    auto hist = [&](int r, double v) {
+        if (res[r].history && res[r].history_len < o->history_cap) res[r].history[res[r].history_len] = v;
+        if (res[r].history_len < o->history_cap) ++res[r].history_len;
+    };
+    // ||b_r||
+    {
+        Prof pr(w, PC_VEC);
+        launch_mdot_block(st, n, K, B.b, nK, 1, B.b, B.part, B.red);
+        w->launches += 2;
+    }
+    RET_IF(read(0, K));
+    std::vector<double> bnorm(K, 0.0), beta(K, 0.0);
+    for (int r = 0; r < k; ++r) bnorm[r] = std::sqrt(B.h_red[r]);
+    for (int r = 0; r < k; ++r)
+        if (!std::isfinite(bnorm[r])) return s->fail(S2L_ERR_NUMERIC, "non-finite right-hand side");
+    std::vector<char> active(K, 0);
+    RET_IF(spmv_block(w, K, B.xk, B.r, B.b, true));
+    RET_IF(read(2 * MC, K));
+    for (int r = 0; r < k; ++r) {
+        if (bnorm[r] == 0.0) {  // x = 0 (src/solver/gmres.cpp:27-32)
+            res[r].converged = 1;
+            hist(r, 0.0);
+            continue;
+        }
+        beta[r] = std::sqrt(B.h_red[2 * MC + r]);
+        hist(r, beta[r] / bnorm[r]);
+        res[r].rel_residual = beta[r] / bnorm[r];
+        active[r] = beta[r] > o->rtol * bnorm[r];
+        res[r].converged = active[r] ? 0 : 1;
+    }
+    std::vector<double> H((size_t)K * (m + 1) * m), cs((size_t)K * m), sn((size_t)K * m), g((size_t)K * (m + 1));
+    std::vector<double> scal(2 * K), coef((size_t)(m + 1) * K), y(m);
+    std::vector<int> kr(K, 0);
+    std::vector<char> run(K, 0), done(K, 0), brk(K, 0), cand(K, 0);
+    auto Hc = [&](int r, int i, int j) -> double& { return H[((size_t)r * m + j) * (m + 1) + i]; };
+    for (;;) {
+        bool any = false;
+        for (int r = 0; r < k; ++r) {
+            run[r] = active[r] && res[r].iterations < o->maxit;
+            any = any || run[r];
+        }
+        if (!any) break;
+        for (int r = 0; r < K; ++r) {
+            if (r < k && !std::isfinite(beta[r]) && run[r]) return s->fail(S2L_ERR_NUMERIC, "non-finite residual");
+            scal[r] = r < k && run[r] ? 1.0 / beta[r] : 0.0;
+            done[r] = r < k && run[r] ? 0 : 1;
+            brk[r] = cand[r] = 0;
+            kr[r] = 0;
+        }
+        std::fill(H.begin(), H.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        for (int r = 0; r < k; ++r) g[(size_t)r * (m + 1)] = beta[r];
+        RET_IF(upload(B.scal, scal.data(), K));
+        {
+            Prof pr(w, PC_VEC);
+            launch_axpby_block(st, n, K, B.scal, B.r, nullptr, B.V);
+            w->launches += 1;
+        }
+        int jmax = 0;
+        for (int j = 0; j < m; ++j) {
+            bool step = false;
+            for (int r = 0; r < k; ++r) step = step || !done[r];
+            if (!step) break;
+            double* Vj = B.V + (size_t)j * nK;
+            double* Zj = flex ? B.Z + (size_t)j * nK : B.z;
+            RET_IF(apply_block(w, K, Vj, Zj));
+            RET_IF(spmv_block(w, K, Zj, B.kw, nullptr, false));
+            {
+                Prof pr(w, PC_VEC);
+                launch_mdot_block(st, n, K, B.V, nK, j + 1, B.kw, B.part, B.red);
+                launch_gemv_update_block(st, n, K, B.V, nK, j + 1, B.red, -1.0, B.kw, nullptr, nullptr);
+                launch_mdot_block(st, n, K, B.V, nK, j + 1, B.kw, B.part, B.red + MC);
+                launch_gemv_update_block(st, n, K, B.V, nK, j + 1, B.red + MC, -1.0, B.kw, B.part, B.red + 2 * MC);
+                w->launches += 7;
+            }
+            CUDA_OK(w, cudaMemcpyAsync(B.h_red, B.red, 3 * MC * sizeof(double), cudaMemcpyDeviceToHost, st));
+            RET_IF(check_err(w));
+            for (int r = 0; r < K; ++r) scal[r] = 0.0;
+            for (int r = 0; r < k; ++r) {
+                if (done[r]) continue;
+                const double hn = std::sqrt(B.h_red[2 * MC + r]);
+                for (int i = 0; i <= j; ++i) Hc(r, i, j) = B.h_red[i * K + r] + B.h_red[MC + i * K + r];
+                Hc(r, j + 1, j) = hn;
+                double* c_ = &cs[(size_t)r * m];
+                double* s_ = &sn[(size_t)r * m];
+                double* g_ = &g[(size_t)r * (m + 1)];
+                for (int i = 0; i < j; ++i) {
+                    const double t = c_[i] * Hc(r, i, j) + s_[i] * Hc(r, i + 1, j);
+                    Hc(r, i + 1, j) = -s_[i] * Hc(r, i, j) + c_[i] * Hc(r, i + 1, j);
+                    Hc(r, i, j) = t;
+                }
+                const double den = std::hypot(Hc(r, j, j), Hc(r, j + 1, j));
+                c_[j] = den > 0.0 ? Hc(r, j, j) / den : 1.0;
+                s_[j] = den > 0.0 ? Hc(r, j + 1, j) / den : 0.0;
+                Hc(r, j, j) = den;
+                Hc(r, j + 1, j) = 0.0;
+                g_[j + 1] = -s_[j] * g_[j];
+                g_[j] = c_[j] * g_[j];
+                ++kr[r];
+                ++res[r].iterations;
+                res[r].rel_residual = std::fabs(g_[j + 1]) / bnorm[r];
+                hist(r, res[r].rel_residual);
+                if (!std::isfinite(res[r].rel_residual)) return s->fail(S2L_ERR_NUMERIC, "non-finite GMRES residual");
+                if (res[r].rel_residual <= o->rtol) {
+                    cand[r] = 1;
+                    done[r] = 1;
+                } else if (hn == 0.0) {
+                    brk[r] = 1;
+                    done[r] = 1;
+                } else if (res[r].iterations >= o->maxit) {
+                    done[r] = 1;
+                }
+                if (!done[r]) scal[r] = 1.0 / hn;
+            }
+            jmax = j + 1;
+            if (j + 1 < m) {  // V_{j+1}: columns still running get w / hn, the others zero
+                RET_IF(upload(B.scal, scal.data(), K));
+                Prof pr(w, PC_VEC);
+                launch_axpby_block(st, n, K, B.scal, B.kw, nullptr, B.V + (size_t)(j + 1) * nK);
+                w->launches += 1;
+            }
+        }
+        // y_r = H_r^-1 g_r, x += M^-1 V y (or Z y)
+        std::fill(coef.begin(), coef.end(), 0.0);
+        for (int r = 0; r < k; ++r) {
+            if (!run[r]) continue;
+            const double* g_ = &g[(size_t)r * (m + 1)];
+            for (int i = kr[r] - 1; i >= 0; --i) {
+                double t = g_[i];
+                for (int c = i + 1; c < kr[r]; ++c) t -= Hc(r, i, c) * y[c];
+                y[i] = t / Hc(r, i, i);
+            }
+            for (int i = 0; i < kr[r]; ++i) coef[(size_t)i * K + r] = y[i];
+        }
+        for (int r = 0; r < K; ++r) scal[r] = scal[K + r] = 1.0;
+        RET_IF(upload(B.coef, coef.data(), jmax * K));
+        RET_IF(upload(B.scal, scal.data(), 2 * K));
+        {
+            Prof pr(w, PC_VEC);
+            launch_gemv_block(st, n, K, flex ? B.Z : B.V, nK, jmax, B.coef, B.u);
+            w->launches += 1;
+        }
+        if (flex) {
+            Prof pr(w, PC_VEC);
+            launch_axpby_block(st, n, K, B.scal, B.u, B.scal + K, B.xk);
+            w->launches += 1;
+        } else {
+            RET_IF(apply_block(w, K, B.u, B.z));
+            Prof pr(w, PC_VEC);
+            launch_axpby_block(st, n, K, B.scal, B.z, B.scal + K, B.xk);
+            w->launches += 1;
+        }
+        RET_IF(spmv_block(w, K, B.xk, B.r, B.b, true));
+        RET_IF(read(2 * MC, K));
+        for (int r = 0; r < k; ++r) {
+            if (!run[r]) continue;
+            beta[r] = std::sqrt(B.h_red[2 * MC + r]);
+            const double slack = o->strict_true_residual ? 1.0 : 1.1;
+            const bool within = beta[r] <= o->rtol * bnorm[r];
+            const bool within_slack = beta[r] <= slack * o->rtol * bnorm[r];
+            bool conv = cand[r] != 0;
+            if (brk[r]) conv = within || conv;
+            if (conv && !within_slack) conv = false;
+            if (beta[r] == 0.0) conv = true;
+            res[r].converged = conv ? 1 : 0;
+            res[r].true_rel_residual = beta[r] / bnorm[r];
+            if (conv) active[r] = 0;
+            else ++res[r].restarts;
+        }
+    }
+    RET_IF(block_out(w, K, k, B.xk, ptr_kind, x));
+    for (int r = 0; r < k; ++r) {
+        if (bnorm[r] != 0.0) continue;
+        if (ptr_kind == S2L_PTR_HOST) std::fill(x + (size_t)r * n, x + (size_t)(r + 1) * n, 0.0);
+        else CUDA_OK(w, cudaMemsetAsync(x + (size_t)r * n, 0, n * sizeof(double), st));
+    }
+    CUDA_OK(w, cudaStreamSynchronize(st));
+    return S2L_OK;
+}
+
+int s2l_gpu_gmres_block(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                        s2l_result* results)
+{
+    return gmres_block_run(s, k, b, x, ptr_kind, o, results);
 }
 
 // ------------------------------------------------------------------------------ batched solves

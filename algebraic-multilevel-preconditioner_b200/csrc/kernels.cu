@@ -23,6 +23,15 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
+// Sum over the warp, valid in every lane (butterfly)
+template <typename Real>
+__device__ __forceinline__ Real warp_allsum(Real v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Sum over the CTA; the result is valid in thread 0.  sh holds one value per warp.
 template <int BS>
 __device__ __forceinline__ double block_sum(double v, double* sh)
@@ -294,33 +303,49 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 // the ready flag of the column is set; 1/diag is folded into the values and the right-hand side,
 // so a row ends with x = b - sum, one write and its flag.  Every wait is bounded: after
 // S2L_SPIN_LIMIT polls the CTA raises *err and all warps leave.
-template <typename Real, bool SMEM, bool FWD>
+template <typename Real, bool SMEM, bool FWD, int KC>
 __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolveArgs<Real> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_word;
     volatile int& abort_flag = abort_word;
-    constexpr int Q = S2L_BATCH_CHUNKS;
-    const int sid = a.sub_list ? a.sub_list[blockIdx.x] : (int)blockIdx.x;
+    constexpr int Q = (sizeof(Real) == 8 && KC > 1) ? S2L_BATCH_CHUNKS / 2 : S2L_BATCH_CHUNKS;
+    // KC right-hand sides per CTA: CTA b takes subdomain b / ngrp and columns grp * KC .. + KC of
+    // the K interleaved columns (the CTAs of one subdomain are neighbours, so they share the
+    // factor stream in L2)
+    const int K = a.K;
+    const int ngrp = K / KC;
+    const int grp = (int)blockIdx.x % ngrp;
+    const int g0 = grp * KC;
+    const int sidx = (int)blockIdx.x / ngrp;
+    const int sid = a.sub_list ? a.sub_list[sidx] : sidx;
     const DevSub sd = a.subs[sid];
     const int64_t lo = sd.loc_off;
     const int T = sd.T;
     const SweepFactor<Real> F = a.f[FWD ? 0 : 1];
     Real* xs;
     volatile uint8_t* flag;
+    int xstride;  // x of slot k, column r: xs[k * xstride + r]
     if (SMEM) {
-        const size_t off1 = (((size_t)T * sizeof(Real)) + 15) & ~(size_t)15;
+        const size_t off1 = (((size_t)T * KC * sizeof(Real)) + 15) & ~(size_t)15;
         xs = reinterpret_cast<Real*>(smem_raw);
         flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off1);
+        xstride = KC;
     } else {
-        xs = (FWD ? a.ybuf : a.xbuf) + lo;
-        flag = a.gflags + lo;
+        xs = (FWD ? a.ybuf : a.xbuf) + lo * K + g0;
+        flag = a.gflags + (int64_t)grp * a.nloc + lo;
+        xstride = K;
     }
     volatile Real* x = xs;
     if (threadIdx.x == 0) abort_flag = 0;
     for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) {
-        const Real b = FWD ? (Real)a.in[a.gather[lo + k]] : a.ybuf[lo + a.u2l[lo + k]];
-        xs[k] = b * F.dinv[lo + k];
+        const Real d = F.dinv[lo + k];
+        const int64_t src = FWD ? (int64_t)a.gather[lo + k] * K : (lo + a.u2l[lo + k]) * K;
+#pragma unroll
+        for (int r = 0; r < KC; ++r) {
+            const Real b = FWD ? (Real)a.in[src + g0 + r] : a.ybuf[src + g0 + r];
+            xs[k * xstride + r] = b * d;
+        }
         flag[k] = 0;
     }
     __syncthreads();
@@ -334,9 +359,17 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
             const Real* W = F.blk_inv + F.blk_ioff[b];
             for (int i = k - 1; i >= 0; --i) {
                 const Real* Wi = W + i * (i + 1) / 2;
-                Real v = Real(0);
-                for (int j = 0; j <= i; ++j) v += Wi[j] * xs[F.blk_slot[o + j]];
-                xs[F.blk_slot[o + i]] = v;
+                Real v[KC];
+#pragma unroll
+                for (int r = 0; r < KC; ++r) v[r] = Real(0);
+                for (int j = 0; j <= i; ++j) {
+                    const int sj = F.blk_slot[o + j];
+#pragma unroll
+                    for (int r = 0; r < KC; ++r) v[r] += Wi[j] * xs[sj * xstride + r];
+                }
+                const int si = F.blk_slot[o + i];
+#pragma unroll
+                for (int r = 0; r < KC; ++r) xs[si * xstride + r] = v[r];
             }
         }
         __syncthreads();
@@ -352,7 +385,9 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
         const int k = lane >> gl2;
         const int slot = k < R ? F.tslot[so + k] : -1;
         so += R;
-        Real acc = Real(0);
+        Real acc[KC];
+#pragma unroll
+        for (int r = 0; r < KC; ++r) acc[r] = Real(0);
         for (int c0 = 0; c0 < C; c0 += Q) {  // C is the same for the whole warp
             int lc[Q];
             Real lv[Q];
@@ -378,25 +413,31 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                 const int c = lc[q];
                 if (c >= 0 && !dead) {
                     int spin = 0;
-                    while (flag[c] == 0) {
-                        if (abort_flag) { dead = true; break; }
-                        if (++spin > S2L_SPIN_LIMIT) {
-                            abort_flag = 1;
-                            atomicExch(a.err, 1);
-                            dead = true;
-                            break;
+                    while (flag[c] == 0) {  // the abort word and the limit are checked every 32 polls
+                        if ((++spin & 31) == 0) {
+                            if (abort_flag) { dead = true; break; }
+                            if (spin > S2L_SPIN_LIMIT) {
+                                abort_flag = 1;
+                                atomicExch(a.err, 1);
+                                dead = true;
+                                break;
+                            }
                         }
                     }
-                    acc += lv[q] * x[c];
+#pragma unroll
+                    for (int r = 0; r < KC; ++r) acc[r] += lv[q] * x[c * xstride + r];
                 }
             }
         }
         eo += (int64_t)C * 32;
         dead = __any_sync(0xffffffffu, dead);  // one decision per warp before its shuffles
         if (dead) break;
-        for (int o = (1 << gl2) >> 1; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, 1 << gl2);
+#pragma unroll
+        for (int r = 0; r < KC; ++r)
+            for (int o = (1 << gl2) >> 1; o; o >>= 1) acc[r] += __shfl_down_sync(0xffffffffu, acc[r], o, 1 << gl2);
         if ((lane & ((1 << gl2) - 1)) == 0 && slot >= 0) {
-            x[slot] = x[slot] - acc;
+#pragma unroll
+            for (int r = 0; r < KC; ++r) x[slot * xstride + r] = x[slot * xstride + r] - acc[r];
             __threadfence_block();
             flag[slot] = 1;
         }
@@ -404,27 +445,85 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     __syncthreads();
     if (FWD) {
         if (SMEM)
-            for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) a.ybuf[lo + k] = xs[k];
+            for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP)
+#pragma unroll
+                for (int r = 0; r < KC; ++r) a.ybuf[(lo + k) * K + g0 + r] = xs[k * KC + r];
         return;
     }
     // epilogue of the backward sweep: x_local[j] from its backward slot (< T) or tail row (>= T)
     const int n = sd.n_local;
-    auto val_at = [&](int q) -> double { return q < T ? (double)xs[q] : (double)a.ybuf[lo + q]; };
+    auto val_at = [&](int q, int r) -> double {
+        return q < T ? (double)xs[q * xstride + r] : (double)a.ybuf[(lo + q) * K + g0 + r];
+    };
     if (a.mode == 0) {
         for (int j = threadIdx.x; j < sd.n_owned; j += S2L_BS_SWEEP) {
-            double v = val_at(a.gout[lo + j]);
-            if (a.base) v += a.base[sd.begin + j];
-            a.out[sd.begin + j] = v;
+            const int q = a.gout[lo + j];
+            const int64_t o = (sd.begin + j) * K + g0;
+#pragma unroll
+            for (int r = 0; r < KC; ++r) {
+                double v = val_at(q, r);
+                if (a.base) v += a.base[o + r];
+                a.out[o + r] = v;
+            }
         }
     } else if (a.mode == 1) {
-        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) a.ylocal[lo + j] = val_at(a.gout[lo + j]);
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) {
+            const int q = a.gout[lo + j];
+#pragma unroll
+            for (int r = 0; r < KC; ++r) a.ylocal[(lo + j) * K + g0 + r] = val_at(q, r);
+        }
     } else {
-        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) a.out[j] = val_at(a.gout[lo + j]);
+        for (int j = threadIdx.x; j < n; j += S2L_BS_SWEEP) a.out[j] = val_at(a.gout[lo + j], 0);
     }
 }
 
-// Tail right-hand side: t(T+i) = b(T+i) - L(T+i, 0:T) y(0:T), one warp per tail row.
-template <typename Real>
+// acc[r] = sum_e val[e] * x[col[e] * K + r] over e in [e0, e1), one warp; for K = 1 four
+// independent gathers are in flight per lane, for K > 1 the K columns give the independence
+template <typename Real, int K>
+__device__ __forceinline__ void warp_gather_dot(const Real* __restrict__ val, const int32_t* __restrict__ col,
+                                                int64_t e0, int64_t e1, const Real* __restrict__ x, int lane,
+                                                Real (&acc)[K])
+{
+    if (K == 1) {
+        Real a0 = Real(0), a1 = Real(0), a2 = Real(0), a3 = Real(0);
+        int64_t e = e0 + lane;
+        for (; e + 96 < e1; e += 128) {
+            const int c0 = col[e], c1 = col[e + 32], c2 = col[e + 64], c3 = col[e + 96];
+            const Real v0 = val[e], v1 = val[e + 32], v2 = val[e + 64], v3 = val[e + 96];
+            a0 += v0 * x[c0];
+            a1 += v1 * x[c1];
+            a2 += v2 * x[c2];
+            a3 += v3 * x[c3];
+        }
+        for (; e < e1; e += 32) a0 += val[e] * x[col[e]];
+        acc[0] = warp_sum((a0 + a1) + (a2 + a3));
+    } else {
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = Real(0);
+        for (int64_t e = e0 + lane; e < e1; e += 32) {
+            const Real v = val[e];
+            const Real* xc = x + (int64_t)col[e] * K;
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += v * xc[r];
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = warp_allsum(acc[r]);  // lane r writes column r
+    }
+}
+
+// lane r < K gets acc[r] (a register array indexed by a runtime lane)
+template <typename Real, int K>
+__device__ __forceinline__ Real pick(const Real (&acc)[K], int lane)
+{
+    Real mine = acc[0];
+#pragma unroll
+    for (int r = 1; r < K; ++r)
+        if (lane == r) mine = acc[r];
+    return mine;
+}
+
+// Tail right-hand side: t(T+i) = b(T+i) - L(T+i, 0:T) y(0:T), one warp per tail row, K columns.
+template <typename Real, int K>
 __global__ void __launch_bounds__(256) tail_rhs_kernel(const LocalSolveArgs<Real> a, int q0, int count)
 {
     const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -433,14 +532,15 @@ __global__ void __launch_bounds__(256) tail_rhs_kernel(const LocalSolveArgs<Real
     const DevSub sd = a.subs[a.tr_sub[q]];
     const int64_t lo = sd.loc_off;
     const int k = sd.T + a.tr_i[q];
-    Real acc = Real(0);
-    for (int64_t e = a.lts_ptr[q] + lane; e < a.lts_ptr[q + 1]; e += 32) acc += a.lts_val[e] * a.ybuf[lo + a.lts_col[e]];
-    acc = warp_sum(acc);
-    if (lane == 0) a.ybuf[lo + k] = (Real)a.in[a.gather[lo + k]] - acc;
+    Real acc[K];
+    warp_gather_dot<Real, K>(a.lts_val, a.lts_col, a.lts_ptr[q], a.lts_ptr[q + 1], a.ybuf + lo * K, lane, acc);
+    if (lane < K)
+        a.ybuf[(lo + k) * K + lane] = (Real)a.in[(int64_t)a.gather[lo + k] * K + lane] - pick<Real, K>(acc, lane);
 }
 
-// Dense tail: out(T+i) = sum_j Minv(i, j) in(T+j), j <= i (lower) or j >= i (upper); warp per row.
-template <typename Real, bool LOWER>
+// Dense tail: out(T+i) = sum_j Minv(i, j) in(T+j), j <= i (lower) or j >= i (upper); warp per row,
+// K columns (Minv is read once for all of them).
+template <typename Real, bool LOWER, int K>
 __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Real> a, const Real* __restrict__ Minv,
                                                         const Real* __restrict__ vin, Real* __restrict__ vout,
                                                         int q0, int count)
@@ -454,19 +554,36 @@ __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Rea
     const int64_t base = sd.loc_off + sd.T;
     const Real* row = Minv + sd.d_off + (int64_t)i * s;
     const int j0 = LOWER ? 0 : i, j1 = LOWER ? i + 1 : s;
-    Real acc0 = Real(0), acc1 = Real(0);
-    int j = j0 + lane;
-    for (; j + 32 < j1; j += 64) {
-        acc0 += row[j] * vin[base + j];
-        acc1 += row[j + 32] * vin[base + j + 32];
+    const Real* v = vin + base * K;
+    if (K == 1) {
+        Real a0 = Real(0), a1 = Real(0), a2 = Real(0), a3 = Real(0);
+        int j = j0 + lane;
+        for (; j + 96 < j1; j += 128) {
+            a0 += row[j] * v[j];
+            a1 += row[j + 32] * v[j + 32];
+            a2 += row[j + 64] * v[j + 64];
+            a3 += row[j + 96] * v[j + 96];
+        }
+        for (; j < j1; j += 32) a0 += row[j] * v[j];
+        const Real acc = warp_sum((a0 + a1) + (a2 + a3));
+        if (lane == 0) vout[base + i] = acc;
+    } else {
+        Real acc[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = Real(0);
+        for (int j = j0 + lane; j < j1; j += 32) {
+            const Real m = row[j];
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += m * v[(int64_t)j * K + r];
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = warp_allsum(acc[r]);  // lane r writes column r
+        if (lane < K) vout[(base + i) * K + lane] = pick<Real, K>(acc, lane);
     }
-    if (j < j1) acc0 += row[j] * vin[base + j];
-    const Real acc = warp_sum(acc0 + acc1);
-    if (lane == 0) vout[base + i] = acc;
 }
 
-// Backward coupling: y(r) -= U(r, T:n) x(T:n) for the sparse rows that have tail columns.
-template <typename Real>
+// Backward coupling: y(r) -= U(r, T:n) x(T:n) for the sparse rows that have tail columns, K columns.
+template <typename Real, int K>
 __global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveArgs<Real> a, int q0, int count)
 {
     const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -474,10 +591,9 @@ __global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveAr
     if (q >= q0 + count) return;
     const DevSub sd = a.subs[a.us_sub[q]];
     const int64_t lo = sd.loc_off;
-    Real acc = Real(0);
-    for (int64_t e = a.ust_ptr[q] + lane; e < a.ust_ptr[q + 1]; e += 32) acc += a.ust_val[e] * a.ybuf[lo + a.ust_col[e]];
-    acc = warp_sum(acc);
-    if (lane == 0) a.ybuf[lo + a.us_r[q]] -= acc;
+    Real acc[K];
+    warp_gather_dot<Real, K>(a.ust_val, a.ust_col, a.ust_ptr[q], a.ust_ptr[q + 1], a.ybuf + lo * K, lane, acc);
+    if (lane < K) a.ybuf[(lo + a.us_r[q]) * K + lane] -= pick<Real, K>(acc, lane);
 }
 
 __global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n)
@@ -586,6 +702,323 @@ __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_prolong_kernel(const int
         plocal[sd.loc_off + l] = s;
 }
 
+// ------------------------------------------------------------------------------ K right-hand sides
+// Block vectors hold K interleaved columns: entry i of column r at i * K + r.
+
+// Y = A X (or B - A X), K columns; with partials, also sum(Y(:, r)^2) per block and column.
+template <int TPR, int K>
+__global__ void __launch_bounds__(S2L_BS_VEC) spmv_block_kernel(int64_t n, const int32_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ ci,
+                                                                const double* __restrict__ v,
+                                                                const double* __restrict__ X, double* __restrict__ Y,
+                                                                const double* __restrict__ B,
+                                                                double* __restrict__ partials)
+{
+    __shared__ double sh[S2L_BS_VEC / 32][K];
+    const int lane = threadIdx.x % TPR;
+    const int64_t g0 = ((int64_t)blockIdx.x * S2L_BS_VEC + threadIdx.x) / TPR;
+    const int64_t stride = (int64_t)gridDim.x * (S2L_BS_VEC / TPR);
+    double nrm[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) nrm[r] = 0.0;
+    for (int64_t row = g0; __any_sync(0xffffffffu, row < n); row += stride) {
+        double acc[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = 0.0;
+        if (row < n) {
+            const int e1 = rp[row + 1];
+            for (int e = rp[row] + lane; e < e1; e += TPR) {
+                const double a = v[e];
+                const double* x = X + (int64_t)ci[e] * K;
+#pragma unroll
+                for (int r = 0; r < K; ++r) acc[r] += a * x[r];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+            for (int o = TPR / 2; o; o >>= 1) acc[r] += __shfl_down_sync(0xffffffffu, acc[r], o, TPR);
+        if (lane == 0 && row < n) {
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                const double y = B ? B[row * K + r] - acc[r] : acc[r];
+                Y[row * K + r] = y;
+                nrm[r] += y * y;
+            }
+        }
+    }
+    if (partials) {
+        const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const double t = warp_sum(nrm[r]);
+            if (wl == 0) sh[warp][r] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < K) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < S2L_BS_VEC / 32; ++w) t += sh[w][threadIdx.x];
+            partials[(int64_t)blockIdx.x * K + threadIdx.x] = t;
+        }
+    }
+}
+
+// Sum over the lanes of a warp that hold the same column (lane % K): afterwards lanes 0..K-1 hold
+// the column sums (K a power of two, at most 32).
+template <int K>
+__device__ __forceinline__ double col_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o >= K; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// h(j, r) = V_j(:, r) . w(:, r) for j < J (V_j at V + j * ldv, n x K interleaved); tiles of 1024
+// entries (w staged in shared memory, entry e of a tile is column e % K), warp owns the columns
+// j = warp + 8q; partials[(b * J + j) * K + r].
+template <int K>
+__global__ void __launch_bounds__(256) mdot_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv, int J,
+                                                         const double* __restrict__ w, double* __restrict__ partials)
+{
+    __shared__ double ws[1024];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+    for (int64_t t0 = (int64_t)blockIdx.x * 1024; t0 < nk; t0 += (int64_t)gridDim.x * 1024) {
+        const int cnt = (int)((nk - t0) < 1024 ? (nk - t0) : 1024);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += 256) ws[i] = w[t0 + i];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int j = warp + 8 * q;
+            if (j < J) {
+                const double* vj = V + (int64_t)j * ldv + t0;
+                double s0 = 0.0;
+                for (int i = lane; i < cnt; i += 32) s0 += vj[i] * ws[i];
+                acc[q] += s0;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int j = warp + 8 * q;
+        if (j < J) {
+            const double t = col_sum<K>(acc[q]);
+            if (lane < K) partials[((int64_t)blockIdx.x * J + j) * K + lane] = t;
+        }
+    }
+}
+
+// w(:, r) += alpha * sum_j V_j(:, r) h(j, r); with partials, also sum(w(:, r)^2) per block
+template <int K>
+__global__ void __launch_bounds__(256) gemv_update_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv,
+                                                                int J, const double* __restrict__ h, double alpha,
+                                                                double* __restrict__ w, double* __restrict__ partials)
+{
+    __shared__ double hs[S2L_MAX_BLOCK_COLS];
+    __shared__ double sh[8][K];
+    for (int c = threadIdx.x; c < J * K; c += 256) hs[c] = h[c];
+    __syncthreads();
+    const int r = (int)(threadIdx.x % K);  // every stride below is a multiple of K
+    double nrm = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256) {
+        double s = 0.0;
+        for (int j = 0; j < J; ++j) s += V[e + (int64_t)j * ldv] * hs[j * K + r];
+        const double wn = w[e] + alpha * s;
+        w[e] = wn;
+        nrm += wn * wn;
+    }
+    if (partials) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const double t = col_sum<K>(nrm);
+        if (lane < K) sh[warp][lane] = t;
+        __syncthreads();
+        if (threadIdx.x < K) {
+            double u = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) u += sh[q][threadIdx.x];
+            partials[(int64_t)blockIdx.x * K + threadIdx.x] = u;
+        }
+    }
+}
+
+// u(:, r) = sum_j V_j(:, r) y(j, r)
+template <int K>
+__global__ void __launch_bounds__(256) gemv_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv, int J,
+                                                         const double* __restrict__ y, double* __restrict__ u)
+{
+    __shared__ double ys[S2L_MAX_BLOCK_COLS];
+    for (int c = threadIdx.x; c < J * K; c += 256) ys[c] = y[c];
+    __syncthreads();
+    const int r = (int)(threadIdx.x % K);
+    for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256) {
+        double s = 0.0;
+        for (int j = 0; j < J; ++j) s += V[e + (int64_t)j * ldv] * ys[j * K + r];
+        u[e] = s;
+    }
+}
+
+// y(:, r) = a(r) x(:, r) + b(r) y(:, r) (b null: y is not read); a, b on the device, K each
+template <int K>
+__global__ void __launch_bounds__(256) axpby_block_kernel(int64_t nk, const double* __restrict__ a,
+                                                          const double* __restrict__ x, const double* __restrict__ b,
+                                                          double* __restrict__ y)
+{
+    const int r = (int)(threadIdx.x % K);
+    const double ar = a[r], br = b ? b[r] : 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256)
+        y[e] = b ? ar * x[e] + br * y[e] : ar * x[e];
+}
+
+// dst (n x K interleaved) from k columns src + r * n (r < k); columns k..K-1 are zero
+__global__ void interleave_kernel(int64_t n, int K, int k, const double* __restrict__ src, double* __restrict__ dst)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / K;
+        const int r = (int)(e % K);
+        dst[e] = r < k ? src[(int64_t)r * n + i] : 0.0;
+    }
+}
+
+// k columns dst + r * n from src (n x K interleaved)
+__global__ void deinterleave_kernel(int64_t n, int K, int k, const double* __restrict__ src, double* __restrict__ dst)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * k; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / n);
+        const int64_t i = e % n;
+        dst[e] = src[i * K + r];
+    }
+}
+
+// out(g, r) = base(g, r) + sum over the copies of g of w_e ylocal(pos, r) (K columns)
+template <int K>
+__global__ void combine_block_kernel(int64_t n, const int64_t* __restrict__ cp_ptr, const int32_t* __restrict__ cp_pos,
+                                     const double* __restrict__ cp_w, const double* __restrict__ ylocal,
+                                     const double* __restrict__ base, double* __restrict__ out)
+{
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        double s[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) s[r] = 0.0;
+        for (int64_t e = cp_ptr[g]; e < cp_ptr[g + 1]; ++e) {
+            const double* y = ylocal + (int64_t)cp_pos[e] * K;
+            const double wgt = cp_w ? cp_w[e] : 1.0;
+#pragma unroll
+            for (int r = 0; r < K; ++r) s[r] += wgt * y[r];
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r) out[g * K + r] = base ? base[g * K + r] + s[r] : s[r];
+    }
+}
+
+// c_i(c, r) = V_i(:, c)^T R(:, r) per 256-row tile of one subdomain: partials[(tile * mmax + c) * K + r].
+template <int K>
+__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
+    const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
+    const DevSub* __restrict__ subs, const double* __restrict__ V, const int32_t* __restrict__ l2g, int boolean_pou,
+    const double* __restrict__ R, int mmax, double* __restrict__ partials)
+{
+    __shared__ double red[S2L_TILE_ROWS / 32][K];
+    const int tile = blockIdx.x;
+    const DevSub sd = subs[t_sub[tile]];
+    const int m = sd.m, nr = t_nrow[tile];
+    const int l = t_row0[tile] + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool act = threadIdx.x < nr;
+    double rv[K];
+    const double* vr = V;
+#pragma unroll
+    for (int r = 0; r < K; ++r) rv[r] = 0.0;
+    if (act) {
+        const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
+#pragma unroll
+        for (int r = 0; r < K; ++r) rv[r] = R[g * K + r];
+        vr = V + sd.v_off + (int64_t)l * m;
+    }
+    for (int c = 0; c < m; ++c) {
+        const double vc = act ? vr[c] : 0.0;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const double p = warp_sum(vc * rv[r]);
+            if (lane == 0) red[warp][r] = p;
+        }
+        __syncthreads();
+        if (threadIdx.x < K) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) s += red[w][threadIdx.x];
+            partials[((int64_t)tile * mmax + c) * K + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
+template <int K>
+__global__ void coarse_reduce_block_kernel(const DevSub* __restrict__ subs, const int32_t* __restrict__ t_first,
+                                           int mmax, const double* __restrict__ partials, double* __restrict__ cvec)
+{
+    const int i = blockIdx.x;
+    const DevSub sd = subs[i];
+    for (int e = threadIdx.x; e < sd.m * K; e += blockDim.x) {
+        double s = 0.0;
+        for (int t = t_first[i]; t < t_first[i + 1]; ++t) s += partials[(int64_t)t * mmax * K + e];
+        cvec[sd.c_off * K + e] = s;
+    }
+}
+
+// Y = M X, M dense row-major n0 x n0, K columns; one warp per row (M is read once for all columns)
+template <int K>
+__global__ void __launch_bounds__(256) dense_gemm_kernel(int n0, const double* __restrict__ M,
+                                                         const double* __restrict__ X, double* __restrict__ Y)
+{
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n0) return;
+    const double* mr = M + (int64_t)row * n0;
+    double s[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) s[r] = 0.0;
+    for (int c = lane; c < n0; c += 32) {
+        const double m = mr[c];
+#pragma unroll
+        for (int r = 0; r < K; ++r) s[r] += m * X[(int64_t)c * K + r];
+    }
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+        const double t = warp_sum(s[r]);
+        if (lane == 0) Y[(int64_t)row * K + r] = t;
+    }
+}
+
+// X0 = V_i Y_i on the owned rows (boolean PoU) or on Omega_i (plocal), K columns
+template <int K>
+__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_prolong_block_kernel(
+    const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
+    const DevSub* __restrict__ subs, const double* __restrict__ V, int boolean_pou, const double* __restrict__ Y,
+    double* __restrict__ out, double* __restrict__ plocal)
+{
+    const int tile = blockIdx.x;
+    if ((int)threadIdx.x >= t_nrow[tile]) return;
+    const DevSub sd = subs[t_sub[tile]];
+    const int l = t_row0[tile] + threadIdx.x;
+    const double* vr = V + sd.v_off + (int64_t)l * sd.m;
+    const double* yc = Y + sd.c_off * K;
+    double s[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) s[r] = 0.0;
+    for (int c = 0; c < sd.m; ++c) {
+        const double v = vr[c];
+#pragma unroll
+        for (int r = 0; r < K; ++r) s[r] += v * yc[c * K + r];
+    }
+    double* o = boolean_pou ? out + (sd.begin + l) * K : plocal + (sd.loc_off + l) * K;
+#pragma unroll
+    for (int r = 0; r < K; ++r) o[r] = s[r];
+}
+
 inline int grid_for(int64_t n, int bs, int cap)
 {
     const int64_t g = (n + bs - 1) / bs;
@@ -598,7 +1031,9 @@ inline int grid_for(int64_t n, int bs, int cap)
 void launch_spmv(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* x,
                  double* y, const double* b, double* partials, double* red_out, int tpr)
 {
-    const int grid = S2L_NB_RED;
+    // the norm partials need the fixed grid (deterministic reduction); a plain product takes one
+    // lane group per row
+    const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
     switch (tpr) {
     case 4: spmv_kernel<4><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 16: spmv_kernel<16><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
@@ -643,6 +1078,106 @@ void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, c
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
 }
 
+// ---- K right-hand sides (K = 1, 2, 4, 8 or 16)
+#define S2L_KSWITCH(K, CALL)                             \
+    switch (K) {                                         \
+    case 1: { constexpr int KK = 1; CALL; break; }       \
+    case 2: { constexpr int KK = 2; CALL; break; }       \
+    case 4: { constexpr int KK = 4; CALL; break; }       \
+    case 8: { constexpr int KK = 8; CALL; break; }       \
+    default: { constexpr int KK = 16; CALL; break; }     \
+    }
+
+void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, const int32_t* ci, const double* v,
+                       const double* X, double* Y, const double* B, double* partials, double* red_out, int tpr)
+{
+    const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
+    if (tpr == 4) {
+        S2L_KSWITCH(K, (spmv_block_kernel<4, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    } else if (tpr == 16) {
+        S2L_KSWITCH(K, (spmv_block_kernel<16, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    } else if (tpr == 32) {
+        S2L_KSWITCH(K, (spmv_block_kernel<32, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    } else {
+        S2L_KSWITCH(K, (spmv_block_kernel<8, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    }
+    if (partials) reduce_kernel<<<(K + 7) / 8, 256, 0, st>>>(partials, grid, K, red_out);
+}
+
+void launch_mdot_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* w,
+                       double* partials, double* out)
+{
+    S2L_KSWITCH(K, (mdot_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, w, partials)));
+    reduce_kernel<<<(J * K + 7) / 8, 256, 0, st>>>(partials, S2L_NB_RED, J * K, out);
+}
+
+void launch_gemv_update_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* h,
+                              double alpha, double* w, double* partials, double* red_out)
+{
+    S2L_KSWITCH(K, (gemv_update_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, h, alpha, w, partials)));
+    if (partials) reduce_kernel<<<(K + 7) / 8, 256, 0, st>>>(partials, S2L_NB_RED, K, red_out);
+}
+
+void launch_gemv_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* y,
+                       double* u)
+{
+    S2L_KSWITCH(K, (gemv_block_kernel<KK><<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n * K, V, ldv, J, y, u)));
+}
+
+void launch_axpby_block(cudaStream_t st, int64_t n, int K, const double* a, const double* x, const double* b,
+                        double* y)
+{
+    S2L_KSWITCH(K, (axpby_block_kernel<KK><<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n * K, a, x, b, y)));
+}
+
+void launch_interleave(cudaStream_t st, int64_t n, int K, int k, const double* src, double* dst)
+{
+    interleave_kernel<<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, K, k, src, dst);
+}
+
+void launch_deinterleave(cudaStream_t st, int64_t n, int K, int k, const double* src, double* dst)
+{
+    deinterleave_kernel<<<grid_for(n * k, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, K, k, src, dst);
+}
+
+void launch_combine_block(cudaStream_t st, int64_t n, int K, const int64_t* cp_ptr, const int32_t* cp_pos,
+                          const double* cp_w, const double* ylocal, const double* base, double* out)
+{
+    S2L_KSWITCH(K, (combine_block_kernel<KK><<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, cp_ptr, cp_pos, cp_w,
+                                                                                                ylocal, base, out)));
+}
+
+void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                  const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                                  int boolean_pou, const double* R, int mmax, double* partials)
+{
+    if (ntiles <= 0) return;
+    S2L_KSWITCH(K, (coarse_restrict_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, 0, st>>>(
+                       t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials)));
+}
+
+void launch_coarse_reduce_block(cudaStream_t st, int K, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,
+                                const double* partials, double* cvec)
+{
+    S2L_KSWITCH(K, (coarse_reduce_block_kernel<KK><<<nsub, 128, 0, st>>>(subs, t_first, mmax, partials, cvec)));
+}
+
+void launch_dense_gemm(cudaStream_t st, int K, int n0, const double* M, const double* X, double* Y)
+{
+    if (n0 <= 0) return;
+    S2L_KSWITCH(K, (dense_gemm_kernel<KK><<<(n0 + 7) / 8, 256, 0, st>>>(n0, M, X, Y)));
+}
+
+void launch_coarse_prolong_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
+                                 const double* Y, double* out, double* plocal)
+{
+    if (ntiles <= 0) return;
+    S2L_KSWITCH(K, (coarse_prolong_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V,
+                                                                                     boolean_pou, Y, out, plocal)));
+}
+#undef S2L_KSWITCH
+
 void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
                double* out)
 {
@@ -678,43 +1213,70 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
     reduce_kernel<<<1, 256, 0, st>>>(partials, S2L_NB_RED, 2, out);
 }
 
-template <typename Real>
-cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
-                               int tr_count, int us_first, int us_count, int* launches)
+template <typename Real, int KC, int K>
+cudaError_t launch_local_solve_k(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
+                                 int tr_count, int us_first, int us_count, int* launches)
 {
     cudaError_t e;
+    const int grid = nblocks * (K / KC);
     if (smem > 0) {
         // the limit is a process-wide attribute of the kernel: always the same cap, so launches of
         // setups with different shared-memory sizes from several threads cannot undercut each other
         if (smem > S2L_SWEEP_SMEM_CAP) return cudaErrorInvalidValue;
-        e = cudaFuncSetAttribute(sweep_kernel<Real, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(sweep_kernel<Real, true, true, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  S2L_SWEEP_SMEM_CAP);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(sweep_kernel<Real, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(sweep_kernel<Real, true, false, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  S2L_SWEEP_SMEM_CAP);
         if (e != cudaSuccess) return e;
-        sweep_kernel<Real, true, true><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
+        sweep_kernel<Real, true, true, KC><<<grid, S2L_BS_SWEEP, smem, st>>>(a);
     } else {
-        sweep_kernel<Real, false, true><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
+        sweep_kernel<Real, false, true, KC><<<grid, S2L_BS_SWEEP, 0, st>>>(a);
     }
     int nl = 1;
     if (tr_count > 0) {
-        const int grid = (tr_count + 7) / 8;
-        tail_rhs_kernel<Real><<<grid, 256, 0, st>>>(a, tr_first, tr_count);
-        tail_gemv_kernel<Real, true><<<grid, 256, 0, st>>>(a, a.linv, a.ybuf, a.xbuf, tr_first, tr_count);
-        tail_gemv_kernel<Real, false><<<grid, 256, 0, st>>>(a, a.uinv, a.xbuf, a.ybuf, tr_first, tr_count);
+        const int g = (tr_count + 7) / 8;
+        tail_rhs_kernel<Real, K><<<g, 256, 0, st>>>(a, tr_first, tr_count);
+        tail_gemv_kernel<Real, true, K><<<g, 256, 0, st>>>(a, a.linv, a.ybuf, a.xbuf, tr_first, tr_count);
+        tail_gemv_kernel<Real, false, K><<<g, 256, 0, st>>>(a, a.uinv, a.xbuf, a.ybuf, tr_first, tr_count);
         nl += 3;
     }
     if (us_count > 0) {
-        sparse_coupling_kernel<Real><<<(us_count + 7) / 8, 256, 0, st>>>(a, us_first, us_count);
+        sparse_coupling_kernel<Real, K><<<(us_count + 7) / 8, 256, 0, st>>>(a, us_first, us_count);
         nl += 1;
     }
     if (smem > 0)
-        sweep_kernel<Real, true, false><<<nblocks, S2L_BS_SWEEP, smem, st>>>(a);
+        sweep_kernel<Real, true, false, KC><<<grid, S2L_BS_SWEEP, smem, st>>>(a);
     else
-        sweep_kernel<Real, false, false><<<nblocks, S2L_BS_SWEEP, 0, st>>>(a);
+        sweep_kernel<Real, false, false, KC><<<grid, S2L_BS_SWEEP, 0, st>>>(a);
     *launches = nl + 1;
     return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
+                               int tr_count, int us_first, int us_count, int* launches)
+{
+    // (KC, K): right-hand sides per sweep CTA and in all; the setup's shared memory fixes KC
+    const int K = a.K, KC = smem > 0 ? a.KC : 1;
+#define S2L_LS(KC_, K_)                                                                                         \
+    if (KC == KC_ && K == K_)                                                                                  \
+    return launch_local_solve_k<Real, KC_, K_>(st, a, nblocks, smem, tr_first, tr_count, us_first, us_count, \
+                                               launches)
+    S2L_LS(1, 1);
+    S2L_LS(1, 2);
+    S2L_LS(2, 2);
+    S2L_LS(1, 4);
+    S2L_LS(2, 4);
+    S2L_LS(4, 4);
+    S2L_LS(1, 8);
+    S2L_LS(2, 8);
+    S2L_LS(4, 8);
+    S2L_LS(1, 16);
+    S2L_LS(2, 16);
+    S2L_LS(4, 16);
+#undef S2L_LS
+    return cudaErrorInvalidValue;
 }
 
 template cudaError_t launch_local_solve<double>(cudaStream_t, const LocalSolveArgs<double>&, int, size_t, int, int, int,

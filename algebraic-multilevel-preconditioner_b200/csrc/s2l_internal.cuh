@@ -22,12 +22,15 @@
 #define S2L_BS_VEC 256        // threads of the vector / SpMV kernels
 #define S2L_NB_RED 592        // blocks of every kernel that produces reduction partials (4 x 148 SMs)
 #define S2L_MAX_RED_COLS 128  // columns of the reduction buffer
+#define S2L_MAX_RHS 16        // right-hand sides of one block solve
+#define S2L_MAX_BLOCK_COLS 1024  // Krylov coefficients of a block step: (restart + 1) x K at most
 #define S2L_TILE_ROWS 256     // rows of one coarse restrict/prolong tile
 #define S2L_SWEEP_WARPS (S2L_BS_SWEEP / 32)
 #define S2L_BATCH_CHUNKS 8    // chunks of a task loaded together (all loads issued before the first wait)
 #define S2L_CHAIN_DEFAULT 8   // rows of a chain block (setup option "chain_block")
 #define S2L_CHAIN_MAX 16
 #define S2L_SWEEP_SMEM_CAP (227 * 1024 - 64)  // dynamic shared memory of a sweep CTA, at most
+#define S2L_ADMIT_WAIT_S 600   // longest wait of a call for a free workspace when the HBM budget is full
 #define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {
@@ -102,6 +105,11 @@ struct LocalSolveArgs {
     uint8_t* gflags;           // ready flags when a sweep does not fit shared memory
     int* err;                  // device error word (1: a sweep wait gave up)
     int mode;                  // 0 direct owned write, 1 local-space write, 2 local input/output
+    // right-hand sides: every vector above holds K interleaved columns (entry i of column r at
+    // i * K + r); a sweep CTA takes KC of them (K / KC CTAs per subdomain); single solves: 1, 1
+    int K;
+    int KC;
+    int64_t nloc;              // local-space size (stride of the per-column-group ready flags)
 };
 
 // launch wrappers (kernels.cu)
@@ -118,6 +126,30 @@ void launch_gemv(cudaStream_t st, int64_t n, const double* V, int64_t ldv, int k
 void launch_axpby(cudaStream_t st, int64_t n, double a, const double* x, double b, double* y);
 void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, const double* z, double* partials,
                  double* out);
+// K right-hand sides (block vectors n x K interleaved; K = 1, 2, 4, 8 or 16)
+void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, const int32_t* ci, const double* v,
+                       const double* X, double* Y, const double* B, double* partials, double* red_out, int tpr);
+void launch_mdot_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* w,
+                       double* partials, double* out);
+void launch_gemv_update_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* h,
+                              double alpha, double* w, double* partials, double* red_out);
+void launch_gemv_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* y,
+                       double* u);
+void launch_axpby_block(cudaStream_t st, int64_t n, int K, const double* a, const double* x, const double* b,
+                        double* y);
+void launch_interleave(cudaStream_t st, int64_t n, int K, int k, const double* src, double* dst);
+void launch_deinterleave(cudaStream_t st, int64_t n, int K, int k, const double* src, double* dst);
+void launch_combine_block(cudaStream_t st, int64_t n, int K, const int64_t* cp_ptr, const int32_t* cp_pos,
+                          const double* cp_w, const double* ylocal, const double* base, double* out);
+void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                  const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                                  int boolean_pou, const double* R, int mmax, double* partials);
+void launch_coarse_reduce_block(cudaStream_t st, int K, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,
+                                const double* partials, double* cvec);
+void launch_dense_gemm(cudaStream_t st, int K, int n0, const double* M, const double* X, double* Y);
+void launch_coarse_prolong_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
+                                 const double* Y, double* out, double* plocal);
 // out[0] = sum |a - alpha c| (c may be nullptr), out[1] = sum a
 void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
                double* out);

@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -32,7 +33,7 @@ EXPORTED = [
     "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes", "s2l_gpu_setup_option",
     "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
-    "s2l_gpu_ticket_free",
+    "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -108,6 +109,8 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_cancel": ([vp], C.c_int),
         "s2l_gpu_ticket_info": ([vp, dp, dp, C.POINTER(C.c_char_p)], C.c_int),
         "s2l_gpu_ticket_free": ([vp], C.c_int),
+        "s2l_gpu_apply_block": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_gmres_block": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -136,6 +139,7 @@ class Context:
         if rc != S2L_OK:
             raise S2LError(rc, "s2l_gpu_create failed (no CUDA device?)")
         self.h = h
+        self._setups = weakref.WeakSet()  # closed before the context (a setup must not outlive it)
 
     def error(self) -> str:
         return self.lib.s2l_gpu_last_error(self.h).decode()
@@ -150,6 +154,8 @@ class Context:
 
     def close(self):
         if self.h:
+            for g in list(self._setups):
+                g.close()
             self.lib.s2l_gpu_destroy(self.h)
             self.h = None
 
@@ -215,6 +221,7 @@ class GpuSetup:
 
     def __init__(self, ctx: Context, st: Setup, one_level=None, coarse=None, pou=None, options=None):
         self.ctx = ctx
+        ctx._setups.add(self)
         self.lib = ctx.lib
         self.n = st.n
         self.nsub = st.nsub
@@ -381,6 +388,39 @@ class GpuSetup:
             self.ctx.check(rc)
         return [(xs[j], _result_dict(res[j], hists[j]), st[j]) for j in range(k)]
 
+    def apply_block(self, R):
+        """Z = M^-1 R for the k rows of R (k x n, host), one block call (s2l_gpu_apply_block)."""
+        R = np.ascontiguousarray(np.atleast_2d(R), dtype=np.float64)
+        Z = np.empty_like(R)
+        self.ctx.check(self.lib.s2l_gpu_apply_block(self.h, R.shape[0], _vp(R), _vp(Z), PTR_HOST))
+        return Z
+
+    def gmres_block(self, B, X0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False,
+                    history_cap=4096, device_out=None):
+        """k right-hand sides in one lockstep block GMRES (s2l_gpu_gmres_block).
+
+        Host: B is k x n (rows are right-hand sides); returns (X k x n, [result dict per row]).
+        Device: B and device_out are device pointers to k * n doubles (pass k=... via B as (ptr, k))."""
+        o = self._opts(restart, rtol, maxit, flexible, strict, history_cap, "l2", 0.0)
+        if isinstance(B, tuple):  # (device pointer, k)
+            ptr, k = B
+            res = (Result * k)()
+            hists = [np.zeros(max(history_cap, 1)) for _ in range(k)]
+            for j in range(k):
+                res[j].history = _p(hists[j], C.c_double)
+            self.ctx.check(self.lib.s2l_gpu_gmres_block(self.h, k, C.c_void_p(ptr), C.c_void_p(device_out), PTR_DEVICE,
+                                                        C.byref(o), res))
+            return device_out, [_result_dict(res[j], hists[j]) for j in range(k)]
+        B = np.ascontiguousarray(np.atleast_2d(B), dtype=np.float64)
+        k = B.shape[0]
+        X = np.zeros_like(B) if X0 is None else np.ascontiguousarray(X0, dtype=np.float64).copy()
+        res = (Result * k)()
+        hists = [np.zeros(max(history_cap, 1)) for _ in range(k)]
+        for j in range(k):
+            res[j].history = _p(hists[j], C.c_double)
+        self.ctx.check(self.lib.s2l_gpu_gmres_block(self.h, k, _vp(B), _vp(X), PTR_HOST, C.byref(o), res))
+        return X, [_result_dict(res[j], hists[j]) for j in range(k)]
+
     def submit(self, b, x0=None, method="gmres", restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False,
                history_cap=4096, stop_norm="l2", atol=0.0) -> Ticket:
         """Queue one solve on the context's worker threads (Context.serve_start) and return at once."""
@@ -433,7 +473,8 @@ class GpuSetup:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.s2l_gpu_setup_destroy(self.h)
+            if self.ctx.h:  # never after its context is destroyed (Context.close closes its setups first)
+                self.lib.s2l_gpu_setup_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--ref-threads", type=int, default=0, help="reference arm: host threads (0 = all)")
     ap.add_argument("--opt", action="append", default=[], help="device layout option key=value (s2l_gpu_setup_option)")
     ap.add_argument("--batch", default="2,4,8", help="batched form: right-hand sides solved at once (comma list)")
+    ap.add_argument("--block", default="4,8,16", help="block form: right-hand sides per block GMRES (comma list)")
     return ap.parse_args()
 
 
@@ -266,6 +267,39 @@ def run_ours(a):
                            "p50_batch_ms": float(np.percentile(per_b, 50)),
                            "p99_batch_ms": float(np.percentile(per_b, 99))}
         del bs, xs
+    # ---- block form: k right-hand sides in one lockstep block GMRES (s2l_gpu_gmres_block): the
+    # preconditioner, A and the orthogonalization run once per step for all k columns
+    block = {}
+    for k in [int(v) for v in str(a.block).split(",") if v.strip() and int(v) >= 1]:
+        rng = np.random.default_rng(4321)
+        Bk = torch.stack([b_dev] + [torch.tensor(rng.uniform(-1.0, 1.0, n), device=dev) for _ in range(k - 1)])
+        Xk = torch.zeros_like(Bk)
+        res_k = None
+        for _ in range(a.warmup):
+            Xk.zero_()
+            _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
+        barrier()
+        per_k = []
+        for _ in range(a.steps):
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            Xk.zero_()
+            _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
+            e_ev.record(stream)
+            e_ev.synchronize()
+            per_k.append(s_ev.elapsed_time(e_ev))
+        barrier()
+        tot = max_over_ranks(sum(per_k))
+        Xh = Xk.cpu().numpy()
+        chk = max(float(np.linalg.norm(Bk[j].cpu().numpy() - st.A @ Xh[j]) / np.linalg.norm(Bk[j].cpu().numpy()))
+                  for j in range(k))
+        block[str(k)] = {"rhs": k, "ms_per_block": tot / a.steps, "ms_per_solve": tot / a.steps / k,
+                         "solves_per_s": world * k * a.steps / (tot * 1e-3),
+                         "iterations": [r["iterations"] for r in res_k],
+                         "converged": all(r["converged"] for r in res_k), "true_rel_residual_host_check": chk,
+                         "p50_block_ms": float(np.percentile(per_k, 50)),
+                         "p99_block_ms": float(np.percentile(per_k, 99))}
+        del Bk, Xk
     # ---- end to end through the C ABI with pinned host buffers (headline form)
     g, kw = forms["mixed"]
     b_pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -323,6 +357,7 @@ def run_ours(a):
             "plain_fp64": {k: plain[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
                                                   "true_rel_residual_host_check", "p50_ms", "p99_ms")},
             "batched_mixed": batched,
+            "block_mixed": block,
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / head["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": head["iterations"][0] - plain["iterations"][0],
         },

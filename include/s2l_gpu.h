@@ -215,6 +215,16 @@ int s2l_gpu_bicgstab(s2l_setup* s, const double* b, double* x, int ptr_kind, con
 int s2l_gpu_solve_batch(s2l_setup* s, int method, int k, const double* const* b, double* const* x, int ptr_kind,
                         const s2l_krylov_opts* opts, s2l_result* results, int* status);
 
+/* k right-hand sides of one matrix in one block (1 <= k <= 16): every preconditioner application,
+ * product with A and orthogonalization runs once for all k columns (the factors, the matrix and
+ * the coarse basis are read once for all of them), while each column keeps its own GMRES
+ * recurrence, restarts and convergence test (L2 test only).  b and x hold k vectors of n doubles
+ * one after another (column r at b + r * n), on the host or the device as ptr_kind says;
+ * results[r] per column.  s2l_gpu_apply_block is the preconditioner alone, z = M^-1 r per column. */
+int s2l_gpu_apply_block(s2l_setup* s, int k, const double* r, double* z, int ptr_kind);
+int s2l_gpu_gmres_block(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
+                        s2l_result* results);
+
 /* Asynchronous solves: s2l_gpu_serve_start starts `workers` native threads on the context; each
  * s2l_gpu_submit queues one solve (first in, first out) and returns a ticket at once.  b, x,
  * result (and result->history) stay owned by the caller and must stay valid until the ticket is

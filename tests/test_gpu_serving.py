@@ -109,3 +109,39 @@ def test_submit_needs_workers_and_reports_errors():
     t.free()
     g.close()
     ctx.close()
+
+
+def test_hbm_admission_waits_for_memory_instead_of_failing():
+    """With a budget that fits one solve's buffers but not two, concurrent solves on one setup are
+    admitted one after another as workspaces come free (each result the same as alone); with a
+    budget below one solve's buffers the call fails with S2L_ERR_OOM instead of waiting."""
+    from s2l_b200 import capi
+    w, st = small_setup("bubbles3d")
+    probe = capi.Context(0)
+    g0 = capi.GpuSetup(probe, st)
+    d0 = g0.device_bytes()
+    bs = _rhs(st.n, 4, 31)
+    alone = [g0.gmres(b, restart=w.restart, rtol=1e-9) for b in bs]
+    d1 = g0.device_bytes()  # setup + one workspace with its Krylov basis
+    g0.close()
+    probe.close()
+    assert d1 > d0
+    ctx = capi.Context(0, hbm_budget=d1 + (d1 - d0) // 2)
+    ctx.serve_start(4)
+    g = capi.GpuSetup(ctx, st)
+    tickets = [g.submit(b, restart=w.restart, rtol=1e-9) for b in bs]
+    for t, (xa, ra) in zip(tickets, alone):
+        x, r, status = t.wait(300.0)
+        assert status == 0, t.info()["error"]
+        assert r["iterations"] == ra["iterations"] and np.array_equal(x, xa)
+        t.free()
+    assert g.device_bytes() <= d1 + (d1 - d0) // 2
+    g.close()
+    ctx.close()
+    tight = capi.Context(0, hbm_budget=d0 + (d1 - d0) // 4)
+    g = capi.GpuSetup(tight, st)
+    with pytest.raises(capi.S2LError) as e:
+        g.gmres(bs[0], restart=w.restart, rtol=1e-9)
+    assert e.value.code == 2 and "budget" in str(e.value)
+    g.close()
+    tight.close()
