@@ -165,7 +165,7 @@ struct s2l_setup {
     std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
-    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT;
+    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
@@ -185,6 +185,7 @@ struct s2l_setup {
     double* d_Einv = nullptr;
     size_t smem_bytes = 0;
     double solve_bytes = 0.0;
+    double solve_vec_bytes = 0.0;  // the part of solve_bytes that every further right-hand side adds
     int max_T = 0;   // largest sparse part of a subdomain (rows)
     int kc_max = 1;  // right-hand sides a sweep CTA can hold in shared memory (1, 2 or 4)
     // workspaces: one per concurrent solve-phase call (workspace 0 is the caller's default)
@@ -1042,6 +1043,19 @@ int ensure_block(s2l_work* w, int K, int m, bool flex)
     B.m = m;
     B.flex = flex;
     return S2L_OK;
+}
+
+// Widest block that keeps one wave of sparse-sweep CTAs: K/KC CTAs per subdomain on the SMs.
+int block_width_best(s2l_setup* s)
+{
+    if (s->opt_block_width > 0) return s->opt_block_width;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->ctx->device) != cudaSuccess || sms <= 0) sms = 148;
+    const int kc = s->need_gflags ? 1 : s->kc_max;
+    int w = kc * std::max(1, sms / std::max(s->nsub, 1));
+    int p = 1;
+    while (p * 2 <= w && p * 2 <= S2L_MAX_RHS) p *= 2;
+    return p;
 }
 
 size_t sweep_smem(const s2l_setup* s, int kc)
@@ -1980,12 +1994,14 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(dev_alloc(s, &s->d_linv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(dev_alloc(s, &s->d_uinv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(invert_tails(s, Ltt, Utt, d_off));
-    // input gather and owned output of one local solve
+    // input gather and owned output of one local solve (per right-hand side)
+    double vec = 0.0;
     for (int i = 0; i < nsub; ++i) {
         const HostSub& h = s->hs[i];
-        bytes += (double)h.n_local() * (4 + 8) + (double)h.n_owned * (4 + 8 + 8);
+        vec += (double)h.n_local() * (4 + 8) + (double)h.n_owned * (4 + 8 + 8);
     }
-    s->solve_bytes = bytes;
+    s->solve_bytes = bytes + vec;
+    s->solve_vec_bytes = vec;
     RET_IF(upload(s, &s->d_gin, gin));
     RET_IF(upload(s, &s->d_pin, pin));
     RET_IF(upload(s, &s->d_gout, gout));
@@ -2143,6 +2159,11 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         const int g = (int)value;
         if (g != 0 && g != 8 && g != 16 && g != 32) return s->fail(S2L_ERR_BADARG, "sweep_group must be 0, 8, 16 or 32");
         s->opt_group = g;
+    } else if (n == "block_width") {
+        const int bw = (int)value;
+        if (bw != 0 && bw != 1 && bw != 2 && bw != 4 && bw != 8 && bw != 16)
+            return s->fail(S2L_ERR_BADARG, "block_width must be 0, 1, 2, 4, 8 or 16");
+        s->opt_block_width = bw;
     } else if (n == "chain_block") {
         const int c = (int)value;
         if (c < 1 || c > S2L_CHAIN_MAX) return s->fail(S2L_ERR_BADARG, "chain_block must be in [1, 16]");
@@ -2164,6 +2185,9 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "levels_max") *value = (double)s->st_levels_max;
     else if (n == "chain_blocks") *value = (double)s->st_blocks;
     else if (n == "sweep_tasks") *value = (double)s->st_tasks;
+    else if (n == "local_solve_column_bytes") *value = s->solve_vec_bytes;
+    else if (n == "kc_max") *value = (double)s->kc_max;
+    else if (n == "block_width") *value = (double)block_width_best(const_cast<s2l_setup*>(s));
     else if (n == "sweep_padding") *value = (double)s->st_pad;
     else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;
     else return S2L_ERR_BADARG;
@@ -2827,7 +2851,7 @@ int s2l_gpu_apply_block(s2l_setup* s, int k, const double* r, double* z, int ptr
 // the preconditioner, the products with A and the orthogonalization act on all columns at once.
 // A column that has converged, broken down or used maxit gets a zero basis vector, so the shared
 // steps leave it unchanged.  L2 stopping test only.
-static int gmres_block_run(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+static int gmres_block_one(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
                            s2l_result* res)
 {
     RET_IF(check_ready(s));
@@ -3040,6 +3064,31 @@ static int gmres_block_run(s2l_setup* s, int k, const double* b, double* x, int 
         else CUDA_OK(w, cudaMemsetAsync(x + (size_t)r * n, 0, n * sizeof(double), st));
     }
     CUDA_OK(w, cudaStreamSynchronize(st));
+    return S2L_OK;
+}
+
+// k right-hand sides: sub-blocks of the best width, run at once on their own workspaces
+static int gmres_block_run(s2l_setup* s, int k, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* o,
+                           s2l_result* res)
+{
+    RET_IF(check_ready(s));
+    if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
+    if (k < 1 || k > S2L_MAX_RHS) return s->fail(S2L_ERR_BADARG, "a block holds 1 to 16 right-hand sides");
+    const int wb = block_width_best(s);
+    if (k <= wb) return gmres_block_one(s, k, b, x, ptr_kind, o, res);
+    const int64_t n = s->n;
+    const int parts = (k + wb - 1) / wb;
+    std::vector<int> rc(parts, S2L_OK);
+    std::vector<std::thread> th;
+    for (int p = 1; p < parts; ++p)
+        th.emplace_back([&, p] {
+            const int off = p * wb, kk = std::min(wb, k - off);
+            rc[p] = gmres_block_one(s, kk, b + off * n, x + off * n, ptr_kind, o, res + off);
+        });
+    rc[0] = gmres_block_one(s, std::min(wb, k), b, x, ptr_kind, o, res);
+    for (auto& t : th) t.join();
+    for (int v : rc)
+        if (v != S2L_OK) return v;
     return S2L_OK;
 }
 

@@ -477,6 +477,26 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     }
 }
 
+// v[0..K) = p[0..K) with 16-byte (or 8-byte) loads; p is K-aligned in a block vector, so its byte
+// offset is a multiple of K * sizeof(Real)
+template <typename Real, int K>
+__device__ __forceinline__ void load_k(const Real* __restrict__ p, Real (&v)[K])
+{
+    if constexpr (sizeof(Real) * K % 16 == 0) {
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(Real) * K / 16); ++i) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(p) + i);
+            __builtin_memcpy(&v[i * 16 / sizeof(Real)], &t, 16);
+        }
+    } else if constexpr (sizeof(Real) * K == 8) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        __builtin_memcpy(&v[0], &t, 8);
+    } else {
+#pragma unroll
+        for (int r = 0; r < K; ++r) v[r] = p[r];
+    }
+}
+
 // acc[r] = sum_e val[e] * x[col[e] * K + r] over e in [e0, e1), one warp; for K = 1 four
 // independent gathers are in flight per lane, for K > 1 the K columns give the independence
 template <typename Real, int K>
@@ -500,11 +520,22 @@ __device__ __forceinline__ void warp_gather_dot(const Real* __restrict__ val, co
     } else {
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = Real(0);
-        for (int64_t e = e0 + lane; e < e1; e += 32) {
-            const Real v = val[e];
-            const Real* xc = x + (int64_t)col[e] * K;
+        int64_t e = e0 + lane;
+        for (; e + 32 < e1; e += 64) {
+            const int c0 = col[e], c1 = col[e + 32];
+            const Real v0 = val[e], v1 = val[e + 32];
+            Real x0[K], x1[K];
+            load_k<Real, K>(x + (int64_t)c0 * K, x0);
+            load_k<Real, K>(x + (int64_t)c1 * K, x1);
 #pragma unroll
-            for (int r = 0; r < K; ++r) acc[r] += v * xc[r];
+            for (int r = 0; r < K; ++r) acc[r] += v0 * x0[r] + v1 * x1[r];
+        }
+        if (e < e1) {
+            const Real v0 = val[e];
+            Real x0[K];
+            load_k<Real, K>(x + (int64_t)col[e] * K, x0);
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += v0 * x0[r];
         }
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = warp_allsum(acc[r]);  // lane r writes column r
@@ -571,10 +602,21 @@ __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Rea
         Real acc[K];
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = Real(0);
-        for (int j = j0 + lane; j < j1; j += 32) {
-            const Real m = row[j];
+        int j = j0 + lane;
+        for (; j + 32 < j1; j += 64) {
+            const Real m0 = row[j], m1 = row[j + 32];
+            Real v0[K], v1[K];
+            load_k<Real, K>(v + (int64_t)j * K, v0);
+            load_k<Real, K>(v + (int64_t)(j + 32) * K, v1);
 #pragma unroll
-            for (int r = 0; r < K; ++r) acc[r] += m * v[(int64_t)j * K + r];
+            for (int r = 0; r < K; ++r) acc[r] += m0 * v0[r] + m1 * v1[r];
+        }
+        if (j < j1) {
+            const Real m0 = row[j];
+            Real v0[K];
+            load_k<Real, K>(v + (int64_t)j * K, v0);
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += m0 * v0[r];
         }
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = warp_allsum(acc[r]);  // lane r writes column r
@@ -915,13 +957,15 @@ __global__ void combine_block_kernel(int64_t n, const int64_t* __restrict__ cp_p
 }
 
 // c_i(c, r) = V_i(:, c)^T R(:, r) per 256-row tile of one subdomain: partials[(tile * mmax + c) * K + r].
+// Every warp sums its 32 rows for all (c, r) into shared memory (mmax * K values per warp, dynamic),
+// then the CTA adds the warps' sums: one barrier per tile.
 template <int K>
 __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
     const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
     const DevSub* __restrict__ subs, const double* __restrict__ V, const int32_t* __restrict__ l2g, int boolean_pou,
     const double* __restrict__ R, int mmax, double* __restrict__ partials)
 {
-    __shared__ double red[S2L_TILE_ROWS / 32][K];
+    extern __shared__ double red[];  // [S2L_TILE_ROWS / 32][mmax * K]
     const int tile = blockIdx.x;
     const DevSub sd = subs[t_sub[tile]];
     const int m = sd.m, nr = t_nrow[tile];
@@ -934,25 +978,24 @@ __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
     for (int r = 0; r < K; ++r) rv[r] = 0.0;
     if (act) {
         const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
-#pragma unroll
-        for (int r = 0; r < K; ++r) rv[r] = R[g * K + r];
+        load_k<double, K>(R + g * K, rv);
         vr = V + sd.v_off + (int64_t)l * m;
     }
+    double* wred = red + (size_t)warp * mmax * K;
     for (int c = 0; c < m; ++c) {
         const double vc = act ? vr[c] : 0.0;
 #pragma unroll
         for (int r = 0; r < K; ++r) {
             const double p = warp_sum(vc * rv[r]);
-            if (lane == 0) red[warp][r] = p;
+            if (lane == 0) wred[c * K + r] = p;
         }
-        __syncthreads();
-        if (threadIdx.x < K) {
-            double s = 0.0;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m * K; e += S2L_TILE_ROWS) {
+        double t = 0.0;
 #pragma unroll
-            for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) s += red[w][threadIdx.x];
-            partials[((int64_t)tile * mmax + c) * K + threadIdx.x] = s;
-        }
-        __syncthreads();
+        for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) t += red[(size_t)w * mmax * K + e];
+        partials[(int64_t)tile * mmax * K + e] = t;
     }
 }
 
@@ -1152,8 +1195,11 @@ void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int3
                                   int boolean_pou, const double* R, int mmax, double* partials)
 {
     if (ntiles <= 0) return;
-    S2L_KSWITCH(K, (coarse_restrict_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, 0, st>>>(
-                       t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials)));
+    const size_t smem = (size_t)(S2L_TILE_ROWS / 32) * mmax * K * sizeof(double);  // <= 131 KB (mmax <= 128, K <= 16)
+    S2L_KSWITCH(K, (cudaFuncSetAttribute(coarse_restrict_block_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)(S2L_TILE_ROWS / 32) * S2L_MAX_RED_COLS * KK * sizeof(double))),
+                    coarse_restrict_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, smem, st>>>(
+                        t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials)));
 }
 
 void launch_coarse_reduce_block(cudaStream_t st, int K, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,

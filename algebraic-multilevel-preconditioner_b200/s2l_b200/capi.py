@@ -413,7 +413,12 @@ class GpuSetup:
             return device_out, [_result_dict(res[j], hists[j]) for j in range(k)]
         B = np.ascontiguousarray(np.atleast_2d(B), dtype=np.float64)
         k = B.shape[0]
-        X = np.zeros_like(B) if X0 is None else np.ascontiguousarray(X0, dtype=np.float64).copy()
+        if X0 is None:
+            X = np.zeros_like(B)
+        elif isinstance(X0, np.ndarray) and X0.dtype == np.float64 and X0.flags.c_contiguous and X0.shape == B.shape:
+            X = X0  # used in place (keeps a pinned buffer pinned)
+        else:
+            X = np.array(X0, dtype=np.float64)
         res = (Result * k)()
         hists = [np.zeros(max(history_cap, 1)) for _ in range(k)]
         for j in range(k):

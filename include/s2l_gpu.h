@@ -143,6 +143,9 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
  *   "sweep_group" (0 = 32, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
  *   entries get G lanes, 32 / G rows of one dependency level share a warp);
+ *   "block_width" (0 = automatic, 1, 2, 4, 8 or 16): the most right-hand sides s2l_gpu_gmres_block
+ *   puts in one block; larger k run as several blocks at once (automatic: the widest block whose
+ *   sparse-sweep CTAs fit the SMs in one wave);
  *   "chain_block" (1..16, default 8; 1 = off): rows of a chain block.  Runs of sparse rows where
  *   each row depends on the one solved just before it (the rows of a supernode) are cut into
  *   blocks of up to this many rows; a block's rows are stored multiplied by the inverse of its
@@ -158,7 +161,11 @@ int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
 /* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
    "sweep_group", "smem_bytes", "levels_max" / "levels_mean" (dependency levels of a sparse sweep,
    largest and mean over subdomains and both factors), "chain_blocks", "sweep_tasks" and
-   "sweep_padding" (padding entries of the lane-interleaved task layout), both factors. */
+   "sweep_padding" (padding entries of the lane-interleaved task layout), both factors;
+   "local_solve_column_bytes": the part of s2l_gpu_local_solve_bytes that each further right-hand
+   side of a block adds (a block of k reads the factors once: bytes + (k - 1) x this);
+   "kc_max": right-hand sides a sparse-sweep CTA holds in shared memory; "block_width": the block
+   width s2l_gpu_gmres_block uses. */
 int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 
 /* ---- solve phase ----------------------------------------------------------------------

@@ -116,3 +116,20 @@ def test_gmres_block_rejects_bad_arguments(ctx):
     with pytest.raises(S2LError):
         g.gmres_block(np.ones((16, st.n)), restart=100)  # (restart + 1) x 16 coefficients too many
     g.close()
+
+
+def test_gmres_block_split_into_concurrent_sub_blocks(ctx):
+    """k above the block width runs as several blocks at once (here forced to width 2): each
+    column still matches its single solve."""
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st, options={"block_width": 2})
+    assert g.stat("block_width") == 2
+    B = np.random.default_rng(8).uniform(-1.0, 1.0, (7, st.n))
+    X, res = g.gmres_block(B, restart=w.restart, rtol=1e-8)
+    for j in range(7):
+        xs, rs = g.gmres(B[j], restart=w.restart, rtol=1e-8)
+        assert res[j]["converged"] and abs(res[j]["iterations"] - rs["iterations"]) <= 1
+        assert np.linalg.norm(B[j] - st.A @ X[j]) <= 1.1e-8 * np.linalg.norm(B[j])
+        assert rel(X[j], xs) <= 1e-6
+    g.close()
