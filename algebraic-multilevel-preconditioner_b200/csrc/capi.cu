@@ -165,7 +165,8 @@ struct s2l_setup {
     std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
-    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0;
+    int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0,
+        opt_tpr = 0;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
@@ -1731,7 +1732,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
             for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) rowsum[r] += s->A.v[e];
         RET_IF(upload(s, &s->d_rowsum, rowsum));
         const double avg = (double)s->nnz / (double)s->n;
-        s->tpr = avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32));
+        s->tpr = s->opt_tpr ? s->opt_tpr : (avg <= 4.5 ? 4 : (avg <= 9 ? 8 : (avg <= 20 ? 16 : 32)));
     }
 
     // ---- per-subdomain factor split, sweep layouts and index maps
@@ -2102,7 +2103,8 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 s->kc_max = kc;
     CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
     // host staging no longer needed
-    s->A = HostCsr();
+    s->A.ci = {};  // the row pointers stay: s2l_gpu_update_matrix recomputes the row sums with them
+    s->A.v = {};
     for (auto& h : s->hs) {
         h.L = HostCsr();
         h.U = HostCsr();
@@ -2135,6 +2137,38 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
     return S2L_OK;
 }
 
+// New values of A, same pattern (the reference's UpdateLevel::Reuse,
+// include/preconditioner/preconditioner.hpp:20-30): the operator changes, the preconditioner stays.
+int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!val) return s->fail(S2L_ERR_BADARG, "null values");
+    if (ptr_kind != S2L_PTR_HOST && ptr_kind != S2L_PTR_DEVICE)
+        return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    std::lock_guard<std::mutex> g(s->wmu);  // no call can take a workspace meanwhile
+    for (char b : s->busy)
+        if (b) return s->fail(S2L_ERR_STATE, "update_matrix while a solve-phase call runs on the setup");
+    if (s->pending.load() > 0) return s->fail(S2L_ERR_STATE, "update_matrix while solves are queued on the setup");
+    if (cudaSetDevice(s->ctx->device) != cudaSuccess) return s->fail(S2L_ERR_CUDA, "cudaSetDevice failed");
+    const int64_t n = s->n, nnz = s->nnz;
+    std::vector<double> v((size_t)nnz);
+    if (ptr_kind == S2L_PTR_HOST) {
+        std::copy(val, val + nnz, v.begin());
+    } else {
+        CUDA_OK(s, cudaMemcpyAsync(v.data(), val, nnz * sizeof(double), cudaMemcpyDeviceToHost, s->setup_stream));
+        CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
+    }
+    for (int64_t e = 0; e < nnz; ++e)
+        if (!std::isfinite(v[e])) return s->fail(S2L_ERR_NUMERIC, "non-finite matrix value");
+    std::vector<double> rowsum((size_t)n, 0.0);  // A 1, in row order as at setup
+    for (int64_t r = 0; r < n; ++r)
+        for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) rowsum[r] += v[e];
+    CUDA_OK(s, cudaMemcpyAsync(s->d_av, v.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, s->setup_stream));
+    CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, rowsum.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->setup_stream));
+    CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
+    return S2L_OK;
+}
+
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
 {
     if (!s || !bytes) return S2L_ERR_BADARG;
@@ -2159,6 +2193,11 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         const int g = (int)value;
         if (g != 0 && g != 8 && g != 16 && g != 32) return s->fail(S2L_ERR_BADARG, "sweep_group must be 0, 8, 16 or 32");
         s->opt_group = g;
+    } else if (n == "spmv_tpr") {
+        const int t = (int)value;
+        if (t != 0 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32)
+            return s->fail(S2L_ERR_BADARG, "spmv_tpr must be 0, 2, 4, 8, 16 or 32");
+        s->opt_tpr = t;
     } else if (n == "block_width") {
         const int bw = (int)value;
         if (bw != 0 && bw != 1 && bw != 2 && bw != 4 && bw != 8 && bw != 16)
@@ -2187,6 +2226,7 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "sweep_tasks") *value = (double)s->st_tasks;
     else if (n == "local_solve_column_bytes") *value = s->solve_vec_bytes;
     else if (n == "kc_max") *value = (double)s->kc_max;
+    else if (n == "spmv_tpr") *value = (double)s->tpr;
     else if (n == "block_width") *value = (double)block_width_best(const_cast<s2l_setup*>(s));
     else if (n == "sweep_padding") *value = (double)s->st_pad;
     else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;

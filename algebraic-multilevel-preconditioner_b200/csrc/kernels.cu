@@ -1078,6 +1078,7 @@ void launch_spmv(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* c
     // lane group per row
     const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
     switch (tpr) {
+    case 2: spmv_kernel<2><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 4: spmv_kernel<4><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 16: spmv_kernel<16><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 32: spmv_kernel<32><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
@@ -1135,7 +1136,9 @@ void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, con
                        const double* X, double* Y, const double* B, double* partials, double* red_out, int tpr)
 {
     const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
-    if (tpr == 4) {
+    if (tpr == 2) {
+        S2L_KSWITCH(K, (spmv_block_kernel<2, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    } else if (tpr == 4) {
         S2L_KSWITCH(K, (spmv_block_kernel<4, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
     } else if (tpr == 16) {
         S2L_KSWITCH(K, (spmv_block_kernel<16, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));

@@ -33,7 +33,7 @@ EXPORTED = [
     "s2l_gpu_profile_enable", "s2l_gpu_profile_get", "s2l_gpu_local_solve_bytes", "s2l_gpu_setup_option",
     "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
-    "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block",
+    "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block", "s2l_gpu_update_matrix",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -110,6 +110,7 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_ticket_info": ([vp, dp, dp, C.POINTER(C.c_char_p)], C.c_int),
         "s2l_gpu_ticket_free": ([vp], C.c_int),
         "s2l_gpu_apply_block": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_update_matrix": ([vp, vp, C.c_int], C.c_int),
         "s2l_gpu_gmres_block": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -387,6 +388,11 @@ class GpuSetup:
         if rc != S2L_OK and all(v == S2L_OK for v in st):
             self.ctx.check(rc)
         return [(xs[j], _result_dict(res[j], hists[j]), st[j]) for j in range(k)]
+
+    def update_matrix(self, values):
+        """New values of A (same pattern, renumbered CSR order); the preconditioner is kept."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.ctx.check(self.lib.s2l_gpu_update_matrix(self.h, _vp(v), PTR_HOST))
 
     def apply_block(self, R):
         """Z = M^-1 R for the k rows of R (k x n, host), one block call (s2l_gpu_apply_block)."""

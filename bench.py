@@ -4,12 +4,16 @@
 Workload (default): 3D 7-point variable-coefficient pressure Poisson 100^3 (n = 1.0M),
 beta = 1/rho with rho = 1e-3 in 200 seeded spheres of radius 3-8 cells, 64 subdomains (recursive
 coordinate bisection), overlap 2, nev 20, deflated two-level RAS, local L L^T, GMRES(50),
-rtol 1e-8, U[-1,1] right-hand side (seed 12345).  Two forms are timed:
-  plain_fp64  : FP64 factors, the reference's GMRES (true-residual restart rule),
+rtol 1e-8, U[-1,1] right-hand sides.  Forms timed:
+  plain_fp64  : FP64 factors, the reference's GMRES (true-residual restart rule), one solve per step;
   mixed       : the same factors stored in FP32 + flexible GMRES(50) in FP64, converged only when
-                the recomputed FP64 true residual is <= rtol.
-A step is one full solve from x0 = 0.  `value` = solves/s of the mixed form with b resident in
-HBM; `e2e` = the same through the C ABI with host buffers (copies inside the timed region).
+                the recomputed FP64 true residual is <= rtol, one solve per step;
+  block_mixed : the mixed form for k right-hand sides per step (s2l_gpu_gmres_block);
+  batched / block_mixed_threads: several solves or blocks from host threads at once;
+  serving     : Poisson arrivals over three resident matrices on the worker threads (p50/p99).
+Headline (`value`): block_mixed at --head-k right-hand sides per step (default 16, the batching
+configuration's right-hand sides per matrix), solves/s with b resident in HBM; `e2e` = the same
+through the C ABI with pinned host buffers (copies inside the timed region).
 
 --impl reference times the reference itself (built from its sources into oracle/_ref/ with an
 in-process thread-rank MPI) on the host cores, same problem and partition.
@@ -50,7 +54,9 @@ def parse():
     ap.add_argument("--opt", action="append", default=[], help="device layout option key=value (s2l_gpu_setup_option)")
     ap.add_argument("--batch", default="2,4,8", help="batched form: right-hand sides solved at once (comma list)")
     ap.add_argument("--block", default="4,8,16", help="block form: right-hand sides per block GMRES (comma list)")
-    ap.add_argument("--head-k", type=int, default=4, help="right-hand sides of the headline block form")
+    ap.add_argument("--head-k", type=int, default=16, help="right-hand sides per step of the headline block form")
+    ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
     return ap.parse_args()
 
@@ -104,6 +110,22 @@ class ClockSampler:
         os.unlink(self.f.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_traffic(algorithmic_bytes: float):
+    """DRAM bytes of one block local solve from the committed ncu summary (measured on a smaller
+    case of the same workload, scaled by its algorithmic bytes), or None."""
+    path = os.path.join(REPO, "profiles", "local_solve_block_traffic.txt")
+    try:
+        vals = {}
+        for line in open(path):
+            if ":" in line and not line.startswith("#"):
+                k, v = line.split(":", 1)
+                vals[k.strip()] = v.strip()
+        ratio = float(vals["traffic_over_algorithmic_bytes"])
+        return ratio * algorithmic_bytes
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def measured_peaks():
@@ -270,11 +292,14 @@ def run_ours(a):
     # preconditioner, A and the orthogonalization run once per step for all k columns
     block = {}
     head = None
+    bw = int(g.stat("block_width"))  # one block of this width is the unit wider steps run concurrently
     ks = [int(v) for v in str(a.block).split(",") if v.strip() and int(v) >= 1]
-    if a.head_k not in ks:
-        ks = [a.head_k] + ks
+    for extra in (bw, a.head_k):
+        if extra not in ks:
+            ks = [extra] + ks
     for k in ks:
         is_head = k == a.head_k
+        is_rf = k == bw
         rng = np.random.default_rng(4321)
         Bk = torch.stack([b_dev] + [torch.tensor(rng.uniform(-1.0, 1.0, n), device=dev) for _ in range(k - 1)])
         Xk = torch.zeros_like(Bk)
@@ -282,8 +307,9 @@ def run_ours(a):
         for _ in range(a.warmup):
             Xk.zero_()
             _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
-        if is_head:
+        if is_rf:
             g.profile(("local_solve",))
+        if is_head:
             sampler = ClockSampler(local)
             sampler.start()
         barrier()
@@ -300,8 +326,9 @@ def run_ours(a):
         tot = max_over_ranks(sum(per_k))
         if is_head:
             head_clocks = sampler.stop()
-            head_ls = g.profile_get("local_solve")
-            head_launches = g.launches()
+        if is_rf:
+            rf_ls = g.profile_get("local_solve")
+            rf_launches = g.launches()
             g.profile(())
         Xh = Xk.cpu().numpy()
         chk = max(float(np.linalg.norm(Bk[j].cpu().numpy() - st.A @ Xh[j]) / np.linalg.norm(Bk[j].cpu().numpy()))
@@ -313,7 +340,9 @@ def run_ours(a):
                          "p50_block_ms": float(np.percentile(per_k, 50)),
                          "p99_block_ms": float(np.percentile(per_k, 99))}
         if is_head:
-            head = dict(block[str(k)], per_block_ms=per_k, clocks=head_clocks, ls=head_ls, launches=head_launches)
+            head = dict(block[str(k)], per_block_ms=per_k, clocks=head_clocks)
+        if is_rf:
+            rf = dict(ls=rf_ls, launches=rf_launches, steps=a.steps)
         del Bk, Xk
     # ---- several k=4 blocks at once from host threads (each on its own workspace and stream)
     block_thr = {}
@@ -360,6 +389,57 @@ def run_ours(a):
         block_thr[str(nt)] = {"threads": nt, "rhs_per_block": 4, "solves_per_s": world * 4 * nt * a.steps / (tot * 1e-3),
                               "converged": all(conv_t)}
         del Bs, Xs
+    # ---- serving: Poisson arrivals of solve requests over three resident matrices (this workload in
+    # mixed precision, the 2D Poisson case, a convection-diffusion case with FP32 LU factors) on the
+    # engine's worker threads; latency = request submitted -> solution ready (host clock)
+    serving = None
+    if a.serve > 0:
+        from s2l_b200.serving import Engine
+        cases = {"bubbles3d": (lambda: st32, dict(restart=wl.restart, rtol=wl.rtol, flexible=True, strict=True))}
+        wp = W.poisson2d()
+        st_p = W.build(wp)
+        cases["poisson2d"] = (lambda: st_p, dict(restart=wp.restart, rtol=wp.rtol))
+        wc = W.convdiff3d(32, 8)
+        st_c = W.build(wc)
+        cases["convdiff3d"] = (lambda: st_c, dict(restart=wc.restart, rtol=wc.rtol, flexible=True, strict=True))
+        eng = Engine(local, hbm_budget=150 << 30, workers=4)
+        for key, (mk, kwk) in cases.items():  # warm: setups built and resident before the arrivals
+            t = eng.submit(key, mk, mk().b, **kwk)
+            t.wait(600.0)
+            t.free()
+        rng = np.random.default_rng(2026)
+        keys = list(cases)
+        mix = [0.5, 0.25, 0.25]
+        gaps = rng.exponential(1.0 / a.serve_rate, a.serve)
+        picks = rng.choice(len(keys), a.serve, p=mix)
+        tickets = []
+        t0 = time.perf_counter()
+        t_next = t0
+        for i in range(a.serve):
+            t_next += gaps[i]
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            key = keys[picks[i]]
+            mk, kwk = cases[key]
+            b_i = rng.uniform(-1.0, 1.0, mk().n)
+            tickets.append((key, eng.submit(key, mk, b_i, history_cap=0, **kwk)))
+        lat = []
+        ok = True
+        for key, t in tickets:
+            _, r, status = t.wait(600.0)
+            ok = ok and status == 0 and r["converged"]
+            info = t.info()
+            lat.append(info["queue_ms"] + info["run_ms"])
+            t.free()
+        t_end = time.perf_counter()
+        serving = {"requests": a.serve, "rate_req_s": a.serve_rate, "mix": dict(zip(keys, mix)),
+                   "all_converged": ok, "solves_per_s": a.serve / (t_end - t0),
+                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                   "max_ms": float(np.max(lat)), "workers": 4, "setups_built": eng.builds,
+                   "clock": "host (submit to solution ready)"}
+        eng.close()
+
     # ---- end to end through the C ABI with pinned host buffers (headline block form): each step
     # copies its k right-hand sides and initial guesses in and its k solutions out
     g, kw = forms["mixed"]
@@ -387,8 +467,9 @@ def run_ours(a):
     plain = results["plain_fp64"]
     # roofline of the headline's dominant kernel group: the block local solve (factors read once,
     # every column's gather and owned write)
-    head_bytes = g32.local_solve_bytes() + (kh - 1) * g32.stat("local_solve_column_bytes")
-    ls_avg_ms = head["ls"][0] / max(head["ls"][1], 1)
+    head_bytes = g32.local_solve_bytes() + (bw - 1) * g32.stat("local_solve_column_bytes")
+    ls_avg_ms = rf["ls"][0] / max(rf["ls"][1], 1)
+    traffic = measured_traffic(head_bytes)
     achieved = head_bytes / (ls_avg_ms * 1e-3) / 1e9 if ls_avg_ms > 0 else 0.0
     ls_avg_ms32 = mixed["local_solve_ms_total"] / max(mixed["local_solve_launches"], 1)
     achieved32 = mixed["local_solve_bytes"] / (ls_avg_ms32 * 1e-3) / 1e9 if ls_avg_ms32 > 0 else 0.0
@@ -433,6 +514,7 @@ def run_ours(a):
                                                   "true_rel_residual_host_check", "p50_ms", "p99_ms")},
             "batched_mixed": batched,
             "block_mixed_threads": block_thr,
+            "serving": serving,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": mixed["iterations"][0] - plain["iterations"][0],
@@ -444,15 +526,18 @@ def run_ours(a):
                 "h2d_bytes_per_step": 2 * 8 * n * kh, "d2h_bytes_per_step": 8 * n * kh,
                 "ms_per_step": e2e_total / a.steps},
         "roofline": {"bound": "hbm",
-                     "kernel": f"local_solve of the headline block ({kh} columns: sweeps, tail coupling, dense tails)",
+                     "kernel": f"local solve of one {bw}-column block (sweeps, tail coupling, dense tails); the "
+                               f"{kh}-column step runs {max(kh // bw, 1)} such blocks at once",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_src, "traffic": None,
+                     "peak_source": peak_src, "traffic": traffic,
                      "bytes_per_launch": head_bytes, "avg_launch_ms": ls_avg_ms,
                      "single_column_fp32": {"achieved": achieved32, "frac": achieved32 / peak,
                                             "avg_launch_ms": ls_avg_ms32, "bytes_per_launch": mixed["local_solve_bytes"]},
                      "single_column_fp64": {"achieved": achieved64, "frac": achieved64 / peak,
                                             "avg_launch_ms": ls_avg_ms64, "bytes_per_launch": plain["local_solve_bytes"]}},
-        "gpu_launches": head["launches"],
+        # kernels launched in the timed region: those of the timed k=bw blocks, times the blocks
+        # a k=head step runs at once
+        "gpu_launches": int(rf["launches"] * max(kh // bw, 1)),
         "clocks": head["clocks"],
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -143,6 +143,7 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
  *   "sweep_group" (0 = 32, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
  *   entries get G lanes, 32 / G rows of one dependency level share a warp);
+ *   "spmv_tpr" (0 = from the mean row length, 2, 4, 8, 16 or 32): lanes per row of the products with A;
  *   "block_width" (0 = automatic, 1, 2, 4, 8 or 16): the most right-hand sides s2l_gpu_gmres_block
  *   puts in one block; larger k run as several blocks at once (automatic: the widest block whose
  *   sparse-sweep CTAs fit the SMs in one wave);
@@ -156,6 +157,13 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 int s2l_gpu_setup_end(s2l_setup* s);
 int s2l_gpu_setup_destroy(s2l_setup* s);
 
+/* New values of A with the pattern given to s2l_gpu_set_matrix (nnz doubles, host or device as
+ * ptr_kind says); the preconditioner (factors, coarse basis, E) is kept.  This is the reference's
+ * UpdateLevel::Reuse along a sequence of matrices (include/preconditioner/preconditioner.hpp:20-30):
+ * the Krylov solves then use the new operator with the lagged preconditioner.  Refused
+ * (S2L_ERR_STATE) while a solve-phase call runs or solves are queued on the setup. */
+int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind);
+
 /* Device bytes held by the setup (matrix, factors, basis, schedules) and its workspaces. */
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
 /* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
@@ -164,7 +172,8 @@ int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
    "sweep_padding" (padding entries of the lane-interleaved task layout), both factors;
    "local_solve_column_bytes": the part of s2l_gpu_local_solve_bytes that each further right-hand
    side of a block adds (a block of k reads the factors once: bytes + (k - 1) x this);
-   "kc_max": right-hand sides a sparse-sweep CTA holds in shared memory; "block_width": the block
+   "kc_max": right-hand sides a sparse-sweep CTA holds in shared memory; "spmv_tpr": lanes per row
+   of the products with A; "block_width": the block
    width s2l_gpu_gmres_block uses. */
 int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 

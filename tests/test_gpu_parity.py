@@ -282,3 +282,23 @@ def test_forced_tail_single_precision(ctx, rng):
         b = rng.standard_normal(s.n_local)
         assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-5
     g.close()
+
+
+@pytest.mark.parametrize("tpr", [2, 4, 8, 16, 32])
+def test_spmv_lanes_per_row(ctx, rng, tpr):
+    """Every lanes-per-row choice of the product with A gives the CSR product (1e-14), for one
+    column and for a block of columns."""
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup("convdiff3d")
+    g = GpuSetup(ctx, st, options={"spmv_tpr": tpr})
+    assert g.stat("spmv_tpr") == tpr
+    x = rng.standard_normal(st.n)
+    assert rel(g.spmv(x), st.A @ x) <= 1e-14
+    xs, res = g.gmres(st.b, restart=40, rtol=1e-8)
+    assert res["converged"] and np.linalg.norm(st.b - st.A @ xs) <= 1.1e-8 * np.linalg.norm(st.b)
+    B = np.random.default_rng(3).uniform(-1.0, 1.0, (4, st.n))
+    X, rb = g.gmres_block(B, restart=40, rtol=1e-8)
+    assert all(r["converged"] for r in rb)
+    for j in range(4):
+        assert np.linalg.norm(B[j] - st.A @ X[j]) <= 1.1e-8 * np.linalg.norm(B[j])
+    g.close()

@@ -145,3 +145,41 @@ def test_hbm_admission_waits_for_memory_instead_of_failing():
     assert e.value.code == 2 and "budget" in str(e.value)
     g.close()
     tight.close()
+
+
+def test_engine_caches_setups_and_evicts_idle_ones_under_the_budget():
+    """Setups are cached per matrix (a repeated request builds nothing); with a budget that holds two
+    of the three setups, a request on the third evicts the least recently used idle one; every
+    result equals the same solve on a context of its own."""
+    from s2l_b200 import capi
+    from s2l_b200.serving import Engine
+    cases = {"a": small_setup("bubbles3d")[1], "b": small_setup("poisson2d")[1], "c": small_setup("convdiff3d")[1]}
+    probe = capi.Context(0)
+    size, alone = {}, {}
+    for key, st in cases.items():
+        g = capi.GpuSetup(probe, st)
+        alone[key] = g.gmres(st.b, restart=30, rtol=1e-9)
+        size[key] = g.device_bytes()
+        g.close()
+    probe.close()
+    pair = max(size["a"] + size["b"], size["b"] + size["c"], size["a"] + size["c"])
+    budget = pair + min(size.values()) // 4
+    assert budget < sum(size.values())
+    eng = Engine(0, hbm_budget=budget, workers=2)
+    made = []
+
+    def maker(key):
+        def make():
+            made.append(key)
+            return cases[key]
+        return make
+
+    for key in ("a", "b", "a", "c", "b", "a"):
+        t = eng.submit(key, maker(key), cases[key].b, restart=30, rtol=1e-9)
+        x, r, status = t.wait(120.0)
+        assert status == 0, t.info()["error"]
+        assert r["iterations"] == alone[key][1]["iterations"] and np.array_equal(x, alone[key][0])
+        t.free()
+    assert made[:2] == ["a", "b"] and "c" in made  # the repeated "a" hit the cache
+    assert eng.evictions >= 1 and len(eng.resident()) <= 2
+    eng.close()
