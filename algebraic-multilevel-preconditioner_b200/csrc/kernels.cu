@@ -423,6 +423,7 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                                 break;
                             }
                         }
+                        if (S2L_SPIN_SLEEP_NS > 0 && spin > 8) __nanosleep(S2L_SPIN_SLEEP_NS);
                     }
 #pragma unroll
                     for (int r = 0; r < KC; ++r) acc[r] += lv[q] * x[c * xstride + r];

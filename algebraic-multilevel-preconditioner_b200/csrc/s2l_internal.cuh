@@ -31,6 +31,9 @@
 #define S2L_CHAIN_MAX 16
 #define S2L_SWEEP_SMEM_CAP (227 * 1024 - 64)  // dynamic shared memory of a sweep CTA, at most
 #define S2L_ADMIT_WAIT_S 600   // longest wait of a call for a free workspace when the HBM budget is full
+#ifndef S2L_SPIN_SLEEP_NS
+#define S2L_SPIN_SLEEP_NS 0   // back-off of a sweep poll after its first 8 (ns; 0 = poll without pause)
+#endif
 #define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {

@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--block", default="4,8,16", help="block form: right-hand sides per block GMRES (comma list)")
     ap.add_argument("--head-k", type=int, default=16, help="right-hand sides per step of the headline block form")
     ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
+    ap.add_argument("--seq", type=int, default=4, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
     return ap.parse_args()
@@ -463,6 +464,44 @@ def run_ours(a):
     barrier()
     e2e_total = max_over_ranks(sum(e2e))
 
+    # ---- sequence: the next matrices of the moving-bubble sequence (bubble centres rise half a cell
+    # per step, same pattern) through s2l_gpu_update_matrix, the preconditioner of the first matrix
+    # kept (the reference's reuse level), each solved for head_k right-hand sides
+    sequence = None
+    if a.seq > 0:
+        import dataclasses
+        import scipy.sparse as sp
+        from s2l_b200 import sequence as seqmod
+        g, kw = forms["mixed"]
+        rng = np.random.default_rng(77)
+        Bq = torch.tensor(rng.uniform(-1.0, 1.0, (kh, n)), device=dev)
+        Xq = torch.zeros_like(Bq)
+        steps_q = []
+        for step in range(a.seq):
+            prob = W.make_problem(dataclasses.replace(wl, time=float(step)))
+            vals, _ = seqmod.values_in_setup_order(prob.A, st)
+            At = sp.csr_matrix((vals, st.A.indices, st.A.indptr), shape=st.A.shape)
+            barrier()
+            s_ev, m_ev, e_ev = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            s_ev.record(stream)
+            g.update_matrix(vals)
+            m_ev.record(stream)
+            Xq.zero_()
+            _, rq = g.gmres_block((Bq.data_ptr(), kh), device_out=Xq.data_ptr(), **kw)
+            e_ev.record(stream)
+            e_ev.synchronize()
+            Xh = Xq.cpu().numpy()
+            Bh = Bq.cpu().numpy()
+            chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(kh))
+            steps_q.append({"step": step, "update_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
+                            "iterations_max": max(r["iterations"] for r in rq),
+                            "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
+        g.update_matrix(st.A.data)  # back to the setup's own matrix
+        tot_ms = sum(q["update_ms"] + q["solve_ms"] for q in steps_q)
+        sequence = {"matrices": a.seq, "rhs_per_matrix": kh, "steps": steps_q,
+                    "solves_per_s": a.seq * kh / (tot_ms * 1e-3)}
+        del Bq, Xq
+
     mixed = results["mixed"]
     plain = results["plain_fp64"]
     # roofline of the headline's dominant kernel group: the block local solve (factors read once,
@@ -515,6 +554,7 @@ def run_ours(a):
             "batched_mixed": batched,
             "block_mixed_threads": block_thr,
             "serving": serving,
+            "sequence_reuse": sequence,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": mixed["iterations"][0] - plain["iterations"][0],

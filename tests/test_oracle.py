@@ -112,3 +112,28 @@ def test_openfoam_norm_warm_start(method):
     r1 = np.abs(st.b - st.A @ x).sum()
     assert res["converged"] and r1 <= 1.1e-6 * r0
     assert abs(res["final_residual_of"] - r1 / F) <= 1e-9 * r1 / F
+
+
+def test_sequence_values_in_setup_order(tmp_path):
+    """A Matrix Market sequence step lands in the setup's renumbered CSR order (the reference's
+    DomainDecomposer::updateValues), and a changed pattern is refused."""
+    import dataclasses
+    import scipy.io
+    import scipy.sparse as sp
+    from s2l_b200 import sequence, workloads as W
+    w = W.bubbles3d(10, 4, nbubbles=4)
+    st = W.build(w, workers=1, use_cache=False)
+    prob = W.make_problem(dataclasses.replace(w, time=2.0))
+    scipy.io.mmwrite(str(tmp_path / "p_0002.mtx"), prob.A)
+    vals, b = sequence.load_step(str(tmp_path / "p_%04d.mtx"), 2, st)
+    n2o = sequence.new_to_old(st)
+    expect = prob.A.tocsr()[n2o][:, n2o].tocsr()
+    expect.sort_indices()
+    assert np.array_equal(vals, expect.data) and b is None
+    x = np.random.default_rng(1).standard_normal(st.n)
+    A2 = sp.csr_matrix((vals, st.A.indices, st.A.indptr), shape=st.A.shape)
+    assert np.allclose(A2 @ x, (prob.A @ x[np.argsort(n2o)])[n2o], rtol=1e-13, atol=1e-12)
+    bad = prob.A.tolil()
+    bad[0, st.n - 1] = 1.0
+    with pytest.raises(sequence.PatternChanged):
+        sequence.values_in_setup_order(bad.tocsr(), st)
