@@ -107,6 +107,16 @@ struct Sweep {
     std::vector<int64_t> blk_off{0}, blk_ioff{0};
     std::vector<int32_t> blk_slot;
     std::vector<double> blk_inv;
+    // refactorization maps (built when build_sweep is given the factor position of every entry of
+    // its matrix): per entry of `col` the position of its value (-1 padding, -2 a row of a chain
+    // block), per slot the position of the row's diagonal (-1: 1 / diagonal = 1), per block the
+    // positions of W packed like blk_inv (-1: 0 off the diagonal, 1 on it), and the entries of the
+    // blocks' rewritten rows: entry index in `col`, row within the block, and its contributions
+    // (block row b, position of M(B[b], c)) of  sum_b W^-1(row, b) M(B[b], c)
+    std::vector<int32_t> src, dsrc, blk_wsrc;
+    std::vector<int64_t> be_off{0}, be_pos, be_cp{0};
+    std::vector<uint8_t> be_row, bc_b;
+    std::vector<int32_t> bc_pos;
 };
 
 }  // namespace
@@ -198,6 +208,33 @@ struct s2l_setup {
     unsigned prof_mask = 0;              // s2l_gpu_profile_enable: inherited by new workspaces
 
     std::atomic<int> pending{0};  // asynchronous solves queued or running on this setup
+
+    // numeric refactorization (setup option "refactor"): factor patterns and the maps from them to
+    // the solve layout, kept on the device (RefactorArgs)
+    int opt_refactor = 0;
+    struct Refac {
+        bool on = false;
+        int64_t nF = 0, nfill = 0, ntc = 0, nlts = 0, nust = 0, nblk[2] = {0, 0};
+        double* F = nullptr;
+        double* S = nullptr;      // dense tails (FP64)
+        double* stage = nullptr;  // the new matrix values until they are committed
+        int* err = nullptr;
+        int64_t *fbase = nullptr, *fcp = nullptr, *frp = nullptr, *lv_off = nullptr;
+        int32_t *fri = nullptr, *fdg = nullptr, *frpos = nullptr, *frk = nullptr, *lv_first = nullptr,
+                *lv_col = nullptr, *tc_sub = nullptr, *tc_col = nullptr;
+        uint8_t* fllt = nullptr;
+        int64_t *fill_src = nullptr, *fill_dst = nullptr, *lts_src = nullptr, *ust_src = nullptr;
+        int32_t *sw_src[2] = {nullptr, nullptr}, *sw_dsrc[2] = {nullptr, nullptr};
+        int64_t *wsrc[2] = {nullptr, nullptr}, *be_off[2] = {nullptr, nullptr}, *be_pos[2] = {nullptr, nullptr},
+                *be_cp[2] = {nullptr, nullptr}, *bc_pos[2] = {nullptr, nullptr};
+        uint8_t *be_row[2] = {nullptr, nullptr}, *bc_b[2] = {nullptr, nullptr};
+        std::vector<int> sz;     // tail size per subdomain
+        std::vector<char> llt;   // per subdomain
+        std::vector<int64_t> d_off;
+        size_t bytes = 0;        // device bytes of the plan
+        cublasHandle_t blas = nullptr;
+        double last_ms = 0.0;
+    } rf;
 
     int fail(int code, const std::string& msg)
     {
@@ -351,23 +388,31 @@ std::vector<std::vector<int32_t>> chain_blocks(const HostCsr& M, int T, bool low
 // W^-1 b(B) (the sweep's prologue): the k-step chain becomes one level.  The replaced rows hold
 // the union of the block rows' patterns; a block stops before a row that would reach 65535 entries.
 void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, int gmax, int chain, Sweep& out,
-                 std::string& err)
+                 std::string& err, const std::vector<int32_t>* mpos = nullptr)
 {
+    const bool track = mpos != nullptr;
     // rows of the sparse part, original numbering: (column, value) outside the diagonal, and diagonal
     std::vector<std::vector<std::pair<int32_t, double>>> rows(T);
     std::vector<double> diag(T, 1.0);
+    std::vector<std::vector<int32_t>> rpos(track ? T : 0);  // factor position of each entry of rows[r]
+    std::vector<int32_t> dpos(track ? T : 0, -1);
     for (int r = 0; r < T; ++r) {
         double dg = 1.0;
         for (int64_t e = M.rp[r]; e < M.rp[r + 1]; ++e) {
             const int c = M.ci[e];
             if (c == r) {
                 dg = M.v[e];
+                if (track) dpos[r] = (*mpos)[e];
                 continue;
             }
             if (lower ? (c > r) : (c < r || c >= T)) continue;
             rows[r].emplace_back(c, M.v[e]);
+            if (track) rpos[r].push_back((*mpos)[e]);
         }
-        if (unit_diag) dg = 1.0;
+        if (unit_diag) {
+            dg = 1.0;
+            if (track) dpos[r] = -1;
+        }
         if (dg == 0.0 || !std::isfinite(dg)) {
             err = "zero or non-finite diagonal in a triangular factor";
             return;
@@ -381,6 +426,12 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
     std::vector<int32_t> mark(T, -1), touched;
     std::vector<std::vector<double>> winv_of;  // per block, packed lower W^-1
     std::vector<int> blk_ids;                  // blocks of >= 2 rows, in solve order
+    // tracking: per rewritten row its block (order in blk_ids) and row, and per entry its
+    // contributions; per kept block the positions of W
+    std::vector<std::pair<int32_t, int32_t>> rblk(track ? T : 0, {-1, -1});
+    std::vector<std::vector<std::vector<std::pair<uint8_t, int32_t>>>> rcons(track ? T : 0);
+    std::vector<std::vector<int32_t>> wsrc_of;
+    std::vector<int32_t> tix(track ? T : 0, -1);
     for (int bi = 0; bi < (int)blocks.size(); ++bi) {
         std::vector<int32_t>& B = blocks[bi];
         int k = (int)B.size();
@@ -388,11 +439,18 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
         for (int32_t r : B) inblk[r] = 1;
         // W (k x k, lower in solve order) and its inverse by forward substitution, column by column
         std::vector<double> W((size_t)k * k, 0.0);
+        std::vector<int32_t> Wp(track ? (size_t)k * k : 0, -1);
         for (int a2 = 0; a2 < k; ++a2) {
             W[(size_t)a2 * k + a2] = diag[B[a2]];
-            for (const auto& cv : rows[B[a2]])
+            if (track) Wp[(size_t)a2 * k + a2] = dpos[B[a2]];
+            for (size_t q = 0; q < rows[B[a2]].size(); ++q) {
+                const auto& cv = rows[B[a2]][q];
                 for (int b2 = 0; b2 < a2; ++b2)
-                    if (cv.first == B[b2]) W[(size_t)a2 * k + b2] = cv.second;
+                    if (cv.first == B[b2]) {
+                        W[(size_t)a2 * k + b2] = cv.second;
+                        if (track) Wp[(size_t)a2 * k + b2] = rpos[B[a2]][q];
+                    }
+            }
         }
         std::vector<double> Wi((size_t)k * k, 0.0);
         for (int j = 0; j < k; ++j)
@@ -403,19 +461,28 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
             }
         // new row a = sum_{b <= a} W^-1(a, b) M(B[b], outside the block)
         std::vector<std::vector<std::pair<int32_t, double>>> nrows(k);
+        std::vector<std::vector<std::vector<std::pair<uint8_t, int32_t>>>> ncons(track ? k : 0);
+        std::vector<std::vector<std::pair<uint8_t, int32_t>>> tcons;
         int kept = k;
         for (int a2 = 0; a2 < k; ++a2) {
             touched.clear();
+            tcons.clear();
             for (int b2 = 0; b2 <= a2; ++b2) {
                 const double w = Wi[(size_t)a2 * k + b2];
-                for (const auto& cv : rows[B[b2]]) {
+                for (size_t q = 0; q < rows[B[b2]].size(); ++q) {
+                    const auto& cv = rows[B[b2]][q];
                     if (inblk[cv.first]) continue;
                     if (mark[cv.first] != a2 + 1 + bi * 64) {
                         mark[cv.first] = a2 + 1 + bi * 64;
                         acc[cv.first] = 0.0;
+                        if (track) {
+                            tix[cv.first] = (int32_t)touched.size();
+                            tcons.emplace_back();
+                        }
                         touched.push_back(cv.first);
                     }
                     acc[cv.first] += w * cv.second;
+                    if (track) tcons[tix[cv.first]].emplace_back((uint8_t)b2, rpos[B[b2]][q]);
                 }
             }
             if (touched.size() >= 65535) {
@@ -424,6 +491,8 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
             }
             std::sort(touched.begin(), touched.end());
             for (int32_t c : touched) nrows[a2].emplace_back(c, acc[c]);
+            if (track)
+                for (int32_t c : touched) ncons[a2].push_back(std::move(tcons[tix[c]]));
         }
         if (kept < 2) {  // too long to block: leave the rows as they are
             for (int32_t r : B) inblk[r] = 0;
@@ -438,17 +507,32 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
             for (int i = 0; i < kept; ++i)
                 for (int j = 0; j < kept; ++j) Wk[(size_t)i * kept + j] = Wi[(size_t)i * k + j];
             Wi.swap(Wk);
+            if (track) {
+                std::vector<int32_t> Wpk((size_t)kept * kept);
+                for (int i = 0; i < kept; ++i)
+                    for (int j = 0; j < kept; ++j) Wpk[(size_t)i * kept + j] = Wp[(size_t)i * k + j];
+                Wp.swap(Wpk);
+            }
             k = kept;
         }
         for (int a2 = 0; a2 < k; ++a2) {
             rows[B[a2]].swap(nrows[a2]);
             diag[B[a2]] = 1.0;
             inblk[B[a2]] = 0;  // the marker covers the block being rewritten only
+            if (track) {
+                rblk[B[a2]] = {(int32_t)blk_ids.size(), a2};
+                rcons[B[a2]] = std::move(ncons[a2]);
+            }
         }
         std::vector<double> packed;
+        std::vector<int32_t> wpacked;
         for (int i = 0; i < k; ++i)
-            for (int j = 0; j <= i; ++j) packed.push_back(Wi[(size_t)i * k + j]);
+            for (int j = 0; j <= i; ++j) {
+                packed.push_back(Wi[(size_t)i * k + j]);
+                if (track) wpacked.push_back(Wp[(size_t)i * k + j]);
+            }
         winv_of.push_back(std::move(packed));
+        if (track) wsrc_of.push_back(std::move(wpacked));
         blk_ids.push_back(bi);
     }
     // dependency levels of the rewritten rows, in solve order
@@ -498,10 +582,17 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
     };
     struct WarpOut {
         std::vector<uint32_t> hdr;
-        std::vector<int32_t> slot, col;
+        std::vector<int32_t> slot, col, src;
         std::vector<double> val;
         double cost = 0.0;
     };
+    // tracking: entries of rewritten rows as (block, row in block, entry index within its warp,
+    // warp, row, entry of the row)
+    struct BlkEnt {
+        int32_t blk, arow, w, r, e;
+        int64_t idx;
+    };
+    std::vector<BlkEnt> bents;
     std::vector<WarpOut> wo(nw);
     out.pad = 0;
     out.ntask = 0;
@@ -533,19 +624,29 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
             for (int c = 0; c < C; ++c)
                 for (int lane = 0; lane < 32; ++lane) {
                     const int k = lane / G, j = lane % G, e = c * G + j;
-                    int32_t colv = -1;
+                    int32_t colv = -1, sv = -1;
                     double v = 0.0;
                     if (k < R) {
                         const int p = items[i0 + k].second;
-                        const auto& row = rows[out.order[p]];
+                        const int r = out.order[p];
+                        const auto& row = rows[r];
                         if (e < (int)row.size()) {
                             colv = out.pos[row[e].first];
                             v = row[e].second * out.dinv[p];
+                            if (track) {
+                                if (rblk[r].first >= 0) {
+                                    sv = -2;
+                                    bents.push_back({rblk[r].first, rblk[r].second, wbest, r, e, (int64_t)W.col.size()});
+                                } else {
+                                    sv = rpos[r][e];
+                                }
+                            }
                         }
                     }
                     if (colv < 0) ++out.pad;
                     W.col.push_back(colv);
                     W.val.push_back(v);
+                    if (track) W.src.push_back(sv);
                 }
             ++out.ntask;
             i0 = i1;
@@ -566,6 +667,7 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
         out.tslot.insert(out.tslot.end(), wo[w].slot.begin(), wo[w].slot.end());
         out.col.insert(out.col.end(), wo[w].col.begin(), wo[w].col.end());
         out.val.insert(out.val.end(), wo[w].val.begin(), wo[w].val.end());
+        if (track) out.src.insert(out.src.end(), wo[w].src.begin(), wo[w].src.end());
     }
     out.wtask[nw] = (int64_t)out.thdr.size();
     out.wslot[nw] = (int64_t)out.tslot.size();
@@ -579,6 +681,31 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
         out.blk_off.push_back((int64_t)out.blk_slot.size());
         out.blk_inv.insert(out.blk_inv.end(), winv_of[q].begin(), winv_of[q].end());
         out.blk_ioff.push_back((int64_t)out.blk_inv.size());
+    }
+    if (!track) return;
+    out.dsrc.assign(T, -1);
+    for (int p = 0; p < T; ++p) {
+        const int r = out.order[p];
+        out.dsrc[p] = rblk[r].first >= 0 ? -1 : dpos[r];
+    }
+    for (const auto& w : wsrc_of) out.blk_wsrc.insert(out.blk_wsrc.end(), w.begin(), w.end());
+    std::sort(bents.begin(), bents.end(), [&](const BlkEnt& a, const BlkEnt& b) {
+        if (a.blk != b.blk) return a.blk < b.blk;
+        return out.went[a.w] + a.idx < out.went[b.w] + b.idx;
+    });
+    size_t q = 0;
+    for (size_t b = 0; b < blk_ids.size(); ++b) {
+        for (; q < bents.size() && bents[q].blk == (int32_t)b; ++q) {
+            const BlkEnt& be = bents[q];
+            out.be_pos.push_back(out.went[be.w] + be.idx);
+            out.be_row.push_back((uint8_t)be.arow);
+            for (const auto& cb : rcons[be.r][be.e]) {
+                out.bc_b.push_back(cb.first);
+                out.bc_pos.push_back(cb.second);
+            }
+            out.be_cp.push_back((int64_t)out.bc_b.size());
+        }
+        out.be_off.push_back((int64_t)out.be_pos.size());
     }
 }
 
@@ -660,6 +787,52 @@ int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model&
         }
     }
     return bestT;
+}
+
+// Combined column pattern of one subdomain's factors (RefactorArgs): L L^T the columns of L, LU and
+// LDL^T the strict upper rows (from U), the diagonal (U's), then the strict lower rows (from L).
+// Rows increase within a column.
+struct FPat {
+    std::vector<int64_t> cp;
+    std::vector<int32_t> ri;
+    std::vector<int32_t> dg;
+    int32_t find(int r, int c) const
+    {
+        const auto b = ri.begin() + cp[c], e = ri.begin() + cp[c + 1];
+        const auto it = std::lower_bound(b, e, r);
+        return (it != e && *it == r) ? (int32_t)(it - ri.begin()) : -1;
+    }
+};
+
+bool make_fpattern(const HostCsr& L, const HostCsr& U, int n, bool llt, FPat& P)
+{
+    P.cp.assign(n + 1, 0);
+    auto visit = [&](const std::function<void(int, int)>& f) {
+        for (int r = 0; r < n; ++r) {
+            for (int64_t e = L.rp[r]; e < L.rp[r + 1]; ++e) {
+                const int c = L.ci[e];
+                if (llt ? c <= r : c < r) f(r, c);
+            }
+            if (!llt)
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
+                    const int c = U.ci[e];
+                    if (c >= r) f(r, c);
+                }
+        }
+    };
+    visit([&](int, int c) { ++P.cp[c + 1]; });
+    for (int c = 0; c < n; ++c) P.cp[c + 1] += P.cp[c];
+    P.ri.resize(P.cp[n]);
+    std::vector<int64_t> nx(P.cp.begin(), P.cp.end() - 1);
+    visit([&](int r, int c) { P.ri[nx[c]++] = r; });  // rows visited in increasing order
+    P.dg.assign(n, 0);
+    for (int c = 0; c < n; ++c) {
+        int64_t q = P.cp[c];
+        while (q < P.cp[c + 1] && P.ri[q] < c) ++q;
+        if (q == P.cp[c + 1] || P.ri[q] != c) return false;
+        P.dg[c] = (int32_t)(q - P.cp[c]);
+    }
+    return true;
 }
 
 // transpose of a lower CSR (values scaled by rowscale[c] of the result rows if given)
@@ -1809,6 +1982,18 @@ int s2l_gpu_setup_end(s2l_setup* s)
     double bytes = 0.0;
     int max_T = 0, max_nl = 0;
     int64_t sparse_nnz = 0;
+    // refactorization plan (host side; see RefactorArgs)
+    const bool rfon = s->opt_refactor != 0;
+    std::vector<int64_t> rf_fbase(1, 0), rf_fcp, rf_frp(1, 0), rf_lvoff(1, 0), rf_fill_src, rf_fill_dst, rf_lts, rf_ust;
+    std::vector<int32_t> rf_fri, rf_fdg, rf_frpos, rf_frk, rf_lvfirst, rf_lvcol, rf_tcsub, rf_tccol;
+    std::vector<uint8_t> rf_fllt;
+    std::vector<int32_t> rf_swsrc[2], rf_swdsrc[2];
+    std::vector<int64_t> rf_wsrc[2], rf_beoff[2] = {{0}, {0}}, rf_bepos[2], rf_becp[2] = {{0}, {0}}, rf_bcpos[2];
+    std::vector<uint8_t> rf_berow[2], rf_bcb[2];
+    if (rfon) {
+        s->rf.sz.assign(nsub, 0);
+        s->rf.llt.assign(nsub, 0);
+    }
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
         const HostCsr& U = Us[i];
@@ -1820,9 +2005,113 @@ int s2l_gpu_setup_end(s2l_setup* s)
         max_T = std::max(max_T, T);
         std::string err;
         Sweep sl, su;
-        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, sl, err);
-        if (err.empty()) build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, su, err);
+        FPat P;
+        std::vector<int32_t> mposL, mposU;
+        const bool llt = h.kind == S2L_FACTOR_LLT;
+        const int64_t fb = rf_fbase.back();
+        if (rfon) {
+            if (!make_fpattern(h.L, U, nl, llt, P))
+                return s->fail(S2L_ERR_BADARG, "subdomain " + std::to_string(i) + ": a factor has no diagonal entry");
+            mposL.assign(h.L.ci.size(), -1);
+            for (int r = 0; r < nl; ++r)
+                for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) {
+                    const int c = h.L.ci[e];
+                    if (llt ? c <= r : c < r) mposL[e] = P.find(r, c);
+                }
+            mposU.assign(U.ci.size(), -1);
+            bool found = true;
+            for (int r = 0; r < nl; ++r) {
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
+                    const int c = U.ci[e];
+                    mposU[e] = llt ? P.find(c, r) : P.find(r, c);
+                    found = found && mposU[e] >= 0;
+                }
+                for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e)
+                    if (llt ? h.L.ci[e] <= r : h.L.ci[e] < r) found = found && mposL[e] >= 0;
+            }
+            if (!found)  // every factor entry must have its place in the combined pattern
+                return s->fail(S2L_ERR_BADARG, "subdomain " + std::to_string(i) + ": inconsistent factor patterns");
+            s->rf.sz[i] = sz;
+            s->rf.llt[i] = llt;
+        }
+        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, sl, err, rfon ? &mposL : nullptr);
+        if (err.empty())
+            build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, su, err, rfon ? &mposU : nullptr);
         if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
+        if (rfon) {
+            // pattern, per-column data, L L^T row lists
+            for (int c = 0; c < nl; ++c) {
+                rf_fcp.push_back(fb + P.cp[c]);
+                rf_fllt.push_back(llt);
+                if (llt)
+                    for (int64_t e = h.L.rp[c]; e < h.L.rp[c + 1]; ++e) {
+                        const int k = h.L.ci[e];
+                        if (k >= c) break;
+                        rf_frpos.push_back(P.find(c, k));
+                        rf_frk.push_back(k);
+                    }
+                rf_frp.push_back((int64_t)rf_frpos.size());
+            }
+            rf_fri.insert(rf_fri.end(), P.ri.begin(), P.ri.end());
+            rf_fdg.insert(rf_fdg.end(), P.dg.begin(), P.dg.end());
+            // fill map: A(l2g(a), l2g(b)) -> F(ipin(a), pout(b)) (lower triangle only for L L^T)
+            std::vector<int32_t> ipin(nl);
+            for (int p = 0; p < nl; ++p) ipin[h.pin[p]] = p;
+            for (int a = 0; a < nl; ++a) {
+                const int64_t g = a < h.n_owned ? h.begin + a : h.ghosts[a - h.n_owned];
+                const int p = ipin[a];
+                for (int64_t e = s->A.rp[g]; e < s->A.rp[g + 1]; ++e) {
+                    const int64_t cg = s->A.ci[e];
+                    int b = -1;
+                    if (cg >= h.begin && cg < h.begin + h.n_owned) {
+                        b = (int)(cg - h.begin);
+                    } else {
+                        const auto it = std::lower_bound(h.ghosts.begin(), h.ghosts.end(), cg);
+                        if (it != h.ghosts.end() && *it == cg) b = h.n_owned + (int)(it - h.ghosts.begin());
+                    }
+                    if (b < 0) continue;
+                    const int q = h.pout[b];
+                    if (llt && p < q) continue;
+                    const int32_t pos = P.find(p, q);
+                    if (pos < 0)
+                        return s->fail(S2L_ERR_BADARG, "subdomain " + std::to_string(i) +
+                                                           ": a matrix entry lies outside the factor pattern (refactor)");
+                    rf_fill_src.push_back(e);
+                    rf_fill_dst.push_back(fb + pos);
+                }
+            }
+            // dependency levels of the sparse columns
+            std::vector<int32_t> lev(T, 0);
+            int nlev = 0;
+            for (int j = 0; j < T; ++j) {
+                int lv = 0;
+                if (llt) {
+                    for (int64_t e = h.L.rp[j]; e < h.L.rp[j + 1]; ++e)
+                        if (h.L.ci[e] < j) lv = std::max(lv, lev[h.L.ci[e]] + 1);
+                } else {
+                    for (int64_t q = P.cp[j]; q < P.cp[j] + P.dg[j]; ++q) lv = std::max(lv, lev[P.ri[q]] + 1);
+                }
+                lev[j] = lv;
+                nlev = std::max(nlev, lv + 1);
+            }
+            rf_lvfirst.push_back((int32_t)(rf_lvoff.size() - 1));
+            {
+                std::vector<int64_t> cnt(nlev + 1, 0);
+                for (int j = 0; j < T; ++j) ++cnt[lev[j] + 1];
+                for (int l = 0; l < nlev; ++l) cnt[l + 1] += cnt[l];
+                std::vector<int32_t> cols(T);
+                std::vector<int64_t> nx(cnt.begin(), cnt.end() - 1);
+                for (int j = 0; j < T; ++j) cols[nx[lev[j]]++] = j;
+                const int64_t base = (int64_t)rf_lvcol.size();
+                rf_lvcol.insert(rf_lvcol.end(), cols.begin(), cols.end());
+                for (int l = 0; l < nlev; ++l) rf_lvoff.push_back(base + cnt[l + 1]);
+            }
+            for (int j = T; j < nl; ++j) {
+                rf_tcsub.push_back(i);
+                rf_tccol.push_back(j);
+            }
+            rf_fbase.push_back(fb + (int64_t)P.ri.size());
+        }
         s->st_levels_max = std::max<int64_t>(s->st_levels_max, std::max(sl.nlev, su.nlev));
         s->st_levels_sum += sl.nlev + su.nlev;
         for (int f = 0; f < 2; ++f) {
@@ -1839,6 +2128,19 @@ int s2l_gpu_setup_end(s2l_setup* s)
             sw_tslot[f].insert(sw_tslot[f].end(), q.tslot.begin(), q.tslot.end());
             sw_dinv[f].insert(sw_dinv[f].end(), q.dinv.begin(), q.dinv.end());
             sw_dinv[f].resize(sw_dinv[f].size() + sz, 1.0);
+            if (rfon) {
+                rf_swsrc[f].insert(rf_swsrc[f].end(), q.src.begin(), q.src.end());
+                rf_swdsrc[f].insert(rf_swdsrc[f].end(), q.dsrc.begin(), q.dsrc.end());
+                rf_swdsrc[f].resize(rf_swdsrc[f].size() + sz, -1);
+                for (int32_t w : q.blk_wsrc) rf_wsrc[f].push_back(w >= 0 ? fb + w : -1);
+                const int64_t eb = (int64_t)rf_bepos[f].size(), cb = (int64_t)rf_bcb[f].size();
+                for (size_t b = 1; b < q.be_off.size(); ++b) rf_beoff[f].push_back(eb + q.be_off[b]);
+                for (int64_t x : q.be_pos) rf_bepos[f].push_back(e0 + x);
+                rf_berow[f].insert(rf_berow[f].end(), q.be_row.begin(), q.be_row.end());
+                for (size_t x = 1; x < q.be_cp.size(); ++x) rf_becp[f].push_back(cb + q.be_cp[x]);
+                rf_bcb[f].insert(rf_bcb[f].end(), q.bc_b.begin(), q.bc_b.end());
+                for (int32_t x : q.bc_pos) rf_bcpos[f].push_back(fb + x);
+            }
             const int64_t real = (int64_t)q.col.size() - q.pad;
             sparse_nnz += real;
             s->st_pad += q.pad;
@@ -1871,6 +2173,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     if (c < T) {
                         lts_col.push_back(sl.pos[c]);
                         lts_val.push_back(h.L.v[e]);
+                        if (rfon) rf_lts.push_back(fb + P.find(k, c));
                     } else if (c < k) {
                         Ltt[i][(size_t)(k - T) * sz + (c - T)] = h.L.v[e];
                     } else if (c == k) {
@@ -1899,6 +2202,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     if (U.ci[e] >= T) {
                         ust_col.push_back(U.ci[e]);
                         ust_val.push_back(U.v[e]);
+                        if (rfon) rf_ust.push_back(fb + (llt ? P.find(U.ci[e], r) : P.find(r, U.ci[e])));
                         any = true;
                     }
                 if (any) {
@@ -1999,6 +2303,54 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(dev_alloc(s, &s->d_linv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(dev_alloc(s, &s->d_uinv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(invert_tails(s, Ltt, Utt, d_off));
+    if (rfon) {
+        auto& R = s->rf;
+        const size_t before = s->bytes;
+        rf_fcp.push_back(rf_fbase.back());
+        rf_lvfirst.push_back((int32_t)(rf_lvoff.size() - 1));
+        R.nF = rf_fbase.back();
+        R.nfill = (int64_t)rf_fill_src.size();
+        R.ntc = (int64_t)rf_tcsub.size();
+        R.nlts = (int64_t)rf_lts.size();
+        R.nust = (int64_t)rf_ust.size();
+        R.d_off = d_off;
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.F), (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.S), (size_t)std::max<int64_t>(d_off[nsub], 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.stage), (size_t)std::max<int64_t>(s->nnz, 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.err), sizeof(int)));
+        RET_IF(upload(s, &R.fbase, rf_fbase));
+        RET_IF(upload(s, &R.fcp, rf_fcp));
+        RET_IF(upload(s, &R.fri, rf_fri));
+        RET_IF(upload(s, &R.fdg, rf_fdg));
+        RET_IF(upload(s, &R.fllt, rf_fllt));
+        RET_IF(upload(s, &R.frp, rf_frp));
+        RET_IF(upload(s, &R.frpos, rf_frpos));
+        RET_IF(upload(s, &R.frk, rf_frk));
+        RET_IF(upload(s, &R.lv_first, rf_lvfirst));
+        RET_IF(upload(s, &R.lv_off, rf_lvoff));
+        RET_IF(upload(s, &R.lv_col, rf_lvcol));
+        RET_IF(upload(s, &R.tc_sub, rf_tcsub));
+        RET_IF(upload(s, &R.tc_col, rf_tccol));
+        RET_IF(upload(s, &R.fill_src, rf_fill_src));
+        RET_IF(upload(s, &R.fill_dst, rf_fill_dst));
+        RET_IF(upload(s, &R.lts_src, rf_lts));
+        RET_IF(upload(s, &R.ust_src, rf_ust));
+        for (int f = 0; f < 2; ++f) {
+            R.nblk[f] = (int64_t)rf_beoff[f].size() - 1;
+            RET_IF(upload(s, &R.sw_src[f], rf_swsrc[f]));
+            RET_IF(upload(s, &R.sw_dsrc[f], rf_swdsrc[f]));
+            RET_IF(upload(s, &R.wsrc[f], rf_wsrc[f]));
+            RET_IF(upload(s, &R.be_off[f], rf_beoff[f]));
+            RET_IF(upload(s, &R.be_pos[f], rf_bepos[f]));
+            RET_IF(upload(s, &R.be_row[f], rf_berow[f]));
+            RET_IF(upload(s, &R.be_cp[f], rf_becp[f]));
+            RET_IF(upload(s, &R.bc_b[f], rf_bcb[f]));
+            RET_IF(upload(s, &R.bc_pos[f], rf_bcpos[f]));
+        }
+        CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
+        R.bytes = s->bytes - before;
+        R.on = true;
+    }
     // input gather and owned output of one local solve (per right-hand side)
     double vec = 0.0;
     for (int i = 0; i < nsub; ++i) {
@@ -2137,6 +2489,7 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
         s->ctx->used -= std::min(s->ctx->used, s->bytes);
     }
     if (s->setup_stream) cudaStreamDestroy(s->setup_stream);
+    if (s->rf.blas) cublasDestroy(s->rf.blas);
     delete s;
     return S2L_OK;
 }
@@ -2171,6 +2524,226 @@ int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind)
     CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, rowsum.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->setup_stream));
     CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
     return S2L_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Temporary device buffers of one call, charged to the context's HBM budget while they live.
+struct TempBufs {
+    s2l_setup* s;
+    std::vector<std::pair<void*, size_t>> held;
+    explicit TempBufs(s2l_setup* s_) : s(s_) {}
+    template <typename T>
+    int get(T** p, size_t count)
+    {
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        {
+            std::lock_guard<std::mutex> g(s->ctx->mu);
+            if (s->ctx->budget && s->ctx->used + bytes > s->ctx->budget) {
+                s->ctx->err = "HBM budget exceeded by the refactorization's work buffers";
+                return S2L_ERR_OOM;
+            }
+            s->ctx->used += bytes;
+        }
+        if (cudaMalloc(reinterpret_cast<void**>(p), bytes) != cudaSuccess) {
+            std::lock_guard<std::mutex> g(s->ctx->mu);
+            s->ctx->used -= bytes;
+            return s->fail(S2L_ERR_OOM, "no device memory for the refactorization's work buffers");
+        }
+        held.emplace_back(*p, bytes);
+        return S2L_OK;
+    }
+    ~TempBufs()
+    {
+        for (auto& h : held) {
+            cudaFree(h.first);
+            std::lock_guard<std::mutex> g(s->ctx->mu);
+            s->ctx->used -= std::min(s->ctx->used, h.second);
+        }
+    }
+};
+
+// E = W^T A W for the matrix values v (device), 16 columns of W at a time: prolongation of unit
+// coarse vectors, product with A, restriction (the kernels of the coarse correction)
+int coarse_matrix_dev(s2l_setup* s, TempBufs& tb, cudaStream_t st, const double* v, double* E)
+{
+    const int64_t n = s->n, n0 = s->n0;
+    const int K = 16;
+    const int boolean = s->pou == S2L_POU_BOOLEAN;
+    double *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr, *C = nullptr, *plocal = nullptr;
+    RET_IF(tb.get(&Y, (size_t)n0 * K));
+    RET_IF(tb.get(&X, (size_t)n * K));
+    RET_IF(tb.get(&AX, (size_t)n * K));
+    RET_IF(tb.get(&cpart, (size_t)s->ntiles * s->mmax * K));
+    RET_IF(tb.get(&C, (size_t)n0 * K));
+    if (!boolean) RET_IF(tb.get(&plocal, (size_t)s->nloc * K));
+    for (int64_t c0 = 0; c0 < n0; c0 += K) {
+        launch_unit_block(st, n0, (int)c0, Y);
+        launch_coarse_prolong_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, Y,
+                                    X, plocal);
+        if (!boolean) launch_combine_block(st, n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, X);
+        launch_spmv_block(st, n, K, s->d_rp, s->d_ci, v, X, AX, nullptr, nullptr, nullptr, s->tpr);
+        launch_coarse_restrict_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+                                     boolean, AX, s->mmax, cpart);
+        launch_coarse_reduce_block(st, K, s->nsub, s->d_subs, s->d_t_first, s->mmax, cpart, C);
+        launch_scatter_columns(st, n0, (int)c0, C, E);
+    }
+    CUDA_OK(s, cudaGetLastError());
+    return S2L_OK;
+}
+
+template <typename Real>
+int refactor_commit_factors(s2l_setup* s, TempBufs& tb, cudaStream_t st)
+{
+    auto& R = s->rf;
+    const int nsub = s->nsub;
+    for (int f = 0; f < 2; ++f) {
+        launch_refactor_dinv<Real>(st, nsub, s->d_subs, R.fbase, R.F, R.sw_dsrc[f], (Real*)s->d_dinv[f]);
+        launch_refactor_sweep_values<Real>(st, nsub, R.fbase, R.F, s->d_wtask[f], s->d_wslot[f], s->d_went[f],
+                                           s->d_thdr[f], s->d_tslot[f], R.sw_src[f], s->d_subs, R.sw_dsrc[f],
+                                           (Real*)s->d_val[f]);
+        launch_refactor_blocks<Real>(st, R.nblk[f], s->d_boff[f], s->d_bioff[f], R.wsrc[f], R.be_off[f], R.be_pos[f],
+                                     R.be_row[f], R.be_cp[f], R.bc_b[f], R.bc_pos[f], R.F, (Real*)s->d_binv[f],
+                                     (Real*)s->d_val[f]);
+    }
+    launch_gather_values<Real>(st, R.nlts, R.lts_src, R.F, (Real*)s->d_lts_val);
+    launch_gather_values<Real>(st, R.nust, R.ust_src, R.F, (Real*)s->d_ust_val);
+    // dense tails: triangles of the factored Schur complements, inverted by triangular solves
+    int smax = 0;
+    for (int i = 0; i < nsub; ++i) smax = std::max(smax, R.sz[i]);
+    if (smax == 0) return S2L_OK;
+    double *Lt = nullptr, *Ut = nullptr, *B = nullptr;
+    RET_IF(tb.get(&Lt, (size_t)smax * smax));
+    RET_IF(tb.get(&Ut, (size_t)smax * smax));
+    RET_IF(tb.get(&B, (size_t)smax * smax));
+    if (!R.blas) {
+        if (cublasCreate(&R.blas) != CUBLAS_STATUS_SUCCESS) {
+            R.blas = nullptr;
+            return s->fail(S2L_ERR_CUDA, "cublasCreate failed");
+        }
+    }
+    if (cublasSetStream(R.blas, st) != CUBLAS_STATUS_SUCCESS) return s->fail(S2L_ERR_CUDA, "cublasSetStream failed");
+    const double one = 1.0;
+    for (int i = 0; i < nsub; ++i) {
+        const int sz = R.sz[i];
+        if (sz == 0) continue;
+        launch_tail_triangles(st, R.S + R.d_off[i], sz, R.llt[i], Lt, Ut);
+        for (int f = 0; f < 2; ++f) {
+            launch_identity(st, B, sz);
+            // row-major lower Lt = column-major upper Lt^T (and row-major upper = column-major lower)
+            if (cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER,
+                            CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, sz, sz, &one, f == 0 ? Lt : Ut, sz, B, sz) !=
+                CUBLAS_STATUS_SUCCESS)
+                return s->fail(S2L_ERR_CUDA, "cublasDtrsm failed");
+            void* dst = f == 0 ? s->d_linv : s->d_uinv;
+            if (s->real == S2L_REAL_F32) launch_to_float(st, B, (float*)dst + R.d_off[i], (int64_t)sz * sz);
+            else CUDA_OK(s, cudaMemcpyAsync((double*)dst + R.d_off[i], B, (size_t)sz * sz * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    return S2L_OK;
+}
+
+int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
+{
+    auto& R = s->rf;
+    cudaStream_t st = s->setup_stream;
+    const int nsub = s->nsub;
+    const int64_t n = s->n, nnz = s->nnz, n0 = s->n0;
+    const auto t0 = std::chrono::steady_clock::now();
+    TempBufs tb(s);
+    CUDA_OK(s, cudaMemcpyAsync(R.stage, val, (size_t)nnz * sizeof(double),
+                               ptr_kind == S2L_PTR_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(s, cudaMemsetAsync(R.err, 0, sizeof(int), st));
+    // row sums of the new matrix: the OpenFOAM normalisation, and a finiteness check of every value
+    double* rowsum = nullptr;
+    RET_IF(tb.get(&rowsum, (size_t)n));
+    launch_row_sums(st, n, s->d_rp, R.stage, rowsum);
+    {
+        std::vector<double> h((size_t)n);
+        CUDA_OK(s, cudaMemcpyAsync(h.data(), rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(s, cudaStreamSynchronize(st));
+        for (double v : h)
+            if (!std::isfinite(v)) return s->fail(S2L_ERR_NUMERIC, "non-finite matrix value");
+    }
+    // coarse matrix with the kept basis, and its inverse
+    double *Enew = nullptr, *colbuf = nullptr;
+    int* piv = nullptr;
+    const bool coarse = s->coarse != S2L_COARSE_NONE && n0 > 0;
+    if (coarse) {
+        RET_IF(tb.get(&Enew, (size_t)n0 * n0));
+        RET_IF(tb.get(&colbuf, (size_t)n0));
+        RET_IF(tb.get(&piv, (size_t)n0));
+        RET_IF(coarse_matrix_dev(s, tb, st, R.stage, Enew));
+        launch_gauss_jordan(st, (int)n0, Enew, colbuf, piv, R.err);
+    }
+    // local factors on their kept patterns
+    RefactorArgs a{};
+    a.subs = s->d_subs;
+    a.F = R.F;
+    a.fbase = R.fbase;
+    a.fcp = R.fcp;
+    a.fri = R.fri;
+    a.fdg = R.fdg;
+    a.fllt = R.fllt;
+    a.frp = R.frp;
+    a.frpos = R.frpos;
+    a.frk = R.frk;
+    a.lv_first = R.lv_first;
+    a.lv_off = R.lv_off;
+    a.lv_col = R.lv_col;
+    a.tc_sub = R.tc_sub;
+    a.tc_col = R.tc_col;
+    a.ntc = R.ntc;
+    a.S = R.S;
+    a.err = R.err;
+    CUDA_OK(s, cudaMemsetAsync(R.F, 0, (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double), st));
+    launch_refactor_fill(st, R.nfill, R.fill_src, R.fill_dst, R.stage, R.F);
+    launch_refactor_sparse(st, a, nsub);
+    launch_refactor_tail_columns(st, a);
+    CUDA_OK(s, cudaMemsetAsync(R.S, 0, (size_t)std::max<int64_t>(R.d_off[nsub], 1) * sizeof(double), st));
+    launch_refactor_gather_tails(st, a);
+    launch_dense_lu(st, a, nsub);
+    CUDA_OK(s, cudaGetLastError());
+    int herr = 0;
+    CUDA_OK(s, cudaMemcpyAsync(&herr, R.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(s, cudaStreamSynchronize(st));
+    if (herr == 1) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a sparse column");
+    if (herr == 2) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a dense tail");
+    if (herr == 3) return s->fail(S2L_ERR_NUMERIC, "refactorization: the coarse matrix is singular");
+    if (herr) return s->fail(S2L_ERR_NUMERIC, "refactorization failed");
+    // commit: the matrix, its row sums, E^-1, then the solve layout of the new factors
+    CUDA_OK(s, cudaMemcpyAsync(s->d_av, R.stage, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (coarse)
+        CUDA_OK(s, cudaMemcpyAsync(s->d_Einv, Enew, (size_t)n0 * n0 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (s->real == S2L_REAL_F32) RET_IF(refactor_commit_factors<float>(s, tb, st));
+    else RET_IF(refactor_commit_factors<double>(s, tb, st));
+    CUDA_OK(s, cudaGetLastError());
+    CUDA_OK(s, cudaStreamSynchronize(st));
+    R.last_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return S2L_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int s2l_gpu_refactor(s2l_setup* s, const double* val, int ptr_kind)
+{
+    RET_IF(check_ready(s));
+    if (!val) return s->fail(S2L_ERR_BADARG, "null values");
+    if (ptr_kind != S2L_PTR_HOST && ptr_kind != S2L_PTR_DEVICE)
+        return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    if (!s->rf.on) return s->fail(S2L_ERR_STATE, "the setup was built without the option refactor = 1");
+    std::lock_guard<std::mutex> g(s->wmu);  // no call can take a workspace meanwhile
+    for (char b : s->busy)
+        if (b) return s->fail(S2L_ERR_STATE, "refactor while a solve-phase call runs on the setup");
+    if (s->pending.load() > 0) return s->fail(S2L_ERR_STATE, "refactor while solves are queued on the setup");
+    if (cudaSetDevice(s->ctx->device) != cudaSuccess) return s->fail(S2L_ERR_CUDA, "cudaSetDevice failed");
+    return refactor_run(s, val, ptr_kind);
 }
 
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
@@ -2211,6 +2784,8 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         const int c = (int)value;
         if (c < 1 || c > S2L_CHAIN_MAX) return s->fail(S2L_ERR_BADARG, "chain_block must be in [1, 16]");
         s->opt_chain = c;
+    } else if (n == "refactor") {
+        s->opt_refactor = value != 0.0;
     } else return s->fail(S2L_ERR_BADARG, "unknown setup option " + n);
     return S2L_OK;
 }
@@ -2234,6 +2809,8 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "block_width") *value = (double)block_width_best(const_cast<s2l_setup*>(s));
     else if (n == "sweep_padding") *value = (double)s->st_pad;
     else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;
+    else if (n == "refactor_bytes") *value = (double)s->rf.bytes;
+    else if (n == "refactor_ms") *value = s->rf.last_ms;
     else return S2L_ERR_BADARG;
     return S2L_OK;
 }

@@ -1,0 +1,645 @@
+// Numeric refactorization of the local factors on their kept patterns, and the refresh of the
+// coarse matrix, on the device (s2l_gpu_refactor).
+//
+// The reference's UpdateLevel::Refactorize (include/preconditioner/preconditioner.hpp:15-30,
+// src/preconditioner/two_level_schwarz.cpp:30-41): refill A_ii with the new values
+// (Subdomain::refillValues, src/partition/subdomain.cpp:107-127), numeric factorization with the
+// symbolic analysis kept (LocalSolver::refactorize, src/linalg/local_solver.cpp:111-118), and
+// A_00 = W^T A W with the old coarse basis (CoarseSpace::refresh,
+// src/preconditioner/coarse_space.cpp:95-105, 186-206).
+//
+// Work split of one subdomain with solve split T (rows [0, T) sparse, [T, n) dense tail):
+//  1. fill: F = 0, then the entries of P_in A_ii Q at their positions in the factor pattern;
+//  2. sparse columns j < T, left-looking, one CTA per subdomain walking the columns' dependency
+//     levels (a column needs the columns k of its U part, or of its row of L for L L^T), one
+//     warp per column, its k in increasing order, the lanes over the rows of column k;
+//  3. tail columns j >= T: the same updates from the sparse columns only (k < T), one warp per
+//     column, all columns independent; the tail block of F then holds the Schur complement S;
+//  4. S gathered dense and factorized (LU without pivoting, one CTA per subdomain); the caller
+//     inverts its triangles for the solve's dense tails.
+// Every column is reduced by one warp in a fixed order, so the result does not depend on timing.
+#include "s2l_internal.cuh"
+
+#include <cmath>
+
+namespace {
+
+// position of row i in the column [c0, c1) of F (rows increasing); the pattern is closed under
+// elimination, so the row is there
+__device__ __forceinline__ int64_t find_row(const int32_t* __restrict__ fri, int64_t c0, int64_t c1, int i)
+{
+    int64_t lo = c0, hi = c1 - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(fri + mid) < i) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void set_err(int* err, int code)
+{
+    atomicCAS(err, 0, code);
+}
+
+// Updates of local column j (global column gj = loc + j) by the finished columns k < klimit.
+// LU: U(k, j) = x(k) in increasing k, x(rows > k of L(:, k)) -= L(:, k) U(k, j).
+// L L^T: x(rows >= j of L(:, k)) -= L(:, k) L(j, k) over the entries L(j, k) of row j.
+__device__ void update_column(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int klimit, int lane)
+{
+    double* __restrict__ F = a.F;
+    const int64_t c0 = a.fcp[gj], c1 = a.fcp[gj + 1];
+    if (a.fllt[gj]) {
+        const int64_t r1 = a.frp[gj + 1];
+        for (int64_t t = a.frp[gj]; t < r1; ++t) {
+            const int k = a.frk[t];
+            if (k >= klimit) break;
+            const int64_t p = fb + a.frpos[t];
+            const double ljk = F[p];
+            const int64_t e1 = a.fcp[loc + k + 1];
+            for (int64_t s = p + lane; s < e1; s += 32) {
+                const int i = a.fri[s];
+                const int64_t q = find_row(a.fri, c0, c1, i);
+                F[q] -= F[s] * ljk;
+            }
+            __syncwarp();
+        }
+    } else {
+        const int64_t u1 = c0 + a.fdg[gj];
+        for (int64_t t = c0; t < u1; ++t) {
+            const int k = a.fri[t];
+            if (k >= klimit) break;
+            const double u = F[t];  // final: every update from a smaller k is done
+            const int64_t gk = loc + k;
+            const int64_t e1 = a.fcp[gk + 1];
+            if (u != 0.0)
+                for (int64_t s = a.fcp[gk] + a.fdg[gk] + 1 + lane; s < e1; s += 32) {
+                    const int i = a.fri[s];
+                    const int64_t q = find_row(a.fri, c0, c1, i);
+                    F[q] -= F[s] * u;
+                }
+            __syncwarp();
+        }
+    }
+}
+
+// pivot of column gj: LU divides the strict lower part by U(j, j); L L^T takes the square root of
+// the diagonal and divides the rows below by it
+__device__ void finish_column(const RefactorArgs& a, int64_t gj, int lane)
+{
+    double* __restrict__ F = a.F;
+    const int64_t c0 = a.fcp[gj], c1 = a.fcp[gj + 1];
+    const int64_t pd = c0 + a.fdg[gj];
+    const double d = F[pd];
+    __syncwarp();
+    if (a.fllt[gj]) {
+        if (!(d > 0.0) || !isfinite(d)) {
+            if (lane == 0) set_err(a.err, 1);
+            return;
+        }
+        const double r = sqrt(d);
+        const double ri = 1.0 / r;
+        if (lane == 0) F[pd] = r;
+        for (int64_t s = pd + 1 + lane; s < c1; s += 32) F[s] *= ri;
+    } else {
+        if (d == 0.0 || !isfinite(d)) {
+            if (lane == 0) set_err(a.err, 1);
+            return;
+        }
+        const double di = 1.0 / d;
+        for (int64_t s = pd + 1 + lane; s < c1; s += 32) F[s] *= di;
+    }
+    __syncwarp();
+}
+
+__global__ void fill_kernel(int64_t count, const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
+                            const double* __restrict__ val, double* __restrict__ F)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x)
+        F[dst[e]] = val[src[e]];
+}
+
+// one CTA per subdomain: the sparse columns level by level
+__global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorArgs a)
+{
+    const int sid = blockIdx.x;
+    const int64_t loc = a.subs[sid].loc_off, fb = a.fbase[sid];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __shared__ int stop;
+    for (int lv = a.lv_first[sid]; lv < a.lv_first[sid + 1]; ++lv) {
+        const int64_t e1 = a.lv_off[lv + 1];
+        for (int64_t c = a.lv_off[lv] + wid; c < e1; c += nw) {
+            const int j = a.lv_col[c];
+            update_column(a, loc, fb, loc + j, j, lane);
+            finish_column(a, loc + j, lane);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) stop = *(volatile int*)a.err;  // a failed pivot anywhere ends the walk
+        __syncthreads();
+        if (stop) return;
+    }
+}
+
+// one warp per tail column: the updates from the sparse columns (k < T)
+__global__ void __launch_bounds__(256) tail_columns_kernel(const RefactorArgs a)
+{
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= a.ntc) return;
+    const int sid = a.tc_sub[w];
+    const DevSub& d = a.subs[sid];
+    update_column(a, d.loc_off, a.fbase[sid], d.loc_off + a.tc_col[w], d.T, lane);
+}
+
+// one warp per tail column: its rows >= T into the dense tail (mirrored for L L^T)
+__global__ void __launch_bounds__(256) gather_tails_kernel(const RefactorArgs a)
+{
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= a.ntc) return;
+    const int sid = a.tc_sub[w];
+    const DevSub& d = a.subs[sid];
+    const int T = d.T, s = d.n_local - T;
+    const int j = a.tc_col[w];
+    const int64_t gj = d.loc_off + j;
+    double* S = a.S + d.d_off;
+    const bool llt = a.fllt[gj];
+    for (int64_t p = a.fcp[gj] + lane; p < a.fcp[gj + 1]; p += 32) {
+        const int i = a.fri[p];
+        if (i < T) continue;
+        const double v = a.F[p];
+        S[(int64_t)(i - T) * s + (j - T)] = v;
+        if (llt && i != j) S[(int64_t)(j - T) * s + (i - T)] = v;
+    }
+}
+
+// Dense LU without pivoting of one s x s row-major matrix per CTA (the row order of the setup's
+// factor is kept), blocked by NB columns: panel factorization, then the trailing update with the
+// panel's U rows staged in shared memory chunk by chunk.
+constexpr int LU_NB = 16;
+constexpr int LU_CHUNK = 256;  // trailing columns per staged chunk (32 KB of shared memory)
+
+__global__ void __launch_bounds__(512, 1) dense_lu_kernel(const RefactorArgs a)
+{
+    __shared__ double us[LU_NB * LU_CHUNK];
+    __shared__ int bad;
+    const DevSub& d = a.subs[blockIdx.x];
+    const int n = d.n_local - d.T;
+    if (n <= 0) return;
+    double* __restrict__ S = a.S + d.d_off;
+    const bool llt = a.fllt[d.loc_off + d.T];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int k0 = 0; k0 < n; k0 += LU_NB) {
+        const int kb = min(LU_NB, n - k0), ke = k0 + kb;
+        // panel: columns [k0, ke) for every row below, and the U rows [k0, ke) to the right
+        for (int k = k0; k < ke; ++k) {
+            const double piv = S[(int64_t)k * n + k];
+            if (piv == 0.0 || !isfinite(piv) || (llt && !(piv > 0.0))) {
+                if (tid == 0) {
+                    bad = 1;
+                    set_err(a.err, 2);
+                }
+            }
+            __syncthreads();
+            if (bad) return;
+            const double pinv = 1.0 / piv;
+            // rows below k: the multiplier, and the update of the remaining panel columns
+            const int w = ke - k - 1;  // panel columns right of k
+            for (int i = k + 1 + tid; i < n; i += nt) {
+                double* Si = S + (int64_t)i * n;
+                const double l = Si[k] * pinv;
+                Si[k] = l;
+                for (int j = 1; j <= w; ++j) Si[k + j] -= l * S[(int64_t)k * n + k + j];
+            }
+            __syncthreads();
+            // the panel's own rows (k, ke): their entries right of the panel
+            const int rows = ke - k - 1, cols = n - ke;
+            for (int64_t e = tid; e < (int64_t)rows * cols; e += nt) {
+                const int i = k + 1 + (int)(e / cols), j = ke + (int)(e % cols);
+                S[(int64_t)i * n + j] -= S[(int64_t)i * n + k] * S[(int64_t)k * n + j];
+            }
+            __syncthreads();
+        }
+        // trailing update: S(ke:, ke:) -= L(ke:, k0:ke) U(k0:ke, ke:)
+        for (int j0 = ke; j0 < n; j0 += LU_CHUNK) {
+            const int cw = min(LU_CHUNK, n - j0);
+            for (int e = tid; e < LU_NB * cw; e += nt) {
+                const int kk = e / cw, jj = e % cw;
+                us[kk * LU_CHUNK + jj] = kk < kb ? S[(int64_t)(k0 + kk) * n + j0 + jj] : 0.0;
+            }
+            __syncthreads();
+            // thread: 4 consecutive columns of one row; rows strided by the thread groups
+            const int groups_per_row = (cw + 3) >> 2;
+            const int rows_per_pass = max(1, nt / groups_per_row);
+            const int g = tid % groups_per_row, r0 = tid / groups_per_row;
+            if (r0 < rows_per_pass) {
+                const int jj0 = g * 4;
+                for (int i = ke + r0; i < n; i += rows_per_pass) {
+                    double* Si = S + (int64_t)i * n;
+                    double l[LU_NB];
+#pragma unroll
+                    for (int kk = 0; kk < LU_NB; ++kk) l[kk] = kk < kb ? Si[k0 + kk] : 0.0;
+                    double acc[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = jj0 + q < cw ? Si[j0 + jj0 + q] : 0.0;
+#pragma unroll
+                    for (int kk = 0; kk < LU_NB; ++kk)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[q] -= l[kk] * us[kk * LU_CHUNK + min(jj0 + q, LU_CHUNK - 1)];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (jj0 + q < cw) Si[j0 + jj0 + q] = acc[q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Lt / Ut row-major from the LU of a tail: LU: Lt unit lower, Ut upper.  L L^T (LU of a symmetric
+// S = L D L^T): Lt = L D^1/2, Ut = Lt^T.
+__global__ void tail_triangles_kernel(const double* __restrict__ S, int s, int llt, double* __restrict__ Lt,
+                                      double* __restrict__ Ut)
+{
+    const int64_t total = (int64_t)s * s;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / s), c = (int)(e % s);
+        double lv = 0.0, uv = 0.0;
+        if (llt) {
+            if (r >= c) lv = (r == c ? 1.0 : S[e]) * sqrt(S[(int64_t)c * s + c]);
+            if (r <= c) uv = (r == c ? 1.0 : S[(int64_t)c * s + r]) * sqrt(S[(int64_t)r * s + r]);
+        } else {
+            if (r > c) lv = S[e];
+            else if (r == c) lv = 1.0;
+            if (r <= c) uv = S[e];
+        }
+        Lt[e] = lv;
+        Ut[e] = uv;
+    }
+}
+
+__global__ void identity_kernel(double* M, int s)
+{
+    const int64_t total = (int64_t)s * s;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+        M[e] = (e / s == e % s) ? 1.0 : 0.0;
+}
+
+// packed sweep values: one warp per (subdomain, sweep warp) walking its tasks in the layout of
+// the sweep; entry value = F(src) / diagonal of its row (padding 0, chain-block rows skipped)
+template <typename Real>
+__global__ void __launch_bounds__(256) sweep_values_kernel(int nsub, const int64_t* __restrict__ fbase,
+                                                           const double* __restrict__ F,
+                                                           const int64_t* __restrict__ wtask,
+                                                           const int64_t* __restrict__ wslot,
+                                                           const int64_t* __restrict__ went,
+                                                           const uint32_t* __restrict__ thdr,
+                                                           const int32_t* __restrict__ tslot,
+                                                           const int32_t* __restrict__ src,
+                                                           const DevSub* __restrict__ subs,
+                                                           const int32_t* __restrict__ dsrc, Real* __restrict__ val)
+{
+    const int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wi >= (int64_t)nsub * S2L_SWEEP_WARPS) return;
+    const int sid = (int)(wi / S2L_SWEEP_WARPS);
+    const int64_t fb = fbase[sid], lo = subs[sid].loc_off;
+    int64_t so = wslot[wi], eo = went[wi];
+    for (int64_t t = wtask[wi]; t < wtask[wi + 1]; ++t) {
+        const uint32_t h = thdr[t];
+        const int C = (int)(h & 0xFFFFu), gl2 = (int)((h >> 16) & 7u), R = (int)((h >> 19) & 31u) + 1;
+        const int k = lane >> gl2;
+        double di = 0.0;  // 1 / diagonal of the lane's row, in FP64 as at setup
+        if (k < R) {
+            const int32_t q = dsrc[lo + tslot[so + k]];
+            di = q >= 0 ? 1.0 / F[fb + q] : 1.0;
+        }
+        so += R;
+        for (int c = 0; c < C; ++c) {
+            const int64_t e = eo + (int64_t)c * 32 + lane;
+            const int32_t p = src[e];
+            if (p >= 0) val[e] = (Real)(F[fb + p] * di);
+            else if (p == -1) val[e] = Real(0);
+        }
+        eo += (int64_t)C * 32;
+    }
+}
+
+// 1 / diagonal per slot (1 where the source is -1: unit diagonals, chain-block rows, tail rows)
+template <typename Real>
+__global__ void dinv_kernel(int nsub, const DevSub* __restrict__ subs, const int64_t* __restrict__ fbase,
+                            const double* __restrict__ F, const int32_t* __restrict__ dsrc, Real* __restrict__ dinv)
+{
+    const int sid = blockIdx.y;
+    const DevSub& d = subs[sid];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.n_local; p += gridDim.x * blockDim.x) {
+        const int32_t q = dsrc[d.loc_off + p];
+        dinv[d.loc_off + p] = q >= 0 ? (Real)(1.0 / F[fbase[sid] + q]) : Real(1);
+    }
+}
+
+// chain blocks: W from F, W^-1 by forward substitution (as at setup), and the rewritten rows
+// sum_b W^-1(a, b) M(B[b], c); one warp per block
+template <typename Real>
+__global__ void __launch_bounds__(256) blocks_kernel(int64_t nblocks, const int64_t* __restrict__ boff,
+                                                     const int64_t* __restrict__ bioff,
+                                                     const int64_t* __restrict__ wsrc,
+                                                     const int64_t* __restrict__ be_off,
+                                                     const int64_t* __restrict__ be_pos,
+                                                     const uint8_t* __restrict__ be_row,
+                                                     const int64_t* __restrict__ be_cp,
+                                                     const uint8_t* __restrict__ bc_b,
+                                                     const int64_t* __restrict__ bc_pos, const double* __restrict__ F,
+                                                     Real* __restrict__ binv, Real* __restrict__ val)
+{
+    __shared__ double wsh[8][S2L_CHAIN_MAX * (S2L_CHAIN_MAX + 1) / 2 * 2];
+    const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, wl = (threadIdx.x >> 5) & 7;
+    if (b >= nblocks) return;
+    const int k = (int)(boff[b + 1] - boff[b]);
+    const int np = k * (k + 1) / 2;
+    double* W = wsh[wl];
+    double* Wi = W + np;
+    const int64_t io = bioff[b];
+    for (int e = lane; e < np; e += 32) {
+        int i = 0;
+        while ((i + 1) * (i + 2) / 2 <= e) ++i;
+        const int j = e - i * (i + 1) / 2;
+        const int64_t q = wsrc[io + e];
+        W[e] = q >= 0 ? F[q] : (i == j ? 1.0 : 0.0);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // Wi = W^-1, column by column (lower, packed row-major)
+        for (int j = 0; j < k; ++j)
+            for (int i = j; i < k; ++i) {
+                double v = i == j ? 1.0 : 0.0;
+                for (int q = j; q < i; ++q) v -= W[i * (i + 1) / 2 + q] * Wi[q * (q + 1) / 2 + j];
+                Wi[i * (i + 1) / 2 + j] = v / W[i * (i + 1) / 2 + i];
+            }
+    }
+    __syncwarp();
+    for (int e = lane; e < np; e += 32) binv[io + e] = (Real)Wi[e];
+    for (int64_t e = be_off[b] + lane; e < be_off[b + 1]; e += 32) {
+        const int arow = be_row[e];
+        double v = 0.0;
+        for (int64_t c = be_cp[e]; c < be_cp[e + 1]; ++c) v += Wi[arow * (arow + 1) / 2 + bc_b[c]] * F[bc_pos[c]];
+        val[be_pos[e]] = (Real)v;
+    }
+}
+
+template <typename Real>
+__global__ void gather_values_kernel(int64_t count, const int64_t* __restrict__ src, const double* __restrict__ F,
+                                     Real* __restrict__ out)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = (Real)F[src[e]];
+}
+
+// A 1 in row order (the same summation order as the host's)
+__global__ void row_sums_kernel(int64_t n, const int32_t* __restrict__ rp, const double* __restrict__ v,
+                                double* __restrict__ out)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int32_t e = rp[r]; e < rp[r + 1]; ++e) s += v[e];
+        out[r] = s;
+    }
+}
+
+// Y (n0 x 16 interleaved) = columns c0 .. c0 + 15 of the identity
+__global__ void unit_block_kernel(int64_t n0, int c0, double* Y)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n0 * 16; e += (int64_t)gridDim.x * blockDim.x)
+        Y[e] = (e / 16 == c0 + e % 16) ? 1.0 : 0.0;
+}
+
+// E(:, c0 + r) = C(:, r) for the columns inside [0, n0) (E row-major)
+__global__ void scatter_columns_kernel(int64_t n0, int c0, const double* C, double* E)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n0 * 16; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = e / 16;
+        const int col = c0 + (int)(e % 16);
+        if (col < n0) E[row * n0 + col] = C[e];
+    }
+}
+
+// Gauss-Jordan step k, part 1 (one CTA): the pivot row (largest |A(i, k)|, i >= k; the first of
+// equals), the row swap, column k saved, row k scaled (A(k, k) <- 1 / pivot)
+__global__ void __launch_bounds__(1024) gj_pivot_kernel(int n, int k, double* A, double* colbuf, int* piv, int* err)
+{
+    __shared__ double bv[32];
+    __shared__ int bi[32];
+    __shared__ int prow;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (*(volatile int*)err) return;
+    double best = -1.0;
+    int besti = n;
+    for (int i = k + tid; i < n; i += blockDim.x) {
+        const double v = fabs(A[(int64_t)i * n + k]);
+        if (v > best || (v == best && i < besti)) {
+            best = v;
+            besti = i;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+        if (ov > best || (ov == best && oi < besti)) {
+            best = ov;
+            besti = oi;
+        }
+    }
+    if (lane == 0) {
+        bv[wid] = best;
+        bi[wid] = besti;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double b = -1.0;
+        int p = n;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            if (bv[w] > b || (bv[w] == b && bi[w] < p)) {
+                b = bv[w];
+                p = bi[w];
+            }
+        prow = (b > 0.0 && isfinite(b)) ? p : -1;
+        if (prow < 0) set_err(err, 3);
+        piv[k] = prow;
+    }
+    __syncthreads();
+    const int p = prow;
+    if (p < 0) return;
+    if (p != k)
+        for (int j = tid; j < n; j += blockDim.x) {
+            const double t = A[(int64_t)k * n + j];
+            A[(int64_t)k * n + j] = A[(int64_t)p * n + j];
+            A[(int64_t)p * n + j] = t;
+        }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) colbuf[i] = A[(int64_t)i * n + k];
+    __syncthreads();
+    const double pinv = 1.0 / colbuf[k];
+    for (int j = tid; j < n; j += blockDim.x) A[(int64_t)k * n + j] = j == k ? pinv : A[(int64_t)k * n + j] * pinv;
+}
+
+// part 2: every other row i: A(i, j) -= A_old(i, k) A(k, j) (j != k), A(i, k) = -A_old(i, k) / pivot
+__global__ void gj_update_kernel(int n, int k, double* A, const double* colbuf, const int* err)
+{
+    if (*(volatile const int*)err) return;
+    const int64_t total = (int64_t)n * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e % n);
+        if (i == k) continue;
+        const double f = colbuf[i];
+        if (j == k) A[e] = -f * A[(int64_t)k * n + k];
+        else if (f != 0.0) A[e] -= f * A[(int64_t)k * n + j];
+    }
+}
+
+// the row swaps undone as column swaps in reverse order (one thread per row)
+__global__ void gj_unpermute_kernel(int n, double* A, const int* piv, const int* err)
+{
+    if (*(volatile const int*)err) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double* Ai = A + (int64_t)i * n;
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k) {
+            const double t = Ai[k];
+            Ai[k] = Ai[p];
+            Ai[p] = t;
+        }
+    }
+}
+
+int grid_for(int64_t work, int bs)
+{
+    const int64_t g = (work + bs - 1) / bs;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+}  // namespace
+
+namespace s2l {
+
+void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, const int64_t* dst, const double* val,
+                          double* F)
+{
+    if (count > 0) fill_kernel<<<grid_for(count, 256), 256, 0, st>>>(count, src, dst, val, F);
+}
+
+void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub)
+{
+    sparse_columns_kernel<<<nsub, 1024, 0, st>>>(a);
+}
+
+void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a)
+{
+    if (a.ntc > 0) tail_columns_kernel<<<(int)((a.ntc * 32 + 255) / 256), 256, 0, st>>>(a);
+}
+
+void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a)
+{
+    if (a.ntc > 0) gather_tails_kernel<<<(int)((a.ntc * 32 + 255) / 256), 256, 0, st>>>(a);
+}
+
+void launch_dense_lu(cudaStream_t st, const RefactorArgs& a, int nsub)
+{
+    dense_lu_kernel<<<nsub, 512, 0, st>>>(a);
+}
+
+void launch_tail_triangles(cudaStream_t st, const double* S, int s, int llt, double* Lt, double* Ut)
+{
+    tail_triangles_kernel<<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(S, s, llt, Lt, Ut);
+}
+
+void launch_identity(cudaStream_t st, double* M, int s)
+{
+    identity_kernel<<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(M, s);
+}
+
+template <typename Real>
+void launch_refactor_sweep_values(cudaStream_t st, int nsub, const int64_t* fbase, const double* F,
+                                  const int64_t* wtask, const int64_t* wslot, const int64_t* went,
+                                  const uint32_t* thdr, const int32_t* tslot, const int32_t* src, const DevSub* subs,
+                                  const int32_t* dsrc, Real* val)
+{
+    const int64_t warps = (int64_t)nsub * S2L_SWEEP_WARPS;
+    sweep_values_kernel<Real><<<(int)((warps * 32 + 255) / 256), 256, 0, st>>>(nsub, fbase, F, wtask, wslot, went, thdr,
+                                                                             tslot, src, subs, dsrc, val);
+}
+
+template <typename Real>
+void launch_refactor_dinv(cudaStream_t st, int nsub, const DevSub* subs, const int64_t* fbase, const double* F,
+                          const int32_t* dsrc, Real* dinv)
+{
+    dinv_kernel<Real><<<dim3(16, nsub), 256, 0, st>>>(nsub, subs, fbase, F, dsrc, dinv);
+}
+
+template <typename Real>
+void launch_refactor_blocks(cudaStream_t st, int64_t nblocks, const int64_t* boff, const int64_t* bioff,
+                            const int64_t* wsrc, const int64_t* be_off, const int64_t* be_pos, const uint8_t* be_row,
+                            const int64_t* be_cp, const uint8_t* bc_b, const int64_t* bc_pos, const double* F,
+                            Real* binv, Real* val)
+{
+    if (nblocks > 0)
+        blocks_kernel<Real><<<(int)((nblocks * 32 + 255) / 256), 256, 0, st>>>(nblocks, boff, bioff, wsrc, be_off,
+                                                                               be_pos, be_row, be_cp, bc_b, bc_pos,
+                                                                               F, binv, val);
+}
+
+template <typename Real>
+void launch_gather_values(cudaStream_t st, int64_t count, const int64_t* src, const double* F, Real* out)
+{
+    if (count > 0) gather_values_kernel<Real><<<grid_for(count, 256), 256, 0, st>>>(count, src, F, out);
+}
+
+void launch_row_sums(cudaStream_t st, int64_t n, const int32_t* rp, const double* v, double* out)
+{
+    row_sums_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, rp, v, out);
+}
+
+void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y)
+{
+    unit_block_kernel<<<grid_for(n0 * 16, 256), 256, 0, st>>>(n0, c0, Y);
+}
+
+void launch_scatter_columns(cudaStream_t st, int64_t n0, int c0, const double* C, double* E)
+{
+    scatter_columns_kernel<<<grid_for(n0 * 16, 256), 256, 0, st>>>(n0, c0, C, E);
+}
+
+void launch_gauss_jordan(cudaStream_t st, int n, double* A, double* colbuf, int* piv, int* err)
+{
+    const int g = grid_for((int64_t)n * n, 256);
+    for (int k = 0; k < n; ++k) {
+        gj_pivot_kernel<<<1, 1024, 0, st>>>(n, k, A, colbuf, piv, err);
+        gj_update_kernel<<<g, 256, 0, st>>>(n, k, A, colbuf, err);
+    }
+    gj_unpermute_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, A, piv, err);
+}
+
+template void launch_refactor_sweep_values<double>(cudaStream_t, int, const int64_t*, const double*, const int64_t*,
+                                                   const int64_t*, const int64_t*, const uint32_t*, const int32_t*,
+                                                   const int32_t*, const DevSub*, const int32_t*, double*);
+template void launch_refactor_sweep_values<float>(cudaStream_t, int, const int64_t*, const double*, const int64_t*,
+                                                  const int64_t*, const int64_t*, const uint32_t*, const int32_t*,
+                                                  const int32_t*, const DevSub*, const int32_t*, float*);
+template void launch_refactor_dinv<double>(cudaStream_t, int, const DevSub*, const int64_t*, const double*,
+                                           const int32_t*, double*);
+template void launch_refactor_dinv<float>(cudaStream_t, int, const DevSub*, const int64_t*, const double*,
+                                          const int32_t*, float*);
+template void launch_refactor_blocks<double>(cudaStream_t, int64_t, const int64_t*, const int64_t*, const int64_t*,
+                                             const int64_t*, const int64_t*, const uint8_t*, const int64_t*,
+                                             const uint8_t*, const int64_t*, const double*, double*, double*);
+template void launch_refactor_blocks<float>(cudaStream_t, int64_t, const int64_t*, const int64_t*, const int64_t*,
+                                            const int64_t*, const int64_t*, const uint8_t*, const int64_t*,
+                                            const uint8_t*, const int64_t*, const double*, float*, float*);
+template void launch_gather_values<double>(cudaStream_t, int64_t, const int64_t*, const double*, double*);
+template void launch_gather_values<float>(cudaStream_t, int64_t, const int64_t*, const double*, float*);
+
+}  // namespace s2l

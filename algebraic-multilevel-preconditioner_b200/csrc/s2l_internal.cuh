@@ -115,6 +115,32 @@ struct LocalSolveArgs {
     int64_t nloc;              // local-space size (stride of the per-column-group ready flags)
 };
 
+// Numeric refactorization of every subdomain's factors on their kept patterns (s2l_gpu_refactor).
+// The factor values live in F, subdomain i's pattern column by column ("combined" CSC: for LU the
+// strict upper rows, the diagonal, then the strict lower rows of each column; for LL^T the lower
+// rows, diagonal first).  Columns are numbered in the local space (loc_off + j).
+struct RefactorArgs {
+    const DevSub* subs;
+    double* F;
+    const int64_t* fbase;      // per subdomain: its first position in F
+    const int64_t* fcp;        // per column (nloc + 1): first position (absolute)
+    const int32_t* fri;        // per position: row (subdomain-local), increasing within a column
+    const int32_t* fdg;        // per column: index of the diagonal within the column
+    const uint8_t* fllt;       // per column: 1 if its subdomain's factor is L L^T
+    const int64_t* frp;        // L L^T: per column j (nloc + 1), range of its row entries L(j, k), k < j
+    const int32_t* frpos;      //   position of L(j, k) (relative to the subdomain's fbase)
+    const int32_t* frk;        //   k (subdomain-local), increasing
+    const int32_t* lv_first;   // per subdomain (nsub + 1): first dependency level of its sparse columns
+    const int64_t* lv_off;     // per level (+1): range in lv_col
+    const int32_t* lv_col;     // sparse columns (j < T, subdomain-local) level by level
+    const int32_t* tc_sub;     // tail columns (j >= T): subdomain and local column
+    const int32_t* tc_col;
+    int64_t ntc;
+    double* S;                 // dense tails (s x s row-major at subs[i].d_off)
+    int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column,
+                               // 2 of a dense tail, 3 singular coarse matrix (0: none)
+};
+
 // launch wrappers (kernels.cu)
 namespace s2l {
 
@@ -186,5 +212,37 @@ void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, co
                            const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
                            const double* y, double* out, double* plocal);
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
+
+// refactorization (refactor.cu)
+void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, const int64_t* dst, const double* val,
+                          double* F);
+void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub);
+void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a);
+void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a);
+void launch_dense_lu(cudaStream_t st, const RefactorArgs& a, int nsub);
+// row-major triangles of subdomain i's factored tail for the inversion: Lt (lower, unit for LU,
+// L of L L^T) and Ut (upper: U, or L^T)
+void launch_tail_triangles(cudaStream_t st, const double* S, int s, int llt, double* Lt, double* Ut);
+void launch_identity(cudaStream_t st, double* M, int s);
+template <typename Real>
+void launch_refactor_sweep_values(cudaStream_t st, int nsub, const int64_t* fbase, const double* F,
+                                  const int64_t* wtask, const int64_t* wslot, const int64_t* went,
+                                  const uint32_t* thdr, const int32_t* tslot, const int32_t* src, const DevSub* subs,
+                                  const int32_t* dsrc, Real* val);
+template <typename Real>
+void launch_refactor_dinv(cudaStream_t st, int nsub, const DevSub* subs, const int64_t* fbase, const double* F,
+                          const int32_t* dsrc, Real* dinv);
+template <typename Real>
+void launch_refactor_blocks(cudaStream_t st, int64_t nblocks, const int64_t* boff, const int64_t* bioff,
+                            const int64_t* wsrc, const int64_t* be_off, const int64_t* be_pos, const uint8_t* be_row,
+                            const int64_t* be_cp, const uint8_t* bc_b, const int64_t* bc_pos, const double* F,
+                            Real* binv, Real* val);
+template <typename Real>
+void launch_gather_values(cudaStream_t st, int64_t count, const int64_t* src, const double* F, Real* out);
+void launch_row_sums(cudaStream_t st, int64_t n, const int32_t* rp, const double* v, double* out);
+// coarse matrix refresh: unit block, E columns, Gauss-Jordan inversion with partial pivoting
+void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y);
+void launch_scatter_columns(cudaStream_t st, int64_t n0, int c0, const double* C, double* E);
+void launch_gauss_jordan(cudaStream_t st, int n, double* A, double* colbuf, int* piv, int* err);
 
 }  // namespace s2l

@@ -34,6 +34,7 @@ EXPORTED = [
     "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
     "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block", "s2l_gpu_update_matrix",
+    "s2l_gpu_refactor",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -111,6 +112,7 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_ticket_free": ([vp], C.c_int),
         "s2l_gpu_apply_block": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
         "s2l_gpu_update_matrix": ([vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_refactor": ([vp, vp, C.c_int], C.c_int),
         "s2l_gpu_gmres_block": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -393,6 +395,16 @@ class GpuSetup:
         """New values of A (same pattern, renumbered CSR order); the preconditioner is kept."""
         v = np.ascontiguousarray(values, dtype=np.float64)
         self.ctx.check(self.lib.s2l_gpu_update_matrix(self.h, _vp(v), PTR_HOST))
+
+    def refactor(self, values):
+        """New values of A (same pattern, renumbered CSR order, host array or a device pointer) and
+        the preconditioner refactorized for them on the device (s2l_gpu_refactor; the setup needs
+        the option refactor=1)."""
+        if isinstance(values, int):
+            self.ctx.check(self.lib.s2l_gpu_refactor(self.h, C.c_void_p(values), PTR_DEVICE))
+            return
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.ctx.check(self.lib.s2l_gpu_refactor(self.h, _vp(v), PTR_HOST))
 
     def apply_block(self, R):
         """Z = M^-1 R for the k rows of R (k x n, host), one block call (s2l_gpu_apply_block)."""

@@ -10,7 +10,9 @@ rtol 1e-8, U[-1,1] right-hand sides.  Forms timed:
                 the recomputed FP64 true residual is <= rtol, one solve per step;
   block_mixed : the mixed form for k right-hand sides per step (s2l_gpu_gmres_block);
   batched / block_mixed_threads: several solves or blocks from host threads at once;
-  serving     : Poisson arrivals over three resident matrices on the worker threads (p50/p99).
+  serving     : Poisson arrivals over three resident matrices on the worker threads (p50/p99);
+  sequence_refactor: the next matrices of the moving-bubble sequence, each refactorized on the
+                device (s2l_gpu_refactor) and solved for --head-k right-hand sides.
 Headline (`value`): block_mixed at --head-k right-hand sides per step (default 16, the batching
 configuration's right-hand sides per matrix), solves/s with b resident in HBM; `e2e` = the same
 through the C ABI with pinned host buffers (copies inside the timed region).
@@ -45,8 +47,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nx", type=int, default=100)
-    ap.add_argument("--nsub", type=int, default=64)
+    ap.add_argument("--workload", default="bubbles3d", choices=["bubbles3d", "convdiff3d"],
+                    help="bubbles3d: the headline configuration; convdiff3d: 128^3 convection-diffusion, "
+                         "128 subdomains, LU factors, FGMRES(40)")
+    ap.add_argument("--nx", type=int, default=0, help="grid size (0: the workload's)")
+    ap.add_argument("--nsub", type=int, default=0, help="subdomains (0: the workload's)")
     ap.add_argument("--nbubbles", type=int, default=200)
     ap.add_argument("--overlap", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -56,7 +61,7 @@ def parse():
     ap.add_argument("--block", default="4,8,16", help="block form: right-hand sides per block GMRES (comma list)")
     ap.add_argument("--head-k", type=int, default=16, help="right-hand sides per step of the headline block form")
     ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
-    ap.add_argument("--seq", type=int, default=4, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
+    ap.add_argument("--seq", type=int, default=8, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
     return ap.parse_args()
@@ -147,7 +152,15 @@ def run_ours(a):
     from s2l_b200 import workloads as W
     from s2l_b200.setup_phase import with_factor_precision
 
-    wl = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap)
+    if a.workload == "convdiff3d":
+        wl = W.convdiff3d(a.nx or 128, a.nsub or 128, precision="double")
+        a.seq = 0  # the moving-bubble sequence belongs to the bubbles workload
+        wdesc = (f"convdiff3d {wl.nx}^3 upwind convection-diffusion (4-mode divergence-free Fourier field), "
+                 f"{wl.nsub} subdomains, overlap 1, nev 24, deflated RAS, LU factors, FGMRES({wl.restart}), rtol 1e-8")
+    else:
+        wl = W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
+        wdesc = (f"bubbles3d {wl.nx}^3 pressure Poisson, {wl.nsub} subdomains, overlap {a.overlap}, nev 20, "
+                 f"deflated RAS, LL^T factors, GMRES({wl.restart}), rtol 1e-8")
     dist = None
     if world > 1:
         import datetime
@@ -174,7 +187,8 @@ def run_ours(a):
     st32 = with_factor_precision(st, "single")
     layout = {kv.split("=")[0]: float(kv.split("=")[1]) for kv in a.opt}
     g64 = capi.GpuSetup(ctx, st, options=layout)
-    g32 = capi.GpuSetup(ctx, st32, options=layout)
+    # the mixed setup keeps its factor patterns on the device for the sequence form's refactorizations
+    g32 = capi.GpuSetup(ctx, st32, options=dict(layout, refactor=1) if a.seq > 0 else layout)
     stream = torch.cuda.current_stream(dev)
     for g in (g64, g32):
         g.set_stream(stream.cuda_stream)
@@ -465,8 +479,9 @@ def run_ours(a):
     e2e_total = max_over_ranks(sum(e2e))
 
     # ---- sequence: the next matrices of the moving-bubble sequence (bubble centres rise half a cell
-    # per step, same pattern) through s2l_gpu_update_matrix, the preconditioner of the first matrix
-    # kept (the reference's reuse level), each solved for head_k right-hand sides
+    # per step, same pattern), each refactorized on the device (s2l_gpu_refactor: new local factors
+    # on the kept patterns, E with the kept basis; the reference's refactorize level) and solved for
+    # head_k right-hand sides; a step is timed from the upload of the new values to the solutions
     sequence = None
     if a.seq > 0:
         import dataclasses
@@ -477,14 +492,14 @@ def run_ours(a):
         Bq = torch.tensor(rng.uniform(-1.0, 1.0, (kh, n)), device=dev)
         Xq = torch.zeros_like(Bq)
         steps_q = []
-        for step in range(a.seq):
+        for step in range(1, a.seq + 1):
             prob = W.make_problem(dataclasses.replace(wl, time=float(step)))
             vals, _ = seqmod.values_in_setup_order(prob.A, st)
             At = sp.csr_matrix((vals, st.A.indices, st.A.indptr), shape=st.A.shape)
             barrier()
             s_ev, m_ev, e_ev = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             s_ev.record(stream)
-            g.update_matrix(vals)
+            g.refactor(vals)
             m_ev.record(stream)
             Xq.zero_()
             _, rq = g.gmres_block((Bq.data_ptr(), kh), device_out=Xq.data_ptr(), **kw)
@@ -493,12 +508,14 @@ def run_ours(a):
             Xh = Xq.cpu().numpy()
             Bh = Bq.cpu().numpy()
             chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(kh))
-            steps_q.append({"step": step, "update_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
+            steps_q.append({"step": step, "refactor_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
                             "iterations_max": max(r["iterations"] for r in rq),
                             "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
-        g.update_matrix(st.A.data)  # back to the setup's own matrix
-        tot_ms = sum(q["update_ms"] + q["solve_ms"] for q in steps_q)
-        sequence = {"matrices": a.seq, "rhs_per_matrix": kh, "steps": steps_q,
+        g.refactor(st32.A.data)  # back to the setup's own matrix
+        tot_ms = sum(q["refactor_ms"] + q["solve_ms"] for q in steps_q)
+        sequence = {"matrices": a.seq, "rhs_per_matrix": kh, "update": "refactorize", "steps": steps_q,
+                    "refactor_ms_mean": float(np.mean([q["refactor_ms"] for q in steps_q])),
+                    "refactor_plan_gb": g.stat("refactor_bytes") / 1e9,
                     "solves_per_s": a.seq * kh / (tot_ms * 1e-3)}
         del Bq, Xq
 
@@ -529,8 +546,7 @@ def run_ours(a):
         "dtype": "f64 (FP32 local factors, FP64 Krylov/coarse/true residual)",
         "data": "synthetic (seeded generator, U[-1,1] right-hand sides)",
         "config": {
-            "workload": f"bubbles3d {a.nx}^3 pressure Poisson, {a.nsub} subdomains, overlap {a.overlap}, nev 20, "
-                        f"deflated RAS, LL^T factors, GMRES(50), rtol 1e-8",
+            "workload": wdesc,
             "form": f"block GMRES, {kh} right-hand sides per step, FP32 local factors, flexible GMRES in FP64, "
                     "converged at FP64 true residual <= rtol",
             "rhs_per_step": kh,
@@ -554,7 +570,7 @@ def run_ours(a):
             "batched_mixed": batched,
             "block_mixed_threads": block_thr,
             "serving": serving,
-            "sequence_reuse": sequence,
+            "sequence_refactor": sequence,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": mixed["iterations"][0] - plain["iterations"][0],
@@ -620,7 +636,7 @@ def run_reference(a):
     from s2l_b200 import workloads as W
     from s2l_b200.rng import random_rhs  # noqa: F401  (the reference draws the same rhs itself)
 
-    wl = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap)
+    wl = W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
     prob = W.make_problem(wl)
     part = W.make_partition(wl, prob).astype(np.int32)
     threads = a.ref_threads or os.cpu_count() or 1

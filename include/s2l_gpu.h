@@ -151,7 +151,9 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "chain_block" (1..16, default 8; 1 = off): rows of a chain block.  Runs of sparse rows where
  *   each row depends on the one solved just before it (the rows of a supernode) are cut into
  *   blocks of up to this many rows; a block's rows are stored multiplied by the inverse of its
- *   diagonal block, so the block is one dependency level of the sweep instead of one per row.
+ *   diagonal block, so the block is one dependency level of the sweep instead of one per row;
+ *   "refactor" (0 or 1, default 0): keep the factor patterns and their maps to the solve layout
+ *   on the device so s2l_gpu_refactor can refactorize for new matrix values.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 
@@ -165,6 +167,19 @@ int s2l_gpu_setup_destroy(s2l_setup* s);
  * (S2L_ERR_STATE) while a solve-phase call runs or solves are queued on the setup. */
 int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind);
 
+/* New values of A with the pattern given to s2l_gpu_set_matrix, and a new preconditioner for them
+ * on the device: the reference's UpdateLevel::Refactorize (include/preconditioner/preconditioner.hpp:
+ * 15-30, src/preconditioner/two_level_schwarz.cpp:30-41).  Every local factor is refactorized
+ * numerically on its kept pattern and permutations (LocalSolver::refactorize,
+ * src/linalg/local_solver.cpp:111-118; LU keeps the setup's row order, it does not pivot again),
+ * and E = W^T A W is recomputed with the kept coarse basis and inverted (CoarseSpace::refresh,
+ * src/preconditioner/coarse_space.cpp:95-105).  Needs the setup option "refactor" = 1, which keeps
+ * the factor patterns and their maps to the solve layout on the device (setup stat
+ * "refactor_bytes"); LU, LL^T and LDL^T factors.  S2L_ERR_NUMERIC for a non-finite value, a zero
+ * (LU) or non-positive (LL^T) pivot or a singular E, and then the setup is unchanged.  Refused
+ * (S2L_ERR_STATE) while a solve-phase call runs or solves are queued on the setup. */
+int s2l_gpu_refactor(s2l_setup* s, const double* val, int ptr_kind);
+
 /* Device bytes held by the setup (matrix, factors, basis, schedules) and its workspaces. */
 int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
 /* Layout statistics after setup_end: "sparse_nnz", "coupling_nnz", "dense_entries", "tail_rows",
@@ -175,7 +190,8 @@ int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes);
    side of a block adds (a block of k reads the factors once: bytes + (k - 1) x this);
    "kc_max": right-hand sides a sparse-sweep CTA holds in shared memory; "spmv_tpr": lanes per row
    of the products with A; "block_width": the block
-   width s2l_gpu_gmres_block uses. */
+   width s2l_gpu_gmres_block uses; "refactor_bytes": device bytes of the refactorization plan
+   (option "refactor"); "refactor_ms": host time of the last s2l_gpu_refactor. */
 int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value);
 
 /* ---- solve phase ----------------------------------------------------------------------

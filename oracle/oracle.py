@@ -53,6 +53,8 @@ def load():
                                  C.c_double, C.POINTER(OResult)]
     lib.oracle_bicgstab.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                     C.POINTER(OResult)]
+    lib.oracle_refactor.restype = C.c_int
+    lib.oracle_refactor.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     _lib = lib
     return lib
 
@@ -172,3 +174,64 @@ class OracleSetup:
             self.close()
         except Exception:
             pass
+
+
+def refactor_factor(fac, Aii):
+    """New factor values for the local matrix Aii on fac's kept pattern and permutations.
+
+    The reference's LocalSolver::refactorize (``src/linalg/local_solver.cpp:111-118``), restated
+    by ``oracle_refactor``: LL^T, or LU with the setup's row order (no new pivoting).  The result
+    keeps fac's value type.  Raises ValueError on a failed pivot or an entry outside the pattern.
+    """
+    import scipy.sparse as sp
+    from s2l_b200.setup_phase import LocalFactor
+    lib = load()
+    if fac.kind not in ("lu", "llt"):
+        raise ValueError("refactorization supports LU and LL^T factors")
+    n = fac.n
+    ipout = np.argsort(fac.perm_out)
+    Ah = sp.csr_matrix(Aii)[fac.perm_in][:, ipout].tocsc()
+    Ah.sort_indices()
+    Ap = np.ascontiguousarray(Ah.indptr, dtype=np.int64)
+    Ai = np.ascontiguousarray(Ah.indices, dtype=np.int32)
+    Ax = np.ascontiguousarray(Ah.data, dtype=np.float64)
+    L = fac.L.astype(np.float64).tocsr()
+    Lp = np.ascontiguousarray(L.indptr, dtype=np.int64)
+    Li = np.ascontiguousarray(L.indices, dtype=np.int32)
+    Lx = np.zeros(L.nnz)
+    Up = Ui = Ux = None
+    if fac.kind == "lu":
+        U = fac.U.astype(np.float64).tocsr()
+        Up = np.ascontiguousarray(U.indptr, dtype=np.int64)
+        Ui = np.ascontiguousarray(U.indices, dtype=np.int32)
+        Ux = np.zeros(U.nnz)
+    rc = lib.oracle_refactor(n, 0 if fac.kind == "lu" else 1, _a(Ap), _a(Ai), _a(Ax), _a(Lp), _a(Li), _a(Lx),
+                             _a(Up), _a(Ui), _a(Ux))
+    if rc == -(n + 1):
+        raise ValueError("an entry of the local matrix lies outside the factor pattern")
+    if rc:
+        raise ValueError(f"refactorization: bad pivot in column {-rc - 1}")
+    dt = fac.L.dtype
+    Ln = sp.csr_matrix((Lx.astype(dt), Li, Lp), shape=(n, n))
+    Un = sp.csr_matrix((Ux.astype(dt), Ui, Up), shape=(n, n)) if Ux is not None else None
+    return LocalFactor(fac.kind, Ln, Un, fac.perm_in, fac.perm_out)
+
+
+def refactor_setup(st, A_new):
+    """The setup after the reference's Refactorize on the new matrix A_new (renumbered, same pattern).
+
+    Local factors refactorized on their patterns (``refactor_factor``), the coarse basis kept and
+    E = W^T A_new W recomputed with it (``CoarseSpace::refresh``,
+    ``src/preconditioner/coarse_space.cpp:95-105, 186-206``).
+    """
+    import dataclasses
+    import scipy.sparse as sp
+    from s2l_b200.setup_phase import coarse_matrix
+    A_new = sp.csr_matrix(A_new)
+    subs = []
+    for s in st.subdomains:
+        idx = s.l2g()
+        Aii = A_new[idx][:, idx]
+        subs.append(dataclasses.replace(s, factor=refactor_factor(s.factor, Aii), Aii=Aii))
+    E = coarse_matrix(A_new, subs, st.offsets) if st.n0 else st.E
+    return dataclasses.replace(st, A=A_new, subdomains=subs, E=E)

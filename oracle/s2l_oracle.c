@@ -654,3 +654,126 @@ int oracle_bicgstab(OSetup *s, const double *b, double *x, double rtol, int maxi
     free(r); free(rh); free(p); free(v); free(y); free(sv); free(z); free(t);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------------- */
+/* Numeric refactorization on a kept factor pattern.
+ *
+ * The reference's UpdateLevel::Refactorize (include/preconditioner/preconditioner.hpp:15-30,
+ * src/preconditioner/two_level_schwarz.cpp:30-41) refills A_ii from the new matrix
+ * (Subdomain::refillValues, src/partition/subdomain.cpp:107-127) and calls
+ * LocalSolver::refactorize (src/linalg/local_solver.cpp:111-118): Eigen's factorize() with the
+ * ordering and elimination tree of analyzePattern() kept.  This restates that numeric step on the
+ * factor pattern of include/s2l_gpu.h: the input is the permuted local matrix Ahat = P_in A_ii Q
+ * (CSC, its pattern inside the factor's), with Ahat(p, q) = A_ii(perm_in[p], j) for
+ * perm_out[j] = q.
+ *   kind 0 (LU): left-looking LU with the setup's row order kept (no new pivoting); L unit lower
+ *                with its diagonal stored, U upper.
+ *   kind 1 (LL^T): left-looking Cholesky.
+ * New values go to Lx (and Ux), in the CSR order of Lp/Li (Up/Ui).  Returns 0; -(j + 1) for a zero
+ * (LU) or non-positive (LL^T) pivot in column j; -(n + 1) when an entry of Ahat lies outside the
+ * factor pattern.
+ */
+int oracle_refactor(int n, int kind, const int64_t *Ap, const int32_t *Ai, const double *Ax, const int64_t *Lp,
+                    const int32_t *Li, double *Lx, const int64_t *Up, const int32_t *Ui, double *Ux)
+{
+    /* column views of the CSR factors: per column, (row, CSR position) in increasing row order */
+    int64_t *lcp = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+    int64_t *ucp = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+    const int64_t lnz = Lp[n], unz = kind == 0 ? Up[n] : 0;
+    int32_t *lrow = (int32_t *)malloc((size_t)(lnz ? lnz : 1) * sizeof(int32_t));
+    int64_t *lpos = (int64_t *)malloc((size_t)(lnz ? lnz : 1) * sizeof(int64_t));
+    int32_t *urow = (int32_t *)malloc((size_t)(unz ? unz : 1) * sizeof(int32_t));
+    int64_t *upos = (int64_t *)malloc((size_t)(unz ? unz : 1) * sizeof(int64_t));
+    double *x = (double *)calloc((size_t)n + 1, sizeof(double));
+    char *in = (char *)calloc((size_t)n + 1, 1);
+    int rc = 0;
+    for (int64_t e = 0; e < lnz; ++e) ++lcp[Li[e] + 1];
+    for (int j = 0; j < n; ++j) lcp[j + 1] += lcp[j];
+    for (int64_t e = 0; e < unz; ++e) ++ucp[Ui[e] + 1];
+    for (int j = 0; j < n; ++j) ucp[j + 1] += ucp[j];
+    {
+        int64_t *nx = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+        memcpy(nx, lcp, ((size_t)n + 1) * sizeof(int64_t));
+        for (int r = 0; r < n; ++r) /* rows in increasing order: each column's rows come out sorted */
+            for (int64_t e = Lp[r]; e < Lp[r + 1]; ++e) {
+                const int64_t q = nx[Li[e]]++;
+                lrow[q] = r;
+                lpos[q] = e;
+            }
+        if (kind == 0) {
+            memcpy(nx, ucp, ((size_t)n + 1) * sizeof(int64_t));
+            for (int r = 0; r < n; ++r)
+                for (int64_t e = Up[r]; e < Up[r + 1]; ++e) {
+                    const int64_t q = nx[Ui[e]]++;
+                    urow[q] = r;
+                    upos[q] = e;
+                }
+        }
+        free(nx);
+    }
+    for (int j = 0; j < n && rc == 0; ++j) {
+        /* work column on the pattern of column j */
+        for (int64_t q = lcp[j]; q < lcp[j + 1]; ++q) {
+            x[lrow[q]] = 0.0;
+            in[lrow[q]] = 1;
+        }
+        for (int64_t q = ucp[j]; q < ucp[j + 1]; ++q) {
+            x[urow[q]] = 0.0;
+            in[urow[q]] = 1;
+        }
+        for (int64_t e = Ap[j]; e < Ap[j + 1]; ++e) {
+            const int i = Ai[e];
+            if (kind == 1 && i < j) continue; /* LL^T reads the lower triangle */
+            if (!in[i]) {
+                rc = -(n + 1);
+                break;
+            }
+            x[i] += Ax[e];
+        }
+        if (rc) break;
+        if (kind == 0) {
+            /* U(:, j) by a sparse triangular solve with the finished columns of L, in row order */
+            for (int64_t q = ucp[j]; q < ucp[j + 1]; ++q) {
+                const int k = urow[q];
+                if (k >= j) break;
+                const double u = x[k];
+                for (int64_t t = lcp[k]; t < lcp[k + 1]; ++t)
+                    if (lrow[t] > k) x[lrow[t]] -= Lx[lpos[t]] * u;
+            }
+            const double piv = x[j];
+            if (piv == 0.0 || !isfinite(piv)) {
+                rc = -(j + 1);
+                break;
+            }
+            for (int64_t q = ucp[j]; q < ucp[j + 1]; ++q) Ux[upos[q]] = x[urow[q]];
+            for (int64_t q = lcp[j]; q < lcp[j + 1]; ++q) Lx[lpos[q]] = lrow[q] == j ? 1.0 : x[lrow[q]] / piv;
+        } else {
+            /* column j of L: Ahat(j:n, j) - sum_k L(j:n, k) L(j, k) over the finished columns k < j */
+            for (int64_t e = Lp[j]; e < Lp[j + 1]; ++e) {
+                const int k = Li[e];
+                if (k >= j) break;
+                const double ljk = Lx[e];
+                for (int64_t t = lcp[k]; t < lcp[k + 1]; ++t)
+                    if (lrow[t] >= j) x[lrow[t]] -= Lx[lpos[t]] * ljk;
+            }
+            const double d = x[j];
+            if (!(d > 0.0) || !isfinite(d)) {
+                rc = -(j + 1);
+                break;
+            }
+            const double ljj = sqrt(d);
+            for (int64_t q = lcp[j]; q < lcp[j + 1]; ++q) Lx[lpos[q]] = lrow[q] == j ? ljj : x[lrow[q]] / ljj;
+        }
+        for (int64_t q = lcp[j]; q < lcp[j + 1]; ++q) in[lrow[q]] = 0;
+        for (int64_t q = ucp[j]; q < ucp[j + 1]; ++q) in[urow[q]] = 0;
+    }
+    free(lcp);
+    free(ucp);
+    free(lrow);
+    free(lpos);
+    free(urow);
+    free(upos);
+    free(x);
+    free(in);
+    return rc;
+}

@@ -137,3 +137,36 @@ def test_sequence_values_in_setup_order(tmp_path):
     bad[0, st.n - 1] = 1.0
     with pytest.raises(sequence.PatternChanged):
         sequence.values_in_setup_order(bad.tocsr(), st)
+
+
+@pytest.mark.parametrize("name", ["bubbles3d", "convdiff3d", "poisson2d"])
+def test_oracle_refactorization_pinned_on_superlu(name):
+    """The oracle's refactorization on a kept pattern (LocalSolver::refactorize) reproduces the
+    setup's SuperLU factors of the same matrix to rounding, and factorizes a matrix with new
+    values of the same pattern exactly (P_in A_ii Q = L U)."""
+    import scipy.sparse as sp
+    from oracle.oracle import refactor_factor
+    _, st = small_setup(name)
+    for s in st.subdomains[:3]:
+        f = s.factor
+        idx = s.l2g()
+        Aii = st.A[idx][:, idx]
+        g = refactor_factor(f, Aii)
+        assert abs(g.L - f.L).max() <= 1e-12 * abs(f.L).max()
+        if f.kind == "lu":
+            assert abs(g.U - f.U).max() <= 1e-12 * abs(f.U).max()
+        d = 1.0 + 0.1 * np.random.default_rng(3).uniform(-1.0, 1.0, Aii.shape[0])
+        A2 = (sp.diags(d) @ Aii @ sp.diags(d)).tocsr()
+        g2 = refactor_factor(f, A2)
+        Ah = A2[f.perm_in][:, np.argsort(f.perm_out)]
+        LU = g2.L @ (g2.U if f.kind == "lu" else g2.L.T)
+        assert abs(LU - Ah).max() <= 1e-13 * abs(Ah).max()
+
+
+def test_oracle_refactorization_reports_bad_pivots():
+    from oracle.oracle import refactor_factor
+    _, st = small_setup("bubbles3d")
+    s = st.subdomains[0]
+    idx = s.l2g()
+    with pytest.raises(ValueError):
+        refactor_factor(s.factor, -st.A[idx][:, idx])
