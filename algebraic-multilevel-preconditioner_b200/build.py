@@ -34,7 +34,7 @@ def build_gpu_lib(force: bool = False, verbose: bool = False, ptxas_info: bool =
     if ptxas_info:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-lcublas", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
+    cmd += ["-lcublas", "-lcusolver", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -9,6 +9,7 @@
 #include "../../include/s2l_gpu.h"
 
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -218,6 +219,8 @@ struct s2l_setup {
         double* F = nullptr;
         double* S = nullptr;      // dense tails (FP64)
         double* stage = nullptr;  // the new matrix values until they are committed
+        double* part = nullptr;   // partial columns of the cooperative column updates
+        int maxcol = 1;
         int* err = nullptr;
         int64_t *fbase = nullptr, *fcp = nullptr, *frp = nullptr, *lv_off = nullptr;
         int32_t *fri = nullptr, *fdg = nullptr, *frpos = nullptr, *frk = nullptr, *lv_first = nullptr,
@@ -232,8 +235,23 @@ struct s2l_setup {
         std::vector<char> llt;   // per subdomain
         std::vector<int64_t> d_off;
         size_t bytes = 0;        // device bytes of the plan
-        cublasHandle_t blas = nullptr;
+        // dense tails factorized and inverted on RF_STREAMS streams at once, each with its cuSOLVER
+        // and cuBLAS handles, factorization workspace and inversion buffer
+        static constexpr int RF_STREAMS = 4;
+        cudaStream_t tstream[RF_STREAMS] = {};
+        cudaEvent_t tev[RF_STREAMS + 1] = {};
+        cublasHandle_t tblas[RF_STREAMS] = {};
+        cusolverDnHandle_t tsolver[RF_STREAMS] = {};
+        double* swork[RF_STREAMS] = {};
+        double* B[RF_STREAMS] = {};
+        int lwork = 0;
+        int* info = nullptr;  // per subdomain: the dense tail factorization's status
+        // coarse matrix refresh: E and its inversion, 16 unit vectors through prolong / A / restrict
+        double *E = nullptr, *colbuf = nullptr, *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr,
+               *C = nullptr, *plocal = nullptr, *rowsum = nullptr;
+        int* piv = nullptr;
         double last_ms = 0.0;
+        double phase_ms[5] = {0, 0, 0, 0, 0};  // coarse matrix, sparse columns, tail columns, dense tails, commit
     } rf;
 
     int fail(int code, const std::string& msg)
@@ -2012,6 +2030,14 @@ int s2l_gpu_setup_end(s2l_setup* s)
         if (rfon) {
             if (!make_fpattern(h.L, U, nl, llt, P))
                 return s->fail(S2L_ERR_BADARG, "subdomain " + std::to_string(i) + ": a factor has no diagonal entry");
+            // the column kernels address a column's tail rows through 16-bit offsets and keep one
+            // row map of the tail per warp in shared memory
+            for (int c = 0; c < nl; ++c) {
+                if (P.cp[c + 1] - P.cp[c] >= 65535)
+                    return s->fail(S2L_ERR_BADARG, "refactor: a factor column has 65535 or more entries");
+                s->rf.maxcol = std::max(s->rf.maxcol, (int)(P.cp[c + 1] - P.cp[c]));
+            }
+            if (sz > 100000) return s->fail(S2L_ERR_BADARG, "refactor: a dense tail of more than 100000 rows");
             mposL.assign(h.L.ci.size(), -1);
             for (int r = 0; r < nl; ++r)
                 for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) {
@@ -2303,54 +2329,6 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(dev_alloc(s, &s->d_linv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(dev_alloc(s, &s->d_uinv, (size_t)std::max<int64_t>(d_off[nsub], 1) * rs));
     RET_IF(invert_tails(s, Ltt, Utt, d_off));
-    if (rfon) {
-        auto& R = s->rf;
-        const size_t before = s->bytes;
-        rf_fcp.push_back(rf_fbase.back());
-        rf_lvfirst.push_back((int32_t)(rf_lvoff.size() - 1));
-        R.nF = rf_fbase.back();
-        R.nfill = (int64_t)rf_fill_src.size();
-        R.ntc = (int64_t)rf_tcsub.size();
-        R.nlts = (int64_t)rf_lts.size();
-        R.nust = (int64_t)rf_ust.size();
-        R.d_off = d_off;
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.F), (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double)));
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.S), (size_t)std::max<int64_t>(d_off[nsub], 1) * sizeof(double)));
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.stage), (size_t)std::max<int64_t>(s->nnz, 1) * sizeof(double)));
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.err), sizeof(int)));
-        RET_IF(upload(s, &R.fbase, rf_fbase));
-        RET_IF(upload(s, &R.fcp, rf_fcp));
-        RET_IF(upload(s, &R.fri, rf_fri));
-        RET_IF(upload(s, &R.fdg, rf_fdg));
-        RET_IF(upload(s, &R.fllt, rf_fllt));
-        RET_IF(upload(s, &R.frp, rf_frp));
-        RET_IF(upload(s, &R.frpos, rf_frpos));
-        RET_IF(upload(s, &R.frk, rf_frk));
-        RET_IF(upload(s, &R.lv_first, rf_lvfirst));
-        RET_IF(upload(s, &R.lv_off, rf_lvoff));
-        RET_IF(upload(s, &R.lv_col, rf_lvcol));
-        RET_IF(upload(s, &R.tc_sub, rf_tcsub));
-        RET_IF(upload(s, &R.tc_col, rf_tccol));
-        RET_IF(upload(s, &R.fill_src, rf_fill_src));
-        RET_IF(upload(s, &R.fill_dst, rf_fill_dst));
-        RET_IF(upload(s, &R.lts_src, rf_lts));
-        RET_IF(upload(s, &R.ust_src, rf_ust));
-        for (int f = 0; f < 2; ++f) {
-            R.nblk[f] = (int64_t)rf_beoff[f].size() - 1;
-            RET_IF(upload(s, &R.sw_src[f], rf_swsrc[f]));
-            RET_IF(upload(s, &R.sw_dsrc[f], rf_swdsrc[f]));
-            RET_IF(upload(s, &R.wsrc[f], rf_wsrc[f]));
-            RET_IF(upload(s, &R.be_off[f], rf_beoff[f]));
-            RET_IF(upload(s, &R.be_pos[f], rf_bepos[f]));
-            RET_IF(upload(s, &R.be_row[f], rf_berow[f]));
-            RET_IF(upload(s, &R.be_cp[f], rf_becp[f]));
-            RET_IF(upload(s, &R.bc_b[f], rf_bcb[f]));
-            RET_IF(upload(s, &R.bc_pos[f], rf_bcpos[f]));
-        }
-        CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
-        R.bytes = s->bytes - before;
-        R.on = true;
-    }
     // input gather and owned output of one local solve (per right-hand side)
     double vec = 0.0;
     for (int i = 0; i < nsub; ++i) {
@@ -2440,6 +2418,99 @@ int s2l_gpu_setup_end(s2l_setup* s)
         RET_IF(upload(s, &s->d_Einv, Einv));
     }
     RET_IF(upload(s, &s->d_subs, s->h_subs));
+    // refactorization plan and work buffers (after the coarse tiles: the refresh of E uses them)
+    if (rfon) {
+        auto& R = s->rf;
+        const size_t before = s->bytes;
+        rf_fcp.push_back(rf_fbase.back());
+        rf_lvfirst.push_back((int32_t)(rf_lvoff.size() - 1));
+        R.nF = rf_fbase.back();
+        R.nfill = (int64_t)rf_fill_src.size();
+        R.ntc = (int64_t)rf_tcsub.size();
+        R.nlts = (int64_t)rf_lts.size();
+        R.nust = (int64_t)rf_ust.size();
+        R.d_off = d_off;
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.F), (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.S), (size_t)std::max<int64_t>(d_off[nsub], 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.stage), (size_t)std::max<int64_t>(s->nnz, 1) * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.err), sizeof(int)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.part), (size_t)nsub * 32 * R.maxcol * sizeof(double)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.info), (size_t)nsub * sizeof(int)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.rowsum), (size_t)s->n * sizeof(double)));
+        {
+            auto dbl = [&](double** p, size_t count) {
+                return dev_alloc(s, reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(double));
+            };
+            const int64_t n0 = std::max<int64_t>(s->n0, 1);
+            RET_IF(dbl(&R.E, (size_t)n0 * n0));
+            RET_IF(dbl(&R.colbuf, (size_t)n0));
+            RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.piv), (size_t)n0 * sizeof(int)));
+            RET_IF(dbl(&R.Y, (size_t)n0 * 16));
+            RET_IF(dbl(&R.X, (size_t)s->n * 16));
+            RET_IF(dbl(&R.AX, (size_t)s->n * 16));
+            RET_IF(dbl(&R.cpart, (size_t)std::max(s->ntiles, 1) * std::max(s->mmax, 1) * 16));
+            RET_IF(dbl(&R.C, (size_t)n0 * 16));
+            if (s->pou != S2L_POU_BOOLEAN) RET_IF(dbl(&R.plocal, (size_t)s->nloc * 16));
+            int smax = 1;
+            for (int sz : R.sz) smax = std::max(smax, sz);
+            constexpr int NS = s2l_setup::Refac::RF_STREAMS;
+            for (int q = 0; q < NS; ++q) {
+                CUDA_OK(s, cudaStreamCreateWithFlags(&R.tstream[q], cudaStreamNonBlocking));
+                if (cublasCreate(&R.tblas[q]) != CUBLAS_STATUS_SUCCESS) {
+                    R.tblas[q] = nullptr;
+                    return s->fail(S2L_ERR_CUDA, "cublasCreate failed");
+                }
+                if (cusolverDnCreate(&R.tsolver[q]) != CUSOLVER_STATUS_SUCCESS) {
+                    R.tsolver[q] = nullptr;
+                    return s->fail(S2L_ERR_CUDA, "cusolverDnCreate failed");
+                }
+                if (cublasSetStream(R.tblas[q], R.tstream[q]) != CUBLAS_STATUS_SUCCESS ||
+                    cusolverDnSetStream(R.tsolver[q], R.tstream[q]) != CUSOLVER_STATUS_SUCCESS)
+                    return s->fail(S2L_ERR_CUDA, "cannot bind the tail handles to their streams");
+                RET_IF(dbl(&R.B[q], (size_t)smax * smax));
+            }
+            for (auto& e : R.tev) CUDA_OK(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            int l1 = 0, l2 = 0;
+            if (cusolverDnDpotrf_bufferSize(R.tsolver[0], CUBLAS_FILL_MODE_UPPER, smax, R.B[0], smax, &l1) !=
+                    CUSOLVER_STATUS_SUCCESS ||
+                cusolverDnDgetrf_bufferSize(R.tsolver[0], smax, smax, R.B[0], smax, &l2) != CUSOLVER_STATUS_SUCCESS)
+                return s->fail(S2L_ERR_CUDA, "cuSOLVER workspace query failed");
+            R.lwork = std::max(std::max(l1, l2), 1);
+            for (int q = 0; q < NS; ++q) RET_IF(dbl(&R.swork[q], (size_t)R.lwork));
+        }
+        RET_IF(upload(s, &R.fbase, rf_fbase));
+        RET_IF(upload(s, &R.fcp, rf_fcp));
+        RET_IF(upload(s, &R.fri, rf_fri));
+        RET_IF(upload(s, &R.fdg, rf_fdg));
+        RET_IF(upload(s, &R.fllt, rf_fllt));
+        RET_IF(upload(s, &R.frp, rf_frp));
+        RET_IF(upload(s, &R.frpos, rf_frpos));
+        RET_IF(upload(s, &R.frk, rf_frk));
+        RET_IF(upload(s, &R.lv_first, rf_lvfirst));
+        RET_IF(upload(s, &R.lv_off, rf_lvoff));
+        RET_IF(upload(s, &R.lv_col, rf_lvcol));
+        RET_IF(upload(s, &R.tc_sub, rf_tcsub));
+        RET_IF(upload(s, &R.tc_col, rf_tccol));
+        RET_IF(upload(s, &R.fill_src, rf_fill_src));
+        RET_IF(upload(s, &R.fill_dst, rf_fill_dst));
+        RET_IF(upload(s, &R.lts_src, rf_lts));
+        RET_IF(upload(s, &R.ust_src, rf_ust));
+        for (int f = 0; f < 2; ++f) {
+            R.nblk[f] = (int64_t)rf_beoff[f].size() - 1;
+            RET_IF(upload(s, &R.sw_src[f], rf_swsrc[f]));
+            RET_IF(upload(s, &R.sw_dsrc[f], rf_swdsrc[f]));
+            RET_IF(upload(s, &R.wsrc[f], rf_wsrc[f]));
+            RET_IF(upload(s, &R.be_off[f], rf_beoff[f]));
+            RET_IF(upload(s, &R.be_pos[f], rf_bepos[f]));
+            RET_IF(upload(s, &R.be_row[f], rf_berow[f]));
+            RET_IF(upload(s, &R.be_cp[f], rf_becp[f]));
+            RET_IF(upload(s, &R.bc_b[f], rf_bcb[f]));
+            RET_IF(upload(s, &R.bc_pos[f], rf_bcpos[f]));
+        }
+        CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
+        R.bytes = s->bytes - before;
+        R.on = true;
+    }
 
     // sweep shared memory: x (T values) + one ready byte per row
     const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15);
@@ -2489,7 +2560,13 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
         s->ctx->used -= std::min(s->ctx->used, s->bytes);
     }
     if (s->setup_stream) cudaStreamDestroy(s->setup_stream);
-    if (s->rf.blas) cublasDestroy(s->rf.blas);
+    for (int q = 0; q < s2l_setup::Refac::RF_STREAMS; ++q) {
+        if (s->rf.tblas[q]) cublasDestroy(s->rf.tblas[q]);
+        if (s->rf.tsolver[q]) cusolverDnDestroy(s->rf.tsolver[q]);
+        if (s->rf.tstream[q]) cudaStreamDestroy(s->rf.tstream[q]);
+    }
+    for (auto e : s->rf.tev)
+        if (e) cudaEventDestroy(e);
     delete s;
     return S2L_OK;
 }
@@ -2530,72 +2607,74 @@ int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind)
 
 namespace {
 
-// Temporary device buffers of one call, charged to the context's HBM budget while they live.
-struct TempBufs {
-    s2l_setup* s;
-    std::vector<std::pair<void*, size_t>> held;
-    explicit TempBufs(s2l_setup* s_) : s(s_) {}
-    template <typename T>
-    int get(T** p, size_t count)
-    {
-        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-        {
-            std::lock_guard<std::mutex> g(s->ctx->mu);
-            if (s->ctx->budget && s->ctx->used + bytes > s->ctx->budget) {
-                s->ctx->err = "HBM budget exceeded by the refactorization's work buffers";
-                return S2L_ERR_OOM;
-            }
-            s->ctx->used += bytes;
-        }
-        if (cudaMalloc(reinterpret_cast<void**>(p), bytes) != cudaSuccess) {
-            std::lock_guard<std::mutex> g(s->ctx->mu);
-            s->ctx->used -= bytes;
-            return s->fail(S2L_ERR_OOM, "no device memory for the refactorization's work buffers");
-        }
-        held.emplace_back(*p, bytes);
-        return S2L_OK;
-    }
-    ~TempBufs()
-    {
-        for (auto& h : held) {
-            cudaFree(h.first);
-            std::lock_guard<std::mutex> g(s->ctx->mu);
-            s->ctx->used -= std::min(s->ctx->used, h.second);
-        }
-    }
-};
-
 // E = W^T A W for the matrix values v (device), 16 columns of W at a time: prolongation of unit
 // coarse vectors, product with A, restriction (the kernels of the coarse correction)
-int coarse_matrix_dev(s2l_setup* s, TempBufs& tb, cudaStream_t st, const double* v, double* E)
+int coarse_matrix_dev(s2l_setup* s, cudaStream_t st, const double* v, double* E)
 {
+    auto& R = s->rf;
     const int64_t n = s->n, n0 = s->n0;
     const int K = 16;
     const int boolean = s->pou == S2L_POU_BOOLEAN;
-    double *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr, *C = nullptr, *plocal = nullptr;
-    RET_IF(tb.get(&Y, (size_t)n0 * K));
-    RET_IF(tb.get(&X, (size_t)n * K));
-    RET_IF(tb.get(&AX, (size_t)n * K));
-    RET_IF(tb.get(&cpart, (size_t)s->ntiles * s->mmax * K));
-    RET_IF(tb.get(&C, (size_t)n0 * K));
-    if (!boolean) RET_IF(tb.get(&plocal, (size_t)s->nloc * K));
     for (int64_t c0 = 0; c0 < n0; c0 += K) {
-        launch_unit_block(st, n0, (int)c0, Y);
-        launch_coarse_prolong_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, Y,
-                                    X, plocal);
-        if (!boolean) launch_combine_block(st, n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, X);
-        launch_spmv_block(st, n, K, s->d_rp, s->d_ci, v, X, AX, nullptr, nullptr, nullptr, s->tpr);
+        launch_unit_block(st, n0, (int)c0, R.Y);
+        launch_coarse_prolong_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
+                                    R.Y, R.X, R.plocal);
+        if (!boolean) launch_combine_block(st, n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, R.plocal, nullptr, R.X);
+        launch_spmv_block(st, n, K, s->d_rp, s->d_ci, v, R.X, R.AX, nullptr, nullptr, nullptr, s->tpr);
         launch_coarse_restrict_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
-                                     boolean, AX, s->mmax, cpart);
-        launch_coarse_reduce_block(st, K, s->nsub, s->d_subs, s->d_t_first, s->mmax, cpart, C);
-        launch_scatter_columns(st, n0, (int)c0, C, E);
+                                     boolean, R.AX, s->mmax, R.cpart);
+        launch_coarse_reduce_block(st, K, s->nsub, s->d_subs, s->d_t_first, s->mmax, R.cpart, R.C);
+        launch_scatter_columns(st, n0, (int)c0, R.C, E);
     }
     CUDA_OK(s, cudaGetLastError());
     return S2L_OK;
 }
 
+// fork the tail streams after the work queued on st / join st after them
+int tails_fork(s2l_setup* s, cudaStream_t st)
+{
+    auto& R = s->rf;
+    constexpr int NS = s2l_setup::Refac::RF_STREAMS;
+    CUDA_OK(s, cudaEventRecord(R.tev[NS], st));
+    for (int q = 0; q < NS; ++q) CUDA_OK(s, cudaStreamWaitEvent(R.tstream[q], R.tev[NS], 0));
+    return S2L_OK;
+}
+
+int tails_join(s2l_setup* s, cudaStream_t st)
+{
+    auto& R = s->rf;
+    constexpr int NS = s2l_setup::Refac::RF_STREAMS;
+    for (int q = 0; q < NS; ++q) {
+        CUDA_OK(s, cudaEventRecord(R.tev[q], R.tstream[q]));
+        CUDA_OK(s, cudaStreamWaitEvent(st, R.tev[q], 0));
+    }
+    return S2L_OK;
+}
+
+// Dense tails in place (S_i, s x s row-major, i.e. S_i^T column-major), the subdomains spread over
+// the tail streams: L L^T by Cholesky (potrf, upper in column-major = the lower L row-major); LU by
+// an LU without pivoting (getrf with no pivot array) of S^T = L' U', which is S = (U'^T)(L'^T) with
+// a lower triangle U'^T and a unit upper L'^T.  A failed pivot leaves info_i > 0.
+int refactor_dense_tails(s2l_setup* s, cudaStream_t st)
+{
+    auto& R = s->rf;
+    constexpr int NS = s2l_setup::Refac::RF_STREAMS;
+    RET_IF(tails_fork(s, st));
+    for (int i = 0; i < s->nsub; ++i) {
+        const int sz = R.sz[i];
+        if (sz == 0) continue;
+        const int q = i % NS;
+        double* Si = R.S + R.d_off[i];
+        const cusolverStatus_t cs =
+            R.llt[i] ? cusolverDnDpotrf(R.tsolver[q], CUBLAS_FILL_MODE_UPPER, sz, Si, sz, R.swork[q], R.lwork, R.info + i)
+                     : cusolverDnDgetrf(R.tsolver[q], sz, sz, Si, sz, R.swork[q], nullptr, R.info + i);
+        if (cs != CUSOLVER_STATUS_SUCCESS) return s->fail(S2L_ERR_CUDA, "dense tail factorization failed to launch");
+    }
+    return tails_join(s, st);
+}
+
 template <typename Real>
-int refactor_commit_factors(s2l_setup* s, TempBufs& tb, cudaStream_t st)
+int refactor_commit_factors(s2l_setup* s, cudaStream_t st)
 {
     auto& R = s->rf;
     const int nsub = s->nsub;
@@ -2610,40 +2689,37 @@ int refactor_commit_factors(s2l_setup* s, TempBufs& tb, cudaStream_t st)
     }
     launch_gather_values<Real>(st, R.nlts, R.lts_src, R.F, (Real*)s->d_lts_val);
     launch_gather_values<Real>(st, R.nust, R.ust_src, R.F, (Real*)s->d_ust_val);
-    // dense tails: triangles of the factored Schur complements, inverted by triangular solves
-    int smax = 0;
-    for (int i = 0; i < nsub; ++i) smax = std::max(smax, R.sz[i]);
-    if (smax == 0) return S2L_OK;
-    double *Lt = nullptr, *Ut = nullptr, *B = nullptr;
-    RET_IF(tb.get(&Lt, (size_t)smax * smax));
-    RET_IF(tb.get(&Ut, (size_t)smax * smax));
-    RET_IF(tb.get(&B, (size_t)smax * smax));
-    if (!R.blas) {
-        if (cublasCreate(&R.blas) != CUBLAS_STATUS_SUCCESS) {
-            R.blas = nullptr;
-            return s->fail(S2L_ERR_CUDA, "cublasCreate failed");
-        }
-    }
-    if (cublasSetStream(R.blas, st) != CUBLAS_STATUS_SUCCESS) return s->fail(S2L_ERR_CUDA, "cublasSetStream failed");
+    // dense tail inverses: triangular solves against the identity with the factored tails, the
+    // subdomains spread over the tail streams.  Row-major lower Lt = column-major upper (the
+    // Cholesky factor, or U'), row-major upper Ut = column-major lower (L', unit diagonal); for
+    // L L^T, Ut^-1 = (Lt^-1)^T.
+    constexpr int NS = s2l_setup::Refac::RF_STREAMS;
+    RET_IF(tails_fork(s, st));
     const double one = 1.0;
     for (int i = 0; i < nsub; ++i) {
         const int sz = R.sz[i];
         if (sz == 0) continue;
-        launch_tail_triangles(st, R.S + R.d_off[i], sz, R.llt[i], Lt, Ut);
+        const int q = i % NS;
+        cudaStream_t sq = R.tstream[q];
+        const double* Si = R.S + R.d_off[i];
         for (int f = 0; f < 2; ++f) {
-            launch_identity(st, B, sz);
-            // row-major lower Lt = column-major upper Lt^T (and row-major upper = column-major lower)
-            if (cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER,
-                            CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, sz, sz, &one, f == 0 ? Lt : Ut, sz, B, sz) !=
-                CUBLAS_STATUS_SUCCESS)
-                return s->fail(S2L_ERR_CUDA, "cublasDtrsm failed");
+            double* B = R.B[q];
             void* dst = f == 0 ? s->d_linv : s->d_uinv;
-            if (s->real == S2L_REAL_F32) launch_to_float(st, B, (float*)dst + R.d_off[i], (int64_t)sz * sz);
+            if (f == 1 && R.llt[i]) {
+                launch_transpose_to<Real>(sq, R.B[q], sz, (Real*)dst + R.d_off[i]);
+                continue;
+            }
+            launch_identity(sq, B, sz);
+            if (cublasDtrsm(R.tblas[q], CUBLAS_SIDE_LEFT, f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER,
+                            CUBLAS_OP_N, f == 0 ? CUBLAS_DIAG_NON_UNIT : CUBLAS_DIAG_UNIT, sz, sz, &one, Si, sz, B,
+                            sz) != CUBLAS_STATUS_SUCCESS)
+                return s->fail(S2L_ERR_CUDA, "cublasDtrsm failed");
+            if (s->real == S2L_REAL_F32) launch_to_float(sq, B, (float*)dst + R.d_off[i], (int64_t)sz * sz);
             else CUDA_OK(s, cudaMemcpyAsync((double*)dst + R.d_off[i], B, (size_t)sz * sz * sizeof(double),
-                                            cudaMemcpyDeviceToDevice, st));
+                                            cudaMemcpyDeviceToDevice, sq));
         }
     }
-    return S2L_OK;
+    return tails_join(s, st);
 }
 
 int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
@@ -2653,31 +2729,35 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     const int nsub = s->nsub;
     const int64_t n = s->n, nnz = s->nnz, n0 = s->n0;
     const auto t0 = std::chrono::steady_clock::now();
-    TempBufs tb(s);
+    // phase timers (events on the setup stream)
+    struct Evs {
+        cudaEvent_t e[6] = {};
+        ~Evs()
+        {
+            for (auto x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    for (auto& x : ev.e) CUDA_OK(s, cudaEventCreate(&x));
     CUDA_OK(s, cudaMemcpyAsync(R.stage, val, (size_t)nnz * sizeof(double),
                                ptr_kind == S2L_PTR_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
     CUDA_OK(s, cudaMemsetAsync(R.err, 0, sizeof(int), st));
+    CUDA_OK(s, cudaMemsetAsync(R.info, 0, (size_t)nsub * sizeof(int), st));
     // row sums of the new matrix: the OpenFOAM normalisation, and a finiteness check of every value
-    double* rowsum = nullptr;
-    RET_IF(tb.get(&rowsum, (size_t)n));
-    launch_row_sums(st, n, s->d_rp, R.stage, rowsum);
+    launch_row_sums(st, n, s->d_rp, R.stage, R.rowsum);
     {
         std::vector<double> h((size_t)n);
-        CUDA_OK(s, cudaMemcpyAsync(h.data(), rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(s, cudaMemcpyAsync(h.data(), R.rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(s, cudaStreamSynchronize(st));
         for (double v : h)
             if (!std::isfinite(v)) return s->fail(S2L_ERR_NUMERIC, "non-finite matrix value");
     }
     // coarse matrix with the kept basis, and its inverse
-    double *Enew = nullptr, *colbuf = nullptr;
-    int* piv = nullptr;
     const bool coarse = s->coarse != S2L_COARSE_NONE && n0 > 0;
+    CUDA_OK(s, cudaEventRecord(ev.e[0], st));
     if (coarse) {
-        RET_IF(tb.get(&Enew, (size_t)n0 * n0));
-        RET_IF(tb.get(&colbuf, (size_t)n0));
-        RET_IF(tb.get(&piv, (size_t)n0));
-        RET_IF(coarse_matrix_dev(s, tb, st, R.stage, Enew));
-        launch_gauss_jordan(st, (int)n0, Enew, colbuf, piv, R.err);
+        RET_IF(coarse_matrix_dev(s, st, R.stage, R.E));
+        launch_gauss_jordan(st, (int)n0, R.E, R.colbuf, R.piv, R.err);
     }
     // local factors on their kept patterns
     RefactorArgs a{};
@@ -2699,31 +2779,49 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     a.ntc = R.ntc;
     a.S = R.S;
     a.err = R.err;
+    a.smax = 1;
+    for (int sz : R.sz) a.smax = std::max(a.smax, sz);
+    a.maxcol = R.maxcol;
+    a.part = R.part;
     CUDA_OK(s, cudaMemsetAsync(R.F, 0, (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double), st));
     launch_refactor_fill(st, R.nfill, R.fill_src, R.fill_dst, R.stage, R.F);
+    CUDA_OK(s, cudaEventRecord(ev.e[1], st));
     launch_refactor_sparse(st, a, nsub);
+    CUDA_OK(s, cudaEventRecord(ev.e[2], st));
     launch_refactor_tail_columns(st, a);
+    CUDA_OK(s, cudaEventRecord(ev.e[3], st));
     CUDA_OK(s, cudaMemsetAsync(R.S, 0, (size_t)std::max<int64_t>(R.d_off[nsub], 1) * sizeof(double), st));
     launch_refactor_gather_tails(st, a);
-    launch_dense_lu(st, a, nsub);
+    RET_IF(refactor_dense_tails(s, st));
+    CUDA_OK(s, cudaEventRecord(ev.e[4], st));
     CUDA_OK(s, cudaGetLastError());
     int herr = 0;
+    std::vector<int> infos((size_t)nsub);
     CUDA_OK(s, cudaMemcpyAsync(&herr, R.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(s, cudaMemcpyAsync(infos.data(), R.info, (size_t)nsub * sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(s, cudaStreamSynchronize(st));
+    for (int i = 0; i < nsub && herr == 0; ++i)
+        if (infos[i] != 0) herr = 2;
     if (herr == 1) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a sparse column");
     if (herr == 2) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a dense tail");
     if (herr == 3) return s->fail(S2L_ERR_NUMERIC, "refactorization: the coarse matrix is singular");
     if (herr) return s->fail(S2L_ERR_NUMERIC, "refactorization failed");
     // commit: the matrix, its row sums, E^-1, then the solve layout of the new factors
     CUDA_OK(s, cudaMemcpyAsync(s->d_av, R.stage, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, R.rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (coarse)
-        CUDA_OK(s, cudaMemcpyAsync(s->d_Einv, Enew, (size_t)n0 * n0 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    if (s->real == S2L_REAL_F32) RET_IF(refactor_commit_factors<float>(s, tb, st));
-    else RET_IF(refactor_commit_factors<double>(s, tb, st));
+        CUDA_OK(s, cudaMemcpyAsync(s->d_Einv, R.E, (size_t)n0 * n0 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (s->real == S2L_REAL_F32) RET_IF(refactor_commit_factors<float>(s, st));
+    else RET_IF(refactor_commit_factors<double>(s, st));
     CUDA_OK(s, cudaGetLastError());
+    CUDA_OK(s, cudaEventRecord(ev.e[5], st));
     CUDA_OK(s, cudaStreamSynchronize(st));
     R.last_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (int q = 0; q < 5; ++q) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev.e[q], ev.e[q + 1]);
+        R.phase_ms[q] = ms;
+    }
     return S2L_OK;
 }
 
@@ -2811,6 +2909,11 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;
     else if (n == "refactor_bytes") *value = (double)s->rf.bytes;
     else if (n == "refactor_ms") *value = s->rf.last_ms;
+    else if (n == "refactor_ms_coarse") *value = s->rf.phase_ms[0];
+    else if (n == "refactor_ms_sparse") *value = s->rf.phase_ms[1];
+    else if (n == "refactor_ms_tail") *value = s->rf.phase_ms[2];
+    else if (n == "refactor_ms_dense") *value = s->rf.phase_ms[3];
+    else if (n == "refactor_ms_commit") *value = s->rf.phase_ms[4];
     else return S2L_ERR_BADARG;
     return S2L_OK;
 }

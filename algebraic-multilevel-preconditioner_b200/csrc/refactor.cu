@@ -15,11 +15,12 @@
 //     warp per column, its k in increasing order, the lanes over the rows of column k;
 //  3. tail columns j >= T: the same updates from the sparse columns only (k < T), one warp per
 //     column, all columns independent; the tail block of F then holds the Schur complement S;
-//  4. S gathered dense and factorized (LU without pivoting, one CTA per subdomain); the caller
-//     inverts its triangles for the solve's dense tails.
+//  4. S gathered dense (the caller factorizes it with cuSOLVER and inverts its triangles for the
+//     solve's dense tails).
 // Every column is reduced by one warp in a fixed order, so the result does not depend on timing.
 #include "s2l_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 namespace {
@@ -42,45 +43,146 @@ __device__ __forceinline__ void set_err(int* err, int code)
     atomicCAS(err, 0, code);
 }
 
-// Updates of local column j (global column gj = loc + j) by the finished columns k < klimit.
+// dest[off(row of s)] -= F[s] m for the positions s in [b, e), the warp's lanes over s, four
+// positions per lane in flight (sources and targets are different columns, targets distinct rows)
+template <typename Off>
+__device__ __forceinline__ void scatter_segment(const double* __restrict__ F, const int32_t* __restrict__ fri,
+                                                int64_t b, int64_t e, double m, double* dest, Off off, int lane)
+{
+    for (int64_t s = b + lane; s < e; s += 128) {
+        int i[4];
+        double v[4], t[4];
+        int64_t o[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t q = s + 32 * u;
+            ok[u] = q < e;
+            i[u] = ok[u] ? fri[q] : 0;
+            v[u] = ok[u] ? F[q] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) o[u] = ok[u] ? off(i[u]) : 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) t[u] = ok[u] ? dest[o[u]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (ok[u]) dest[o[u]] = t[u] - v[u] * m;
+    }
+}
+
+// Where a row lands in column j (offsets from the column's first position): rows >= T (the tail
+// rows, where the long coupling segments land) through the warp's map, filled here; rows < T by
+// binary search among the column's rows < T.
+struct ColumnView {
+    int64_t c0, c1, cT;
+    int T;
+    const int32_t* fri;
+    const uint16_t* map;
+    __device__ int64_t operator()(int i) const
+    {
+        return i >= T ? (int64_t)map[i - T] : find_row(fri, c0, cT, i) - c0;
+    }
+};
+
+__device__ ColumnView column_view(const RefactorArgs& a, int64_t gj, int T, uint16_t* map, int lane)
+{
+    ColumnView cv;
+    cv.c0 = a.fcp[gj];
+    cv.c1 = a.fcp[gj + 1];
+    cv.cT = T > 0 ? find_row(a.fri, cv.c0, cv.c1 + 1, T) : cv.c0;  // c1 when every row is < T
+    cv.T = T;
+    cv.fri = a.fri;
+    cv.map = map;
+    for (int64_t p = cv.cT + lane; p < cv.c1; p += 32) map[a.fri[p] - T] = (uint16_t)(p - cv.c0);
+    __syncwarp();
+    return cv;
+}
+
+// Updates of local column j (global column gj = loc + j) by the finished columns k < klimit, one warp.
 // LU: U(k, j) = x(k) in increasing k, x(rows > k of L(:, k)) -= L(:, k) U(k, j).
 // L L^T: x(rows >= j of L(:, k)) -= L(:, k) L(j, k) over the entries L(j, k) of row j.
-__device__ void update_column(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int klimit, int lane)
+__device__ void update_column(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int klimit, int T,
+                              uint16_t* map, int lane)
 {
     double* __restrict__ F = a.F;
-    const int64_t c0 = a.fcp[gj], c1 = a.fcp[gj + 1];
+    const ColumnView cv = column_view(a, gj, T, map, lane);
+    double* col = F + cv.c0;
     if (a.fllt[gj]) {
         const int64_t r1 = a.frp[gj + 1];
         for (int64_t t = a.frp[gj]; t < r1; ++t) {
             const int k = a.frk[t];
             if (k >= klimit) break;
             const int64_t p = fb + a.frpos[t];
-            const double ljk = F[p];
-            const int64_t e1 = a.fcp[loc + k + 1];
-            for (int64_t s = p + lane; s < e1; s += 32) {
-                const int i = a.fri[s];
-                const int64_t q = find_row(a.fri, c0, c1, i);
-                F[q] -= F[s] * ljk;
-            }
+            scatter_segment(F, a.fri, p, a.fcp[loc + k + 1], F[p], col, cv, lane);
             __syncwarp();
         }
     } else {
-        const int64_t u1 = c0 + a.fdg[gj];
-        for (int64_t t = c0; t < u1; ++t) {
+        const int64_t u1 = cv.c0 + a.fdg[gj];
+        for (int64_t t = cv.c0; t < u1; ++t) {
             const int k = a.fri[t];
             if (k >= klimit) break;
             const double u = F[t];  // final: every update from a smaller k is done
             const int64_t gk = loc + k;
-            const int64_t e1 = a.fcp[gk + 1];
-            if (u != 0.0)
-                for (int64_t s = a.fcp[gk] + a.fdg[gk] + 1 + lane; s < e1; s += 32) {
-                    const int i = a.fri[s];
-                    const int64_t q = find_row(a.fri, c0, c1, i);
-                    F[q] -= F[s] * u;
-                }
+            if (u != 0.0) scatter_segment(F, a.fri, a.fcp[gk] + a.fdg[gk] + 1, a.fcp[gk + 1], u, col, cv, lane);
             __syncwarp();
         }
     }
+}
+
+// The same for one column with every warp of the CTA.  The sum over k is split: for LU the part
+// of U(:, j) (rows < j, a sequential triangular solve) is done by warp 0 first; then the updates of
+// rows >= j, independent over k, go round-robin to the warps, each into its own partial column
+// (part), which are added in a fixed order at the end.  Every thread of the CTA calls this.
+__device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int j, int T,
+                                   uint16_t* map, double* part, int wid, int nw, int lane)
+{
+    double* __restrict__ F = a.F;
+    const ColumnView cv = column_view(a, gj, T, map, lane);
+    const int64_t len = cv.c1 - cv.c0;
+    double* mine = part + (size_t)wid * a.maxcol;
+    for (int64_t q = lane; q < len; q += 32) mine[q] = 0.0;
+    const bool llt = a.fllt[gj];
+    const int64_t u0 = cv.c0, u1 = cv.c0 + a.fdg[gj];
+    if (!llt && wid == 0) {
+        // U(:, j): the rows < j of the segments, in increasing k
+        for (int64_t t = u0; t < u1; ++t) {
+            const int k = a.fri[t];
+            const double u = F[t];
+            const int64_t gk = loc + k;
+            const int64_t b = a.fcp[gk] + a.fdg[gk] + 1, e = a.fcp[gk + 1];
+            const int64_t ej = find_row(a.fri, b, e + 1, j);  // first row >= j
+            if (u != 0.0) scatter_segment(F, a.fri, b, ej, u, F + cv.c0, cv, lane);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (llt) {
+        const int64_t r0 = a.frp[gj], r1 = a.frp[gj + 1];
+        for (int64_t t = r0 + wid; t < r1; t += nw) {
+            const int k = a.frk[t];
+            const int64_t p = fb + a.frpos[t];
+            scatter_segment(F, a.fri, p, a.fcp[loc + k + 1], F[p], mine, cv, lane);
+            __syncwarp();
+        }
+    } else {
+        for (int64_t t = u0 + wid; t < u1; t += nw) {
+            const int k = a.fri[t];
+            const double u = F[t];
+            const int64_t gk = loc + k;
+            const int64_t b = a.fcp[gk] + a.fdg[gk] + 1, e = a.fcp[gk + 1];
+            const int64_t ej = find_row(a.fri, b, e + 1, j);
+            if (u != 0.0) scatter_segment(F, a.fri, ej, e, u, mine, cv, lane);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int64_t q = threadIdx.x; q < len; q += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < nw; ++w) sum += part[(size_t)w * a.maxcol + q];
+        F[cv.c0 + q] += sum;
+    }
+    __syncthreads();
 }
 
 // pivot of column gj: LU divides the strict lower part by U(j, j); L L^T takes the square root of
@@ -122,16 +224,30 @@ __global__ void fill_kernel(int64_t count, const int64_t* __restrict__ src, cons
 // one CTA per subdomain: the sparse columns level by level
 __global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorArgs a)
 {
+    extern __shared__ uint16_t rmap[];
     const int sid = blockIdx.x;
     const int64_t loc = a.subs[sid].loc_off, fb = a.fbase[sid];
+    const int T = a.subs[sid].T;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    uint16_t* map = rmap + (size_t)wid * a.smax;
     __shared__ int stop;
+    double* part = a.part + (size_t)sid * nw * a.maxcol;
     for (int lv = a.lv_first[sid]; lv < a.lv_first[sid + 1]; ++lv) {
-        const int64_t e1 = a.lv_off[lv + 1];
-        for (int64_t c = a.lv_off[lv] + wid; c < e1; c += nw) {
-            const int j = a.lv_col[c];
-            update_column(a, loc, fb, loc + j, j, lane);
-            finish_column(a, loc + j, lane);
+        const int64_t e0 = a.lv_off[lv], e1 = a.lv_off[lv + 1];
+        if (e1 - e0 <= nw / 4) {
+            // few columns (the chains near the top of the sparse part): each with the whole CTA
+            for (int64_t c = e0; c < e1; ++c) {
+                const int j = a.lv_col[c];
+                update_column_coop(a, loc, fb, loc + j, j, T, map, part, wid, nw, lane);
+                if (wid == 0) finish_column(a, loc + j, lane);
+                __syncthreads();
+            }
+        } else {
+            for (int64_t c = e0 + wid; c < e1; c += nw) {
+                const int j = a.lv_col[c];
+                update_column(a, loc, fb, loc + j, j, T, map, lane);
+                finish_column(a, loc + j, lane);
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) stop = *(volatile int*)a.err;  // a failed pivot anywhere ends the walk
@@ -143,12 +259,14 @@ __global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorA
 // one warp per tail column: the updates from the sparse columns (k < T)
 __global__ void __launch_bounds__(256) tail_columns_kernel(const RefactorArgs a)
 {
+    extern __shared__ uint16_t rmap[];
     const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= a.ntc) return;
     const int sid = a.tc_sub[w];
     const DevSub& d = a.subs[sid];
-    update_column(a, d.loc_off, a.fbase[sid], d.loc_off + a.tc_col[w], d.T, lane);
+    update_column(a, d.loc_off, a.fbase[sid], d.loc_off + a.tc_col[w], d.T, d.T,
+                  rmap + (size_t)(threadIdx.x >> 5) * a.smax, lane);
 }
 
 // one warp per tail column: its rows >= T into the dense tail (mirrored for L L^T)
@@ -173,110 +291,20 @@ __global__ void __launch_bounds__(256) gather_tails_kernel(const RefactorArgs a)
     }
 }
 
-// Dense LU without pivoting of one s x s row-major matrix per CTA (the row order of the setup's
-// factor is kept), blocked by NB columns: panel factorization, then the trailing update with the
-// panel's U rows staged in shared memory chunk by chunk.
-constexpr int LU_NB = 16;
-constexpr int LU_CHUNK = 256;  // trailing columns per staged chunk (32 KB of shared memory)
-
-__global__ void __launch_bounds__(512, 1) dense_lu_kernel(const RefactorArgs a)
+// dst (Real) = src^T, s x s
+template <typename Real>
+__global__ void transpose_to_kernel(const double* __restrict__ src, int s, Real* __restrict__ dst)
 {
-    __shared__ double us[LU_NB * LU_CHUNK];
-    __shared__ int bad;
-    const DevSub& d = a.subs[blockIdx.x];
-    const int n = d.n_local - d.T;
-    if (n <= 0) return;
-    double* __restrict__ S = a.S + d.d_off;
-    const bool llt = a.fllt[d.loc_off + d.T];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0) bad = 0;
-    __syncthreads();
-    for (int k0 = 0; k0 < n; k0 += LU_NB) {
-        const int kb = min(LU_NB, n - k0), ke = k0 + kb;
-        // panel: columns [k0, ke) for every row below, and the U rows [k0, ke) to the right
-        for (int k = k0; k < ke; ++k) {
-            const double piv = S[(int64_t)k * n + k];
-            if (piv == 0.0 || !isfinite(piv) || (llt && !(piv > 0.0))) {
-                if (tid == 0) {
-                    bad = 1;
-                    set_err(a.err, 2);
-                }
-            }
-            __syncthreads();
-            if (bad) return;
-            const double pinv = 1.0 / piv;
-            // rows below k: the multiplier, and the update of the remaining panel columns
-            const int w = ke - k - 1;  // panel columns right of k
-            for (int i = k + 1 + tid; i < n; i += nt) {
-                double* Si = S + (int64_t)i * n;
-                const double l = Si[k] * pinv;
-                Si[k] = l;
-                for (int j = 1; j <= w; ++j) Si[k + j] -= l * S[(int64_t)k * n + k + j];
-            }
-            __syncthreads();
-            // the panel's own rows (k, ke): their entries right of the panel
-            const int rows = ke - k - 1, cols = n - ke;
-            for (int64_t e = tid; e < (int64_t)rows * cols; e += nt) {
-                const int i = k + 1 + (int)(e / cols), j = ke + (int)(e % cols);
-                S[(int64_t)i * n + j] -= S[(int64_t)i * n + k] * S[(int64_t)k * n + j];
-            }
-            __syncthreads();
-        }
-        // trailing update: S(ke:, ke:) -= L(ke:, k0:ke) U(k0:ke, ke:)
-        for (int j0 = ke; j0 < n; j0 += LU_CHUNK) {
-            const int cw = min(LU_CHUNK, n - j0);
-            for (int e = tid; e < LU_NB * cw; e += nt) {
-                const int kk = e / cw, jj = e % cw;
-                us[kk * LU_CHUNK + jj] = kk < kb ? S[(int64_t)(k0 + kk) * n + j0 + jj] : 0.0;
-            }
-            __syncthreads();
-            // thread: 4 consecutive columns of one row; rows strided by the thread groups
-            const int groups_per_row = (cw + 3) >> 2;
-            const int rows_per_pass = max(1, nt / groups_per_row);
-            const int g = tid % groups_per_row, r0 = tid / groups_per_row;
-            if (r0 < rows_per_pass) {
-                const int jj0 = g * 4;
-                for (int i = ke + r0; i < n; i += rows_per_pass) {
-                    double* Si = S + (int64_t)i * n;
-                    double l[LU_NB];
-#pragma unroll
-                    for (int kk = 0; kk < LU_NB; ++kk) l[kk] = kk < kb ? Si[k0 + kk] : 0.0;
-                    double acc[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[q] = jj0 + q < cw ? Si[j0 + jj0 + q] : 0.0;
-#pragma unroll
-                    for (int kk = 0; kk < LU_NB; ++kk)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc[q] -= l[kk] * us[kk * LU_CHUNK + min(jj0 + q, LU_CHUNK - 1)];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (jj0 + q < cw) Si[j0 + jj0 + q] = acc[q];
-                }
-            }
-            __syncthreads();
-        }
+    __shared__ double t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = by + y, c = bx + threadIdx.x;
+        if (r < s && c < s) t[y][threadIdx.x] = src[(int64_t)r * s + c];
     }
-}
-
-// Lt / Ut row-major from the LU of a tail: LU: Lt unit lower, Ut upper.  L L^T (LU of a symmetric
-// S = L D L^T): Lt = L D^1/2, Ut = Lt^T.
-__global__ void tail_triangles_kernel(const double* __restrict__ S, int s, int llt, double* __restrict__ Lt,
-                                      double* __restrict__ Ut)
-{
-    const int64_t total = (int64_t)s * s;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(e / s), c = (int)(e % s);
-        double lv = 0.0, uv = 0.0;
-        if (llt) {
-            if (r >= c) lv = (r == c ? 1.0 : S[e]) * sqrt(S[(int64_t)c * s + c]);
-            if (r <= c) uv = (r == c ? 1.0 : S[(int64_t)c * s + r]) * sqrt(S[(int64_t)r * s + r]);
-        } else {
-            if (r > c) lv = S[e];
-            else if (r == c) lv = 1.0;
-            if (r <= c) uv = S[e];
-        }
-        Lt[e] = lv;
-        Ut[e] = uv;
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = bx + y, c = by + threadIdx.x;
+        if (r < s && c < s) dst[(int64_t)r * s + c] = (Real)t[threadIdx.x][y];
     }
 }
 
@@ -532,14 +560,35 @@ void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, co
     if (count > 0) fill_kernel<<<grid_for(count, 256), 256, 0, st>>>(count, src, dst, val, F);
 }
 
+size_t refactor_map_bytes(int smax, int warps)
+{
+    return (size_t)std::max(smax, 1) * sizeof(uint16_t) * warps;
+}
+
+// warps of a sparse-columns CTA: as many as 32 whose row maps fit the shared memory
+static int sparse_warps(int smax)
+{
+    const size_t cap = 220 * 1024;
+    int w = 32;
+    while (w > 1 && refactor_map_bytes(smax, w) > cap) --w;
+    return w;
+}
+
 void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub)
 {
-    sparse_columns_kernel<<<nsub, 1024, 0, st>>>(a);
+    const int w = sparse_warps(a.smax);
+    const size_t smem = refactor_map_bytes(a.smax, w);
+    cudaFuncSetAttribute(sparse_columns_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    sparse_columns_kernel<<<nsub, 32 * w, smem, st>>>(a);
 }
 
 void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a)
 {
-    if (a.ntc > 0) tail_columns_kernel<<<(int)((a.ntc * 32 + 255) / 256), 256, 0, st>>>(a);
+    if (a.ntc <= 0) return;
+    const int w = std::min(8, sparse_warps(a.smax));
+    const size_t smem = refactor_map_bytes(a.smax, w);
+    cudaFuncSetAttribute(tail_columns_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    tail_columns_kernel<<<(int)((a.ntc + w - 1) / w), 32 * w, smem, st>>>(a);
 }
 
 void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a)
@@ -547,14 +596,11 @@ void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a)
     if (a.ntc > 0) gather_tails_kernel<<<(int)((a.ntc * 32 + 255) / 256), 256, 0, st>>>(a);
 }
 
-void launch_dense_lu(cudaStream_t st, const RefactorArgs& a, int nsub)
+template <typename Real>
+void launch_transpose_to(cudaStream_t st, const double* src, int s, Real* dst)
 {
-    dense_lu_kernel<<<nsub, 512, 0, st>>>(a);
-}
-
-void launch_tail_triangles(cudaStream_t st, const double* S, int s, int llt, double* Lt, double* Ut)
-{
-    tail_triangles_kernel<<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(S, s, llt, Lt, Ut);
+    const dim3 g((s + 31) / 32, (s + 31) / 32);
+    transpose_to_kernel<Real><<<g, dim3(32, 8), 0, st>>>(src, s, dst);
 }
 
 void launch_identity(cudaStream_t st, double* M, int s)
@@ -639,6 +685,8 @@ template void launch_refactor_blocks<double>(cudaStream_t, int64_t, const int64_
 template void launch_refactor_blocks<float>(cudaStream_t, int64_t, const int64_t*, const int64_t*, const int64_t*,
                                             const int64_t*, const int64_t*, const uint8_t*, const int64_t*,
                                             const uint8_t*, const int64_t*, const double*, float*, float*);
+template void launch_transpose_to<double>(cudaStream_t, const double*, int, double*);
+template void launch_transpose_to<float>(cudaStream_t, const double*, int, float*);
 template void launch_gather_values<double>(cudaStream_t, int64_t, const int64_t*, const double*, double*);
 template void launch_gather_values<float>(cudaStream_t, int64_t, const int64_t*, const double*, float*);
 

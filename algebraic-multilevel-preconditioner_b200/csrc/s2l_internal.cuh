@@ -137,8 +137,12 @@ struct RefactorArgs {
     const int32_t* tc_col;
     int64_t ntc;
     double* S;                 // dense tails (s x s row-major at subs[i].d_off)
+    int smax;                  // largest tail: the per-warp row maps hold smax uint16 positions
+    int maxcol;                // longest column of F
+    double* part;              // partial columns of the cooperative column updates: per subdomain
+                               // and warp, maxcol doubles
     int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column,
-                               // 2 of a dense tail, 3 singular coarse matrix (0: none)
+                               // 3 singular coarse matrix (0: none)
 };
 
 // launch wrappers (kernels.cu)
@@ -217,13 +221,12 @@ void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, const int64_t* dst, const double* val,
                           double* F);
 void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub);
+size_t refactor_map_bytes(int smax, int warps);
 void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a);
 void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a);
-void launch_dense_lu(cudaStream_t st, const RefactorArgs& a, int nsub);
-// row-major triangles of subdomain i's factored tail for the inversion: Lt (lower, unit for LU,
-// L of L L^T) and Ut (upper: U, or L^T)
-void launch_tail_triangles(cudaStream_t st, const double* S, int s, int llt, double* Lt, double* Ut);
 void launch_identity(cudaStream_t st, double* M, int s);
+template <typename Real>
+void launch_transpose_to(cudaStream_t st, const double* src, int s, Real* dst);
 template <typename Real>
 void launch_refactor_sweep_values(cudaStream_t st, int nsub, const int64_t* fbase, const double* F,
                                   const int64_t* wtask, const int64_t* wslot, const int64_t* went,

@@ -186,9 +186,10 @@ int coarse_code(const core::SolverConfig& c)
 // ------------------------------------------------------------------------- GpuSolvePhase
 GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchwarz& one,
                              const prec::TwoLevelSchwarz* two, const core::SolverConfig& cfg, int device,
-                             size_t hbm_budget)
-    : comm_(sd.comm())
+                             size_t hbm_budget, bool refactorize)
+    : comm_(sd.comm()), sd_(&sd)
 {
+    op_version_ = prec_version_ = sd.valuesVersion();
     rank_ = core::mpiRank(comm_);
     np_ = core::mpiSize(comm_);
     const core::LocalSystem& sys = sd.system();
@@ -264,6 +265,8 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
             const auto col = rd.get<int64_t>();
             const auto val = rd.get<double>();
             for (int r = 0; r < nI; ++r) grp.push_back(grp.back() + (rp[r + 1] - rp[r]));
+            nnz_displs_.push_back((int)gval.size());
+            nnz_counts_.push_back((int)val.size());
             gcol.insert(gcol.end(), col.begin(), col.end());
             gval.insert(gval.end(), val.begin(), val.end());
             const auto ghosts = rd.get<int64_t>();
@@ -329,6 +332,7 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
             Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor> Er = E;
             status = s2l_gpu_set_coarse(setup_, n0, offsets.data(), Er.data());
         }
+        if (status == S2L_OK && refactorize) status = s2l_gpu_setup_option(setup_, "refactor", 1.0);
         if (status == S2L_OK) status = s2l_gpu_setup_end(setup_);
         if (status != S2L_OK) msg = ctx_ ? s2l_gpu_last_error(ctx_) : "no CUDA device";
     }
@@ -367,7 +371,43 @@ void GpuSolvePhase::scatter(const std::vector<double>& global, core::Vec& owned)
                  counts_[rank_], MPI_DOUBLE, 0, comm_);
 }
 
+bool GpuSolvePhase::operatorCurrent() const { return op_version_ == sd_->valuesVersion(); }
+
+bool GpuSolvePhase::preconditionerCurrent() const { return prec_version_ == sd_->valuesVersion(); }
+
+void GpuSolvePhase::pushValues(prec::UpdateLevel level)
+{
+    const std::vector<core::Scalar>& v = sd_->system().val;
+    std::vector<double> all;
+    if (rank_ == 0) all.resize(nnz_counts_.empty() ? 0 : (size_t)nnz_displs_.back() + nnz_counts_.back());
+    MPI_Gatherv(v.data(), (int)v.size(), MPI_DOUBLE, rank_ == 0 ? all.data() : nullptr,
+                rank_ == 0 ? nnz_counts_.data() : nullptr, rank_ == 0 ? nnz_displs_.data() : nullptr, MPI_DOUBLE, 0,
+                comm_);
+    const bool refac = level == prec::UpdateLevel::Refactorize;
+    int st = S2L_OK;
+    if (rank_ == 0)
+        st = refac ? s2l_gpu_refactor(setup_, all.data(), S2L_PTR_HOST)
+                   : s2l_gpu_update_matrix(setup_, all.data(), S2L_PTR_HOST);
+    check(st, refac ? "GPU refactorization" : "GPU matrix update");
+    op_version_ = sd_->valuesVersion();
+    if (refac) prec_version_ = op_version_;
+}
+
 // ------------------------------------------------------------------------- GpuTwoLevelSchwarz
+prec::UpdateLevel GpuTwoLevelSchwarz::update(prec::UpdateLevel requested)
+{
+    requested = prec::agree(requested, phase_->comm());
+    if (requested == prec::UpdateLevel::Rebuild)
+        throw std::logic_error("GpuTwoLevelSchwarz: Rebuild recomputes the coarse basis on the host; build a new "
+                               "GpuSolvePhase from the rebuilt reference preconditioner");
+    if (requested == prec::UpdateLevel::Refactorize && !phase_->preconditionerCurrent()) {
+        phase_->pushValues(prec::UpdateLevel::Refactorize);
+        return prec::UpdateLevel::Refactorize;
+    }
+    if (!phase_->operatorCurrent()) phase_->pushValues(prec::UpdateLevel::Reuse);
+    return prec::UpdateLevel::Reuse;
+}
+
 void GpuTwoLevelSchwarz::apply(const core::Vec& r, core::Vec& z) const
 {
     std::vector<double> rg, zg;

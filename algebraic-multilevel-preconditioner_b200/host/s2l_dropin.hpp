@@ -46,10 +46,12 @@ public:
      * @param cfg    Configuration (variants, precision).
      * @param device CUDA device of rank 0.
      * @param hbm_budget Device bytes the setup may use (0 = no limit).
+     * @param refactorize Keep the factor patterns on the device so that update(Refactorize) can
+     *                    refactorize there (setup option "refactor").
      */
     GpuSolvePhase(const schwarz2lvl::part::Subdomain& sd, const schwarz2lvl::prec::OneLevelSchwarz& one,
                   const schwarz2lvl::prec::TwoLevelSchwarz* two, const schwarz2lvl::core::SolverConfig& cfg,
-                  int device = 0, size_t hbm_budget = 0);
+                  int device = 0, size_t hbm_budget = 0, bool refactorize = false);
     ~GpuSolvePhase();
     GpuSolvePhase(const GpuSolvePhase&) = delete;
     GpuSolvePhase& operator=(const GpuSolvePhase&) = delete;
@@ -64,6 +66,15 @@ public:
     s2l_setup* setup() const { return setup_; }
     /// @brief Throws the exception type of a failed status (rank 0), agreed on by every rank.
     void check(int status, const char* what) const;
+    /// @brief The matrix values of every rank's rows (Subdomain::system(), after
+    ///        Subdomain::updateValues) to the device (collective): Reuse gives the operator its new
+    ///        values and keeps the preconditioner (s2l_gpu_update_matrix); Refactorize also
+    ///        refactorizes the local factors and refreshes E on the device (s2l_gpu_refactor).
+    void pushValues(schwarz2lvl::prec::UpdateLevel level);
+    /// @brief The device operator holds the subdomain's current values.
+    bool operatorCurrent() const;
+    /// @brief The device preconditioner was built (or refactorized) from the current values.
+    bool preconditionerCurrent() const;
 
 private:
     MPI_Comm comm_;
@@ -72,6 +83,9 @@ private:
     std::vector<int> counts_, displs_;
     s2l_ctx* ctx_ = nullptr;
     s2l_setup* setup_ = nullptr;
+    const schwarz2lvl::part::Subdomain* sd_ = nullptr;
+    std::vector<int> nnz_counts_, nnz_displs_;  // matrix values per rank (rank 0)
+    long op_version_ = 0, prec_version_ = 0;     // Subdomain::valuesVersion() of the device copies
 };
 
 /// @brief z = M^{-1} r on the GPU: the two-level (or one-level) Schwarz apply of the reference.
@@ -80,6 +94,13 @@ public:
     GpuTwoLevelSchwarz(std::shared_ptr<GpuSolvePhase> phase, std::string name)
         : phase_(std::move(phase)), name_(std::move(name)) {}
     void apply(const schwarz2lvl::core::Vec& r, schwarz2lvl::core::Vec& z) const override;
+    /// @brief The reference's update contract (include/preconditioner/preconditioner.hpp:64-96,
+    ///        src/preconditioner/two_level_schwarz.cpp:30-41), collective: Reuse keeps the
+    ///        preconditioner (the device operator takes the new values), Refactorize refactorizes on
+    ///        the device (returns Reuse when already up to date); Rebuild recomputes the coarse basis
+    ///        on the host and needs a new GpuSolvePhase (std::logic_error).
+    schwarz2lvl::prec::UpdateLevel update(schwarz2lvl::prec::UpdateLevel requested) override;
+    bool upToDate() const override { return phase_->preconditionerCurrent(); }
     std::string name() const override { return name_ + " (B200)"; }
     const std::shared_ptr<GpuSolvePhase>& phase() const { return phase_; }
 

@@ -2,7 +2,8 @@
 
 Requests name a matrix by key.  The engine keeps one device setup per key (least recently used
 first out), reuses it for every request on that matrix and along a sequence of values of it
-(``update``: the reference's UpdateLevel::Reuse, preconditioner kept), and runs the solves on the
+(``update``: the reference's UpdateLevel::Reuse, preconditioner kept, or Refactorize on the
+device), and runs the solves on the
 native worker threads of the context (``s2l_gpu_serve_start``), so requests that arrive while
 others are on the GPU overlap with them.  Memory is admitted by the context's HBM budget: a
 solve whose buffers do not fit waits in the library for a workspace of its setup to come free,
@@ -62,11 +63,18 @@ class Engine:
                     return True
         return False
 
-    def update(self, key, values) -> None:
-        """Next matrix of a sequence on `key`: new values of A, same pattern, preconditioner kept."""
+    def update(self, key, values, level: str = "reuse") -> None:
+        """Next matrix of a sequence on `key` (new values of A, same pattern).  level "reuse" keeps
+        the preconditioner (UpdateLevel::Reuse); "refactorize" refactorizes it on the device
+        (UpdateLevel::Refactorize; the setup must have been made with options {"refactor": 1})."""
         with self._lock:
             g = self._cache[key]
-        g.update_matrix(values)
+        if level == "reuse":
+            g.update_matrix(values)
+        elif level == "refactorize":
+            g.refactor(values)
+        else:
+            raise ValueError(f"unknown update level {level!r}")
 
     def submit(self, key, make, b, x0=None, method="gmres", options=None, **kw) -> capi.Ticket:
         """Queue one solve of matrix `key` and return its ticket at once."""

@@ -440,18 +440,28 @@ def run_ours(a):
             b_i = rng.uniform(-1.0, 1.0, mk().n)
             tickets.append((key, eng.submit(key, mk, b_i, history_cap=0, **kwk)))
         lat = []
+        per_key = {k: {"lat": [], "run": [], "its": []} for k in keys}
         ok = True
         for key, t in tickets:
             _, r, status = t.wait(600.0)
             ok = ok and status == 0 and r["converged"]
             info = t.info()
             lat.append(info["queue_ms"] + info["run_ms"])
+            per_key[key]["lat"].append(info["queue_ms"] + info["run_ms"])
+            per_key[key]["run"].append(info["run_ms"])
+            per_key[key]["its"].append(r["iterations"])
             t.free()
         t_end = time.perf_counter()
         serving = {"requests": a.serve, "rate_req_s": a.serve_rate, "mix": dict(zip(keys, mix)),
                    "all_converged": ok, "solves_per_s": a.serve / (t_end - t0),
                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                    "max_ms": float(np.max(lat)), "workers": 4, "setups_built": eng.builds,
+                   "per_case": {k: {"requests": len(v["lat"]),
+                                    "p50_ms": float(np.percentile(v["lat"], 50)) if v["lat"] else None,
+                                    "p99_ms": float(np.percentile(v["lat"], 99)) if v["lat"] else None,
+                                    "run_ms_mean": float(np.mean(v["run"])) if v["run"] else None,
+                                    "iterations_mean": float(np.mean(v["its"])) if v["its"] else None}
+                                for k, v in per_key.items()},
                    "clock": "host (submit to solution ready)"}
         eng.close()
 
@@ -509,6 +519,8 @@ def run_ours(a):
             Bh = Bq.cpu().numpy()
             chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(kh))
             steps_q.append({"step": step, "refactor_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
+                            "refactor_phases_ms": {k: round(g.stat("refactor_ms_" + k), 2)
+                                                   for k in ("coarse", "sparse", "tail", "dense", "commit")},
                             "iterations_max": max(r["iterations"] for r in rq),
                             "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
         g.refactor(st32.A.data)  # back to the setup's own matrix

@@ -4,14 +4,18 @@
 // With the reference's flags it builds, on S2L_NP thread-ranks, the reference's own
 // preconditioner and Krylov solver and the drop-in GpuTwoLevelSchwarz / GpuKrylov from the same
 // set-up objects, then compares: Preconditioner::apply of seeded vectors (relative difference), and
-// KrylovSolver::solve (iterations, convergence, true residual, solution).  Rank 0 prints one JSON
-// line; the exit code is 0 when every comparison is within tolerance.
+// KrylovSolver::solve (iterations, convergence, true residual, solution).  With S2L_DROPIN_UPDATE
+// set to "reuse" or "refactorize" it then gives the matrix new values (D A D, same pattern,
+// Subdomain::updateValues), calls update() with that level on both preconditioners and compares
+// again.  Rank 0 prints one JSON line; the exit code is 0 when every comparison is within tolerance.
 #include "s2l_dropin.hpp"
 
 #include "domain_decomposer.hpp"
 #include "mpi_utils.hpp"
 
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <iomanip>
 #include <iostream>
 #include <random>
@@ -29,6 +33,8 @@ int main(int argc, char** argv)
         const core::SolverConfig cfg = core::SolverConfig::fromCommandLine(argc, argv);
         part::DecompositionInfo info;
         core::LocalSystem sys = part::DomainDecomposer::decompose(cfg, comm, info);
+        const char* upd = std::getenv("S2L_DROPIN_UPDATE");
+        const std::string update_level = upd ? upd : "";
         part::Subdomain sd(sys, cfg.pou);
         linalg::DistributedMatrix A(sd);
         std::unique_ptr<prec::Preconditioner> M;
@@ -46,24 +52,46 @@ int main(int argc, char** argv)
             one = &p->oneLevel();
             M = std::move(p);
         }
-        auto phase = std::make_shared<s2l::dropin::GpuSolvePhase>(sd, *one, two, cfg, 0, 0);
+        auto phase = std::make_shared<s2l::dropin::GpuSolvePhase>(sd, *one, two, cfg, 0, 0,
+                                                                  update_level == "refactorize");
         s2l::dropin::GpuTwoLevelSchwarz G(phase, M->name());
         // apply parity on seeded vectors (U[-1,1], owned part of a global renumbered vector)
-        double worst = 0.0;
-        for (int k = 0; k < 3; ++k) {
-            std::mt19937_64 g(4242 + k);
-            std::uniform_real_distribution<double> u(-1.0, 1.0);
-            std::vector<double> rg((size_t)sys.n_global);
-            for (auto& v : rg) v = u(g);
-            core::Vec r(sys.nOwned()), z1, z2;
-            for (int i = 0; i < sys.nOwned(); ++i) r[i] = rg[(size_t)(sys.rowBegin() + i)];
-            M->apply(r, z1);
-            G.apply(r, z2);
-            double num = (z1 - z2).squaredNorm(), den = z1.squaredNorm();
-            double gn = 0.0, gd = 0.0;
-            MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
-            MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
-            worst = std::max(worst, std::sqrt(gn / gd));
+        auto apply_diff = [&]() {
+            double worst = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                std::mt19937_64 g(4242 + k);
+                std::uniform_real_distribution<double> u(-1.0, 1.0);
+                std::vector<double> rg((size_t)sys.n_global);
+                for (auto& v : rg) v = u(g);
+                core::Vec r(sys.nOwned()), z1, z2;
+                for (int i = 0; i < sys.nOwned(); ++i) r[i] = rg[(size_t)(sys.rowBegin() + i)];
+                M->apply(r, z1);
+                G.apply(r, z2);
+                double num = (z1 - z2).squaredNorm(), den = z1.squaredNorm();
+                double gn = 0.0, gd = 0.0;
+                MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
+                MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
+                worst = std::max(worst, std::sqrt(gn / gd));
+            }
+            return worst;
+        };
+        double worst = apply_diff();
+        std::string level_out;
+        if (!update_level.empty()) {
+            // new values D A D with d(g) = 1 + 0.1 sin(1 + 0.37 g) (same pattern, symmetric kept)
+            auto d = [](int64_t g) { return 1.0 + 0.1 * std::sin(1.0 + 0.37 * (double)g); };
+            for (int i = 0; i < sys.nOwned(); ++i)
+                for (int64_t e = sys.row_ptr[i]; e < sys.row_ptr[i + 1]; ++e)
+                    sys.val[e] *= d(sys.rowBegin() + i) * d(sys.col[e]);
+            sd.updateValues();
+            const prec::UpdateLevel want =
+                update_level == "refactorize" ? prec::UpdateLevel::Refactorize : prec::UpdateLevel::Reuse;
+            const prec::UpdateLevel l1 = M->update(want);
+            const prec::UpdateLevel l2 = G.update(want);
+            if (l1 != l2) throw std::runtime_error("update levels differ");
+            level_out = prec::toString(l2);
+            if (G.upToDate() != M->upToDate()) throw std::runtime_error("upToDate differs");
+            worst = std::max(worst, apply_diff());
         }
         // solves: the reference's Krylov solver with its preconditioner, the GPU's with the drop-in
         const core::Vec b = Eigen::Map<const core::Vec>(sys.rhs.data(), (Eigen::Index)sys.rhs.size());
@@ -92,7 +120,7 @@ int main(int argc, char** argv)
               << ", \"gpu_true_rel_residual\": " << r2.true_rel_residual << ", \"ref_true_rel_residual\": "
               << r1.true_rel_residual << ", \"gpu_final_residual_of\": " << r2.final_residual_of
               << ", \"ref_final_residual_of\": " << r1.final_residual_of << ", \"x_rel_diff\": " << xdiff
-              << ", \"gpu_solver\": \"" << gk->name()
+              << ", \"gpu_solver\": \"" << gk->name() << "\", \"update\": \"" << level_out
               << "\", \"ok\": " << (ok ? "true" : "false") << "}";
             std::cout << s.str() << std::endl;
         }

@@ -48,3 +48,29 @@ def test_dropin_matches_reference(case):
     res = json.loads(lines[-1])
     assert res["ok"], res
     assert r.returncode == 0
+
+
+# Preconditioner::update through the drop-in after new matrix values (D A D, same pattern):
+# Refactorize (the device refactorization) and Reuse, compared with the reference's own update()
+UPDATE_CASES = {
+    "bubbles3d_llt_refactorize": ("refactorize", "bubbles3d_ras_deflated_llt"),
+    "bubbles3d_llt_reuse": ("reuse", "bubbles3d_ras_deflated_llt"),
+    "laplace2d_lu_additive_refactorize": ("refactorize", "laplace2d_ras_additive_lu"),
+    "convdiff3d_single_lu_refactorize": ("refactorize", "convdiff3d_single_lu"),
+    "laplace2d_asm_mult_refactorize": ("refactorize", "laplace2d_asm_mult_bicgstab"),
+}
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="oracle/_ref/dropin_check is built only where the reference sources are")
+@pytest.mark.parametrize("case", sorted(UPDATE_CASES))
+def test_dropin_update_matches_reference(case):
+    level, base = UPDATE_CASES[case]
+    np_, args = CASES[base]
+    env = dict(os.environ, S2L_NP=str(np_), OMP_NUM_THREADS="1", S2L_DROPIN_UPDATE=level)
+    r = subprocess.run([BIN, *COMMON, *args], env=env, capture_output=True, text=True, timeout=600)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert lines, f"no result (rc={r.returncode}): {r.stderr[-2000:]}"
+    res = json.loads(lines[-1])
+    assert res["update"] == level, res
+    assert res["ok"], res
+    assert r.returncode == 0

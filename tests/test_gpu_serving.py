@@ -183,3 +183,36 @@ def test_engine_caches_setups_and_evicts_idle_ones_under_the_budget():
     assert made[:2] == ["a", "b"] and "c" in made  # the repeated "a" hit the cache
     assert eng.evictions >= 1 and len(eng.resident()) <= 2
     eng.close()
+
+
+def test_engine_sequence_update_levels():
+    """Engine.update along a sequence: "refactorize" gives the solve of the oracle refactorized on
+    the new values (iterations +-1), "reuse" the oracle with the old preconditioner."""
+    import dataclasses
+    import scipy.sparse as sp
+    from oracle.oracle import OracleSetup, refactor_setup
+    from s2l_b200.serving import Engine
+    w, st = small_setup("bubbles3d")
+    eng = Engine(0, workers=1)
+    eng.setup("m", lambda: st, options={"refactor": 1})
+    rng = np.random.default_rng(12)
+    for level in ("refactorize", "reuse"):
+        d = 1.0 + 0.1 * rng.uniform(-1.0, 1.0, st.n)
+        A = st.A.tocsr()
+        rows = np.repeat(np.arange(st.n), np.diff(A.indptr))
+        A2 = sp.csr_matrix((A.data * d[rows] * d[A.indices], A.indices, A.indptr), shape=A.shape)
+        eng.update("m", A2.data, level=level)
+        ref = refactor_setup(st, A2) if level == "refactorize" else None
+        if ref is None:  # reuse: the preconditioner of the last refactorization, the new operator
+            ref = dataclasses.replace(last, A=A2)
+        o = OracleSetup(ref)
+        t = eng.submit("m", lambda: st, st.b, restart=w.restart, rtol=1e-8)
+        x, r, status = t.wait(120.0)
+        t.free()
+        _, ro = o.gmres(st.b, restart=w.restart, rtol=1e-8)
+        assert status == 0 and r["converged"] and abs(r["iterations"] - ro["iterations"]) <= 1
+        assert np.linalg.norm(st.b - A2 @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+        o.close()
+        if level == "refactorize":
+            last = ref
+    eng.close()
