@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
     ap.add_argument("--seq", type=int, default=8, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
+    ap.add_argument("--serve-mix", type=int, default=0,
+                    help="serving-mix form: requests over 40 seeded cases of the three families (0 = off)")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
     return ap.parse_args()
 
@@ -465,6 +467,8 @@ def run_ours(a):
                    "clock": "host (submit to solution ready)"}
         eng.close()
 
+    serving_mix = serve_mix(a, local) if a.serve_mix > 0 else None
+
     # ---- end to end through the C ABI with pinned host buffers (headline block form): each step
     # copies its k right-hand sides and initial guesses in and its k solutions out
     g, kw = forms["mixed"]
@@ -582,6 +586,7 @@ def run_ours(a):
             "batched_mixed": batched,
             "block_mixed_threads": block_thr,
             "serving": serving,
+            "serving_mix": serving_mix,
             "sequence_refactor": sequence,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
@@ -617,6 +622,79 @@ def run_ours(a):
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def serve_mix(a, device: int) -> dict:
+    """Poisson arrivals (a.serve_rate per second) of a.serve_mix solve requests, each on one of 40
+    seeded cases of the three workload families at several sizes (2D Poisson with LU factors,
+    bubbles3d with L L^T factors, convdiff3d with FP32 LU factors and flexible GMRES), on an engine
+    with a 150 GB HBM budget and 4 workers.  Every case is set up and resident before the first
+    arrival; latency = request submitted -> solution ready (host clock)."""
+    import numpy as np
+    from s2l_b200 import workloads as W
+    from s2l_b200.serving import Engine
+    cases = []
+    for nx in (100, 120, 140, 160, 180, 200):
+        for nsub in (4, 8):
+            cases.append(("poisson2d", W.poisson2d(nx, nsub)))
+    for nx, nsub in ((24, 8), (24, 16), (28, 8), (28, 16), (32, 8), (32, 16), (32, 32), (36, 8), (36, 16), (36, 32),
+                     (40, 8), (40, 16), (40, 32), (44, 16), (44, 32), (48, 16), (48, 32), (48, 64)):
+        w = W.bubbles3d(nx, nsub, nbubbles=max(4, (nx * nx * nx) // 5000), overlap=2)
+        cases.append(("bubbles3d", w))
+    for nx in (24, 28, 32, 40, 48):
+        for nsub in (8, 16):
+            cases.append(("convdiff3d", W.convdiff3d(nx, nsub)))
+    assert len(cases) == 40
+    for q, (_, w) in enumerate(cases):
+        w.seed = 1000 + q
+    t0 = time.time()
+    built = [W.build(w) for _, w in cases]
+    setup_s = time.time() - t0
+    eng = Engine(device, hbm_budget=150 << 30, workers=4)
+    kws = []
+    for (fam, w), st in zip(cases, built):
+        flex = w.opts.local_precision == "single"
+        kws.append(dict(restart=w.restart, rtol=w.rtol, flexible=flex, strict=flex, history_cap=0))
+    for q, st in enumerate(built):  # setups resident before the arrivals (first solve of each)
+        t = eng.submit(q, (lambda st=st: st), st.b, **kws[q])
+        t.wait(600.0)
+        t.free()
+    rng = np.random.default_rng(2027)
+    gaps = rng.exponential(1.0 / a.serve_rate, a.serve_mix)
+    picks = rng.integers(0, len(cases), a.serve_mix)
+    tickets = []
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i in range(a.serve_mix):
+        t_next += gaps[i]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        q = int(picks[i])
+        st = built[q]
+        b_i = rng.uniform(-1.0, 1.0, st.n)
+        tickets.append((q, eng.submit(q, (lambda st=st: st), b_i, **kws[q])))
+    lat, fam_lat = [], {}
+    ok = True
+    for q, t in tickets:
+        _, r, status = t.wait(600.0)
+        ok = ok and status == 0 and r["converged"]
+        info = t.info()
+        ms = info["queue_ms"] + info["run_ms"]
+        lat.append(ms)
+        fam_lat.setdefault(cases[q][0], []).append(ms)
+        t.free()
+    t_end = time.perf_counter()
+    out = {"requests": a.serve_mix, "rate_req_s": a.serve_rate, "cases": len(cases),
+           "sizes_n": [int(min(st.n for st in built)), int(max(st.n for st in built))],
+           "hbm_budget_gb": 150, "all_converged": ok, "solves_per_s": a.serve_mix / (t_end - t_start),
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "max_ms": float(np.max(lat)), "setups_built": eng.builds, "evictions": eng.evictions,
+           "per_family": {f: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)),
+                              "p99_ms": float(np.percentile(v, 99))} for f, v in fam_lat.items()},
+           "host_setup_s": setup_s, "clock": "host (submit to solution ready)"}
+    eng.close()
+    return out
 
 
 def cpu_baseline(st, iterations: int, restart: int) -> dict:
