@@ -247,11 +247,13 @@ struct s2l_setup {
         int lwork = 0;
         int* info = nullptr;  // per subdomain: the dense tail factorization's status
         // coarse matrix refresh: E and its inversion, 16 unit vectors through prolong / A / restrict
-        double *E = nullptr, *colbuf = nullptr, *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr,
-               *C = nullptr, *plocal = nullptr, *rowsum = nullptr;
+        double *E = nullptr, *Einv = nullptr, *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr,
+               *C = nullptr, *plocal = nullptr, *rowsum = nullptr, *ework = nullptr;
         int* piv = nullptr;
+        int elwork = 0;
         double last_ms = 0.0;
-        double phase_ms[5] = {0, 0, 0, 0, 0};  // coarse matrix, sparse columns, tail columns, dense tails, commit
+        double phase_ms[6] = {0, 0, 0, 0, 0, 0};  // coarse matrix, its inverse, sparse columns, tail columns,
+                                                  // dense tails, commit
     } rf;
 
     int fail(int code, const std::string& msg)
@@ -2037,7 +2039,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     return s->fail(S2L_ERR_BADARG, "refactor: a factor column has 65535 or more entries");
                 s->rf.maxcol = std::max(s->rf.maxcol, (int)(P.cp[c + 1] - P.cp[c]));
             }
-            if (sz > 100000) return s->fail(S2L_ERR_BADARG, "refactor: a dense tail of more than 100000 rows");
+            if (nl > 100000) return s->fail(S2L_ERR_BADARG, "refactor: a subdomain of more than 100000 rows");
             mposL.assign(h.L.ci.size(), -1);
             for (int r = 0; r < nl; ++r)
                 for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) {
@@ -2435,7 +2437,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.stage), (size_t)std::max<int64_t>(s->nnz, 1) * sizeof(double)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.err), sizeof(int)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.part), (size_t)nsub * 32 * R.maxcol * sizeof(double)));
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.info), (size_t)nsub * sizeof(int)));
+        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.info), (size_t)(nsub + 2) * sizeof(int)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.rowsum), (size_t)s->n * sizeof(double)));
         {
             auto dbl = [&](double** p, size_t count) {
@@ -2443,7 +2445,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
             };
             const int64_t n0 = std::max<int64_t>(s->n0, 1);
             RET_IF(dbl(&R.E, (size_t)n0 * n0));
-            RET_IF(dbl(&R.colbuf, (size_t)n0));
+            RET_IF(dbl(&R.Einv, (size_t)n0 * n0));
             RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.piv), (size_t)n0 * sizeof(int)));
             RET_IF(dbl(&R.Y, (size_t)n0 * 16));
             RET_IF(dbl(&R.X, (size_t)s->n * 16));
@@ -2477,6 +2479,11 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 return s->fail(S2L_ERR_CUDA, "cuSOLVER workspace query failed");
             R.lwork = std::max(std::max(l1, l2), 1);
             for (int q = 0; q < NS; ++q) RET_IF(dbl(&R.swork[q], (size_t)R.lwork));
+            int l3 = 0;
+            if (cusolverDnDgetrf_bufferSize(R.tsolver[0], (int)n0, (int)n0, R.E, (int)n0, &l3) != CUSOLVER_STATUS_SUCCESS)
+                return s->fail(S2L_ERR_CUDA, "cuSOLVER workspace query failed");
+            R.elwork = std::max(l3, 1);
+            RET_IF(dbl(&R.ework, (size_t)R.elwork));
         }
         RET_IF(upload(s, &R.fbase, rf_fbase));
         RET_IF(upload(s, &R.fcp, rf_fcp));
@@ -2731,7 +2738,7 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     const auto t0 = std::chrono::steady_clock::now();
     // phase timers (events on the setup stream)
     struct Evs {
-        cudaEvent_t e[6] = {};
+        cudaEvent_t e[7] = {};
         ~Evs()
         {
             for (auto x : e)
@@ -2742,7 +2749,7 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     CUDA_OK(s, cudaMemcpyAsync(R.stage, val, (size_t)nnz * sizeof(double),
                                ptr_kind == S2L_PTR_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
     CUDA_OK(s, cudaMemsetAsync(R.err, 0, sizeof(int), st));
-    CUDA_OK(s, cudaMemsetAsync(R.info, 0, (size_t)nsub * sizeof(int), st));
+    CUDA_OK(s, cudaMemsetAsync(R.info, 0, (size_t)(nsub + 2) * sizeof(int), st));
     // row sums of the new matrix: the OpenFOAM normalisation, and a finiteness check of every value
     launch_row_sums(st, n, s->d_rp, R.stage, R.rowsum);
     {
@@ -2755,9 +2762,19 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     // coarse matrix with the kept basis, and its inverse
     const bool coarse = s->coarse != S2L_COARSE_NONE && n0 > 0;
     CUDA_OK(s, cudaEventRecord(ev.e[0], st));
+    if (coarse) RET_IF(coarse_matrix_dev(s, st, R.stage, R.E));
+    CUDA_OK(s, cudaEventRecord(ev.e[1], st));
     if (coarse) {
-        RET_IF(coarse_matrix_dev(s, st, R.stage, R.E));
-        launch_gauss_jordan(st, (int)n0, R.E, R.colbuf, R.piv, R.err);
+        // E^-1: LU with partial pivoting (E row-major is E^T column-major; the solve against the
+        // identity gives (E^T)^-1 column-major = E^-1 row-major); info > 0: singular
+        RET_IF(tails_fork(s, st));
+        launch_identity(R.tstream[0], R.Einv, (int)n0);
+        if (cusolverDnDgetrf(R.tsolver[0], (int)n0, (int)n0, R.E, (int)n0, R.ework, R.piv, R.info + nsub) !=
+                CUSOLVER_STATUS_SUCCESS ||
+            cusolverDnDgetrs(R.tsolver[0], CUBLAS_OP_N, (int)n0, (int)n0, R.E, (int)n0, R.piv, R.Einv, (int)n0,
+                             R.info + nsub + 1) != CUSOLVER_STATUS_SUCCESS)
+            return s->fail(S2L_ERR_CUDA, "coarse inversion failed to launch");
+        RET_IF(tails_join(s, st));
     }
     // local factors on their kept patterns
     RefactorArgs a{};
@@ -2782,26 +2799,28 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     a.smax = 1;
     for (int sz : R.sz) a.smax = std::max(a.smax, sz);
     a.maxcol = R.maxcol;
+    a.nlmax = s->max_nl;
     a.part = R.part;
     CUDA_OK(s, cudaMemsetAsync(R.F, 0, (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double), st));
     launch_refactor_fill(st, R.nfill, R.fill_src, R.fill_dst, R.stage, R.F);
-    CUDA_OK(s, cudaEventRecord(ev.e[1], st));
-    launch_refactor_sparse(st, a, nsub);
     CUDA_OK(s, cudaEventRecord(ev.e[2], st));
-    launch_refactor_tail_columns(st, a);
+    launch_refactor_sparse(st, a, nsub);
     CUDA_OK(s, cudaEventRecord(ev.e[3], st));
+    launch_refactor_tail_columns(st, a);
+    CUDA_OK(s, cudaEventRecord(ev.e[4], st));
     CUDA_OK(s, cudaMemsetAsync(R.S, 0, (size_t)std::max<int64_t>(R.d_off[nsub], 1) * sizeof(double), st));
     launch_refactor_gather_tails(st, a);
     RET_IF(refactor_dense_tails(s, st));
-    CUDA_OK(s, cudaEventRecord(ev.e[4], st));
+    CUDA_OK(s, cudaEventRecord(ev.e[5], st));
     CUDA_OK(s, cudaGetLastError());
     int herr = 0;
-    std::vector<int> infos((size_t)nsub);
+    std::vector<int> infos((size_t)nsub + 2);
     CUDA_OK(s, cudaMemcpyAsync(&herr, R.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(s, cudaMemcpyAsync(infos.data(), R.info, (size_t)nsub * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(s, cudaMemcpyAsync(infos.data(), R.info, (size_t)(nsub + 2) * sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(s, cudaStreamSynchronize(st));
     for (int i = 0; i < nsub && herr == 0; ++i)
         if (infos[i] != 0) herr = 2;
+    if (herr == 0 && coarse && (infos[nsub] != 0 || infos[nsub + 1] != 0)) herr = 3;
     if (herr == 1) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a sparse column");
     if (herr == 2) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a dense tail");
     if (herr == 3) return s->fail(S2L_ERR_NUMERIC, "refactorization: the coarse matrix is singular");
@@ -2810,14 +2829,14 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     CUDA_OK(s, cudaMemcpyAsync(s->d_av, R.stage, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CUDA_OK(s, cudaMemcpyAsync(s->d_rowsum, R.rowsum, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (coarse)
-        CUDA_OK(s, cudaMemcpyAsync(s->d_Einv, R.E, (size_t)n0 * n0 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CUDA_OK(s, cudaMemcpyAsync(s->d_Einv, R.Einv, (size_t)n0 * n0 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (s->real == S2L_REAL_F32) RET_IF(refactor_commit_factors<float>(s, st));
     else RET_IF(refactor_commit_factors<double>(s, st));
     CUDA_OK(s, cudaGetLastError());
-    CUDA_OK(s, cudaEventRecord(ev.e[5], st));
+    CUDA_OK(s, cudaEventRecord(ev.e[6], st));
     CUDA_OK(s, cudaStreamSynchronize(st));
     R.last_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    for (int q = 0; q < 5; ++q) {
+    for (int q = 0; q < 6; ++q) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev.e[q], ev.e[q + 1]);
         R.phase_ms[q] = ms;
@@ -2910,10 +2929,11 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "refactor_bytes") *value = (double)s->rf.bytes;
     else if (n == "refactor_ms") *value = s->rf.last_ms;
     else if (n == "refactor_ms_coarse") *value = s->rf.phase_ms[0];
-    else if (n == "refactor_ms_sparse") *value = s->rf.phase_ms[1];
-    else if (n == "refactor_ms_tail") *value = s->rf.phase_ms[2];
-    else if (n == "refactor_ms_dense") *value = s->rf.phase_ms[3];
-    else if (n == "refactor_ms_commit") *value = s->rf.phase_ms[4];
+    else if (n == "refactor_ms_coarse_inverse") *value = s->rf.phase_ms[1];
+    else if (n == "refactor_ms_sparse") *value = s->rf.phase_ms[2];
+    else if (n == "refactor_ms_tail") *value = s->rf.phase_ms[3];
+    else if (n == "refactor_ms_dense") *value = s->rf.phase_ms[4];
+    else if (n == "refactor_ms_commit") *value = s->rf.phase_ms[5];
     else return S2L_ERR_BADARG;
     return S2L_OK;
 }

@@ -130,18 +130,31 @@ __device__ void update_column(const RefactorArgs& a, int64_t loc, int64_t fb, in
     }
 }
 
+// offset of row i in the column whose full row map is m (every row of the subdomain)
+struct FullMap {
+    const uint16_t* m;
+    __device__ int64_t operator()(int i) const { return m[i]; }
+};
+
 // The same for one column with every warp of the CTA.  The sum over k is split: for LU the part
 // of U(:, j) (rows < j, a sequential triangular solve) is done by warp 0 first; then the updates of
 // rows >= j, independent over k, go round-robin to the warps, each into its own partial column
-// (part), which are added in a fixed order at the end.  Every thread of the CTA calls this.
-__device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int j, int T,
-                                   uint16_t* map, double* part, int wid, int nw, int lane)
+// (part), which are added in a fixed order at the end.  Rows are located through one map of the
+// whole column in shared memory (cmap, a row of the subdomain -> offset).  Every thread of the
+// CTA calls this.
+__device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int j,
+                                   uint16_t* cmap, double* part, int wid, int nw, int lane)
 {
     double* __restrict__ F = a.F;
-    const ColumnView cv = column_view(a, gj, T, map, lane);
+    ColumnView cv;
+    cv.c0 = a.fcp[gj];
+    cv.c1 = a.fcp[gj + 1];
     const int64_t len = cv.c1 - cv.c0;
+    for (int64_t p = cv.c0 + threadIdx.x; p < cv.c1; p += blockDim.x) cmap[a.fri[p]] = (uint16_t)(p - cv.c0);
+    const FullMap fm{cmap};
     double* mine = part + (size_t)wid * a.maxcol;
     for (int64_t q = lane; q < len; q += 32) mine[q] = 0.0;
+    __syncthreads();  // the column map is complete
     const bool llt = a.fllt[gj];
     const int64_t u0 = cv.c0, u1 = cv.c0 + a.fdg[gj];
     if (!llt && wid == 0) {
@@ -152,7 +165,7 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
             const int64_t gk = loc + k;
             const int64_t b = a.fcp[gk] + a.fdg[gk] + 1, e = a.fcp[gk + 1];
             const int64_t ej = find_row(a.fri, b, e + 1, j);  // first row >= j
-            if (u != 0.0) scatter_segment(F, a.fri, b, ej, u, F + cv.c0, cv, lane);
+            if (u != 0.0) scatter_segment(F, a.fri, b, ej, u, F + cv.c0, fm, lane);
             __syncwarp();
         }
     }
@@ -162,7 +175,7 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
         for (int64_t t = r0 + wid; t < r1; t += nw) {
             const int k = a.frk[t];
             const int64_t p = fb + a.frpos[t];
-            scatter_segment(F, a.fri, p, a.fcp[loc + k + 1], F[p], mine, cv, lane);
+            scatter_segment(F, a.fri, p, a.fcp[loc + k + 1], F[p], mine, fm, lane);
             __syncwarp();
         }
     } else {
@@ -172,7 +185,7 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
             const int64_t gk = loc + k;
             const int64_t b = a.fcp[gk] + a.fdg[gk] + 1, e = a.fcp[gk + 1];
             const int64_t ej = find_row(a.fri, b, e + 1, j);
-            if (u != 0.0) scatter_segment(F, a.fri, ej, e, u, mine, cv, lane);
+            if (u != 0.0) scatter_segment(F, a.fri, ej, e, u, mine, fm, lane);
             __syncwarp();
         }
     }
@@ -238,7 +251,7 @@ __global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorA
             // few columns (the chains near the top of the sparse part): each with the whole CTA
             for (int64_t c = e0; c < e1; ++c) {
                 const int j = a.lv_col[c];
-                update_column_coop(a, loc, fb, loc + j, j, T, map, part, wid, nw, lane);
+                update_column_coop(a, loc, fb, loc + j, j, rmap, part, wid, nw, lane);
                 if (wid == 0) finish_column(a, loc + j, lane);
                 __syncthreads();
             }
@@ -454,96 +467,6 @@ __global__ void scatter_columns_kernel(int64_t n0, int c0, const double* C, doub
     }
 }
 
-// Gauss-Jordan step k, part 1 (one CTA): the pivot row (largest |A(i, k)|, i >= k; the first of
-// equals), the row swap, column k saved, row k scaled (A(k, k) <- 1 / pivot)
-__global__ void __launch_bounds__(1024) gj_pivot_kernel(int n, int k, double* A, double* colbuf, int* piv, int* err)
-{
-    __shared__ double bv[32];
-    __shared__ int bi[32];
-    __shared__ int prow;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (*(volatile int*)err) return;
-    double best = -1.0;
-    int besti = n;
-    for (int i = k + tid; i < n; i += blockDim.x) {
-        const double v = fabs(A[(int64_t)i * n + k]);
-        if (v > best || (v == best && i < besti)) {
-            best = v;
-            besti = i;
-        }
-    }
-    for (int o = 16; o; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
-        if (ov > best || (ov == best && oi < besti)) {
-            best = ov;
-            besti = oi;
-        }
-    }
-    if (lane == 0) {
-        bv[wid] = best;
-        bi[wid] = besti;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double b = -1.0;
-        int p = n;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
-            if (bv[w] > b || (bv[w] == b && bi[w] < p)) {
-                b = bv[w];
-                p = bi[w];
-            }
-        prow = (b > 0.0 && isfinite(b)) ? p : -1;
-        if (prow < 0) set_err(err, 3);
-        piv[k] = prow;
-    }
-    __syncthreads();
-    const int p = prow;
-    if (p < 0) return;
-    if (p != k)
-        for (int j = tid; j < n; j += blockDim.x) {
-            const double t = A[(int64_t)k * n + j];
-            A[(int64_t)k * n + j] = A[(int64_t)p * n + j];
-            A[(int64_t)p * n + j] = t;
-        }
-    __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) colbuf[i] = A[(int64_t)i * n + k];
-    __syncthreads();
-    const double pinv = 1.0 / colbuf[k];
-    for (int j = tid; j < n; j += blockDim.x) A[(int64_t)k * n + j] = j == k ? pinv : A[(int64_t)k * n + j] * pinv;
-}
-
-// part 2: every other row i: A(i, j) -= A_old(i, k) A(k, j) (j != k), A(i, k) = -A_old(i, k) / pivot
-__global__ void gj_update_kernel(int n, int k, double* A, const double* colbuf, const int* err)
-{
-    if (*(volatile const int*)err) return;
-    const int64_t total = (int64_t)n * n;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / n), j = (int)(e % n);
-        if (i == k) continue;
-        const double f = colbuf[i];
-        if (j == k) A[e] = -f * A[(int64_t)k * n + k];
-        else if (f != 0.0) A[e] -= f * A[(int64_t)k * n + j];
-    }
-}
-
-// the row swaps undone as column swaps in reverse order (one thread per row)
-__global__ void gj_unpermute_kernel(int n, double* A, const int* piv, const int* err)
-{
-    if (*(volatile const int*)err) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double* Ai = A + (int64_t)i * n;
-    for (int k = n - 1; k >= 0; --k) {
-        const int p = piv[k];
-        if (p != k) {
-            const double t = Ai[k];
-            Ai[k] = Ai[p];
-            Ai[p] = t;
-        }
-    }
-}
-
 int grid_for(int64_t work, int bs)
 {
     const int64_t g = (work + bs - 1) / bs;
@@ -577,7 +500,8 @@ static int sparse_warps(int smax)
 void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub)
 {
     const int w = sparse_warps(a.smax);
-    const size_t smem = refactor_map_bytes(a.smax, w);
+    // the per-warp tail maps, or (cooperative columns) one map of every row of a subdomain
+    const size_t smem = std::max(refactor_map_bytes(a.smax, w), (size_t)a.nlmax * sizeof(uint16_t));
     cudaFuncSetAttribute(sparse_columns_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     sparse_columns_kernel<<<nsub, 32 * w, smem, st>>>(a);
 }
@@ -657,16 +581,6 @@ void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y)
 void launch_scatter_columns(cudaStream_t st, int64_t n0, int c0, const double* C, double* E)
 {
     scatter_columns_kernel<<<grid_for(n0 * 16, 256), 256, 0, st>>>(n0, c0, C, E);
-}
-
-void launch_gauss_jordan(cudaStream_t st, int n, double* A, double* colbuf, int* piv, int* err)
-{
-    const int g = grid_for((int64_t)n * n, 256);
-    for (int k = 0; k < n; ++k) {
-        gj_pivot_kernel<<<1, 1024, 0, st>>>(n, k, A, colbuf, piv, err);
-        gj_update_kernel<<<g, 256, 0, st>>>(n, k, A, colbuf, err);
-    }
-    gj_unpermute_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, A, piv, err);
 }
 
 template void launch_refactor_sweep_values<double>(cudaStream_t, int, const int64_t*, const double*, const int64_t*,

@@ -139,10 +139,10 @@ struct RefactorArgs {
     double* S;                 // dense tails (s x s row-major at subs[i].d_off)
     int smax;                  // largest tail: the per-warp row maps hold smax uint16 positions
     int maxcol;                // longest column of F
+    int nlmax;                 // largest subdomain (rows): the cooperative column map
     double* part;              // partial columns of the cooperative column updates: per subdomain
                                // and warp, maxcol doubles
-    int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column,
-                               // 3 singular coarse matrix (0: none)
+    int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column (0: none)
 };
 
 // launch wrappers (kernels.cu)
@@ -243,9 +243,8 @@ void launch_refactor_blocks(cudaStream_t st, int64_t nblocks, const int64_t* bof
 template <typename Real>
 void launch_gather_values(cudaStream_t st, int64_t count, const int64_t* src, const double* F, Real* out);
 void launch_row_sums(cudaStream_t st, int64_t n, const int32_t* rp, const double* v, double* out);
-// coarse matrix refresh: unit block, E columns, Gauss-Jordan inversion with partial pivoting
+// coarse matrix refresh: unit block, E columns
 void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y);
 void launch_scatter_columns(cudaStream_t st, int64_t n0, int c0, const double* C, double* E);
-void launch_gauss_jordan(cudaStream_t st, int n, double* A, double* colbuf, int* piv, int* err);
 
 }  // namespace s2l

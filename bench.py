@@ -524,7 +524,8 @@ def run_ours(a):
             chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(kh))
             steps_q.append({"step": step, "refactor_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
                             "refactor_phases_ms": {k: round(g.stat("refactor_ms_" + k), 2)
-                                                   for k in ("coarse", "sparse", "tail", "dense", "commit")},
+                                                   for k in ("coarse", "coarse_inverse", "sparse", "tail", "dense",
+                                                             "commit")},
                             "iterations_max": max(r["iterations"] for r in rq),
                             "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
         g.refactor(st32.A.data)  # back to the setup's own matrix
