@@ -221,6 +221,7 @@ struct s2l_setup {
         double* stage = nullptr;  // the new matrix values until they are committed
         double* part = nullptr;   // partial columns of the cooperative column updates
         int maxcol = 1;
+        int cs = 1;               // CTAs (a cluster) per subdomain in the sparse-column walk
         int* err = nullptr;
         int64_t *fbase = nullptr, *fcp = nullptr, *frp = nullptr, *lv_off = nullptr;
         int32_t *fri = nullptr, *fdg = nullptr, *frpos = nullptr, *frk = nullptr, *lv_first = nullptr,
@@ -2436,7 +2437,17 @@ int s2l_gpu_setup_end(s2l_setup* s)
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.S), (size_t)std::max<int64_t>(d_off[nsub], 1) * sizeof(double)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.stage), (size_t)std::max<int64_t>(s->nnz, 1) * sizeof(double)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.err), sizeof(int)));
-        RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.part), (size_t)nsub * 32 * R.maxcol * sizeof(double)));
+        {
+            // clusters of 4 or 2 CTAs per subdomain when they fit the SMs at once, else one
+            int sms = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->ctx->device) != cudaSuccess || sms <= 0)
+                sms = 148;
+            R.cs = nsub * 4 <= sms ? 4 : (nsub * 2 <= sms ? 2 : 1);
+            int smax = 1;
+            for (int sz : R.sz) smax = std::max(smax, sz);
+            const size_t warps = (size_t)R.cs * refactor_sparse_warps(smax);
+            RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.part), (size_t)nsub * warps * R.maxcol * sizeof(double)));
+        }
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.info), (size_t)(nsub + 2) * sizeof(int)));
         RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.rowsum), (size_t)s->n * sizeof(double)));
         {
@@ -2804,7 +2815,7 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     CUDA_OK(s, cudaMemsetAsync(R.F, 0, (size_t)std::max<int64_t>(R.nF, 1) * sizeof(double), st));
     launch_refactor_fill(st, R.nfill, R.fill_src, R.fill_dst, R.stage, R.F);
     CUDA_OK(s, cudaEventRecord(ev.e[2], st));
-    launch_refactor_sparse(st, a, nsub);
+    launch_refactor_sparse(st, a, nsub, R.cs);
     CUDA_OK(s, cudaEventRecord(ev.e[3], st));
     launch_refactor_tail_columns(st, a);
     CUDA_OK(s, cudaEventRecord(ev.e[4], st));
@@ -2928,6 +2939,7 @@ int s2l_gpu_setup_stat(const s2l_setup* s, const char* name, double* value)
     else if (n == "levels_mean") *value = s->nsub ? (double)s->st_levels_sum / (2.0 * s->nsub) : 0.0;
     else if (n == "refactor_bytes") *value = (double)s->rf.bytes;
     else if (n == "refactor_ms") *value = s->rf.last_ms;
+    else if (n == "refactor_cluster") *value = (double)s->rf.cs;
     else if (n == "refactor_ms_coarse") *value = s->rf.phase_ms[0];
     else if (n == "refactor_ms_coarse_inverse") *value = s->rf.phase_ms[1];
     else if (n == "refactor_ms_sparse") *value = s->rf.phase_ms[2];

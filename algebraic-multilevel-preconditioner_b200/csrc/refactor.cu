@@ -20,8 +20,12 @@
 // Every column is reduced by one warp in a fixed order, so the result does not depend on timing.
 #include "s2l_internal.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -143,21 +147,19 @@ struct FullMap {
 // whole column in shared memory (cmap, a row of the subdomain -> offset).  Every thread of the
 // CTA calls this.
 __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t fb, int64_t gj, int j,
-                                   uint16_t* cmap, double* part, int wid, int nw, int lane)
+                                   uint16_t* cmap, double* part, int gw, int nw, int lane, cg::cluster_group& cl)
 {
     double* __restrict__ F = a.F;
-    ColumnView cv;
-    cv.c0 = a.fcp[gj];
-    cv.c1 = a.fcp[gj + 1];
-    const int64_t len = cv.c1 - cv.c0;
-    for (int64_t p = cv.c0 + threadIdx.x; p < cv.c1; p += blockDim.x) cmap[a.fri[p]] = (uint16_t)(p - cv.c0);
+    const int64_t c0 = a.fcp[gj], c1 = a.fcp[gj + 1];
+    const int64_t len = c1 - c0;
+    for (int64_t p = c0 + threadIdx.x; p < c1; p += blockDim.x) cmap[a.fri[p]] = (uint16_t)(p - c0);
     const FullMap fm{cmap};
-    double* mine = part + (size_t)wid * a.maxcol;
+    double* mine = part + (size_t)gw * a.maxcol;
     for (int64_t q = lane; q < len; q += 32) mine[q] = 0.0;
-    __syncthreads();  // the column map is complete
+    cl.sync();  // every CTA's column map is complete
     const bool llt = a.fllt[gj];
-    const int64_t u0 = cv.c0, u1 = cv.c0 + a.fdg[gj];
-    if (!llt && wid == 0) {
+    const int64_t u0 = c0, u1 = c0 + a.fdg[gj];
+    if (!llt && gw == 0) {
         // U(:, j): the rows < j of the segments, in increasing k
         for (int64_t t = u0; t < u1; ++t) {
             const int k = a.fri[t];
@@ -165,21 +167,21 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
             const int64_t gk = loc + k;
             const int64_t b = a.fcp[gk] + a.fdg[gk] + 1, e = a.fcp[gk + 1];
             const int64_t ej = find_row(a.fri, b, e + 1, j);  // first row >= j
-            if (u != 0.0) scatter_segment(F, a.fri, b, ej, u, F + cv.c0, fm, lane);
+            if (u != 0.0) scatter_segment(F, a.fri, b, ej, u, F + c0, fm, lane);
             __syncwarp();
         }
     }
-    __syncthreads();
+    cl.sync();
     if (llt) {
         const int64_t r0 = a.frp[gj], r1 = a.frp[gj + 1];
-        for (int64_t t = r0 + wid; t < r1; t += nw) {
+        for (int64_t t = r0 + gw; t < r1; t += nw) {
             const int k = a.frk[t];
             const int64_t p = fb + a.frpos[t];
             scatter_segment(F, a.fri, p, a.fcp[loc + k + 1], F[p], mine, fm, lane);
             __syncwarp();
         }
     } else {
-        for (int64_t t = u0 + wid; t < u1; t += nw) {
+        for (int64_t t = u0 + gw; t < u1; t += nw) {
             const int k = a.fri[t];
             const double u = F[t];
             const int64_t gk = loc + k;
@@ -189,13 +191,14 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
             __syncwarp();
         }
     }
-    __syncthreads();
-    for (int64_t q = threadIdx.x; q < len; q += blockDim.x) {
+    cl.sync();
+    const int64_t stride = (int64_t)cl.num_blocks() * blockDim.x;
+    for (int64_t q = (int64_t)cl.block_rank() * blockDim.x + threadIdx.x; q < len; q += stride) {
         double sum = 0.0;
         for (int w = 0; w < nw; ++w) sum += part[(size_t)w * a.maxcol + q];
-        F[cv.c0 + q] += sum;
+        F[c0 + q] += sum;
     }
-    __syncthreads();
+    cl.sync();
 }
 
 // pivot of column gj: LU divides the strict lower part by U(j, j); L L^T takes the square root of
@@ -238,34 +241,36 @@ __global__ void fill_kernel(int64_t count, const int64_t* __restrict__ src, cons
 __global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorArgs a)
 {
     extern __shared__ uint16_t rmap[];
-    const int sid = blockIdx.x;
+    cg::cluster_group cl = cg::this_cluster();
+    const int cs = (int)cl.num_blocks();
+    const int sid = blockIdx.x / cs;
     const int64_t loc = a.subs[sid].loc_off, fb = a.fbase[sid];
     const int T = a.subs[sid].T;
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = cs * (int)(blockDim.x >> 5);                        // warps of the cluster
+    const int gw = (int)cl.block_rank() * (int)(blockDim.x >> 5) + wid;  // this warp among them
     uint16_t* map = rmap + (size_t)wid * a.smax;
-    __shared__ int stop;
     double* part = a.part + (size_t)sid * nw * a.maxcol;
+    // Control flow is the same in every CTA of the cluster, so every thread reaches every
+    // cluster barrier; a failed pivot only sets the error word (every loop is bounded).
     for (int lv = a.lv_first[sid]; lv < a.lv_first[sid + 1]; ++lv) {
         const int64_t e0 = a.lv_off[lv], e1 = a.lv_off[lv + 1];
         if (e1 - e0 <= nw / 4) {
-            // few columns (the chains near the top of the sparse part): each with the whole CTA
+            // few columns (the chains near the top of the sparse part): each with the whole cluster
             for (int64_t c = e0; c < e1; ++c) {
                 const int j = a.lv_col[c];
-                update_column_coop(a, loc, fb, loc + j, j, rmap, part, wid, nw, lane);
-                if (wid == 0) finish_column(a, loc + j, lane);
-                __syncthreads();
+                update_column_coop(a, loc, fb, loc + j, j, rmap, part, gw, nw, lane, cl);
+                if (gw == 0) finish_column(a, loc + j, lane);
+                cl.sync();
             }
         } else {
-            for (int64_t c = e0 + wid; c < e1; c += nw) {
+            for (int64_t c = e0 + gw; c < e1; c += nw) {
                 const int j = a.lv_col[c];
                 update_column(a, loc, fb, loc + j, j, T, map, lane);
                 finish_column(a, loc + j, lane);
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) stop = *(volatile int*)a.err;  // a failed pivot anywhere ends the walk
-        __syncthreads();
-        if (stop) return;
+        cl.sync();
     }
 }
 
@@ -497,13 +502,31 @@ static int sparse_warps(int smax)
     return w;
 }
 
-void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub)
+int refactor_sparse_warps(int smax)
+{
+    return sparse_warps(smax);
+}
+
+void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub, int cs)
 {
     const int w = sparse_warps(a.smax);
     // the per-warp tail maps, or (cooperative columns) one map of every row of a subdomain
     const size_t smem = std::max(refactor_map_bytes(a.smax, w), (size_t)a.nlmax * sizeof(uint16_t));
     cudaFuncSetAttribute(sparse_columns_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    sparse_columns_kernel<<<nsub, 32 * w, smem, st>>>(a);
+    // a cluster of cs CTAs (cs SMs) per subdomain
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nsub * cs));
+    cfg.blockDim = dim3((unsigned)(32 * w));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, sparse_columns_kernel, a);
 }
 
 void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a)

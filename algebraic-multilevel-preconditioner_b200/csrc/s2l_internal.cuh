@@ -220,7 +220,10 @@ void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 // refactorization (refactor.cu)
 void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, const int64_t* dst, const double* val,
                           double* F);
-void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub);
+// cs CTAs (a thread-block cluster) per subdomain; the partial columns hold nsub x cs x
+// refactor_sparse_warps(smax) x maxcol doubles
+void launch_refactor_sparse(cudaStream_t st, const RefactorArgs& a, int nsub, int cs);
+int refactor_sparse_warps(int smax);
 size_t refactor_map_bytes(int smax, int warps);
 void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a);
 void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a);
