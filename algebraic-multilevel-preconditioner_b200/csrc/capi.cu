@@ -250,6 +250,12 @@ struct s2l_setup {
         // coarse matrix refresh: E and its inversion, 16 unit vectors through prolong / A / restrict
         double *E = nullptr, *Einv = nullptr, *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr,
                *C = nullptr, *plocal = nullptr, *rowsum = nullptr, *ework = nullptr;
+        // direct coarse assembly (boolean partition of unity): row slots and subdomain pairs
+        bool direct = false;
+        int npairs = 0;
+        int32_t *owner = nullptr, *rs_sub = nullptr, *pair_j = nullptr, *pair_i = nullptr, *pair_rl = nullptr;
+        int64_t *rs_ptr = nullptr, *rs_zoff = nullptr, *pair_ptr = nullptr, *pair_zoff = nullptr;
+        double* Z = nullptr;
         int* piv = nullptr;
         int elwork = 0;
         double last_ms = 0.0;
@@ -2457,6 +2463,63 @@ int s2l_gpu_setup_end(s2l_setup* s)
             const int64_t n0 = std::max<int64_t>(s->n0, 1);
             RET_IF(dbl(&R.E, (size_t)n0 * n0));
             RET_IF(dbl(&R.Einv, (size_t)n0 * n0));
+            if (s->coarse != S2L_COARSE_NONE && s->n0 > 0 && s->pou == S2L_POU_BOOLEAN) {
+                // per row: the subdomains owning its columns (slots of m_i values in Z); per pair
+                // (owner of the row, owner of a column): the rows and their slots
+                std::vector<int32_t> owner((size_t)s->n), rs_sub, pj, pi, prl;
+                std::vector<int64_t> rs_ptr(1, 0), rs_zoff, pptr;
+                for (int i = 0; i < nsub; ++i)
+                    for (int r = 0; r < s->hs[i].n_owned; ++r) owner[(size_t)(s->hs[i].begin + r)] = i;
+                std::vector<std::vector<std::pair<int32_t, int64_t>>> rows_of;  // per pair
+                std::vector<std::vector<int32_t>> pair_of(nsub);                // pair id by (j, i)
+                std::vector<int32_t> subs_in_row;
+                int64_t z = 0;
+                for (int64_t r = 0; r < s->n; ++r) {
+                    subs_in_row.clear();
+                    for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) {
+                        const int32_t i = owner[(size_t)s->A.ci[e]];
+                        if (std::find(subs_in_row.begin(), subs_in_row.end(), i) == subs_in_row.end())
+                            subs_in_row.push_back(i);
+                    }
+                    std::sort(subs_in_row.begin(), subs_in_row.end());
+                    const int32_t j = owner[(size_t)r];
+                    for (int32_t i : subs_in_row) {
+                        rs_sub.push_back(i);
+                        rs_zoff.push_back(z);
+                        if (pair_of[j].empty()) pair_of[j].assign(nsub, -1);
+                        if (pair_of[j][i] < 0) {
+                            pair_of[j][i] = (int32_t)rows_of.size();
+                            rows_of.emplace_back();
+                            pj.push_back(j);
+                            pi.push_back(i);
+                        }
+                        rows_of[pair_of[j][i]].emplace_back((int32_t)(r - s->hs[j].begin), z);
+                        z += s->hs[i].m;
+                    }
+                    rs_ptr.push_back((int64_t)rs_sub.size());
+                }
+                std::vector<int64_t> pzoff;
+                pptr.push_back(0);
+                for (const auto& v : rows_of) {
+                    for (const auto& q : v) {
+                        prl.push_back(q.first);
+                        pzoff.push_back(q.second);
+                    }
+                    pptr.push_back((int64_t)prl.size());
+                }
+                R.npairs = (int)rows_of.size();
+                RET_IF(upload(s, &R.owner, owner));
+                RET_IF(upload(s, &R.rs_ptr, rs_ptr));
+                RET_IF(upload(s, &R.rs_sub, rs_sub));
+                RET_IF(upload(s, &R.rs_zoff, rs_zoff));
+                RET_IF(upload(s, &R.pair_j, pj));
+                RET_IF(upload(s, &R.pair_i, pi));
+                RET_IF(upload(s, &R.pair_ptr, pptr));
+                RET_IF(upload(s, &R.pair_rl, prl));
+                RET_IF(upload(s, &R.pair_zoff, pzoff));
+                RET_IF(dbl(&R.Z, (size_t)std::max<int64_t>(z, 1)));
+                R.direct = true;
+            }
             RET_IF(dev_alloc(s, reinterpret_cast<void**>(&R.piv), (size_t)n0 * sizeof(int)));
             RET_IF(dbl(&R.Y, (size_t)n0 * 16));
             RET_IF(dbl(&R.X, (size_t)s->n * 16));
@@ -2773,7 +2836,11 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     // coarse matrix with the kept basis, and its inverse
     const bool coarse = s->coarse != S2L_COARSE_NONE && n0 > 0;
     CUDA_OK(s, cudaEventRecord(ev.e[0], st));
-    if (coarse) RET_IF(coarse_matrix_dev(s, st, R.stage, R.E));
+    if (coarse && R.direct)
+        launch_coarse_direct(st, n, s->d_rp, s->d_ci, R.stage, R.owner, R.rs_ptr, R.rs_sub, R.rs_zoff, R.npairs,
+                             R.pair_j, R.pair_i, R.pair_ptr, R.pair_rl, R.pair_zoff, s->d_subs, s->d_V, R.Z, n0, R.E);
+    else if (coarse)
+        RET_IF(coarse_matrix_dev(s, st, R.stage, R.E));
     CUDA_OK(s, cudaEventRecord(ev.e[1], st));
     if (coarse) {
         // E^-1: LU with partial pivoting (E row-major is E^T column-major; the solve against the

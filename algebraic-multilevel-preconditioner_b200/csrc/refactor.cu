@@ -472,6 +472,61 @@ __global__ void scatter_columns_kernel(int64_t n0, int c0, const double* C, doub
     }
 }
 
+// Coarse matrix E = W^T A W for a boolean partition of unity, where column (i, a) of W is
+// V_i(:, a) on the owned rows of subdomain i.  Step 1, per row r: for every subdomain i owning a
+// column of the row, u_{r,i} = sum over the entries (r, c), c owned by i, of A(r, c) V_i(c, :).
+__global__ void __launch_bounds__(256) coarse_z_kernel(int64_t n, const int32_t* __restrict__ rp,
+                                                       const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                                       const int32_t* __restrict__ owner,
+                                                       const int64_t* __restrict__ rs_ptr,
+                                                       const int32_t* __restrict__ rs_sub,
+                                                       const int64_t* __restrict__ rs_zoff,
+                                                       const DevSub* __restrict__ subs, const double* __restrict__ V,
+                                                       double* __restrict__ Z)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s0 = rs_ptr[r], s1 = rs_ptr[r + 1];
+        for (int64_t q = s0; q < s1; ++q) {
+            const int m = subs[rs_sub[q]].m;
+            for (int a = 0; a < m; ++a) Z[rs_zoff[q] + a] = 0.0;
+        }
+        for (int32_t e = rp[r]; e < rp[r + 1]; ++e) {
+            const int c = ci[e];
+            const int i = owner[c];
+            int64_t q = s0;
+            while (q + 1 < s1 && rs_sub[q] != i) ++q;
+            const DevSub& d = subs[i];
+            const double* vr = V + d.v_off + (int64_t)(c - d.begin) * d.m;
+            double* z = Z + rs_zoff[q];
+            const double av = v[e];
+            for (int a = 0; a < d.m; ++a) z[a] += av * vr[a];
+        }
+    }
+}
+
+// Step 2, one CTA per pair (j, i) of subdomains that meet in a row:
+// E(c_off_j + b, c_off_i + a) = sum over the owned rows r of j with a slot for i of V_j(r, b) u_{r,i}(a)
+__global__ void __launch_bounds__(256) coarse_pairs_kernel(const int32_t* __restrict__ pair_j,
+                                                           const int32_t* __restrict__ pair_i,
+                                                           const int64_t* __restrict__ pair_ptr,
+                                                           const int32_t* __restrict__ pair_rl,
+                                                           const int64_t* __restrict__ pair_zoff,
+                                                           const DevSub* __restrict__ subs,
+                                                           const double* __restrict__ V, const double* __restrict__ Z,
+                                                           int64_t n0, double* __restrict__ E)
+{
+    const int p = blockIdx.x;
+    const DevSub dj = subs[pair_j[p]], di = subs[pair_i[p]];
+    const int mj = dj.m, mi = di.m;
+    const int64_t q0 = pair_ptr[p], q1 = pair_ptr[p + 1];
+    for (int o = threadIdx.x; o < mj * mi; o += blockDim.x) {
+        const int b = o / mi, a = o % mi;
+        double acc = 0.0;
+        for (int64_t q = q0; q < q1; ++q) acc += V[dj.v_off + (int64_t)pair_rl[q] * mj + b] * Z[pair_zoff[q] + a];
+        E[(dj.c_off + b) * n0 + di.c_off + a] = acc;
+    }
+}
+
 int grid_for(int64_t work, int bs)
 {
     const int64_t g = (work + bs - 1) / bs;
@@ -594,6 +649,18 @@ void launch_gather_values(cudaStream_t st, int64_t count, const int64_t* src, co
 void launch_row_sums(cudaStream_t st, int64_t n, const int32_t* rp, const double* v, double* out)
 {
     row_sums_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, rp, v, out);
+}
+
+void launch_coarse_direct(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                          const int32_t* owner, const int64_t* rs_ptr, const int32_t* rs_sub, const int64_t* rs_zoff,
+                          int npairs, const int32_t* pair_j, const int32_t* pair_i, const int64_t* pair_ptr,
+                          const int32_t* pair_rl, const int64_t* pair_zoff, const DevSub* subs, const double* V,
+                          double* Z, int64_t n0, double* E)
+{
+    coarse_z_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, rp, ci, v, owner, rs_ptr, rs_sub, rs_zoff, subs, V, Z);
+    cudaMemsetAsync(E, 0, (size_t)n0 * n0 * sizeof(double), st);
+    if (npairs > 0)
+        coarse_pairs_kernel<<<npairs, 256, 0, st>>>(pair_j, pair_i, pair_ptr, pair_rl, pair_zoff, subs, V, Z, n0, E);
 }
 
 void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y)

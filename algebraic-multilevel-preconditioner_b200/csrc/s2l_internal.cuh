@@ -246,7 +246,14 @@ void launch_refactor_blocks(cudaStream_t st, int64_t nblocks, const int64_t* bof
 template <typename Real>
 void launch_gather_values(cudaStream_t st, int64_t count, const int64_t* src, const double* F, Real* out);
 void launch_row_sums(cudaStream_t st, int64_t n, const int32_t* rp, const double* v, double* out);
-// coarse matrix refresh: unit block, E columns
+// coarse matrix for a boolean partition of unity, directly: per row the products with the bases of
+// the subdomains owning its columns (Z), then one block of E per pair of subdomains meeting in a row
+void launch_coarse_direct(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                          const int32_t* owner, const int64_t* rs_ptr, const int32_t* rs_sub, const int64_t* rs_zoff,
+                          int npairs, const int32_t* pair_j, const int32_t* pair_i, const int64_t* pair_ptr,
+                          const int32_t* pair_rl, const int64_t* pair_zoff, const DevSub* subs, const double* V,
+                          double* Z, int64_t n0, double* E);
+// coarse matrix refresh, general partition of unity: unit block, E columns
 void launch_unit_block(cudaStream_t st, int64_t n0, int c0, double* Y);
 void launch_scatter_columns(cudaStream_t st, int64_t n0, int c0, const double* C, double* E);
 
