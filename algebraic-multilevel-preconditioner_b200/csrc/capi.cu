@@ -237,15 +237,17 @@ struct s2l_setup {
         std::vector<int64_t> d_off;
         size_t bytes = 0;        // device bytes of the plan
         // dense tails factorized and inverted on RF_STREAMS streams at once, each with its cuSOLVER
-        // and cuBLAS handles, factorization workspace and inversion buffer
-        static constexpr int RF_STREAMS = 4;
+        // handle and its factorization and inversion workspaces
+        static constexpr int RF_STREAMS = 8;
         cudaStream_t tstream[RF_STREAMS] = {};
         cudaEvent_t tev[RF_STREAMS + 1] = {};
-        cublasHandle_t tblas[RF_STREAMS] = {};
         cusolverDnHandle_t tsolver[RF_STREAMS] = {};
         double* swork[RF_STREAMS] = {};
-        double* B[RF_STREAMS] = {};
         int lwork = 0;
+        void* iwork[RF_STREAMS] = {};         // triangular inversion workspace (device) per stream
+        double* B[RF_STREAMS] = {};           // copy of an LU tail whose unit lower triangle is inverted
+        size_t iwork_bytes = 0;
+        std::vector<char> ihost[RF_STREAMS];  // and its host part
         int* info = nullptr;  // per subdomain: the dense tail factorization's status
         // coarse matrix refresh: E and its inversion, 16 unit vectors through prolong / A / restrict
         double *E = nullptr, *Einv = nullptr, *Y = nullptr, *X = nullptr, *AX = nullptr, *cpart = nullptr,
@@ -2532,27 +2534,34 @@ int s2l_gpu_setup_end(s2l_setup* s)
             constexpr int NS = s2l_setup::Refac::RF_STREAMS;
             for (int q = 0; q < NS; ++q) {
                 CUDA_OK(s, cudaStreamCreateWithFlags(&R.tstream[q], cudaStreamNonBlocking));
-                if (cublasCreate(&R.tblas[q]) != CUBLAS_STATUS_SUCCESS) {
-                    R.tblas[q] = nullptr;
-                    return s->fail(S2L_ERR_CUDA, "cublasCreate failed");
-                }
                 if (cusolverDnCreate(&R.tsolver[q]) != CUSOLVER_STATUS_SUCCESS) {
                     R.tsolver[q] = nullptr;
                     return s->fail(S2L_ERR_CUDA, "cusolverDnCreate failed");
                 }
-                if (cublasSetStream(R.tblas[q], R.tstream[q]) != CUBLAS_STATUS_SUCCESS ||
-                    cusolverDnSetStream(R.tsolver[q], R.tstream[q]) != CUSOLVER_STATUS_SUCCESS)
+                if (cusolverDnSetStream(R.tsolver[q], R.tstream[q]) != CUSOLVER_STATUS_SUCCESS)
                     return s->fail(S2L_ERR_CUDA, "cannot bind the tail handles to their streams");
-                RET_IF(dbl(&R.B[q], (size_t)smax * smax));
             }
             for (auto& e : R.tev) CUDA_OK(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             int l1 = 0, l2 = 0;
-            if (cusolverDnDpotrf_bufferSize(R.tsolver[0], CUBLAS_FILL_MODE_UPPER, smax, R.B[0], smax, &l1) !=
+            size_t id1 = 0, ih1 = 0, id2 = 0, ih2 = 0;
+            if (cusolverDnDpotrf_bufferSize(R.tsolver[0], CUBLAS_FILL_MODE_UPPER, smax, R.S, smax, &l1) !=
                     CUSOLVER_STATUS_SUCCESS ||
-                cusolverDnDgetrf_bufferSize(R.tsolver[0], smax, smax, R.B[0], smax, &l2) != CUSOLVER_STATUS_SUCCESS)
+                cusolverDnDgetrf_bufferSize(R.tsolver[0], smax, smax, R.S, smax, &l2) != CUSOLVER_STATUS_SUCCESS ||
+                cusolverDnXtrtri_bufferSize(R.tsolver[0], CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, smax,
+                                            CUDA_R_64F, R.S, smax, &id1, &ih1) != CUSOLVER_STATUS_SUCCESS ||
+                cusolverDnXtrtri_bufferSize(R.tsolver[0], CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_UNIT, smax,
+                                            CUDA_R_64F, R.S, smax, &id2, &ih2) != CUSOLVER_STATUS_SUCCESS)
                 return s->fail(S2L_ERR_CUDA, "cuSOLVER workspace query failed");
             R.lwork = std::max(std::max(l1, l2), 1);
-            for (int q = 0; q < NS; ++q) RET_IF(dbl(&R.swork[q], (size_t)R.lwork));
+            R.iwork_bytes = std::max<size_t>(std::max(id1, id2), 16);
+            for (int q = 0; q < NS; ++q) {
+                RET_IF(dbl(&R.swork[q], (size_t)R.lwork));
+                RET_IF(dev_alloc(s, &R.iwork[q], R.iwork_bytes));
+                bool any_lu = false;
+                for (char l : R.llt) any_lu = any_lu || !l;
+                if (any_lu) RET_IF(dbl(&R.B[q], (size_t)smax * smax));
+                R.ihost[q].assign(std::max<size_t>(std::max(ih1, ih2), 16), 0);
+            }
             int l3 = 0;
             if (cusolverDnDgetrf_bufferSize(R.tsolver[0], (int)n0, (int)n0, R.E, (int)n0, &l3) != CUSOLVER_STATUS_SUCCESS)
                 return s->fail(S2L_ERR_CUDA, "cuSOLVER workspace query failed");
@@ -2642,7 +2651,6 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
     }
     if (s->setup_stream) cudaStreamDestroy(s->setup_stream);
     for (int q = 0; q < s2l_setup::Refac::RF_STREAMS; ++q) {
-        if (s->rf.tblas[q]) cublasDestroy(s->rf.tblas[q]);
         if (s->rf.tsolver[q]) cusolverDnDestroy(s->rf.tsolver[q]);
         if (s->rf.tstream[q]) cudaStreamDestroy(s->rf.tstream[q]);
     }
@@ -2770,35 +2778,30 @@ int refactor_commit_factors(s2l_setup* s, cudaStream_t st)
     }
     launch_gather_values<Real>(st, R.nlts, R.lts_src, R.F, (Real*)s->d_lts_val);
     launch_gather_values<Real>(st, R.nust, R.ust_src, R.F, (Real*)s->d_ust_val);
-    // dense tail inverses: triangular solves against the identity with the factored tails, the
-    // subdomains spread over the tail streams.  Row-major lower Lt = column-major upper (the
-    // Cholesky factor, or U'), row-major upper Ut = column-major lower (L', unit diagonal); for
-    // L L^T, Ut^-1 = (Lt^-1)^T.
+    // dense tail inverses: the triangles of each factored tail inverted (cusolverDnXtrtri), the
+    // subdomains spread over the tail streams.  Column-major, the tail holds the Cholesky factor
+    // U_c (upper; row-major that is the lower L) or U' (upper) and L' (strict lower, unit diagonal);
+    // their inverses are row-major Lt^-1 (lower) and Ut^-1 (strict upper, unit diagonal).  U_c / U'
+    // is inverted in place, L' in a copy of the tail (the two inversions do not share storage).
     constexpr int NS = s2l_setup::Refac::RF_STREAMS;
     RET_IF(tails_fork(s, st));
-    const double one = 1.0;
     for (int i = 0; i < nsub; ++i) {
         const int sz = R.sz[i];
         if (sz == 0) continue;
         const int q = i % NS;
         cudaStream_t sq = R.tstream[q];
-        const double* Si = R.S + R.d_off[i];
-        for (int f = 0; f < 2; ++f) {
-            double* B = R.B[q];
-            void* dst = f == 0 ? s->d_linv : s->d_uinv;
-            if (f == 1 && R.llt[i]) {
-                launch_transpose_to<Real>(sq, R.B[q], sz, (Real*)dst + R.d_off[i]);
-                continue;
-            }
-            launch_identity(sq, B, sz);
-            if (cublasDtrsm(R.tblas[q], CUBLAS_SIDE_LEFT, f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER,
-                            CUBLAS_OP_N, f == 0 ? CUBLAS_DIAG_NON_UNIT : CUBLAS_DIAG_UNIT, sz, sz, &one, Si, sz, B,
-                            sz) != CUBLAS_STATUS_SUCCESS)
-                return s->fail(S2L_ERR_CUDA, "cublasDtrsm failed");
-            if (s->real == S2L_REAL_F32) launch_to_float(sq, B, (float*)dst + R.d_off[i], (int64_t)sz * sz);
-            else CUDA_OK(s, cudaMemcpyAsync((double*)dst + R.d_off[i], B, (size_t)sz * sz * sizeof(double),
-                                            cudaMemcpyDeviceToDevice, sq));
+        double* Si = R.S + R.d_off[i];
+        double* Bq = R.llt[i] ? nullptr : R.B[q];
+        if (Bq) CUDA_OK(s, cudaMemcpyAsync(Bq, Si, (size_t)sz * sz * sizeof(double), cudaMemcpyDeviceToDevice, sq));
+        for (int f = 0; f < (Bq ? 2 : 1); ++f) {
+            if (cusolverDnXtrtri(R.tsolver[q], f == 0 ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER,
+                                 f == 0 ? CUBLAS_DIAG_NON_UNIT : CUBLAS_DIAG_UNIT, sz, CUDA_R_64F, f == 0 ? Si : Bq,
+                                 sz, R.iwork[q], R.iwork_bytes, R.ihost[q].data(), R.ihost[q].size(), R.info + i) !=
+                CUSOLVER_STATUS_SUCCESS)
+                return s->fail(S2L_ERR_CUDA, "cusolverDnXtrtri failed");
         }
+        launch_tail_inverses<Real>(sq, Si, Bq, sz, R.llt[i], (Real*)s->d_linv + R.d_off[i],
+                                   (Real*)s->d_uinv + R.d_off[i]);
     }
     return tails_join(s, st);
 }

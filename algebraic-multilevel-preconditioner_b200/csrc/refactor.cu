@@ -309,20 +309,22 @@ __global__ void __launch_bounds__(256) gather_tails_kernel(const RefactorArgs a)
     }
 }
 
-// dst (Real) = src^T, s x s
+// The solve's dense tail inverses from inverted triangles (row-major views of column-major
+// results): S holds the inverted upper triangle (column-major), i.e. row-major lower part with the
+// diagonal = Lt^-1; B (LU only) holds the inverted unit lower triangle, row-major strict upper part
+// = Ut^-1 with a unit diagonal; for L L^T Ut^-1 = (Lt^-1)^T.  The other triangles are 0.
 template <typename Real>
-__global__ void transpose_to_kernel(const double* __restrict__ src, int s, Real* __restrict__ dst)
+__global__ void tail_inverses_kernel(const double* __restrict__ S, const double* __restrict__ B, int s, int llt,
+                                     Real* __restrict__ linv, Real* __restrict__ uinv)
 {
-    __shared__ double t[32][33];
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int y = threadIdx.y; y < 32; y += 8) {
-        const int r = by + y, c = bx + threadIdx.x;
-        if (r < s && c < s) t[y][threadIdx.x] = src[(int64_t)r * s + c];
-    }
-    __syncthreads();
-    for (int y = threadIdx.y; y < 32; y += 8) {
-        const int r = bx + y, c = by + threadIdx.x;
-        if (r < s && c < s) dst[(int64_t)r * s + c] = (Real)t[threadIdx.x][y];
+    const int64_t total = (int64_t)s * s;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / s), c = (int)(e % s);
+        linv[e] = (Real)(c <= r ? S[e] : 0.0);
+        double u;
+        if (llt) u = c >= r ? S[(int64_t)c * s + r] : 0.0;
+        else u = c > r ? B[e] : (c == r ? 1.0 : 0.0);
+        uinv[e] = (Real)u;
     }
 }
 
@@ -599,10 +601,9 @@ void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a)
 }
 
 template <typename Real>
-void launch_transpose_to(cudaStream_t st, const double* src, int s, Real* dst)
+void launch_tail_inverses(cudaStream_t st, const double* S, const double* B, int s, int llt, Real* linv, Real* uinv)
 {
-    const dim3 g((s + 31) / 32, (s + 31) / 32);
-    transpose_to_kernel<Real><<<g, dim3(32, 8), 0, st>>>(src, s, dst);
+    tail_inverses_kernel<Real><<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(S, B, s, llt, linv, uinv);
 }
 
 void launch_identity(cudaStream_t st, double* M, int s)
@@ -689,8 +690,8 @@ template void launch_refactor_blocks<double>(cudaStream_t, int64_t, const int64_
 template void launch_refactor_blocks<float>(cudaStream_t, int64_t, const int64_t*, const int64_t*, const int64_t*,
                                             const int64_t*, const int64_t*, const uint8_t*, const int64_t*,
                                             const uint8_t*, const int64_t*, const double*, float*, float*);
-template void launch_transpose_to<double>(cudaStream_t, const double*, int, double*);
-template void launch_transpose_to<float>(cudaStream_t, const double*, int, float*);
+template void launch_tail_inverses<double>(cudaStream_t, const double*, const double*, int, int, double*, double*);
+template void launch_tail_inverses<float>(cudaStream_t, const double*, const double*, int, int, float*, float*);
 template void launch_gather_values<double>(cudaStream_t, int64_t, const int64_t*, const double*, double*);
 template void launch_gather_values<float>(cudaStream_t, int64_t, const int64_t*, const double*, float*);
 

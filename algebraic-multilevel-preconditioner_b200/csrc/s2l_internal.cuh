@@ -229,7 +229,7 @@ void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a);
 void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a);
 void launch_identity(cudaStream_t st, double* M, int s);
 template <typename Real>
-void launch_transpose_to(cudaStream_t st, const double* src, int s, Real* dst);
+void launch_tail_inverses(cudaStream_t st, const double* S, const double* B, int s, int llt, Real* linv, Real* uinv);
 template <typename Real>
 void launch_refactor_sweep_values(cudaStream_t st, int nsub, const int64_t* fbase, const double* F,
                                   const int64_t* wtask, const int64_t* wslot, const int64_t* went,
