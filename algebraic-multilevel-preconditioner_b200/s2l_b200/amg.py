@@ -1,0 +1,178 @@
+"""AMG hierarchy of a local matrix: the inexact local solver of the reference (``--local-approx amg``).
+
+The reference approximates A_ii^-1 by one V-cycle of AMGCL (``src/linalg/inexact_solver.cpp:45-178``:
+``amgcl::amg`` with the builtin backend, smoothed aggregation, Gauss-Seidel smoothing, one cycle
+from x = 0 per application, coarsest level at most ``coarse_enough`` unknowns solved directly).
+AMGCL (MIT licence, vendored with the reference under ``external/amgcl``) is third-party code; this
+module restates its published setup algorithm for the configuration the reference builds:
+
+* strength of connection (``coarsening/plain_aggregates.hpp``): off-diagonal a_ij is strong when
+  eps^2 a_ii a_jj < a_ij^2, eps = 0.08 (a float) on the finest level, halved on every coarser one
+  (``coarsening/smoothed_aggregation.hpp``);
+* plain aggregation, in row order: an unaggregated row with strong connections starts an
+  aggregate with its strong neighbours (taking them from earlier aggregates too), then the
+  unaggregated strong neighbours of those neighbours; rows without strong connections belong to
+  no aggregate; empty aggregates are squeezed out;
+* tentative prolongation P0(i, aggregate(i)) = 1;
+* smoothing P = (I - omega D_F^-1 A_F) P0 with omega = 2/3 and the filtered matrix A_F (weak
+  off-diagonal entries added to the diagonal): P(i, :) = sum over the strong and diagonal entries
+  of row i, in column order, of ((1 - omega) on the diagonal, -omega a_ij / d_F(i) elsewhere) P0(j, :);
+* R = P^T, coarse operator R (A P) by row-wise sparse products (``coarsening/detail/galerkin.hpp``,
+  ``detail/spgemm.hpp``: Saad's algorithm, the accumulation order of scipy's product too);
+* levels are added while a level has more than ``coarse_enough`` rows; the last one is solved
+  directly (AMGCL's skyline LU; any exact solve agrees to rounding).
+
+The cycle itself (Gauss-Seidel, residual, restriction, coarse correction) is applied by the solve
+phase; its CPU restatement is the oracle's ``oracle_amg_apply``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+EPS_STRONG = np.float32(0.08)
+OMEGA = 1.0 * (2.0 / 3.0)  # relax (1) times 2/3: no spectral-radius estimate in the reference's setup
+
+
+@dataclass
+class AmgLevel:
+    A: sp.csr_matrix                  # operator of the level (sorted columns)
+    P: sp.csr_matrix | None = None    # prolongation from the next level (rows of this level)
+    R: sp.csr_matrix | None = None    # restriction to the next level
+
+
+@dataclass
+class AmgHierarchy:
+    levels: list = field(default_factory=list)
+    coarse: np.ndarray | None = None  # the coarsest operator, dense, solved directly (None: smoothed only)
+    sweeps: int = 1
+
+    @property
+    def n(self) -> int:
+        return self.levels[0].A.shape[0] if self.levels else self.coarse.shape[0]
+
+    def nnz(self) -> int:
+        """Stored entries of every operator and transfer matrix (what one V-cycle reads)."""
+        t = 0
+        for l in self.levels:
+            t += l.A.nnz + (l.P.nnz + l.R.nnz if l.P is not None else 0)
+        if self.coarse is not None:
+            t += self.coarse.size
+        return int(t)
+
+
+def _sorted_csr(M) -> sp.csr_matrix:
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    return M
+
+
+def _aggregates(A: sp.csr_matrix, eps: np.float32):
+    """Strong connections (per stored entry) and aggregate ids (-2: none) and their count."""
+    n = A.shape[0]
+    rp, ci, va = A.indptr, A.indices, A.data
+    dia = A.diagonal()
+    eps2 = float(np.float32(eps) * np.float32(eps))  # the product of two floats, in float
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    strong = (ci != rows) & ((eps2 * dia[rows]) * dia[ci] < va * va)
+    UNDEF, REMOVED = -1, -2
+    has_strong = np.add.reduceat(strong.astype(np.int64), rp[:-1]) if n else np.zeros(0, np.int64)
+    has_strong[np.diff(rp) == 0] = 0
+    aid = np.where(has_strong > 0, UNDEF, REMOVED).astype(np.int64)
+    count = 0
+    rp_l, ci_l, st_l = rp.tolist(), ci.tolist(), strong.tolist()
+    aid_l = aid.tolist()
+    for i in range(n):
+        if aid_l[i] != UNDEF:
+            continue
+        cur = count
+        count += 1
+        aid_l[i] = cur
+        neib = []
+        for j in range(rp_l[i], rp_l[i + 1]):
+            c = ci_l[j]
+            if st_l[j] and aid_l[c] != REMOVED:
+                aid_l[c] = cur
+                neib.append(c)
+        for c in neib:
+            for j in range(rp_l[c], rp_l[c + 1]):
+                cc = ci_l[j]
+                if st_l[j] and aid_l[cc] == UNDEF:
+                    aid_l[cc] = cur
+    aid = np.asarray(aid_l, dtype=np.int64)
+    if count == 0:
+        return strong, aid, 0
+    used = np.zeros(count, dtype=np.int64)
+    used[aid[aid >= 0]] = 1
+    cs = np.cumsum(used)
+    if cs[-1] < count:  # aggregates emptied by later ones: renumber without gaps
+        aid = np.where(aid >= 0, cs[np.maximum(aid, 0)] - 1, aid)
+        count = int(cs[-1])
+    return strong, aid, count
+
+
+def _transfer(A: sp.csr_matrix, eps: np.float32):
+    """(P, R) of one level, or None when no row has a strong connection."""
+    n = A.shape[0]
+    strong, aid, count = _aggregates(A, eps)
+    if count == 0:
+        return None
+    rp, ci, va = A.indptr, A.indices, A.data
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    keep = (ci == rows) | strong                      # entries of the filtered matrix's pattern
+    # filtered diagonal: the diagonal plus the weak entries, summed in row order
+    weak_or_diag = ~strong
+    dia_f = np.zeros(n)
+    for i in range(n):  # sequential sum in the row's order (as the reference's loop)
+        s = 0.0
+        for j in range(rp[i], rp[i + 1]):
+            if weak_or_diag[j]:
+                s += va[j]
+        dia_f[i] = s
+    scale = np.where(dia_f != 0.0, -OMEGA * (1.0 / np.where(dia_f != 0.0, dia_f, 1.0)), 0.0)
+    vals = np.where(ci == rows, 1.0 - OMEGA, scale[rows] * va)
+    target = aid[ci]
+    sel = (keep & (target >= 0)).tolist()
+    vals_l, tgt_l = vals.tolist(), target.tolist()
+    # P(i, aggregate) = sum of vals over the selected entries of row i, in row order
+    pp, pc, pv = [0], [], []
+    for i in range(n):
+        acc = {}
+        for j in range(rp[i], rp[i + 1]):
+            if sel[j]:
+                t = tgt_l[j]
+                acc[t] = acc[t] + vals_l[j] if t in acc else vals_l[j]
+        for t in sorted(acc):
+            pc.append(t)
+            pv.append(acc[t])
+        pp.append(len(pc))
+    P = sp.csr_matrix((np.asarray(pv), np.asarray(pc, dtype=np.int64), np.asarray(pp, dtype=np.int64)),
+                      shape=(n, count))
+    R = _sorted_csr(P.T)
+    return P, R
+
+
+def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1) -> AmgHierarchy:
+    """The reference's AMG setup for one local matrix (see the module docstring)."""
+    A = _sorted_csr(sp.csr_matrix(A, dtype=np.float64))
+    H = AmgHierarchy(sweeps=int(sweeps))
+    eps = EPS_STRONG
+    direct = True
+    while A is not None and A.shape[0] > coarse_enough:
+        lvl = AmgLevel(A)
+        H.levels.append(lvl)
+        tr = _transfer(A, eps)
+        eps = np.float32(eps * np.float32(0.5))
+        if tr is None:  # nothing to aggregate: the last level is smoothed only
+            A = None
+            direct = False
+            break
+        lvl.P, lvl.R = tr
+        A = _sorted_csr(lvl.R @ (A @ lvl.P))
+    if A is None or A.shape[0] > coarse_enough:
+        direct = False
+    if direct:
+        H.coarse = A.toarray()
+    return H

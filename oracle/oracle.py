@@ -53,6 +53,9 @@ def load():
                                  C.c_double, C.POINTER(OResult)]
     lib.oracle_bicgstab.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                     C.POINTER(OResult)]
+    lib.oracle_dense_lu.restype = C.c_int
+    lib.oracle_dense_lu.argtypes = [C.c_int, vp, vp]
+    lib.oracle_amg_apply.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.oracle_refactor.restype = C.c_int
     lib.oracle_refactor.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     _lib = lib
@@ -235,3 +238,45 @@ def refactor_setup(st, A_new):
         subs.append(dataclasses.replace(s, factor=refactor_factor(s.factor, Aii), Aii=Aii))
     E = coarse_matrix(A_new, subs, st.offsets) if st.n0 else st.E
     return dataclasses.replace(st, A=A_new, subdomains=subs, E=E)
+
+
+def amg_apply(H, b):
+    """One V-cycle of the AMG hierarchy H (s2l_b200.amg.AmgHierarchy) from x = 0, on the CPU
+    (``oracle_amg_apply``: the reference's inexact local solve)."""
+    lib = load()
+    nlev = len(H.levels)
+    keep = []
+
+    def arr(x, dt):
+        a = np.ascontiguousarray(x, dtype=dt)
+        keep.append(a)
+        return a
+
+    def ptrs(mats, part, dt):
+        out = (C.c_void_p * max(nlev, 1))()
+        for l, M in enumerate(mats):
+            if M is None:
+                out[l] = None
+                continue
+            a = arr(getattr(M, part), dt)
+            out[l] = a.ctypes.data
+        return out
+
+    A = [l.A for l in H.levels]
+    P = [l.P for l in H.levels]
+    R = [l.R for l in H.levels]
+    nc = 0 if H.coarse is None else H.coarse.shape[0]
+    nrow = arr([M.shape[0] for M in A] + [nc], np.int32)
+    CLU = arr(H.coarse if H.coarse is not None else np.zeros((1, 1)), np.float64).copy()
+    keep.append(CLU)
+    piv = arr(np.zeros(max(nc, 1)), np.int32)
+    if nc and not lib.oracle_dense_lu(nc, _a(CLU), _a(piv)):
+        raise ValueError("singular coarse AMG level")
+    n = H.n
+    b = arr(b, np.float64)
+    x = np.zeros(n)
+    lib.oracle_amg_apply(nlev, H.sweeps, _a(nrow), ptrs(A, "indptr", np.int64), ptrs(A, "indices", np.int32),
+                         ptrs(A, "data", np.float64), ptrs(P, "indptr", np.int64), ptrs(P, "indices", np.int32),
+                         ptrs(P, "data", np.float64), ptrs(R, "indptr", np.int64), ptrs(R, "indices", np.int32),
+                         ptrs(R, "data", np.float64), _a(CLU), _a(piv), _a(b), _a(x))
+    return x

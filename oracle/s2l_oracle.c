@@ -777,3 +777,140 @@ int oracle_refactor(int n, int kind, const int64_t *Ap, const int32_t *Ai, const
     free(in);
     return rc;
 }
+
+/* ---------------------------------------------------------------------------------------- */
+/* One AMG V-cycle from x = 0: the reference's inexact local solve (--local-approx amg,
+ * src/linalg/inexact_solver.cpp:89-95, AMGCL amg::apply / amg::cycle with serial Gauss-Seidel,
+ * relaxation/gauss_seidel.hpp).  Levels 0 .. nlev-1 carry A_l (CSR, sorted columns) and, except a
+ * last smoothed-only level, P_l (n_l x n_{l+1}) and R_l; the coarsest operator, when present, is
+ * solved with its LU (row-major, partial pivoting, from oracle_dense_lu).
+ *   level l: `sweeps` forward Gauss-Seidel sweeps on A_l x = f (x_i = (f_i - sum_{j != i} a_ij x_j)
+ *            / a_ii in increasing i, updated values used at once), t = f - A_l x, f_{l+1} = R_l t,
+ *            x_{l+1} = cycle(l + 1), x += P_l x_{l+1}, `sweeps` backward sweeps (decreasing i);
+ *   coarsest: x = A_c^-1 f;  a last level without coarse solve: forward then backward sweeps.
+ * Arrays: Ap/Ai/Ax[l], Pp/Pi/Px[l], Rp/Ri/Rx[l], nrow[l] (nlev + 1 sizes: nrow[nlev] = coarse
+ * size, 0 without a coarse solve). */
+typedef struct {
+    int nlev, sweeps;
+    const int *nrow;
+    const int64_t *const *Ap, *const *Pp, *const *Rp;
+    const int32_t *const *Ai, *const *Pi, *const *Ri;
+    const double *const *Ax, *const *Px, *const *Rx;
+    const double *CLU; /* coarse LU, row-major, partial pivoting */
+    const int *Cpiv;
+} OAmg;
+
+static void gs_sweep(int n, const int64_t *p, const int32_t *ci, const double *v, const double *f, double *x,
+                     int forward)
+{
+    for (int q = 0; q < n; ++q) {
+        const int i = forward ? q : n - 1 - q;
+        double D = 1.0, X = f[i];
+        for (int64_t e = p[i]; e < p[i + 1]; ++e) {
+            if (ci[e] == i) D = v[e];
+            else X -= v[e] * x[ci[e]];
+        }
+        x[i] = (1.0 / D) * X;
+    }
+}
+
+static void lu_solve(int n, const double *LU, const int *piv, const double *b, double *x)
+{
+    for (int i = 0; i < n; ++i) x[i] = b[i];
+    for (int k = 0; k < n; ++k) {
+        const int p = piv[k];
+        if (p != k) {
+            const double t = x[k];
+            x[k] = x[p];
+            x[p] = t;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        double s = x[i];
+        for (int k = 0; k < i; ++k) s -= LU[(size_t)i * n + k] * x[k];
+        x[i] = s;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = x[i];
+        for (int k = i + 1; k < n; ++k) s -= LU[(size_t)i * n + k] * x[k];
+        x[i] = s / LU[(size_t)i * n + i];
+    }
+}
+
+static void amg_cycle(const OAmg *h, int l, const double *f, double *x)
+{
+    if (l == h->nlev) { /* coarsest, solved directly */
+        lu_solve(h->nrow[l], h->CLU, h->Cpiv, f, x);
+        return;
+    }
+    const int n = h->nrow[l];
+    const int last_smoothed = (l == h->nlev - 1) && h->nrow[h->nlev] == 0;
+    for (int s = 0; s < h->sweeps; ++s) gs_sweep(n, h->Ap[l], h->Ai[l], h->Ax[l], f, x, 1);
+    if (last_smoothed) {
+        for (int s = 0; s < h->sweeps; ++s) gs_sweep(n, h->Ap[l], h->Ai[l], h->Ax[l], f, x, 0);
+        return;
+    }
+    const int nc = h->nrow[l + 1];
+    double *t = (double *)malloc((size_t)(n ? n : 1) * sizeof(double));
+    double *fc = (double *)malloc((size_t)(nc ? nc : 1) * sizeof(double));
+    double *xc = (double *)calloc((size_t)(nc ? nc : 1), sizeof(double));
+    for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int64_t e = h->Ap[l][i]; e < h->Ap[l][i + 1]; ++e) s += h->Ax[l][e] * x[h->Ai[l][e]];
+        t[i] = f[i] - s;
+    }
+    for (int i = 0; i < nc; ++i) {
+        double s = 0.0;
+        for (int64_t e = h->Rp[l][i]; e < h->Rp[l][i + 1]; ++e) s += h->Rx[l][e] * t[h->Ri[l][e]];
+        fc[i] = s;
+    }
+    amg_cycle(h, l + 1, fc, xc);
+    for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int64_t e = h->Pp[l][i]; e < h->Pp[l][i + 1]; ++e) s += h->Px[l][e] * xc[h->Pi[l][e]];
+        x[i] += s;
+    }
+    for (int s = 0; s < h->sweeps; ++s) gs_sweep(n, h->Ap[l], h->Ai[l], h->Ax[l], f, x, 0);
+    free(t);
+    free(fc);
+    free(xc);
+}
+
+/* LU with partial pivoting of a dense row-major n x n matrix, in place; 0 if singular. */
+int oracle_dense_lu(int n, double *A, int *piv)
+{
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        double best = fabs(A[(size_t)k * n + k]);
+        for (int i = k + 1; i < n; ++i)
+            if (fabs(A[(size_t)i * n + k]) > best) {
+                best = fabs(A[(size_t)i * n + k]);
+                p = i;
+            }
+        if (best == 0.0) return 0;
+        piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < n; ++j) {
+                const double t = A[(size_t)k * n + j];
+                A[(size_t)k * n + j] = A[(size_t)p * n + j];
+                A[(size_t)p * n + j] = t;
+            }
+        for (int i = k + 1; i < n; ++i) {
+            const double l = A[(size_t)i * n + k] / A[(size_t)k * n + k];
+            A[(size_t)i * n + k] = l;
+            for (int j = k + 1; j < n; ++j) A[(size_t)i * n + j] -= l * A[(size_t)k * n + j];
+        }
+    }
+    return 1;
+}
+
+void oracle_amg_apply(int nlev, int sweeps, const int *nrow, const int64_t *const *Ap, const int32_t *const *Ai,
+                      const double *const *Ax, const int64_t *const *Pp, const int32_t *const *Pi,
+                      const double *const *Px, const int64_t *const *Rp, const int32_t *const *Ri,
+                      const double *const *Rx, const double *CLU, const int *Cpiv, const double *b, double *x)
+{
+    OAmg h = {nlev, sweeps, nrow, Ap, Pp, Rp, Ai, Pi, Ri, Ax, Px, Rx, CLU, Cpiv};
+    const int n = nlev > 0 ? nrow[0] : nrow[0];
+    for (int i = 0; i < n; ++i) x[i] = 0.0;
+    amg_cycle(&h, 0, b, x);
+}

@@ -4,6 +4,8 @@ Mirrors the reference's own test pattern (test/test_preconditioner.cpp:104-192):
 apply on the same partition is compared with a dense matrix assembled from the global matrix, the
 subdomain index sets, D_i and V_i, at 1e-9 there; the oracle must do far better (1e-12).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -170,3 +172,25 @@ def test_oracle_refactorization_reports_bad_pivots():
     idx = s.l2g()
     with pytest.raises(ValueError):
         refactor_factor(s.factor, -st.A[idx][:, idx])
+
+
+AMG_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden")) if f.startswith("amg_"))
+
+
+@pytest.mark.parametrize("fixture", AMG_GOLDEN)
+def test_amg_hierarchy_and_cycle_pinned_on_the_reference(fixture):
+    """The AMG local solver (--local-approx amg): the setup restatement (s2l_b200.amg) plus the
+    oracle's V-cycle reproduce the reference's own solve() (AMGCL, run by
+    tests/golden/make_amg_golden.py) to rounding, on 1 to 3 levels, 1 or 2 sweeps."""
+    import scipy.sparse as sp
+    from oracle.oracle import amg_apply
+    from s2l_b200.amg import build_hierarchy
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture))
+    n = g["indptr"].size - 1
+    A = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
+    H = build_hierarchy(A, coarse_enough=int(g["coarse_enough"]), sweeps=int(g["sweeps"]))
+    levels = str(g["info"]).split("[")[1].split(" levels")[0]
+    assert len(H.levels) + (H.coarse is not None) == int(levels)
+    for v, ref in zip(g["vecs"], g["out"]):
+        x = amg_apply(H, v)
+        assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
