@@ -11,7 +11,7 @@ REPO = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 GPU_LIB = os.path.join(LIB_DIR, "libs2l_gpu.so")
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["kernels.cu", "refactor.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "refactor.cu", "amg.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,154 @@
+// AMG local solves (the reference's --local-approx amg, src/linalg/inexact_solver.cpp:45-178): one
+// V-cycle from x = 0 per subdomain, every subdomain at once.
+//
+// Layout: level l of every subdomain that has it is concatenated into the level space l (subdomain
+// i at lvl_off[l][i]); A_l, R_l (rows in level l + 1) and P_l (rows in level l) are block-diagonal
+// CSR matrices over these spaces, so a residual, a restriction or a prolongation is one launch for
+// all subdomains.  Gauss-Seidel sweeps run one CTA per subdomain over wavefronts of its rows (rows
+// of one wavefront read no row updated in the same wavefront, and no row of a later wavefront has
+// been updated yet), a thread per row, each row summed in column order as the serial sweep does.
+// The coarsest level of a subdomain is solved with its dense inverse.
+#include "s2l_internal.cuh"
+
+#include <algorithm>
+
+namespace {
+
+int amg_grid(int64_t work, int bs)
+{
+    const int64_t g = (work + bs - 1) / bs;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+// x(i) = (f(i) - sum_{j != i} A(i, j) x(j)) / A(i, i) over the rows of each wavefront in turn
+__global__ void __launch_bounds__(512) gs_sweep_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                       const double* __restrict__ v, const double* __restrict__ f,
+                                                       double* x, const int32_t* __restrict__ sched,
+                                                       const int64_t* __restrict__ wf_ptr,
+                                                       const int32_t* __restrict__ sub_wf)
+{
+    const int b = blockIdx.x;
+    for (int w = sub_wf[b]; w < sub_wf[b + 1]; ++w) {
+        for (int64_t k = wf_ptr[w] + threadIdx.x; k < wf_ptr[w + 1]; k += blockDim.x) {
+            const int i = sched[k];
+            double D = 1.0, X = f[i];
+            for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
+                const int c = ci[e];
+                if (c == i) D = v[e];
+                else X -= v[e] * x[c];
+            }
+            x[i] = (1.0 / D) * X;
+        }
+        __syncthreads();
+    }
+}
+
+// y = M x (beta = 0) or y += M x (beta = 1), one thread per row
+__global__ void csr_mv_kernel(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                              const double* __restrict__ v, const double* __restrict__ x, double* __restrict__ y,
+                              int accumulate)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int64_t e = rp[i]; e < rp[i + 1]; ++e) s += v[e] * x[ci[e]];
+        y[i] = accumulate ? y[i] + s : s;
+    }
+}
+
+// t = f - A x
+__global__ void csr_residual_kernel(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                    const double* __restrict__ v, const double* __restrict__ f,
+                                    const double* __restrict__ x, double* __restrict__ t)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int64_t e = rp[i]; e < rp[i + 1]; ++e) s += v[e] * x[ci[e]];
+        t[i] = f[i] - s;
+    }
+}
+
+// x_c = C^-1 f_c for every subdomain whose coarsest level is this one (one CTA each)
+__global__ void coarse_inverse_kernel(const int32_t* __restrict__ c_sub_off, const int32_t* __restrict__ c_n,
+                                      const int64_t* __restrict__ c_inv_off, const double* __restrict__ Cinv,
+                                      const double* __restrict__ f, double* __restrict__ x)
+{
+    const int b = blockIdx.x;
+    const int n = c_n[b];
+    const int64_t o = c_sub_off[b];
+    const double* M = Cinv + c_inv_off[b];
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < n; ++c) s += M[(int64_t)r * n + c] * f[o + c];
+        x[o + r] = s;
+    }
+}
+
+// level-0 right-hand side: f(p) = in(l2g(p)) (global input) or local_in(p - off) (one subdomain)
+__global__ void amg_gather_kernel(int64_t n, const int32_t* __restrict__ l2g, const double* __restrict__ in,
+                                  const double* __restrict__ local_in, int64_t lo, int64_t hi,
+                                  double* __restrict__ f)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        if (local_in) f[p] = (p >= lo && p < hi) ? local_in[p - lo] : 0.0;
+        else f[p] = in[l2g[p]];
+    }
+}
+
+// outputs of the level-0 solution: owned rows to out (+ base), the local space, or one subdomain
+__global__ void amg_scatter_kernel(int64_t n, const int32_t* __restrict__ out_idx, const double* __restrict__ x,
+                                   const double* __restrict__ base, double* __restrict__ out, int mode, int64_t lo,
+                                   int64_t hi)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        if (mode == 0) {
+            const int32_t g = out_idx[p];
+            if (g >= 0) out[g] = base ? x[p] + base[g] : x[p];
+        } else if (mode == 1) {
+            out[p] = x[p];
+        } else if (p >= lo && p < hi) {
+            out[p - lo] = x[p];
+        }
+    }
+}
+
+}  // namespace
+
+namespace s2l {
+
+void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
+                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf)
+{
+    if (nsub_lvl > 0) gs_sweep_kernel<<<nsub_lvl, 512, 0, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf);
+}
+
+void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
+                   double* y, int accumulate)
+{
+    if (n > 0) csr_mv_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, y, accumulate);
+}
+
+void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,
+                         const double* f, const double* x, double* t)
+{
+    if (n > 0) csr_residual_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, f, x, t);
+}
+
+void launch_coarse_inverse(cudaStream_t st, int ncoarse, const int32_t* c_sub_off, const int32_t* c_n,
+                           const int64_t* c_inv_off, const double* Cinv, const double* f, double* x)
+{
+    if (ncoarse > 0) coarse_inverse_kernel<<<ncoarse, 256, 0, st>>>(c_sub_off, c_n, c_inv_off, Cinv, f, x);
+}
+
+void launch_amg_gather(cudaStream_t st, int64_t n, const int32_t* l2g, const double* in, const double* local_in,
+                       int64_t lo, int64_t hi, double* f)
+{
+    if (n > 0) amg_gather_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, l2g, in, local_in, lo, hi, f);
+}
+
+void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const double* x, const double* base,
+                        double* out, int mode, int64_t lo, int64_t hi)
+{
+    if (n > 0) amg_scatter_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, out_idx, x, base, out, mode, lo, hi);
+}
+
+}  // namespace s2l

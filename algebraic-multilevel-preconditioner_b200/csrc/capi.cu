@@ -87,6 +87,13 @@ struct HostSub {
     std::vector<double> d;
     int m = 0;
     std::vector<double> V;  // column-major n_local x m
+    // AMG local solver instead of factors (s2l_gpu_add_subdomain_amg): smoothed levels and the
+    // coarsest operator (row-major, amg_nc x amg_nc; none when amg_nc is 0)
+    bool amg = false;
+    int amg_sweeps = 1;
+    std::vector<HostCsr> amgA, amgP, amgR;
+    int amg_nc = 0;
+    std::vector<double> amgC;
     int n_local() const { return n_owned + n_ghost; }
 };
 
@@ -130,6 +137,7 @@ struct s2l_setup {
     int nsub = 0;
     int one_level = 0, coarse = 0, pou = 0;
     int real = -1;
+    int local_kind = -1;  // 0: exact factors (s2l_gpu_add_subdomain), 1: AMG (s2l_gpu_add_subdomain_amg)
     bool ended = false;
     cudaStream_t setup_stream = nullptr;  // uploads and the tail inversion
 
@@ -209,6 +217,28 @@ struct s2l_setup {
     unsigned prof_mask = 0;              // s2l_gpu_profile_enable: inherited by new workspaces
 
     std::atomic<int> pending{0};  // asynchronous solves queued or running on this setup
+
+    // AMG local solvers (s2l_gpu_add_subdomain_amg): level spaces and block-diagonal operators
+    struct AmgDev {
+        bool on = false;
+        int nlev = 0;                       // level spaces (smoothed levels and coarsest ones)
+        int sweeps = 1;
+        std::vector<int64_t> nspace;        // per level space: rows
+        std::vector<int64_t> voff;          // per level space: offset of its vectors in a workspace block
+        int64_t vtotal = 0;                 // doubles of one of the three work vectors (f, x, t)
+        std::vector<int64_t*> Arp, Rrp, Prp;
+        std::vector<int32_t*> Aci, Rci, Pci;
+        std::vector<double*> Av, Rv, Pv;
+        std::vector<int> nsmooth;           // per level: subdomains smoothed on it (CTAs of a sweep)
+        std::vector<int32_t*> fsched, bsched, fsub, bsub;
+        std::vector<int64_t*> fwf, bwf;
+        std::vector<int> ncoarse;           // per level: subdomains whose coarsest level it is
+        std::vector<int32_t*> c_off, c_n;
+        std::vector<int64_t*> c_inv;
+        double* Cinv = nullptr;
+        int32_t* out_idx = nullptr;         // local-space row -> owned global row, or -1
+        double cycle_bytes = 0.0;           // algorithmic bytes of one V-cycle of every subdomain
+    } amgd;
 
     // numeric refactorization (setup option "refactor"): factor patterns and the maps from them to
     // the solve layout, kept on the device (RefactorArgs)
@@ -303,6 +333,7 @@ struct s2l_work {
            *d_xk = nullptr, *d_u = nullptr;
     double *d_rh = nullptr, *d_p = nullptr, *d_v = nullptr, *d_s = nullptr, *d_t = nullptr, *d_yb = nullptr;
     double* d_coef = nullptr;
+    double* d_amg = nullptr;  // AMG local solves: f, x, t of every level space
     // block solves (K interleaved right-hand sides), allocated on first use
     struct Block {
         int K = 0, m = -1;
@@ -1092,11 +1123,62 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
 
 // Local solves of every subdomain (only_sub < 0) or of one: in -> (mode 0) out[owned] (+ base),
 // (mode 1) ylocal, (mode 2: local input/output of subdomain only_sub) out.
+// The AMG local solves of every subdomain: one V-cycle from x = 0 (the reference's
+// --local-approx amg), with the outputs of run_local_solve's modes.
+int amg_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
+                    const double* local_in)
+{
+    s2l_setup* s = w->s;
+    const auto& G = s->amgd;
+    cudaStream_t st = w->stream;
+    const int L = G.nlev;
+    double* f = w->d_amg;
+    double* x = w->d_amg + G.vtotal;
+    double* t = w->d_amg + 2 * G.vtotal;
+    int64_t lo = 0, hi = 0;
+    if (only_sub >= 0) {
+        lo = s->h_subs[only_sub].loc_off;
+        hi = lo + s->h_subs[only_sub].n_local;
+    }
+    launch_amg_gather(st, G.nspace[0], s->d_l2g, in, mode == 2 ? local_in : nullptr, lo, hi, f);
+    CUDA_OK(w, cudaMemsetAsync(x, 0, (size_t)G.vtotal * sizeof(double), st));
+    int launched = 2;
+    for (int l = 0; l < L; ++l) {
+        double *fl = f + G.voff[l], *xl = x + G.voff[l], *tl = t + G.voff[l];
+        for (int k = 0; k < G.sweeps; ++k)
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.fsched[l], G.fwf[l], G.fsub[l]);
+        launch_coarse_inverse(st, G.ncoarse[l], G.c_off[l], G.c_n[l], G.c_inv[l], G.Cinv, f + G.voff[l], xl);
+        launched += G.sweeps + 1;
+        if (l + 1 < L) {
+            launch_csr_residual(st, G.nspace[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, tl);
+            launch_csr_mv(st, G.nspace[l + 1], G.Rrp[l], G.Rci[l], G.Rv[l], tl, f + G.voff[l + 1], 0);
+            launched += 2;
+        }
+    }
+    // the deepest level space: its smoothed subdomains have no coarser level (backward sweeps now)
+    for (int k = 0; k < G.sweeps; ++k)
+        launch_gs_sweep(st, G.nsmooth[L - 1], G.Arp[L - 1], G.Aci[L - 1], G.Av[L - 1], f + G.voff[L - 1],
+                        x + G.voff[L - 1], G.bsched[L - 1], G.bwf[L - 1], G.bsub[L - 1]);
+    for (int l = L - 2; l >= 0; --l) {
+        double *fl = f + G.voff[l], *xl = x + G.voff[l];
+        launch_csr_mv(st, G.nspace[l], G.Prp[l], G.Pci[l], G.Pv[l], x + G.voff[l + 1], xl, 1);
+        for (int k = 0; k < G.sweeps; ++k)
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.bsched[l], G.bwf[l], G.bsub[l]);
+        launched += G.sweeps + 1;
+    }
+    launch_amg_scatter(st, G.nspace[0], G.out_idx, x, base, mode == 1 ? w->d_ylocal : out, mode, lo, hi);
+    w->launches += launched + 1;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("AMG local solve launch: ") + cudaGetErrorString(e));
+    return S2L_OK;
+}
+
 int run_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
                     const double* local_in)
 {
     s2l_setup* s = w->s;
     Prof pr(w, PC_SOLVE);
+    if (s->amgd.on) return amg_local_solve(w, in, base, out, mode, only_sub, local_in);
     const int nb = only_sub >= 0 ? 1 : s->nsub;
     int32_t* sub_list = nullptr;
     int tr0 = 0, trn = s->tr_first_h[s->nsub], us0 = 0, usn = s->us_first_h[s->nsub];
@@ -1595,6 +1677,7 @@ int work_create(s2l_setup* s, s2l_work** out)
     A(reinterpret_cast<void**>(&w->d_out), (size_t)std::max<int64_t>(s->n, s->max_nl) * sizeof(double));
     A(reinterpret_cast<void**>(&w->d_part), (size_t)S2L_NB_RED * S2L_MAX_RED_COLS * sizeof(double));
     A(reinterpret_cast<void**>(&w->d_red), 512 * sizeof(double));
+    if (s->amgd.on) A(reinterpret_cast<void**>(&w->d_amg), (size_t)std::max<int64_t>(3 * s->amgd.vtotal, 1) * sizeof(double));
     if (rc == S2L_OK && cudaMallocHost(&w->h_red, 512 * sizeof(double)) != cudaSuccess)
         rc = s->fail(S2L_ERR_OOM, "cannot allocate pinned host memory");
     if (rc == S2L_OK && cudaMemsetAsync(w->d_err, 0, 16, w->stream) != cudaSuccess) rc = S2L_ERR_CUDA;
@@ -1817,6 +1900,8 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
     if (real_type != S2L_REAL_F64 && real_type != S2L_REAL_F32) return s->fail(S2L_ERR_BADARG, "unknown real type");
     if (s->real >= 0 && s->real != real_type)
         return s->fail(S2L_ERR_BADARG, "all subdomains must store their factors in the same precision");
+    if (s->local_kind == 1) return s->fail(S2L_ERR_BADARG, "a setup's subdomains all use factors or all AMG");
+    s->local_kind = 0;
     if (factor_kind < S2L_FACTOR_LU || factor_kind > S2L_FACTOR_LDLT) return s->fail(S2L_ERR_BADARG, "unknown factor kind");
     if (!D || !perm_in || !perm_out || !L_rowptr || !L_col || !L_val || (n_ghost && !ghosts))
         return s->fail(S2L_ERR_BADARG, "null array");
@@ -1881,6 +1966,83 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
     return S2L_OK;
 }
 
+int s2l_gpu_add_subdomain_amg(s2l_setup* s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t* ghosts,
+                              const double* D, int nlev, int sweeps, const int32_t* nrow,
+                              const int64_t* const* A_rowptr, const int32_t* const* A_col, const double* const* A_val,
+                              const int64_t* const* P_rowptr, const int32_t* const* P_col, const double* const* P_val,
+                              const int64_t* const* R_rowptr, const int32_t* const* R_col, const double* const* R_val,
+                              int n_coarse, const double* coarse, int m, const double* V)
+{
+    if (!s) return S2L_ERR_BADARG;
+    if (s->ended) return s->fail(S2L_ERR_STATE, "add_subdomain_amg after setup_end");
+    if (i < 0 || i >= s->nsub) return s->fail(S2L_ERR_BADARG, "subdomain index out of range");
+    if (n_owned <= 0 || n_ghost < 0) return s->fail(S2L_ERR_BADARG, "n_owned must be > 0 and n_ghost >= 0");
+    if (begin < 0 || begin + n_owned > s->n) return s->fail(S2L_ERR_BADARG, "owned range outside [0, n)");
+    if (s->local_kind == 0) return s->fail(S2L_ERR_BADARG, "a setup's subdomains all use factors or all AMG");
+    if (s->real == S2L_REAL_F32) return s->fail(S2L_ERR_BADARG, "AMG local solvers run in FP64");
+    if (!D || (n_ghost && !ghosts)) return s->fail(S2L_ERR_BADARG, "null array");
+    if (nlev < 0 || nlev > 32 || sweeps < 1 || sweeps > 16 || n_coarse < 0)
+        return s->fail(S2L_ERR_BADARG, "bad AMG hierarchy: levels in [0, 32], sweeps in [1, 16]");
+    if (m < 0 || m > S2L_MAX_RED_COLS || (m > 0 && !V)) return s->fail(S2L_ERR_BADARG, "bad coarse basis (m <= 128)");
+    const int nl = n_owned + n_ghost;
+    if (nlev == 0 && n_coarse != nl) return s->fail(S2L_ERR_BADARG, "a hierarchy without levels needs a coarse solve of n_local rows");
+    if (nlev > 0 && (!nrow || nrow[0] != nl)) return s->fail(S2L_ERR_BADARG, "the first AMG level must have n_local rows");
+    if (n_coarse > 0 && !coarse) return s->fail(S2L_ERR_BADARG, "null coarse operator");
+    s->local_kind = 1;
+    s->real = S2L_REAL_F64;
+    HostSub& h = s->hs[i];
+    h = HostSub();
+    h.begin = begin;
+    h.n_owned = n_owned;
+    h.n_ghost = n_ghost;
+    h.ghosts.assign(ghosts, ghosts + n_ghost);
+    for (int k = 0; k < n_ghost; ++k) {
+        if (ghosts[k] < 0 || ghosts[k] >= s->n) return s->fail(S2L_ERR_BADARG, "ghost id out of range");
+        if (ghosts[k] >= begin && ghosts[k] < begin + n_owned) return s->fail(S2L_ERR_BADARG, "ghost is an owned row");
+        if (k && ghosts[k] <= ghosts[k - 1]) return s->fail(S2L_ERR_BADARG, "ghosts must be sorted and unique");
+    }
+    h.D.assign(D, D + nl);
+    h.amg = true;
+    h.amg_sweeps = sweeps;
+    auto copy = [&](HostCsr& dst, int rows, int cols, const int64_t* rp, const int32_t* ci, const double* v) -> int {
+        if (!rp || !ci || !v || rp[0] != 0) return s->fail(S2L_ERR_BADARG, "bad AMG level matrix");
+        dst.rp.assign(rp, rp + rows + 1);
+        const int64_t nz = rp[rows];
+        dst.ci.assign(ci, ci + nz);
+        dst.v.assign(v, v + nz);
+        for (int r = 0; r < rows; ++r) {
+            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "AMG level matrix: rowptr not monotone");
+            for (int64_t e = rp[r]; e < rp[r + 1]; ++e)
+                if (ci[e] < 0 || ci[e] >= cols || (e > rp[r] && ci[e] <= ci[e - 1]))
+                    return s->fail(S2L_ERR_BADARG, "AMG level matrix: columns out of range or not sorted");
+        }
+        return S2L_OK;
+    };
+    h.amgA.resize(nlev);
+    h.amgP.resize(nlev);
+    h.amgR.resize(nlev);
+    for (int l = 0; l < nlev; ++l) {
+        if (nrow[l] <= 0) return s->fail(S2L_ERR_BADARG, "an AMG level without rows");
+        RET_IF(copy(h.amgA[l], nrow[l], nrow[l], A_rowptr[l], A_col[l], A_val[l]));
+        const int next = l + 1 < nlev ? nrow[l + 1] : n_coarse;
+        if (next > 0) {  // the transfer operators to the next level (none after a last smoothed-only level)
+            RET_IF(copy(h.amgP[l], nrow[l], next, P_rowptr[l], P_col[l], P_val[l]));
+            RET_IF(copy(h.amgR[l], next, nrow[l], R_rowptr[l], R_col[l], R_val[l]));
+        } else if (l + 1 < nlev) {
+            return s->fail(S2L_ERR_BADARG, "only the last AMG level may have no coarser level");
+        }
+    }
+    h.amg_nc = n_coarse;
+    if (n_coarse > 0) h.amgC.assign(coarse, coarse + (size_t)n_coarse * n_coarse);
+    h.m = m;
+    if (m) h.V.assign(V, V + (size_t)nl * m);
+    h.pin.resize(nl);
+    h.pout.resize(nl);
+    for (int k = 0; k < nl; ++k) h.pin[k] = h.pout[k] = k;
+    h.set = true;
+    return S2L_OK;
+}
+
 int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E)
 {
     if (!s) return S2L_ERR_BADARG;
@@ -1894,6 +2056,191 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
     return S2L_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Gauss-Seidel wavefronts of one matrix (rows in sweep order: increasing when forward): a row
+// comes after every earlier row it reads or that reads it, so a wavefront's rows see exactly the
+// values a serial sweep would.  Returns per row its wavefront.
+std::vector<int32_t> gs_wavefronts(const HostCsr& A, int n, bool forward)
+{
+    std::vector<int32_t> wf(n, 0);
+    for (int q = 0; q < n; ++q) {
+        const int r = forward ? q : n - 1 - q;
+        auto earlier = [&](int c) { return forward ? c < r : c > r; };
+        int w = wf[r];
+        for (int64_t e = A.rp[r]; e < A.rp[r + 1]; ++e)
+            if (earlier(A.ci[e])) w = std::max(w, wf[A.ci[e]] + 1);
+        wf[r] = w;
+        for (int64_t e = A.rp[r]; e < A.rp[r + 1]; ++e) {
+            const int c = A.ci[e];
+            if (c != r && !earlier(c)) wf[c] = std::max(wf[c], w + 1);  // c reads r's new value later
+        }
+    }
+    return wf;
+}
+
+// Device data of the AMG local solvers: per level space the block-diagonal A, R, P, the sweeps'
+// wavefronts and the coarsest levels' inverses.
+int amg_build(s2l_setup* s)
+{
+    auto& G = s->amgd;
+    const int nsub = s->nsub;
+    int L = 0;
+    for (int i = 0; i < nsub; ++i) {
+        const HostSub& h = s->hs[i];
+        L = std::max(L, (int)h.amgA.size() + (h.amg_nc > 0 ? 1 : 0));
+        G.sweeps = h.amg_sweeps;
+    }
+    for (int i = 0; i < nsub; ++i)
+        if (s->hs[i].amg_sweeps != G.sweeps) return s->fail(S2L_ERR_BADARG, "all AMG hierarchies need the same sweeps");
+    G.nlev = L;
+    auto rows_at = [&](const HostSub& h, int l) -> int64_t {
+        const int nl = (int)h.amgA.size();
+        if (l < nl) return (int64_t)h.amgA[l].rp.size() - 1;
+        return (l == nl && h.amg_nc > 0) ? h.amg_nc : 0;
+    };
+    std::vector<std::vector<int64_t>> off(L + 1, std::vector<int64_t>(nsub + 1, 0));
+    G.nspace.assign(L, 0);
+    G.voff.assign(L + 1, 0);
+    for (int l = 0; l < L; ++l) {
+        for (int i = 0; i < nsub; ++i) off[l][i + 1] = off[l][i] + rows_at(s->hs[i], l);
+        G.nspace[l] = off[l][nsub];
+        G.voff[l + 1] = G.voff[l] + G.nspace[l];
+    }
+    G.vtotal = G.voff[L];
+    if (L == 0 || G.nspace[0] != s->nloc) return s->fail(S2L_ERR_BADARG, "the AMG first levels must span the local space");
+    G.Arp.assign(L, nullptr), G.Rrp.assign(L, nullptr), G.Prp.assign(L, nullptr);
+    G.Aci.assign(L, nullptr), G.Rci.assign(L, nullptr), G.Pci.assign(L, nullptr);
+    G.Av.assign(L, nullptr), G.Rv.assign(L, nullptr), G.Pv.assign(L, nullptr);
+    G.fsched.assign(L, nullptr), G.bsched.assign(L, nullptr), G.fsub.assign(L, nullptr), G.bsub.assign(L, nullptr);
+    G.fwf.assign(L, nullptr), G.bwf.assign(L, nullptr);
+    G.nsmooth.assign(L, 0), G.ncoarse.assign(L, 0);
+    G.c_off.assign(L, nullptr), G.c_n.assign(L, nullptr), G.c_inv.assign(L, nullptr);
+    std::vector<double> cinv_all;
+    double bytes = 0.0;
+    const double sw = (double)G.sweeps;
+    for (int l = 0; l < L; ++l) {
+        // concatenated A_l (rows of space l), P_l (rows of space l), R_l (rows of space l + 1)
+        std::vector<int64_t> arp(1, 0), prp(1, 0), rrp(1, 0);
+        std::vector<int32_t> aci, pci, rci;
+        std::vector<double> av, pv, rv;
+        std::vector<int32_t> fs, bs, fsub(1, 0), bsub(1, 0), coff, cn;
+        std::vector<int64_t> fwf(1, 0), bwf(1, 0), cinvoff;
+        for (int i = 0; i < nsub; ++i) {
+            const HostSub& h = s->hs[i];
+            const int nlv = (int)h.amgA.size();
+            const int64_t o = off[l][i], on = l + 1 < L ? off[l + 1][i] : 0;
+            if (l < nlv) {
+                const HostCsr& A = h.amgA[l];
+                const int n = (int)A.rp.size() - 1;
+                for (int r = 0; r < n; ++r) {
+                    for (int64_t e = A.rp[r]; e < A.rp[r + 1]; ++e) {
+                        aci.push_back((int32_t)(o + A.ci[e]));
+                        av.push_back(A.v[e]);
+                    }
+                    arp.push_back((int64_t)aci.size());
+                }
+                const bool transfer = !h.amgP[l].rp.empty();
+                for (int r = 0; r < n; ++r) {
+                    if (transfer)
+                        for (int64_t e = h.amgP[l].rp[r]; e < h.amgP[l].rp[r + 1]; ++e) {
+                            pci.push_back((int32_t)(on + h.amgP[l].ci[e]));
+                            pv.push_back(h.amgP[l].v[e]);
+                        }
+                    prp.push_back((int64_t)pci.size());
+                }
+                if (transfer) {
+                    const int nr = (int)h.amgR[l].rp.size() - 1;
+                    for (int r = 0; r < nr; ++r) {
+                        for (int64_t e = h.amgR[l].rp[r]; e < h.amgR[l].rp[r + 1]; ++e) {
+                            rci.push_back((int32_t)(o + h.amgR[l].ci[e]));
+                            rv.push_back(h.amgR[l].v[e]);
+                        }
+                        rrp.push_back((int64_t)rci.size());
+                    }
+                    bytes += (double)(h.amgP[l].ci.size() + h.amgR[l].ci.size()) * 12.0;
+                }
+                // sweeps' wavefronts (rows as level-space indices)
+                for (int f = 0; f < 2; ++f) {
+                    const std::vector<int32_t> wf = gs_wavefronts(A, n, f == 0);
+                    int nw = 0;
+                    for (int32_t x : wf) nw = std::max(nw, x + 1);
+                    std::vector<int64_t> cnt(nw + 1, 0);
+                    for (int32_t x : wf) ++cnt[x + 1];
+                    for (int k = 0; k < nw; ++k) cnt[k + 1] += cnt[k];
+                    std::vector<int32_t> ord(n);
+                    std::vector<int64_t> nx(cnt.begin(), cnt.end() - 1);
+                    for (int r = 0; r < n; ++r) ord[nx[wf[r]]++] = (int32_t)(o + r);
+                    std::vector<int32_t>& sched = f == 0 ? fs : bs;
+                    std::vector<int64_t>& wptr = f == 0 ? fwf : bwf;
+                    std::vector<int32_t>& sub = f == 0 ? fsub : bsub;
+                    const int64_t base = (int64_t)sched.size();
+                    sched.insert(sched.end(), ord.begin(), ord.end());
+                    for (int k = 0; k < nw; ++k) wptr.push_back(base + cnt[k + 1]);
+                    sub.push_back((int32_t)(wptr.size() - 1));
+                }
+                G.nsmooth[l] += 1;
+                bytes += (double)A.ci.size() * 12.0 * (2.0 * sw + 1.0) + (double)n * 8.0 * 6.0;
+            } else {
+                const int64_t n = rows_at(h, l);  // a coarsest level: no rows of A_l, P_l
+                for (int64_t r = 0; r < n; ++r) {
+                    arp.push_back((int64_t)aci.size());
+                    prp.push_back((int64_t)pci.size());
+                }
+                if (l == nlv && h.amg_nc > 0) {
+                    const int nc = h.amg_nc;
+                    std::vector<double> Cc = h.amgC, Ci;
+                    if (!dense_inverse(Cc, nc, Ci))
+                        return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": singular coarsest AMG level");
+                    coff.push_back((int32_t)o);
+                    cn.push_back(nc);
+                    cinvoff.push_back((int64_t)cinv_all.size());
+                    cinv_all.insert(cinv_all.end(), Ci.begin(), Ci.end());
+                    G.ncoarse[l] += 1;
+                    bytes += (double)nc * nc * 8.0;
+                }
+            }
+            // rows of space l + 1 that come from subdomains without a transfer at level l
+            if (l + 1 < L && !(l < nlv && !h.amgP[l].rp.empty()))
+                for (int64_t r = off[l + 1][i]; r < off[l + 1][i + 1]; ++r) rrp.push_back((int64_t)rci.size());
+        }
+        RET_IF(upload(s, &G.Arp[l], arp));
+        RET_IF(upload(s, &G.Aci[l], aci));
+        RET_IF(upload(s, &G.Av[l], av));
+        RET_IF(upload(s, &G.Prp[l], prp));
+        RET_IF(upload(s, &G.Pci[l], pci));
+        RET_IF(upload(s, &G.Pv[l], pv));
+        RET_IF(upload(s, &G.Rrp[l], rrp));
+        RET_IF(upload(s, &G.Rci[l], rci));
+        RET_IF(upload(s, &G.Rv[l], rv));
+        RET_IF(upload(s, &G.fsched[l], fs));
+        RET_IF(upload(s, &G.bsched[l], bs));
+        RET_IF(upload(s, &G.fwf[l], fwf));
+        RET_IF(upload(s, &G.bwf[l], bwf));
+        RET_IF(upload(s, &G.fsub[l], fsub));
+        RET_IF(upload(s, &G.bsub[l], bsub));
+        RET_IF(upload(s, &G.c_off[l], coff));
+        RET_IF(upload(s, &G.c_n[l], cn));
+        RET_IF(upload(s, &G.c_inv[l], cinvoff));
+    }
+    RET_IF(upload(s, &G.Cinv, cinv_all));
+    std::vector<int32_t> out_idx((size_t)s->nloc, -1);
+    for (int i = 0; i < nsub; ++i) {
+        const DevSub& d = s->h_subs[i];
+        for (int j = 0; j < d.n_owned; ++j) out_idx[(size_t)(d.loc_off + j)] = (int32_t)(d.begin + j);
+    }
+    RET_IF(upload(s, &G.out_idx, out_idx));
+    G.cycle_bytes = bytes;
+    G.on = true;
+    return S2L_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int s2l_gpu_setup_end(s2l_setup* s)
 {
     if (!s) return S2L_ERR_BADARG;
@@ -1901,6 +2248,8 @@ int s2l_gpu_setup_end(s2l_setup* s)
     if (!s->have_A) return s->fail(S2L_ERR_STATE, "set_matrix was not called");
     if (cudaSetDevice(s->ctx->device) != cudaSuccess) return S2L_ERR_CUDA;
     const int nsub = s->nsub;
+    if (s->local_kind == 1 && s->opt_refactor)
+        return s->fail(S2L_ERR_BADARG, "the option refactor needs exact local factors");
     // ---- ownership checks: contiguous ranges covering [0, n)
     {
         int64_t next = 0;
@@ -1960,6 +2309,10 @@ int s2l_gpu_setup_end(s2l_setup* s)
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
         const int nl = h.n_local();
+        if (h.amg) {  // no factors: the whole local space is "sparse part" without a tail
+            Ts[i] = nl;
+            continue;
+        }
         if (h.kind == S2L_FACTOR_LU) {
             Us[i] = std::move(h.U);
         } else {
@@ -2028,6 +2381,36 @@ int s2l_gpu_setup_end(s2l_setup* s)
         const HostCsr& U = Us[i];
         const int nl = h.n_local();
         max_nl = std::max(max_nl, nl);
+        if (h.amg) {  // AMG local solver: the local space in natural order, no sweeps or tails
+            s->tr_first_h[i] = (int)tr_sub.size();
+            s->us_first_h[i] = (int)us_sub.size();
+            d_off[i + 1] = d_off[i];
+            DevSub d{};
+            d.begin = h.begin;
+            d.loc_off = loc;
+            d.n_owned = h.n_owned;
+            d.n_local = nl;
+            d.T = nl;
+            d.tr_first = s->tr_first_h[i];
+            d.us_first = s->us_first_h[i];
+            d.d_off = d_off[i];
+            d.m = h.m;
+            d.v_rows = boolean ? h.n_owned : nl;
+            d.c_off = s->coarse != S2L_COARSE_NONE ? s->coff[i] : 0;
+            s->h_subs[i] = d;
+            for (int j = 0; j < nl; ++j) {
+                const int64_t g = j < h.n_owned ? h.begin + j : h.ghosts[j - h.n_owned];
+                l2g.push_back((int32_t)g);
+            }
+            for (int k = 0; k < nl; ++k) {
+                gin.push_back(l2g[loc + k]);
+                pin.push_back(k);
+                gout.push_back(k);
+            }
+            Dall.insert(Dall.end(), h.D.begin(), h.D.end());
+            loc += nl;
+            continue;
+        }
         const bool unitL = h.kind != S2L_FACTOR_LLT;
         const int T = Ts[i];
         const int sz = nl - T;
@@ -2429,6 +2812,10 @@ int s2l_gpu_setup_end(s2l_setup* s)
         RET_IF(upload(s, &s->d_Einv, Einv));
     }
     RET_IF(upload(s, &s->d_subs, s->h_subs));
+    if (s->local_kind == 1) {
+        RET_IF(amg_build(s));
+        s->solve_bytes = s->amgd.cycle_bytes + s->solve_vec_bytes;
+    }
     // refactorization plan and work buffers (after the coarse tiles: the refresh of E uses them)
     if (rfon) {
         auto& R = s->rf;
@@ -3653,6 +4040,7 @@ static int block_out(s2l_work* w, int K, int k, const double* src, int ptr_kind,
 static int block_width(s2l_setup* s, int k, int* K)
 {
     if (k < 1 || k > S2L_MAX_RHS) return s->fail(S2L_ERR_BADARG, "a block holds 1 to 16 right-hand sides");
+    if (s->amgd.on) return s->fail(S2L_ERR_BADARG, "block solves need exact local factors (AMG: one right-hand side per call)");
     *K = 1;
     while (*K < k) *K <<= 1;
     return S2L_OK;
@@ -3900,6 +4288,7 @@ static int gmres_block_run(s2l_setup* s, int k, const double* b, double* x, int 
     RET_IF(check_ready(s));
     if (!b || !x || !o || !res) return s->fail(S2L_ERR_BADARG, "null argument");
     if (k < 1 || k > S2L_MAX_RHS) return s->fail(S2L_ERR_BADARG, "a block holds 1 to 16 right-hand sides");
+    if (s->amgd.on) return s->fail(S2L_ERR_BADARG, "block solves need exact local factors (AMG: one right-hand side per call)");
     const int wb = block_width_best(s);
     if (k <= wb) return gmres_block_one(s, k, b, x, ptr_kind, o, res);
     const int64_t n = s->n;

@@ -217,6 +217,20 @@ void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, co
                            const double* y, double* out, double* plocal);
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 
+// AMG local solves (amg.cu)
+void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
+                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf);
+void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
+                   double* y, int accumulate);
+void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,
+                         const double* f, const double* x, double* t);
+void launch_coarse_inverse(cudaStream_t st, int ncoarse, const int32_t* c_sub_off, const int32_t* c_n,
+                           const int64_t* c_inv_off, const double* Cinv, const double* f, double* x);
+void launch_amg_gather(cudaStream_t st, int64_t n, const int32_t* l2g, const double* in, const double* local_in,
+                       int64_t lo, int64_t hi, double* f);
+void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const double* x, const double* base,
+                        double* out, int mode, int64_t lo, int64_t hi);
+
 // refactorization (refactor.cu)
 void launch_refactor_fill(cudaStream_t st, int64_t count, const int64_t* src, const int64_t* dst, const double* val,
                           double* F);

@@ -34,7 +34,7 @@ EXPORTED = [
     "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
     "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block", "s2l_gpu_update_matrix",
-    "s2l_gpu_refactor",
+    "s2l_gpu_refactor", "s2l_gpu_add_subdomain_amg",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -113,6 +113,8 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_apply_block": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
         "s2l_gpu_update_matrix": ([vp, vp, C.c_int], C.c_int),
         "s2l_gpu_refactor": ([vp, vp, C.c_int], C.c_int),
+        "s2l_gpu_add_subdomain_amg": ([vp, C.c_int, C.c_int64, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, vp,
+                                       vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "s2l_gpu_gmres_block": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -250,6 +252,10 @@ class GpuSetup:
         ctx.check(lib.s2l_gpu_set_matrix(self.h, _p(rp, C.c_int64), _p(ci, C.c_int64), _p(av, C.c_double)))
         self.local_sizes = []
         for i, s in enumerate(st.subdomains):
+            if getattr(s, "amg", None) is not None:
+                ctx.check(self._add_amg(i, s, coarse))
+                self.local_sizes.append(s.n_local)
+                continue
             f = s.factor
             real = 1 if f.L.dtype == np.float32 else 0
             vt = np.float32 if real else np.float64
@@ -395,6 +401,42 @@ class GpuSetup:
         """New values of A (same pattern, renumbered CSR order); the preconditioner is kept."""
         v = np.ascontiguousarray(values, dtype=np.float64)
         self.ctx.check(self.lib.s2l_gpu_update_matrix(self.h, _vp(v), PTR_HOST))
+
+    def _add_amg(self, i, s, coarse):
+        """Subdomain i with its AMG hierarchy (s2l_gpu_add_subdomain_amg)."""
+        H = s.amg
+        keep = self._keep_amg = getattr(self, "_keep_amg", [])
+        nlev = len(H.levels)
+
+        def arr(x, dt):
+            a = np.ascontiguousarray(x, dtype=dt)
+            keep.append(a)
+            return a
+
+        def ptrs(mats, part, dt):
+            out = (C.c_void_p * max(nlev, 1))()
+            for l, M in enumerate(mats):
+                out[l] = arr(getattr(M, part), dt).ctypes.data if M is not None else None
+            keep.append(out)
+            return C.cast(out, C.c_void_p)
+
+        A = [l.A for l in H.levels]
+        P = [l.P for l in H.levels]
+        R = [l.R for l in H.levels]
+        nrow = arr([M.shape[0] for M in A] or [0], np.int32)
+        nc = 0 if H.coarse is None else H.coarse.shape[0]
+        Cm = arr(H.coarse if H.coarse is not None else np.zeros(1), np.float64)
+        gh = arr(s.ghosts, np.int64)
+        D = arr(s.D, np.float64)
+        m = s.V.shape[1] if coarse != "none" else 0
+        V = np.asfortranarray(s.V, dtype=np.float64) if m else np.zeros(1)
+        keep.append(V)
+        return self.lib.s2l_gpu_add_subdomain_amg(
+            self.h, i, int(s.begin), int(s.n_owned), int(gh.size), _vp(gh), _vp(D), nlev, int(H.sweeps), _vp(nrow),
+            ptrs(A, "indptr", np.int64), ptrs(A, "indices", np.int32), ptrs(A, "data", np.float64),
+            ptrs(P, "indptr", np.int64), ptrs(P, "indices", np.int32), ptrs(P, "data", np.float64),
+            ptrs(R, "indptr", np.int64), ptrs(R, "indices", np.int32), ptrs(R, "data", np.float64),
+            nc, _vp(Cm) if nc else None, m, _vp(V))
 
     def refactor(self, values):
         """New values of A (same pattern, renumbered CSR order, host array or a device pointer) and

@@ -58,6 +58,9 @@ class SchwarzOptions:
     orth_tol: float = 1e-10
     local_factorization: str = "auto"  # auto | lu | cholesky
     local_precision: str = "double"    # double | single
+    local_approx: str = "none"         # none (exact factors) | amg (one AMG V-cycle, --local-approx amg)
+    amg_coarse_enough: int = 500       # --amg-coarse-enough: largest coarsest AMG level
+    amg_sweeps: int = 1                # --amg-sweeps: Gauss-Seidel steps before / after the coarse correction
 
 
 @dataclass
@@ -111,6 +114,7 @@ class SubdomainData:
     factor: LocalFactor | None
     V: np.ndarray              # orthonormal coarse basis on Omega_i (n_i x m_i)
     Aii: sp.csr_matrix | None = None
+    amg: object = None         # AMG hierarchy (s2l_b200.amg.AmgHierarchy) when factor is None
 
     @property
     def n_local(self) -> int:
@@ -329,7 +333,11 @@ def factorize_local(Aii: sp.csr_matrix, symmetric: bool, request: str, precision
 
 def _subdomain_work(args):
     Aii, Atil, D, opts, symmetric, want_coarse = args
-    fac = factorize_local(Aii, symmetric, opts.local_factorization, opts.local_precision)
+    if opts.local_approx == "amg":
+        from .amg import build_hierarchy
+        fac = build_hierarchy(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps)
+    else:
+        fac = factorize_local(Aii, symmetric, opts.local_factorization, opts.local_precision)
     Z, info = (local_coarse_vectors(Aii, Atil, D, opts, symmetric) if want_coarse
                else (np.zeros((Aii.shape[0], 0)), {}))
     return fac, Z, info
@@ -440,7 +448,10 @@ def build_setup(A_orig: sp.csr_matrix, b_orig: np.ndarray, part: np.ndarray, nsu
         V = orth_basis(D[:, None] * Z, opts.orth_tol) if Z.shape[1] else np.zeros((Aii.shape[0], 0))
         if opts.pou == "boolean" and V.shape[1]:
             V[nI:, :] = 0.0
-        subs.append(SubdomainData(beg, nI, ghosts, D, fac, np.ascontiguousarray(V), Aii))
+        if opts.local_approx == "amg":
+            subs.append(SubdomainData(beg, nI, ghosts, D, None, np.ascontiguousarray(V), Aii, amg=fac))
+        else:
+            subs.append(SubdomainData(beg, nI, ghosts, D, fac, np.ascontiguousarray(V), Aii))
         ms.append(V.shape[1])
         infos.append(info)
     offsets = np.zeros(nsub + 1, dtype=np.int64)
@@ -448,7 +459,7 @@ def build_setup(A_orig: sp.csr_matrix, b_orig: np.ndarray, part: np.ndarray, nsu
     E = coarse_matrix(A, subs, offsets) if want_coarse else np.zeros((0, 0))
     st = Setup(A, b, ownership, subs, offsets, E, opts, symmetric, n2o, description)
     st.stats = {"n0": int(offsets[-1]), "m_min": int(min(ms)) if ms else 0, "m_max": int(max(ms)) if ms else 0,
-                "nnz_factors": int(sum(s.factor.nnz() for s in subs)),
+                "nnz_factors": int(sum(s.factor.nnz() if s.factor is not None else s.amg.nnz() for s in subs)),
                 "kernel_subdomains": int(sum(1 for i in infos if i.get("kernel_dim", 0) > 0))}
     return st
 

@@ -130,6 +130,24 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
                           const int64_t* U_rowptr, const int32_t* U_col, const void* U_val, const void* ldlt_d,
                           int m, const double* V);
 
+/* Subdomain i with the reference's inexact local solver instead of exact factors: one AMG V-cycle
+ * from x = 0 approximates A_ii^-1 (--local-approx amg, src/linalg/inexact_solver.cpp:45-178;
+ * AMGCL smoothed aggregation with Gauss-Seidel smoothing).  The hierarchy is built on the host and
+ * given level by level: nlev smoothed levels, level l with nrow[l] rows (nrow[0] = n_local) and
+ * its operator A_l (CSR, sorted columns), and unless it is a last level without a coarser one, P_l
+ * (nrow[l] x next) and R_l (next x nrow[l]) to the next level, whose size is nrow[l + 1] or, after
+ * the last smoothed level, n_coarse.  The coarsest level (n_coarse rows, row-major operator; 0 for
+ * none) is solved exactly.  A level is smoothed by `sweeps` forward Gauss-Seidel sweeps before the
+ * coarse correction and `sweeps` backward sweeps after it.  FP64; every subdomain of a setup uses
+ * the same kind of local solver and the same sweeps; block calls (s2l_gpu_apply_block,
+ * s2l_gpu_gmres_block) need factors.  Owned range, ghosts, D, m and V as for s2l_gpu_add_subdomain. */
+int s2l_gpu_add_subdomain_amg(s2l_setup* s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t* ghosts,
+                              const double* D, int nlev, int sweeps, const int32_t* nrow,
+                              const int64_t* const* A_rowptr, const int32_t* const* A_col, const double* const* A_val,
+                              const int64_t* const* P_rowptr, const int32_t* const* P_col, const double* const* P_val,
+                              const int64_t* const* R_rowptr, const int32_t* const* R_col, const double* const* R_val,
+                              int n_coarse, const double* coarse, int m, const double* V);
+
 /* Coarse matrix E = R0 A R0^T (n0 x n0, row-major) and coarse offsets (nsub+1 entries). */
 int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E);
 

@@ -56,6 +56,9 @@ def load():
     lib.oracle_dense_lu.restype = C.c_int
     lib.oracle_dense_lu.argtypes = [C.c_int, vp, vp]
     lib.oracle_amg_apply.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.oracle_add_subdomain_amg.restype = C.c_int
+    lib.oracle_add_subdomain_amg.argtypes = [vp, C.c_int, C.c_int64, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, vp,
+                                             vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int, vp, C.c_int, vp]
     lib.oracle_refactor.restype = C.c_int
     lib.oracle_refactor.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     _lib = lib
@@ -88,6 +91,10 @@ class OracleSetup:
         lib.oracle_set_matrix(self.h, _a(rp), _a(ci), _a(av))
         self.local_sizes = []
         for i, s in enumerate(st.subdomains):
+            if getattr(s, "amg", None) is not None:
+                self._add_amg(lib, i, s, coarse)
+                self.local_sizes.append(s.n_local)
+                continue
             f = s.factor
             single = 1 if f.L.dtype == np.float32 else 0
             vt = np.float32 if single else np.float64
@@ -113,6 +120,41 @@ class OracleSetup:
             E = np.ascontiguousarray(st.E, dtype=np.float64) if st.n0 else np.zeros(1)
             if not lib.oracle_set_coarse(self.h, int(st.n0), _a(off), _a(E)):
                 raise RuntimeError("oracle: singular coarse matrix")
+
+    def _add_amg(self, lib, i, s, coarse):
+        H = s.amg
+        nlev = len(H.levels)
+        keep = self._keep
+
+        def arr(x, dt):
+            a = np.ascontiguousarray(x, dtype=dt)
+            keep.append(a)
+            return a
+
+        def ptrs(mats, part, dt):
+            out = (C.c_void_p * max(nlev, 1))()
+            for l, M in enumerate(mats):
+                out[l] = arr(getattr(M, part), dt).ctypes.data if M is not None else None
+            keep.append(out)
+            return C.cast(out, C.c_void_p)
+
+        A = [l.A for l in H.levels]
+        P = [l.P for l in H.levels]
+        R = [l.R for l in H.levels]
+        nrow = arr([M.shape[0] for M in A] or [0], np.int32)
+        nc = 0 if H.coarse is None else H.coarse.shape[0]
+        Cm = arr(H.coarse if H.coarse is not None else np.zeros(1), np.float64)
+        m = s.V.shape[1] if coarse != "none" else 0
+        V = arr(np.asfortranarray(s.V).ravel(order="F") if m else np.zeros(1), np.float64)
+        ok = lib.oracle_add_subdomain_amg(
+            self.h, i, int(s.begin), int(s.n_owned), int(s.ghosts.size), _a(arr(s.ghosts, np.int64)),
+            _a(arr(s.D, np.float64)), nlev, int(H.sweeps), _a(nrow),
+            ptrs(A, "indptr", np.int64), ptrs(A, "indices", np.int32), ptrs(A, "data", np.float64),
+            ptrs(P, "indptr", np.int64), ptrs(P, "indices", np.int32), ptrs(P, "data", np.float64),
+            ptrs(R, "indptr", np.int64), ptrs(R, "indices", np.int32), ptrs(R, "data", np.float64),
+            nc, _a(Cm) if nc else None, m, _a(V))
+        if not ok:
+            raise RuntimeError("oracle: singular coarsest AMG level")
 
     def _v(self, f, x):
         x = np.ascontiguousarray(x, dtype=np.float64)

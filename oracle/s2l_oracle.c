@@ -40,6 +40,7 @@ typedef struct {
     int m;
     double *V;           /* n_local x m column-major */
     double *rloc, *yloc; /* work */
+    void *amg;           /* AMG local solver (oracle_add_subdomain_amg) instead of factors, or NULL */
 } OSub;
 
 typedef struct {
@@ -54,6 +55,9 @@ typedef struct {
     int *piv;
     double *c, *y, *x0, *w, *z1, *tmp;
 } OSetup;
+
+static void amg_local(const void *h, const double *b, double *x);
+static void amg_free(void *h);
 
 /* ---------------------------------------------------------------------------------------- */
 OSetup *oracle_setup_create(int64_t n, int nsub, int one_level, int coarse, int pou)
@@ -79,6 +83,7 @@ void oracle_setup_destroy(OSetup *s)
         OSub *q = &s->sub[i];
         free(q->l2g); free(q->D); free(q->pin); free(q->pout); free(q->Lp); free(q->Up); free(q->Li);
         free(q->Ui); free(q->Lx); free(q->Ux); free(q->d); free(q->V); free(q->rloc); free(q->yloc);
+        amg_free(q->amg);
     }
     free(s->sub); free(s->Ap); free(s->Ai); free(s->Ax); free(s->coff); free(s->ELU); free(s->piv);
     free(s->c); free(s->y); free(s->x0); free(s->w); free(s->z1); free(s->tmp);
@@ -278,6 +283,10 @@ static void local_solve_f(const OSub *q, const double *b, double *x, float *t)
 void oracle_local_solve(const OSetup *s, int i, const double *b, double *x)
 {
     const OSub *q = &s->sub[i];
+    if (q->amg) {
+        amg_local(q->amg, b, x);
+        return;
+    }
     if (q->single) {
         float *t = (float *)malloc((size_t)q->n_local * sizeof(float));
         local_solve_f(q, b, x, t);
@@ -913,4 +922,106 @@ void oracle_amg_apply(int nlev, int sweeps, const int *nrow, const int64_t *cons
     const int n = nlev > 0 ? nrow[0] : nrow[0];
     for (int i = 0; i < n; ++i) x[i] = 0.0;
     amg_cycle(&h, 0, b, x);
+}
+
+/* An owned copy of a hierarchy, for a subdomain of an OSetup (the reference's --local-approx amg). */
+typedef struct {
+    int nlev, sweeps;
+    int *nrow; /* nlev + 1 entries, the last the coarse size (0: none) */
+    int64_t **Ap, **Pp, **Rp;
+    int32_t **Ai, **Pi, **Ri;
+    double **Ax, **Px, **Rx;
+    double *CLU;
+    int *Cpiv;
+} OAmgOwn;
+
+static void *dupb(const void *p, size_t bytes)
+{
+    void *q = malloc(bytes ? bytes : 1);
+    if (bytes) memcpy(q, p, bytes);
+    return q;
+}
+
+static void amg_local(const void *hv, const double *b, double *x)
+{
+    const OAmgOwn *h = (const OAmgOwn *)hv;
+    oracle_amg_apply(h->nlev, h->sweeps, h->nrow, (const int64_t *const *)h->Ap, (const int32_t *const *)h->Ai,
+                     (const double *const *)h->Ax, (const int64_t *const *)h->Pp, (const int32_t *const *)h->Pi,
+                     (const double *const *)h->Px, (const int64_t *const *)h->Rp, (const int32_t *const *)h->Ri,
+                     (const double *const *)h->Rx, h->CLU, h->Cpiv, b, x);
+}
+
+static void amg_free(void *hv)
+{
+    OAmgOwn *h = (OAmgOwn *)hv;
+    if (!h) return;
+    for (int l = 0; l < h->nlev; ++l) {
+        free(h->Ap[l]); free(h->Ai[l]); free(h->Ax[l]);
+        free(h->Pp[l]); free(h->Pi[l]); free(h->Px[l]);
+        free(h->Rp[l]); free(h->Ri[l]); free(h->Rx[l]);
+    }
+    free(h->Ap); free(h->Ai); free(h->Ax); free(h->Pp); free(h->Pi); free(h->Px);
+    free(h->Rp); free(h->Ri); free(h->Rx); free(h->nrow); free(h->CLU); free(h->Cpiv);
+    free(h);
+}
+
+/* Subdomain i with the AMG local solver (arguments as s2l_gpu_add_subdomain_amg).  Returns 0 if the
+   coarsest operator is singular. */
+int oracle_add_subdomain_amg(OSetup *s, int i, int64_t begin, int n_owned, int n_ghost, const int64_t *ghosts,
+                             const double *D, int nlev, int sweeps, const int32_t *nrow,
+                             const int64_t *const *Ap, const int32_t *const *Ai, const double *const *Ax,
+                             const int64_t *const *Pp, const int32_t *const *Pi, const double *const *Px,
+                             const int64_t *const *Rp, const int32_t *const *Ri, const double *const *Rx, int nc,
+                             const double *C, int m, const double *V)
+{
+    OSub *q = &s->sub[i];
+    const int nl = n_owned + n_ghost;
+    memset(q, 0, sizeof(*q));
+    q->begin = begin;
+    q->n_owned = n_owned;
+    q->n_local = nl;
+    q->l2g = (int64_t *)malloc((size_t)nl * sizeof(int64_t));
+    for (int j = 0; j < n_owned; ++j) q->l2g[j] = begin + j;
+    for (int j = 0; j < n_ghost; ++j) q->l2g[n_owned + j] = ghosts[j];
+    q->D = (double *)dupb(D, (size_t)nl * sizeof(double));
+    q->m = m;
+    if (m) q->V = (double *)dupb(V, (size_t)nl * m * sizeof(double));
+    q->rloc = (double *)calloc((size_t)nl, sizeof(double));
+    q->yloc = (double *)calloc((size_t)nl, sizeof(double));
+    OAmgOwn *h = (OAmgOwn *)calloc(1, sizeof(OAmgOwn));
+    h->nlev = nlev;
+    h->sweeps = sweeps;
+    h->nrow = (int *)malloc((size_t)(nlev + 1) * sizeof(int));
+    for (int l = 0; l < nlev; ++l) h->nrow[l] = nrow[l];
+    h->nrow[nlev] = nc;
+    const int L = nlev ? nlev : 1;
+    h->Ap = (int64_t **)calloc((size_t)L, sizeof(void *));
+    h->Pp = (int64_t **)calloc((size_t)L, sizeof(void *));
+    h->Rp = (int64_t **)calloc((size_t)L, sizeof(void *));
+    h->Ai = (int32_t **)calloc((size_t)L, sizeof(void *));
+    h->Pi = (int32_t **)calloc((size_t)L, sizeof(void *));
+    h->Ri = (int32_t **)calloc((size_t)L, sizeof(void *));
+    h->Ax = (double **)calloc((size_t)L, sizeof(void *));
+    h->Px = (double **)calloc((size_t)L, sizeof(void *));
+    h->Rx = (double **)calloc((size_t)L, sizeof(void *));
+    for (int l = 0; l < nlev; ++l) {
+        const int n = nrow[l];
+        const int next = l + 1 < nlev ? nrow[l + 1] : nc;
+        h->Ap[l] = (int64_t *)dupb(Ap[l], (size_t)(n + 1) * sizeof(int64_t));
+        h->Ai[l] = (int32_t *)dupb(Ai[l], (size_t)Ap[l][n] * sizeof(int32_t));
+        h->Ax[l] = (double *)dupb(Ax[l], (size_t)Ap[l][n] * sizeof(double));
+        if (next > 0) {
+            h->Pp[l] = (int64_t *)dupb(Pp[l], (size_t)(n + 1) * sizeof(int64_t));
+            h->Pi[l] = (int32_t *)dupb(Pi[l], (size_t)Pp[l][n] * sizeof(int32_t));
+            h->Px[l] = (double *)dupb(Px[l], (size_t)Pp[l][n] * sizeof(double));
+            h->Rp[l] = (int64_t *)dupb(Rp[l], (size_t)(next + 1) * sizeof(int64_t));
+            h->Ri[l] = (int32_t *)dupb(Ri[l], (size_t)Rp[l][next] * sizeof(int32_t));
+            h->Rx[l] = (double *)dupb(Rx[l], (size_t)Rp[l][next] * sizeof(double));
+        }
+    }
+    h->CLU = (double *)dupb(C ? C : D, C ? (size_t)nc * nc * sizeof(double) : 0);
+    h->Cpiv = (int *)calloc((size_t)(nc ? nc : 1), sizeof(int));
+    q->amg = h;
+    if (nc && !oracle_dense_lu(nc, h->CLU, h->Cpiv)) return 0;
+    return 1;
 }

@@ -1,0 +1,85 @@
+"""AMG local solves on the GPU (the reference's --local-approx amg).
+
+Setups whose subdomains carry an AMG hierarchy (s2l_b200.amg, pinned on the reference's AMGCL by
+tests/test_oracle.py) instead of factors: the GPU's local solves, one-level and two-level applies
+must equal the oracle's (one V-cycle from x = 0 per subdomain, Gauss-Seidel in the serial order)
+to 1e-12, GMRES must take the oracle's iterations +-1 and reach the FP64 true residual rtol.
+"""
+import numpy as np
+import pytest
+
+from conftest import small_setup
+from oracle.oracle import OracleSetup
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from s2l_b200 import capi
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+CASES = [
+    ("bubbles3d", {"amg_coarse_enough": 100}),
+    ("bubbles3d", {"amg_coarse_enough": 5000}),  # one coarsest level: the local matrix itself
+    ("convdiff3d", {"amg_coarse_enough": 50, "amg_sweeps": 2}),
+    ("poisson2d", {"amg_coarse_enough": 100, "pou": "multiplicity", "one_level": "asm", "coarse": "additive"}),
+    ("poisson2d", {"amg_coarse_enough": 30, "coarse": "none"}),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_amg_local_solves_and_applies_match_oracle(ctx, case):
+    from s2l_b200.capi import GpuSetup
+    name, kw = CASES[case]
+    w, st = small_setup(name, local_approx="amg", **kw)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    rng = np.random.default_rng(60 + case)
+    for i in range(st.nsub):
+        b = rng.standard_normal(st.subdomains[i].n_local)
+        assert rel(g.local_solve(i, b), o.local_solve(i, b)) <= 1e-12, i
+    for _ in range(2):  # two calls in a row: the work vectors start clean every time
+        r = rng.standard_normal(st.n)
+        assert rel(g.one_level_apply(r), o.one_level_apply(r)) <= 1e-12
+        assert rel(g.apply(r), o.apply(r)) <= 1e-12
+    xg, rg = g.gmres(st.b, restart=w.restart, rtol=1e-8, maxit=2000)
+    xo, ro = o.gmres(st.b, restart=w.restart, rtol=1e-8, maxit=2000)
+    assert rg["converged"] and ro["converged"]
+    assert abs(rg["iterations"] - ro["iterations"]) <= 1
+    assert np.linalg.norm(st.b - st.A @ xg) <= 1.1e-8 * np.linalg.norm(st.b)
+    o.close()
+    g.close()
+
+
+def test_amg_bicgstab_matches_oracle(ctx):
+    from s2l_b200.capi import GpuSetup
+    w, st = small_setup("bubbles3d", local_approx="amg", amg_coarse_enough=100)
+    g = GpuSetup(ctx, st)
+    o = OracleSetup(st)
+    xg, rg = g.bicgstab(st.b, rtol=1e-8, maxit=2000)
+    _, ro = o.bicgstab(st.b, rtol=1e-8, maxit=2000)
+    assert rg["converged"] and abs(rg["iterations"] - ro["iterations"]) <= 1
+    assert np.linalg.norm(st.b - st.A @ xg) <= 1.1e-8 * np.linalg.norm(st.b)
+    o.close()
+    g.close()
+
+
+def test_amg_setups_refuse_block_calls_and_refactor(ctx):
+    from s2l_b200.capi import GpuSetup, S2LError
+    _, st = small_setup("bubbles3d", local_approx="amg", amg_coarse_enough=100)
+    g = GpuSetup(ctx, st)
+    with pytest.raises(S2LError) as e:
+        g.apply_block(np.ones((2, st.n)))
+    assert e.value.code == 1
+    g.close()
+    with pytest.raises(S2LError) as e:
+        GpuSetup(ctx, st, options={"refactor": 1})
+    assert e.value.code == 1

@@ -194,3 +194,24 @@ def test_amg_hierarchy_and_cycle_pinned_on_the_reference(fixture):
     for v, ref in zip(g["vecs"], g["out"]):
         x = amg_apply(H, v)
         assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("name,kw", [("bubbles3d", {"amg_coarse_enough": 100}),
+                                     ("convdiff3d", {"amg_coarse_enough": 50, "amg_sweeps": 2}),
+                                     ("poisson2d", {"amg_coarse_enough": 100, "pou": "multiplicity",
+                                                    "one_level": "asm", "coarse": "additive"})])
+def test_oracle_two_level_with_amg_local_solves(name, kw):
+    """Setups with --local-approx amg: the oracle's local solves are the hierarchy's V-cycle, and
+    its GMRES converges with the two-level preconditioner built on them."""
+    from oracle.oracle import amg_apply
+    w, st = small_setup(name, local_approx="amg", **kw)
+    assert all(s.factor is None and s.amg is not None for s in st.subdomains)
+    o = OracleSetup(st)
+    rng = np.random.default_rng(5)
+    for i in (0, st.nsub - 1):
+        b = rng.standard_normal(st.subdomains[i].n_local)
+        assert np.array_equal(o.local_solve(i, b), amg_apply(st.subdomains[i].amg, b))
+    x, r = o.gmres(st.b, restart=w.restart, rtol=1e-8, maxit=2000)
+    assert r["converged"]
+    assert np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+    o.close()
