@@ -6,7 +6,7 @@
 // CSR matrices over these spaces, so a residual, a restriction or a prolongation is one launch for
 // all subdomains.  Gauss-Seidel sweeps run one CTA per subdomain over wavefronts of its rows (rows
 // of one wavefront read no row updated in the same wavefront, and no row of a later wavefront has
-// been updated yet), a thread per row, each row summed in column order as the serial sweep does.
+// been updated yet), a group of lanes per row.
 // The coarsest level of a subdomain is solved with its dense inverse.
 #include "s2l_internal.cuh"
 
@@ -20,27 +20,65 @@ int amg_grid(int64_t work, int bs)
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
 }
 
-// x(i) = (f(i) - sum_{j != i} A(i, j) x(j)) / A(i, i) over the rows of each wavefront in turn
-__global__ void __launch_bounds__(512) gs_sweep_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                       const double* __restrict__ v, const double* __restrict__ f,
-                                                       double* x, const int32_t* __restrict__ sched,
-                                                       const int64_t* __restrict__ wf_ptr,
-                                                       const int32_t* __restrict__ sub_wf)
+// x(i) = (f(i) - sum_{j != i} A(i, j) x(j)) / A(i, i) over the rows of each wavefront in turn, a
+// group of G lanes per row (the lanes split the row's entries, then add their parts by shuffles;
+// the sum is reassociated, the serial sweep's rounding is not kept).  With SMEM the subdomain's x
+// (rows [o, o + n) of the level space) lives in shared memory for the whole sweep (the operator is
+// block-diagonal, so a row reads no other subdomain's x).
+template <bool SMEM, int G>
+__global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                        const double* __restrict__ v, const double* __restrict__ f,
+                                                        double* x, const int32_t* __restrict__ sched,
+                                                        const int64_t* __restrict__ wf_ptr,
+                                                        const int32_t* __restrict__ sub_wf,
+                                                        const int64_t* __restrict__ sub_off,
+                                                        const int32_t* __restrict__ sub_n)
 {
+    extern __shared__ double xs[];
     const int b = blockIdx.x;
+    const int64_t o = sub_off[b];
+    const int n = sub_n[b];
+    const int lg = threadIdx.x & (G - 1), grp = threadIdx.x / G, ngrp = blockDim.x / G;
+    if (SMEM) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) xs[k] = x[o + k];
+        __syncthreads();
+    }
     for (int w = sub_wf[b]; w < sub_wf[b + 1]; ++w) {
-        for (int64_t k = wf_ptr[w] + threadIdx.x; k < wf_ptr[w + 1]; k += blockDim.x) {
-            const int i = sched[k];
-            double D = 1.0, X = f[i];
-            for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
-                const int c = ci[e];
-                if (c == i) D = v[e];
-                else X -= v[e] * x[c];
+        const int64_t end = wf_ptr[w + 1];
+        for (int64_t kb = wf_ptr[w]; kb < end; kb += ngrp) {  // the same trip count for every lane
+            const int64_t k = kb + grp;
+            const bool valid = k < end;
+            const int i = valid ? sched[k] : 0;
+            double part = 0.0, dpart = 0.0;
+            int has = 0;
+            if (valid)
+                for (int64_t e = rp[i] + lg; e < rp[i + 1]; e += G) {
+                    const int c = ci[e];
+                    const double a = v[e];
+                    if (c == i) {
+                        dpart = a;
+                        has = 1;
+                    } else {
+                        part += a * (SMEM ? xs[c - o] : x[c]);
+                    }
+                }
+#pragma unroll
+            for (int m = G / 2; m; m >>= 1) {
+                part += __shfl_xor_sync(0xffffffffu, part, m, G);
+                dpart += __shfl_xor_sync(0xffffffffu, dpart, m, G);
+                has += __shfl_xor_sync(0xffffffffu, has, m, G);
             }
-            x[i] = (1.0 / D) * X;
+            if (valid && lg == 0) {
+                const double D = has ? dpart : 1.0;
+                const double val = (1.0 / D) * (f[i] - part);
+                if (SMEM) xs[i - o] = val;
+                else x[i] = val;
+            }
         }
         __syncthreads();
     }
+    if (SMEM)
+        for (int k = threadIdx.x; k < n; k += blockDim.x) x[o + k] = xs[k];
 }
 
 // y = M x (beta = 0) or y += M x (beta = 1), one thread per row
@@ -67,7 +105,8 @@ __global__ void csr_residual_kernel(int64_t n, const int64_t* __restrict__ rp, c
     }
 }
 
-// x_c = C^-1 f_c for every subdomain whose coarsest level is this one (one CTA each)
+// x_c = C^-1 f_c for every subdomain whose coarsest level is this one (one CTA each; C^-1 stored
+// column by column, so the threads of a row block read consecutive entries)
 __global__ void coarse_inverse_kernel(const int32_t* __restrict__ c_sub_off, const int32_t* __restrict__ c_n,
                                       const int64_t* __restrict__ c_inv_off, const double* __restrict__ Cinv,
                                       const double* __restrict__ f, double* __restrict__ x)
@@ -78,7 +117,7 @@ __global__ void coarse_inverse_kernel(const int32_t* __restrict__ c_sub_off, con
     const double* M = Cinv + c_inv_off[b];
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
         double s = 0.0;
-        for (int c = 0; c < n; ++c) s += M[(int64_t)r * n + c] * f[o + c];
+        for (int c = 0; c < n; ++c) s += M[(int64_t)c * n + r] * f[o + c];  // M stored transposed
         x[o + r] = s;
     }
 }
@@ -115,10 +154,32 @@ __global__ void amg_scatter_kernel(int64_t n, const int32_t* __restrict__ out_id
 
 namespace s2l {
 
-void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
-                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf)
+template <int G>
+void gs_launch(cudaStream_t st, int nsub_lvl, bool sm, size_t smem, const int64_t* rp, const int32_t* ci,
+               const double* v, const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr,
+               const int32_t* sub_wf, const int64_t* sub_off, const int32_t* sub_n)
 {
-    if (nsub_lvl > 0) gs_sweep_kernel<<<nsub_lvl, 512, 0, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf);
+    if (sm) {
+        cudaFuncSetAttribute(gs_sweep_kernel<true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S2L_GS_SMEM_CAP);
+        gs_sweep_kernel<true, G><<<nsub_lvl, 1024, smem, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n);
+    } else {
+        gs_sweep_kernel<false, G><<<nsub_lvl, 1024, 0, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n);
+    }
+}
+
+void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
+                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
+                     const int64_t* sub_off, const int32_t* sub_n, int max_n, int lanes)
+{
+    if (nsub_lvl <= 0) return;
+    const size_t smem = (size_t)max_n * sizeof(double);
+    const bool sm = smem <= S2L_GS_SMEM_CAP;
+    switch (lanes) {
+    case 4: gs_launch<4>(st, nsub_lvl, sm, smem, rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n); break;
+    case 8: gs_launch<8>(st, nsub_lvl, sm, smem, rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n); break;
+    case 16: gs_launch<16>(st, nsub_lvl, sm, smem, rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n); break;
+    default: gs_launch<32>(st, nsub_lvl, sm, smem, rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n); break;
+    }
 }
 
 void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,

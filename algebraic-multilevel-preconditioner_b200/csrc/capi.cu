@@ -232,6 +232,10 @@ struct s2l_setup {
         std::vector<int> nsmooth;           // per level: subdomains smoothed on it (CTAs of a sweep)
         std::vector<int32_t*> fsched, bsched, fsub, bsub;
         std::vector<int64_t*> fwf, bwf;
+        std::vector<int64_t*> soff;         // per level: level-space offset of each smoothed subdomain
+        std::vector<int32_t*> sn;           //   and its rows
+        std::vector<int> smax;              //   the most rows
+        std::vector<int> lanes;             // per level: lanes per row of a sweep (from the mean row length)
         std::vector<int> ncoarse;           // per level: subdomains whose coarsest level it is
         std::vector<int32_t*> c_off, c_n;
         std::vector<int64_t*> c_inv;
@@ -1146,7 +1150,8 @@ int amg_local_solve(s2l_work* w, const double* in, const double* base, double* o
     for (int l = 0; l < L; ++l) {
         double *fl = f + G.voff[l], *xl = x + G.voff[l], *tl = t + G.voff[l];
         for (int k = 0; k < G.sweeps; ++k)
-            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.fsched[l], G.fwf[l], G.fsub[l]);
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.fsched[l], G.fwf[l], G.fsub[l],
+                            G.soff[l], G.sn[l], G.smax[l], G.lanes[l]);
         launch_coarse_inverse(st, G.ncoarse[l], G.c_off[l], G.c_n[l], G.c_inv[l], G.Cinv, f + G.voff[l], xl);
         launched += G.sweeps + 1;
         if (l + 1 < L) {
@@ -1158,12 +1163,14 @@ int amg_local_solve(s2l_work* w, const double* in, const double* base, double* o
     // the deepest level space: its smoothed subdomains have no coarser level (backward sweeps now)
     for (int k = 0; k < G.sweeps; ++k)
         launch_gs_sweep(st, G.nsmooth[L - 1], G.Arp[L - 1], G.Aci[L - 1], G.Av[L - 1], f + G.voff[L - 1],
-                        x + G.voff[L - 1], G.bsched[L - 1], G.bwf[L - 1], G.bsub[L - 1]);
+                        x + G.voff[L - 1], G.bsched[L - 1], G.bwf[L - 1], G.bsub[L - 1], G.soff[L - 1], G.sn[L - 1],
+                        G.smax[L - 1], G.lanes[L - 1]);
     for (int l = L - 2; l >= 0; --l) {
         double *fl = f + G.voff[l], *xl = x + G.voff[l];
         launch_csr_mv(st, G.nspace[l], G.Prp[l], G.Pci[l], G.Pv[l], x + G.voff[l + 1], xl, 1);
         for (int k = 0; k < G.sweeps; ++k)
-            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.bsched[l], G.bwf[l], G.bsub[l]);
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.bsched[l], G.bwf[l], G.bsub[l],
+                            G.soff[l], G.sn[l], G.smax[l], G.lanes[l]);
         launched += G.sweeps + 1;
     }
     launch_amg_scatter(st, G.nspace[0], G.out_idx, x, base, mode == 1 ? w->d_ylocal : out, mode, lo, hi);
@@ -2116,6 +2123,7 @@ int amg_build(s2l_setup* s)
     G.Av.assign(L, nullptr), G.Rv.assign(L, nullptr), G.Pv.assign(L, nullptr);
     G.fsched.assign(L, nullptr), G.bsched.assign(L, nullptr), G.fsub.assign(L, nullptr), G.bsub.assign(L, nullptr);
     G.fwf.assign(L, nullptr), G.bwf.assign(L, nullptr);
+    G.soff.assign(L, nullptr), G.sn.assign(L, nullptr), G.smax.assign(L, 0), G.lanes.assign(L, 32);
     G.nsmooth.assign(L, 0), G.ncoarse.assign(L, 0);
     G.c_off.assign(L, nullptr), G.c_n.assign(L, nullptr), G.c_inv.assign(L, nullptr);
     std::vector<double> cinv_all;
@@ -2126,7 +2134,8 @@ int amg_build(s2l_setup* s)
         std::vector<int64_t> arp(1, 0), prp(1, 0), rrp(1, 0);
         std::vector<int32_t> aci, pci, rci;
         std::vector<double> av, pv, rv;
-        std::vector<int32_t> fs, bs, fsub(1, 0), bsub(1, 0), coff, cn;
+        std::vector<int32_t> fs, bs, fsub(1, 0), bsub(1, 0), coff, cn, sn;
+        std::vector<int64_t> soff;
         std::vector<int64_t> fwf(1, 0), bwf(1, 0), cinvoff;
         for (int i = 0; i < nsub; ++i) {
             const HostSub& h = s->hs[i];
@@ -2182,6 +2191,9 @@ int amg_build(s2l_setup* s)
                     sub.push_back((int32_t)(wptr.size() - 1));
                 }
                 G.nsmooth[l] += 1;
+                soff.push_back(o);
+                sn.push_back(n);
+                G.smax[l] = std::max(G.smax[l], n);
                 bytes += (double)A.ci.size() * 12.0 * (2.0 * sw + 1.0) + (double)n * 8.0 * 6.0;
             } else {
                 const int64_t n = rows_at(h, l);  // a coarsest level: no rows of A_l, P_l
@@ -2197,7 +2209,8 @@ int amg_build(s2l_setup* s)
                     coff.push_back((int32_t)o);
                     cn.push_back(nc);
                     cinvoff.push_back((int64_t)cinv_all.size());
-                    cinv_all.insert(cinv_all.end(), Ci.begin(), Ci.end());
+                    for (int c = 0; c < nc; ++c)  // stored transposed (column by column)
+                        for (int r = 0; r < nc; ++r) cinv_all.push_back(Ci[(size_t)r * nc + c]);
                     G.ncoarse[l] += 1;
                     bytes += (double)nc * nc * 8.0;
                 }
@@ -2221,6 +2234,12 @@ int amg_build(s2l_setup* s)
         RET_IF(upload(s, &G.bwf[l], bwf));
         RET_IF(upload(s, &G.fsub[l], fsub));
         RET_IF(upload(s, &G.bsub[l], bsub));
+        {
+            const double mean = arp.size() > 1 && aci.size() ? (double)aci.size() / (double)(arp.size() - 1) : 0.0;
+            G.lanes[l] = mean <= 10.0 ? 4 : (mean <= 20.0 ? 8 : (mean <= 40.0 ? 16 : 32));
+        }
+        RET_IF(upload(s, &G.soff[l], soff));
+        RET_IF(upload(s, &G.sn[l], sn));
         RET_IF(upload(s, &G.c_off[l], coff));
         RET_IF(upload(s, &G.c_n[l], cn));
         RET_IF(upload(s, &G.c_inv[l], cinvoff));

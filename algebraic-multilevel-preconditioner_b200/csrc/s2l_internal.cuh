@@ -34,7 +34,8 @@
 #ifndef S2L_SPIN_SLEEP_NS
 #define S2L_SPIN_SLEEP_NS 0   // back-off of a sweep poll after its first 8 (ns; 0 = poll without pause)
 #endif
-#define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
+#define S2L_SPIN_LIMIT (1 << 24)
+#define S2L_GS_SMEM_CAP (224 * 1024)  // shared memory of a Gauss-Seidel sweep CTA (its subdomain's x)  // polls of one ready flag before a sweep gives up (error 1)
 
 struct DevSub {
     int64_t begin;      // first owned global row
@@ -218,8 +219,12 @@ void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, co
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 
 // AMG local solves (amg.cu)
+// a Gauss-Seidel sweep of every smoothed subdomain of a level (CTA b: rows [sub_off[b], + sub_n[b])
+// of the level space, kept in shared memory when max_n doubles fit S2L_GS_SMEM_CAP), `lanes`
+// (4, 8, 16 or 32) lanes per row
 void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
-                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf);
+                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
+                     const int64_t* sub_off, const int32_t* sub_n, int max_n, int lanes);
 void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
                    double* y, int accumulate);
 void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,

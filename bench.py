@@ -12,7 +12,8 @@ rtol 1e-8, U[-1,1] right-hand sides.  Forms timed:
   batched / block_mixed_threads: several solves or blocks from host threads at once;
   serving     : Poisson arrivals over three resident matrices on the worker threads (p50/p99);
   sequence_refactor: the next matrices of the moving-bubble sequence, each refactorized on the
-                device (s2l_gpu_refactor) and solved for --head-k right-hand sides.
+                device (s2l_gpu_refactor) and solved for --head-k right-hand sides;
+  amg_local_solves: the same matrix with AMG local solvers (--local-approx amg), plain FP64 GMRES.
 Headline (`value`): block_mixed at --head-k right-hand sides per step (default 16, the batching
 configuration's right-hand sides per matrix), solves/s with b resident in HBM; `e2e` = the same
 through the C ABI with pinned host buffers (copies inside the timed region).
@@ -63,6 +64,8 @@ def parse():
     ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
     ap.add_argument("--seq", type=int, default=8, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
+    ap.add_argument("--amg", type=int, default=1,
+                    help="AMG form: the same matrix with AMG local solvers (--local-approx amg), 0 = off")
     ap.add_argument("--serve-mix", type=int, default=0,
                     help="serving-mix form: requests over 40 seeded cases of the three families (0 = off)")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
@@ -469,6 +472,48 @@ def run_ours(a):
 
     serving_mix = serve_mix(a, local) if a.serve_mix > 0 else None
 
+    # ---- AMG local solvers (the reference's --local-approx amg): the same matrix, partition and
+    # coarse basis, each subdomain's A_ii^-1 replaced by one AMG V-cycle; plain FP64 GMRES
+    amg_form = None
+    if a.amg and a.workload == "bubbles3d":
+        import dataclasses
+        from s2l_b200.amg import build_hierarchy
+        t0a = time.time()
+        subs_amg = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii)) for sd in st.subdomains]
+        st_amg = dataclasses.replace(st, subdomains=subs_amg)
+        amg_setup_s = time.time() - t0a
+        ga = capi.GpuSetup(ctx, st_amg)
+        ga.set_stream(stream.cuda_stream)
+        kwa = dict(restart=wl.restart, rtol=wl.rtol, flexible=False, strict=False, maxit=2000)
+        for _ in range(a.warmup):
+            x_dev.zero_()
+            ga.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kwa)
+        ga.profile(("local_solve",))
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        its_a = []
+        for k in range(a.steps):
+            evs[k][0].record(stream)
+            x_dev.zero_()
+            _, ra = ga.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kwa)
+            evs[k][1].record(stream)
+            its_a.append(ra["iterations"])
+        barrier()
+        per_a = [s_.elapsed_time(e_) for s_, e_ in evs]
+        vc_ms, vc_n = ga.profile_get("local_solve")
+        ga.profile(())
+        xa = x_dev.cpu().numpy()
+        levels = sorted({len(sd.amg.levels) + (sd.amg.coarse is not None) for sd in subs_amg})
+        amg_form = {"ms_per_solve": max_over_ranks(sum(per_a)) / a.steps, "iterations": its_a,
+                    "converged": bool(ra["converged"]),
+                    "true_rel_residual_host_check": float(np.linalg.norm(st.b - st.A @ xa) / np.linalg.norm(st.b)),
+                    "v_cycle_ms": vc_ms / max(vc_n, 1), "levels": levels,
+                    "operator_entries": int(sum(sd.amg.nnz() for sd in subs_amg)),
+                    "host_setup_s": amg_setup_s,
+                    "vs_plain_fp64_exact": {"ms_per_solve": results["plain_fp64"]["ms_per_solve"],
+                                            "iterations": results["plain_fp64"]["iterations"]}}
+        ga.close()
+
     # ---- end to end through the C ABI with pinned host buffers (headline block form): each step
     # copies its k right-hand sides and initial guesses in and its k solutions out
     g, kw = forms["mixed"]
@@ -588,6 +633,7 @@ def run_ours(a):
             "block_mixed_threads": block_thr,
             "serving": serving,
             "serving_mix": serving_mix,
+            "amg_local_solves": amg_form,
             "sequence_refactor": sequence,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
