@@ -83,3 +83,65 @@ class MT19937_64:
 def random_rhs(n: int, seed: int) -> np.ndarray:
     """U[-1, 1] right-hand side in the original ordering, as the reference draws it."""
     return MT19937_64(seed).uniform(n, -1.0, 1.0)
+
+
+_M32 = 0xFFFFFFFF
+
+
+def seed_seq_generate(seeds, count: int) -> list:
+    """``std::seed_seq(seeds).generate()`` of ``count`` 32-bit words: the algorithm the C++ standard
+    specifies for ``seed_seq::generate`` ([rand.util.seedseq]), restated over Python integers."""
+    v = [int(s) & _M32 for s in seeds]
+    s, n = len(v), int(count)
+    if n == 0:
+        return []
+    b = [0x8B8B8B8B] * n
+    t = 11 if n >= 623 else 7 if n >= 68 else 5 if n >= 39 else 3 if n >= 7 else (n - 1) // 2
+    p = (n - t) // 2
+    q = p + t
+    m = max(s + 1, n)
+
+    def mix(x):
+        return x ^ (x >> 27)
+
+    for k in range(m):
+        r1 = (1664525 * mix(b[k % n] ^ b[(k + p) % n] ^ b[(k - 1) % n])) & _M32
+        if k == 0:
+            r2 = r1 + s
+        elif k <= s:
+            r2 = r1 + k % n + v[k - 1]
+        else:
+            r2 = r1 + k % n
+        r2 &= _M32
+        b[(k + p) % n] = (b[(k + p) % n] + r1) & _M32
+        b[(k + q) % n] = (b[(k + q) % n] + r2) & _M32
+        b[k % n] = r2
+    for k in range(m, m + n):
+        r3 = (1566083941 * mix((b[k % n] + b[(k + p) % n] + b[(k - 1) % n]) & _M32)) & _M32
+        r4 = (r3 - k % n) & _M32
+        b[(k + p) % n] ^= r3
+        b[(k + q) % n] ^= r4
+        b[k % n] = r4
+    return b
+
+
+def mt19937_64_from_seed_seq(seeds) -> MT19937_64:
+    """``std::mt19937_64(std::seed_seq{seeds...})``: 2 words of the sequence per 64-bit state word
+    (low word first); an all-zero state (top 33 bits of the first word included) becomes 2^63."""
+    words = seed_seq_generate(seeds, 2 * _NN)
+    st = [(words[2 * i] | (words[2 * i + 1] << 32)) for i in range(_NN)]
+    if (st[0] & int(_UM)) == 0 and not any(st[1:]):
+        st[0] = 1 << 63
+    eng = MT19937_64(0)
+    eng._mt = np.asarray(st, dtype=np.uint64)
+    eng._buf = np.empty(0, dtype=np.uint64)
+    eng._pos = 0
+    return eng
+
+
+def random_rhs_step(n: int, seed: int, step: int, corrector: int) -> np.ndarray:
+    """U[-1, 1] right-hand side of solve (step, corrector) of a sequence, original ordering: the
+    reference's ``randomRhs`` (``src/solver/time_loop.cpp:31-43``), an ``std::mt19937_64`` seeded
+    with ``std::seed_seq{seed, step, corrector, 0x5eed}``."""
+    eng = mt19937_64_from_seed_seq([int(seed) & _M32, int(step) & _M32, int(corrector) & _M32, 0x5EED])
+    return eng.uniform(n, -1.0, 1.0)
