@@ -1879,10 +1879,11 @@ int s2l_gpu_set_matrix(s2l_setup* s, const int64_t* rowptr, const int64_t* col, 
     if (rowptr[0] != 0) return s->fail(S2L_ERR_BADARG, "rowptr[0] must be 0");
     const int64_t nnz = rowptr[n];
     if (nnz < 0 || nnz >= (int64_t)INT32_MAX) return s->fail(S2L_ERR_BADARG, "nnz must be in [0, 2^31)");
+    for (int64_t r = 0; r < n; ++r)  // monotone: every row ends within [0, nnz]
+        if (rowptr[r + 1] < rowptr[r]) return s->fail(S2L_ERR_BADARG, "rowptr not monotone");
     s->A.rp.assign(rowptr, rowptr + n + 1);
     s->A.ci.resize(nnz);
     for (int64_t r = 0; r < n; ++r) {
-        if (rowptr[r + 1] < rowptr[r]) return s->fail(S2L_ERR_BADARG, "rowptr not monotone");
         for (int64_t e = rowptr[r]; e < rowptr[r + 1]; ++e) {
             if (col[e] < 0 || col[e] >= n) return s->fail(S2L_ERR_BADARG, "column index out of range");
             s->A.ci[e] = (int32_t)col[e];
@@ -1942,6 +1943,8 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
     }
     auto copy_csr = [&](HostCsr& dst, const int64_t* rp, const int32_t* ci, const void* v, bool lower) -> int {
         if (rp[0] != 0) return s->fail(S2L_ERR_BADARG, "factor rowptr[0] must be 0");
+        for (int r = 0; r < nl; ++r)
+            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "factor rowptr not monotone");
         dst.rp.assign(rp, rp + nl + 1);
         const int64_t nz = rp[nl];
         dst.ci.assign(ci, ci + nz);
@@ -1951,7 +1954,6 @@ int s2l_gpu_add_subdomain(s2l_setup* s, int i, int64_t begin, int n_owned, int n
         else
             std::copy((const float*)v, (const float*)v + nz, dst.v.begin());
         for (int r = 0; r < nl; ++r) {
-            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "factor rowptr not monotone");
             for (int64_t e = rp[r]; e < rp[r + 1]; ++e) {
                 const int c = ci[e];
                 if (c < 0 || c >= nl) return s->fail(S2L_ERR_BADARG, "factor column out of range");
@@ -2013,12 +2015,13 @@ int s2l_gpu_add_subdomain_amg(s2l_setup* s, int i, int64_t begin, int n_owned, i
     h.amg_sweeps = sweeps;
     auto copy = [&](HostCsr& dst, int rows, int cols, const int64_t* rp, const int32_t* ci, const double* v) -> int {
         if (!rp || !ci || !v || rp[0] != 0) return s->fail(S2L_ERR_BADARG, "bad AMG level matrix");
+        for (int r = 0; r < rows; ++r)
+            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "AMG level matrix: rowptr not monotone");
         dst.rp.assign(rp, rp + rows + 1);
         const int64_t nz = rp[rows];
         dst.ci.assign(ci, ci + nz);
         dst.v.assign(v, v + nz);
         for (int r = 0; r < rows; ++r) {
-            if (rp[r + 1] < rp[r]) return s->fail(S2L_ERR_BADARG, "AMG level matrix: rowptr not monotone");
             for (int64_t e = rp[r]; e < rp[r + 1]; ++e)
                 if (ci[e] < 0 || ci[e] >= cols || (e > rp[r] && ci[e] <= ci[e - 1]))
                     return s->fail(S2L_ERR_BADARG, "AMG level matrix: columns out of range or not sorted");

@@ -224,6 +224,30 @@ def test_bad_arguments_fail_loudly(ctx):
     g.close()
 
 
+def test_malformed_csr_is_refused_before_it_is_read(ctx):
+    """A row pointer that runs past the entries and then back is refused (S2L_ERR_BADARG) before
+    any entry is copied, for the matrix and for a factor."""
+    import dataclasses
+    import types
+    from s2l_b200 import capi
+    _, st = small_setup("poisson2d")
+    rp = st.A.indptr.astype(np.int64).copy()
+    rp[1] = rp[-1] + 1000
+    bad = types.SimpleNamespace(indptr=rp, indices=st.A.indices, data=st.A.data, shape=st.A.shape)
+    with pytest.raises(capi.S2LError) as e:
+        capi.GpuSetup(ctx, dataclasses.replace(st, A=bad))
+    assert e.value.code == 1 and "monotone" in str(e.value)
+    f = st.subdomains[0].factor
+    Lrp = f.L.indptr.astype(np.int64).copy()
+    Lrp[1] = Lrp[-1] + 1000
+    badL = types.SimpleNamespace(indptr=Lrp, indices=f.L.indices, data=f.L.data, dtype=f.L.dtype)
+    subs = list(st.subdomains)
+    subs[0] = dataclasses.replace(subs[0], factor=dataclasses.replace(f, L=badL))
+    with pytest.raises(capi.S2LError) as e:
+        capi.GpuSetup(ctx, dataclasses.replace(st, subdomains=subs))
+    assert e.value.code == 1 and "monotone" in str(e.value)
+
+
 def test_hbm_budget_refusal():
     from s2l_b200 import capi
     _, st = small_setup("poisson2d")
