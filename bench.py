@@ -139,6 +139,39 @@ def measured_traffic(algorithmic_bytes: float):
         return None
 
 
+def spmv_bytes(st, k: int = 1) -> float:
+    """Algorithmic bytes of y = A x for k columns: the CSR once (FP64 values, int32 columns and row
+    pointers), x read and y written per column."""
+    n = st.n
+    return st.A.nnz * 12 + (n + 1) * 4 + k * 16 * n
+
+
+def gmres_solve_bytes(st, its_cols, restart: int, ls_bytes: float, ls_col_bytes: float) -> float:
+    """Algorithmic bytes of one (block) right-preconditioned GMRES(restart) solve whose columns took
+    its_cols iterations: per Arnoldi step, the preconditioner (local solve: factors once plus
+    ls_col_bytes per column; coarse basis and E once, three vectors per column; the deflated
+    form's product with A), the product with A, and CGS2 over the column's basis.  Restarts and
+    the Hessenberg work are left out, so this is a lower bound of the traffic."""
+    n, n0 = st.n, st.n0
+    deflated = n0 > 0 and st.opts.coarse == "deflated"
+    basis = sum(s.n_owned * s.V.shape[1] for s in st.subdomains) if n0 else 0
+    fixed = (ls_bytes - ls_col_bytes) + spmv_bytes(st, 0) * (2 if deflated else 1)
+    if n0:
+        fixed += 2 * 8 * basis + 8 * n0 * n0
+    total = 0.0
+    for i in range(max(its_cols) if len(its_cols) else 0):
+        k = sum(1 for t in its_cols if t > i)
+        j = i % restart
+        col = ls_col_bytes + 16 * n + 3 * 8 * n           # local solve, A x, apply's vector updates
+        if n0:
+            col += 3 * 8 * n                              # restriction read, prolongation read/write
+        if deflated:
+            col += 16 * n + 8 * n                         # r - A x0
+        col += 2 * (2 * (j + 1) * 8 * n + 16 * n)        # CGS2: dots and update, twice
+        total += fixed + k * col
+    return total
+
+
 def measured_peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -225,7 +258,7 @@ def run_ours(a):
             x_dev.zero_()
             g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
         headline = False
-        g.profile(("local_solve",))
+        g.profile(("local_solve", "spmv"))
         barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
         its = []
@@ -244,6 +277,7 @@ def run_ours(a):
         total_ms = max_over_ranks(sum(per))
         clocks = sampler.stop() if headline else None
         ls_ms, ls_n = g.profile_get("local_solve")
+        sp_ms, sp_n = g.profile_get("spmv")
         launches = g.launches()
         g.profile(())
         # independent FP64 check of the last solution
@@ -254,6 +288,8 @@ def run_ours(a):
             "true_rel_residual": max(true_res), "true_rel_residual_host_check": true_chk,
             "local_solve_ms_total": ls_ms, "local_solve_launches": ls_n, "launches": launches,
             "local_solve_bytes": g.local_solve_bytes(), "clocks": clocks,
+            "local_solve_column_bytes": g.stat("local_solve_column_bytes"),
+            "spmv_ms_total": sp_ms, "spmv_calls": sp_n,
             "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
         }
     # ---- batched form: k right-hand sides solved at once on one setup (k host threads, each call on
@@ -328,7 +364,7 @@ def run_ours(a):
             Xk.zero_()
             _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
         if is_rf:
-            g.profile(("local_solve",))
+            g.profile(("local_solve", "spmv"))
         if is_head:
             sampler = ClockSampler(local)
             sampler.start()
@@ -348,6 +384,7 @@ def run_ours(a):
             head_clocks = sampler.stop()
         if is_rf:
             rf_ls = g.profile_get("local_solve")
+            rf_sp = g.profile_get("spmv")
             rf_launches = g.launches()
             g.profile(())
         Xh = Xk.cpu().numpy()
@@ -362,7 +399,7 @@ def run_ours(a):
         if is_head:
             head = dict(block[str(k)], per_block_ms=per_k, clocks=head_clocks)
         if is_rf:
-            rf = dict(ls=rf_ls, launches=rf_launches, steps=a.steps)
+            rf = dict(ls=rf_ls, sp=rf_sp, launches=rf_launches, steps=a.steps)
         del Bk, Xk
     # ---- several k=4 blocks at once from host threads (each on its own workspace and stream)
     block_thr = {}
@@ -593,6 +630,34 @@ def run_ours(a):
     achieved32 = mixed["local_solve_bytes"] / (ls_avg_ms32 * 1e-3) / 1e9 if ls_avg_ms32 > 0 else 0.0
     ls_avg_ms64 = plain["local_solve_ms_total"] / max(plain["local_solve_launches"], 1)
     achieved64 = plain["local_solve_bytes"] / (ls_avg_ms64 * 1e-3) / 1e9 if ls_avg_ms64 > 0 else 0.0
+
+    def rate(nbytes, ms):
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        return {"achieved": gbs, "frac": gbs / peak}
+
+    # SpMV (y = A x and the residual forms, averaged over every call; bytes of y = A x, so a lower bound)
+    spmv = {"single_column_fp32": dict(rate(spmv_bytes(st), mixed["spmv_ms_total"] / max(mixed["spmv_calls"], 1)),
+                                       bytes_per_launch=spmv_bytes(st), calls=mixed["spmv_calls"]),
+            "single_column_fp64": dict(rate(spmv_bytes(st), plain["spmv_ms_total"] / max(plain["spmv_calls"], 1)),
+                                       bytes_per_launch=spmv_bytes(st), calls=plain["spmv_calls"]),
+            f"block_{bw}": dict(rate(spmv_bytes(st, bw), rf["sp"][0] / max(rf["sp"][1], 1)),
+                                bytes_per_launch=spmv_bytes(st, bw), calls=rf["sp"][1])}
+    # whole solves: algorithmic bytes of every Arnoldi step over the solve's wall time
+    col32 = mixed["local_solve_column_bytes"]
+    per_solve = {
+        "headline_block": dict(rate(gmres_solve_bytes(st, head["iterations"], wl.restart, mixed["local_solve_bytes"],
+                                                      col32), head["ms_per_block"]),
+                               bytes=gmres_solve_bytes(st, head["iterations"], wl.restart,
+                                                       mixed["local_solve_bytes"], col32)),
+        "mixed": dict(rate(gmres_solve_bytes(st, mixed["iterations"][:1], wl.restart, mixed["local_solve_bytes"],
+                                             col32), mixed["ms_per_solve"]),
+                      bytes=gmres_solve_bytes(st, mixed["iterations"][:1], wl.restart, mixed["local_solve_bytes"],
+                                              col32)),
+        "plain_fp64": dict(rate(gmres_solve_bytes(st, plain["iterations"][:1], wl.restart, plain["local_solve_bytes"],
+                                                  plain["local_solve_column_bytes"]), plain["ms_per_solve"]),
+                           bytes=gmres_solve_bytes(st, plain["iterations"][:1], wl.restart,
+                                                   plain["local_solve_bytes"], plain["local_solve_column_bytes"])),
+    }
     out = {
         "metric": METRIC,
         # whole-job throughput of the headline form: blocks of k right-hand sides, mixed precision
@@ -654,7 +719,8 @@ def run_ours(a):
                      "single_column_fp32": {"achieved": achieved32, "frac": achieved32 / peak,
                                             "avg_launch_ms": ls_avg_ms32, "bytes_per_launch": mixed["local_solve_bytes"]},
                      "single_column_fp64": {"achieved": achieved64, "frac": achieved64 / peak,
-                                            "avg_launch_ms": ls_avg_ms64, "bytes_per_launch": plain["local_solve_bytes"]}},
+                                            "avg_launch_ms": ls_avg_ms64, "bytes_per_launch": plain["local_solve_bytes"]},
+                     "spmv": spmv, "per_solve": per_solve},
         # kernels launched in the timed region: those of the timed k=bw blocks, times the blocks
         # a k=head step runs at once
         "gpu_launches": int(rf["launches"] * max(kh // bw, 1)),
