@@ -181,11 +181,53 @@ def measured_peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
+class Replicas:
+    """The ranks of a run on N GPUs: independent replicas of the solve phase, no data-path
+    collective.  A gloo group carries the barriers around the timed regions and the max over ranks
+    of the device-timed totals (RANK / WORLD_SIZE / LOCAL_RANK / MASTER_* from the launcher)."""
+
+    def __init__(self, timeout_s: float = 900.0):
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self, sync=None):
+        """sync() (the device), then every rank."""
+        if sync is not None:
+            sync()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.dist is None:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rank0_first(self, make):
+        """make() on rank 0, then on the others (rank 0 fills a cache the others read)."""
+        out = make() if self.rank == 0 else None
+        self.barrier()
+        return make() if self.rank != 0 else out
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ------------------------------------------------------------------------------------ our arm
 def run_ours(a):
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
+    reps = Replicas()
+    rank, world, local = reps.rank, reps.world, reps.local
     os.environ.setdefault("S2L_CACHE_DIR", os.path.join(REPO, "_cache"))
     from s2l_b200 import workloads as W
     from s2l_b200.setup_phase import with_factor_precision
@@ -199,17 +241,9 @@ def run_ours(a):
         wl = W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
         wdesc = (f"bubbles3d {wl.nx}^3 pressure Poisson, {wl.nsub} subdomains, overlap {a.overlap}, nev 20, "
                  f"deflated RAS, LL^T factors, GMRES({wl.restart}), rtol 1e-8")
-    dist = None
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=900))
         # rank 0 fills the setup cache first; the replicas then load it (setup is outside the timing)
-        if rank == 0:
-            st = W.build(wl)
-        dist.barrier()
-        if rank != 0:
-            st = W.build(wl)
+        st = reps.rank0_first(lambda: W.build(wl))
     else:
         t0 = time.time()
         st = W.build(wl)
@@ -239,16 +273,9 @@ def run_ours(a):
     }
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        reps.barrier(torch.cuda.synchronize)
 
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = reps.max
 
     results = {}
     peak, peak_src = measured_peaks()
@@ -733,8 +760,7 @@ def run_ours(a):
     g64.close()
     g32.close()
     ctx.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
 
 
 def serve_mix(a, device: int) -> dict:

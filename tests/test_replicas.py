@@ -1,0 +1,68 @@
+"""bench.py on N GPUs: independent replicas, a gloo group for the barriers and the max over ranks.
+
+Run here as two CPU processes (world size 2, gloo on 127.0.0.1): every rank gets the max of the
+ranks' timings, rank 0 builds first and the other rank after the barrier, and the reference arm
+runs on rank 0 alone (the other rank exits 0 without output).
+"""
+import os
+import socket
+import subprocess
+import sys
+import textwrap
+
+from conftest import REPO
+
+
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+CHILD = textwrap.dedent("""
+    import importlib.util, json, os, sys
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(sys.argv[1], "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    reps = bench.Replicas(timeout_s=60)
+    order = os.path.join(sys.argv[2], "order.txt")
+
+    def make():
+        with open(order, "a") as f:
+            f.write(str(reps.rank))
+        return reps.rank
+
+    built = reps.rank0_first(make)
+    synced = []
+    reps.barrier(lambda: synced.append(1))
+    m = reps.max(1.5 + reps.rank)
+    reps.close()
+    print(json.dumps({"rank": reps.rank, "world": reps.world, "max": m, "built": built, "synced": len(synced)}))
+""")
+
+
+def test_two_replicas_share_barriers_and_the_max(tmp_path):
+    port = free_port()
+    procs = []
+    for r in range(2):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, "-c", CHILD, REPO, str(tmp_path)], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = [p.communicate(timeout=120) for p in procs]
+    import json
+    res = []
+    for p, (o, e) in zip(procs, outs):
+        assert p.returncode == 0, e
+        res.append(json.loads(o.strip().splitlines()[-1]))
+    assert [r["rank"] for r in res] == [0, 1] and all(r["world"] == 2 for r in res)
+    assert all(r["max"] == 2.5 for r in res)
+    assert [r["built"] for r in res] == [0, 1] and all(r["synced"] == 1 for r in res)
+    assert (tmp_path / "order.txt").read_text() == "01"
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    p = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0 and p.stdout.strip() == ""
