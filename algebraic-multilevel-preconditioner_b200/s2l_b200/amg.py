@@ -176,3 +176,20 @@ def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1) -> AmgHierarch
     if direct:
         H.coarse = A.toarray()
     return H
+
+
+def rebuild_hierarchy(H: AmgHierarchy, A) -> AmgHierarchy:
+    """The hierarchy of new values of the same matrix with H's transfer operators kept: every
+    coarser operator is recomputed as R (A P) and the coarsest is solved directly again
+    (AMGCL's ``amg::rebuild``, ``amg.hpp:250-269``, ``level::rebuild``; the reference's
+    refactorize() with ``--amg-reuse``, ``src/linalg/inexact_solver.cpp:73-85``)."""
+    A = _sorted_csr(sp.csr_matrix(A, dtype=np.float64))
+    if H.n != A.shape[0]:
+        raise ValueError(f"rebuild: {A.shape[0]} rows, the hierarchy has {H.n}")
+    out = AmgHierarchy(sweeps=H.sweeps)
+    for lvl in H.levels:
+        out.levels.append(AmgLevel(A, lvl.P, lvl.R))
+        A = _sorted_csr(lvl.R @ (A @ lvl.P)) if lvl.P is not None else None
+    if H.coarse is not None:
+        out.coarse = A.toarray()
+    return out

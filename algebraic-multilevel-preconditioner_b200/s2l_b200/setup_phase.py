@@ -61,6 +61,7 @@ class SchwarzOptions:
     local_approx: str = "none"         # none (exact factors) | amg (one AMG V-cycle, --local-approx amg)
     amg_coarse_enough: int = 500       # --amg-coarse-enough: largest coarsest AMG level
     amg_sweeps: int = 1                # --amg-sweeps: Gauss-Seidel steps before / after the coarse correction
+    amg_reuse: bool = False            # --amg-reuse: refactorization keeps the transfer operators
 
 
 @dataclass
@@ -532,4 +533,42 @@ def with_factor_precision(st: Setup, precision: str) -> Setup:
         ns.factor = nf
         subs.append(ns)
     out.subdomains = subs
+    return out
+
+
+def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
+    """The setup after the reference's Refactorize with AMG local solvers, for new values of A
+    (renumbered ordering, same pattern): every subdomain's hierarchy is set up again on its new
+    A_ii (``AmgSolver::refactorize``, ``src/linalg/inexact_solver.cpp:73-85``: a new hierarchy, or
+    with ``amg_reuse`` the kept transfer operators and new Galerkin products), the coarse basis is
+    kept and E = W^T A_new W recomputed with it (``CoarseSpace::refresh``,
+    ``src/preconditioner/coarse_space.cpp:95-105, 186-206``)."""
+    import copy
+    from .amg import build_hierarchy, rebuild_hierarchy
+    A_new = sp.csr_matrix(A_new, dtype=np.float64)
+    A_new.sort_indices()
+    if A_new.shape != st.A.shape:
+        raise ValueError(f"size changed: {A_new.shape} != {st.A.shape}")
+    o = st.opts
+    subs = []
+    for sd in st.subdomains:
+        if sd.amg is None:
+            raise ValueError("refactor_amg_setup: a subdomain without an AMG hierarchy")
+        idx = sd.l2g()
+        Aii = sp.csr_matrix(A_new[idx][:, idx])
+        Aii.sort_indices()
+        if o.amg_reuse:
+            H = rebuild_hierarchy(sd.amg, Aii)
+        else:
+            H = build_hierarchy(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps)
+        ns = copy.copy(sd)
+        ns.Aii = Aii
+        ns.amg = H
+        subs.append(ns)
+    out = copy.copy(st)
+    out.A = A_new
+    out.subdomains = subs
+    out.E = coarse_matrix(A_new, subs, st.offsets) if st.n0 else st.E
+    out.stats = dict(st.stats)
+    out.stats["nnz_factors"] = int(sum(sd.amg.nnz() for sd in subs))
     return out

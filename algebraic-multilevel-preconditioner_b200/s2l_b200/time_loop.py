@@ -9,7 +9,9 @@ setup:
 
 * ``Reuse``: the setup is kept as it is (the policy only asks for it when the matrix did not change);
 * ``Refactorize``: ``GpuSetup.refactor`` (``s2l_gpu_refactor``: the local factors refactorized on their
-  kept patterns, E recomputed with the kept coarse basis, on the device);
+  kept patterns, E recomputed with the kept coarse basis, on the device); with AMG local solvers
+  the hierarchies are set up again on the host (``setup_phase.refactor_amg_setup``, new or with
+  kept transfer operators as ``--amg-reuse``) and the setup is uploaded anew;
 * ``Rebuild``: a new host setup of the current matrix on the same partition, uploaded as a new
   device setup (the reference's full ``TwoLevelSchwarz`` construction).
 
@@ -29,11 +31,12 @@ import time
 from dataclasses import dataclass
 
 import numpy as np
+import scipy.sparse as sp
 
 from . import sequence as seqmod
 from . import workloads as W
 from .rng import random_rhs_step
-from .setup_phase import build_setup
+from .setup_phase import build_setup, refactor_amg_setup
 
 
 class UpdateLevel(enum.IntEnum):
@@ -235,10 +238,10 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
     # a one-level preconditioner has no coarse basis to age: auto behaves as refactor
     if one_level and mode == ReusePolicy.AUTO:
         mode = ReusePolicy.REFACTOR
-    if mode != ReusePolicy.OFF and w.opts.local_approx == "amg":
-        raise ValueError("AMG local solvers are not refactorized on the device: use reuse 'off'")
     policy = ReusePolicy(mode, cfg.rebuild_growth, cfg.rebuild_every)
-    refactor = mode != ReusePolicy.OFF
+    amg = w.opts.local_approx == "amg"
+    # factors are refactorized on the device; AMG hierarchies on the host, then uploaded anew
+    refactor = mode != ReusePolicy.OFF and not amg
     if matrix is None:
         def matrix(step):
             return W.make_problem(dataclasses.replace(w, time=float(step))).A
@@ -280,7 +283,14 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
                     g = make_solver(st, refactor)
                 elif level == UpdateLevel.REFACTORIZE:
                     vals, _ = seqmod.values_in_setup_order(A_cur, st)
-                    g.refactor(vals)
+                    if amg:
+                        st = refactor_amg_setup(st, sp.csr_matrix((vals, st.A.indices, st.A.indptr),
+                                                                  shape=st.A.shape))
+                        g.close()
+                        g = None
+                        g = make_solver(st, False)
+                    else:
+                        g.refactor(vals)
                 current = True
                 t_update = time.perf_counter() - t0
                 b = np.ascontiguousarray(b_orig[st.new_to_old])

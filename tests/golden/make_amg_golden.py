@@ -3,7 +3,9 @@
 Runs the reference itself (oracle/_ref/amg_dump, built from the reference's sources by
 oracle/ref/Makefile) on local matrices A_ii of the three workload families and stores A_ii, seeded
 vectors and the reference's solve() of each (one AMGCL V-cycle from x = 0, smoothed aggregation,
-Gauss-Seidel) in tests/golden/amg_<case>.npz.  Test infrastructure; run it where the reference
+Gauss-Seidel) in tests/golden/amg_<case>.npz; and, for the reference's refactorize() along the
+moving-bubble sequence (a new hierarchy, or --amg-reuse), in tests/golden/amg_refactor_<case>.npz.
+Test infrastructure; run it where the reference
 sources are:  python tests/golden/make_amg_golden.py
 """
 import os
@@ -29,18 +31,38 @@ CASES = {  # name: (family, setup keywords, subdomain, coarse_enough, sweeps)
 }
 
 
-def reference_apply(A, vecs, coarse_enough, sweeps):
+# refactorization: the reference's solver set up on A_ii of the bubble sequence at time 0, then
+# refactorize()d with A_ii at a later time (bubbles moved), with and without --amg-reuse
+REFACTOR_CASES = {  # name: (subdomain, coarse_enough, sweeps, time of the new matrix, reuse)
+    "bubbles3d_reuse": (0, 50, 1, 4.0, 1),
+    "bubbles3d_new": (0, 50, 1, 4.0, 0),
+    "bubbles3d_reuse_2lev": (3, 200, 2, 6.0, 1),
+}
+
+
+def write_matrix(path, A, vecs=()):
+    with open(path, "wb") as f:
+        np.array([A.shape[0], A.nnz, len(vecs)], dtype=np.int64).tofile(f)
+        A.indptr.astype(np.int64).tofile(f)
+        A.indices.astype(np.int64).tofile(f)
+        A.data.astype(np.float64).tofile(f)
+        if len(vecs):
+            np.asarray(vecs, dtype=np.float64).tofile(f)
+
+
+def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0):
     A = sp.csr_matrix(A)
     A.sort_indices()
     with tempfile.TemporaryDirectory() as d:
-        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
-        with open(fin, "wb") as f:
-            np.array([A.shape[0], A.nnz, len(vecs)], dtype=np.int64).tofile(f)
-            A.indptr.astype(np.int64).tofile(f)
-            A.indices.astype(np.int64).tofile(f)
-            A.data.astype(np.float64).tofile(f)
-            np.asarray(vecs, dtype=np.float64).tofile(f)
-        r = subprocess.run([DUMP, fin, fout, str(coarse_enough), str(sweeps), "sa"], capture_output=True, text=True)
+        fin, fout, fnext = os.path.join(d, "in.bin"), os.path.join(d, "out.bin"), os.path.join(d, "next.bin")
+        write_matrix(fin, A, vecs)
+        cmd = [DUMP, fin, fout, str(coarse_enough), str(sweeps), "sa"]
+        if A_next is not None:
+            A_next = sp.csr_matrix(A_next)
+            A_next.sort_indices()
+            write_matrix(fnext, A_next)
+            cmd += [fnext, str(int(reuse))]
+        r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError(r.stderr)
         return np.fromfile(fout).reshape(len(vecs), -1), r.stderr.strip()
@@ -59,6 +81,25 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"amg_{name}.npz"), indptr=A.indptr, indices=A.indices, data=A.data,
                             vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps, info=info)
         print(name, A.shape[0], info)
+    import dataclasses
+    from s2l_b200 import sequence as seqmod
+    from s2l_b200 import workloads as W
+    w, st = small_setup("bubbles3d")
+    for name, (i, ce, sweeps, t, reuse) in REFACTOR_CASES.items():
+        s = st.subdomains[i]
+        idx = s.l2g()
+        A0 = sp.csr_matrix(st.A[idx][:, idx])
+        A0.sort_indices()
+        vals, _ = seqmod.values_in_setup_order(W.make_problem(dataclasses.replace(w, time=t)).A, st)
+        A1g = sp.csr_matrix((vals, st.A.indices, st.A.indptr), shape=st.A.shape)
+        A1 = sp.csr_matrix(A1g[idx][:, idx])
+        A1.sort_indices()
+        vecs = np.random.default_rng(800 + i).uniform(-1.0, 1.0, (2, A0.shape[0]))
+        out, info = reference_apply(A0, vecs, ce, sweeps, A_next=A1, reuse=reuse)
+        np.savez_compressed(os.path.join(HERE, f"amg_refactor_{name}.npz"), indptr=A0.indptr, indices=A0.indices,
+                            data=A0.data, data_next=A1.data, vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps,
+                            reuse=reuse, info=info)
+        print("refactor", name, A0.shape[0], info)
 
 
 if __name__ == "__main__":

@@ -90,3 +90,15 @@ def test_time_loop_warm_start_final_tolerances_match_oracle(ctx):
     w = small_bubbles()
     recs = both(ctx, w, steps=2, correctors=3, reuse="refactor", warm_start=True, final_rtol=1e-10)
     assert [r.final_corrector for r in recs] == [False, False, True] * 2
+
+
+@pytest.mark.parametrize("reuse", [False, True])
+def test_time_loop_amg_local_solvers_match_oracle(ctx, reuse):
+    """AMG local solvers along the sequence: each Refactorize sets the hierarchies up again on the
+    host (new, or with kept transfer operators) and uploads them; every solve matches the oracle's."""
+    w = small_bubbles()
+    w.opts.local_approx = "amg"
+    w.opts.amg_coarse_enough = 100
+    w.opts.amg_reuse = reuse
+    recs = both(ctx, w, steps=3, correctors=1, reuse="refactor")
+    assert levels(recs) == "211"

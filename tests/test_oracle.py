@@ -174,7 +174,10 @@ def test_oracle_refactorization_reports_bad_pivots():
         refactor_factor(s.factor, -st.A[idx][:, idx])
 
 
-AMG_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden")) if f.startswith("amg_"))
+AMG_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden"))
+                    if f.startswith("amg_") and not f.startswith("amg_refactor_"))
+AMG_REFACTOR_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden"))
+                             if f.startswith("amg_refactor_"))
 
 
 @pytest.mark.parametrize("fixture", AMG_GOLDEN)
@@ -194,6 +197,49 @@ def test_amg_hierarchy_and_cycle_pinned_on_the_reference(fixture):
     for v, ref in zip(g["vecs"], g["out"]):
         x = amg_apply(H, v)
         assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("fixture", AMG_REFACTOR_GOLDEN)
+def test_amg_refactorization_pinned_on_the_reference(fixture):
+    """The reference's refactorize() of its AMG local solver along the moving-bubble sequence: a new
+    hierarchy on the new A_ii (build_hierarchy), or with --amg-reuse the kept transfer operators and
+    new Galerkin products (rebuild_hierarchy); the oracle's V-cycle on either reproduces the
+    reference's solve() after refactorize() to rounding."""
+    import scipy.sparse as sp
+    from oracle.oracle import amg_apply
+    from s2l_b200.amg import build_hierarchy, rebuild_hierarchy
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture))
+    n = g["indptr"].size - 1
+    A0 = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
+    A1 = sp.csr_matrix((g["data_next"], g["indices"], g["indptr"]), shape=(n, n))
+    ce, sweeps = int(g["coarse_enough"]), int(g["sweeps"])
+    H0 = build_hierarchy(A0, coarse_enough=ce, sweeps=sweeps)
+    H1 = rebuild_hierarchy(H0, A1) if int(g["reuse"]) else build_hierarchy(A1, coarse_enough=ce, sweeps=sweeps)
+    if int(g["reuse"]):
+        assert all(a.P is b.P and a.R is b.R for a, b in zip(H0.levels, H1.levels))
+    for v, ref in zip(g["vecs"], g["out"]):
+        x = amg_apply(H1, v)
+        assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
+    # the other choice gives another operator: the fixture tells them apart
+    H2 = build_hierarchy(A1, coarse_enough=ce, sweeps=sweeps) if int(g["reuse"]) else rebuild_hierarchy(H0, A1)
+    assert np.linalg.norm(amg_apply(H2, g["vecs"][0]) - g["out"][0]) > 1e-8 * np.linalg.norm(g["out"][0])
+
+
+def test_amg_rebuild_with_the_same_values_is_the_same_hierarchy():
+    import scipy.sparse as sp
+    from s2l_b200.amg import build_hierarchy, rebuild_hierarchy
+    _, st = small_setup("bubbles3d")
+    s = st.subdomains[0]
+    idx = s.l2g()
+    A = sp.csr_matrix(st.A[idx][:, idx])
+    H = build_hierarchy(A, coarse_enough=50)
+    H2 = rebuild_hierarchy(H, A)
+    assert len(H2.levels) == len(H.levels)
+    for a, b in zip(H.levels, H2.levels):
+        assert (a.A != b.A).nnz == 0
+    assert np.array_equal(H.coarse, H2.coarse)
+    with pytest.raises(ValueError):
+        rebuild_hierarchy(H, A[:-1, :-1])
 
 
 @pytest.mark.parametrize("name,kw", [("bubbles3d", {"amg_coarse_enough": 100}),

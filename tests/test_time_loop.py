@@ -192,7 +192,26 @@ def test_time_loop_rejects_bad_options():
                {"stop_norm": "linf"}, {"steps": 0}):
         with pytest.raises(ValueError):
             run_time_loop(w, TimeLoopConfig(**kw), make_solver=Recorder, workers=1)
-    wa = small_bubbles()
-    wa.opts.local_approx = "amg"
-    with pytest.raises(ValueError):
-        run_time_loop(wa, TimeLoopConfig(reuse="refactor"), make_solver=Recorder, workers=1)
+
+
+@pytest.mark.parametrize("reuse", [False, True])
+def test_time_loop_amg_refactorizes_on_the_host(reuse):
+    """AMG local solvers: Refactorize sets the hierarchies up again on the host (new, or with the
+    transfer operators kept under amg_reuse) with the coarse basis kept, and uploads a new setup."""
+    w = small_bubbles()
+    w.opts.local_approx = "amg"
+    w.opts.amg_coarse_enough = 100
+    w.opts.amg_reuse = reuse
+    recs, log = run(w, steps=3, correctors=2, reuse="refactor")
+    assert levels(recs) == "201010"
+    builds = [e[1] for e in log if e[0] == "build"]
+    assert len(builds) == 3 and not any(e[0] == "refactor" for e in log)
+    assert [e[0] for e in log].count("close") == 3
+    st0, st1 = builds[0], builds[1]
+    assert st1.subdomains[0].V is st0.subdomains[0].V                 # the coarse basis is kept
+    same = [a.P is b.P for a, b in zip(st0.subdomains[0].amg.levels, st1.subdomains[0].amg.levels)]
+    assert all(same) if reuse else not any(same)
+    import dataclasses
+    A1 = W.make_problem(dataclasses.replace(w, time=1.0)).A
+    want, _ = seqmod.values_in_setup_order(A1, st0)
+    assert np.array_equal(st1.A.data, want)
