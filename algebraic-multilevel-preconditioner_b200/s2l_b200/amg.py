@@ -22,6 +22,11 @@ module restates its published setup algorithm for the configuration the referenc
 * levels are added while a level has more than ``coarse_enough`` rows; the last one is solved
   directly (AMGCL's skyline LU; any exact solve agrees to rounding).
 
+With ``--amg-coarsening rs`` the levels come from AMGCL's classic Ruge-Stuben coarsening
+(``coarsening/ruge_stuben.hpp``, default parameters): negative strong couplings
+(eps_str = 0.25), C/F splitting by decreasing measure in AMGCL's bucket order, direct
+interpolation with truncation (eps_tr = 0.2) and rescaling, R = P^T, the same Galerkin product.
+
 The cycle itself (Gauss-Seidel, residual, restriction, coarse correction) is applied by the solve
 phase; its CPU restatement is the oracle's ``oracle_amg_apply``.
 """
@@ -154,8 +159,192 @@ def _transfer(A: sp.csr_matrix, eps: np.float32):
     return P, R
 
 
-def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1) -> AmgHierarchy:
-    """The reference's AMG setup for one local matrix (see the module docstring)."""
+# Ruge-Stuben (--amg-coarsening rs, AMGCL's coarsening/ruge_stuben.hpp with its default parameters)
+RS_EPS_STRONG = float(np.float32(0.25))  # a_ij strong when a_ij < eps_str * min_k a_ik (negative couplings)
+RS_EPS_TRUNC = float(np.float32(0.2))    # the float 0.2f as the double it widens to
+_TINY = 2.0 * float(np.finfo(np.float64).eps)  # AMGCL's detail::eps<double>(1)
+_U, _F, _C = 0, 1, 2
+
+
+def _rs_strength(A: sp.csr_matrix):
+    """Strong couplings per stored entry and the initial C/F marks: a row without a negative
+    off-diagonal entry is F with no strong coupling; else a_ij (j != i) is strong when
+    a_ij < eps_str * min_k a_ik."""
+    n = A.shape[0]
+    rp, ci, va = A.indptr, A.indices, A.data
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    off = ci != rows
+    amin = np.zeros(n)
+    np.minimum.at(amin, rows[off], va[off])  # min(0, off-diagonal entries): exact in any order
+    weak_row = np.abs(amin) < _TINY
+    thr = amin * RS_EPS_STRONG
+    strong = off & (va < thr[rows]) & ~weak_row[rows]
+    cf = [_F if w else _U for w in weak_row.tolist()]
+    return strong, cf
+
+
+def _rs_split(A: sp.csr_matrix, strong: np.ndarray, cf: list) -> list:
+    """Classic C/F splitting by decreasing measure lambda_i (the number of undecided variables
+    that depend strongly on i, F ones counted twice), with AMGCL's bucket order: variables sit in
+    groups of equal lambda, by increasing index at the start; the last variable of the highest
+    group becomes C, the undecided variables depending on it F, and the measures move by one
+    between adjacent groups (a rise to the end of the group above, a drop to the start of the
+    group below)."""
+    n = A.shape[0]
+    rp, ci = A.indptr.tolist(), A.indices.tolist()
+    st = strong.tolist()
+    # transposed strength graph: for column c, the rows that depend strongly on c, by row
+    tp = [0] * (n + 1)
+    for j, s in enumerate(st):
+        if s:
+            tp[ci[j] + 1] += 1
+    for i in range(n):
+        tp[i + 1] += tp[i]
+    tcol = [0] * tp[n]
+    fill = tp[:n]
+    for i in range(n):
+        for j in range(rp[i], rp[i + 1]):
+            if st[j]:
+                c = ci[j]
+                tcol[fill[c]] = i
+                fill[c] += 1
+    lam = [sum(1 if cf[k] == _U else 2 for k in tcol[tp[i]:tp[i + 1]]) for i in range(n)]
+    size = max(n, max(lam, default=0) + 1)
+    ptr = [0] * (size + 1)
+    cnt = [0] * size
+    for v in lam:
+        ptr[v + 1] += 1
+    for k in range(size):
+        ptr[k + 1] += ptr[k]
+    i2n = [0] * n
+    n2i = [0] * n
+    for i in range(n):
+        v = lam[i]
+        pos = ptr[v] + cnt[v]
+        cnt[v] += 1
+        i2n[pos] = i
+        n2i[i] = pos
+
+    def move(x, old_pos, new_pos):
+        y = i2n[new_pos]
+        n2i[x], n2i[y] = new_pos, old_pos
+        i2n[old_pos], i2n[new_pos] = y, x
+
+    for top in range(n - 1, -1, -1):
+        i = i2n[top]
+        li = lam[i]
+        if li == 0:
+            return [_C if m == _U else m for m in cf]
+        cnt[li] -= 1
+        if cf[i] == _F:
+            continue
+        cf[i] = _C
+        for c in tcol[tp[i]:tp[i + 1]]:
+            if cf[c] != _U:
+                continue
+            cf[c] = _F
+            for aj in range(rp[c], rp[c + 1]):  # the undecided variables c depends on rise by one
+                if not st[aj]:
+                    continue
+                a = ci[aj]
+                la = lam[a]
+                if cf[a] != _U or la + 1 >= n:
+                    continue
+                move(a, n2i[a], ptr[la] + cnt[la] - 1)
+                cnt[la] -= 1
+                cnt[la + 1] += 1
+                ptr[la + 1] = ptr[la] + cnt[la]
+                lam[a] = la + 1
+        for j in range(rp[i], rp[i + 1]):  # the undecided variables i depends on drop by one
+            if not st[j]:
+                continue
+            c = ci[j]
+            lc = lam[c]
+            if cf[c] != _U or lc == 0:
+                continue
+            move(c, n2i[c], ptr[lc])
+            cnt[lc] -= 1
+            cnt[lc - 1] += 1
+            ptr[lc] += 1
+            lam[c] = lc - 1
+    return cf
+
+
+def _rs_transfer(A: sp.csr_matrix):
+    """(P, R) of one Ruge-Stuben level (direct interpolation with truncation), or None without
+    C variables.  Row i of P: 1 at i's coarse index for C; for F, a_ij scaled by alpha (negative
+    a_ij) or beta (positive) over the strong C couplings that survive truncation (outside
+    [eps_tr * min, eps_tr * max] of them), alpha = -|sum of negative a_ik| / (|a_ii| |sum of the
+    negative strong C ones|) rescaled for what truncation dropped, beta likewise; positive
+    couplings without a strong positive C coupling are lumped into the diagonal."""
+    n = A.shape[0]
+    strong, cf = _rs_strength(A)
+    cf = _rs_split(A, strong, cf)
+    cidx = [0] * n
+    nc = 0
+    for i in range(n):
+        if cf[i] == _C:
+            cidx[i] = nc
+            nc += 1
+    if nc == 0:
+        return None
+    rp, ci, va, st = A.indptr.tolist(), A.indices.tolist(), A.data.tolist(), strong.tolist()
+    pp, pc, pv = [0], [], []
+    for i in range(n):
+        if cf[i] == _C:
+            pc.append(cidx[i])
+            pv.append(1.0)
+            pp.append(len(pc))
+            continue
+        lo = hi = 0.0
+        for j in range(rp[i], rp[i + 1]):
+            if st[j] and cf[ci[j]] == _C:
+                lo = min(lo, va[j])
+                hi = max(hi, va[j])
+        lo *= RS_EPS_TRUNC
+        hi *= RS_EPS_TRUNC
+        dia = a_num = a_den = b_num = b_den = d_neg = d_pos = 0.0
+        for j in range(rp[i], rp[i + 1]):
+            c, v = ci[j], va[j]
+            if c == i:
+                dia = v
+                continue
+            sc = st[j] and cf[c] == _C
+            if v < 0.0:
+                a_num += v
+                if sc:
+                    a_den += v
+                    if lo < v:
+                        d_neg += v
+            else:
+                b_num += v
+                if sc:
+                    b_den += v
+                    if v < hi:
+                        d_pos += v
+        cf_neg = abs(a_den) / abs(a_den - d_neg) if abs(a_den - d_neg) > _TINY else 1.0
+        cf_pos = abs(b_den) / abs(b_den - d_pos) if abs(b_den - d_pos) > _TINY else 1.0
+        if 0.0 < b_num and abs(b_den) < _TINY:
+            dia += b_num
+        alpha = -cf_neg * abs(a_num) / (abs(dia) * abs(a_den)) if abs(a_den) > _TINY else 0.0
+        beta = -cf_pos * abs(b_num) / (abs(dia) * abs(b_den)) if abs(b_den) > _TINY else 0.0
+        for j in range(rp[i], rp[i + 1]):
+            c, v = ci[j], va[j]
+            if not (st[j] and cf[c] == _C) or lo <= v <= hi:
+                continue
+            pc.append(cidx[c])
+            pv.append((alpha if v < 0.0 else beta) * v)
+        pp.append(len(pc))
+    P = _sorted_csr(sp.csr_matrix((np.asarray(pv, dtype=np.float64), np.asarray(pc, dtype=np.int64),
+                                   np.asarray(pp, dtype=np.int64)), shape=(n, nc)))
+    return P, _sorted_csr(P.T)
+
+
+def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1, coarsening: str = "sa") -> AmgHierarchy:
+    """The reference's AMG setup for one local matrix (see the module docstring); coarsening "sa"
+    (smoothed aggregation) or "rs" (Ruge-Stuben, ``--amg-coarsening rs``)."""
+    if coarsening not in ("sa", "rs"):
+        raise ValueError(f"unknown AMG coarsening '{coarsening}' (sa|rs)")
     A = _sorted_csr(sp.csr_matrix(A, dtype=np.float64))
     H = AmgHierarchy(sweeps=int(sweeps))
     eps = EPS_STRONG
@@ -163,8 +352,11 @@ def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1) -> AmgHierarch
     while A is not None and A.shape[0] > coarse_enough:
         lvl = AmgLevel(A)
         H.levels.append(lvl)
-        tr = _transfer(A, eps)
-        eps = np.float32(eps * np.float32(0.5))
+        if coarsening == "rs":
+            tr = _rs_transfer(A)
+        else:
+            tr = _transfer(A, eps)
+            eps = np.float32(eps * np.float32(0.5))
         if tr is None:  # nothing to aggregate: the last level is smoothed only
             A = None
             direct = False

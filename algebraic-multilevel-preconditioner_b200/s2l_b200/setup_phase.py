@@ -62,6 +62,7 @@ class SchwarzOptions:
     amg_coarse_enough: int = 500       # --amg-coarse-enough: largest coarsest AMG level
     amg_sweeps: int = 1                # --amg-sweeps: Gauss-Seidel steps before / after the coarse correction
     amg_reuse: bool = False            # --amg-reuse: refactorization keeps the transfer operators
+    amg_coarsening: str = "sa"         # --amg-coarsening: sa (smoothed aggregation) | rs (Ruge-Stuben)
 
 
 @dataclass
@@ -336,7 +337,8 @@ def _subdomain_work(args):
     Aii, Atil, D, opts, symmetric, want_coarse = args
     if opts.local_approx == "amg":
         from .amg import build_hierarchy
-        fac = build_hierarchy(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps)
+        fac = build_hierarchy(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps,
+                              coarsening=opts.amg_coarsening)
     else:
         fac = factorize_local(Aii, symmetric, opts.local_factorization, opts.local_precision)
     Z, info = (local_coarse_vectors(Aii, Atil, D, opts, symmetric) if want_coarse
@@ -560,7 +562,8 @@ def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
         if o.amg_reuse:
             H = rebuild_hierarchy(sd.amg, Aii)
         else:
-            H = build_hierarchy(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps)
+            H = build_hierarchy(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps,
+                                coarsening=o.amg_coarsening)
         ns = copy.copy(sd)
         ns.Aii = Aii
         ns.amg = H

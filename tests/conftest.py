@@ -35,7 +35,8 @@ def small_setup(name: str, **kw):
         w.opts.nev = kw.get("nev", 8)
     else:
         raise ValueError(name)
-    for k in ("one_level", "coarse", "pou", "overlap", "local_approx", "amg_coarse_enough", "amg_sweeps"):
+    for k in ("one_level", "coarse", "pou", "overlap", "local_approx", "amg_coarse_enough", "amg_sweeps",
+              "amg_coarsening"):
         if k in kw:
             setattr(w.opts, k, kw[k])
     st = W.build(w, workers=1, use_cache=False)

@@ -2,8 +2,8 @@
 
 Runs the reference itself (oracle/_ref/amg_dump, built from the reference's sources by
 oracle/ref/Makefile) on local matrices A_ii of the three workload families and stores A_ii, seeded
-vectors and the reference's solve() of each (one AMGCL V-cycle from x = 0, smoothed aggregation,
-Gauss-Seidel) in tests/golden/amg_<case>.npz; and, for the reference's refactorize() along the
+vectors and the reference's solve() of each (one AMGCL V-cycle from x = 0, smoothed aggregation or
+Ruge-Stuben coarsening, Gauss-Seidel) in tests/golden/amg_<case>.npz; and, for the reference's refactorize() along the
 moving-bubble sequence (a new hierarchy, or --amg-reuse), in tests/golden/amg_refactor_<case>.npz.
 Test infrastructure; run it where the reference
 sources are:  python tests/golden/make_amg_golden.py
@@ -22,12 +22,17 @@ sys.path.insert(0, os.path.join(REPO, "tests"))
 sys.path.insert(0, os.path.join(REPO, "algebraic-multilevel-preconditioner_b200"))
 DUMP = os.path.join(REPO, "oracle", "_ref", "amg_dump")
 
-CASES = {  # name: (family, setup keywords, subdomain, coarse_enough, sweeps)
+CASES = {  # name: (family, setup keywords, subdomain, coarse_enough, sweeps[, coarsening])
     "bubbles3d_3lev": ("bubbles3d", {}, 0, 50, 1),
     "bubbles3d_2lev_sweeps2": ("bubbles3d", {}, 1, 200, 2),
     "poisson2d_3lev": ("poisson2d", {}, 0, 50, 1),
     "convdiff3d_3lev": ("convdiff3d", {}, 0, 50, 1),
     "convdiff3d_direct": ("convdiff3d", {}, 2, 500, 1),
+    # Ruge-Stuben coarsening (--amg-coarsening rs)
+    "rs_bubbles3d": ("bubbles3d", {}, 0, 50, 1, "rs"),
+    "rs_bubbles3d_sweeps2": ("bubbles3d", {}, 5, 100, 2, "rs"),
+    "rs_poisson2d": ("poisson2d", {}, 1, 30, 1, "rs"),
+    "rs_convdiff3d": ("convdiff3d", {}, 0, 50, 1, "rs"),
 }
 
 
@@ -50,13 +55,13 @@ def write_matrix(path, A, vecs=()):
             np.asarray(vecs, dtype=np.float64).tofile(f)
 
 
-def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0):
+def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0, coarsening="sa"):
     A = sp.csr_matrix(A)
     A.sort_indices()
     with tempfile.TemporaryDirectory() as d:
         fin, fout, fnext = os.path.join(d, "in.bin"), os.path.join(d, "out.bin"), os.path.join(d, "next.bin")
         write_matrix(fin, A, vecs)
-        cmd = [DUMP, fin, fout, str(coarse_enough), str(sweeps), "sa"]
+        cmd = [DUMP, fin, fout, str(coarse_enough), str(sweeps), coarsening]
         if A_next is not None:
             A_next = sp.csr_matrix(A_next)
             A_next.sort_indices()
@@ -70,16 +75,19 @@ def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0):
 
 def main():
     from conftest import small_setup
-    for name, (fam, kw, i, ce, sweeps) in CASES.items():
+    for name, case in CASES.items():
+        fam, kw, i, ce, sweeps = case[:5]
+        coarsening = case[5] if len(case) > 5 else "sa"
         _, st = small_setup(fam, **kw)
         s = st.subdomains[i]
         idx = s.l2g()
         A = sp.csr_matrix(st.A[idx][:, idx])
         A.sort_indices()
         vecs = np.random.default_rng(700 + i).uniform(-1.0, 1.0, (2, A.shape[0]))
-        out, info = reference_apply(A, vecs, ce, sweeps)
+        out, info = reference_apply(A, vecs, ce, sweeps, coarsening=coarsening)
+        extra = {"coarsening": coarsening} if coarsening != "sa" else {}
         np.savez_compressed(os.path.join(HERE, f"amg_{name}.npz"), indptr=A.indptr, indices=A.indices, data=A.data,
-                            vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps, info=info)
+                            vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps, info=info, **extra)
         print(name, A.shape[0], info)
     import dataclasses
     from s2l_b200 import sequence as seqmod

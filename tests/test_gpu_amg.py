@@ -32,6 +32,8 @@ CASES = [
     ("convdiff3d", {"amg_coarse_enough": 50, "amg_sweeps": 2}),
     ("poisson2d", {"amg_coarse_enough": 100, "pou": "multiplicity", "one_level": "asm", "coarse": "additive"}),
     ("poisson2d", {"amg_coarse_enough": 30, "coarse": "none"}),
+    ("bubbles3d", {"amg_coarse_enough": 100, "amg_coarsening": "rs"}),   # Ruge-Stuben levels
+    ("convdiff3d", {"amg_coarse_enough": 50, "amg_coarsening": "rs"}),
 ]
 
 

@@ -184,14 +184,16 @@ AMG_REFACTOR_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(
 def test_amg_hierarchy_and_cycle_pinned_on_the_reference(fixture):
     """The AMG local solver (--local-approx amg): the setup restatement (s2l_b200.amg) plus the
     oracle's V-cycle reproduce the reference's own solve() (AMGCL, run by
-    tests/golden/make_amg_golden.py) to rounding, on 1 to 3 levels, 1 or 2 sweeps."""
+    tests/golden/make_amg_golden.py) to rounding, on 1 to 4 levels, 1 or 2 sweeps, smoothed
+    aggregation or Ruge-Stuben coarsening (amg_rs_*)."""
     import scipy.sparse as sp
     from oracle.oracle import amg_apply
     from s2l_b200.amg import build_hierarchy
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture))
     n = g["indptr"].size - 1
     A = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
-    H = build_hierarchy(A, coarse_enough=int(g["coarse_enough"]), sweeps=int(g["sweeps"]))
+    coarsening = str(g["coarsening"]) if "coarsening" in g.files else "sa"
+    H = build_hierarchy(A, coarse_enough=int(g["coarse_enough"]), sweeps=int(g["sweeps"]), coarsening=coarsening)
     levels = str(g["info"]).split("[")[1].split(" levels")[0]
     assert len(H.levels) + (H.coarse is not None) == int(levels)
     for v, ref in zip(g["vecs"], g["out"]):
@@ -245,7 +247,8 @@ def test_amg_rebuild_with_the_same_values_is_the_same_hierarchy():
 @pytest.mark.parametrize("name,kw", [("bubbles3d", {"amg_coarse_enough": 100}),
                                      ("convdiff3d", {"amg_coarse_enough": 50, "amg_sweeps": 2}),
                                      ("poisson2d", {"amg_coarse_enough": 100, "pou": "multiplicity",
-                                                    "one_level": "asm", "coarse": "additive"})])
+                                                    "one_level": "asm", "coarse": "additive"}),
+                                     ("bubbles3d", {"amg_coarse_enough": 100, "amg_coarsening": "rs"})])
 def test_oracle_two_level_with_amg_local_solves(name, kw):
     """Setups with --local-approx amg: the oracle's local solves are the hierarchy's V-cycle, and
     its GMRES converges with the two-level preconditioner built on them."""
