@@ -11,7 +11,7 @@ REPO = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 GPU_LIB = os.path.join(LIB_DIR, "libs2l_gpu.so")
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["kernels.cu", "refactor.cu", "amg.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "refactor.cu", "amg.cu", "capi.cu", "amg_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -29,7 +29,7 @@ def build_gpu_lib(force: bool = False, verbose: bool = False, ptxas_info: bool =
         return GPU_LIB
     os.makedirs(LIB_DIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-shared",
+    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-shared",
            "-I", os.path.join(REPO, "include"), "-o", GPU_LIB + ".tmp"]
     if ptxas_info:
         cmd += ["-Xptxas", "-v"]

@@ -34,7 +34,8 @@ EXPORTED = [
     "s2l_gpu_setup_stat", "s2l_gpu_coarse_apply_noalloc", "s2l_gpu_solve_batch", "s2l_gpu_serve_start",
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
     "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block", "s2l_gpu_update_matrix",
-    "s2l_gpu_refactor", "s2l_gpu_add_subdomain_amg",
+    "s2l_gpu_refactor", "s2l_gpu_add_subdomain_amg", "s2l_amg_build", "s2l_amg_rebuild", "s2l_amg_shape",
+    "s2l_amg_matrix", "s2l_amg_coarse", "s2l_amg_free",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -116,6 +117,13 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_add_subdomain_amg": ([vp, C.c_int, C.c_int64, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, vp,
                                        vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "s2l_gpu_gmres_block": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result)], C.c_int),
+        "s2l_amg_build": ([C.c_int64, vp, vp, vp, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+        "s2l_amg_rebuild": ([vp, vp, vp, vp, C.POINTER(vp)], C.c_int),
+        "s2l_amg_shape": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)], C.c_int),
+        "s2l_amg_matrix": ([vp, C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(vp),
+                            C.POINTER(vp), C.POINTER(vp)], C.c_int),
+        "s2l_amg_coarse": ([vp, C.POINTER(vp)], C.c_int),
+        "s2l_amg_free": ([vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -540,6 +548,88 @@ class GpuSetup:
         if getattr(self, "h", None):
             if self.ctx.h:  # never after its context is destroyed (Context.close closes its setups first)
                 self.lib.s2l_gpu_setup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NativeAmg:
+    """An AMG hierarchy built by the library on the host (s2l_amg_build / s2l_amg_rebuild: the
+    reference's AMGCL setup restated in C++, no device needed)."""
+    CODES = {"sa": 0, "rs": 1}
+
+    def __init__(self, h, lib):
+        self.h, self.lib = h, lib
+
+    @classmethod
+    def build(cls, A, coarse_enough: int = 500, coarsening: str = "sa") -> "NativeAmg":
+        import scipy.sparse as sp
+        lib = load()
+        A = sp.csr_matrix(A, dtype=np.float64)
+        A.sort_indices()
+        rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+        v = np.ascontiguousarray(A.data, dtype=np.float64)
+        h = C.c_void_p()
+        rc = lib.s2l_amg_build(A.shape[0], _vp(rp), _vp(ci), _vp(v), int(coarse_enough), cls.CODES[coarsening],
+                               C.byref(h))
+        if rc != S2L_OK:
+            raise S2LError(rc, "s2l_amg_build")
+        return cls(h, lib)
+
+    def rebuild(self, A) -> "NativeAmg":
+        """New values of the same pattern, the transfer operators kept."""
+        import scipy.sparse as sp
+        A = sp.csr_matrix(A, dtype=np.float64)
+        A.sort_indices()
+        rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+        v = np.ascontiguousarray(A.data, dtype=np.float64)
+        h = C.c_void_p()
+        rc = self.lib.s2l_amg_rebuild(self.h, _vp(rp), _vp(ci), _vp(v), C.byref(h))
+        if rc != S2L_OK:
+            raise S2LError(rc, "s2l_amg_rebuild")
+        return NativeAmg(h, self.lib)
+
+    def _matrix(self, level, which):
+        import scipy.sparse as sp
+        rows, cols = C.c_int64(), C.c_int64()
+        rp, ci, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        rc = self.lib.s2l_amg_matrix(self.h, level, which, C.byref(rows), C.byref(cols), C.byref(rp), C.byref(ci),
+                                     C.byref(v))
+        if rc != S2L_OK:
+            raise S2LError(rc, "s2l_amg_matrix")
+        if rows.value == 0:
+            return None
+        n = rows.value
+        indptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int64)), (n + 1,)).copy()
+        nnz = int(indptr[-1])
+        indices = (np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (nnz,)).copy() if nnz
+                   else np.zeros(0, np.int32))
+        data = np.ctypeslib.as_array(C.cast(v, C.POINTER(C.c_double)), (nnz,)).copy() if nnz else np.zeros(0)
+        return sp.csr_matrix((data, indices, indptr), shape=(n, cols.value))
+
+    def hierarchy(self, sweeps: int = 1):
+        """The levels as an s2l_b200.amg.AmgHierarchy (copies)."""
+        from .amg import AmgHierarchy, AmgLevel
+        nlev, nc = C.c_int(), C.c_int64()
+        self.lib.s2l_amg_shape(self.h, C.byref(nlev), C.byref(nc))
+        H = AmgHierarchy(sweeps=int(sweeps))
+        for l in range(nlev.value):
+            H.levels.append(AmgLevel(self._matrix(l, 0), self._matrix(l, 1), self._matrix(l, 2)))
+        if nc.value:
+            d = C.c_void_p()
+            self.lib.s2l_amg_coarse(self.h, C.byref(d))
+            H.coarse = np.ctypeslib.as_array(C.cast(d, C.POINTER(C.c_double)), (nc.value, nc.value)).copy()
+        return H
+
+    def close(self):
+        if self.h:
+            self.lib.s2l_amg_free(self.h)
             self.h = None
 
     def __del__(self):

@@ -148,6 +148,27 @@ int s2l_gpu_add_subdomain_amg(s2l_setup* s, int i, int64_t begin, int n_owned, i
                               const int64_t* const* R_rowptr, const int32_t* const* R_col, const double* const* R_val,
                               int n_coarse, const double* coarse, int m, const double* V);
 
+/* ---- AMG hierarchies on the host (no device needed) ---------------------------------------
+ * The hierarchy of one local matrix A_ii (n rows, CSR with sorted unique columns) as the
+ * reference's AMGCL setup builds it for --local-approx amg (src/linalg/inexact_solver.cpp:45-178,
+ * default parameters): S2L_AMG_SA smoothed aggregation or S2L_AMG_RS Ruge-Stuben
+ * (--amg-coarsening), levels while a level has more than coarse_enough rows, the last one dense.
+ * s2l_amg_rebuild keeps the transfer operators of `old` and recomputes the coarser operators
+ * R (A P) for new values of the same pattern (--amg-reuse, AMGCL's amg::rebuild).  The levels are
+ * read with s2l_amg_shape / s2l_amg_matrix (which: 0 A_l, 1 P_l, 2 R_l; rows = 0 for a last level
+ * without a coarser one) / s2l_amg_coarse (row-major, n_coarse^2) in the layout
+ * s2l_gpu_add_subdomain_amg takes; the pointers stay valid until s2l_amg_free. */
+typedef struct s2l_amg s2l_amg;
+enum { S2L_AMG_SA = 0, S2L_AMG_RS = 1 };
+int s2l_amg_build(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val, int coarse_enough,
+                  int coarsening, s2l_amg** out);
+int s2l_amg_rebuild(const s2l_amg* old, const int64_t* rowptr, const int32_t* col, const double* val, s2l_amg** out);
+int s2l_amg_shape(const s2l_amg* h, int* nlev, int64_t* n_coarse);
+int s2l_amg_matrix(const s2l_amg* h, int level, int which, int64_t* rows, int64_t* cols, const int64_t** rowptr,
+                   const int32_t** col, const double** val);
+int s2l_amg_coarse(const s2l_amg* h, const double** dense);
+int s2l_amg_free(s2l_amg* h);
+
 /* Coarse matrix E = R0 A R0^T (n0 x n0, row-major) and coarse offsets (nsub+1 entries). */
 int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const double* E);
 
