@@ -187,7 +187,7 @@ int coarse_code(const core::SolverConfig& c)
 GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchwarz& one,
                              const prec::TwoLevelSchwarz* two, const core::SolverConfig& cfg, int device,
                              size_t hbm_budget, bool refactorize)
-    : comm_(sd.comm()), sd_(&sd)
+    : comm_(sd.comm()), sd_(&sd), cfg_(cfg), device_(device), hbm_budget_(hbm_budget), refactorize_(refactorize)
 {
     op_version_ = prec_version_ = sd.valuesVersion();
     rank_ = core::mpiRank(comm_);
@@ -200,8 +200,53 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
         counts_[p] = (int)(sys.ownership[p + 1] - sys.ownership[p]);
         displs_[p] = (int)sys.ownership[p];
     }
-    if (cfg.local_approx != "none") throw std::invalid_argument("the GPU solve phase needs exact local factors (--local-approx none)");
+    if (cfg.local_approx != "none" && cfg.local_approx != "amg")
+        throw std::invalid_argument("unknown local approximation '" + cfg.local_approx + "' (none|amg)");
+    amg_on_ = cfg.local_approx == "amg";
+    if (amg_on_ && cfg.local_precision == "single")
+        throw std::invalid_argument("the GPU AMG local solver runs in FP64 (--local-precision double)");
+    coarse_ = two && two->coarse().dimension() > 0 && cfg.coarse != "none";
+    if (two && two->coarse().dimension() > 0) {
+        const core::Mat& V = two->coarse().basis();
+        m_ = (int)V.cols();
+        V_.assign(V.data(), V.data() + V.size());
+    }
+    if (amg_on_) buildAmg(false);
+    else factorization_ = (int)one.localSolver().factorization();
+    upload();
+}
 
+void GpuSolvePhase::buildAmg(bool keep_transfer)
+{
+    // A_ii in CSR with sorted columns (what AMGCL receives from the reference, inexact_solver.cpp:62)
+    Eigen::SparseMatrix<double, Eigen::RowMajor, int> R = sd_->Aii();
+    R.makeCompressed();
+    const int64_t n = R.rows();
+    std::vector<int64_t> rp(R.outerIndexPtr(), R.outerIndexPtr() + n + 1);
+    std::vector<int32_t> ci(R.innerIndexPtr(), R.innerIndexPtr() + R.nonZeros());
+    s2l_amg* h = nullptr;
+    int st;
+    if (keep_transfer && amg_) {
+        st = s2l_amg_rebuild(amg_, rp.data(), ci.data(), R.valuePtr(), &h);
+    } else {
+        st = s2l_amg_build(n, rp.data(), ci.data(), R.valuePtr(), cfg_.amg_coarse_enough,
+                           cfg_.amg_coarsening == "rs" ? S2L_AMG_RS : S2L_AMG_SA, &h);
+    }
+    int worst = st;
+    MPI_Allreduce(&st, &worst, 1, MPI_INT, MPI_MAX, comm_);
+    if (worst != S2L_OK) {
+        if (h) s2l_amg_free(h);
+        throw std::invalid_argument("GPU setup: the host AMG setup of A_ii failed on a rank (status " +
+                                    std::to_string(worst) + ")");
+    }
+    if (amg_) s2l_amg_free(amg_);
+    amg_ = h;
+}
+
+void GpuSolvePhase::upload()
+{
+    const core::LocalSystem& sys = sd_->system();
+    const part::Subdomain& sd = *sd_;
     // ---- this rank's part
     Blob blob;
     {
@@ -212,23 +257,43 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
         blob.put(sys.val);
         blob.put(sd.ghosts());
         blob.put(sd.pou().data(), (size_t)sd.pou().size());
-        const auto f = one.localSolver().factorization();
-        if (cfg.local_precision == "single")
-            export_factor<float>(sd.Aii(), f, blob);
-        else
-            export_factor<double>(sd.Aii(), f, blob);
-        if (two && two->coarse().dimension() > 0) {
-            const core::Mat& V = two->coarse().basis();
-            std::vector<int64_t> vm = {(int64_t)V.cols()};
-            blob.put(vm);
-            blob.put(V.data(), (size_t)V.size());
+        if (amg_on_) {
+            // AMG levels: kind -1, sweeps, levels, coarsest size; per level A, P, R ([rows, cols] and
+            // CSR; rows = 0 for none); the coarsest operator, row-major
+            int nlev = 0;
+            int64_t nc = 0;
+            s2l_amg_shape(amg_, &nlev, &nc);
+            std::vector<int64_t> fmeta = {-1, (int64_t)cfg_.amg_sweeps, (int64_t)nlev, nc};
+            blob.put(fmeta);
+            for (int l = 0; l < nlev; ++l)
+                for (int which = 0; which < 3; ++which) {
+                    int64_t rows = 0, cols = 0;
+                    const int64_t* mrp = nullptr;
+                    const int32_t* mci = nullptr;
+                    const double* mv = nullptr;
+                    s2l_amg_matrix(amg_, l, which, &rows, &cols, &mrp, &mci, &mv);
+                    std::vector<int64_t> shape = {rows, cols};
+                    blob.put(shape);
+                    const int64_t nz = rows ? mrp[rows] : 0;
+                    blob.put(mrp, rows ? (size_t)rows + 1 : 0);
+                    blob.put(mci, (size_t)nz);
+                    blob.put(mv, (size_t)nz);
+                }
+            const double* dense = nullptr;
+            s2l_amg_coarse(amg_, &dense);
+            blob.put(dense, (size_t)(nc * nc));
         } else {
-            std::vector<int64_t> vm = {0};
-            blob.put(vm);
-            blob.put(std::vector<double>());
+            const auto f = (linalg::Factorization)factorization_;
+            if (cfg_.local_precision == "single")
+                export_factor<float>(sd.Aii(), f, blob);
+            else
+                export_factor<double>(sd.Aii(), f, blob);
         }
+        std::vector<int64_t> vm = {(int64_t)m_};
+        blob.put(vm);
+        blob.put(V_);
     }
-    // ---- rank 0 receives every part in rank order and uploads it
+    // ---- rank 0 receives every part in rank order and uploads it as a new setup
     int status = S2L_OK;
     std::string msg;
     const int tag = 7311;
@@ -237,8 +302,15 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
         MPI_Send(&sz, 1, MPI_LONG_LONG, 0, tag, comm_);
         MPI_Send(blob.b.data(), (int)sz, MPI_CHAR, 0, tag + 1, comm_);
     } else {
-        const bool coarse = two && two->coarse().dimension() > 0 && cfg.coarse != "none";
-        status = s2l_gpu_create(device, hbm_budget, &ctx_);
+        const core::SolverConfig& cfg = cfg_;
+        const bool coarse = coarse_;
+        if (setup_) {
+            s2l_gpu_setup_destroy(setup_);
+            setup_ = nullptr;
+        }
+        nnz_counts_.clear();
+        nnz_displs_.clear();
+        if (!ctx_) status = s2l_gpu_create(device_, hbm_budget_, &ctx_);
         if (status == S2L_OK)
             status = s2l_gpu_setup_begin(ctx_, n_, np_, one_level_code(cfg), coarse ? coarse_code(cfg) : S2L_COARSE_NONE,
                                          sd.booleanPou() ? S2L_POU_BOOLEAN : S2L_POU_MULTIPLICITY, &setup_);
@@ -272,6 +344,60 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
             const auto ghosts = rd.get<int64_t>();
             const auto D = rd.get<double>();
             const auto fmeta = rd.get<int64_t>();
+            if (fmeta[0] < 0) {  // AMG levels
+                const int sweeps = (int)fmeta[1], nlev = (int)fmeta[2];
+                const int64_t nc = fmeta[3];
+                std::vector<std::vector<int64_t>> rps(3 * (size_t)nlev);
+                std::vector<std::vector<int32_t>> cis(3 * (size_t)nlev);
+                std::vector<std::vector<double>> vs(3 * (size_t)nlev);
+                std::vector<int32_t> nrow((size_t)std::max(nlev, 1), 0);
+                for (int l = 0; l < nlev; ++l)
+                    for (int which = 0; which < 3; ++which) {
+                        const size_t k = 3 * (size_t)l + which;
+                        const auto shape = rd.get<int64_t>();
+                        if (which == 0) nrow[l] = (int32_t)shape[0];
+                        rps[k] = rd.get<int64_t>();
+                        cis[k] = rd.get<int32_t>();
+                        vs[k] = rd.get<double>();
+                    }
+                const auto dense = rd.get<double>();
+                std::vector<const int64_t*> Arp(nlev), Prp(nlev), Rrp(nlev);
+                std::vector<const int32_t*> Aci(nlev), Pci(nlev), Rci(nlev);
+                std::vector<const double*> Av(nlev), Pv(nlev), Rv(nlev);
+                for (int l = 0; l < nlev; ++l) {
+                    auto ptrs = [&](int which, const int64_t*& r, const int32_t*& c, const double*& v) {
+                        const size_t k = 3 * (size_t)l + which;
+                        r = rps[k].empty() ? nullptr : rps[k].data();
+                        c = cis[k].empty() ? nullptr : cis[k].data();
+                        v = vs[k].empty() ? nullptr : vs[k].data();
+                        // an empty operator still passes valid (empty) arrays when it has rows
+                        static const int32_t no_ci = 0;
+                        static const double no_v = 0.0;
+                        if (r && !c) c = &no_ci;
+                        if (r && !v) v = &no_v;
+                    };
+                    ptrs(0, Arp[l], Aci[l], Av[l]);
+                    ptrs(1, Prp[l], Pci[l], Pv[l]);
+                    ptrs(2, Rrp[l], Rci[l], Rv[l]);
+                }
+                const auto vm = rd.get<int64_t>();
+                const int m = (int)vm[0];
+                const auto V = rd.get<double>();
+                offsets[p + 1] = offsets[p] + (coarse ? m : 0);
+                if (coarse)
+                    for (int a = 0; a < m; ++a)
+                        for (int j = 0; j < nl; ++j) {
+                            const double v = V[(size_t)a * nl + j];
+                            if (v != 0.0) wt.emplace_back(j < nI ? begin + j : ghosts[j - nI], offsets[p] + a, v);
+                        }
+                if (status == S2L_OK)
+                    status = s2l_gpu_add_subdomain_amg(setup_, p, begin, nI, nG, ghosts.data(), D.data(), nlev, sweeps,
+                                                       nrow.data(), Arp.data(), Aci.data(), Av.data(), Prp.data(),
+                                                       Pci.data(), Pv.data(), Rrp.data(), Rci.data(), Rv.data(), (int)nc,
+                                                       nc ? dense.data() : nullptr, coarse ? m : 0,
+                                                       coarse ? V.data() : nullptr);
+                continue;
+            }
             const int kind = (int)fmeta[0], single = (int)fmeta[1];
             const auto pin = rd.get<int32_t>();
             const auto pout = rd.get<int32_t>();
@@ -332,7 +458,8 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
             Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor> Er = E;
             status = s2l_gpu_set_coarse(setup_, n0, offsets.data(), Er.data());
         }
-        if (status == S2L_OK && refactorize) status = s2l_gpu_setup_option(setup_, "refactor", 1.0);
+        // factors are refactorized on the device; AMG hierarchies on the host, then uploaded again
+        if (status == S2L_OK && refactorize_ && !amg_on_) status = s2l_gpu_setup_option(setup_, "refactor", 1.0);
         if (status == S2L_OK) status = s2l_gpu_setup_end(setup_);
         if (status != S2L_OK) msg = ctx_ ? s2l_gpu_last_error(ctx_) : "no CUDA device";
     }
@@ -343,6 +470,7 @@ GpuSolvePhase::~GpuSolvePhase()
 {
     if (setup_) s2l_gpu_setup_destroy(setup_);
     if (ctx_) s2l_gpu_destroy(ctx_);
+    if (amg_) s2l_amg_free(amg_);
 }
 
 void GpuSolvePhase::check(int status, const char* what) const
@@ -377,13 +505,19 @@ bool GpuSolvePhase::preconditionerCurrent() const { return prec_version_ == sd_-
 
 void GpuSolvePhase::pushValues(prec::UpdateLevel level)
 {
+    const bool refac = level == prec::UpdateLevel::Refactorize;
+    if (refac && amg_on_) {  // AMG local solvers: the hierarchies again on the host, a new setup
+        buildAmg(cfg_.amg_reuse);
+        upload();
+        op_version_ = prec_version_ = sd_->valuesVersion();
+        return;
+    }
     const std::vector<core::Scalar>& v = sd_->system().val;
     std::vector<double> all;
     if (rank_ == 0) all.resize(nnz_counts_.empty() ? 0 : (size_t)nnz_displs_.back() + nnz_counts_.back());
     MPI_Gatherv(v.data(), (int)v.size(), MPI_DOUBLE, rank_ == 0 ? all.data() : nullptr,
                 rank_ == 0 ? nnz_counts_.data() : nullptr, rank_ == 0 ? nnz_displs_.data() : nullptr, MPI_DOUBLE, 0,
                 comm_);
-    const bool refac = level == prec::UpdateLevel::Refactorize;
     int st = S2L_OK;
     if (rank_ == 0)
         st = refac ? s2l_gpu_refactor(setup_, all.data(), S2L_PTR_HOST)

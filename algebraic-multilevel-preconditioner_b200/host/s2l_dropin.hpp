@@ -48,6 +48,10 @@ public:
      * @param hbm_budget Device bytes the setup may use (0 = no limit).
      * @param refactorize Keep the factor patterns on the device so that update(Refactorize) can
      *                    refactorize there (setup option "refactor").
+     * With --local-approx amg every rank builds the AMG hierarchy of its A_ii with the library's
+     * host setup (s2l_amg_build, the reference's AMGCL setup restated; FP64 only), and
+     * update(Refactorize) builds it again (or, with --amg-reuse, keeps its transfer operators) and
+     * uploads the setup anew with the kept coarse basis.
      */
     GpuSolvePhase(const schwarz2lvl::part::Subdomain& sd, const schwarz2lvl::prec::OneLevelSchwarz& one,
                   const schwarz2lvl::prec::TwoLevelSchwarz* two, const schwarz2lvl::core::SolverConfig& cfg,
@@ -77,6 +81,12 @@ public:
     bool preconditionerCurrent() const;
 
 private:
+    /// @brief This rank's part (rows, ghosts, D, local factors or AMG levels, V) to rank 0, which
+    ///        uploads every part as a new device setup (collective).
+    void upload();
+    /// @brief This rank's AMG hierarchy of sd.Aii() (collective: every rank agrees on the status).
+    void buildAmg(bool keep_transfer);
+
     MPI_Comm comm_;
     int rank_ = 0, np_ = 1;
     schwarz2lvl::core::GlobalIndex n_ = 0;
@@ -86,6 +96,15 @@ private:
     const schwarz2lvl::part::Subdomain* sd_ = nullptr;
     std::vector<int> nnz_counts_, nnz_displs_;  // matrix values per rank (rank 0)
     long op_version_ = 0, prec_version_ = 0;     // Subdomain::valuesVersion() of the device copies
+    // what upload() needs again after a refactorization of AMG local solvers
+    schwarz2lvl::core::SolverConfig cfg_;
+    int device_ = 0;
+    size_t hbm_budget_ = 0;
+    bool refactorize_ = false, coarse_ = false, amg_on_ = false;
+    int factorization_ = 0;     // linalg::Factorization of the reference's local solver (factors)
+    std::vector<double> V_;     // this rank's coarse basis (column-major, n_local x m_)
+    int m_ = 0;
+    s2l_amg* amg_ = nullptr;    // this rank's AMG hierarchy (--local-approx amg)
 };
 
 /// @brief z = M^{-1} r on the GPU: the two-level (or one-level) Schwarz apply of the reference.
@@ -97,7 +116,8 @@ public:
     /// @brief The reference's update contract (include/preconditioner/preconditioner.hpp:64-96,
     ///        src/preconditioner/two_level_schwarz.cpp:30-41), collective: Reuse keeps the
     ///        preconditioner (the device operator takes the new values), Refactorize refactorizes on
-    ///        the device (returns Reuse when already up to date); Rebuild recomputes the coarse basis
+    ///        the device (AMG local solvers: on the host, then uploaded; returns Reuse when already
+    ///        up to date); Rebuild recomputes the coarse basis
     ///        on the host and needs a new GpuSolvePhase (std::logic_error).
     schwarz2lvl::prec::UpdateLevel update(schwarz2lvl::prec::UpdateLevel requested) override;
     bool upToDate() const override { return phase_->preconditionerCurrent(); }

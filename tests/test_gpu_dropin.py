@@ -34,6 +34,17 @@ CASES = {
     "laplace2d_bicgstab_openfoam_atol": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--coarse",
                                              "additive", "--local-factorization", "lu", "--krylov", "bicgstab",
                                              "--stop-norm", "openfoam", "--rtol", "0", "--atol", "1e-9"]),
+    # AMG local solvers (--local-approx amg): every rank's hierarchy from the library's host setup
+    "bubbles3d_amg_sa": (4, ["--generate", "bubbles3d", "--nx", "16", "--nbubbles", "8", "--radius", "0.12",
+                             "--nev", "10", "--coarse", "deflated", "--local-factorization", "cholesky",
+                             "--restart", "50", "--local-approx", "amg", "--amg-coarse-enough", "100"]),
+    "bubbles3d_amg_sa_reuse": (4, ["--generate", "bubbles3d", "--nx", "16", "--nbubbles", "8", "--radius", "0.12",
+                                   "--nev", "10", "--coarse", "deflated", "--local-factorization", "cholesky",
+                                   "--restart", "50", "--local-approx", "amg", "--amg-coarse-enough", "100",
+                                   "--amg-reuse", "1"]),
+    "convdiff3d_amg_rs": (4, ["--generate", "convdiff3d", "--nx", "12", "--nev", "8", "--coarse", "deflated",
+                              "--local-factorization", "lu", "--restart", "40", "--local-approx", "amg",
+                              "--amg-coarsening", "rs", "--amg-coarse-enough", "50"]),
 }
 
 
@@ -58,6 +69,11 @@ UPDATE_CASES = {
     "laplace2d_lu_additive_refactorize": ("refactorize", "laplace2d_ras_additive_lu"),
     "convdiff3d_single_lu_refactorize": ("refactorize", "convdiff3d_single_lu"),
     "laplace2d_asm_mult_refactorize": ("refactorize", "laplace2d_asm_mult_bicgstab"),
+    # AMG: a new hierarchy, or the transfer operators kept (--amg-reuse), uploaded as a new setup
+    "bubbles3d_amg_refactorize": ("refactorize", "bubbles3d_amg_sa"),
+    "bubbles3d_amg_reuse_refactorize": ("refactorize", "bubbles3d_amg_sa_reuse"),
+    "convdiff3d_amg_rs_refactorize": ("refactorize", "convdiff3d_amg_rs"),
+    "bubbles3d_amg_reuse_level": ("reuse", "bubbles3d_amg_sa"),
 }
 
 
