@@ -85,3 +85,23 @@ def test_amg_setups_refuse_block_calls_and_refactor(ctx):
     with pytest.raises(S2LError) as e:
         GpuSetup(ctx, st, options={"refactor": 1})
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("coarsening", ["sa", "rs"])
+def test_amg_local_solve_is_a_fixed_linear_operator(ctx, coarsening):
+    """As the reference requires of its AMG local solver (test/test_inexact.cpp:6-9, for plain
+    GMRES): B(b1 + 2 b2) = B b1 + 2 B b2 to rounding, and the same right-hand side twice gives
+    bitwise-identical results, for the local solves and the two-level apply."""
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup("bubbles3d", local_approx="amg", amg_coarse_enough=100, amg_coarsening=coarsening)
+    g = GpuSetup(ctx, st)
+    rng = np.random.default_rng(77)
+    for i in (0, st.nsub - 1):
+        n = st.subdomains[i].n_local
+        b1, b2 = rng.standard_normal(n), rng.standard_normal(n)
+        y1, y2, y12 = g.local_solve(i, b1), g.local_solve(i, b2), g.local_solve(i, b1 + 2.0 * b2)
+        assert rel(y12, y1 + 2.0 * y2) <= 1e-13
+        assert np.array_equal(g.local_solve(i, b1), y1)
+    r = rng.standard_normal(st.n)
+    assert np.array_equal(g.apply(r), g.apply(r))
+    g.close()
