@@ -264,3 +264,14 @@ def test_oracle_two_level_with_amg_local_solves(name, kw):
     assert r["converged"]
     assert np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
     o.close()
+
+
+def test_amg_local_solvers_keep_the_coarse_space():
+    """As in the reference (test/test_inexact.cpp:12-15): with --local-approx amg only the local
+    solves change; the coarse basis and E are those of the exact-factor setup."""
+    _, st = small_setup("bubbles3d")
+    _, sa = small_setup("bubbles3d", local_approx="amg", amg_coarse_enough=100)
+    assert np.array_equal(st.offsets, sa.offsets)
+    for a, b in zip(st.subdomains, sa.subdomains):
+        assert np.array_equal(a.V, b.V) and a.factor is not None and b.factor is None and b.amg is not None
+    assert np.array_equal(st.E, sa.E)
