@@ -147,3 +147,29 @@ def test_refactor_needs_the_option(ctx):
         g.refactor(st.A.data)
     assert e.value.code == 7
     g.close()
+
+
+def test_refactor_makes_the_coarse_correction_consistent_with_the_new_matrix(ctx):
+    """The reference's check of update(Refactorize) (test/test_reuse.cpp:16-19): with Q = W E^-1 W^T,
+    W^T (r - A Q r) = 0 for the new A once E is recomputed, and not while the preconditioner is kept
+    (Reuse: the operator has the new values, E the old ones)."""
+    from s2l_b200.capi import GpuSetup
+    _, st = small_setup("bubbles3d")
+    g = GpuSetup(ctx, st, options={"refactor": 1})
+    rows, cols, vals = [], [], []
+    for i, s in enumerate(st.subdomains):
+        l2g = s.l2g()
+        for a in range(s.V.shape[1]):
+            rows.append(l2g)
+            cols.append(np.full(l2g.size, st.offsets[i] + a))
+            vals.append(s.V[:, a])
+    W = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(st.n, st.n0))
+    A2 = _new_values(st, 77, True)
+    r = np.random.default_rng(8).standard_normal(st.n)
+    scale = np.linalg.norm(W.T @ r)
+    g.update_matrix(A2.data)
+    stale = np.linalg.norm(W.T @ (r - A2 @ g.coarse_apply(r))) / scale
+    g.refactor(A2.data)
+    fresh = np.linalg.norm(W.T @ (r - A2 @ g.coarse_apply(r))) / scale
+    assert fresh <= 1e-10 and stale > 1e-4, (fresh, stale)
+    g.close()
