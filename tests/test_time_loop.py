@@ -215,3 +215,24 @@ def test_time_loop_amg_refactorizes_on_the_host(reuse):
     A1 = W.make_problem(dataclasses.replace(w, time=1.0)).A
     want, _ = seqmod.values_in_setup_order(A1, st0)
     assert np.array_equal(st1.A.data, want)
+
+
+def test_time_loop_from_matrix_market_files_matches_the_generator(tmp_path):
+    """The reference's --matrix p_%02d.mtx sequence (test/test_reuse.cpp:446-470): the same
+    sequence read from Matrix Market files gives the same setups and refactorizations."""
+    import dataclasses
+    import scipy.io
+    w = small_bubbles()
+    for s in range(3):
+        scipy.io.mmwrite(str(tmp_path / f"p_{s:02d}.mtx"), W.make_problem(dataclasses.replace(w, time=float(s))).A)
+    gen, log_gen = run(w, steps=3, correctors=1, reuse="refactor")
+    Recorder.log = []
+    files = run_time_loop(w, TimeLoopConfig(steps=3, correctors=1, reuse="refactor"), make_solver=Recorder, workers=1,
+                          matrix=lambda s: seqmod.read_mtx(str(tmp_path / f"p_{s:02d}.mtx")))
+    log_files = list(Recorder.log)
+    assert levels(files) == levels(gen) == "211"
+    ref_gen = [e[1] for e in log_gen if e[0] == "refactor"]
+    ref_files = [e[1] for e in log_files if e[0] == "refactor"]
+    assert len(ref_gen) == len(ref_files) == 2
+    for a, b in zip(ref_gen, ref_files):
+        assert np.array_equal(a, b)
