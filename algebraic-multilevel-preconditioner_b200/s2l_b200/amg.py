@@ -385,3 +385,18 @@ def rebuild_hierarchy(H: AmgHierarchy, A) -> AmgHierarchy:
     if H.coarse is not None:
         out.coarse = A.toarray()
     return out
+
+
+def build_hierarchy_native(A, coarse_enough: int = 500, sweeps: int = 1, coarsening: str = "sa") -> AmgHierarchy:
+    """build_hierarchy computed by the library's host setup (s2l_amg_build, the same algorithms in
+    C++, bit-identical levels) when libs2l_gpu.so is built, else by the Python restatement; used by
+    the setup producer, where the Python loops would dominate the setup of large subdomains."""
+    try:
+        from . import capi
+        N = capi.NativeAmg.build(A, coarse_enough, coarsening)
+    except FileNotFoundError:
+        return build_hierarchy(A, coarse_enough=coarse_enough, sweeps=sweeps, coarsening=coarsening)
+    try:
+        return N.hierarchy(sweeps=sweeps)
+    finally:
+        N.close()

@@ -336,9 +336,9 @@ def factorize_local(Aii: sp.csr_matrix, symmetric: bool, request: str, precision
 def _subdomain_work(args):
     Aii, Atil, D, opts, symmetric, want_coarse = args
     if opts.local_approx == "amg":
-        from .amg import build_hierarchy
-        fac = build_hierarchy(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps,
-                              coarsening=opts.amg_coarsening)
+        from .amg import build_hierarchy_native
+        fac = build_hierarchy_native(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps,
+                                     coarsening=opts.amg_coarsening)
     else:
         fac = factorize_local(Aii, symmetric, opts.local_factorization, opts.local_precision)
     Z, info = (local_coarse_vectors(Aii, Atil, D, opts, symmetric) if want_coarse
@@ -546,7 +546,7 @@ def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
     kept and E = W^T A_new W recomputed with it (``CoarseSpace::refresh``,
     ``src/preconditioner/coarse_space.cpp:95-105, 186-206``)."""
     import copy
-    from .amg import build_hierarchy, rebuild_hierarchy
+    from .amg import build_hierarchy_native, rebuild_hierarchy
     A_new = sp.csr_matrix(A_new, dtype=np.float64)
     A_new.sort_indices()
     if A_new.shape != st.A.shape:
@@ -562,8 +562,8 @@ def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
         if o.amg_reuse:
             H = rebuild_hierarchy(sd.amg, Aii)
         else:
-            H = build_hierarchy(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps,
-                                coarsening=o.amg_coarsening)
+            H = build_hierarchy_native(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps,
+                                       coarsening=o.amg_coarsening)
         ns = copy.copy(sd)
         ns.Aii = Aii
         ns.amg = H

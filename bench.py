@@ -541,7 +541,7 @@ def run_ours(a):
     amg_form = None
     if a.amg and a.workload == "bubbles3d":
         import dataclasses
-        from s2l_b200.amg import build_hierarchy
+        from s2l_b200.amg import build_hierarchy_native as build_hierarchy
         t0a = time.time()
         subs_amg = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii)) for sd in st.subdomains]
         st_amg = dataclasses.replace(st, subdomains=subs_amg)
