@@ -324,3 +324,38 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
         if g is not None:
             g.close()
     return records
+
+
+def summary(records) -> dict:
+    """Totals of a time loop (``printTimeLoopSummary``, ``src/solver/time_loop.cpp:192-237``): the
+    initial setup, the updates per level after it (count and total time), the solves (time,
+    iterations average and maximum, converged count), and for correctors that differ from the last
+    one of a step (warm start, final tolerances) their iterations and times apart."""
+    if not records:
+        return {}
+    count = {lv: 0 for lv in UpdateLevel}
+    t_level = {lv: 0.0 for lv in UpdateLevel}
+    for r in records[1:]:  # the first solve's update is the initial setup
+        count[r.level] += 1
+        t_level[r.level] += r.t_update
+    its = [r.iterations for r in records]
+    out = {
+        "solves": len(records),
+        "converged": sum(1 for r in records if r.converged),
+        "initial_setup_s": records[0].t_update,
+        "updates_s": sum(t_level.values()),
+        "reuse": count[UpdateLevel.REUSE],
+        "refactorize": count[UpdateLevel.REFACTORIZE],
+        "refactorize_mean_s": t_level[UpdateLevel.REFACTORIZE] / max(count[UpdateLevel.REFACTORIZE], 1),
+        "rebuild": count[UpdateLevel.REBUILD],
+        "rebuild_mean_s": t_level[UpdateLevel.REBUILD] / max(count[UpdateLevel.REBUILD], 1),
+        "solves_s": sum(r.t_solve for r in records),
+        "iterations_mean": sum(its) / len(its),
+        "iterations_max": max(its),
+    }
+    out["total_s"] = out["initial_setup_s"] + out["updates_s"] + out["solves_s"]
+    for key, sel in (("correctors", [r for r in records if not r.final_corrector]),
+                     ("last_corrector", [r for r in records if r.final_corrector])):
+        out[key] = {"iterations_mean": sum(r.iterations for r in sel) / len(sel) if sel else 0.0,
+                    "solves_s": sum(r.t_solve for r in sel)}
+    return out

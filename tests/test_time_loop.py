@@ -236,3 +236,15 @@ def test_time_loop_from_matrix_market_files_matches_the_generator(tmp_path):
     assert len(ref_gen) == len(ref_files) == 2
     for a, b in zip(ref_gen, ref_files):
         assert np.array_equal(a, b)
+
+
+def test_time_loop_summary_counts_levels_after_the_initial_setup():
+    from s2l_b200.time_loop import summary
+    w = small_bubbles()
+    recs, _ = run(w, steps=3, correctors=2, reuse="refactor")
+    s = summary(recs)
+    assert s["solves"] == 6 and s["converged"] == 6
+    assert (s["reuse"], s["refactorize"], s["rebuild"]) == (3, 2, 0)
+    assert s["initial_setup_s"] == recs[0].t_update and s["iterations_max"] == 10
+    assert abs(s["total_s"] - (s["initial_setup_s"] + s["updates_s"] + s["solves_s"])) < 1e-12
+    assert s["last_corrector"]["iterations_mean"] == 10.0 and summary([]) == {}
