@@ -374,7 +374,7 @@ def rebuild_hierarchy(H: AmgHierarchy, A) -> AmgHierarchy:
     """The hierarchy of new values of the same matrix with H's transfer operators kept: every
     coarser operator is recomputed as R (A P) and the coarsest is solved directly again
     (AMGCL's ``amg::rebuild``, ``amg.hpp:250-269``, ``level::rebuild``; the reference's
-    refactorize() with ``--amg-reuse``, ``src/linalg/inexact_solver.cpp:73-85``)."""
+    refactorize() with ``--amg-reuse``, ``src/linalg/inexact_solver.cpp:77-89``)."""
     A = _sorted_csr(sp.csr_matrix(A, dtype=np.float64))
     if H.n != A.shape[0]:
         raise ValueError(f"rebuild: {A.shape[0]} rows, the hierarchy has {H.n}")

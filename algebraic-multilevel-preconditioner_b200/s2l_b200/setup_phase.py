@@ -541,7 +541,7 @@ def with_factor_precision(st: Setup, precision: str) -> Setup:
 def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
     """The setup after the reference's Refactorize with AMG local solvers, for new values of A
     (renumbered ordering, same pattern): every subdomain's hierarchy is set up again on its new
-    A_ii (``AmgSolver::refactorize``, ``src/linalg/inexact_solver.cpp:73-85``: a new hierarchy, or
+    A_ii (``AmgSolver::refactorize``, ``src/linalg/inexact_solver.cpp:77-89``: a new hierarchy, or
     with ``amg_reuse`` the kept transfer operators and new Galerkin products), the coarse basis is
     kept and E = W^T A_new W recomputed with it (``CoarseSpace::refresh``,
     ``src/preconditioner/coarse_space.cpp:95-105, 186-206``)."""

@@ -1,7 +1,7 @@
 """Sequences of solves with setup reuse: the reference's time loop and reuse policy on the device.
 
 The reference emulates the pressure equation of a PISO/PIMPLE loop (``runTimeLoop``,
-``src/solver/time_loop.cpp:58-190``): every step has new matrix values on the same pattern, every
+``src/solver/time_loop.cpp:57-195``): every step has new matrix values on the same pattern, every
 corrector of a step a new right-hand side; before each solve a ``ReusePolicy``
 (``include/preconditioner/reuse_policy.hpp``, ``src/preconditioner/reuse_policy.cpp``) chooses the
 ``UpdateLevel`` and the preconditioner performs it.  Here the three levels map onto the device
@@ -47,7 +47,7 @@ class UpdateLevel(enum.IntEnum):
 
 
 class ReusePolicy:
-    """Chooses the update level before each solve of a sequence (``reuse_policy.hpp:65-150``).
+    """Chooses the update level before each solve of a sequence (``reuse_policy.hpp:63-132``).
 
     Modes ``off`` (rebuild before every solve), ``refactor`` (never rebuild after the first setup)
     and ``auto`` (reuse on an unchanged matrix, refactorize on a changed one, rebuild once the time
@@ -218,7 +218,7 @@ def _device_solver(ctx, options):
 
 def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, rhs=None, make_solver=None,
                   options=None, part=None, symmetric=None, workers=None, out=None) -> list:
-    """``cfg.steps`` steps of ``cfg.correctors`` solves of workload `w` (``time_loop.cpp:58-190``).
+    """``cfg.steps`` steps of ``cfg.correctors`` solves of workload `w` (``time_loop.cpp:57-195``).
 
     matrix(step): the matrix of a step (CSR, original ordering; default: the workload's problem at
     time = step, the moving-bubble sequence for bubbles3d; Matrix Market files through
@@ -327,7 +327,7 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
 
 
 def summary(records) -> dict:
-    """Totals of a time loop (``printTimeLoopSummary``, ``src/solver/time_loop.cpp:192-237``): the
+    """Totals of a time loop (``printTimeLoopSummary``, ``src/solver/time_loop.cpp:197-240``): the
     initial setup, the updates per level after it (count and total time), the solves (time,
     iterations average and maximum, converged count), and for correctors that differ from the last
     one of a step (warm start, final tolerances) their iterations and times apart."""

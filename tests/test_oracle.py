@@ -267,7 +267,7 @@ def test_oracle_two_level_with_amg_local_solves(name, kw):
 
 
 def test_amg_local_solvers_keep_the_coarse_space():
-    """As in the reference (test/test_inexact.cpp:12-15): with --local-approx amg only the local
+    """As in the reference (test/test_inexact.cpp:15-18): with --local-approx amg only the local
     solves change; the coarse basis and E are those of the exact-factor setup."""
     _, st = small_setup("bubbles3d")
     _, sa = small_setup("bubbles3d", local_approx="amg", amg_coarse_enough=100)

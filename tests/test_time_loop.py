@@ -218,7 +218,7 @@ def test_time_loop_amg_refactorizes_on_the_host(reuse):
 
 
 def test_time_loop_from_matrix_market_files_matches_the_generator(tmp_path):
-    """The reference's --matrix p_%02d.mtx sequence (test/test_reuse.cpp:446-470): the same
+    """The reference's --matrix p_%02d.mtx sequence (test/test_reuse.cpp:446-471): the same
     sequence read from Matrix Market files gives the same setups and refactorizations."""
     import dataclasses
     import scipy.io
