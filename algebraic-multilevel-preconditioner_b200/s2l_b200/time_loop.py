@@ -252,6 +252,8 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
     final_rtol = cfg.final_rtol if cfg.final_rtol is not None else w.rtol
     final_atol = cfg.final_atol if cfg.final_atol is not None else cfg.atol
     of_stop = cfg.stop_norm == "openfoam"
+    # FP32 factors: converged only at the recomputed FP64 true residual, as the drop-in's solver
+    strict = w.opts.local_precision == "single"
 
     if part is None or symmetric is None:
         prob0 = W.make_problem(dataclasses.replace(w, time=0.0))
@@ -300,10 +302,11 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
                 rtol, atol = (final_rtol, final_atol) if (final_tols and last) else (w.rtol, cfg.atol)
                 t0 = time.perf_counter()
                 if w.krylov == "bicgstab":
-                    x, res = g.bicgstab(b, x0=x, rtol=rtol, maxit=cfg.maxit, stop_norm=cfg.stop_norm, atol=atol)
+                    x, res = g.bicgstab(b, x0=x, rtol=rtol, maxit=cfg.maxit, strict=strict, stop_norm=cfg.stop_norm,
+                                        atol=atol)
                 else:
                     x, res = g.gmres(b, x0=x, restart=w.restart, rtol=rtol, maxit=cfg.maxit, flexible=w.flexible,
-                                     stop_norm=cfg.stop_norm, atol=atol)
+                                     strict=strict, stop_norm=cfg.stop_norm, atol=atol)
                 t_solve = time.perf_counter() - t0
                 hist = res["history"]
                 r0 = res["initial_residual_of"] if of_stop else (float(hist[0]) if len(hist) else 1.0)
@@ -317,7 +320,7 @@ def run_time_loop(w: "W.Workload", cfg: TimeLoopConfig, ctx=None, matrix=None, r
                                   float(res["initial_residual_of"]), float(res["final_residual_of"]), last)
                 records.append(rec)
                 if out is not None:
-                    out.write(f"{step:7d}{corr:5d}  {level.name.capitalize():<12}{t_update:10.4f}{t_solve:10.4f}"
+                    out.write(f"{step:7d}{corr:5d}  {level.name.lower():<12}{t_update:10.4f}{t_solve:10.4f}"
                               f"{rec.iterations:5d}{rec.per_decade:11.2f}{rec.n0:8d}{rec.wasted:11.4f}"
                               f"{'' if rec.converged else '  NOT converged'}\n")
     finally:

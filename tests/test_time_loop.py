@@ -119,7 +119,8 @@ class Recorder:
         self.A = sp.csr_matrix((np.asarray(vals), self.st.A.indices, self.st.A.indptr), shape=self.st.A.shape)
         Recorder.log.append(("refactor", np.array(vals)))
 
-    def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, stop_norm="l2", atol=0.0):
+    def gmres(self, b, x0=None, restart=30, rtol=1e-8, maxit=1000, flexible=False, strict=False, stop_norm="l2",
+              atol=0.0):
         Recorder.log.append(("gmres", np.array(x0), rtol, atol, stop_norm, np.array(b)))
         x = sp.linalg.spsolve(self.A.tocsc(), b)
         r0 = np.linalg.norm(b - self.A @ x0) / np.linalg.norm(b)
