@@ -362,3 +362,85 @@ def summary(records) -> dict:
         out[key] = {"iterations_mean": sum(r.iterations for r in sel) / len(sel) if sel else 0.0,
                     "solves_s": sum(r.t_solve for r in sel)}
     return out
+
+
+def parse_args(argv=None):
+    """(workload, TimeLoopConfig, device) from the reference's sequence flags (``--steps``,
+    ``--correctors``, ``--reuse``, ``--rebuild-growth``, ``--rebuild-every``, ``--warm-start``,
+    ``--final-rtol``, ``--final-atol``, ``--stop-norm``, ``--atol``, ``--maxit``, ``--local-approx``,
+    ``--amg-*``) and a named workload of this package at a chosen size."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m s2l_b200.time_loop",
+                                 description="A sequence of solves with setup reuse on the GPU.")
+    ap.add_argument("--workload", default="bubbles3d", choices=["poisson2d", "bubbles3d", "convdiff3d"])
+    ap.add_argument("--nx", type=int, default=0, help="grid size (0: the workload's)")
+    ap.add_argument("--nsub", type=int, default=0, help="subdomains (0: the workload's)")
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--correctors", type=int, default=3)
+    ap.add_argument("--reuse", default="auto", choices=["off", "refactor", "auto"])
+    ap.add_argument("--rebuild-growth", type=float, default=4.0)
+    ap.add_argument("--rebuild-every", type=int, default=0)
+    ap.add_argument("--warm-start", action="store_true")
+    ap.add_argument("--final-rtol", type=float, default=-1.0, help="< 0: rtol")
+    ap.add_argument("--final-atol", type=float, default=-1.0, help="< 0: atol")
+    ap.add_argument("--stop-norm", default="l2", choices=["l2", "openfoam"])
+    ap.add_argument("--atol", type=float, default=0.0)
+    ap.add_argument("--maxit", type=int, default=1000)
+    ap.add_argument("--local-approx", default="none", choices=["none", "amg"])
+    ap.add_argument("--amg-coarsening", default="sa", choices=["sa", "rs"])
+    ap.add_argument("--amg-sweeps", type=int, default=1)
+    ap.add_argument("--amg-coarse-enough", type=int, default=500)
+    ap.add_argument("--amg-reuse", type=int, default=0)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    if a.workload == "poisson2d":
+        w = W.poisson2d(a.nx or 200, a.nsub or 8)
+    elif a.workload == "convdiff3d":
+        w = W.convdiff3d(a.nx or 128, a.nsub or 128)
+    else:
+        w = W.bubbles3d(a.nx or 100, a.nsub or 64)
+    w.opts.local_approx = a.local_approx
+    w.opts.amg_coarsening = a.amg_coarsening
+    w.opts.amg_sweeps = a.amg_sweeps
+    w.opts.amg_coarse_enough = a.amg_coarse_enough
+    w.opts.amg_reuse = bool(a.amg_reuse)
+    if a.local_approx == "amg":
+        w.opts.local_precision = "double"  # the device AMG is FP64
+        w.flexible = False
+    cfg = TimeLoopConfig(steps=a.steps, correctors=a.correctors, reuse=a.reuse, rebuild_growth=a.rebuild_growth,
+                         rebuild_every=a.rebuild_every, warm_start=a.warm_start,
+                         final_rtol=a.final_rtol if a.final_rtol >= 0.0 else None,
+                         final_atol=a.final_atol if a.final_atol >= 0.0 else None, stop_norm=a.stop_norm,
+                         atol=a.atol, maxit=a.maxit)
+    cfg.validate()
+    return w, cfg, a.device
+
+
+def main(argv=None) -> int:
+    """Runs the loop on the GPU and prints every solve and the totals, as the reference's
+    ``--steps`` run does; exit status 0 when every solve converged, 2 otherwise."""
+    import sys
+    from . import capi
+    w, cfg, device = parse_args(argv)
+    ctx = capi.Context(device)
+    try:
+        sys.stdout.write(f"Time loop: {cfg.steps} steps x {cfg.correctors} correctors, reuse {cfg.reuse}, "
+                         f"{w.name} {w.nx}, {w.nsub} subdomains\n"
+                         "   step corr  level         update[s]  solve[s]  its  it/decade      n0  wasted[s]\n")
+        recs = run_time_loop(w, cfg, ctx=ctx, out=sys.stdout)
+    finally:
+        ctx.close()
+    s = summary(recs)
+    sys.stdout.write(f"Time loop summary (reuse {cfg.reuse}, {s['solves']} solves, {s['converged']} converged)\n"
+                     f"  initial setup              {s['initial_setup_s']:.3f} s\n"
+                     f"  updates                    {s['updates_s']:.3f} s   (reuse {s['reuse']} x, refactorize "
+                     f"{s['refactorize']} x {s['refactorize_mean_s']:.3f} s, rebuild {s['rebuild']} x "
+                     f"{s['rebuild_mean_s']:.3f} s)\n"
+                     f"  solves                     {s['solves_s']:.3f} s   (iterations avg {s['iterations_mean']:.1f}, "
+                     f"max {s['iterations_max']})\n"
+                     f"  total setup + updates + solves {s['total_s']:.3f} s\n")
+    return 0 if s["converged"] == s["solves"] else 2
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -249,3 +249,17 @@ def test_time_loop_summary_counts_levels_after_the_initial_setup():
     assert s["initial_setup_s"] == recs[0].t_update and s["iterations_max"] == 10
     assert abs(s["total_s"] - (s["initial_setup_s"] + s["updates_s"] + s["solves_s"])) < 1e-12
     assert s["last_corrector"]["iterations_mean"] == 10.0 and summary([]) == {}
+
+
+def test_command_line_maps_the_reference_flags():
+    from s2l_b200.time_loop import parse_args
+    w, cfg, dev = parse_args(["--workload", "poisson2d", "--nx", "40", "--nsub", "4", "--steps", "5", "--correctors",
+                              "2", "--reuse", "refactor", "--rebuild-every", "3", "--warm-start", "--final-rtol",
+                              "1e-6", "--stop-norm", "openfoam", "--atol", "1e-12", "--local-approx", "amg",
+                              "--amg-coarsening", "rs", "--amg-reuse", "1"])
+    assert (w.name, w.nx, w.nsub) == ("poisson2d", 40, 4)
+    assert (cfg.steps, cfg.correctors, cfg.reuse, cfg.rebuild_every, cfg.warm_start) == (5, 2, "refactor", 3, True)
+    assert cfg.final_rtol == 1e-6 and cfg.final_atol is None and cfg.stop_norm == "openfoam" and cfg.atol == 1e-12
+    assert w.opts.local_approx == "amg" and w.opts.amg_coarsening == "rs" and w.opts.amg_reuse and dev == 0
+    with pytest.raises(ValueError):
+        parse_args(["--correctors", "0"])
