@@ -34,6 +34,8 @@ CASES = {
     "laplace2d_bicgstab_openfoam_atol": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--coarse",
                                              "additive", "--local-factorization", "lu", "--krylov", "bicgstab",
                                              "--stop-norm", "openfoam", "--rtol", "0", "--atol", "1e-9"]),
+    "laplace2d_ldlt_deflated": (3, ["--generate", "laplace2d", "--nx", "24", "--nev", "6", "--coarse", "deflated",
+                                    "--local-factorization", "ldlt"]),
     # a coupled problem (2 unknowns per cell, nonsymmetric): the solve phase is block-agnostic CSR
     "coupled2d_ncomp2_lu": (4, ["--generate", "coupled2d", "--nx", "20", "--ncomp", "2", "--nev", "8", "--coarse",
                                 "deflated", "--local-factorization", "lu", "--restart", "40"]),
