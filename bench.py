@@ -42,7 +42,7 @@ for _p in (REPO, PKG):
 METRIC = "solve time to FP64 residual 1e-8 (mixed/batched vs plain FP64 GPU); p50/p99 latency"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--serve-mix", type=int, default=0,
                     help="serving-mix form: requests over 40 seeded cases of the three families (0 = off)")
     ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ------------------------------------------------------------------------------------ clocks
@@ -852,6 +852,13 @@ def cpu_baseline(st, iterations: int, restart: int) -> dict:
 
 
 # ------------------------------------------------------------------------------------ reference arm
+def reference_workload(a):
+    """The headline workload at the sizes of the arguments (0: the workload's own, 100^3 and 64
+    subdomains): the reference runs one thread-rank per subdomain on the same partition."""
+    from s2l_b200 import workloads as W
+    return W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
@@ -865,7 +872,7 @@ def run_reference(a):
     from s2l_b200 import workloads as W
     from s2l_b200.rng import random_rhs  # noqa: F401  (the reference draws the same rhs itself)
 
-    wl = W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
+    wl = reference_workload(a)
     prob = W.make_problem(wl)
     part = W.make_partition(wl, prob).astype(np.int32)
     threads = a.ref_threads or os.cpu_count() or 1
@@ -874,7 +881,7 @@ def run_reference(a):
         write_mtx(mtx, prob.A)
         pf = os.path.join(td, "part.bin")
         part.tofile(pf)
-        env = dict(os.environ, S2L_NP=str(a.nsub), S2L_PART_FILE=pf, OMP_NUM_THREADS="1",
+        env = dict(os.environ, S2L_NP=str(wl.nsub), S2L_PART_FILE=pf, OMP_NUM_THREADS="1",
                    S2L_REF_THREADS=str(threads))
         cmd = [binary, "--matrix", mtx, "--rhs", "random", "--seed", str(wl.seed), "--pou", "boolean",
                "--one-level", "ras", "--coarse", "deflated", "--nev", "20", "--local-solver", "sparselu",
@@ -894,14 +901,14 @@ def run_reference(a):
         "metric": METRIC, "impl": "reference", "value": value, "unit": "solves/s", "n_gpus": a.gpus,
         "steps": len(per), "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (same generator, partition and rhs)",
-        "config": {"workload": f"bubbles3d {a.nx}^3 pressure Poisson, {a.nsub} subdomains, overlap 1 (the "
+        "config": {"workload": f"bubbles3d {wl.nx}^3 pressure Poisson, {wl.nsub} subdomains, overlap 1 (the "
                                f"reference has no overlap 2), nev 20, deflated RAS, Eigen LL^T, root coarse "
                                f"solver, GMRES(50), rtol 1e-8",
                    "n": int(prob.n), "iterations": rec.get("iterations"), "setup_s": rec.get("setup_s"),
                    "true_rel_residual": rec.get("true_rel_residual")},
         "p50_ms": float(np.percentile(np.array(per) * 1e3, 50)), "p99_ms": float(np.percentile(np.array(per) * 1e3, 99)),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(per)} full solves, {a.nsub} thread-ranks on {threads} host threads"},
+                         "sample": f"{len(per)} full solves, {wl.nsub} thread-ranks on {threads} host threads"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

@@ -66,3 +66,27 @@ def test_reference_arm_runs_on_rank_zero_only():
     p = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0 and p.stdout.strip() == ""
+
+
+def test_reference_arm_runs_the_workload_sizes():
+    """The reference arm runs one thread-rank per subdomain of the workload: by default the
+    headline's 100^3 and 64 subdomains (not the 0 that stands for "the workload's" in the flags);
+    on a small case its line names the sizes it ran."""
+    import importlib.util
+    import json
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(REPO, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    wl = bench.reference_workload(bench.parse([]))
+    assert (wl.nx, wl.nsub) == (100, 64)
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "s2l_ref")):
+        return
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1")
+    p = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--nx", "12",
+                        "--nsub", "4", "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads([l for l in p.stdout.splitlines() if l.startswith("{")][-1])
+    assert "12^3" in line["config"]["workload"] and "4 subdomains" in line["config"]["workload"]
+    assert line["cpu_baseline"]["sample"].startswith("1 full solves, 4 thread-ranks")
+    assert line["config"]["true_rel_residual"] <= 1.1e-8
