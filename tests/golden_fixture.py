@@ -15,8 +15,9 @@ KINDS = {0: "lu", 1: "llt", 2: "ldlt"}
 
 
 def cases():
-    # the AMG fixtures (amg_*.npz, tests/golden/make_amg_golden.py) are of another kind
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("amg_"))
+    # the AMG fixtures (amg_*.npz) and the generator fixture (*_generator.npz) are of other kinds
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and not f.startswith("amg_") and not f.endswith("_generator.npz"))
 
 
 def _flag(cmd: list, name: str, default: str) -> str:

@@ -275,3 +275,22 @@ def test_amg_local_solvers_keep_the_coarse_space():
     for a, b in zip(st.subdomains, sa.subdomains):
         assert np.array_equal(a.V, b.V) and a.factor is not None and b.factor is None and b.amg is not None
     assert np.array_equal(st.E, sa.E)
+
+
+def test_bubbles_generator_reproduces_the_reference_fixture():
+    """The bubbles3d generator (s2l_b200.problems.bubbles, single radius) against the reference's
+    own 24^3 fixture (test/gamg/run_gamg_23038420/check_s2l*.mtx: nb=150, R=0.04, rho_ratio=1000,
+    cfl=0.5, t=3, seed=2024; tests/golden/make_bubbles_fixture.py): the same pattern, values and
+    generated right-hand side to rounding."""
+    import hashlib
+    from s2l_b200 import problems
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "bubbles3d_24_generator.npz"))
+    p = problems.bubbles(3, 24, nbubbles=150, radius=0.04, rho_ratio=1000.0, cfl=0.5, time=3.0, seed=2024)
+    A = p.A.tocsr()
+    A.sort_indices()
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(A.indptr, dtype=np.int64).tobytes())
+    h.update(np.ascontiguousarray(A.indices, dtype=np.int64).tobytes())
+    assert h.hexdigest() == str(g["pattern_sha256"])
+    assert np.abs(A.data - g["data"]).max() <= 1e-13 * np.abs(g["data"]).max()
+    assert np.abs(p.rhs_generated - g["rhs"]).max() <= 1e-13 * np.abs(g["rhs"]).max()
