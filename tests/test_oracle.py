@@ -294,3 +294,24 @@ def test_bubbles_generator_reproduces_the_reference_fixture():
     assert h.hexdigest() == str(g["pattern_sha256"])
     assert np.abs(A.data - g["data"]).max() <= 1e-13 * np.abs(g["data"]).max()
     assert np.abs(p.rhs_generated - g["rhs"]).max() <= 1e-13 * np.abs(g["rhs"]).max()
+
+
+@pytest.mark.parametrize("fixture,make", [
+    ("laplace2d_ras_additive_lu", lambda P: P.laplace(2, 24)),
+    ("laplace2d_asm_deflated_mult", lambda P: P.laplace(2, 20)),
+    ("bubbles3d_ras_deflated_llt", lambda P: P.bubbles(3, 12, nbubbles=6, radius=0.15, rho_ratio=1000.0)),
+])
+def test_generators_reproduce_the_reference_golden_matrices(fixture, make):
+    """The laplace2d and bubbles3d generators against the matrices the reference's own generator
+    produced for the golden fixtures (tests/golden/make_golden.py), in the fixture's numbering."""
+    import scipy.sparse as sp
+    from s2l_b200 import problems
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture + ".npz"))
+    n = g["global_A_rp"].size - 1
+    R = sp.csr_matrix((g["global_A_v"], g["global_A_ci"], g["global_A_rp"]), shape=(n, n))
+    n2o = g["global_new_to_old"]
+    A = make(problems).A.tocsr()[n2o][:, n2o].tocsr()
+    A.sort_indices()
+    R.sort_indices()
+    assert np.array_equal(A.indptr, R.indptr) and np.array_equal(A.indices, R.indices)
+    assert abs(A - R).max() <= 1e-13 * abs(R).max()
