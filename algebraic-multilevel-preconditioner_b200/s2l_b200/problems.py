@@ -101,6 +101,113 @@ def laplace(dim: int, nx: int, ny: int = 0, nz: int = 0) -> Problem:
     return Problem(A, (nx, ny, nz), True, desc, rhs)
 
 
+def _segment_distance(px, py, ax, ay, bx, by):
+    vx, vy = bx - ax, by - ay
+    t = np.clip(((px - ax) * vx + (py - ay) * vy) / (vx * vx + vy * vy), 0.0, 1.0)
+    dx, dy = px - (ax + t * vx), py - (ay + t * vy)
+    return np.sqrt(dx * dx + dy * dy)
+
+
+def kappa(x, y):
+    """The reference's heterogeneous diffusivity (``MatrixGenerator::kappa``,
+    ``src/utils/matrix_generators.cpp:33-44``): 2 in a rectangle, 0.06 in two channels and in a
+    periodic lattice of square inclusions, 1 elsewhere."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    px, py = np.fmod(x, 0.2) - 0.1, np.fmod(y, 0.2) - 0.1
+    k = np.where((np.abs(px) < 0.035) & (np.abs(py) < 0.035), 6e-2, 1.0)
+    k = np.where(_segment_distance(x, y, 0.55, 0.62, 0.90, 0.35) < 0.03, 6e-2, k)
+    k = np.where(_segment_distance(x, y, 0.15, 0.62, 0.75, 0.70) < 0.04, 6e-2, k)
+    return np.where((x >= 0.10) & (x <= 0.45) & (y >= 0.12) & (y <= 0.30), 2.0, k)
+
+
+def convdiff(dim: int, nx: int, ny: int = 0, nz: int = 0, nu: float = 1.0, ncomp: int = 1, pulse: float = 0.0,
+             time: float = 0.0, pulse_period: int = 20, coupled: bool = False) -> Problem:
+    """The reference's convdiff{2d,3d} and coupled{2d,3d} generators (``--generate``,
+    ``src/utils/matrix_generators.cpp:57-192``): upwind finite volumes of -div(nu kappa grad u) +
+    div(V u) with the Section-4.2 velocity (exact face integrals of V.n, scaled by
+    1 + pulse sin(2 pi t / period)), harmonic-mean diffusivity on x/y faces, Dirichlet faces
+    (2D: y = 0 -> 0, y = 1 -> 1; 3D: z = 0 -> 1, z = 1 -> 0); `coupled` repeats it for ncomp
+    components (viscosity nu (1 + c)) with a nonsymmetric cyclic coupling between them."""
+    ny = ny or nx
+    nz = (nz or nx) if dim == 3 else 1
+    nc = max(1, ncomp) if coupled else 1
+    hx, hy = 1.0 / nx, 1.0 / ny
+    hz = 1.0 / nz if dim == 3 else 1.0
+    ncell = nx * ny * nz
+    n = ncell * nc
+    conv = 1.0 + pulse * np.sin(2.0 * np.pi * time / max(1, pulse_period))
+    c = np.arange(ncell, dtype=np.int64)
+    i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
+    kP = kappa((i + 0.5) * hx, (j + 0.5) * hy)
+    x0, x1, y0, y1 = i * hx, (i + 1) * hx, j * hy, (j + 1) * hy
+    z0, z1 = k * hz, (k + 1) * hz
+
+    def P1(t):
+        return t * t - t
+
+    rows, cols, vals = [], [], []
+    rhs = np.zeros(n)
+
+    def face(m, N, geom, F):
+        P = c[m]
+        F = F * conv
+        for comp in range(nc):
+            D = nu * (1.0 + comp) * geom
+            p, q = P * nc + comp, N * nc + comp
+            rows.extend([p, p, q, q])
+            cols.extend([p, q, q, p])
+            vals.extend([D + np.maximum(F, 0.0), -D - np.maximum(-F, 0.0), D + np.maximum(-F, 0.0),
+                         -D - np.maximum(F, 0.0)])
+
+    m = i + 1 < nx
+    kN = kappa((i[m] + 1.5) * hx, (j[m] + 0.5) * hy)
+    kf = 2.0 * kP[m] * kN / (kP[m] + kN)
+    xf = x1[m]
+    if dim == 2:
+        F = xf * (1.0 - xf) * (P1(y1[m]) - P1(y0[m]))
+    else:
+        F = 2.0 * xf * (1.0 - xf) * (P1(y1[m]) - P1(y0[m])) * 0.5 * (z1[m] * z1[m] - z0[m] * z0[m])
+    face(m, c[m] + 1, kf * (hy * hz) / hx, F)
+    m = j + 1 < ny
+    kN = kappa((i[m] + 0.5) * hx, (j[m] + 1.5) * hy)
+    kf = 2.0 * kP[m] * kN / (kP[m] + kN)
+    yf = y1[m]
+    F = -yf * (1.0 - yf) * (P1(x1[m]) - P1(x0[m])) * (1.0 if dim == 2 else (z1[m] - z0[m]))
+    face(m, c[m] + nx, kf * (hx * hz) / hy, F)
+    if dim == 3:
+        m = k + 1 < nz
+        zf = z1[m]
+        F = -zf * (1.0 - zf) * (P1(x1[m]) - P1(x0[m])) * (P1(y1[m]) - P1(y0[m]))
+        face(m, c[m] + nx * ny, kP[m] * (hx * hy) / hz, F)
+    if dim == 2:
+        bnd = [(j == 0, kP * hx / (0.5 * hy), 0.0), (j == ny - 1, kP * hx / (0.5 * hy), 1.0)]
+    else:
+        bnd = [(k == 0, kP * hx * hy / (0.5 * hz), 1.0), (k == nz - 1, kP * hx * hy / (0.5 * hz), 0.0)]
+    for m, geom, ub in bnd:
+        for comp in range(nc):
+            D = nu * (1.0 + comp) * geom[m]
+            p = c[m] * nc + comp
+            rows.append(p)
+            cols.append(p)
+            vals.append(D)
+            np.add.at(rhs, p, D * ub)
+    if nc > 1:
+        gamma = nu * (hy / hx if dim == 2 else hy * hz / hx)
+        for comp in range(nc):
+            p = c * nc + comp
+            rows.extend([p, p])
+            cols.extend([p, c * nc + (comp + 1) % nc])
+            vals.extend([np.full(ncell, gamma), np.full(ncell, -gamma)])
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    name = ("coupled" if coupled else "convdiff") + f"{dim}d"
+    desc = f"{name} {nx}x{ny}" + (f"x{nz}" if dim == 3 else "") + f" nu={nu:g}" + \
+        (f" ncomp={nc}" if nc > 1 else "") + f" (n={n}, nnz={A.nnz})"
+    return Problem(A, (nx, ny, nz), False, desc, rhs)
+
+
 def bubble_alpha(dim, nx, ny, nz, nbubbles, radius, cfl, time, seed, radius_cells=None):
     """Gas fraction of every cell (``include/utils/bubble_field.hpp:56-117,150-156``).
 

@@ -300,9 +300,10 @@ def test_bubbles_generator_reproduces_the_reference_fixture():
     ("laplace2d_ras_additive_lu", lambda P: P.laplace(2, 24)),
     ("laplace2d_asm_deflated_mult", lambda P: P.laplace(2, 20)),
     ("bubbles3d_ras_deflated_llt", lambda P: P.bubbles(3, 12, nbubbles=6, radius=0.15, rho_ratio=1000.0)),
+    ("convdiff3d_ras_deflated_lu_single", lambda P: P.convdiff(3, 10)),
 ])
 def test_generators_reproduce_the_reference_golden_matrices(fixture, make):
-    """The laplace2d and bubbles3d generators against the matrices the reference's own generator
+    """The laplace2d, bubbles3d and convdiff3d generators against the matrices the reference's own generator
     produced for the golden fixtures (tests/golden/make_golden.py), in the fixture's numbering."""
     import scipy.sparse as sp
     from s2l_b200 import problems
@@ -315,3 +316,24 @@ def test_generators_reproduce_the_reference_golden_matrices(fixture, make):
     R.sort_indices()
     assert np.array_equal(A.indptr, R.indptr) and np.array_equal(A.indices, R.indices)
     assert abs(A - R).max() <= 1e-13 * abs(R).max()
+
+
+def test_coupled_generator_structure():
+    """coupled2d (the reference's --generate coupled2d): ncomp unknowns per cell; component c is the
+    convection-diffusion operator with viscosity nu (1 + c) plus gamma on the diagonal, coupled to
+    component c + 1 (cyclically) by -gamma; with one component it is convdiff2d."""
+    import scipy.sparse as sp
+    from s2l_b200 import problems
+    cpl = problems.convdiff(2, 12, ncomp=3, coupled=True)
+    n = 144
+    assert cpl.A.shape == (3 * n, 3 * n) and not cpl.symmetric
+    A = cpl.A.tocsr()
+    gamma = 1.0 * (1.0 / 12) / (1.0 / 12)
+    for comp in range(3):
+        idx = np.arange(n) * 3 + comp
+        block = A[idx][:, idx]
+        want = problems.convdiff(2, 12, nu=1.0 + comp).A + gamma * sp.identity(n)
+        assert abs(block - want).max() <= 1e-14 * abs(want).max()
+        nxt = np.arange(n) * 3 + (comp + 1) % 3
+        assert np.allclose(A[idx][:, nxt].toarray(), -gamma * np.eye(n))
+    assert abs(problems.convdiff(2, 12, ncomp=1, coupled=True).A - problems.convdiff(2, 12).A).max() == 0.0
