@@ -70,6 +70,15 @@ def convdiff3d(nx=128, nsub=128, precision="single") -> Workload:
                     restart=40, flexible=True)
 
 
+def reference_generator(kind: str, nx=32, nsub=8, **extra) -> Workload:
+    """A workload on one of the reference's own generators (``--generate convdiff2d`` etc.):
+    kind reference_convdiff2d | reference_convdiff3d | reference_coupled2d | reference_coupled3d;
+    extra: nu, ncomp, pulse, pulse_period.  Deflated RAS, LU factors, GMRES(40)."""
+    return Workload(kind, kind, nx, nsub,
+                    SchwarzOptions(one_level="ras", coarse="deflated", pou="boolean", overlap=1, nev=8,
+                                   local_factorization="lu"), restart=40, extra=dict(extra))
+
+
 def make_problem(w: Workload):
     if w.kind == "laplace2d":
         return problems.laplace(2, w.nx)
@@ -80,11 +89,22 @@ def make_problem(w: Workload):
                                 time=w.time, seed=w.extra.get("bubble_seed", 2024))
     if w.kind == "convdiff3d":
         return problems.convdiff_fourier(w.nx, seed=w.extra.get("field_seed", 7))
+    if w.kind in ("reference_convdiff2d", "reference_convdiff3d", "reference_coupled2d", "reference_coupled3d"):
+        # the reference's own --generate convdiff{2d,3d} / coupled{2d,3d}; with a pulse the
+        # convection changes with the time step (a nonsymmetric sequence on one pattern)
+        e = w.extra
+        return problems.convdiff(3 if w.kind.endswith("3d") else 2, w.nx, nu=e.get("nu", 1.0),
+                                 ncomp=e.get("ncomp", 4), pulse=e.get("pulse", 0.0), time=w.time,
+                                 pulse_period=e.get("pulse_period", 20), coupled="coupled" in w.kind)
     raise ValueError(f"unknown workload kind {w.kind}")
 
 
 def make_partition(w: Workload, prob) -> np.ndarray:
-    return partmod.rcb(prob.cell_coords().astype(np.float64), w.nsub, imbalance=w.imbalance)
+    """Subdomain of every unknown: cells by recursive coordinate bisection, the unknowns of a cell
+    (coupled problems) with their cell."""
+    part = partmod.rcb(prob.cell_coords().astype(np.float64), w.nsub, imbalance=w.imbalance)
+    per_cell = prob.A.shape[0] // part.size
+    return np.repeat(part, per_cell) if per_cell > 1 else part
 
 
 def build(w: Workload, workers=None, use_cache=True):

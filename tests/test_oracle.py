@@ -337,3 +337,21 @@ def test_coupled_generator_structure():
         nxt = np.arange(n) * 3 + (comp + 1) % 3
         assert np.allclose(A[idx][:, nxt].toarray(), -gamma * np.eye(n))
     assert abs(problems.convdiff(2, 12, ncomp=1, coupled=True).A - problems.convdiff(2, 12).A).max() == 0.0
+
+
+@pytest.mark.parametrize("kind,extra", [("reference_convdiff2d", {"pulse": 0.5, "pulse_period": 10}),
+                                        ("reference_coupled2d", {"ncomp": 2})])
+def test_reference_generator_workloads_solve(kind, extra):
+    """Workloads on the reference's own generators (nonsymmetric convdiff with a pulsating
+    convection, coupled with two unknowns per cell): the setup builds, the unknowns of a cell stay
+    in one subdomain, and the oracle's two-level GMRES converges."""
+    from s2l_b200 import workloads as W
+    w = W.reference_generator(kind, nx=20, nsub=4, **extra)
+    st = W.build(w, workers=1, use_cache=False)
+    part = st.stats["part"]
+    if kind.endswith("coupled2d"):
+        assert st.n == 2 * 400 and np.array_equal(part[0::2], part[1::2])
+    o = OracleSetup(st)
+    x, res = o.gmres(st.b, restart=w.restart, rtol=1e-8)
+    assert res["converged"] and np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
+    o.close()

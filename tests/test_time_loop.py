@@ -263,3 +263,13 @@ def test_command_line_maps_the_reference_flags():
     assert w.opts.local_approx == "amg" and w.opts.amg_coarsening == "rs" and w.opts.amg_reuse and dev == 0
     with pytest.raises(ValueError):
         parse_args(["--correctors", "0"])
+
+
+def test_time_loop_on_the_reference_pulsating_convection():
+    """The reference's own nonsymmetric sequence (convdiff2d, pulse 0.5, period 10, as its reuse
+    test): every step refactorizes with new values on the same pattern."""
+    w = W.reference_generator("reference_convdiff2d", nx=16, nsub=4, pulse=0.5, pulse_period=10)
+    recs, log = run(w, steps=3, correctors=1, reuse="refactor")
+    assert levels(recs) == "211"
+    vals = [e[1] for e in log if e[0] == "refactor"]
+    assert len(vals) == 2 and not np.array_equal(vals[0], vals[1])
