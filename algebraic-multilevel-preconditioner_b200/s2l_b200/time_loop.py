@@ -372,7 +372,14 @@ def parse_args(argv=None):
     import argparse
     ap = argparse.ArgumentParser(prog="python -m s2l_b200.time_loop",
                                  description="A sequence of solves with setup reuse on the GPU.")
-    ap.add_argument("--workload", default="bubbles3d", choices=["poisson2d", "bubbles3d", "convdiff3d"])
+    ap.add_argument("--workload", default="bubbles3d",
+                    choices=["poisson2d", "bubbles3d", "convdiff3d", "reference_convdiff2d", "reference_convdiff3d",
+                             "reference_coupled2d", "reference_coupled3d"],
+                    help="reference_*: the reference's own --generate convdiff/coupled problems")
+    ap.add_argument("--nu", type=float, default=1.0, help="reference_*: viscosity")
+    ap.add_argument("--ncomp", type=int, default=4, help="reference_coupled*: unknowns per cell")
+    ap.add_argument("--pulse", type=float, default=0.0, help="reference_*: amplitude of the convection pulsation")
+    ap.add_argument("--pulse-period", type=int, default=20, help="reference_*: period of the pulsation [steps]")
     ap.add_argument("--nx", type=int, default=0, help="grid size (0: the workload's)")
     ap.add_argument("--nsub", type=int, default=0, help="subdomains (0: the workload's)")
     ap.add_argument("--steps", type=int, default=4)
@@ -393,7 +400,10 @@ def parse_args(argv=None):
     ap.add_argument("--amg-reuse", type=int, default=0)
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
-    if a.workload == "poisson2d":
+    if a.workload.startswith("reference_"):
+        w = W.reference_generator(a.workload, nx=a.nx or 32, nsub=a.nsub or 8, nu=a.nu, ncomp=a.ncomp,
+                                  pulse=a.pulse, pulse_period=a.pulse_period)
+    elif a.workload == "poisson2d":
         w = W.poisson2d(a.nx or 200, a.nsub or 8)
     elif a.workload == "convdiff3d":
         w = W.convdiff3d(a.nx or 128, a.nsub or 128)

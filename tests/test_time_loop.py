@@ -263,6 +263,8 @@ def test_command_line_maps_the_reference_flags():
     assert w.opts.local_approx == "amg" and w.opts.amg_coarsening == "rs" and w.opts.amg_reuse and dev == 0
     with pytest.raises(ValueError):
         parse_args(["--correctors", "0"])
+    w, _, _ = parse_args(["--workload", "reference_coupled2d", "--nx", "16", "--ncomp", "2", "--pulse", "0.5"])
+    assert w.kind == "reference_coupled2d" and w.extra == {"nu": 1.0, "ncomp": 2, "pulse": 0.5, "pulse_period": 20}
 
 
 def test_time_loop_on_the_reference_pulsating_convection():
