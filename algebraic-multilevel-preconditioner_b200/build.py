@@ -28,20 +28,37 @@ def build_gpu_lib(force: bool = False, verbose: bool = False, ptxas_info: bool =
     if not force and not ptxas_info and _newer(GPU_LIB, deps):
         return GPU_LIB
     os.makedirs(LIB_DIR, exist_ok=True)
+    obj_dir = os.path.join(LIB_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-shared",
-           "-I", os.path.join(REPO, "include"), "-o", GPU_LIB + ".tmp"]
+    common = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off",
+              "-I", os.path.join(REPO, "include")]
     if ptxas_info:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-lcublas", "-lcusolver", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
+        common += ["-Xptxas", "-v"]
+
+    def compile_one(f):  # one translation unit (they only share host launch wrappers)
+        obj = os.path.join(obj_dir, f + ".o")
+        cmd = common + ["-c", os.path.join(CSRC, f), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(SOURCES)) as ex:
+        done = list(ex.map(compile_one, SOURCES))
+    for obj, r in done:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({r.returncode}) on {obj}:\n{r.stdout}\n{r.stderr}")
+        if ptxas_info:
+            sys.stdout.write(r.stderr)
+    cuda_lib = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
+    cmd = [nvcc, *ARCH, "-shared", "-o", GPU_LIB + ".tmp", *[o for o, _ in done], "-lcublas", "-lcusolver",
+           "-Xlinker", f"-rpath,{cuda_lib}"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
-    if ptxas_info:
-        sys.stdout.write(r.stderr)
+        raise RuntimeError(f"nvcc link failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
     os.replace(GPU_LIB + ".tmp", GPU_LIB)
     return GPU_LIB
 

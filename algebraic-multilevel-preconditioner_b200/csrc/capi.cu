@@ -28,6 +28,9 @@
 using namespace s2l;
 
 struct s2l_ticket;
+namespace {
+struct Runner;
+}
 
 // Worker threads of the asynchronous solves (s2l_gpu_serve_start / s2l_gpu_submit)
 struct s2l_serve {
@@ -36,6 +39,10 @@ struct s2l_serve {
     std::deque<s2l_ticket*> queue;
     std::vector<std::thread> workers;
     bool stop = false;
+    // continuous batching (s2l_gpu_serve_batching): slots per block runner (< 0 automatic, 0 off)
+    // and the runners at work
+    int slots = -1;
+    std::vector<Runner*> runners;
 };
 
 struct s2l_ctx {
@@ -45,6 +52,10 @@ struct s2l_ctx {
     std::string err;
     std::mutex mu;
     s2l_serve* serve = nullptr;
+    // device address of the static scratch of s2l_gpu_coarse_apply_noalloc, looked up by the first
+    // such call on this context (with its device current); a context created after a reset of the
+    // device looks it up anew
+    double* noalloc_scratch = nullptr;
 };
 
 namespace {
@@ -187,6 +198,8 @@ struct s2l_setup {
     int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0,
         opt_tpr = 0;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
+    std::atomic<int> opt_spin_limit{S2L_SPIN_LIMIT};  // polls of a sweep wait before it gives up
+    double opt_pivot_tol = 1e-6;  // refactorization of LU factors: largest multiplier 1 / pivot_tol
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
     int64_t st_levels_max = 0, st_levels_sum = 0;  // sweep dependency levels (both factors)
@@ -217,6 +230,7 @@ struct s2l_setup {
     unsigned prof_mask = 0;              // s2l_gpu_profile_enable: inherited by new workspaces
 
     std::atomic<int> pending{0};  // asynchronous solves queued or running on this setup
+    std::atomic<int> runners{0};  // block runners of the serving workers holding a workspace of it
 
     // AMG local solvers (s2l_gpu_add_subdomain_amg): level spaces and block-diagonal operators
     struct AmgDev {
@@ -1122,6 +1136,7 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
     a.K = 1;
     a.KC = 1;
     a.nloc = s->nloc;
+    a.spin_limit = s->opt_spin_limit.load();
     return a;
 }
 
@@ -1313,7 +1328,7 @@ int ensure_block(s2l_work* w, int K, int m, bool flex)
         D(&B.y, (size_t)std::max<int64_t>(s->n0, 1) * K);
     }
     D(&B.V, (size_t)n * K * (m + 1));
-    if (flex) D(&B.Z, (size_t)n * K * m);
+    if (flex) D(&B.Z, (size_t)n * K * (m + 1));  // m + 1: the serving runners keep Z in a ring like V
     D(&B.r, (size_t)n * K);
     D(&B.z, (size_t)n * K);
     D(&B.kw, (size_t)n * K);
@@ -2259,6 +2274,19 @@ int amg_build(s2l_setup* s)
     return S2L_OK;
 }
 
+// A block runner of the serving workers gives its workspace back right after its last request
+// finishes.  Calls that need the setup idle (update, refactor, destroy) wait for that, bounded, when
+// no request is queued or running on the setup.
+int wait_runners_gone(s2l_setup* s)
+{
+    if (s->pending.load() > 0) return S2L_OK;  // the caller refuses
+    for (int i = 0; s->runners.load() > 0; ++i) {
+        if (i > 100000) return s->fail(S2L_ERR_STATE, "a serving block runner still holds a workspace of this setup");
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+    return S2L_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -3050,6 +3078,7 @@ int s2l_gpu_setup_destroy(s2l_setup* s)
 {
     if (!s) return S2L_OK;
     if (s->pending.load() > 0) return s->fail(S2L_ERR_STATE, "asynchronous solves are queued or running on this setup");
+    RET_IF(wait_runners_gone(s));
     cudaSetDevice(s->ctx->device);
     for (s2l_work* w : s->works) work_destroy(w);
     if (s->setup_stream) cudaStreamSynchronize(s->setup_stream);
@@ -3077,6 +3106,7 @@ int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind)
     if (!val) return s->fail(S2L_ERR_BADARG, "null values");
     if (ptr_kind != S2L_PTR_HOST && ptr_kind != S2L_PTR_DEVICE)
         return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
+    RET_IF(wait_runners_gone(s));
     std::lock_guard<std::mutex> g(s->wmu);  // no call can take a workspace meanwhile
     for (char b : s->busy)
         if (b) return s->fail(S2L_ERR_STATE, "update_matrix while a solve-phase call runs on the setup");
@@ -3167,6 +3197,7 @@ int refactor_dense_tails(s2l_setup* s, cudaStream_t st)
             R.llt[i] ? cusolverDnDpotrf(R.tsolver[q], CUBLAS_FILL_MODE_UPPER, sz, Si, sz, R.swork[q], R.lwork, R.info + i)
                      : cusolverDnDgetrf(R.tsolver[q], sz, sz, Si, sz, R.swork[q], nullptr, R.info + i);
         if (cs != CUSOLVER_STATUS_SUCCESS) return s->fail(S2L_ERR_CUDA, "dense tail factorization failed to launch");
+        if (!R.llt[i]) launch_tail_growth(R.tstream[q], Si, sz, s->opt_pivot_tol, R.err);
     }
     return tails_join(s, st);
 }
@@ -3286,6 +3317,7 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     a.ntc = R.ntc;
     a.S = R.S;
     a.err = R.err;
+    a.pivot_tol = s->opt_pivot_tol;
     a.smax = 1;
     for (int sz : R.sz) a.smax = std::max(a.smax, sz);
     a.maxcol = R.maxcol;
@@ -3313,6 +3345,10 @@ int refactor_run(s2l_setup* s, const double* val, int ptr_kind)
     if (herr == 0 && coarse && (infos[nsub] != 0 || infos[nsub + 1] != 0)) herr = 3;
     if (herr == 1) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a sparse column");
     if (herr == 2) return s->fail(S2L_ERR_NUMERIC, "refactorization: zero or non-positive pivot in a dense tail");
+    if (herr == 4)
+        return s->fail(S2L_ERR_NUMERIC, "refactorization: an LU pivot is below pivot_tol relative to its column (a "
+                                        "multiplier above 1 / pivot_tol); the kept pivot order no longer suits the "
+                                        "matrix: rebuild the factorization");
     if (herr == 3) return s->fail(S2L_ERR_NUMERIC, "refactorization: the coarse matrix is singular");
     if (herr) return s->fail(S2L_ERR_NUMERIC, "refactorization failed");
     // commit: the matrix, its row sums, E^-1, then the solve layout of the new factors
@@ -3345,6 +3381,7 @@ int s2l_gpu_refactor(s2l_setup* s, const double* val, int ptr_kind)
     if (ptr_kind != S2L_PTR_HOST && ptr_kind != S2L_PTR_DEVICE)
         return s->fail(S2L_ERR_BADARG, "ptr_kind must be S2L_PTR_HOST or S2L_PTR_DEVICE");
     if (!s->rf.on) return s->fail(S2L_ERR_STATE, "the setup was built without the option refactor = 1");
+    RET_IF(wait_runners_gone(s));
     std::lock_guard<std::mutex> g(s->wmu);  // no call can take a workspace meanwhile
     for (char b : s->busy)
         if (b) return s->fail(S2L_ERR_STATE, "refactor while a solve-phase call runs on the setup");
@@ -3366,8 +3403,13 @@ int s2l_gpu_setup_bytes(const s2l_setup* s, size_t* bytes)
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
 {
     if (!s || !name) return S2L_ERR_BADARG;
-    if (s->ended) return s->fail(S2L_ERR_STATE, "setup_option after setup_end");
     const std::string n(name);
+    if (n == "spin_limit") {  // read at every launch: may change after setup_end
+        if (!(value >= 1.0 && value <= 2147483647.0)) return s->fail(S2L_ERR_BADARG, "spin_limit must be in [1, 2^31)");
+        s->opt_spin_limit.store((int)value);
+        return S2L_OK;
+    }
+    if (s->ended) return s->fail(S2L_ERR_STATE, "setup_option after setup_end");
     if (n == "tail_min") s->opt_tail_min = (int)value;
     else if (n == "tail_max") s->opt_tail_max = (int)value;
     else if (n == "tail_rows") s->opt_tail_rows = (int)value;
@@ -3393,6 +3435,9 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         s->opt_chain = c;
     } else if (n == "refactor") {
         s->opt_refactor = value != 0.0;
+    } else if (n == "pivot_tol") {
+        if (!(value >= 0.0 && value < 1.0)) return s->fail(S2L_ERR_BADARG, "pivot_tol must be in [0, 1)");
+        s->opt_pivot_tol = value;
     } else return s->fail(S2L_ERR_BADARG, "unknown setup option " + n);
     return S2L_OK;
 }
@@ -3545,26 +3590,22 @@ int s2l_gpu_coarse_apply(s2l_setup* s, const double* r, double* x0, int ptr_kind
 static __device__ __align__(256) double s2l_noalloc_scratch[S2L_NOALLOC_SCRATCH_DOUBLES];
 
 namespace {
-std::mutex g_noalloc_mu;
-std::vector<double*> g_noalloc_addr;  // per device, filled on the first call
-
+// The device address of the static scratch for the context's device.  The device is current when
+// this runs (the entry point sets it), so the lookup resolves the array of that device.
 int noalloc_scratch(s2l_setup* s, double** out)
 {
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    const int dev = s->ctx->device;
-    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
-    if (!g_noalloc_addr[dev]) {
-        int prev = 0;
-        CUDA_OK(s, cudaGetDevice(&prev));
-        CUDA_OK(s, cudaSetDevice(dev));
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (!s->ctx->noalloc_scratch) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, s2l_noalloc_scratch);
-        cudaSetDevice(prev);
-        if (e != cudaSuccess)
-            return s->fail(S2L_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
-        g_noalloc_addr[dev] = static_cast<double*>(p);
+        if (e != cudaSuccess) {
+            t_last_error = std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e);
+            s->ctx->err = t_last_error;
+            return S2L_ERR_CUDA;
+        }
+        s->ctx->noalloc_scratch = static_cast<double*>(p);
     }
-    *out = g_noalloc_addr[dev];
+    *out = s->ctx->noalloc_scratch;
     return S2L_OK;
 }
 }  // namespace
@@ -3580,22 +3621,29 @@ extern "C" int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, doubl
         return s->fail(S2L_ERR_BADARG, "coarse_apply_noalloc: this setup needs " + std::to_string(need) +
                                            " doubles of scratch; the static no-alloc scratch holds " +
                                            std::to_string(S2L_NOALLOC_SCRATCH_DOUBLES));
+    // the setup's device is made current, as every other solve-phase call does (its pointers and
+    // its stream belong to that device)
+    if (cudaSetDevice(s->ctx->device) != cudaSuccess) return s->fail(S2L_ERR_CUDA, "cudaSetDevice failed");
     double* scr = nullptr;
     RET_IF(noalloc_scratch(s, &scr));
-    // launched on the stream of workspace 0 (the caller's stream from s2l_gpu_set_stream)
-    s2l_work* w = s->works[0];
+    // the stream of workspace 0 (the caller's stream from s2l_gpu_set_stream) is read, and the
+    // kernels enqueued, under the workspace lock: s2l_gpu_set_stream, s2l_gpu_update_matrix and
+    // s2l_gpu_refactor take the same lock and cannot change the stream or the setup meanwhile
+    std::lock_guard<std::mutex> g(s->wmu);
+    cudaStream_t st = s->works[0]->stream;
     double* part = scr;
     double* c = part + (int64_t)s->ntiles * s->mmax;
     double* y = c + s->n0;
     double* plocal = y + s->n0;
-    launch_coarse_restrict(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
+    launch_coarse_restrict(st, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
                            boolean, r, s->mmax, part);
-    launch_coarse_reduce(w->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
-    launch_dense_gemv(w->stream, (int)s->n0, s->d_Einv, c, y);
-    launch_coarse_prolong(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
+    launch_coarse_reduce(st, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
+    launch_dense_gemv(st, (int)s->n0, s->d_Einv, c, y);
+    launch_coarse_prolong(st, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
                           plocal);
-    if (!boolean) launch_combine(w->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
-    CUDA_OK(w, cudaGetLastError());
+    if (!boolean) launch_combine(st, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("coarse_apply_noalloc launch: ") + cudaGetErrorString(e));
     return S2L_OK;
 }
 
@@ -4391,18 +4439,548 @@ void ticket_finish(s2l_ticket* t, int state, int status)
     t->cv.notify_all();
 }
 
+// ------------------------------------------------------------------------------ continuous batching
+// A block runner serves the GMRES requests of one setup (same restart length and variant) from one
+// workspace: up to K requests at once, each in a column slot of a block of K right-hand sides.
+// Every Arnoldi step runs the preconditioner, the product with A and both CGS2 passes once for all
+// occupied slots; each column keeps its own Hessenberg matrix, rotations, restart cycle and
+// convergence test (src/solver/gmres.cpp:18-161).  A request that arrives while the others run
+// takes a free slot at the next step boundary and starts its own cycle there; a column that
+// converges (or uses maxit) writes its solution out and frees its slot at once.
+//
+// Columns start their cycles at different steps, so the basis is a ring of restart + 1 blocks:
+// the basis vector of every running column at global step T sits in block T % (restart + 1), and a
+// column whose cycle started at step t0 owns the blocks of steps t0 .. T.  The orthogonalization
+// runs over the union of these windows with the coefficients of blocks outside a column's own
+// window set to zero: each column then computes exactly what it computes alone (the extra terms
+// add exact zeros), whatever the other slots hold.
+struct Runner {
+    s2l_setup* s = nullptr;
+    int m = 0;
+    bool flex = false;
+    int K = 1;
+    int free_slots = 0;  // slots not holding a request (guarded by the serve mutex)
+};
+
+bool batchable(const s2l_serve* sv, const s2l_ticket* t)
+{
+    const s2l_setup* s = t->s;
+    return sv->slots != 0 && t->method == S2L_KRYLOV_GMRES && t->opts.stop_norm == S2L_STOP_L2 &&
+           t->opts.atol == 0.0 && !s->amgd.on && t->opts.restart >= 1 && t->opts.restart <= 63 &&
+           t->opts.maxit >= 0 && t->opts.rtol >= 0.0;
+}
+
+bool runner_takes(const Runner* R, const s2l_ticket* t)
+{
+    return R->s == t->s && R->m == t->opts.restart && R->flex == (t->opts.flexible != 0);
+}
+
+// slots of a runner on setup s with restart m: the setting of s2l_gpu_serve_batching, or the
+// setup's best block width, and never more than the coefficient buffers hold
+int runner_width(const s2l_serve* sv, s2l_setup* s, int m)
+{
+    int K = sv->slots > 0 ? sv->slots : block_width_best(s);
+    int p = 1;
+    while (p * 2 <= K && p * 2 <= S2L_MAX_RHS && (m + 1) * p * 2 <= S2L_MAX_BLOCK_COLS) p *= 2;
+    return p;
+}
+
+struct Slot {
+    s2l_ticket* t = nullptr;
+    bool run = false;      // a restart cycle is running
+    bool ending = false;   // its cycle ended at the last step: solution update and restart test
+    bool cand = false, brk = false;
+    int64_t t0 = 0;        // global step of the cycle's first basis vector
+    int kr = 0;            // steps of the cycle so far
+    double bnorm = 0.0, beta = 0.0, hn = 0.0;
+    std::vector<double> H, cs, sn, g;
+};
+
+void slot_reset_cycle(Slot& c, int m)
+{
+    std::fill(c.H.begin(), c.H.end(), 0.0);
+    std::fill(c.g.begin(), c.g.end(), 0.0);
+    c.kr = 0;
+    c.cand = c.brk = false;
+    (void)m;
+}
+
+void block_runner(s2l_ctx* ctx, Runner* R, s2l_ticket* first)
+{
+    s2l_serve* sv = ctx->serve;
+    s2l_setup* s = R->s;
+    const int m = R->m, ring = m + 1;
+    const bool flex = R->flex;
+    std::vector<s2l_ticket*> incoming{first};
+    std::vector<Slot> slots;
+    // leaves the runner: every ticket still held fails with rc, the runner is deregistered
+    auto leave = [&](int rc, const std::string& msg) {
+        std::vector<s2l_ticket*> held;
+        for (auto& c : slots)
+            if (c.t) held.push_back(c.t);
+        for (s2l_ticket* t : incoming) held.push_back(t);
+        {
+            std::lock_guard<std::mutex> g(sv->mu);
+            auto it = std::find(sv->runners.begin(), sv->runners.end(), R);
+            if (it != sv->runners.end()) sv->runners.erase(it);
+        }
+        sv->cv.notify_all();
+        for (s2l_ticket* t : held) {
+            t->err = msg;
+            ticket_finish(t, rc == S2L_ERR_CANCELED ? S2L_JOB_CANCELED : S2L_JOB_DONE, rc);
+        }
+        delete R;
+    };
+    // the block buffers of K slots; when they do not fit the HBM budget (and no other workspace of
+    // the setup is busy to wait for), half as many slots
+    t_last_error.clear();
+    std::unique_ptr<Lease> lease;
+    for (;;) {
+        const int Kt = R->K;
+        lease.reset(new Lease(s, [&](s2l_work* lw) { return ensure_block(lw, Kt, m, flex); }));
+        if (lease->rc == S2L_ERR_OOM && Kt > 1) {
+            lease.reset();
+            std::lock_guard<std::mutex> g(sv->mu);
+            R->K = Kt / 2;
+            R->free_slots = R->K - 1;
+            continue;
+        }
+        break;
+    }
+    if (lease->rc != S2L_OK) {
+        leave(lease->rc, t_last_error);
+        return;
+    }
+    const int K = R->K;
+    slots.resize(K);
+    for (auto& c : slots) {
+        c.H.assign((size_t)(m + 1) * m, 0.0);
+        c.cs.assign(m, 0.0);
+        c.sn.assign(m, 0.0);
+        c.g.assign(m + 1, 0.0);
+    }
+    s2l_work* w = lease->w;
+    s2l_work::Block& B = w->blk;
+    const int64_t n = s->n, nK = n * K;
+    cudaStream_t st = w->stream;
+    const int MC = S2L_MAX_BLOCK_COLS;
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        leave(S2L_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    // a clean block: every ring block, the right-hand sides, iterates and work vectors zero
+    {
+        cudaError_t e = cudaSuccess;
+        for (double* p : {B.V, B.Z, B.b, B.xk, B.kw, B.r, B.z, B.u})
+            if (p && e == cudaSuccess)
+                e = cudaMemsetAsync(p, 0, (size_t)nK * sizeof(double) * (p == B.V || p == B.Z ? ring : 1), st);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    }
+    auto read = [&](int off, int count) -> int {
+        const cudaError_t e = cudaMemcpyAsync(B.h_red + off, B.red + off, count * sizeof(double),
+                                              cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+        return check_err(w);
+    };
+    auto hist = [&](Slot& c, double v) {
+        s2l_result* res = c.t->res;
+        if (res->history && res->history_len < c.t->opts.history_cap) res->history[res->history_len] = v;
+        if (res->history_len < c.t->opts.history_cap) ++res->history_len;
+    };
+    auto Hc = [&](Slot& c, int i, int j) -> double& { return c.H[(size_t)j * (m + 1) + i]; };
+    std::vector<int> done_slots;  // finished at this boundary: tickets to complete after the copies
+    std::vector<int> done_state, done_status;
+    std::vector<std::string> done_err;
+    auto complete = [&](int r, int state, int status, const std::string& err) {
+        done_slots.push_back(r);
+        done_state.push_back(state);
+        done_status.push_back(status);
+        done_err.push_back(err);
+    };
+    // solution column r out to its ticket (host or device), queued on the stream
+    auto write_out = [&](int r) -> int {
+        s2l_ticket* t = slots[r].t;
+        if (t->ptr_kind == S2L_PTR_DEVICE) {
+            launch_column_out(st, n, K, r, B.xk, t->x);
+            w->launches += 1;
+        } else {
+            double* stage = B.u;  // n doubles; the outputs of one boundary go one after another
+            launch_column_out(st, n, K, r, B.xk, stage);
+            w->launches += 1;
+            CUDA_OK(w, cudaMemcpyAsync(t->x, stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CUDA_OK(w, cudaStreamSynchronize(st));
+        }
+        return S2L_OK;
+    };
+    int64_t T = 0;  // the next Arnoldi step
+    for (;;) {
+        // ---------------------------------------------------------------- boundary before step T
+        done_slots.clear();
+        done_state.clear();
+        done_status.clear();
+        done_err.clear();
+        for (int r = 0; r < K; ++r)
+            if (slots[r].t && slots[r].t->cancel.load()) {
+                complete(r, S2L_JOB_CANCELED, S2L_ERR_CANCELED, "solve canceled");
+                slots[r].run = slots[r].ending = false;
+            }
+        // requests queued for this runner take the free slots
+        {
+            std::lock_guard<std::mutex> g(sv->mu);
+            int freeable = 0;
+            for (int r = 0; r < K; ++r)
+                if (!slots[r].t) ++freeable;
+            freeable -= (int)incoming.size();
+            for (auto it = sv->queue.begin(); it != sv->queue.end() && freeable > 0;) {
+                if (runner_takes(R, *it) && batchable(sv, *it) && !(*it)->cancel.load()) {
+                    incoming.push_back(*it);
+                    it = sv->queue.erase(it);
+                    --freeable;
+                    --R->free_slots;
+                } else {
+                    ++it;
+                }
+            }
+        }
+        std::vector<int> adm;
+        for (s2l_ticket* t : incoming) {
+            int r = 0;
+            while (slots[r].t) ++r;
+            slots[r].t = t;
+            slots[r].run = slots[r].ending = false;
+            t->t_start = std::chrono::steady_clock::now();
+            t->state.store(S2L_JOB_RUNNING);
+            s2l_result* res = t->res;
+            res->converged = res->breakdown = res->iterations = res->restarts = 0;
+            res->history_len = 0;
+            res->rel_residual = res->true_rel_residual = 0.0;
+            res->initial_residual_of = res->final_residual_of = 0.0;
+            adm.push_back(r);
+        }
+        incoming.clear();
+        bool any_end = false;
+        for (int r = 0; r < K; ++r) any_end = any_end || slots[r].ending;
+        int rc = S2L_OK;
+        if (any_end) {
+            // x += Z y (flexible) or x += M^-1 (V y) for the columns whose cycle ended at step T - 1
+            int64_t tmin = T;
+            for (int r = 0; r < K; ++r)
+                if (slots[r].ending) tmin = std::min(tmin, slots[r].t0);
+            const int Lw = (int)(T - tmin);
+            std::vector<double> coef((size_t)Lw * K, 0.0), y(m);
+            for (int r = 0; r < K; ++r) {
+                Slot& c = slots[r];
+                if (!c.ending) continue;
+                for (int i = c.kr - 1; i >= 0; --i) {
+                    double v = c.g[i];
+                    for (int q = i + 1; q < c.kr; ++q) v -= Hc(c, i, q) * y[q];
+                    y[i] = v / Hc(c, i, i);
+                }
+                const int off = (int)(c.t0 - tmin);
+                for (int i = 0; i < c.kr; ++i) coef[(size_t)(off + i) * K + r] = y[i];
+            }
+            cudaError_t e = cudaMemcpyAsync(B.coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+            {
+                Prof pr(w, PC_VEC);
+                launch_gemv_block(st, n, K, flex ? B.Z : B.V, nK, Lw, B.coef, B.u, (int)(tmin % ring), ring);
+                w->launches += 1;
+            }
+            ColScale one{};
+            for (int r = 0; r < K; ++r) one.v[r] = 1.0;
+            if (flex) {
+                Prof pr(w, PC_VEC);
+                launch_combine2_block(st, n, K, one, B.u, one, B.xk, B.xk);
+                w->launches += 1;
+            } else {
+                rc = apply_block(w, K, B.u, B.z);
+                if (rc != S2L_OK) return leave(rc, t_last_error);
+                Prof pr(w, PC_VEC);
+                launch_combine2_block(st, n, K, one, B.z, one, B.xk, B.xk);
+                w->launches += 1;
+            }
+        }
+        // the admitted requests' right-hand sides and initial guesses into their columns
+        for (int r : adm) {
+            s2l_ticket* t = slots[r].t;
+            const double* src[2] = {t->b, t->x};
+            double* dst[2] = {B.b, B.xk};
+            for (int q = 0; q < 2; ++q) {
+                if (t->ptr_kind == S2L_PTR_HOST) {
+                    cudaError_t e = cudaMemcpyAsync(B.u, src[q], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+                    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+                    launch_column_in(st, n, K, r, B.u, dst[q]);
+                } else {
+                    launch_column_in(st, n, K, r, src[q], dst[q]);
+                }
+                w->launches += 1;
+            }
+        }
+        if (any_end || !adm.empty()) {
+            if (!adm.empty()) {
+                Prof pr(w, PC_VEC);
+                launch_mdot_block(st, n, K, B.b, nK, 1, B.b, B.part, B.red);
+                w->launches += 2;
+            }
+            rc = spmv_block(w, K, B.xk, B.r, B.b, true);
+            if (rc == S2L_OK && !adm.empty()) rc = read(0, K);
+            if (rc == S2L_OK) rc = read(2 * MC, K);
+            if (rc != S2L_OK) return leave(rc, t_last_error);
+            for (int r = 0; r < K; ++r) {
+                Slot& c = slots[r];
+                if (!c.ending) continue;
+                c.ending = false;
+                s2l_result* res = c.t->res;
+                const s2l_krylov_opts& o = c.t->opts;
+                c.beta = std::sqrt(B.h_red[2 * MC + r]);
+                const double slack = o.strict_true_residual ? 1.0 : 1.1;
+                const bool within = c.beta <= o.rtol * c.bnorm;
+                const bool within_slack = c.beta <= slack * o.rtol * c.bnorm;
+                bool conv = c.cand;
+                if (c.brk) conv = within || conv;
+                if (conv && !within_slack) conv = false;
+                if (c.beta == 0.0) conv = true;
+                res->converged = conv ? 1 : 0;
+                res->true_rel_residual = c.beta / c.bnorm;
+                if (!std::isfinite(c.beta)) {
+                    complete(r, S2L_JOB_DONE, S2L_ERR_NUMERIC, "non-finite residual");
+                    c.run = false;
+                } else if (conv || res->iterations >= o.maxit) {
+                    if (write_out(r) != S2L_OK) return leave(S2L_ERR_CUDA, t_last_error);
+                    complete(r, S2L_JOB_DONE, S2L_OK, "");
+                    c.run = false;
+                } else {
+                    ++res->restarts;
+                    slot_reset_cycle(c, m);
+                    c.t0 = T;
+                    c.run = true;
+                }
+            }
+            for (int r : adm) {
+                Slot& c = slots[r];
+                s2l_result* res = c.t->res;
+                const s2l_krylov_opts& o = c.t->opts;
+                c.bnorm = std::sqrt(B.h_red[r]);
+                c.beta = std::sqrt(B.h_red[2 * MC + r]);
+                if (!std::isfinite(c.bnorm)) {
+                    complete(r, S2L_JOB_DONE, S2L_ERR_NUMERIC, "non-finite right-hand side");
+                    continue;
+                }
+                if (c.bnorm == 0.0) {  // x = 0 (src/solver/gmres.cpp:27-32)
+                    hist(c, 0.0);
+                    res->converged = 1;
+                    launch_column_fill(st, n, K, r, 1, nK, 0.0, B.xk);
+                    w->launches += 1;
+                    if (write_out(r) != S2L_OK) return leave(S2L_ERR_CUDA, t_last_error);
+                    complete(r, S2L_JOB_DONE, S2L_OK, "");
+                    continue;
+                }
+                if (!std::isfinite(c.beta)) {
+                    complete(r, S2L_JOB_DONE, S2L_ERR_NUMERIC, "non-finite residual");
+                    continue;
+                }
+                hist(c, c.beta / c.bnorm);
+                res->rel_residual = c.beta / c.bnorm;
+                res->true_rel_residual = c.beta / c.bnorm;
+                if (c.beta <= o.rtol * c.bnorm || o.maxit <= 0) {
+                    res->converged = c.beta <= o.rtol * c.bnorm ? 1 : 0;
+                    if (write_out(r) != S2L_OK) return leave(S2L_ERR_CUDA, t_last_error);
+                    complete(r, S2L_JOB_DONE, S2L_OK, "");
+                    continue;
+                }
+                slot_reset_cycle(c, m);
+                c.t0 = T;
+                c.run = true;
+            }
+        }
+        // complete the finished tickets (their solutions are on the host or queued before the
+        // stream synchronization below); a column that failed is cleared in every ring block so
+        // no non-finite value stays behind for the next request of that slot
+        if (!done_slots.empty()) {
+            for (size_t q = 0; q < done_slots.size(); ++q)
+                if (done_status[q] != S2L_OK && done_status[q] != S2L_ERR_CANCELED) {
+                    const int r = done_slots[q];
+                    launch_column_fill(st, n, K, r, ring, nK, 0.0, B.V);
+                    if (flex) launch_column_fill(st, n, K, r, ring, nK, 0.0, B.Z);
+                    launch_column_fill(st, n, K, r, 1, nK, 0.0, B.kw);
+                    w->launches += flex ? 3 : 2;
+                }
+            const cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+            {
+                std::lock_guard<std::mutex> g(sv->mu);
+                R->free_slots += (int)done_slots.size();
+            }
+            for (size_t q = 0; q < done_slots.size(); ++q) {
+                Slot& c = slots[done_slots[q]];
+                s2l_ticket* t = c.t;
+                c.t = nullptr;
+                c.run = c.ending = false;
+                if (!done_err[q].empty()) t->err = done_err[q];
+                ticket_finish(t, done_state[q], done_status[q]);
+            }
+            sv->cv.notify_all();
+        }
+        bool any_run = false;
+        for (int r = 0; r < K; ++r) any_run = any_run || slots[r].run;
+        if (!any_run) {
+            // nothing running: leave unless a request for this runner is queued
+            std::lock_guard<std::mutex> g(sv->mu);
+            bool more = false;
+            for (s2l_ticket* t : sv->queue)
+                more = more || (runner_takes(R, t) && batchable(sv, t) && !t->cancel.load());
+            if (!more) {
+                auto it = std::find(sv->runners.begin(), sv->runners.end(), R);
+                if (it != sv->runners.end()) sv->runners.erase(it);
+                sv->cv.notify_all();
+                delete R;
+                return;
+            }
+            continue;
+        }
+        // ---------------------------------------------------------------- Arnoldi step T
+        const int p = (int)(T % ring);
+        ColScale a{}, c0{};
+        for (int r = 0; r < K; ++r) {
+            const Slot& c = slots[r];
+            if (!c.run) continue;
+            if (c.t0 == T) c0.v[r] = 1.0 / c.beta;  // first vector of a cycle: r / beta
+            else a.v[r] = 1.0 / c.hn;               // next vector: w / h(j + 1, j)
+        }
+        double* Vp = B.V + (size_t)p * nK;
+        {
+            Prof pr(w, PC_VEC);
+            launch_combine2_block(st, n, K, a, B.kw, c0, B.r, Vp);
+            w->launches += 1;
+        }
+        double* Zp = flex ? B.Z + (size_t)p * nK : B.z;
+        rc = apply_block(w, K, Vp, Zp);
+        if (rc == S2L_OK) rc = spmv_block(w, K, Zp, B.kw, nullptr, false);
+        if (rc != S2L_OK) return leave(rc, t_last_error);
+        int64_t tmin = T;
+        for (int r = 0; r < K; ++r)
+            if (slots[r].run) tmin = std::min(tmin, slots[r].t0);
+        const int Lw = (int)(T - tmin + 1), j0 = (int)(tmin % ring);
+        ColFirst first{};
+        for (int r = 0; r < K; ++r) first.f[r] = slots[r].run ? (int)(slots[r].t0 - tmin) : Lw;
+        {
+            Prof pr(w, PC_VEC);
+            launch_mdot_block(st, n, K, B.V, nK, Lw, B.kw, B.part, B.red, j0, ring);
+            launch_gemv_update_block(st, n, K, B.V, nK, Lw, B.red, -1.0, B.kw, nullptr, nullptr, j0, ring, &first);
+            launch_mdot_block(st, n, K, B.V, nK, Lw, B.kw, B.part, B.red + MC, j0, ring);
+            launch_gemv_update_block(st, n, K, B.V, nK, Lw, B.red + MC, -1.0, B.kw, B.part, B.red + 2 * MC, j0, ring,
+                                     &first);
+            w->launches += 7;
+        }
+        {
+            const cudaError_t e = cudaMemcpyAsync(B.h_red, B.red, 3 * MC * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+            rc = check_err(w);
+            if (rc != S2L_OK) return leave(rc, t_last_error);
+        }
+        for (int r = 0; r < K; ++r) {
+            Slot& c = slots[r];
+            if (!c.run) continue;
+            s2l_result* res = c.t->res;
+            const s2l_krylov_opts& o = c.t->opts;
+            const int j = (int)(T - c.t0);
+            const int f = first.f[r];
+            const double hn = std::sqrt(B.h_red[2 * MC + r]);
+            for (int i = 0; i <= j; ++i) Hc(c, i, j) = B.h_red[(f + i) * K + r] + B.h_red[MC + (f + i) * K + r];
+            Hc(c, j + 1, j) = hn;
+            for (int i = 0; i < j; ++i) {
+                const double tt = c.cs[i] * Hc(c, i, j) + c.sn[i] * Hc(c, i + 1, j);
+                Hc(c, i + 1, j) = -c.sn[i] * Hc(c, i, j) + c.cs[i] * Hc(c, i + 1, j);
+                Hc(c, i, j) = tt;
+            }
+            const double den = std::hypot(Hc(c, j, j), Hc(c, j + 1, j));
+            c.cs[j] = den > 0.0 ? Hc(c, j, j) / den : 1.0;
+            c.sn[j] = den > 0.0 ? Hc(c, j + 1, j) / den : 0.0;
+            Hc(c, j, j) = den;
+            Hc(c, j + 1, j) = 0.0;
+            if (j == 0) c.g[0] = c.beta;
+            c.g[j + 1] = -c.sn[j] * c.g[j];
+            c.g[j] = c.cs[j] * c.g[j];
+            c.kr = j + 1;
+            ++res->iterations;
+            res->rel_residual = std::fabs(c.g[j + 1]) / c.bnorm;
+            hist(c, res->rel_residual);
+            bool end = false;
+            if (!std::isfinite(res->rel_residual)) {
+                end = true;  // the boundary's residual check reports it
+            } else if (res->rel_residual <= o.rtol) {
+                c.cand = true;
+                end = true;
+            } else if (hn == 0.0) {
+                c.brk = true;
+                res->breakdown = 1;
+                end = true;
+            } else if (res->iterations >= o.maxit || j + 1 == m) {
+                end = true;
+            }
+            c.hn = hn;
+            if (end) {
+                c.run = false;
+                c.ending = true;
+            }
+        }
+        ++T;
+    }
+}
+
+// The next ticket this worker runs (serve mutex held): the first queued one that no block runner
+// with a free slot is going to take.  A batchable ticket starts a new runner (returned in *nr).
+s2l_ticket* pick_ticket(s2l_serve* sv, Runner** nr)
+{
+    *nr = nullptr;
+    std::vector<int> room;  // free slots of each runner not yet promised to a queued ticket
+    for (Runner* R : sv->runners) room.push_back(R->free_slots);
+    for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
+        s2l_ticket* t = *it;
+        if (batchable(sv, t) && !t->cancel.load()) {
+            bool promised = false;
+            for (size_t q = 0; q < sv->runners.size() && !promised; ++q)
+                if (room[q] > 0 && runner_takes(sv->runners[q], t)) {
+                    --room[q];
+                    promised = true;
+                }
+            if (promised) continue;
+            auto* R = new Runner;
+            R->s = t->s;
+            R->m = t->opts.restart;
+            R->flex = t->opts.flexible != 0;
+            R->K = runner_width(sv, t->s, R->m);
+            R->free_slots = R->K - 1;
+            sv->runners.push_back(R);
+            t->s->runners.fetch_add(1);
+            *nr = R;
+        }
+        sv->queue.erase(it);
+        return t;
+    }
+    return nullptr;
+}
+
 void serve_worker(s2l_ctx* ctx)
 {
     s2l_serve* sv = ctx->serve;
     cudaSetDevice(ctx->device);
     for (;;) {
         s2l_ticket* t = nullptr;
+        Runner* R = nullptr;
         {
             std::unique_lock<std::mutex> g(sv->mu);
-            sv->cv.wait(g, [&] { return sv->stop || !sv->queue.empty(); });
-            if (sv->queue.empty()) return;  // stop requested and nothing left
-            t = sv->queue.front();
-            sv->queue.pop_front();
+            for (;;) {
+                t = pick_ticket(sv, &R);
+                if (t) break;
+                if (sv->stop && sv->queue.empty()) return;  // stop requested and nothing left
+                sv->cv.wait(g);
+            }
+        }
+        if (R) {  // continuous batching: this worker runs the block runner until it has no request left
+            s2l_setup* s = R->s;
+            block_runner(ctx, R, t);
+            s->runners.fetch_sub(1);
+            continue;
         }
         if (t->cancel.load()) {
             t->err = "solve canceled before it started";
@@ -4457,6 +5035,19 @@ int s2l_gpu_serve_start(s2l_ctx* ctx, int workers)
     return S2L_OK;
 }
 
+int s2l_gpu_serve_batching(s2l_ctx* ctx, int slots)
+{
+    if (!ctx || slots > S2L_MAX_RHS) return S2L_ERR_BADARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!ctx->serve) {
+        ctx->err = "s2l_gpu_serve_start was not called on this context";
+        return S2L_ERR_STATE;
+    }
+    std::lock_guard<std::mutex> q(ctx->serve->mu);
+    ctx->serve->slots = slots < 0 ? -1 : slots;
+    return S2L_OK;
+}
+
 int s2l_gpu_submit(s2l_setup* s, int method, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
                    s2l_result* result, s2l_ticket** ticket)
 {
@@ -4487,7 +5078,7 @@ int s2l_gpu_submit(s2l_setup* s, int method, const double* b, double* x, int ptr
         }
         sv->queue.push_back(t);
     }
-    sv->cv.notify_one();
+    sv->cv.notify_all();  // an idle worker, or none when a block runner has a slot for it
     *ticket = t;
     return S2L_OK;
 }

@@ -302,7 +302,8 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 // wait on a ready flag) and the next batch is hinted into L2.  For each entry a lane waits until
 // the ready flag of the column is set; 1/diag is folded into the values and the right-hand side,
 // so a row ends with x = b - sum, one write and its flag.  Every wait is bounded: after
-// S2L_SPIN_LIMIT polls the CTA raises *err and all warps leave.
+// a.spin_limit polls (the setup option "spin_limit", S2L_SPIN_LIMIT by default) the CTA raises
+// *err and all warps leave.
 template <typename Real, bool SMEM, bool FWD, int KC>
 __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolveArgs<Real> a)
 {
@@ -416,7 +417,7 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                     while (flag[c] == 0) {  // the abort word and the limit are checked every 32 polls
                         if ((++spin & 31) == 0) {
                             if (abort_flag) { dead = true; break; }
-                            if (spin > S2L_SPIN_LIMIT) {
+                            if (spin > a.spin_limit) {
                                 abort_flag = 1;
                                 atomicExch(a.err, 1);
                                 dead = true;
@@ -817,12 +818,19 @@ __device__ __forceinline__ double col_sum(double v)
     return v;
 }
 
-// h(j, r) = V_j(:, r) . w(:, r) for j < J (V_j at V + j * ldv, n x K interleaved); tiles of 1024
-// entries (w staged in shared memory, entry e of a tile is column e % K), warp owns the columns
-// j = warp + 8q; partials[(b * J + j) * K + r].
+// h(j, r) = V_j(:, r) . w(:, r) for j < J (V_j at V + ring_block(j) * ldv, n x K interleaved); tiles
+// of 1024 entries (w staged in shared memory, entry e of a tile is column e % K), warp owns the
+// columns j = warp + 8q; partials[(b * J + j) * K + r].  Each (j, r) is summed in the same order
+// whatever J, the ring position and the other columns hold.
+__device__ __forceinline__ int64_t ring_block(int j, int j0, int ring)
+{
+    return ring ? (j0 + j) % ring : j0 + j;
+}
+
 template <int K>
 __global__ void __launch_bounds__(256) mdot_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv, int J,
-                                                         const double* __restrict__ w, double* __restrict__ partials)
+                                                         const double* __restrict__ w, double* __restrict__ partials,
+                                                         int j0, int ring)
 {
     __shared__ double ws[1024];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -838,7 +846,7 @@ __global__ void __launch_bounds__(256) mdot_block_kernel(int64_t nk, const doubl
         for (int q = 0; q < 8; ++q) {
             const int j = warp + 8 * q;
             if (j < J) {
-                const double* vj = V + (int64_t)j * ldv + t0;
+                const double* vj = V + ring_block(j, j0, ring) * ldv + t0;
                 double s0 = 0.0;
                 for (int i = lane; i < cnt; i += 32) s0 += vj[i] * ws[i];
                 acc[q] += s0;
@@ -855,21 +863,24 @@ __global__ void __launch_bounds__(256) mdot_block_kernel(int64_t nk, const doubl
     }
 }
 
-// w(:, r) += alpha * sum_j V_j(:, r) h(j, r); with partials, also sum(w(:, r)^2) per block
+// w(:, r) += alpha * sum_j V_j(:, r) h(j, r); with partials, also sum(w(:, r)^2) per block.  With
+// `first`, h(j, r) counts as zero for j < first.f[r] (a column whose own basis starts later in the
+// window): the terms before it add exact zeros, so the sum is the same as over its own basis.
 template <int K>
 __global__ void __launch_bounds__(256) gemv_update_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv,
                                                                 int J, const double* __restrict__ h, double alpha,
-                                                                double* __restrict__ w, double* __restrict__ partials)
+                                                                double* __restrict__ w, double* __restrict__ partials,
+                                                                int j0, int ring, ColFirst first, int masked)
 {
     __shared__ double hs[S2L_MAX_BLOCK_COLS];
     __shared__ double sh[8][K];
-    for (int c = threadIdx.x; c < J * K; c += 256) hs[c] = h[c];
+    for (int c = threadIdx.x; c < J * K; c += 256) hs[c] = (masked && c / K < first.f[c % K]) ? 0.0 : h[c];
     __syncthreads();
     const int r = (int)(threadIdx.x % K);  // every stride below is a multiple of K
     double nrm = 0.0;
     for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256) {
         double s = 0.0;
-        for (int j = 0; j < J; ++j) s += V[e + (int64_t)j * ldv] * hs[j * K + r];
+        for (int j = 0; j < J; ++j) s += V[e + ring_block(j, j0, ring) * ldv] * hs[j * K + r];
         const double wn = w[e] + alpha * s;
         w[e] = wn;
         nrm += wn * wn;
@@ -891,7 +902,8 @@ __global__ void __launch_bounds__(256) gemv_update_block_kernel(int64_t nk, cons
 // u(:, r) = sum_j V_j(:, r) y(j, r)
 template <int K>
 __global__ void __launch_bounds__(256) gemv_block_kernel(int64_t nk, const double* __restrict__ V, int64_t ldv, int J,
-                                                         const double* __restrict__ y, double* __restrict__ u)
+                                                         const double* __restrict__ y, double* __restrict__ u, int j0,
+                                                         int ring)
 {
     __shared__ double ys[S2L_MAX_BLOCK_COLS];
     for (int c = threadIdx.x; c < J * K; c += 256) ys[c] = y[c];
@@ -899,7 +911,7 @@ __global__ void __launch_bounds__(256) gemv_block_kernel(int64_t nk, const doubl
     const int r = (int)(threadIdx.x % K);
     for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256) {
         double s = 0.0;
-        for (int j = 0; j < J; ++j) s += V[e + (int64_t)j * ldv] * ys[j * K + r];
+        for (int j = 0; j < J; ++j) s += V[e + ring_block(j, j0, ring) * ldv] * ys[j * K + r];
         u[e] = s;
     }
 }
@@ -914,6 +926,44 @@ __global__ void __launch_bounds__(256) axpby_block_kernel(int64_t nk, const doub
     const double ar = a[r], br = b ? b[r] : 0.0;
     for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256)
         y[e] = b ? ar * x[e] + br * y[e] : ar * x[e];
+}
+
+// y(:, r) = a(r) x(:, r) + c(r) z(:, r), a source with a zero coefficient not read (so a stale
+// value there never reaches y); a, c by value
+template <int K>
+__global__ void __launch_bounds__(256) combine2_block_kernel(int64_t nk, ColScale a, const double* __restrict__ x,
+                                                             ColScale c, const double* __restrict__ z,
+                                                             double* __restrict__ y)
+{
+    const int r = (int)(threadIdx.x % K);
+    const double ar = a.v[r], cr = c.v[r];
+    for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < nk; e += (int64_t)gridDim.x * 256) {
+        const double p = ar != 0.0 ? ar * x[e] : 0.0;
+        const double q = cr != 0.0 ? cr * z[e] : 0.0;
+        y[e] = p + q;
+    }
+}
+
+// column r of dst (n x K interleaved) from src (n), or (out) src column r to dst
+__global__ void column_in_kernel(int64_t n, int K, int r, const double* __restrict__ src, double* __restrict__ dst)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i * K + r] = src[i];
+}
+
+__global__ void column_out_kernel(int64_t n, int K, int r, const double* __restrict__ src, double* __restrict__ dst)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i * K + r];
+}
+
+// column r of every block of a ring (count blocks of n x K) set to v
+__global__ void column_fill_kernel(int64_t n, int K, int r, int count, int64_t ld, double v, double* __restrict__ dst)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * count; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = e / n, i = e - b * n;
+        dst[b * ld + i * K + r] = v;
+    }
 }
 
 // dst (n x K interleaved) from k columns src + r * n (r < k); columns k..K-1 are zero
@@ -1152,23 +1202,50 @@ void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, con
 }
 
 void launch_mdot_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* w,
-                       double* partials, double* out)
+                       double* partials, double* out, int j0, int ring)
 {
-    S2L_KSWITCH(K, (mdot_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, w, partials)));
+    S2L_KSWITCH(K, (mdot_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, w, partials, j0, ring)));
     reduce_kernel<<<(J * K + 7) / 8, 256, 0, st>>>(partials, S2L_NB_RED, J * K, out);
 }
 
 void launch_gemv_update_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* h,
-                              double alpha, double* w, double* partials, double* red_out)
+                              double alpha, double* w, double* partials, double* red_out, int j0, int ring,
+                              const ColFirst* first)
 {
-    S2L_KSWITCH(K, (gemv_update_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, h, alpha, w, partials)));
+    const ColFirst f = first ? *first : ColFirst{};
+    const int masked = first ? 1 : 0;
+    S2L_KSWITCH(K, (gemv_update_block_kernel<KK><<<S2L_NB_RED, 256, 0, st>>>(n * K, V, ldv, J, h, alpha, w, partials,
+                                                                             j0, ring, f, masked)));
     if (partials) reduce_kernel<<<(K + 7) / 8, 256, 0, st>>>(partials, S2L_NB_RED, K, red_out);
 }
 
 void launch_gemv_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* y,
-                       double* u)
+                       double* u, int j0, int ring)
 {
-    S2L_KSWITCH(K, (gemv_block_kernel<KK><<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n * K, V, ldv, J, y, u)));
+    S2L_KSWITCH(K, (gemv_block_kernel<KK><<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n * K, V, ldv, J, y, u,
+                                                                                                 j0, ring)));
+}
+
+void launch_combine2_block(cudaStream_t st, int64_t n, int K, const ColScale& a, const double* x, const ColScale& c,
+                           const double* z, double* y)
+{
+    S2L_KSWITCH(K, (combine2_block_kernel<KK><<<grid_for(n * K, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n * K, a, x, c, z,
+                                                                                                     y)));
+}
+
+void launch_column_in(cudaStream_t st, int64_t n, int K, int r, const double* src, double* dst)
+{
+    column_in_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, K, r, src, dst);
+}
+
+void launch_column_out(cudaStream_t st, int64_t n, int K, int r, const double* src, double* dst)
+{
+    column_out_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, K, r, src, dst);
+}
+
+void launch_column_fill(cudaStream_t st, int64_t n, int K, int r, int count, int64_t ld, double v, double* dst)
+{
+    if (count > 0) column_fill_kernel<<<grid_for(n * count, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, K, r, count, ld, v, dst);
 }
 
 void launch_axpby_block(cudaStream_t st, int64_t n, int K, const double* a, const double* x, const double* b,

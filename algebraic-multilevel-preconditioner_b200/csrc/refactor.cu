@@ -202,7 +202,9 @@ __device__ void update_column_coop(const RefactorArgs& a, int64_t loc, int64_t f
 }
 
 // pivot of column gj: LU divides the strict lower part by U(j, j); L L^T takes the square root of
-// the diagonal and divides the rows below by it
+// the diagonal and divides the rows below by it.  LU keeps the setup's pivot order, so a pivot that
+// has become small against the entries below it (a multiplier |L(i, j)| > 1 / pivot_tol) is
+// reported (error 4): the kept order no longer suits the values and the caller should rebuild.
 __device__ void finish_column(const RefactorArgs& a, int64_t gj, int lane)
 {
     double* __restrict__ F = a.F;
@@ -223,6 +225,12 @@ __device__ void finish_column(const RefactorArgs& a, int64_t gj, int lane)
         if (d == 0.0 || !isfinite(d)) {
             if (lane == 0) set_err(a.err, 1);
             return;
+        }
+        if (a.pivot_tol > 0.0) {
+            double mx = 0.0;
+            for (int64_t s = pd + 1 + lane; s < c1; s += 32) mx = fmax(mx, fabs(F[s]));
+            for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0 && a.pivot_tol * mx > fabs(d)) set_err(a.err, 4);
         }
         const double di = 1.0 / d;
         for (int64_t s = pd + 1 + lane; s < c1; s += 32) F[s] *= di;
@@ -272,6 +280,21 @@ __global__ void __launch_bounds__(1024, 1) sparse_columns_kernel(const RefactorA
         }
         cl.sync();
     }
+}
+
+// The multipliers of an LU dense tail factored without pivoting (column-major S^T = L' U', L' in
+// the strict lower part): error 4 when one exceeds 1 / tol in magnitude (a pivot that is small
+// against its row of S).
+__global__ void __launch_bounds__(256) tail_growth_kernel(const double* __restrict__ S, int s, double tol,
+                                                          int* err)
+{
+    const int64_t total = (int64_t)s * s;
+    bool bad = false;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = e / s, i = e - j * s;  // column-major: row i of column j
+        if (i > j && tol * fabs(S[e]) > 1.0) bad = true;
+    }
+    if (bad) set_err(err, 4);
 }
 
 // one warp per tail column: the updates from the sparse columns (k < T)
@@ -604,6 +627,11 @@ template <typename Real>
 void launch_tail_inverses(cudaStream_t st, const double* S, const double* B, int s, int llt, Real* linv, Real* uinv)
 {
     tail_inverses_kernel<Real><<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(S, B, s, llt, linv, uinv);
+}
+
+void launch_tail_growth(cudaStream_t st, const double* S, int s, double tol, int* err)
+{
+    if (s > 1 && tol > 0.0) tail_growth_kernel<<<grid_for((int64_t)s * s, 256), 256, 0, st>>>(S, s, tol, err);
 }
 
 void launch_identity(cudaStream_t st, double* M, int s)

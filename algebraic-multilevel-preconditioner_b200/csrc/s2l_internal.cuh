@@ -114,6 +114,7 @@ struct LocalSolveArgs {
     int K;
     int KC;
     int64_t nloc;              // local-space size (stride of the per-column-group ready flags)
+    int spin_limit;            // polls of one ready flag before a sweep gives up (S2L_SPIN_LIMIT by default)
 };
 
 // Numeric refactorization of every subdomain's factors on their kept patterns (s2l_gpu_refactor).
@@ -143,7 +144,9 @@ struct RefactorArgs {
     int nlmax;                 // largest subdomain (rows): the cooperative column map
     double* part;              // partial columns of the cooperative column updates: per subdomain
                                // and warp, maxcol doubles
-    int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column (0: none)
+    int* err;                  // first failure: 1 zero / non-positive pivot of a sparse column, 4 an LU
+                               // pivot below pivot_tol relative to its column (0: none)
+    double pivot_tol;          // LU: largest allowed multiplier is 1 / pivot_tol (0: no check)
 };
 
 // launch wrappers (kernels.cu)
@@ -163,12 +166,29 @@ void launch_dot2(cudaStream_t st, int64_t n, const double* x, const double* y, c
 // K right-hand sides (block vectors n x K interleaved; K = 1, 2, 4, 8 or 16)
 void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, const int32_t* ci, const double* v,
                        const double* X, double* Y, const double* B, double* partials, double* red_out, int tpr);
+// Block Krylov bases may sit in a ring of `ring` blocks: basis vector j is block (j0 + j) % ring
+// (ring 0: block j0 + j).  A ColFirst mask makes the update coefficients h(j, r) with j < f[r]
+// zero (column r's own basis starts there).
+struct ColFirst {
+    int f[S2L_MAX_RHS];
+};
+struct ColScale {
+    double v[S2L_MAX_RHS];
+};
 void launch_mdot_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* w,
-                       double* partials, double* out);
+                       double* partials, double* out, int j0 = 0, int ring = 0);
 void launch_gemv_update_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* h,
-                              double alpha, double* w, double* partials, double* red_out);
+                              double alpha, double* w, double* partials, double* red_out, int j0 = 0, int ring = 0,
+                              const ColFirst* first = nullptr);
 void launch_gemv_block(cudaStream_t st, int64_t n, int K, const double* V, int64_t ldv, int J, const double* y,
-                       double* u);
+                       double* u, int j0 = 0, int ring = 0);
+// y(:, r) = a(r) x(:, r) + c(r) z(:, r) (a source with a zero coefficient is not read)
+void launch_combine2_block(cudaStream_t st, int64_t n, int K, const ColScale& a, const double* x, const ColScale& c,
+                           const double* z, double* y);
+// column r of an n x K interleaved block from / to a plain vector; column r of count blocks set to v
+void launch_column_in(cudaStream_t st, int64_t n, int K, int r, const double* src, double* dst);
+void launch_column_out(cudaStream_t st, int64_t n, int K, int r, const double* src, double* dst);
+void launch_column_fill(cudaStream_t st, int64_t n, int K, int r, int count, int64_t ld, double v, double* dst);
 void launch_axpby_block(cudaStream_t st, int64_t n, int K, const double* a, const double* x, const double* b,
                         double* y);
 void launch_interleave(cudaStream_t st, int64_t n, int K, int k, const double* src, double* dst);
@@ -246,6 +266,7 @@ int refactor_sparse_warps(int smax);
 size_t refactor_map_bytes(int smax, int warps);
 void launch_refactor_tail_columns(cudaStream_t st, const RefactorArgs& a);
 void launch_refactor_gather_tails(cudaStream_t st, const RefactorArgs& a);
+void launch_tail_growth(cudaStream_t st, const double* S, int s, double tol, int* err);
 void launch_identity(cudaStream_t st, double* M, int s);
 template <typename Real>
 void launch_tail_inverses(cudaStream_t st, const double* S, const double* B, int s, int llt, Real* linv, Real* uinv);

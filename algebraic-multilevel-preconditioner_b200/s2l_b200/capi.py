@@ -35,7 +35,7 @@ EXPORTED = [
     "s2l_gpu_submit", "s2l_gpu_poll", "s2l_gpu_wait", "s2l_gpu_cancel", "s2l_gpu_ticket_info",
     "s2l_gpu_ticket_free", "s2l_gpu_apply_block", "s2l_gpu_gmres_block", "s2l_gpu_update_matrix",
     "s2l_gpu_refactor", "s2l_gpu_add_subdomain_amg", "s2l_amg_build", "s2l_amg_rebuild", "s2l_amg_shape",
-    "s2l_amg_matrix", "s2l_amg_coarse", "s2l_amg_free",
+    "s2l_amg_matrix", "s2l_amg_coarse", "s2l_amg_free", "s2l_gpu_serve_batching",
 ]
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELED = 0, 1, 2, 3
 ERR_TIMEOUT, ERR_CANCELED = 5, 8
@@ -104,6 +104,7 @@ def load(path: str = LIB_PATH):
         "s2l_gpu_solve_batch": ([vp, C.c_int, C.c_int, C.POINTER(vp), C.POINTER(vp), C.c_int, C.POINTER(KrylovOpts),
                                  C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
         "s2l_gpu_serve_start": ([vp, C.c_int], C.c_int),
+        "s2l_gpu_serve_batching": ([vp, C.c_int], C.c_int),
         "s2l_gpu_submit": ([vp, C.c_int, vp, vp, C.c_int, C.POINTER(KrylovOpts), C.POINTER(Result), C.POINTER(vp)],
                            C.c_int),
         "s2l_gpu_poll": ([vp, C.POINTER(C.c_int)], C.c_int),
@@ -161,9 +162,15 @@ class Context:
         if rc != S2L_OK:
             raise S2LError(rc, self.error())
 
-    def serve_start(self, workers: int = 4):
-        """Start the native worker threads of the asynchronous solves (GpuSetup.submit)."""
+    def serve_start(self, workers: int = 4, batching: int = -1):
+        """Start the native worker threads of the asynchronous solves (GpuSetup.submit).  batching:
+        slots of the continuous-batching block runners (-1 automatic, 0 off: every GMRES request
+        alone on its worker)."""
         self.check(self.lib.s2l_gpu_serve_start(self.h, workers))
+        self.serve_batching(batching)
+
+    def serve_batching(self, slots: int):
+        self.check(self.lib.s2l_gpu_serve_batching(self.h, slots))
 
     def close(self):
         if self.h:
@@ -510,6 +517,10 @@ class GpuSetup:
 
     def set_stream(self, stream_ptr: int | None):
         self.ctx.check(self.lib.s2l_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def set_option(self, name: str, value: float):
+        """A setup option that may change after the upload ("spin_limit")."""
+        self.ctx.check(self.lib.s2l_gpu_setup_option(self.h, name.encode(), float(value)))
 
     PROF = {"spmv": 1, "local_solve": 2, "coarse": 4, "combine": 8, "krylov_vec": 16, "all": 31}
 

@@ -204,7 +204,8 @@ def convdiff(dim: int, nx: int, ny: int = 0, nz: int = 0, nu: float = 1.0, ncomp
     A.sort_indices()
     name = ("coupled" if coupled else "convdiff") + f"{dim}d"
     desc = f"{name} {nx}x{ny}" + (f"x{nz}" if dim == 3 else "") + f" nu={nu:g}" + \
-        (f" ncomp={nc}" if nc > 1 else "") + f" (n={n}, nnz={A.nnz})"
+        (f" ncomp={nc}" if nc > 1 else "") + (f" pulse={pulse:g} t={time:g}" if pulse != 0.0 else "") + \
+        f" (n={n}, nnz={A.nnz})"
     return Problem(A, (nx, ny, nz), False, desc, rhs)
 
 

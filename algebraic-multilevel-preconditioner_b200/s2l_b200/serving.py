@@ -5,7 +5,9 @@ first out), reuses it for every request on that matrix and along a sequence of v
 (``update``: the reference's UpdateLevel::Reuse, preconditioner kept, or Refactorize on the
 device), and runs the solves on the
 native worker threads of the context (``s2l_gpu_serve_start``), so requests that arrive while
-others are on the GPU overlap with them.  Memory is admitted by the context's HBM budget: a
+others are on the GPU overlap with them.  GMRES requests on one matrix are batched continuously
+(``s2l_gpu_serve_batching``): they share the Arnoldi steps of a block runner, joining it as slots
+free up and leaving it as they converge.  Memory is admitted by the context's HBM budget: a
 solve whose buffers do not fit waits in the library for a workspace of its setup to come free,
 and a new setup that does not fit evicts idle setups (those with no queued or running solve)
 until it does.
@@ -19,9 +21,9 @@ from . import capi
 
 
 class Engine:
-    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4):
+    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4, batching: int = -1):
         self.ctx = capi.Context(device, int(hbm_budget))
-        self.ctx.serve_start(workers)
+        self.ctx.serve_start(workers, batching=batching)
         self._cache: OrderedDict[object, capi.GpuSetup] = OrderedDict()
         self._lock = threading.Lock()
         self.builds = 0  # device setups created (cache misses)

@@ -123,7 +123,7 @@ class ReusePolicy:
         """Outcome of a solve performed after level `done` (``reuse_policy.cpp:54-82``)."""
         if done == UpdateLevel.REBUILD:
             self.age = 0
-            self._ref = [0.0] * len(self._ref)  # every kind needs a new reference
+            self._ref = [0.0] * len(self._ref)  # a rebuild invalidates the baseline of each level
             self._last_ref = 0.0
             self.wasted = 0.0
             if t_update > 0.0:

@@ -1,22 +1,34 @@
 #!/usr/bin/env python
 """Benchmark of the B200 solve phase: solves to a true FP64 residual of 1e-8.
 
-Workload (default): 3D 7-point variable-coefficient pressure Poisson 100^3 (n = 1.0M),
-beta = 1/rho with rho = 1e-3 in 200 seeded spheres of radius 3-8 cells, 64 subdomains (recursive
-coordinate bisection), overlap 2, nev 20, deflated two-level RAS, local L L^T, GMRES(50),
-rtol 1e-8, U[-1,1] right-hand sides.  Forms timed:
-  plain_fp64  : FP64 factors, the reference's GMRES (true-residual restart rule), one solve per step;
+Main workload: 3D 7-point variable-coefficient pressure Poisson 100^3 (n = 1.0M), beta = 1/rho with
+rho = 1e-3 in 200 seeded spheres of radius 3-8 cells, 64 subdomains (recursive coordinate
+bisection), deflated two-level RAS, nev 20, local L L^T, GMRES(50), rtol 1e-8, U[-1,1] right-hand
+sides.  Overlap 1 by default: the reference's own overlap, so the reference arm (--impl reference)
+runs this very matrix, partition, right-hand side and preconditioner.  Forms timed on it:
+  plain_fp64  : FP64 factors, the reference's GMRES, one solve per step (the reference arm's
+                configuration exactly: the same-config anchor);
   mixed       : the same factors stored in FP32 + flexible GMRES(50) in FP64, converged only when
                 the recomputed FP64 true residual is <= rtol, one solve per step;
   block_mixed : the mixed form for k right-hand sides per step (s2l_gpu_gmres_block);
-  batched / block_mixed_threads: several solves or blocks from host threads at once;
-  serving     : Poisson arrivals over three resident matrices on the worker threads (p50/p99);
-  sequence_refactor: the next matrices of the moving-bubble sequence, each refactorized on the
-                device (s2l_gpu_refactor) and solved for --head-k right-hand sides;
-  amg_local_solves: the same matrix with AMG local solvers (--local-approx amg), plain FP64 GMRES.
-Headline (`value`): block_mixed at --head-k right-hand sides per step (default 16, the batching
-configuration's right-hand sides per matrix), solves/s with b resident in HBM; `e2e` = the same
-through the C ABI with pinned host buffers (copies inside the timed region).
+  serving     : continuous batching (s2l_gpu_serve_batching) of Poisson arrivals of solve requests
+                on this matrix (p50/p99 latency, solves/s, error against the FP64 solution);
+  amg_local_solves: AMG local solvers (--local-approx amg), plain FP64 GMRES.
+Other configurations, as their own forms:
+  c2_overlap2 : the same problem at overlap 2 (plain FP64, mixed, 16-right-hand-side block);
+  sequence    : 32 matrices of the moving-bubble sequence (bubbles rise half a cell per step) on 64
+                uneven subdomains (10k-25k rows), 16 right-hand sides per matrix, the update before
+                each matrix (Refactorize on the device, or Rebuild) chosen by the reference's reuse
+                policy (--reuse auto);
+  c3_convdiff : 3D upwind convection-diffusion 128^3 (n = 2.1M), 128 subdomains, LU factors,
+                FGMRES(40) (plain FP64, mixed FP32 factors, 16-right-hand-side block);
+  serving_mix : 2000 Poisson arrivals at 50 req/s over 40 seeded cases of the three families;
+  parity      : in the CPU-baseline leg, the drop-in check (oracle/_ref/dropin_check) on the main
+                workload and at the c1 size: the reference's apply and GMRES against the GPU's on
+                the same objects.
+Headline (`value`): block_mixed at --head-k right-hand sides per step (default 16), solves/s with b
+resident in HBM; `e2e` = the same through the C ABI with pinned host buffers (copies inside the
+timed region).  cpu_baseline: the reference itself (oracle/_ref/s2l_ref) on the main workload.
 
 --impl reference times the reference itself (built from its sources into oracle/_ref/ with an
 in-process thread-rank MPI) on the host cores, same problem and partition.
@@ -40,6 +52,7 @@ for _p in (REPO, PKG):
         sys.path.insert(0, _p)
 
 METRIC = "solve time to FP64 residual 1e-8 (mixed/batched vs plain FP64 GPU); p50/p99 latency"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "s2l_ref")
 
 
 def parse(argv=None):
@@ -48,27 +61,27 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bubbles3d", choices=["bubbles3d", "convdiff3d"],
-                    help="bubbles3d: the headline configuration; convdiff3d: 128^3 convection-diffusion, "
-                         "128 subdomains, LU factors, FGMRES(40)")
-    ap.add_argument("--nx", type=int, default=0, help="grid size (0: the workload's)")
-    ap.add_argument("--nsub", type=int, default=0, help="subdomains (0: the workload's)")
+    ap.add_argument("--nx", type=int, default=100, help="main workload grid size")
+    ap.add_argument("--nsub", type=int, default=64, help="main workload subdomains")
     ap.add_argument("--nbubbles", type=int, default=200)
-    ap.add_argument("--overlap", type=int, default=2)
+    ap.add_argument("--overlap", type=int, default=1, help="main workload overlap (1: the reference's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-threads", type=int, default=0, help="reference arm: host threads (0 = all)")
     ap.add_argument("--opt", action="append", default=[], help="device layout option key=value (s2l_gpu_setup_option)")
-    ap.add_argument("--batch", default="2,4,8", help="batched form: right-hand sides solved at once (comma list)")
     ap.add_argument("--block", default="4,8,16", help="block form: right-hand sides per block GMRES (comma list)")
     ap.add_argument("--head-k", type=int, default=16, help="right-hand sides per step of the headline block form")
-    ap.add_argument("--serve", type=int, default=120, help="serving form: requests (0 = off)")
-    ap.add_argument("--seq", type=int, default=8, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
-    ap.add_argument("--serve-rate", type=float, default=50.0, help="serving form: mean arrivals per second")
-    ap.add_argument("--amg", type=int, default=1,
-                    help="AMG form: the same matrix with AMG local solvers (--local-approx amg), 0 = off")
-    ap.add_argument("--serve-mix", type=int, default=0,
-                    help="serving-mix form: requests over 40 seeded cases of the three families (0 = off)")
-    ap.add_argument("--block-threads", default="2,4", help="block form with k=4 blocks from several host threads")
+    ap.add_argument("--serve", type=int, default=400, help="serving form: requests on the main matrix (0 = off)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="serving form: mean arrivals per second")
+    ap.add_argument("--overlap2", type=int, default=1, help="c2 at overlap 2 (0 = off)")
+    ap.add_argument("--seq", type=int, default=32, help="sequence form: matrices of the moving-bubble sequence (0 = off)")
+    ap.add_argument("--seq-reuse", default="auto", choices=["auto", "refactor"])
+    ap.add_argument("--c3", type=int, default=128, help="convection-diffusion form: grid size (0 = off)")
+    ap.add_argument("--c3-nsub", type=int, default=128)
+    ap.add_argument("--amg", type=int, default=1, help="AMG form: AMG local solvers on the main matrix (0 = off)")
+    ap.add_argument("--serve-mix", type=int, default=2000, help="serving-mix form: requests over 40 cases (0 = off)")
+    ap.add_argument("--serve-mix-rate", type=float, default=50.0)
+    ap.add_argument("--parity", type=int, default=1,
+                    help="the CPU-baseline leg also runs the drop-in parity check on the main workload and c1 (0 = off)")
     return ap.parse_args(argv)
 
 
@@ -224,32 +237,183 @@ class Replicas:
             self.dist = None
 
 
+def workload_desc(w, overlap) -> str:
+    """The main workload, the same words in both arms' lines."""
+    return (f"bubbles3d {w.nx}^3 pressure Poisson ({w.nbubbles} bubbles of radius 3-8 cells, density ratio "
+            f"{w.rho_ratio:g}), {w.nsub} subdomains, overlap {overlap}, nev {w.opts.nev}, deflated RAS, "
+            f"L L^T local factors, GMRES({w.restart}), rtol {w.rtol:g}, U[-1,1] right-hand side")
+
+
+def main_workload(a):
+    from s2l_b200 import workloads as W
+    return W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap)
+
+
+def rel_err(x, y) -> float:
+    import numpy as np
+    return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+
+
 # ------------------------------------------------------------------------------------ our arm
+class Timer:
+    """Device timing of a form: W warm-up steps, then K steps each bracketed by CUDA events on the
+    launching stream, a barrier (device sync + every rank) around the timed steps, max over ranks."""
+
+    def __init__(self, a, reps, stream):
+        import torch
+        self.a, self.reps, self.stream, self.torch = a, reps, stream, torch
+
+    def barrier(self):
+        self.reps.barrier(self.torch.cuda.synchronize)
+
+    def run(self, step, steps=None, warmup=None, before=None, after=None):
+        """step() -> anything; returns (per-step ms list, total ms max over ranks, last output)."""
+        torch = self.torch
+        steps = self.a.steps if steps is None else steps
+        warmup = self.a.warmup if warmup is None else warmup
+        out = None
+        for _ in range(warmup):
+            out = step()
+        if before:
+            before()
+        self.barrier()
+        per = []
+        for _ in range(steps):
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(self.stream)
+            out = step()
+            e_ev.record(self.stream)
+            e_ev.synchronize()
+            per.append(s_ev.elapsed_time(e_ev))
+        self.barrier()
+        if after:
+            after()
+        return per, self.reps.max(sum(per)), out
+
+
+def single_form(tm, g, b_dev, x_dev, kw, x_ref=None, prof=True):
+    """One right-hand side per step (x from zero), with the library's kernel timers."""
+    import numpy as np
+    res_all = []
+
+    def step():
+        x_dev.zero_()
+        _, res = g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
+        res_all.append(res)
+        return res
+
+    g.profile(("local_solve", "spmv") if prof else ())
+    per, tot, _ = tm.run(step, before=lambda: res_all.clear())
+    ls_ms, ls_n = g.profile_get("local_solve")
+    sp_ms, sp_n = g.profile_get("spmv")
+    launches = g.launches()
+    g.profile(())
+    x = x_dev.cpu().numpy()
+    out = {"ms_per_solve": tot / len(per), "per_solve_ms": per, "iterations": [r["iterations"] for r in res_all],
+           "converged": all(r["converged"] for r in res_all),
+           "true_rel_residual": max(r["true_rel_residual"] for r in res_all),
+           "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+           "local_solve_ms_total": ls_ms, "local_solve_launches": ls_n, "spmv_ms_total": sp_ms,
+           "spmv_calls": sp_n, "launches": launches, "local_solve_bytes": g.local_solve_bytes(),
+           "local_solve_column_bytes": g.stat("local_solve_column_bytes")}
+    if x_ref is not None:
+        out["rel_error_vs_fp64"] = rel_err(x, x_ref)
+    return out, x
+
+
+def block_form(tm, g, Bk, Xk, k, kw, X_ref=None, prof=False, sampler=None):
+    """k right-hand sides per step in one lockstep block GMRES."""
+    import numpy as np
+    res_k = []
+
+    def step():
+        Xk.zero_()
+        _, r = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
+        res_k[:] = r
+        return r
+
+    if prof:
+        g.profile(("local_solve", "spmv"))
+    per, tot, _ = tm.run(step, before=(sampler.start if sampler else None))
+    clocks = sampler.stop() if sampler else None
+    prof_out = None
+    if prof:
+        prof_out = dict(ls=g.profile_get("local_solve"), sp=g.profile_get("spmv"), launches=g.launches())
+        g.profile(())
+    out = {"rhs": k, "ms_per_block": tot / len(per), "ms_per_solve": tot / len(per) / k,
+           "solves_per_s": tm.reps.world * k * len(per) / (tot * 1e-3),
+           "iterations": [r["iterations"] for r in res_k], "converged": all(r["converged"] for r in res_k),
+           "true_rel_residual": max(r["true_rel_residual"] for r in res_k),
+           "p50_block_ms": float(np.percentile(per, 50)), "p99_block_ms": float(np.percentile(per, 99))}
+    if X_ref is not None:
+        Xh = Xk.cpu().numpy()
+        out["rel_error_vs_fp64"] = max(rel_err(Xh[j], X_ref[j]) for j in range(k))
+    return out, per, clocks, prof_out
+
+
+def fp64_solutions(g64, B, kw):
+    """The plain FP64 solutions of the rows of B (host), the reference point of every error."""
+    import numpy as np
+    return np.stack([g64.gmres(B[j], **kw)[0] for j in range(B.shape[0])])
+
+
+def serve_form(local, st, kw, n_req, rate, bpool, xpool, workers=4):
+    """Poisson arrivals of solve requests on one matrix through the serving engine (continuous
+    batching, native workers); latency = submitted -> solution ready (host clock)."""
+    import numpy as np
+    from s2l_b200.serving import Engine
+    eng = Engine(local, hbm_budget=150 << 30, workers=workers)
+    t = eng.submit("m", lambda: st, bpool[0], history_cap=0, **kw)  # setup resident, runner warm
+    t.wait(600.0)
+    t.free()
+    rng = np.random.default_rng(2026)
+    gaps = rng.exponential(1.0 / rate, n_req)
+    tickets = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for i in range(n_req):
+        t_next += gaps[i]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        j = i % len(bpool)
+        tickets.append((j, eng.submit("m", lambda: st, bpool[j], history_cap=0, **kw)))
+    lat, run, its, err = [], [], [], 0.0
+    ok = True
+    for j, t in tickets:
+        x, r, status = t.wait(600.0)
+        ok = ok and status == 0 and r["converged"]
+        info = t.info()
+        lat.append(info["queue_ms"] + info["run_ms"])
+        run.append(info["run_ms"])
+        its.append(r["iterations"])
+        err = max(err, rel_err(x, xpool[j]))
+        t.free()
+    t_end = time.perf_counter()
+    eng.close()
+    return {"requests": n_req, "rate_req_s": rate, "workers": workers, "batching": "continuous (automatic slots)",
+            "all_converged": ok, "solves_per_s": n_req / (t_end - t0),
+            "ms_per_solve": (t_end - t0) * 1e3 / n_req,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(np.max(lat)), "run_ms_mean": float(np.mean(run)),
+            "iterations_mean": float(np.mean(its)), "iterations_max": int(np.max(its)),
+            "rel_error_vs_fp64_max": err, "clock": "host (submit to solution ready)"}
+
+
 def run_ours(a):
     reps = Replicas()
     rank, world, local = reps.rank, reps.world, reps.local
     os.environ.setdefault("S2L_CACHE_DIR", os.path.join(REPO, "_cache"))
+    import numpy as np
     from s2l_b200 import workloads as W
     from s2l_b200.setup_phase import with_factor_precision
 
-    if a.workload == "convdiff3d":
-        wl = W.convdiff3d(a.nx or 128, a.nsub or 128, precision="double")
-        a.seq = 0  # the moving-bubble sequence belongs to the bubbles workload
-        wdesc = (f"convdiff3d {wl.nx}^3 upwind convection-diffusion (4-mode divergence-free Fourier field), "
-                 f"{wl.nsub} subdomains, overlap 1, nev 24, deflated RAS, LU factors, FGMRES({wl.restart}), rtol 1e-8")
-    else:
-        wl = W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
-        wdesc = (f"bubbles3d {wl.nx}^3 pressure Poisson, {wl.nsub} subdomains, overlap {a.overlap}, nev 20, "
-                 f"deflated RAS, LL^T factors, GMRES({wl.restart}), rtol 1e-8")
-    if world > 1:
-        # rank 0 fills the setup cache first; the replicas then load it (setup is outside the timing)
-        st = reps.rank0_first(lambda: W.build(wl))
-    else:
-        t0 = time.time()
-        st = W.build(wl)
-        setup_s = time.time() - t0
+    wl = main_workload(a)
+    wdesc = workload_desc(wl, a.overlap)
+    t0 = time.time()
+    st = reps.rank0_first(lambda: W.build(wl)) if world > 1 else W.build(wl)
+    setup_s = time.time() - t0
     # ---- device (no CUDA call before the setup's process pool is done)
-    import numpy as np
     import torch
     from s2l_b200 import capi
 
@@ -259,432 +423,115 @@ def run_ours(a):
     st32 = with_factor_precision(st, "single")
     layout = {kv.split("=")[0]: float(kv.split("=")[1]) for kv in a.opt}
     g64 = capi.GpuSetup(ctx, st, options=layout)
-    # the mixed setup keeps its factor patterns on the device for the sequence form's refactorizations
-    g32 = capi.GpuSetup(ctx, st32, options=dict(layout, refactor=1) if a.seq > 0 else layout)
+    g32 = capi.GpuSetup(ctx, st32, options=layout)
     stream = torch.cuda.current_stream(dev)
     for g in (g64, g32):
         g.set_stream(stream.cuda_stream)
+    tm = Timer(a, reps, stream)
     n = st.n
+    kw64 = dict(restart=wl.restart, rtol=wl.rtol, flexible=False, strict=False)
+    kw32 = dict(restart=wl.restart, rtol=wl.rtol, flexible=True, strict=True)
+    peak, peak_src = measured_peaks()
     b_dev = torch.tensor(st.b, device=dev, dtype=torch.float64)
     x_dev = torch.zeros(n, device=dev, dtype=torch.float64)
-    forms = {
-        "plain_fp64": (g64, dict(restart=wl.restart, rtol=wl.rtol, flexible=False, strict=False)),
-        "mixed": (g32, dict(restart=wl.restart, rtol=wl.rtol, flexible=True, strict=True)),
-    }
 
-    def barrier():
-        reps.barrier(torch.cuda.synchronize)
+    # ---- one right-hand side per step: plain FP64 (the reference arm's configuration) and mixed
+    plain, x64 = single_form(tm, g64, b_dev, x_dev, kw64)
+    plain["true_rel_residual_host_check"] = float(np.linalg.norm(st.b - st.A @ x64) / np.linalg.norm(st.b))
+    mixed, xm = single_form(tm, g32, b_dev, x_dev, kw32, x_ref=x64)
+    mixed["true_rel_residual_host_check"] = float(np.linalg.norm(st.b - st.A @ xm) / np.linalg.norm(st.b))
 
-    max_over_ranks = reps.max
-
-    results = {}
-    peak, peak_src = measured_peaks()
-    sampler = None
-    for name, (g, kw) in forms.items():
-        for _ in range(a.warmup):
-            x_dev.zero_()
-            g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
-        headline = False
-        g.profile(("local_solve", "spmv"))
-        barrier()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-        its = []
-        conv = []
-        true_res = []
-        for k in range(a.steps):
-            ev[k][0].record(stream)
-            x_dev.zero_()
-            _, res = g.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kw)
-            ev[k][1].record(stream)
-            its.append(res["iterations"])
-            conv.append(res["converged"])
-            true_res.append(res["true_rel_residual"])
-        barrier()
-        per = [s.elapsed_time(e) for s, e in ev]
-        total_ms = max_over_ranks(sum(per))
-        clocks = sampler.stop() if headline else None
-        ls_ms, ls_n = g.profile_get("local_solve")
-        sp_ms, sp_n = g.profile_get("spmv")
-        launches = g.launches()
-        g.profile(())
-        # independent FP64 check of the last solution
-        x = x_dev.cpu().numpy()
-        true_chk = float(np.linalg.norm(st.b - st.A @ x) / np.linalg.norm(st.b))
-        results[name] = {
-            "ms_per_solve": total_ms / a.steps, "per_solve_ms": per, "iterations": its, "converged": all(conv),
-            "true_rel_residual": max(true_res), "true_rel_residual_host_check": true_chk,
-            "local_solve_ms_total": ls_ms, "local_solve_launches": ls_n, "launches": launches,
-            "local_solve_bytes": g.local_solve_bytes(), "clocks": clocks,
-            "local_solve_column_bytes": g.stat("local_solve_column_bytes"),
-            "spmv_ms_total": sp_ms, "spmv_calls": sp_n,
-            "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
-        }
-    # ---- batched form: k right-hand sides solved at once on one setup (k host threads, each call on
-    # its own workspace and stream); a step is one batch, timed from the first call to the last return
-    import threading
-    g, kw = forms["mixed"]
-    batched = {}
-    for k in [int(v) for v in str(a.batch).split(",") if v.strip() and int(v) > 1]:
-        rng = np.random.default_rng(4321)
-        bs = [b_dev] + [torch.tensor(rng.uniform(-1.0, 1.0, n), device=dev) for _ in range(k - 1)]
-        xs = [torch.zeros(n, device=dev, dtype=torch.float64) for _ in range(k)]
-        its_k = [None] * k
-        conv_k = [None] * k
-
-        def one_batch():
-            errs = []
-
-            def body(j):
-                try:
-                    _, r = g.gmres(bs[j].data_ptr(), device_out=xs[j].data_ptr(), **kw)
-                    its_k[j] = r["iterations"]
-                    conv_k[j] = r["converged"] and r["true_rel_residual"] <= wl.rtol
-                except Exception as e:  # re-raised below
-                    errs.append(e)
-
-            for x in xs:
-                x.zero_()
-            torch.cuda.synchronize()
-            ts = [threading.Thread(target=body, args=(j,)) for j in range(k)]
-            for t in ts:
-                t.start()
-            for t in ts:
-                t.join()
-            if errs:
-                raise errs[0]
-
-        for _ in range(a.warmup):
-            one_batch()
-        barrier()
-        per_b = []
-        for _ in range(a.steps):
-            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s_ev.record(stream)
-            one_batch()
-            e_ev.record(stream)  # every call of the batch has returned with its work complete
-            e_ev.synchronize()
-            per_b.append(s_ev.elapsed_time(e_ev))
-        barrier()
-        tot = max_over_ranks(sum(per_b))
-        batched[str(k)] = {"rhs": k, "ms_per_batch": tot / a.steps, "solves_per_s": world * k * a.steps / (tot * 1e-3),
-                           "iterations": list(its_k), "converged": all(conv_k),
-                           "p50_batch_ms": float(np.percentile(per_b, 50)),
-                           "p99_batch_ms": float(np.percentile(per_b, 99))}
-        del bs, xs
-    # ---- block form: k right-hand sides in one lockstep block GMRES (s2l_gpu_gmres_block): the
-    # preconditioner, A and the orthogonalization run once per step for all k columns
-    block = {}
-    head = None
-    bw = int(g.stat("block_width"))  # one block of this width is the unit wider steps run concurrently
+    # ---- blocks of k right-hand sides (the first is the workload's b), errors against FP64
+    kh = a.head_k
+    rng = np.random.default_rng(4321)
+    B_host = np.stack([st.b] + [rng.uniform(-1.0, 1.0, n) for _ in range(max(kh, 16) - 1)])
+    X64 = fp64_solutions(g64, B_host, kw64)
+    bw = int(g32.stat("block_width"))
     ks = [int(v) for v in str(a.block).split(",") if v.strip() and int(v) >= 1]
-    for extra in (bw, a.head_k):
+    for extra in (bw, kh):
         if extra not in ks:
             ks = [extra] + ks
+    block, head, rf = {}, None, None
     for k in ks:
-        is_head = k == a.head_k
-        is_rf = k == bw
-        rng = np.random.default_rng(4321)
-        Bk = torch.stack([b_dev] + [torch.tensor(rng.uniform(-1.0, 1.0, n), device=dev) for _ in range(k - 1)])
+        Bk = torch.tensor(B_host[:k], device=dev)
         Xk = torch.zeros_like(Bk)
-        res_k = None
-        for _ in range(a.warmup):
-            Xk.zero_()
-            _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
-        if is_rf:
-            g.profile(("local_solve", "spmv"))
-        if is_head:
-            sampler = ClockSampler(local)
-            sampler.start()
-        barrier()
-        per_k = []
-        for _ in range(a.steps):
-            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s_ev.record(stream)
-            Xk.zero_()
-            _, res_k = g.gmres_block((Bk.data_ptr(), k), device_out=Xk.data_ptr(), **kw)
-            e_ev.record(stream)
-            e_ev.synchronize()
-            per_k.append(s_ev.elapsed_time(e_ev))
-        barrier()
-        tot = max_over_ranks(sum(per_k))
-        if is_head:
-            head_clocks = sampler.stop()
-        if is_rf:
-            rf_ls = g.profile_get("local_solve")
-            rf_sp = g.profile_get("spmv")
-            rf_launches = g.launches()
-            g.profile(())
-        Xh = Xk.cpu().numpy()
-        chk = max(float(np.linalg.norm(Bk[j].cpu().numpy() - st.A @ Xh[j]) / np.linalg.norm(Bk[j].cpu().numpy()))
-                  for j in range(k))
-        block[str(k)] = {"rhs": k, "ms_per_block": tot / a.steps, "ms_per_solve": tot / a.steps / k,
-                         "solves_per_s": world * k * a.steps / (tot * 1e-3),
-                         "iterations": [r["iterations"] for r in res_k],
-                         "converged": all(r["converged"] for r in res_k), "true_rel_residual_host_check": chk,
-                         "p50_block_ms": float(np.percentile(per_k, 50)),
-                         "p99_block_ms": float(np.percentile(per_k, 99))}
-        if is_head:
-            head = dict(block[str(k)], per_block_ms=per_k, clocks=head_clocks)
-        if is_rf:
-            rf = dict(ls=rf_ls, sp=rf_sp, launches=rf_launches, steps=a.steps)
+        sampler = ClockSampler(local) if k == kh else None
+        out, per, clocks, prof = block_form(tm, g32, Bk, Xk, k, kw32, X_ref=X64[:k], prof=(k == bw), sampler=sampler)
+        block[str(k)] = out
+        if k == kh:
+            head = dict(out, per_block_ms=per, clocks=clocks)
+        if k == bw:
+            rf = prof
         del Bk, Xk
-    # ---- several k=4 blocks at once from host threads (each on its own workspace and stream)
-    block_thr = {}
-    for nt in [int(v) for v in str(a.block_threads).split(",") if v.strip() and int(v) > 1]:
-        rng = np.random.default_rng(99)
-        Bs = [torch.tensor(rng.uniform(-1.0, 1.0, (4, n)), device=dev) for _ in range(nt)]
-        Xs = [torch.zeros_like(B_) for B_ in Bs]
-        conv_t = [True] * nt
-
-        def one_round():
-            errs = []
-
-            def body(j):
-                try:
-                    _, rr = g.gmres_block((Bs[j].data_ptr(), 4), device_out=Xs[j].data_ptr(), **kw)
-                    conv_t[j] = all(r["converged"] for r in rr)
-                except Exception as e:  # re-raised below
-                    errs.append(e)
-
-            for X_ in Xs:
-                X_.zero_()
-            torch.cuda.synchronize()
-            ts = [threading.Thread(target=body, args=(j,)) for j in range(nt)]
-            for t in ts:
-                t.start()
-            for t in ts:
-                t.join()
-            if errs:
-                raise errs[0]
-
-        for _ in range(a.warmup):
-            one_round()
-        barrier()
-        per_t = []
-        for _ in range(a.steps):
-            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s_ev.record(stream)
-            one_round()
-            e_ev.record(stream)
-            e_ev.synchronize()
-            per_t.append(s_ev.elapsed_time(e_ev))
-        barrier()
-        tot = max_over_ranks(sum(per_t))
-        block_thr[str(nt)] = {"threads": nt, "rhs_per_block": 4, "solves_per_s": world * 4 * nt * a.steps / (tot * 1e-3),
-                              "converged": all(conv_t)}
-        del Bs, Xs
-    # ---- serving: Poisson arrivals of solve requests over three resident matrices (this workload in
-    # mixed precision, the 2D Poisson case, a convection-diffusion case with FP32 LU factors) on the
-    # engine's worker threads; latency = request submitted -> solution ready (host clock)
-    serving = None
-    if a.serve > 0:
-        from s2l_b200.serving import Engine
-        cases = {"bubbles3d": (lambda: st32, dict(restart=wl.restart, rtol=wl.rtol, flexible=True, strict=True))}
-        wp = W.poisson2d()
-        st_p = W.build(wp)
-        cases["poisson2d"] = (lambda: st_p, dict(restart=wp.restart, rtol=wp.rtol))
-        wc = W.convdiff3d(32, 8)
-        st_c = W.build(wc)
-        cases["convdiff3d"] = (lambda: st_c, dict(restart=wc.restart, rtol=wc.rtol, flexible=True, strict=True))
-        eng = Engine(local, hbm_budget=150 << 30, workers=4)
-        for key, (mk, kwk) in cases.items():  # warm: setups built and resident before the arrivals
-            t = eng.submit(key, mk, mk().b, **kwk)
-            t.wait(600.0)
-            t.free()
-        rng = np.random.default_rng(2026)
-        keys = list(cases)
-        mix = [0.5, 0.25, 0.25]
-        gaps = rng.exponential(1.0 / a.serve_rate, a.serve)
-        picks = rng.choice(len(keys), a.serve, p=mix)
-        tickets = []
-        t0 = time.perf_counter()
-        t_next = t0
-        for i in range(a.serve):
-            t_next += gaps[i]
-            dt = t_next - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            key = keys[picks[i]]
-            mk, kwk = cases[key]
-            b_i = rng.uniform(-1.0, 1.0, mk().n)
-            tickets.append((key, eng.submit(key, mk, b_i, history_cap=0, **kwk)))
-        lat = []
-        per_key = {k: {"lat": [], "run": [], "its": []} for k in keys}
-        ok = True
-        for key, t in tickets:
-            _, r, status = t.wait(600.0)
-            ok = ok and status == 0 and r["converged"]
-            info = t.info()
-            lat.append(info["queue_ms"] + info["run_ms"])
-            per_key[key]["lat"].append(info["queue_ms"] + info["run_ms"])
-            per_key[key]["run"].append(info["run_ms"])
-            per_key[key]["its"].append(r["iterations"])
-            t.free()
-        t_end = time.perf_counter()
-        serving = {"requests": a.serve, "rate_req_s": a.serve_rate, "mix": dict(zip(keys, mix)),
-                   "all_converged": ok, "solves_per_s": a.serve / (t_end - t0),
-                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                   "max_ms": float(np.max(lat)), "workers": 4, "setups_built": eng.builds,
-                   "per_case": {k: {"requests": len(v["lat"]),
-                                    "p50_ms": float(np.percentile(v["lat"], 50)) if v["lat"] else None,
-                                    "p99_ms": float(np.percentile(v["lat"], 99)) if v["lat"] else None,
-                                    "run_ms_mean": float(np.mean(v["run"])) if v["run"] else None,
-                                    "iterations_mean": float(np.mean(v["its"])) if v["its"] else None}
-                                for k, v in per_key.items()},
-                   "clock": "host (submit to solution ready)"}
-        eng.close()
-
-    serving_mix = serve_mix(a, local) if a.serve_mix > 0 else None
-
-    # ---- AMG local solvers (the reference's --local-approx amg): the same matrix, partition and
-    # coarse basis, each subdomain's A_ii^-1 replaced by one AMG V-cycle; plain FP64 GMRES
-    amg_form = None
-    if a.amg and a.workload == "bubbles3d":
-        import dataclasses
-        from s2l_b200.amg import build_hierarchy_native as build_hierarchy
-        t0a = time.time()
-        subs_amg = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii)) for sd in st.subdomains]
-        st_amg = dataclasses.replace(st, subdomains=subs_amg)
-        amg_setup_s = time.time() - t0a
-        ga = capi.GpuSetup(ctx, st_amg)
-        ga.set_stream(stream.cuda_stream)
-        kwa = dict(restart=wl.restart, rtol=wl.rtol, flexible=False, strict=False, maxit=2000)
-        for _ in range(a.warmup):
-            x_dev.zero_()
-            ga.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kwa)
-        ga.profile(("local_solve",))
-        barrier()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-        its_a = []
-        for k in range(a.steps):
-            evs[k][0].record(stream)
-            x_dev.zero_()
-            _, ra = ga.gmres(b_dev.data_ptr(), device_out=x_dev.data_ptr(), **kwa)
-            evs[k][1].record(stream)
-            its_a.append(ra["iterations"])
-        barrier()
-        per_a = [s_.elapsed_time(e_) for s_, e_ in evs]
-        vc_ms, vc_n = ga.profile_get("local_solve")
-        ga.profile(())
-        xa = x_dev.cpu().numpy()
-        levels = sorted({len(sd.amg.levels) + (sd.amg.coarse is not None) for sd in subs_amg})
-        amg_form = {"ms_per_solve": max_over_ranks(sum(per_a)) / a.steps, "iterations": its_a,
-                    "converged": bool(ra["converged"]),
-                    "true_rel_residual_host_check": float(np.linalg.norm(st.b - st.A @ xa) / np.linalg.norm(st.b)),
-                    "v_cycle_ms": vc_ms / max(vc_n, 1), "levels": levels,
-                    "operator_entries": int(sum(sd.amg.nnz() for sd in subs_amg)),
-                    "host_setup_s": amg_setup_s,
-                    "vs_plain_fp64_exact": {"ms_per_solve": results["plain_fp64"]["ms_per_solve"],
-                                            "iterations": results["plain_fp64"]["iterations"]}}
-        ga.close()
 
     # ---- end to end through the C ABI with pinned host buffers (headline block form): each step
     # copies its k right-hand sides and initial guesses in and its k solutions out
-    g, kw = forms["mixed"]
-    kh = a.head_k
-    rng = np.random.default_rng(4321)
     b_pin = torch.empty((kh, n), dtype=torch.float64, pin_memory=True)
-    b_pin.numpy()[0] = st.b
-    for j in range(1, kh):
-        b_pin.numpy()[j] = rng.uniform(-1.0, 1.0, n)
+    b_pin.numpy()[:] = B_host[:kh]
     x_pin = torch.zeros((kh, n), dtype=torch.float64, pin_memory=True)
-    barrier()
-    e2e = []
-    for _ in range(a.steps):
-        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def e2e_step():
         x_pin.zero_()
-        s_ev.record(stream)
-        g.gmres_block(b_pin.numpy(), X0=x_pin.numpy(), history_cap=0, **kw)
-        e_ev.record(stream)
-        e_ev.synchronize()
-        e2e.append(s_ev.elapsed_time(e_ev))
-    barrier()
-    e2e_total = max_over_ranks(sum(e2e))
+        return g32.gmres_block(b_pin.numpy(), X0=x_pin.numpy(), history_cap=0, **kw32)
 
-    # ---- sequence: the next matrices of the moving-bubble sequence (bubble centres rise half a cell
-    # per step, same pattern), each refactorized on the device (s2l_gpu_refactor: new local factors
-    # on the kept patterns, E with the kept basis; the reference's refactorize level) and solved for
-    # head_k right-hand sides; a step is timed from the upload of the new values to the solutions
-    sequence = None
-    if a.seq > 0:
-        import dataclasses
-        import scipy.sparse as sp
-        from s2l_b200 import sequence as seqmod
-        g, kw = forms["mixed"]
-        rng = np.random.default_rng(77)
-        Bq = torch.tensor(rng.uniform(-1.0, 1.0, (kh, n)), device=dev)
-        Xq = torch.zeros_like(Bq)
-        steps_q = []
-        for step in range(1, a.seq + 1):
-            prob = W.make_problem(dataclasses.replace(wl, time=float(step)))
-            vals, _ = seqmod.values_in_setup_order(prob.A, st)
-            At = sp.csr_matrix((vals, st.A.indices, st.A.indptr), shape=st.A.shape)
-            barrier()
-            s_ev, m_ev, e_ev = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            s_ev.record(stream)
-            g.refactor(vals)
-            m_ev.record(stream)
-            Xq.zero_()
-            _, rq = g.gmres_block((Bq.data_ptr(), kh), device_out=Xq.data_ptr(), **kw)
-            e_ev.record(stream)
-            e_ev.synchronize()
-            Xh = Xq.cpu().numpy()
-            Bh = Bq.cpu().numpy()
-            chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(kh))
-            steps_q.append({"step": step, "refactor_ms": s_ev.elapsed_time(m_ev), "solve_ms": m_ev.elapsed_time(e_ev),
-                            "refactor_phases_ms": {k: round(g.stat("refactor_ms_" + k), 2)
-                                                   for k in ("coarse", "coarse_inverse", "sparse", "tail", "dense",
-                                                             "commit")},
-                            "iterations_max": max(r["iterations"] for r in rq),
-                            "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
-        g.refactor(st32.A.data)  # back to the setup's own matrix
-        tot_ms = sum(q["refactor_ms"] + q["solve_ms"] for q in steps_q)
-        sequence = {"matrices": a.seq, "rhs_per_matrix": kh, "update": "refactorize", "steps": steps_q,
-                    "refactor_ms_mean": float(np.mean([q["refactor_ms"] for q in steps_q])),
-                    "refactor_plan_gb": g.stat("refactor_bytes") / 1e9,
-                    "solves_per_s": a.seq * kh / (tot_ms * 1e-3)}
-        del Bq, Xq
+    e2e_per, e2e_total, _ = tm.run(e2e_step, warmup=1)
+    e2e_err = max(rel_err(x_pin.numpy()[j], X64[j]) for j in range(kh))
 
-    mixed = results["mixed"]
-    plain = results["plain_fp64"]
+    # ---- serving: continuous batching of Poisson arrivals on this matrix (mixed precision)
+    serving = None
+    if a.serve > 0:
+        bpool = B_host[:16]
+        serving = serve_form(local, st32, kw32, a.serve, a.serve_rate, bpool, X64[:16])
+        serving["speedup_vs_plain_fp64_per_solve"] = plain["ms_per_solve"] / serving["ms_per_solve"]
+
+    # ---- AMG local solvers (the reference's --local-approx amg) on the same matrix and basis
+    amg_form = amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64) if a.amg else None
+
     # roofline of the headline's dominant kernel group: the block local solve (factors read once,
-    # every column's gather and owned write)
+    # every column's gather and owned write), and of the single-column forms and the SpMV
     head_bytes = g32.local_solve_bytes() + (bw - 1) * g32.stat("local_solve_column_bytes")
     ls_avg_ms = rf["ls"][0] / max(rf["ls"][1], 1)
     traffic = measured_traffic(head_bytes)
     achieved = head_bytes / (ls_avg_ms * 1e-3) / 1e9 if ls_avg_ms > 0 else 0.0
-    ls_avg_ms32 = mixed["local_solve_ms_total"] / max(mixed["local_solve_launches"], 1)
-    achieved32 = mixed["local_solve_bytes"] / (ls_avg_ms32 * 1e-3) / 1e9 if ls_avg_ms32 > 0 else 0.0
-    ls_avg_ms64 = plain["local_solve_ms_total"] / max(plain["local_solve_launches"], 1)
-    achieved64 = plain["local_solve_bytes"] / (ls_avg_ms64 * 1e-3) / 1e9 if ls_avg_ms64 > 0 else 0.0
 
     def rate(nbytes, ms):
         gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
         return {"achieved": gbs, "frac": gbs / peak}
 
-    # SpMV (y = A x and the residual forms, averaged over every call; bytes of y = A x, so a lower bound)
+    def ls_rate(f):
+        ms = f["local_solve_ms_total"] / max(f["local_solve_launches"], 1)
+        return dict(rate(f["local_solve_bytes"], ms), avg_launch_ms=ms, bytes_per_launch=f["local_solve_bytes"])
+
     spmv = {"single_column_fp32": dict(rate(spmv_bytes(st), mixed["spmv_ms_total"] / max(mixed["spmv_calls"], 1)),
                                        bytes_per_launch=spmv_bytes(st), calls=mixed["spmv_calls"]),
             "single_column_fp64": dict(rate(spmv_bytes(st), plain["spmv_ms_total"] / max(plain["spmv_calls"], 1)),
                                        bytes_per_launch=spmv_bytes(st), calls=plain["spmv_calls"]),
             f"block_{bw}": dict(rate(spmv_bytes(st, bw), rf["sp"][0] / max(rf["sp"][1], 1)),
                                 bytes_per_launch=spmv_bytes(st, bw), calls=rf["sp"][1])}
-    # whole solves: algorithmic bytes of every Arnoldi step over the solve's wall time
     col32 = mixed["local_solve_column_bytes"]
-    per_solve = {
-        "headline_block": dict(rate(gmres_solve_bytes(st, head["iterations"], wl.restart, mixed["local_solve_bytes"],
-                                                      col32), head["ms_per_block"]),
-                               bytes=gmres_solve_bytes(st, head["iterations"], wl.restart,
-                                                       mixed["local_solve_bytes"], col32)),
-        "mixed": dict(rate(gmres_solve_bytes(st, mixed["iterations"][:1], wl.restart, mixed["local_solve_bytes"],
-                                             col32), mixed["ms_per_solve"]),
-                      bytes=gmres_solve_bytes(st, mixed["iterations"][:1], wl.restart, mixed["local_solve_bytes"],
-                                              col32)),
-        "plain_fp64": dict(rate(gmres_solve_bytes(st, plain["iterations"][:1], wl.restart, plain["local_solve_bytes"],
-                                                  plain["local_solve_column_bytes"]), plain["ms_per_solve"]),
-                           bytes=gmres_solve_bytes(st, plain["iterations"][:1], wl.restart,
-                                                   plain["local_solve_bytes"], plain["local_solve_column_bytes"])),
-    }
+    hb = gmres_solve_bytes(st, head["iterations"], wl.restart, mixed["local_solve_bytes"], col32)
+    mb = gmres_solve_bytes(st, mixed["iterations"][:1], wl.restart, mixed["local_solve_bytes"], col32)
+    pb = gmres_solve_bytes(st, plain["iterations"][:1], wl.restart, plain["local_solve_bytes"],
+                           plain["local_solve_column_bytes"])
+    per_solve = {"headline_block": dict(rate(hb, head["ms_per_block"]), bytes=hb),
+                 "mixed": dict(rate(mb, mixed["ms_per_solve"]), bytes=mb),
+                 "plain_fp64": dict(rate(pb, plain["ms_per_solve"]), bytes=pb)}
+    layout_stats = {"options": layout, "tail_rows": g64.stat("tail_rows"), "sparse_nnz": g64.stat("sparse_nnz"),
+                    "coupling_nnz": g64.stat("coupling_nnz"), "dense_entries": g64.stat("dense_entries"),
+                    "sweep_group": g64.stat("sweep_group"), "levels_max": g64.stat("levels_max"),
+                    "chain_blocks": g64.stat("chain_blocks"), "sweep_tasks": g64.stat("sweep_tasks"),
+                    "sweep_padding": g64.stat("sweep_padding"), "kc_max_fp32": g32.stat("kc_max"),
+                    "levels_mean": round(g64.stat("levels_mean"), 1), "block_width": bw}
+    g64.close()
+    g32.close()
+    del b_dev, x_dev
+
+    # ---- the other configurations (each builds, times and frees its own setups)
+    c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if a.overlap2 and a.overlap != 2 else None
+    sequence = sequence_form(a, tm, ctx, stream, dev) if a.seq > 0 else None
+    c3 = c3_form(a, tm, ctx, stream, dev) if a.c3 > 0 else None
+    serving_mix = serve_mix(a, local) if a.serve_mix > 0 and world == 1 else None
+
     out = {
         "metric": METRIC,
         # whole-job throughput of the headline form: blocks of k right-hand sides, mixed precision
@@ -707,46 +554,42 @@ def run_ours(a):
             "n": st.n, "nnz": int(st.A.nnz), "n0": st.n0, "nnz_factors": st.stats.get("nnz_factors"),
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU, all subdomains resident",
             "l2": "inputs larger than L2 (local factors %.1f GB per form)" % (mixed["local_solve_bytes"] / 1e9),
-            "setup_s": round(setup_s, 1) if world == 1 else None,
-            "layout": {"options": layout, "tail_rows": g64.stat("tail_rows"), "sparse_nnz": g64.stat("sparse_nnz"),
-                       "coupling_nnz": g64.stat("coupling_nnz"), "dense_entries": g64.stat("dense_entries"),
-                       "sweep_group": g64.stat("sweep_group"), "levels_max": g64.stat("levels_max"),
-                       "chain_blocks": g64.stat("chain_blocks"), "sweep_tasks": g64.stat("sweep_tasks"),
-                       "sweep_padding": g64.stat("sweep_padding"), "kc_max_fp32": g32.stat("kc_max"),
-                       "levels_mean": round(g64.stat("levels_mean"), 1)},
+            "setup_s": round(setup_s, 1),
+            "layout": layout_stats,
         },
         "forms": {
             "block_mixed": block,
             "mixed": {k: mixed[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
-                                             "true_rel_residual_host_check", "p50_ms", "p99_ms")},
-            "plain_fp64": {k: plain[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
-                                                  "true_rel_residual_host_check", "p50_ms", "p99_ms")},
-            "batched_mixed": batched,
-            "block_mixed_threads": block_thr,
+                                             "true_rel_residual_host_check", "p50_ms", "p99_ms",
+                                             "rel_error_vs_fp64")},
+            "plain_fp64": dict({k: plain[k] for k in ("ms_per_solve", "iterations", "converged", "true_rel_residual",
+                                                      "true_rel_residual_host_check", "p50_ms", "p99_ms")},
+                               note="the reference arm's configuration: same matrix, partition, right-hand "
+                                    "side, overlap, FP64 L L^T factors, GMRES(50), one right-hand side per solve"),
             "serving": serving,
-            "serving_mix": serving_mix,
             "amg_local_solves": amg_form,
-            "sequence_refactor": sequence,
+            "c2_overlap2": c2_overlap2,
+            "sequence": sequence,
+            "c3_convdiff": c3,
+            "serving_mix": serving_mix,
             "speedup_head_vs_plain_per_solve": plain["ms_per_solve"] / head["ms_per_solve"],
             "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
             "iteration_delta_mixed_vs_plain": mixed["iterations"][0] - plain["iterations"][0],
             "iteration_delta_head_vs_plain": max(head["iterations"]) - plain["iterations"][0],
+            "rel_error_head_vs_fp64": head.get("rel_error_vs_fp64"),
         },
         "p50_ms": head["p50_block_ms"],
         "p99_ms": head["p99_block_ms"],
-        "e2e": {"value": world * kh * a.steps / (e2e_total * 1e-3), "unit": "solves/s",
+        "e2e": {"value": world * kh * len(e2e_per) / (e2e_total * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": 2 * 8 * n * kh, "d2h_bytes_per_step": 8 * n * kh,
-                "ms_per_step": e2e_total / a.steps},
+                "ms_per_step": e2e_total / len(e2e_per), "rel_error_vs_fp64": e2e_err},
         "roofline": {"bound": "hbm",
                      "kernel": f"local solve of one {bw}-column block (sweeps, tail coupling, dense tails); the "
                                f"{kh}-column step runs {max(kh // bw, 1)} such blocks at once",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "traffic": traffic,
                      "bytes_per_launch": head_bytes, "avg_launch_ms": ls_avg_ms,
-                     "single_column_fp32": {"achieved": achieved32, "frac": achieved32 / peak,
-                                            "avg_launch_ms": ls_avg_ms32, "bytes_per_launch": mixed["local_solve_bytes"]},
-                     "single_column_fp64": {"achieved": achieved64, "frac": achieved64 / peak,
-                                            "avg_launch_ms": ls_avg_ms64, "bytes_per_launch": plain["local_solve_bytes"]},
+                     "single_column_fp32": ls_rate(mixed), "single_column_fp64": ls_rate(plain),
                      "spmv": spmv, "per_solve": per_solve},
         # kernels launched in the timed region: those of the timed k=bw blocks, times the blocks
         # a k=head step runs at once
@@ -754,34 +597,206 @@ def run_ours(a):
         "clocks": head["clocks"],
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(st, plain["iterations"][0], wl.restart)
+        cb, parity = cpu_baseline_leg(a, wl) if a.overlap == 1 else (None, None)
+        if cb is not None:
+            out["cpu_baseline"] = cb
+            out["forms"]["plain_fp64"]["speedup_vs_reference_same_config"] = cb["ms_per_solve"] / plain["ms_per_solve"]
+            out["forms"]["speedup_head_vs_reference_per_solve"] = cb["ms_per_solve"] / head["ms_per_solve"]
+        if parity is not None and a.parity:
+            out["parity"] = parity
     if rank == 0:
         print(json.dumps(out), flush=True)
-    g64.close()
-    g32.close()
     ctx.close()
     reps.close()
 
 
+def amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64):
+    """The same matrix, partition and coarse basis with each A_ii^-1 replaced by one AMG V-cycle."""
+    import dataclasses
+    import numpy as np
+    from s2l_b200 import capi
+    from s2l_b200.amg import build_hierarchy_native as build_hierarchy
+    t0 = time.time()
+    subs = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii)) for sd in st.subdomains]
+    st_amg = dataclasses.replace(st, subdomains=subs)
+    host_s = time.time() - t0
+    ga = capi.GpuSetup(ctx, st_amg)
+    ga.set_stream(stream.cuda_stream)
+    kw = dict(restart=50, rtol=1e-8, flexible=False, strict=False, maxit=2000)
+    f, xa = single_form(tm, ga, b_dev, x_dev, kw, x_ref=x64)
+    ga.close()
+    levels = sorted({len(sd.amg.levels) + (sd.amg.coarse is not None) for sd in subs})
+    return {"ms_per_solve": f["ms_per_solve"], "iterations": f["iterations"], "converged": f["converged"],
+            "true_rel_residual_host_check": float(np.linalg.norm(st.b - st.A @ xa) / np.linalg.norm(st.b)),
+            "rel_error_vs_fp64": f["rel_error_vs_fp64"],
+            "v_cycle_ms": f["local_solve_ms_total"] / max(f["local_solve_launches"], 1), "levels": levels,
+            "operator_entries": int(sum(sd.amg.nnz() for sd in subs)), "host_setup_s": host_s,
+            "vs_plain_fp64_exact": {"ms_per_solve": plain["ms_per_solve"], "iterations": plain["iterations"]}}
+
+
+def three_forms(tm, ctx, st, w, stream, dev, k=16):
+    """Plain FP64, mixed (FP32 factors, flexible FP64 GMRES) and a k-right-hand-side mixed block on a
+    host setup; errors against the plain FP64 solutions."""
+    import numpy as np
+    import torch
+    from s2l_b200 import capi
+    from s2l_b200.setup_phase import with_factor_precision
+    st32 = with_factor_precision(st, "single")
+    st64 = with_factor_precision(st, "double")
+    g64, g32 = capi.GpuSetup(ctx, st64), capi.GpuSetup(ctx, st32)
+    for g in (g64, g32):
+        g.set_stream(stream.cuda_stream)
+    kw64 = dict(restart=w.restart, rtol=w.rtol, flexible=False, strict=False)
+    kw32 = dict(restart=w.restart, rtol=w.rtol, flexible=True, strict=True)
+    b_dev = torch.tensor(st.b, device=dev, dtype=torch.float64)
+    x_dev = torch.zeros(st.n, device=dev, dtype=torch.float64)
+    plain, x64 = single_form(tm, g64, b_dev, x_dev, kw64, prof=False)
+    mixed, _ = single_form(tm, g32, b_dev, x_dev, kw32, x_ref=x64, prof=False)
+    rng = np.random.default_rng(99)
+    B = np.stack([st.b] + [rng.uniform(-1.0, 1.0, st.n) for _ in range(k - 1)])
+    X64 = fp64_solutions(g64, B, kw64)
+    Bk = torch.tensor(B, device=dev)
+    Xk = torch.zeros_like(Bk)
+    blk, _, _, _ = block_form(tm, g32, Bk, Xk, k, kw32, X_ref=X64)
+    keep = ("ms_per_solve", "iterations", "converged", "true_rel_residual", "p50_ms", "p99_ms")
+    out = {"plain_fp64": {q: plain[q] for q in keep},
+           "mixed": dict({q: mixed[q] for q in keep}, rel_error_vs_fp64=mixed["rel_error_vs_fp64"]),
+           f"block_mixed_{k}": blk,
+           "speedup_mixed_vs_plain": plain["ms_per_solve"] / mixed["ms_per_solve"],
+           f"speedup_block_{k}_vs_plain_per_solve": plain["ms_per_solve"] / blk["ms_per_solve"],
+           "n": st.n, "n0": st.n0, "nnz_factors": st.stats.get("nnz_factors"),
+           "local_solve_gb_fp32": g32.local_solve_bytes() / 1e9}
+    g64.close()
+    g32.close()
+    return out
+
+
+def c2_overlap2_form(a, tm, ctx, stream, dev):
+    """The main problem at overlap 2 (the configuration as stated; the reference has overlap 1 only)."""
+    from s2l_b200 import workloads as W
+    w = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=2)
+    t0 = time.time()
+    st = W.build(w)
+    setup_s = time.time() - t0
+    out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
+    out.update(workload=workload_desc(w, 2), setup_s=round(setup_s, 1))
+    return out
+
+
+def c3_form(a, tm, ctx, stream, dev):
+    """3D upwind convection-diffusion 128^3 (4-mode divergence-free Fourier field, cell Peclet
+    0.1-10), 128 subdomains, overlap 1, nev 24, deflated RAS, LU factors, FGMRES(40)."""
+    from s2l_b200 import workloads as W
+    w = W.convdiff3d(a.c3, a.c3_nsub, precision="double")
+    t0 = time.time()
+    st = W.build(w)
+    setup_s = time.time() - t0
+    out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
+    out.update(workload=f"convdiff3d {w.nx}^3 upwind convection-diffusion, {w.nsub} subdomains, overlap 1, nev 24, "
+                        f"deflated RAS, LU factors, FGMRES({w.restart}), rtol 1e-8",
+               setup_s=round(setup_s, 1))
+    return out
+
+
+def sequence_form(a, tm, ctx, stream, dev):
+    """The moving-bubble sequence: a.seq matrices on one pattern (bubbles rise half a cell per step),
+    64 uneven subdomains (10k-25k rows), 16 right-hand sides per matrix solved as one block.  Before
+    each matrix the reference's reuse policy (time_loop.ReusePolicy, --reuse auto or refactor)
+    chooses the update: Refactorize (s2l_gpu_refactor on the device: new local factors on the kept
+    patterns, E with the kept basis) or Rebuild (a new host setup, uploaded).  A step is timed from
+    the update to the 16 solutions."""
+    import dataclasses
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from s2l_b200 import capi, workloads as W
+    from s2l_b200 import sequence as seqmod
+    from s2l_b200.setup_phase import build_setup, with_factor_precision
+    from s2l_b200.time_loop import ReusePolicy, UpdateLevel
+    w = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=a.overlap, precision="single")
+    w.imbalance = 0.15
+    prob0 = W.make_problem(w)
+    part = W.make_partition(w, prob0)
+    sizes = np.bincount(part, minlength=w.nsub)
+    k = a.head_k
+    kw = dict(restart=w.restart, rtol=w.rtol, flexible=True, strict=True, history_cap=0)
+    rng = np.random.default_rng(77)
+    B = rng.uniform(-1.0, 1.0, (k, prob0.n))  # original ordering; renumbered per setup
+    policy = ReusePolicy(a.seq_reuse)
+    g = st = None
+    steps = []
+    Bq = Xq = None
+    try:
+        for step in range(a.seq):
+            A = prob0.A if step == 0 else W.make_problem(dataclasses.replace(w, time=float(step))).A
+            level = UpdateLevel.REBUILD if g is None else policy.decide(True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if level == UpdateLevel.REBUILD:
+                st = with_factor_precision(build_setup(A, B[0], part, w.nsub, w.opts, prob0.symmetric), "single")
+                if g is not None:
+                    g.close()
+                g = capi.GpuSetup(ctx, st, options={"refactor": 1})
+                g.set_stream(stream.cuda_stream)
+                Bq = torch.tensor(B[:, st.new_to_old], device=dev)
+                Xq = torch.zeros_like(Bq)
+            else:
+                vals, _ = seqmod.values_in_setup_order(A, st)
+                g.refactor(vals)
+            torch.cuda.synchronize()
+            t_update = time.perf_counter() - t0
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            Xq.zero_()
+            _, rq = g.gmres_block((Bq.data_ptr(), k), device_out=Xq.data_ptr(), **kw)
+            e_ev.record(stream)
+            e_ev.synchronize()
+            t_solve = s_ev.elapsed_time(e_ev) * 1e-3
+            for j, r in enumerate(rq):  # one record per solve, as the reference's loop per corrector
+                red = r["true_rel_residual"]
+                policy.record(level if j == 0 else UpdateLevel.REUSE, r["iterations"], red, r["converged"],
+                              t_update if j == 0 else 0.0, t_solve / k)
+            Xh, Bh = Xq.cpu().numpy(), Bq.cpu().numpy()
+            At = sp.csr_matrix((st.A.data if level == UpdateLevel.REBUILD else vals, st.A.indices, st.A.indptr),
+                               shape=st.A.shape)
+            chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(k))
+            steps.append({"step": step, "level": level.name.lower(), "update_ms": t_update * 1e3,
+                          "solve_ms": t_solve * 1e3, "iterations_max": max(r["iterations"] for r in rq),
+                          "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
+    finally:
+        if g is not None:
+            g.close()
+    tot = sum(q["update_ms"] + q["solve_ms"] for q in steps[1:])
+    refac = [q["update_ms"] for q in steps if q["level"] == "refactorize"]
+    return {"matrices": a.seq, "rhs_per_matrix": k, "reuse": a.seq_reuse,
+            "levels": "".join(str(int(UpdateLevel[q["level"].upper()])) for q in steps),
+            "subdomain_rows": [int(sizes.min()), int(sizes.max())],
+            "rebuilds": sum(q["level"] == "rebuild" for q in steps),
+            "refactor_ms_mean": float(np.mean(refac)) if refac else None,
+            "solve_ms_mean": float(np.mean([q["solve_ms"] for q in steps])),
+            "solves_per_s_after_first": (a.seq - 1) * k / (tot * 1e-3) if tot > 0 else None,
+            "all_converged": all(q["converged"] for q in steps), "steps": steps}
+
+
 def serve_mix(a, device: int) -> dict:
-    """Poisson arrivals (a.serve_rate per second) of a.serve_mix solve requests, each on one of 40
-    seeded cases of the three workload families at several sizes (2D Poisson with LU factors,
+    """Poisson arrivals (a.serve_mix_rate per second) of a.serve_mix solve requests, each on one of
+    40 seeded cases of the three workload families at several sizes (2D Poisson with LU factors,
     bubbles3d with L L^T factors, convdiff3d with FP32 LU factors and flexible GMRES), on an engine
-    with a 150 GB HBM budget and 4 workers.  Every case is set up and resident before the first
-    arrival; latency = request submitted -> solution ready (host clock)."""
+    with a 150 GB HBM budget, 4 workers and continuous batching.  Every case is set up and
+    resident before the first arrival; latency = request submitted -> solution ready (host clock)."""
     import numpy as np
     from s2l_b200 import workloads as W
     from s2l_b200.serving import Engine
     cases = []
-    for nx in (100, 120, 140, 160, 180, 200):
-        for nsub in (4, 8):
+    for nx in (100, 200, 400, 700, 1000, 1400):
+        for nsub in (8, 32):
             cases.append(("poisson2d", W.poisson2d(nx, nsub)))
-    for nx, nsub in ((24, 8), (24, 16), (28, 8), (28, 16), (32, 8), (32, 16), (32, 32), (36, 8), (36, 16), (36, 32),
-                     (40, 8), (40, 16), (40, 32), (44, 16), (44, 32), (48, 16), (48, 32), (48, 64)):
-        w = W.bubbles3d(nx, nsub, nbubbles=max(4, (nx * nx * nx) // 5000), overlap=2)
+    for nx, nsub in ((24, 8), (28, 8), (32, 8), (32, 16), (36, 16), (40, 16), (40, 32), (44, 16), (48, 16), (48, 32),
+                     (56, 32), (56, 64), (64, 32), (64, 64), (72, 64), (80, 64), (90, 64), (100, 64)):
+        w = W.bubbles3d(nx, nsub, nbubbles=max(4, (nx * nx * nx) // 5000), overlap=1)
         cases.append(("bubbles3d", w))
-    for nx in (24, 28, 32, 40, 48):
-        for nsub in (8, 16):
+    for nx in (24, 32, 48, 64, 80):
+        for nsub in (8, 32):
             cases.append(("convdiff3d", W.convdiff3d(nx, nsub)))
     assert len(cases) == 40
     for q, (_, w) in enumerate(cases):
@@ -799,8 +814,9 @@ def serve_mix(a, device: int) -> dict:
         t.wait(600.0)
         t.free()
     rng = np.random.default_rng(2027)
-    gaps = rng.exponential(1.0 / a.serve_rate, a.serve_mix)
+    gaps = rng.exponential(1.0 / a.serve_mix_rate, a.serve_mix)
     picks = rng.integers(0, len(cases), a.serve_mix)
+    pools = {}
     tickets = []
     t_start = time.perf_counter()
     t_next = t_start
@@ -811,7 +827,9 @@ def serve_mix(a, device: int) -> dict:
             time.sleep(dt)
         q = int(picks[i])
         st = built[q]
-        b_i = rng.uniform(-1.0, 1.0, st.n)
+        if q not in pools:
+            pools[q] = [rng.uniform(-1.0, 1.0, st.n) for _ in range(4)]
+        b_i = pools[q][i % 4]
         tickets.append((q, eng.submit(q, (lambda st=st: st), b_i, **kws[q])))
     lat, fam_lat = [], {}
     ok = True
@@ -824,11 +842,12 @@ def serve_mix(a, device: int) -> dict:
         fam_lat.setdefault(cases[q][0], []).append(ms)
         t.free()
     t_end = time.perf_counter()
-    out = {"requests": a.serve_mix, "rate_req_s": a.serve_rate, "cases": len(cases),
+    out = {"requests": a.serve_mix, "rate_req_s": a.serve_mix_rate, "cases": len(cases),
            "sizes_n": [int(min(st.n for st in built)), int(max(st.n for st in built))],
            "hbm_budget_gb": 150, "all_converged": ok, "solves_per_s": a.serve_mix / (t_end - t_start),
            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
            "max_ms": float(np.max(lat)), "setups_built": eng.builds, "evictions": eng.evictions,
+           "batching": "continuous (automatic slots)",
            "per_family": {f: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)),
                               "p99_ms": float(np.percentile(v, 99))} for f, v in fam_lat.items()},
            "host_setup_s": setup_s, "clock": "host (submit to solution ready)"}
@@ -836,75 +855,102 @@ def serve_mix(a, device: int) -> dict:
     return out
 
 
-def cpu_baseline(st, iterations: int, restart: int) -> dict:
-    """The oracle (sequential C restatement) on a bounded sample: 3 GMRES iterations of the same solve."""
-    from oracle.oracle import OracleSetup
-    o = OracleSetup(st)
-    t0 = time.perf_counter()
-    _, res = o.gmres(st.b, restart=restart, rtol=1e-8, maxit=3)
-    dt = time.perf_counter() - t0
-    o.close()
-    per_it = dt / max(res["iterations"], 1)
-    est = per_it * iterations
-    return {"value": 1.0 / est, "unit": "solves/s", "cores": 1, "kind": "port",
-            "sample": f"{res['iterations']} GMRES iterations of the same FP64 solve ({dt:.1f} s, "
-                      f"{per_it * 1e3:.0f} ms/iteration), scaled to the GPU's {iterations} iterations"}
+def reference_flags(wl) -> list:
+    """The reference's command-line flags for the main workload's preconditioner and solver."""
+    return ["--rhs", "random", "--seed", str(wl.seed), "--pou", "boolean", "--one-level", "ras", "--coarse", "deflated",
+            "--nev", str(wl.opts.nev), "--local-solver", "sparselu", "--local-factorization", "cholesky",
+            "--coarse-solver", "root", "--krylov", "gmres", "--restart", str(wl.restart), "--rtol", str(wl.rtol)]
 
 
-# ------------------------------------------------------------------------------------ reference arm
-def reference_workload(a):
-    """The headline workload at the sizes of the arguments (0: the workload's own, 100^3 and 64
-    subdomains): the reference runs one thread-rank per subdomain on the same partition."""
+def reference_case(wl):
+    """The main workload's matrix and partition as the reference reads them (oracle.reference_runs)."""
+    import numpy as np
+    from oracle.reference_runs import MatrixCase
     from s2l_b200 import workloads as W
-    return W.bubbles3d(a.nx or 100, a.nsub or 64, nbubbles=a.nbubbles, overlap=a.overlap)
+    prob = W.make_problem(wl)
+    part = W.make_partition(wl, prob).astype(np.int32)
+    return MatrixCase(prob.A, part, wl.nsub, reference_flags(wl))
+
+
+def cpu_baseline_leg(a, wl) -> tuple:
+    """Rank 0 at N = 1, after every timed region.  The reference itself (oracle/_ref, built from its
+    sources) as the baseline and the checker:
+      baseline: its bench mode on the main workload (the same matrix, partition, right-hand side and
+                preconditioner as plain_fp64), one thread-rank per subdomain on the host's cores,
+                2 timed solves after its setup (its own barrier-to-barrier solve timer);
+      parity:   the drop-in check (oracle/_ref/dropin_check) on the main workload and at the c1 size:
+                the reference's TwoLevelSchwarz::apply and GMRES against the GPU drop-in's on the same
+                set-up objects (apply difference, iterations of both, GPU true residual).
+    Returns (cpu_baseline dict or None, parity dict or None)."""
+    from oracle import reference_runs as R
+    if not os.path.exists(R.REF_BIN):
+        return None, None
+    threads = a.ref_threads or os.cpu_count() or 1
+    case = reference_case(wl)
+    try:
+        rec = case.bench(steps=2, warmup=0)
+        cb = None
+        if rec is not None:
+            ms = 1e3 * sum(rec["solve_s"]) / len(rec["solve_s"])
+            cb = {"value": 1e3 / ms, "unit": "solves/s", "cores": threads, "kind": "reference", "ms_per_solve": ms,
+                  "iterations": rec.get("iterations"), "setup_s": rec.get("setup_s"),
+                  "sample": f"{len(rec['solve_s'])} full solves after the setup, {wl.nsub} thread-ranks on {threads} "
+                            f"host threads ({wl.nsub / threads:.1f} thread-ranks per thread), same matrix, partition, "
+                            f"right-hand side and preconditioner as plain_fp64"}
+        parity = {}
+        if os.path.exists(R.DROPIN_BIN):
+            runs = [(f"main_{wl.nx}cube_{wl.nsub}sub_overlap1", case.dropin)]
+            np1, args1 = R.FULL_SIZE["c1_laplace2d_200_8sub"]
+            runs.append(("c1_laplace2d_200_8sub", lambda: R.dropin(np1, args1)))
+            for name, fn in runs:
+                t0 = time.time()
+                try:
+                    r = fn()
+                    parity[name] = {"apply_rel": r["apply_rel_diff"], "its_ref": r["ref_iterations"],
+                                    "its_gpu": r["gpu_iterations"], "gpu_true_rel_residual": r["gpu_true_rel_residual"],
+                                    "x_rel_diff": r["x_rel_diff"], "ok": bool(r["ok"]),
+                                    "wall_s": round(time.time() - t0, 1)}
+                except Exception as e:  # reported in the line, not fatal to it
+                    parity[name] = {"error": str(e)[-300:]}
+        return cb, parity or None
+    finally:
+        case.close()
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    binary = os.path.join(REPO, "oracle", "_ref", "s2l_ref")
-    if not os.path.exists(binary):
+    if not os.path.exists(REF_BIN):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/s2l_ref was not built "
                                                              "(the reference compiles only where its sources are)"}))
         return
     import numpy as np
-    from s2l_b200 import workloads as W
-    from s2l_b200.rng import random_rhs  # noqa: F401  (the reference draws the same rhs itself)
-
-    wl = reference_workload(a)
-    prob = W.make_problem(wl)
-    part = W.make_partition(wl, prob).astype(np.int32)
-    threads = a.ref_threads or os.cpu_count() or 1
-    with tempfile.TemporaryDirectory() as td:
-        mtx = os.path.join(td, "A.mtx")
-        write_mtx(mtx, prob.A)
-        pf = os.path.join(td, "part.bin")
-        part.tofile(pf)
-        env = dict(os.environ, S2L_NP=str(wl.nsub), S2L_PART_FILE=pf, OMP_NUM_THREADS="1",
-                   S2L_REF_THREADS=str(threads))
-        cmd = [binary, "--matrix", mtx, "--rhs", "random", "--seed", str(wl.seed), "--pou", "boolean",
-               "--one-level", "ras", "--coarse", "deflated", "--nev", "20", "--local-solver", "sparselu",
-               "--local-factorization", "cholesky", "--coarse-solver", "root", "--krylov", "gmres",
-               "--restart", str(wl.restart), "--rtol", str(wl.rtol), "--verbose", "0",
-               "--bench-steps", str(a.steps), "--bench-warmup", str(a.warmup)]
-        r = subprocess.run(cmd, env=env, capture_output=True, text=True)
-    if r.returncode != 0:
-        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed ({r.returncode}): "
-                                                              f"{r.stderr.strip().splitlines()[-1:]}"}))
+    wl = main_workload(a)
+    if a.overlap != 1:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's overlap is one layer"}))
         return
-    rec = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    threads = a.ref_threads or os.cpu_count() or 1
+    case = reference_case(wl)
+    try:
+        rec = case.bench(a.steps, a.warmup)
+    finally:
+        case.close()
+    if rec is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+        return
     per = rec["solve_s"]
     ms = 1e3 * sum(per) / len(per)
     value = 1e3 / ms
     out = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "solves/s", "n_gpus": a.gpus,
         "steps": len(per), "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (same generator, partition and rhs)",
-        "config": {"workload": f"bubbles3d {wl.nx}^3 pressure Poisson, {wl.nsub} subdomains, overlap 1 (the "
-                               f"reference has no overlap 2), nev 20, deflated RAS, Eigen LL^T, root coarse "
-                               f"solver, GMRES(50), rtol 1e-8",
-                   "n": int(prob.n), "iterations": rec.get("iterations"), "setup_s": rec.get("setup_s"),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, U[-1,1] right-hand sides)",
+        "config": {"workload": workload_desc(wl, 1),
+                   "form": f"the reference's GMRES with its TwoLevelSchwarz (Eigen L L^T factors in FP64, root "
+                           f"coarse solver), one right-hand side per solve, {wl.nsub} thread-ranks on {threads} host "
+                           f"threads",
+                   "n": int(wl.nx ** 3), "iterations": rec.get("iterations"), "setup_s": rec.get("setup_s"),
                    "true_rel_residual": rec.get("true_rel_residual")},
         "p50_ms": float(np.percentile(np.array(per) * 1e3, 50)), "p99_ms": float(np.percentile(np.array(per) * 1e3, 99)),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
@@ -912,17 +958,6 @@ def run_reference(a):
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
-
-
-def write_mtx(path, A):
-    """Matrix Market coordinate file (1-based), full precision."""
-    import numpy as np
-    A = A.tocoo()
-    with open(path, "w") as f:
-        f.write("%%MatrixMarket matrix coordinate real general\n")
-        f.write(f"{A.shape[0]} {A.shape[1]} {A.nnz}\n")
-        data = np.column_stack([A.row + 1, A.col + 1, A.data])
-        np.savetxt(f, data, fmt=["%d", "%d", "%.17g"])
 
 
 if __name__ == "__main__":

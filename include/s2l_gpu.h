@@ -192,7 +192,14 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   blocks of up to this many rows; a block's rows are stored multiplied by the inverse of its
  *   diagonal block, so the block is one dependency level of the sweep instead of one per row;
  *   "refactor" (0 or 1, default 0): keep the factor patterns and their maps to the solve layout
- *   on the device so s2l_gpu_refactor can refactorize for new matrix values.
+ *   on the device so s2l_gpu_refactor can refactorize for new matrix values;
+ *   "pivot_tol" (default 1e-6, 0 = no check): s2l_gpu_refactor of LU (and LDL^T) factors keeps
+ *   the setup's pivot order, and reports S2L_ERR_NUMERIC when a pivot has become small against the
+ *   entries it divides (a multiplier larger than 1 / pivot_tol);
+ *   "spin_limit" (default 2^24): polls of one ready flag after which a sparse sweep gives up and
+ *   the call returns S2L_ERR_TIMEOUT (every wait of the sweeps is bounded).  Unlike the options
+ *   above it may also be set after s2l_gpu_setup_end; it applies to the launches that follow and
+ *   must not be changed while a solve-phase call runs on the setup.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 
@@ -215,7 +222,9 @@ int s2l_gpu_update_matrix(s2l_setup* s, const double* val, int ptr_kind);
  * src/preconditioner/coarse_space.cpp:95-105).  Needs the setup option "refactor" = 1, which keeps
  * the factor patterns and their maps to the solve layout on the device (setup stat
  * "refactor_bytes"); LU, LL^T and LDL^T factors.  S2L_ERR_NUMERIC for a non-finite value, a zero
- * (LU) or non-positive (LL^T) pivot or a singular E, and then the setup is unchanged.  Refused
+ * (LU) or non-positive (LL^T) pivot, an LU pivot small against its column (option "pivot_tol": the
+ * reference's refactorization would pivot again, this one keeps the order, so the caller rebuilds)
+ * or a singular E, and then the setup is unchanged.  Refused
  * (S2L_ERR_STATE) while a solve-phase call runs or solves are queued on the setup. */
 int s2l_gpu_refactor(s2l_setup* s, const double* val, int ptr_kind);
 
@@ -259,14 +268,18 @@ int s2l_gpu_apply(s2l_setup* s, const double* r, double* z, int ptr_kind);
  * (2 MiB), which every GPU that loads this library holds until the process exits.  A setup needs
  * (coarse tiles x largest m) + 2 n0 doubles of it, plus the local-space size for the multiplicity
  * partition of unity; a setup that needs more is rejected with S2L_ERR_BADARG before any launch.
- * r and x0 are device pointers (n doubles each).  The kernels are enqueued on the setup's stream
- * and the call returns; x0 is ready once that stream is synchronized.
+ * r and x0 are device pointers (n doubles each).  The call makes the setup's device current (as
+ * every solve-phase call does), enqueues the kernels on the setup's stream (s2l_gpu_set_stream) and
+ * returns; x0 is ready once that stream is synchronized.  Synchronize that stream before calling
+ * s2l_gpu_update_matrix, s2l_gpu_refactor, s2l_gpu_set_stream or s2l_gpu_setup_destroy on the same
+ * setup: they change what the enqueued kernels read.
  *
- * The first call on a device looks up the device address of the static array (with that device
- * current): make that first call before any stream capture on the device.  Every call shares the
- * one array and leaves its contents behind; every scratch element a call reads is written earlier
- * in the same call, so nothing needs clearing, but calls that overlap on the GPU (other streams,
- * other setups on the same device) race on it.
+ * The first call on a context looks up the device address of the static array (with the
+ * context's device current) and the context keeps it: make that first call before any stream
+ * capture on the device.  A context created after a reset of the device (cudaDeviceReset) looks it
+ * up anew.  Every call shares the one array and leaves its contents behind; every scratch element
+ * a call reads is written earlier in the same call, so nothing needs clearing, but calls that
+ * overlap on the GPU (other streams, other setups on the same device) race on it.
  */
 #define S2L_NOALLOC_SCRATCH_DOUBLES 262144
 int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, double* x0);
@@ -309,6 +322,20 @@ int s2l_gpu_gmres_block(s2l_setup* s, int k, const double* b, double* x, int ptr
 typedef struct s2l_ticket s2l_ticket;
 enum { S2L_JOB_QUEUED = 0, S2L_JOB_RUNNING = 1, S2L_JOB_DONE = 2, S2L_JOB_CANCELED = 3 };
 int s2l_gpu_serve_start(s2l_ctx* ctx, int workers);
+/* Continuous batching of the asynchronous GMRES solves (on by default, slots < 0: automatic).
+ * A worker that takes a GMRES request (L2 stopping test, restart <= 63, exact local factors) runs
+ * a block runner for its setup, restart length and variant: up to `slots` requests at once (the
+ * automatic width is the setup's block width, s2l_gpu_setup_stat "block_width"), each in a column
+ * of one block, so the preconditioner, the product with A and the orthogonalization of every
+ * Arnoldi step run once for all of them.  Each request keeps its own GMRES recurrence, restart
+ * cycle and convergence test; a request that arrives while the runner works takes a free slot at
+ * the next Arnoldi step and a request that converges returns at once, giving its slot to the next.
+ * A request's result does not depend on which others share the block (it is bitwise the same as
+ * alone in a runner of the same width).  More requests than slots start more runners on more
+ * workers; when a runner's block buffers do not fit the HBM budget it uses half the slots.
+ * slots = 0 turns batching off: every request then runs alone on its worker (first in, first
+ * out), as BiCGStab requests, the OpenFOAM stopping test and AMG local solvers always do. */
+int s2l_gpu_serve_batching(s2l_ctx* ctx, int slots);
 int s2l_gpu_submit(s2l_setup* s, int method, const double* b, double* x, int ptr_kind, const s2l_krylov_opts* opts,
                    s2l_result* result, s2l_ticket** ticket);
 /* state: S2L_JOB_* */

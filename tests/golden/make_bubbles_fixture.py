@@ -15,7 +15,7 @@ import scipy.io
 import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = "/root/reference/test/gamg/run_gamg_23038420"
+SRC = os.path.join(os.environ.get("S2L_REFERENCE_DIR", "/root/reference"), "test/gamg/run_gamg_23038420")
 
 
 def pattern_hash(A: sp.csr_matrix) -> str:

@@ -14,6 +14,7 @@ import subprocess
 import pytest
 
 from conftest import REPO
+from oracle.reference_runs import FULL_SIZE, dropin
 
 pytestmark = pytest.mark.gpu
 BIN = os.path.join(REPO, "oracle", "_ref", "dropin_check")
@@ -51,6 +52,20 @@ CASES = {
                               "--local-factorization", "lu", "--restart", "40", "--local-approx", "amg",
                               "--amg-coarsening", "rs", "--amg-coarse-enough", "50"]),
 }
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="oracle/_ref/dropin_check is built only where the reference sources are")
+@pytest.mark.parametrize("case", sorted(FULL_SIZE))
+def test_full_size_configuration_matches_reference(case):
+    """The parity targets at the benchmark sizes (oracle.reference_runs.FULL_SIZE: c1, and c2 at the
+    reference's overlap of one layer): apply within 1e-12 of the reference's
+    TwoLevelSchwarz::apply, GMRES iterations within +-1, FP64 true residual <= 1.1 rtol."""
+    np_, args = FULL_SIZE[case]
+    res = dropin(np_, args)
+    assert res["apply_rel_diff"] <= 1e-12, res
+    assert abs(res["ref_iterations"] - res["gpu_iterations"]) <= 1, res
+    assert res["gpu_converged"] and res["gpu_true_rel_residual"] <= 1.1e-8, res
+    assert res["ok"] and res["rc"] == 0, res
 
 
 @pytest.mark.skipif(not os.path.exists(BIN), reason="oracle/_ref/dropin_check is built only where the reference sources are")

@@ -173,3 +173,54 @@ def test_refactor_makes_the_coarse_correction_consistent_with_the_new_matrix(ctx
     fresh = np.linalg.norm(W.T @ (r - A2 @ g.coarse_apply(r))) / scale
     assert fresh <= 1e-10 and stale > 1e-4, (fresh, stale)
     g.close()
+
+
+def _permuted(st, sub: int):
+    """P_in A_ii Q of subdomain `sub` in the kept pivot order, with the global CSR position of each
+    of its entries."""
+    s = st.subdomains[sub]
+    f = s.factor
+    l2g = s.l2g()
+    rows, cols = l2g[f.perm_in], l2g[np.argsort(f.perm_out)]
+    A = st.A.tocsr()
+    pos = sp.csr_matrix((np.arange(A.nnz, dtype=np.float64) + 1.0, A.indices, A.indptr), shape=A.shape)
+    P = pos[rows][:, cols].toarray().astype(np.int64) - 1  # -1: not in the pattern
+    return P
+
+
+def _shrink_pivot(st, sub: int, k: int, factor: float):
+    """Matrix values with entry (k, k) of P_in A_ii Q of subdomain `sub` multiplied by `factor`."""
+    P = _permuted(st, sub)
+    assert P[k, k] >= 0
+    v = st.A.data.copy()
+    v[P[k, k]] *= factor
+    return v
+
+
+@pytest.mark.parametrize("where", ["sparse", "tail"])
+def test_refactor_reports_a_small_relative_pivot(ctx, where):
+    """LU refactorization keeps the setup's pivot order (the reference's SparseLU pivots again).  A
+    pivot that became small against the entries it divides is reported, and the setup is left
+    unchanged; with the check off (pivot_tol 0) the same values refactorize.
+    sparse: no tail (tail_max 0), the first pivot (column 0 has no updates, its multipliers are
+    A(i, 0) / A(0, 0));  tail: one sparse row (tail_rows >= every subdomain), the tail's first pivot
+    is entry (1, 1) when A(0, 1) = 0 (no update from column 0), its multipliers are its row."""
+    from s2l_b200.capi import GpuSetup, S2LError
+    _, st = small_setup("convdiff3d")
+    assert st.subdomains[0].factor.kind == "lu"
+    if where == "sparse":
+        layout, v = {"tail_max": 0}, _shrink_pivot(st, 0, 0, 1e-9)
+    else:
+        sub = next(i for i in range(st.nsub) if _permuted(st, i)[0, 1] < 0)
+        layout, v = {"tail_rows": 4096}, _shrink_pivot(st, sub, 1, 1e-9)
+    g = GpuSetup(ctx, st, options=dict(layout, refactor=1))
+    r = np.random.default_rng(5).standard_normal(st.n)
+    z0 = g.apply(r)
+    with pytest.raises(S2LError) as e:
+        g.refactor(v)
+    assert e.value.code == 4 and "pivot_tol" in str(e.value)
+    assert rel(g.apply(r), z0) <= 1e-15
+    g.close()
+    g = GpuSetup(ctx, st, options=dict(layout, refactor=1, pivot_tol=0.0))
+    g.refactor(v)
+    g.close()

@@ -339,6 +339,17 @@ def test_coupled_generator_structure():
     assert abs(problems.convdiff(2, 12, ncomp=1, coupled=True).A - problems.convdiff(2, 12).A).max() == 0.0
 
 
+def test_convdiff_description_as_the_reference_prints_it():
+    """The description line of the reference's generator (src/utils/matrix_generators.cpp:184-191):
+    the pulse and the time appear only for a pulsating convection, before (n=..., nnz=...)."""
+    from s2l_b200 import problems
+    p = problems.convdiff(2, 12, pulse=0.5, time=3.0, pulse_period=10)
+    assert p.description.startswith("convdiff2d 12x12 nu=1 pulse=0.5 t=3 (n=144, nnz="), p.description
+    q = problems.convdiff(3, 6, ncomp=2, coupled=True)
+    assert q.description.startswith("coupled3d 6x6x6 nu=1 ncomp=2 (n=432, nnz="), q.description
+    assert "pulse" not in q.description
+
+
 @pytest.mark.parametrize("kind,extra", [("reference_convdiff2d", {"pulse": 0.5, "pulse_period": 10}),
                                         ("reference_coupled2d", {"ncomp": 2})])
 def test_reference_generator_workloads_solve(kind, extra):

@@ -69,16 +69,18 @@ def test_reference_arm_runs_on_rank_zero_only():
 
 
 def test_reference_arm_runs_the_workload_sizes():
-    """The reference arm runs one thread-rank per subdomain of the workload: by default the
-    headline's 100^3 and 64 subdomains (not the 0 that stands for "the workload's" in the flags);
-    on a small case its line names the sizes it ran."""
+    """The reference arm runs one thread-rank per subdomain of the main workload: by default 100^3,
+    64 subdomains and overlap 1 (the reference's, so both arms run the same matrix, partition and
+    preconditioner and name it in the same words); on a small case its line names the sizes it ran."""
     import importlib.util
     import json
     spec = importlib.util.spec_from_file_location("bench_module", os.path.join(REPO, "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
-    wl = bench.reference_workload(bench.parse([]))
-    assert (wl.nx, wl.nsub) == (100, 64)
+    a = bench.parse([])
+    wl = bench.main_workload(a)
+    assert (wl.nx, wl.nsub, wl.opts.overlap, a.overlap) == (100, 64, 1, 1)
+    assert "overlap 1" in bench.workload_desc(wl, a.overlap)
     if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "s2l_ref")):
         return
     env = dict(os.environ, RANK="0", WORLD_SIZE="1")
@@ -88,5 +90,7 @@ def test_reference_arm_runs_the_workload_sizes():
     assert p.returncode == 0, p.stderr[-2000:]
     line = json.loads([l for l in p.stdout.splitlines() if l.startswith("{")][-1])
     assert "12^3" in line["config"]["workload"] and "4 subdomains" in line["config"]["workload"]
+    small = bench.parse(["--nx", "12", "--nsub", "4"])
+    assert line["config"]["workload"] == bench.workload_desc(bench.main_workload(small), 1)
     assert line["cpu_baseline"]["sample"].startswith("1 full solves, 4 thread-ranks")
     assert line["config"]["true_rel_residual"] <= 1.1e-8

@@ -47,6 +47,36 @@ def test_noalloc_matches_coarse_apply_twice(name, kw):
     ctx.close()
 
 
+def test_noalloc_on_the_callers_stream():
+    """With s2l_gpu_set_stream the kernels go on the caller's stream: writing r on a side stream,
+    calling the entry point and synchronizing only that stream gives the allocating path's result."""
+    import torch
+    from s2l_b200 import capi
+    ctx = capi.Context(0)
+    _, st = small_setup("bubbles3d")
+    g = capi.GpuSetup(ctx, st)
+    side = torch.cuda.Stream()
+    g.set_stream(side.cuda_stream)
+    rng = np.random.default_rng(7)
+    for call in range(2):
+        r = rng.standard_normal(st.n)
+        ref = g.coarse_apply(r)
+        r_host = torch.tensor(r, dtype=torch.float64).pin_memory()
+        with torch.cuda.stream(side):
+            rd = torch.empty(st.n, device="cuda", dtype=torch.float64)
+            xd = torch.empty_like(rd)
+            xd.fill_(float("nan"))
+            rd.copy_(r_host, non_blocking=True)  # r is written on the side stream only
+        g.coarse_apply_noalloc(rd.data_ptr(), xd.data_ptr())
+        side.synchronize()  # only the caller's stream
+        x = xd.cpu().numpy()
+        assert np.all(np.isfinite(x)), f"call {call}: output not fully written"
+        assert rel(x, ref) <= 1e-12, f"call {call}: {rel(x, ref):.3e}"
+    g.set_stream(None)
+    g.close()
+    ctx.close()
+
+
 def test_noalloc_refuses_setups_beyond_its_scratch():
     import torch
     from s2l_b200 import capi
