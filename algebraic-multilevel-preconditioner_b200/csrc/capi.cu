@@ -1263,8 +1263,8 @@ int coarse_apply(s2l_work* w, const double* r, double* x0)
                            boolean, r, s->mmax, w->d_cpart);
     launch_coarse_reduce(w->stream, s->nsub, s->d_subs, s->d_t_first, s->mmax, w->d_cpart, w->d_c);
     launch_dense_gemv(w->stream, (int)s->n0, s->d_Einv, w->d_c, w->d_y);
-    launch_coarse_prolong(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
-                          w->d_y, x0, w->d_plocal);
+    launch_coarse_prolong(w->stream, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->mmax,
+                          boolean, w->d_y, x0, w->d_plocal);
     if (!boolean) launch_combine(w->stream, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, w->d_plocal, nullptr, x0);
     w->launches += boolean ? 4 : 5;
     return S2L_OK;
@@ -1426,7 +1426,7 @@ int coarse_block(s2l_work* w, int K, const double* r, double* x0)
     launch_coarse_reduce_block(w->stream, K, s->nsub, s->d_subs, s->d_t_first, s->mmax, B.cpart, B.c);
     launch_dense_gemm(w->stream, K, (int)s->n0, s->d_Einv, B.c, B.y);
     launch_coarse_prolong_block(w->stream, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V,
-                                boolean, B.y, x0, B.plocal);
+                                s->mmax, boolean, B.y, x0, B.plocal);
     if (!boolean) launch_combine_block(w->stream, s->n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, B.plocal, nullptr, x0);
     w->launches += boolean ? 4 : 5;
     return S2L_OK;
@@ -2333,10 +2333,12 @@ int s2l_gpu_setup_end(s2l_setup* s)
             for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) rowsum[r] += s->A.v[e];
         RET_IF(upload(s, &s->d_rowsum, rowsum));
         const double avg = (double)s->nnz / (double)s->n;
-        // lanes per row: about four entries per lane (2 lanes for 5- and 7-point rows measured
-        // 1.5x faster than 8), between 2 and 32
+        // short rows (up to 16 entries on average): chunk mode, a warp per 32 rows with coalesced
+        // loads of their entries (spmv_tpr 1); longer rows: lanes per row for about four entries
+        // per lane, between 2 and 32
         int tpr = 2;
         while (tpr < 32 && tpr * 4 < avg) tpr *= 2;
+        if (avg <= 16.0) tpr = 1;
         s->tpr = s->opt_tpr ? s->opt_tpr : tpr;
     }
 
@@ -3145,8 +3147,8 @@ int coarse_matrix_dev(s2l_setup* s, cudaStream_t st, const double* v, double* E)
     const int boolean = s->pou == S2L_POU_BOOLEAN;
     for (int64_t c0 = 0; c0 < n0; c0 += K) {
         launch_unit_block(st, n0, (int)c0, R.Y);
-        launch_coarse_prolong_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean,
-                                    R.Y, R.X, R.plocal);
+        launch_coarse_prolong_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->mmax,
+                                    boolean, R.Y, R.X, R.plocal);
         if (!boolean) launch_combine_block(st, n, K, s->d_cp_ptr, s->d_cp_pos, nullptr, R.plocal, nullptr, R.X);
         launch_spmv_block(st, n, K, s->d_rp, s->d_ci, v, R.X, R.AX, nullptr, nullptr, nullptr, s->tpr);
         launch_coarse_restrict_block(st, K, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->d_l2g,
@@ -3421,8 +3423,8 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         s->opt_group = g;
     } else if (n == "spmv_tpr") {
         const int t = (int)value;
-        if (t != 0 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32)
-            return s->fail(S2L_ERR_BADARG, "spmv_tpr must be 0, 2, 4, 8, 16 or 32");
+        if (t != 0 && t != 1 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32)
+            return s->fail(S2L_ERR_BADARG, "spmv_tpr must be 0, 1, 2, 4, 8, 16 or 32");
         s->opt_tpr = t;
     } else if (n == "block_width") {
         const int bw = (int)value;
@@ -3639,8 +3641,8 @@ extern "C" int s2l_gpu_coarse_apply_noalloc(s2l_setup* s, const double* r, doubl
                            boolean, r, s->mmax, part);
     launch_coarse_reduce(st, s->nsub, s->d_subs, s->d_t_first, s->mmax, part, c);
     launch_dense_gemv(st, (int)s->n0, s->d_Einv, c, y);
-    launch_coarse_prolong(st, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, boolean, y, x0,
-                          plocal);
+    launch_coarse_prolong(st, s->ntiles, s->d_t_sub, s->d_t_row0, s->d_t_nrow, s->d_subs, s->d_V, s->mmax, boolean, y,
+                          x0, plocal);
     if (!boolean) launch_combine(st, s->n, s->d_cp_ptr, s->d_cp_pos, nullptr, plocal, nullptr, x0);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return s->fail(S2L_ERR_CUDA, std::string("coarse_apply_noalloc launch: ") + cudaGetErrorString(e));

@@ -379,10 +379,21 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     const int64_t wi = (int64_t)sid * S2L_SWEEP_WARPS + wid;
     const int64_t t1 = F.wtask[wi + 1];
     int64_t so = F.wslot[wi], eo = F.went[wi];
+    const int64_t e_end = F.went[wi + 1];  // the warp's entries are [went[wi], went[wi + 1])
     bool dead = false;
     for (int64_t t = F.wtask[wi]; t < t1; ++t) {
         const uint32_t h = F.thdr[t];
         const int C = (int)(h & 0xFFFFu), gl2 = (int)((h >> 16) & 7u), R = (int)((h >> 19) & 31u) + 1;
+        // the warp's entries are one contiguous stream: hint the first Q chunks after this task (the
+        // next tasks' loads) into L2 while this task waits on its ready flags
+        if (lane < Q) {
+            const int64_t e = eo + (int64_t)(C + lane) * 32;
+            if (e < e_end) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F.col + e));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e));
+                if (sizeof(Real) == 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e + 16));
+            }
+        }
         const int k = lane >> gl2;
         const int slot = k < R ? F.tslot[so + k] : -1;
         so += R;
@@ -523,6 +534,17 @@ __device__ __forceinline__ void warp_gather_dot(const Real* __restrict__ val, co
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = Real(0);
         int64_t e = e0 + lane;
+        for (; e + 96 < e1; e += 128) {  // four entries in flight per lane
+            const int c0 = col[e], c1 = col[e + 32], c2 = col[e + 64], c3 = col[e + 96];
+            const Real v0 = val[e], v1 = val[e + 32], v2 = val[e + 64], v3 = val[e + 96];
+            Real x0[K], x1[K], x2[K], x3[K];
+            load_k<Real, K>(x + (int64_t)c0 * K, x0);
+            load_k<Real, K>(x + (int64_t)c1 * K, x1);
+            load_k<Real, K>(x + (int64_t)c2 * K, x2);
+            load_k<Real, K>(x + (int64_t)c3 * K, x3);
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += (v0 * x0[r] + v1 * x1[r]) + (v2 * x2[r] + v3 * x3[r]);
+        }
         for (; e + 32 < e1; e += 64) {
             const int c0 = col[e], c1 = col[e + 32];
             const Real v0 = val[e], v1 = val[e + 32];
@@ -572,12 +594,16 @@ __global__ void __launch_bounds__(256) tail_rhs_kernel(const LocalSolveArgs<Real
 }
 
 // Dense tail: out(T+i) = sum_j Minv(i, j) in(T+j), j <= i (lower) or j >= i (upper); warp per row,
-// K columns (Minv is read once for all of them).
+// K columns (Minv is read once for all of them).  The row is streamed with 16-byte loads (VEC
+// entries per lane, two in flight per lane: 1 KB per warp), the few entries before the first
+// 16-byte boundary and after the last full vector one per lane.  Every column's sum runs in the same
+// order whatever K is.
 template <typename Real, bool LOWER, int K>
 __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Real> a, const Real* __restrict__ Minv,
                                                         const Real* __restrict__ vin, Real* __restrict__ vout,
                                                         int q0, int count)
 {
+    constexpr int VEC = 16 / (int)sizeof(Real);
     const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (q >= q0 + count) return;
@@ -588,38 +614,45 @@ __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Rea
     const Real* row = Minv + sd.d_off + (int64_t)i * s;
     const int j0 = LOWER ? 0 : i, j1 = LOWER ? i + 1 : s;
     const Real* v = vin + base * K;
+    Real acc[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) acc[r] = Real(0);
+    auto fma_entry = [&](Real m, int j) {
+        Real x[K];
+        load_k<Real, K>(v + (int64_t)j * K, x);
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] += m * x[r];
+    };
+    // first 16-byte boundary at or after j0 (the allocation is 256-byte aligned)
+    const int mis = (int)((reinterpret_cast<uintptr_t>(row + j0) & 15) / sizeof(Real));
+    const int ja = mis ? min(j1, j0 + (VEC - mis)) : j0;
+    if (j0 + lane < ja) fma_entry(row[j0 + lane], j0 + lane);
+    const int nvec = (j1 - ja) / VEC;  // full 16-byte vectors
+    const uint4* rv = reinterpret_cast<const uint4*>(row + ja);
+    int t = lane;
+    for (; t + 32 < nvec; t += 64) {
+        const uint4 w0 = __ldg(rv + t), w1 = __ldg(rv + t + 32);
+        Real m0[VEC], m1[VEC];
+        __builtin_memcpy(m0, &w0, 16);
+        __builtin_memcpy(m1, &w1, 16);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) fma_entry(m0[u], ja + t * VEC + u);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) fma_entry(m1[u], ja + (t + 32) * VEC + u);
+    }
+    if (t < nvec) {
+        const uint4 w0 = __ldg(rv + t);
+        Real m0[VEC];
+        __builtin_memcpy(m0, &w0, 16);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) fma_entry(m0[u], ja + t * VEC + u);
+    }
+    const int jt = ja + nvec * VEC;  // fewer than VEC entries left
+    if (jt + lane < j1) fma_entry(row[jt + lane], jt + lane);
     if (K == 1) {
-        Real a0 = Real(0), a1 = Real(0), a2 = Real(0), a3 = Real(0);
-        int j = j0 + lane;
-        for (; j + 96 < j1; j += 128) {
-            a0 += row[j] * v[j];
-            a1 += row[j + 32] * v[j + 32];
-            a2 += row[j + 64] * v[j + 64];
-            a3 += row[j + 96] * v[j + 96];
-        }
-        for (; j < j1; j += 32) a0 += row[j] * v[j];
-        const Real acc = warp_sum((a0 + a1) + (a2 + a3));
-        if (lane == 0) vout[base + i] = acc;
+        const Real sum = warp_sum(acc[0]);
+        if (lane == 0) vout[base + i] = sum;
     } else {
-        Real acc[K];
-#pragma unroll
-        for (int r = 0; r < K; ++r) acc[r] = Real(0);
-        int j = j0 + lane;
-        for (; j + 32 < j1; j += 64) {
-            const Real m0 = row[j], m1 = row[j + 32];
-            Real v0[K], v1[K];
-            load_k<Real, K>(v + (int64_t)j * K, v0);
-            load_k<Real, K>(v + (int64_t)(j + 32) * K, v1);
-#pragma unroll
-            for (int r = 0; r < K; ++r) acc[r] += m0 * v0[r] + m1 * v1[r];
-        }
-        if (j < j1) {
-            const Real m0 = row[j];
-            Real v0[K];
-            load_k<Real, K>(v + (int64_t)j * K, v0);
-#pragma unroll
-            for (int r = 0; r < K; ++r) acc[r] += m0 * v0[r];
-        }
 #pragma unroll
         for (int r = 0; r < K; ++r) acc[r] = warp_allsum(acc[r]);  // lane r writes column r
         if (lane < K) vout[(base + i) * K + lane] = pick<Real, K>(acc, lane);
@@ -659,42 +692,6 @@ __global__ void combine_kernel(int64_t n, const int64_t* __restrict__ cp_ptr, co
 }
 
 // ------------------------------------------------------------------------------ coarse space (K4-K6)
-// c_i = V_i^T r per 256-row tile of one subdomain: partials[tile * mmax + c].
-__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_kernel(const int32_t* __restrict__ t_sub,
-                                                                        const int32_t* __restrict__ t_row0,
-                                                                        const int32_t* __restrict__ t_nrow,
-                                                                        const DevSub* __restrict__ subs,
-                                                                        const double* __restrict__ V,
-                                                                        const int32_t* __restrict__ l2g,
-                                                                        int boolean_pou, const double* __restrict__ r,
-                                                                        int mmax, double* __restrict__ partials)
-{
-    __shared__ double red[S2L_TILE_ROWS / 32][S2L_MAX_RED_COLS];
-    const int tile = blockIdx.x;
-    const DevSub sd = subs[t_sub[tile]];
-    const int m = sd.m, nr = t_nrow[tile];
-    const int l = t_row0[tile] + threadIdx.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool act = threadIdx.x < nr;
-    double rv = 0.0;
-    const double* vr = V;
-    if (act) {
-        rv = boolean_pou ? r[sd.begin + l] : r[l2g[sd.loc_off + l]];
-        vr = V + sd.v_off + (int64_t)l * m;
-    }
-    for (int c = 0; c < m; ++c) {
-        const double p = warp_sum(act ? rv * vr[c] : 0.0);
-        if (lane == 0) red[warp][c] = p;
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < m; c += S2L_TILE_ROWS) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) s += red[w][c];
-        partials[(int64_t)tile * mmax + c] = s;
-    }
-}
-
 __global__ void coarse_reduce_kernel(const DevSub* __restrict__ subs, const int32_t* __restrict__ t_first, int mmax,
                                      const double* __restrict__ partials, double* __restrict__ cvec)
 {
@@ -719,31 +716,6 @@ __global__ void __launch_bounds__(256) dense_gemv_kernel(int n0, const double* _
     for (int c = lane; c < n0; c += 32) s += mr[c] * x[c];
     s = warp_sum(s);
     if (lane == 0) y[row] = s;
-}
-
-// x0 = V_i y_i on the owned rows (boolean PoU: direct global write) or on Omega_i (plocal, summed
-// over the copies afterwards).
-__global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_prolong_kernel(const int32_t* __restrict__ t_sub,
-                                                                       const int32_t* __restrict__ t_row0,
-                                                                       const int32_t* __restrict__ t_nrow,
-                                                                       const DevSub* __restrict__ subs,
-                                                                       const double* __restrict__ V, int boolean_pou,
-                                                                       const double* __restrict__ y,
-                                                                       double* __restrict__ out,
-                                                                       double* __restrict__ plocal)
-{
-    const int tile = blockIdx.x;
-    if ((int)threadIdx.x >= t_nrow[tile]) return;
-    const DevSub sd = subs[t_sub[tile]];
-    const int l = t_row0[tile] + threadIdx.x;
-    const double* vr = V + sd.v_off + (int64_t)l * sd.m;
-    const double* yc = y + sd.c_off;
-    double s = 0.0;
-    for (int c = 0; c < sd.m; ++c) s += vr[c] * yc[c];
-    if (boolean_pou)
-        out[sd.begin + l] = s;
-    else
-        plocal[sd.loc_off + l] = s;
 }
 
 // ------------------------------------------------------------------------------ K right-hand sides
@@ -797,6 +769,78 @@ __global__ void __launch_bounds__(S2L_BS_VEC) spmv_block_kernel(int64_t n, const
         for (int r = 0; r < K; ++r) {
             const double t = warp_sum(nrm[r]);
             if (wl == 0) sh[warp][r] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < K) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < S2L_BS_VEC / 32; ++w) t += sh[w][threadIdx.x];
+            partials[(int64_t)blockIdx.x * K + threadIdx.x] = t;
+        }
+    }
+}
+
+// Y = A X (or B - A X) for short rows, K columns (chunk mode, spmv_tpr 1).  A warp takes 32
+// consecutive rows; their entries are contiguous in the CSR arrays, so the warp loads them with
+// coalesced loads, multiplies each by the gathered row of X and leaves the products in shared
+// memory (pieces of `cap` entries); lane j then adds row j's products in entry order.  With
+// partials, also sum(Y(:, r)^2) per block and column.
+template <int K>
+__global__ void __launch_bounds__(S2L_BS_VEC) spmv_chunk_kernel(int64_t n, const int32_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ ci,
+                                                                const double* __restrict__ v,
+                                                                const double* __restrict__ X, double* __restrict__ Y,
+                                                                const double* __restrict__ B,
+                                                                double* __restrict__ partials)
+{
+    constexpr int CAP = 512 / K;  // entries of a piece: 4 KB of products per warp
+    __shared__ double prod[S2L_BS_VEC / 32][CAP * K];
+    __shared__ double sh[S2L_BS_VEC / 32][K];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* wp = prod[warp];
+    double nrm[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) nrm[r] = 0.0;
+    const int64_t nchunks = (n + 31) / 32;
+    for (int64_t ch = (int64_t)blockIdx.x * (S2L_BS_VEC / 32) + warp; ch < nchunks;
+         ch += (int64_t)gridDim.x * (S2L_BS_VEC / 32)) {
+        const int64_t r0 = ch * 32, row = r0 + lane;
+        const int64_t rend = r0 + 32 < n ? r0 + 32 : n;
+        const int e_lo = rp[r0], e_hi = rp[rend];
+        const int my0 = row < n ? rp[row] : e_hi, my1 = row < n ? rp[row + 1] : e_hi;
+        double acc[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = 0.0;
+        for (int base = e_lo; base < e_hi; base += CAP) {
+            const int cnt = e_hi - base < CAP ? e_hi - base : CAP;
+            for (int e = lane; e < cnt; e += 32) {
+                const double a = v[base + e];
+                double x[K];
+                load_k<double, K>(X + (int64_t)ci[base + e] * K, x);
+#pragma unroll
+                for (int r = 0; r < K; ++r) wp[e * K + r] = a * x[r];
+            }
+            __syncwarp();
+            const int s0 = (my0 > base ? my0 : base) - base, s1 = (my1 < base + cnt ? my1 : base + cnt) - base;
+            for (int e = s0; e < s1; ++e)
+#pragma unroll
+                for (int r = 0; r < K; ++r) acc[r] += wp[e * K + r];
+            __syncwarp();
+        }
+        if (row < n) {
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                const double y = B ? B[row * K + r] - acc[r] : acc[r];
+                Y[row * K + r] = y;
+                nrm[r] += y * y;
+            }
+        }
+    }
+    if (partials) {
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const double t = warp_sum(nrm[r]);
+            if (lane == 0) sh[warp][r] = t;
         }
         __syncthreads();
         if (threadIdx.x < K) {
@@ -1008,8 +1052,10 @@ __global__ void combine_block_kernel(int64_t n, const int64_t* __restrict__ cp_p
 }
 
 // c_i(c, r) = V_i(:, c)^T R(:, r) per 256-row tile of one subdomain: partials[(tile * mmax + c) * K + r].
-// Every warp sums its 32 rows for all (c, r) into shared memory (mmax * K values per warp, dynamic),
-// then the CTA adds the warps' sums: one barrier per tile.
+// Warp w takes the tile rows w, w + 8, ...; lane c keeps the sums of coarse column c (32 columns at a
+// time) for the K right-hand sides, so a row of V (m contiguous doubles) is one coalesced load and
+// the K values of R at the row one broadcast load; no shuffle per row.  The warps' sums are added in
+// warp order after one barrier.
 template <int K>
 __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
     const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
@@ -1019,27 +1065,28 @@ __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
     extern __shared__ double red[];  // [S2L_TILE_ROWS / 32][mmax * K]
     const int tile = blockIdx.x;
     const DevSub sd = subs[t_sub[tile]];
-    const int m = sd.m, nr = t_nrow[tile];
-    const int l = t_row0[tile] + threadIdx.x;
+    const int m = sd.m, nr = t_nrow[tile], row0 = t_row0[tile];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool act = threadIdx.x < nr;
-    double rv[K];
-    const double* vr = V;
-#pragma unroll
-    for (int r = 0; r < K; ++r) rv[r] = 0.0;
-    if (act) {
-        const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
-        load_k<double, K>(R + g * K, rv);
-        vr = V + sd.v_off + (int64_t)l * m;
-    }
+    const double* Vs = V + sd.v_off;
     double* wred = red + (size_t)warp * mmax * K;
-    for (int c = 0; c < m; ++c) {
-        const double vc = act ? vr[c] : 0.0;
+    for (int c0 = 0; c0 < m; c0 += 32) {
+        const int c = c0 + lane;
+        double acc[K];
 #pragma unroll
-        for (int r = 0; r < K; ++r) {
-            const double p = warp_sum(vc * rv[r]);
-            if (lane == 0) wred[c * K + r] = p;
+        for (int r = 0; r < K; ++r) acc[r] = 0.0;
+#pragma unroll 4
+        for (int i = warp; i < nr; i += S2L_TILE_ROWS / 32) {
+            const int l = row0 + i;
+            const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
+            double rv[K];
+            load_k<double, K>(R + g * K, rv);
+            const double vc = c < m ? Vs[(int64_t)l * m + c] : 0.0;
+#pragma unroll
+            for (int r = 0; r < K; ++r) acc[r] += vc * rv[r];
         }
+        if (c < m)
+#pragma unroll
+            for (int r = 0; r < K; ++r) wred[c * K + r] = acc[r];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < m * K; e += S2L_TILE_ROWS) {
@@ -1087,23 +1134,44 @@ __global__ void __launch_bounds__(256) dense_gemm_kernel(int n0, const double* _
     }
 }
 
-// X0 = V_i Y_i on the owned rows (boolean PoU) or on Omega_i (plocal), K columns
+// X0 = V_i Y_i on the owned rows (boolean PoU) or on Omega_i (plocal), K columns.  With `staged`,
+// the tile's rows of V (nr x m contiguous doubles) are first copied to shared memory with coalesced
+// loads (rows padded to m + 1 doubles) and Y_i next to them; a thread then sums its row there.
 template <int K>
 __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_prolong_block_kernel(
     const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
     const DevSub* __restrict__ subs, const double* __restrict__ V, int boolean_pou, const double* __restrict__ Y,
-    double* __restrict__ out, double* __restrict__ plocal)
+    double* __restrict__ out, double* __restrict__ plocal, int staged)
 {
+    extern __shared__ double sm[];
     const int tile = blockIdx.x;
-    if ((int)threadIdx.x >= t_nrow[tile]) return;
     const DevSub sd = subs[t_sub[tile]];
-    const int l = t_row0[tile] + threadIdx.x;
-    const double* vr = V + sd.v_off + (int64_t)l * sd.m;
-    const double* yc = Y + sd.c_off * K;
+    const int m = sd.m, nr = t_nrow[tile], row0 = t_row0[tile];
+    const double* vr;
+    const double* yc;
+    if (staged) {
+        const int ld = m + 1;
+        double* vs = sm;
+        double* ys = sm + (size_t)S2L_TILE_ROWS * ld;
+        const double* src = V + sd.v_off + (int64_t)row0 * m;
+        for (int e = threadIdx.x; e < nr * m; e += S2L_TILE_ROWS) {
+            const int l = e / m;
+            vs[l * ld + (e - l * m)] = src[e];
+        }
+        for (int e = threadIdx.x; e < m * K; e += S2L_TILE_ROWS) ys[e] = Y[sd.c_off * K + e];
+        __syncthreads();
+        vr = vs + (size_t)threadIdx.x * ld;
+        yc = ys;
+    } else {
+        vr = V + sd.v_off + (int64_t)(row0 + (int)threadIdx.x) * m;
+        yc = Y + sd.c_off * K;
+    }
+    if ((int)threadIdx.x >= nr) return;
+    const int l = row0 + threadIdx.x;
     double s[K];
 #pragma unroll
     for (int r = 0; r < K; ++r) s[r] = 0.0;
-    for (int c = 0; c < sd.m; ++c) {
+    for (int c = 0; c < m; ++c) {
         const double v = vr[c];
 #pragma unroll
         for (int r = 0; r < K; ++r) s[r] += v * yc[c * K + r];
@@ -1129,6 +1197,7 @@ void launch_spmv(cudaStream_t st, int64_t n, const int32_t* rp, const int32_t* c
     // lane group per row
     const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
     switch (tpr) {
+    case 1: spmv_chunk_kernel<1><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 2: spmv_kernel<2><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 4: spmv_kernel<4><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
     case 16: spmv_kernel<16><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, x, y, b, partials); break;
@@ -1187,7 +1256,9 @@ void launch_spmv_block(cudaStream_t st, int64_t n, int K, const int32_t* rp, con
                        const double* X, double* Y, const double* B, double* partials, double* red_out, int tpr)
 {
     const int grid = partials ? S2L_NB_RED : grid_for(n * tpr, S2L_BS_VEC, 1 << 20);
-    if (tpr == 2) {
+    if (tpr == 1) {
+        S2L_KSWITCH(K, (spmv_chunk_kernel<KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
+    } else if (tpr == 2) {
         S2L_KSWITCH(K, (spmv_block_kernel<2, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
     } else if (tpr == 4) {
         S2L_KSWITCH(K, (spmv_block_kernel<4, KK><<<grid, S2L_BS_VEC, 0, st>>>(n, rp, ci, v, X, Y, B, partials)));
@@ -1271,9 +1342,9 @@ void launch_combine_block(cudaStream_t st, int64_t n, int K, const int64_t* cp_p
                                                                                                 ylocal, base, out)));
 }
 
-void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                                  const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
-                                  int boolean_pou, const double* R, int mmax, double* partials)
+static void restrict_tiles(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                           const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                           int boolean_pou, const double* R, int mmax, double* partials)
 {
     if (ntiles <= 0) return;
     const size_t smem = (size_t)(S2L_TILE_ROWS / 32) * mmax * K * sizeof(double);  // <= 131 KB (mmax <= 128, K <= 16)
@@ -1281,6 +1352,13 @@ void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int3
                                          (int)((size_t)(S2L_TILE_ROWS / 32) * S2L_MAX_RED_COLS * KK * sizeof(double))),
                     coarse_restrict_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, smem, st>>>(
                         t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials)));
+}
+
+void launch_coarse_restrict_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                  const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                                  int boolean_pou, const double* R, int mmax, double* partials)
+{
+    restrict_tiles(st, K, ntiles, t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials);
 }
 
 void launch_coarse_reduce_block(cudaStream_t st, int K, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,
@@ -1295,14 +1373,41 @@ void launch_dense_gemm(cudaStream_t st, int K, int n0, const double* M, const do
     S2L_KSWITCH(K, (dense_gemm_kernel<KK><<<(n0 + 7) / 8, 256, 0, st>>>(n0, M, X, Y)));
 }
 
-void launch_coarse_prolong_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
-                                 const double* Y, double* out, double* plocal)
+static void prolong_tiles(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                          const int32_t* t_nrow, const DevSub* subs, const double* V, int mmax, int boolean_pou,
+                          const double* Y, double* out, double* plocal)
 {
     if (ntiles <= 0) return;
-    S2L_KSWITCH(K, (coarse_prolong_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V,
-                                                                                     boolean_pou, Y, out, plocal)));
+    // staged through shared memory when a tile's padded rows and Y_i fit (mmax up to about 100)
+    const size_t smem = ((size_t)S2L_TILE_ROWS * (mmax + 1) + (size_t)mmax * K) * sizeof(double);
+    const int staged = smem <= 200 * 1024 ? 1 : 0;
+    S2L_KSWITCH(K, (cudaFuncSetAttribute(coarse_prolong_block_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024),
+                    coarse_prolong_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, staged ? smem : 0, st>>>(
+                        t_sub, t_row0, t_nrow, subs, V, boolean_pou, Y, out, plocal, staged)));
 }
+
+void launch_coarse_prolong_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int mmax, int boolean_pou,
+                                 const double* Y, double* out, double* plocal)
+{
+    prolong_tiles(st, K, ntiles, t_sub, t_row0, t_nrow, subs, V, mmax, boolean_pou, Y, out, plocal);
+}
+
+void launch_coarse_restrict(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                            const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
+                            int boolean_pou, const double* r, int mmax, double* partials)
+{
+    restrict_tiles(st, 1, ntiles, t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, r, mmax, partials);
+}
+
+void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
+                           const int32_t* t_nrow, const DevSub* subs, const double* V, int mmax, int boolean_pou,
+                           const double* y, double* out, double* plocal)
+{
+    prolong_tiles(st, 1, ntiles, t_sub, t_row0, t_nrow, subs, V, mmax, boolean_pou, y, out, plocal);
+}
+
 #undef S2L_KSWITCH
 
 void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
@@ -1422,14 +1527,6 @@ void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int
     combine_kernel<<<grid_for(n, 256, 4 * S2L_NB_RED), 256, 0, st>>>(n, cp_ptr, cp_pos, cp_w, ylocal, base, out);
 }
 
-void launch_coarse_restrict(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                            const int32_t* t_nrow, const DevSub* subs, const double* V, const int32_t* l2g,
-                            int boolean_pou, const double* r, int mmax, double* partials)
-{
-    coarse_restrict_kernel<<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, r,
-                                                             mmax, partials);
-}
-
 void launch_coarse_reduce(cudaStream_t st, int nsub, const DevSub* subs, const int32_t* t_first, int mmax,
                           const double* partials, double* c)
 {
@@ -1439,14 +1536,6 @@ void launch_coarse_reduce(cudaStream_t st, int nsub, const DevSub* subs, const i
 void launch_dense_gemv(cudaStream_t st, int n0, const double* M, const double* x, double* y)
 {
     dense_gemv_kernel<<<(n0 + 7) / 8, 256, 0, st>>>(n0, M, x, y);
-}
-
-void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                           const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
-                           const double* y, double* out, double* plocal)
-{
-    coarse_prolong_kernel<<<ntiles, S2L_TILE_ROWS, 0, st>>>(t_sub, t_row0, t_nrow, subs, V, boolean_pou, y, out,
-                                                            plocal);
 }
 
 }  // namespace s2l

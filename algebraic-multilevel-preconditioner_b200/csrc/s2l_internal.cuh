@@ -202,7 +202,7 @@ void launch_coarse_reduce_block(cudaStream_t st, int K, int nsub, const DevSub* 
                                 const double* partials, double* cvec);
 void launch_dense_gemm(cudaStream_t st, int K, int n0, const double* M, const double* X, double* Y);
 void launch_coarse_prolong_block(cudaStream_t st, int K, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
+                                 const int32_t* t_nrow, const DevSub* subs, const double* V, int mmax, int boolean_pou,
                                  const double* Y, double* out, double* plocal);
 // out[0] = sum |a - alpha c| (c may be nullptr), out[1] = sum a
 void launch_l1(cudaStream_t st, int64_t n, const double* a, double alpha, const double* c, double* partials,
@@ -234,7 +234,7 @@ void launch_coarse_reduce(cudaStream_t st, int nsub, const DevSub* subs, const i
                           const double* partials, double* c);
 void launch_dense_gemv(cudaStream_t st, int n0, const double* M, const double* x, double* y);
 void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, const int32_t* t_row0,
-                           const int32_t* t_nrow, const DevSub* subs, const double* V, int boolean_pou,
+                           const int32_t* t_nrow, const DevSub* subs, const double* V, int mmax, int boolean_pou,
                            const double* y, double* out, double* plocal);
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 

@@ -52,6 +52,12 @@ for _p in (REPO, PKG):
         sys.path.insert(0, _p)
 
 METRIC = "solve time to FP64 residual 1e-8 (mixed/batched vs plain FP64 GPU); p50/p99 latency"
+_T0 = time.time()
+
+
+def log(msg: str) -> None:
+    """Progress on stderr (the JSON line is the only stdout)."""
+    print(f"[bench {time.time() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "s2l_ref")
 
 
@@ -80,6 +86,8 @@ def parse(argv=None):
     ap.add_argument("--amg", type=int, default=1, help="AMG form: AMG local solvers on the main matrix (0 = off)")
     ap.add_argument("--serve-mix", type=int, default=2000, help="serving-mix form: requests over 40 cases (0 = off)")
     ap.add_argument("--serve-mix-rate", type=float, default=50.0)
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="tune the mixed setup's device layout (s2l_b200.autotune) before the timed forms (0 = off)")
     ap.add_argument("--parity", type=int, default=1,
                     help="the CPU-baseline leg also runs the drop-in parity check on the main workload and c1 (0 = off)")
     return ap.parse_args(argv)
@@ -413,6 +421,7 @@ def run_ours(a):
     t0 = time.time()
     st = reps.rank0_first(lambda: W.build(wl)) if world > 1 else W.build(wl)
     setup_s = time.time() - t0
+    log(f"main workload host setup {setup_s:.1f} s (n = {st.n})")
     # ---- device (no CUDA call before the setup's process pool is done)
     import torch
     from s2l_b200 import capi
@@ -422,8 +431,17 @@ def run_ours(a):
     ctx = capi.Context(local)
     st32 = with_factor_precision(st, "single")
     layout = {kv.split("=")[0]: float(kv.split("=")[1]) for kv in a.opt}
+    tuning = None
+    if a.autotune:
+        # the mixed setup's layout chosen by timing candidates on the device (4-column blocks, the
+        # width of the headline's blocks); the FP64 setup takes the same options
+        from s2l_b200 import autotune
+        g32, tuning = autotune.tune(ctx, st32, k=4, reps=3, base=layout)
+        layout = dict(layout, **tuning["chosen"])
+    else:
+        g32 = capi.GpuSetup(ctx, st32, options=layout)
     g64 = capi.GpuSetup(ctx, st, options=layout)
-    g32 = capi.GpuSetup(ctx, st32, options=layout)
+    log(f"device setups ready (layout {layout})")
     stream = torch.cuda.current_stream(dev)
     for g in (g64, g32):
         g.set_stream(stream.cuda_stream)
@@ -441,6 +459,7 @@ def run_ours(a):
     mixed, xm = single_form(tm, g32, b_dev, x_dev, kw32, x_ref=x64)
     mixed["true_rel_residual_host_check"] = float(np.linalg.norm(st.b - st.A @ xm) / np.linalg.norm(st.b))
 
+    log(f"plain {plain['ms_per_solve']:.2f} ms, mixed {mixed['ms_per_solve']:.2f} ms per solve")
     # ---- blocks of k right-hand sides (the first is the workload's b), errors against FP64
     kh = a.head_k
     rng = np.random.default_rng(4321)
@@ -464,6 +483,7 @@ def run_ours(a):
             rf = prof
         del Bk, Xk
 
+    log(f"blocks done: head {head['ms_per_block']:.2f} ms per {kh}-column step")
     # ---- end to end through the C ABI with pinned host buffers (headline block form): each step
     # copies its k right-hand sides and initial guesses in and its k solutions out
     b_pin = torch.empty((kh, n), dtype=torch.float64, pin_memory=True)
@@ -484,6 +504,7 @@ def run_ours(a):
         serving = serve_form(local, st32, kw32, a.serve, a.serve_rate, bpool, X64[:16])
         serving["speedup_vs_plain_fp64_per_solve"] = plain["ms_per_solve"] / serving["ms_per_solve"]
 
+    log(f"serving done: {serving and round(serving['solves_per_s'], 1)} solves/s")
     # ---- AMG local solvers (the reference's --local-approx amg) on the same matrix and basis
     amg_form = amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64) if a.amg else None
 
@@ -527,10 +548,15 @@ def run_ours(a):
     del b_dev, x_dev
 
     # ---- the other configurations (each builds, times and frees its own setups)
+    log("main workload done")
     c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if a.overlap2 and a.overlap != 2 else None
+    log("c2 overlap 2 done")
     sequence = sequence_form(a, tm, ctx, stream, dev) if a.seq > 0 else None
+    log("sequence done")
     c3 = c3_form(a, tm, ctx, stream, dev) if a.c3 > 0 else None
+    log("c3 done")
     serving_mix = serve_mix(a, local) if a.serve_mix > 0 and world == 1 else None
+    log("serving mix done")
 
     out = {
         "metric": METRIC,
@@ -556,6 +582,7 @@ def run_ours(a):
             "l2": "inputs larger than L2 (local factors %.1f GB per form)" % (mixed["local_solve_bytes"] / 1e9),
             "setup_s": round(setup_s, 1),
             "layout": layout_stats,
+            "autotune": tuning,
         },
         "forms": {
             "block_mixed": block,
@@ -598,6 +625,7 @@ def run_ours(a):
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cb, parity = cpu_baseline_leg(a, wl) if a.overlap == 1 else (None, None)
+        log("cpu baseline and parity done")
         if cb is not None:
             out["cpu_baseline"] = cb
             out["forms"]["plain_fp64"]["speedup_vs_reference_same_config"] = cb["ms_per_solve"] / plain["ms_per_solve"]
@@ -760,6 +788,7 @@ def sequence_form(a, tm, ctx, stream, dev):
             At = sp.csr_matrix((st.A.data if level == UpdateLevel.REBUILD else vals, st.A.indices, st.A.indptr),
                                shape=st.A.shape)
             chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(k))
+            log(f"sequence step {step}: {level.name.lower()} {t_update * 1e3:.0f} ms, solve {t_solve * 1e3:.0f} ms")
             steps.append({"step": step, "level": level.name.lower(), "update_ms": t_update * 1e3,
                           "solve_ms": t_solve * 1e3, "iterations_max": max(r["iterations"] for r in rq),
                           "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
@@ -788,22 +817,23 @@ def serve_mix(a, device: int) -> dict:
     from s2l_b200 import workloads as W
     from s2l_b200.serving import Engine
     cases = []
-    for nx in (100, 200, 400, 700, 1000, 1400):
-        for nsub in (8, 32):
-            cases.append(("poisson2d", W.poisson2d(nx, nsub)))
+    # 2D Poisson n = 1e4 - 4e6, bubbly pressure n = 1.4e4 - 1e6, convection-diffusion n = 1.4e4 - 1e6
+    for nx, nsub in ((100, 8), (150, 8), (200, 8), (300, 8), (400, 16), (500, 16), (700, 16), (850, 32), (1000, 32),
+                     (1200, 32), (1500, 64), (2000, 64)):
+        cases.append(("poisson2d", W.poisson2d(nx, nsub)))
     for nx, nsub in ((24, 8), (28, 8), (32, 8), (32, 16), (36, 16), (40, 16), (40, 32), (44, 16), (48, 16), (48, 32),
                      (56, 32), (56, 64), (64, 32), (64, 64), (72, 64), (80, 64), (90, 64), (100, 64)):
         w = W.bubbles3d(nx, nsub, nbubbles=max(4, (nx * nx * nx) // 5000), overlap=1)
         cases.append(("bubbles3d", w))
-    for nx in (24, 32, 48, 64, 80):
-        for nsub in (8, 32):
-            cases.append(("convdiff3d", W.convdiff3d(nx, nsub)))
+    for nx, nsub in ((24, 8), (32, 8), (40, 16), (48, 16), (56, 32), (64, 32), (72, 64), (80, 64), (90, 64), (100, 128)):
+        cases.append(("convdiff3d", W.convdiff3d(nx, nsub)))
     assert len(cases) == 40
     for q, (_, w) in enumerate(cases):
         w.seed = 1000 + q
     t0 = time.time()
     built = [W.build(w) for _, w in cases]
     setup_s = time.time() - t0
+    log(f"serving mix: 40 host setups in {setup_s:.1f} s")
     eng = Engine(device, hbm_budget=150 << 30, workers=4)
     kws = []
     for (fam, w), st in zip(cases, built):

@@ -182,8 +182,9 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
  *   "sweep_group" (0 = 32, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
  *   entries get G lanes, 32 / G rows of one dependency level share a warp);
- *   "spmv_tpr" (0 = about four entries per lane from the mean row length, 2, 4, 8, 16 or 32): lanes
- *   per row of the products with A;
+ *   "spmv_tpr" (0 = automatic, 1, 2, 4, 8, 16 or 32): lanes per row of the products with A; 1 is
+ *   chunk mode (a warp per 32 consecutive rows, their entries loaded together; automatic for rows of
+ *   up to 16 entries on average), otherwise about four entries per lane from the mean row length;
  *   "block_width" (0 = automatic, 1, 2, 4, 8 or 16): the most right-hand sides s2l_gpu_gmres_block
  *   puts in one block; larger k run as several blocks at once (automatic: the widest block whose
  *   sparse-sweep CTAs fit the SMs in one wave);

@@ -103,6 +103,11 @@ int main(int argc, char** argv)
         MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
         MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
         const double xdiff = std::sqrt(gn / gd);
+        // residual histories (||r|| / ||b|| after every application of M^-1), common prefix
+        double hdiff = 0.0;
+        const size_t nh = std::min(r1.history.size(), r2.history.size());
+        for (size_t i = 0; i < nh; ++i)
+            hdiff = std::max(hdiff, std::abs(r1.history[i] - r2.history[i]) / std::max(std::abs(r1.history[i]), 1e-300));
         const bool single = cfg.local_precision == "single";
         const double tol = single ? 1e-5 : 1e-12;
         const bool of = cfg.stop_norm == "openfoam";
@@ -120,6 +125,7 @@ int main(int argc, char** argv)
               << ", \"gpu_true_rel_residual\": " << r2.true_rel_residual << ", \"ref_true_rel_residual\": "
               << r1.true_rel_residual << ", \"gpu_final_residual_of\": " << r2.final_residual_of
               << ", \"ref_final_residual_of\": " << r1.final_residual_of << ", \"x_rel_diff\": " << xdiff
+              << ", \"history_rel_diff\": " << hdiff
               << ", \"gpu_solver\": \"" << gk->name() << "\", \"update\": \"" << level_out
               << "\", \"ok\": " << (ok ? "true" : "false") << "}";
             std::cout << s.str() << std::endl;

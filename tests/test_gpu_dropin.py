@@ -59,10 +59,12 @@ CASES = {
 def test_full_size_configuration_matches_reference(case):
     """The parity targets at the benchmark sizes (oracle.reference_runs.FULL_SIZE: c1, and c2 at the
     reference's overlap of one layer): apply within 1e-12 of the reference's
-    TwoLevelSchwarz::apply, GMRES iterations within +-1, FP64 true residual <= 1.1 rtol."""
+    TwoLevelSchwarz::apply, GMRES iterations within +-1, residual histories within 1e-6 over their
+    common steps, FP64 true residual <= 1.1 rtol."""
     np_, args = FULL_SIZE[case]
     res = dropin(np_, args)
     assert res["apply_rel_diff"] <= 1e-12, res
+    assert res["history_rel_diff"] <= 1e-6, res
     assert abs(res["ref_iterations"] - res["gpu_iterations"]) <= 1, res
     assert res["gpu_converged"] and res["gpu_true_rel_residual"] <= 1.1e-8, res
     assert res["ok"] and res["rc"] == 0, res

@@ -308,10 +308,10 @@ def test_forced_tail_single_precision(ctx, rng):
     g.close()
 
 
-@pytest.mark.parametrize("tpr", [2, 4, 8, 16, 32])
+@pytest.mark.parametrize("tpr", [1, 2, 4, 8, 16, 32])
 def test_spmv_lanes_per_row(ctx, rng, tpr):
-    """Every lanes-per-row choice of the product with A gives the CSR product (1e-14), for one
-    column and for a block of columns."""
+    """Every lanes-per-row choice of the product with A (1: chunk mode) gives the CSR product
+    (1e-14), for one column and for a block of columns."""
     from s2l_b200.capi import GpuSetup
     _, st = small_setup("convdiff3d")
     g = GpuSetup(ctx, st, options={"spmv_tpr": tpr})
