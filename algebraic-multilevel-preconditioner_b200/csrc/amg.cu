@@ -81,27 +81,35 @@ __global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restric
         for (int k = threadIdx.x; k < n; k += blockDim.x) x[o + k] = xs[k];
 }
 
-// y = M x (beta = 0) or y += M x (beta = 1), one thread per row
-__global__ void csr_mv_kernel(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                              const double* __restrict__ v, const double* __restrict__ x, double* __restrict__ y,
-                              int accumulate)
+// mode 0: y = M x, 1: y += M x, 2: y = f - M x.  A warp takes 32 consecutive rows: their entries
+// are contiguous, so the warp loads them with coalesced loads and leaves the products in shared
+// memory (pieces of 512 entries); lane j then adds row j's products in entry order.
+__global__ void __launch_bounds__(256) csr_chunk_kernel(int64_t n, const int64_t* __restrict__ rp,
+                                                        const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                                        const double* __restrict__ x, const double* __restrict__ f,
+                                                        double* __restrict__ y, int mode)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    constexpr int CAP = 512;
+    __shared__ double prod[8][CAP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* wp = prod[warp];
+    const int64_t nchunks = (n + 31) / 32;
+    for (int64_t ch = (int64_t)blockIdx.x * 8 + warp; ch < nchunks; ch += (int64_t)gridDim.x * 8) {
+        const int64_t r0 = ch * 32, row = r0 + lane;
+        const int64_t rend = r0 + 32 < n ? r0 + 32 : n;
+        const int64_t e_lo = rp[r0], e_hi = rp[rend];
+        const int64_t my0 = row < n ? rp[row] : e_hi, my1 = row < n ? rp[row + 1] : e_hi;
         double s = 0.0;
-        for (int64_t e = rp[i]; e < rp[i + 1]; ++e) s += v[e] * x[ci[e]];
-        y[i] = accumulate ? y[i] + s : s;
-    }
-}
-
-// t = f - A x
-__global__ void csr_residual_kernel(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                    const double* __restrict__ v, const double* __restrict__ f,
-                                    const double* __restrict__ x, double* __restrict__ t)
-{
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int64_t e = rp[i]; e < rp[i + 1]; ++e) s += v[e] * x[ci[e]];
-        t[i] = f[i] - s;
+        for (int64_t base = e_lo; base < e_hi; base += CAP) {
+            const int cnt = (int)(e_hi - base < CAP ? e_hi - base : CAP);
+            for (int e = lane; e < cnt; e += 32) wp[e] = v[base + e] * x[ci[base + e]];
+            __syncwarp();
+            const int64_t s0 = (my0 > base ? my0 : base) - base;
+            const int64_t s1 = (my1 < base + cnt ? my1 : base + cnt) - base;
+            for (int64_t e = s0; e < s1; ++e) s += wp[e];
+            __syncwarp();
+        }
+        if (row < n) y[row] = mode == 2 ? f[row] - s : (mode == 1 ? y[row] + s : s);
     }
 }
 
@@ -185,13 +193,13 @@ void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int
 void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
                    double* y, int accumulate)
 {
-    if (n > 0) csr_mv_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, y, accumulate);
+    if (n > 0) csr_chunk_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, nullptr, y, accumulate ? 1 : 0);
 }
 
 void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,
                          const double* f, const double* x, double* t)
 {
-    if (n > 0) csr_residual_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, f, x, t);
+    if (n > 0) csr_chunk_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, f, t, 2);
 }
 
 void launch_coarse_inverse(cudaStream_t st, int ncoarse, const int32_t* c_sub_off, const int32_t* c_n,

@@ -4477,11 +4477,13 @@ bool runner_takes(const Runner* R, const s2l_ticket* t)
     return R->s == t->s && R->m == t->opts.restart && R->flex == (t->opts.flexible != 0);
 }
 
-// slots of a runner on setup s with restart m: the setting of s2l_gpu_serve_batching, or the
-// setup's best block width, and never more than the coefficient buffers hold
+// slots of a runner on setup s with restart m: the setting of s2l_gpu_serve_batching, or
+// automatically the setup's best block width but at most 4 (a step costs about the same for 1 to 4
+// occupied columns, so a lightly loaded runner stays as fast as a single solve; more load starts
+// more runners), and never more than the coefficient buffers hold
 int runner_width(const s2l_serve* sv, s2l_setup* s, int m)
 {
-    int K = sv->slots > 0 ? sv->slots : block_width_best(s);
+    int K = sv->slots > 0 ? sv->slots : std::min(block_width_best(s), 4);
     int p = 1;
     while (p * 2 <= K && p * 2 <= S2L_MAX_RHS && (m + 1) * p * 2 <= S2L_MAX_BLOCK_COLS) p *= 2;
     return p;

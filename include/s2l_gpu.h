@@ -326,7 +326,7 @@ int s2l_gpu_serve_start(s2l_ctx* ctx, int workers);
 /* Continuous batching of the asynchronous GMRES solves (on by default, slots < 0: automatic).
  * A worker that takes a GMRES request (L2 stopping test, restart <= 63, exact local factors) runs
  * a block runner for its setup, restart length and variant: up to `slots` requests at once (the
- * automatic width is the setup's block width, s2l_gpu_setup_stat "block_width"), each in a column
+ * automatic width is the setup's block width, s2l_gpu_setup_stat "block_width", at most 4), each in a column
  * of one block, so the preconditioner, the product with A and the orthogonalization of every
  * Arnoldi step run once for all of them.  Each request keeps its own GMRES recurrence, restart
  * cycle and convergence test; a request that arrives while the runner works takes a free slot at

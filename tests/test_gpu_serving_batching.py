@@ -201,7 +201,7 @@ def test_runner_fits_the_hbm_budget_with_fewer_slots():
     assert width >= 4
     budget = d0 + (d2 - d0) // 3  # room for a block of about a third of the width
     ctx = capi.Context(0, hbm_budget=budget)
-    ctx.serve_start(1)
+    ctx.serve_start(1, batching=width)  # runners of the full width: they must halve to fit
     g = capi.GpuSetup(ctx, st)
     bs = _rhs(st.n, 5, 62)
     tickets = [g.submit(b, restart=w.restart, rtol=1e-9) for b in bs]
