@@ -25,16 +25,17 @@ int amg_grid(int64_t work, int bs)
 // the sum is reassociated, the serial sweep's rounding is not kept).  With SMEM the subdomain's x
 // (rows [o, o + n) of the level space) lives in shared memory for the whole sweep (the operator is
 // block-diagonal, so a row reads no other subdomain's x).
-template <bool SMEM, int G>
+template <bool SMEM, int G, typename Real>
 __global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                        const double* __restrict__ v, const double* __restrict__ f,
-                                                        double* x, const int32_t* __restrict__ sched,
+                                                        const Real* __restrict__ v, const Real* __restrict__ f,
+                                                        Real* x, const int32_t* __restrict__ sched,
                                                         const int64_t* __restrict__ wf_ptr,
                                                         const int32_t* __restrict__ sub_wf,
                                                         const int64_t* __restrict__ sub_off,
                                                         const int32_t* __restrict__ sub_n)
 {
-    extern __shared__ double xs[];
+    extern __shared__ __align__(16) unsigned char gs_smem[];
+    Real* xs = reinterpret_cast<Real*>(gs_smem);
     const int b = blockIdx.x;
     const int64_t o = sub_off[b];
     const int n = sub_n[b];
@@ -49,12 +50,12 @@ __global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restric
             const int64_t k = kb + grp;
             const bool valid = k < end;
             const int i = valid ? sched[k] : 0;
-            double part = 0.0, dpart = 0.0;
+            Real part = Real(0), dpart = Real(0);
             int has = 0;
             if (valid)
                 for (int64_t e = rp[i] + lg; e < rp[i + 1]; e += G) {
                     const int c = ci[e];
-                    const double a = v[e];
+                    const Real a = v[e];
                     if (c == i) {
                         dpart = a;
                         has = 1;
@@ -69,8 +70,8 @@ __global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restric
                 has += __shfl_xor_sync(0xffffffffu, has, m, G);
             }
             if (valid && lg == 0) {
-                const double D = has ? dpart : 1.0;
-                const double val = (1.0 / D) * (f[i] - part);
+                const Real D = has ? dpart : Real(1);
+                const Real val = (Real(1) / D) * (f[i] - part);
                 if (SMEM) xs[i - o] = val;
                 else x[i] = val;
             }
@@ -84,22 +85,23 @@ __global__ void __launch_bounds__(1024) gs_sweep_kernel(const int64_t* __restric
 // mode 0: y = M x, 1: y += M x, 2: y = f - M x.  A warp takes 32 consecutive rows: their entries
 // are contiguous, so the warp loads them with coalesced loads and leaves the products in shared
 // memory (pieces of 512 entries); lane j then adds row j's products in entry order.
+template <typename Real>
 __global__ void __launch_bounds__(256) csr_chunk_kernel(int64_t n, const int64_t* __restrict__ rp,
-                                                        const int32_t* __restrict__ ci, const double* __restrict__ v,
-                                                        const double* __restrict__ x, const double* __restrict__ f,
-                                                        double* __restrict__ y, int mode)
+                                                        const int32_t* __restrict__ ci, const Real* __restrict__ v,
+                                                        const Real* __restrict__ x, const Real* __restrict__ f,
+                                                        Real* __restrict__ y, int mode)
 {
     constexpr int CAP = 512;
-    __shared__ double prod[8][CAP];
+    __shared__ Real prod[8][CAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* wp = prod[warp];
+    Real* wp = prod[warp];
     const int64_t nchunks = (n + 31) / 32;
     for (int64_t ch = (int64_t)blockIdx.x * 8 + warp; ch < nchunks; ch += (int64_t)gridDim.x * 8) {
         const int64_t r0 = ch * 32, row = r0 + lane;
         const int64_t rend = r0 + 32 < n ? r0 + 32 : n;
         const int64_t e_lo = rp[r0], e_hi = rp[rend];
         const int64_t my0 = row < n ? rp[row] : e_hi, my1 = row < n ? rp[row + 1] : e_hi;
-        double s = 0.0;
+        Real s = Real(0);
         for (int64_t base = e_lo; base < e_hi; base += CAP) {
             const int cnt = (int)(e_hi - base < CAP ? e_hi - base : CAP);
             for (int e = lane; e < cnt; e += 32) wp[e] = v[base + e] * x[ci[base + e]];
@@ -115,45 +117,49 @@ __global__ void __launch_bounds__(256) csr_chunk_kernel(int64_t n, const int64_t
 
 // x_c = C^-1 f_c for every subdomain whose coarsest level is this one (one CTA each; C^-1 stored
 // column by column, so the threads of a row block read consecutive entries)
+template <typename Real>
 __global__ void coarse_inverse_kernel(const int32_t* __restrict__ c_sub_off, const int32_t* __restrict__ c_n,
-                                      const int64_t* __restrict__ c_inv_off, const double* __restrict__ Cinv,
-                                      const double* __restrict__ f, double* __restrict__ x)
+                                      const int64_t* __restrict__ c_inv_off, const Real* __restrict__ Cinv,
+                                      const Real* __restrict__ f, Real* __restrict__ x)
 {
     const int b = blockIdx.x;
     const int n = c_n[b];
     const int64_t o = c_sub_off[b];
-    const double* M = Cinv + c_inv_off[b];
+    const Real* M = Cinv + c_inv_off[b];
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        double s = 0.0;
+        Real s = Real(0);
         for (int c = 0; c < n; ++c) s += M[(int64_t)c * n + r] * f[o + c];  // M stored transposed
         x[o + r] = s;
     }
 }
 
 // level-0 right-hand side: f(p) = in(l2g(p)) (global input) or local_in(p - off) (one subdomain)
+template <typename Real>
 __global__ void amg_gather_kernel(int64_t n, const int32_t* __restrict__ l2g, const double* __restrict__ in,
                                   const double* __restrict__ local_in, int64_t lo, int64_t hi,
-                                  double* __restrict__ f)
+                                  Real* __restrict__ f)
 {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        if (local_in) f[p] = (p >= lo && p < hi) ? local_in[p - lo] : 0.0;
-        else f[p] = in[l2g[p]];
+        if (local_in) f[p] = (Real)((p >= lo && p < hi) ? local_in[p - lo] : 0.0);
+        else f[p] = (Real)in[l2g[p]];
     }
 }
 
 // outputs of the level-0 solution: owned rows to out (+ base), the local space, or one subdomain
-__global__ void amg_scatter_kernel(int64_t n, const int32_t* __restrict__ out_idx, const double* __restrict__ x,
+template <typename Real>
+__global__ void amg_scatter_kernel(int64_t n, const int32_t* __restrict__ out_idx, const Real* __restrict__ x,
                                    const double* __restrict__ base, double* __restrict__ out, int mode, int64_t lo,
                                    int64_t hi)
 {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const double xp = (double)x[p];
         if (mode == 0) {
             const int32_t g = out_idx[p];
-            if (g >= 0) out[g] = base ? x[p] + base[g] : x[p];
+            if (g >= 0) out[g] = base ? xp + base[g] : xp;
         } else if (mode == 1) {
-            out[p] = x[p];
+            out[p] = xp;
         } else if (p >= lo && p < hi) {
-            out[p - lo] = x[p];
+            out[p - lo] = xp;
         }
     }
 }
@@ -162,25 +168,29 @@ __global__ void amg_scatter_kernel(int64_t n, const int32_t* __restrict__ out_id
 
 namespace s2l {
 
-template <int G>
+template <int G, typename Real>
 void gs_launch(cudaStream_t st, int nsub_lvl, bool sm, size_t smem, const int64_t* rp, const int32_t* ci,
-               const double* v, const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr,
+               const Real* v, const Real* f, Real* x, const int32_t* sched, const int64_t* wf_ptr,
                const int32_t* sub_wf, const int64_t* sub_off, const int32_t* sub_n)
 {
     if (sm) {
-        cudaFuncSetAttribute(gs_sweep_kernel<true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S2L_GS_SMEM_CAP);
-        gs_sweep_kernel<true, G><<<nsub_lvl, 1024, smem, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n);
+        cudaFuncSetAttribute(gs_sweep_kernel<true, G, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)S2L_GS_SMEM_CAP);
+        gs_sweep_kernel<true, G, Real><<<nsub_lvl, 1024, smem, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off,
+                                                                   sub_n);
     } else {
-        gs_sweep_kernel<false, G><<<nsub_lvl, 1024, 0, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n);
+        gs_sweep_kernel<false, G, Real><<<nsub_lvl, 1024, 0, st>>>(rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off,
+                                                                 sub_n);
     }
 }
 
-void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
-                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
+template <typename Real>
+void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const Real* v, const Real* f,
+                     Real* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
                      const int64_t* sub_off, const int32_t* sub_n, int max_n, int lanes)
 {
     if (nsub_lvl <= 0) return;
-    const size_t smem = (size_t)max_n * sizeof(double);
+    const size_t smem = (size_t)max_n * sizeof(Real);
     const bool sm = smem <= S2L_GS_SMEM_CAP;
     switch (lanes) {
     case 4: gs_launch<4>(st, nsub_lvl, sm, smem, rp, ci, v, f, x, sched, wf_ptr, sub_wf, sub_off, sub_n); break;
@@ -190,34 +200,58 @@ void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int
     }
 }
 
-void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
-                   double* y, int accumulate)
+template <typename Real>
+void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const Real* v, const Real* x,
+                   Real* y, int accumulate)
 {
-    if (n > 0) csr_chunk_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, nullptr, y, accumulate ? 1 : 0);
+    if (n > 0)
+        csr_chunk_kernel<Real><<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, nullptr, y, accumulate ? 1 : 0);
 }
 
-void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,
-                         const double* f, const double* x, double* t)
+template <typename Real>
+void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const Real* v,
+                         const Real* f, const Real* x, Real* t)
 {
-    if (n > 0) csr_chunk_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, f, t, 2);
+    if (n > 0) csr_chunk_kernel<Real><<<amg_grid(n, 256), 256, 0, st>>>(n, rp, ci, v, x, f, t, 2);
 }
 
+template <typename Real>
 void launch_coarse_inverse(cudaStream_t st, int ncoarse, const int32_t* c_sub_off, const int32_t* c_n,
-                           const int64_t* c_inv_off, const double* Cinv, const double* f, double* x)
+                           const int64_t* c_inv_off, const Real* Cinv, const Real* f, Real* x)
 {
-    if (ncoarse > 0) coarse_inverse_kernel<<<ncoarse, 256, 0, st>>>(c_sub_off, c_n, c_inv_off, Cinv, f, x);
+    if (ncoarse > 0) coarse_inverse_kernel<Real><<<ncoarse, 256, 0, st>>>(c_sub_off, c_n, c_inv_off, Cinv, f, x);
 }
 
+template <typename Real>
 void launch_amg_gather(cudaStream_t st, int64_t n, const int32_t* l2g, const double* in, const double* local_in,
-                       int64_t lo, int64_t hi, double* f)
+                       int64_t lo, int64_t hi, Real* f)
 {
-    if (n > 0) amg_gather_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, l2g, in, local_in, lo, hi, f);
+    if (n > 0) amg_gather_kernel<Real><<<amg_grid(n, 256), 256, 0, st>>>(n, l2g, in, local_in, lo, hi, f);
 }
 
-void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const double* x, const double* base,
+template <typename Real>
+void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const Real* x, const double* base,
                         double* out, int mode, int64_t lo, int64_t hi)
 {
-    if (n > 0) amg_scatter_kernel<<<amg_grid(n, 256), 256, 0, st>>>(n, out_idx, x, base, out, mode, lo, hi);
+    if (n > 0) amg_scatter_kernel<Real><<<amg_grid(n, 256), 256, 0, st>>>(n, out_idx, x, base, out, mode, lo, hi);
 }
+
+#define S2L_AMG_INSTANTIATE(Real)                                                                                      \
+    template void launch_gs_sweep<Real>(cudaStream_t, int, const int64_t*, const int32_t*, const Real*, const Real*,   \
+                                        Real*, const int32_t*, const int64_t*, const int32_t*, const int64_t*,         \
+                                        const int32_t*, int, int);                                                     \
+    template void launch_csr_mv<Real>(cudaStream_t, int64_t, const int64_t*, const int32_t*, const Real*, const Real*, \
+                                      Real*, int);                                                                     \
+    template void launch_csr_residual<Real>(cudaStream_t, int64_t, const int64_t*, const int32_t*, const Real*,       \
+                                            const Real*, const Real*, Real*);                                          \
+    template void launch_coarse_inverse<Real>(cudaStream_t, int, const int32_t*, const int32_t*, const int64_t*,      \
+                                              const Real*, const Real*, Real*);                                        \
+    template void launch_amg_gather<Real>(cudaStream_t, int64_t, const int32_t*, const double*, const double*, int64_t, \
+                                          int64_t, Real*);                                                             \
+    template void launch_amg_scatter<Real>(cudaStream_t, int64_t, const int32_t*, const Real*, const double*, double*,  \
+                                           int, int64_t, int64_t);
+S2L_AMG_INSTANTIATE(double)
+S2L_AMG_INSTANTIATE(float)
+#undef S2L_AMG_INSTANTIATE
 
 }  // namespace s2l

@@ -22,32 +22,54 @@
 
 namespace {
 
-struct Csr {
+// Every step runs in the precision Real of the setup: double, or float for the reference's
+// --local-precision single (AMGCL's builtin<float> backend computes its whole setup in float).
+template <typename Real>
+struct CsrT {
     int64_t rows = 0, cols = 0;
     std::vector<int64_t> rp;
     std::vector<int32_t> ci;
-    std::vector<double> v;
+    std::vector<Real> v;
 };
+using Csr = CsrT<double>;
+
+template <typename Real, typename From>
+CsrT<Real> convert(const CsrT<From>& A)
+{
+    CsrT<Real> B;
+    B.rows = A.rows;
+    B.cols = A.cols;
+    B.rp = A.rp;
+    B.ci = A.ci;
+    B.v.assign(A.v.begin(), A.v.end());
+    return B;
+}
 
 constexpr int kUndef = -1, kRemoved = -2;
-constexpr double kTiny = 2.0 * std::numeric_limits<double>::epsilon();  // AMGCL detail::eps<double>(1)
+// AMGCL detail::eps<Real>(1): twice the machine epsilon of the precision
+template <typename Real>
+constexpr Real tiny()
+{
+    return Real(2) * std::numeric_limits<Real>::epsilon();
+}
 
 // C = A B (rows of A times B), accumulated in A's row order then B's, exact zeros dropped, columns
 // sorted
-Csr product(const Csr& A, const Csr& B)
+template <typename Real>
+CsrT<Real> product(const CsrT<Real>& A, const CsrT<Real>& B)
 {
-    Csr C;
+    CsrT<Real> C;
     C.rows = A.rows;
     C.cols = B.cols;
     C.rp.assign((size_t)A.rows + 1, 0);
-    std::vector<double> sums((size_t)B.cols, 0.0);
+    std::vector<Real> sums((size_t)B.cols, Real(0));
     std::vector<int64_t> mark((size_t)B.cols, -1);
     std::vector<int32_t> cols;
     for (int64_t i = 0; i < A.rows; ++i) {
         cols.clear();
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) {
             const int32_t k = A.ci[e];
-            const double a = A.v[e];
+            const Real a = A.v[e];
             for (int64_t f = B.rp[k]; f < B.rp[k + 1]; ++f) {
                 const int32_t j = B.ci[f];
                 sums[j] += a * B.v[f];
@@ -59,20 +81,21 @@ Csr product(const Csr& A, const Csr& B)
         }
         std::sort(cols.begin(), cols.end());
         for (int32_t j : cols) {
-            if (sums[j] != 0.0) {
+            if (sums[j] != Real(0)) {
                 C.ci.push_back(j);
                 C.v.push_back(sums[j]);
             }
-            sums[j] = 0.0;
+            sums[j] = Real(0);
         }
         C.rp[i + 1] = (int64_t)C.ci.size();
     }
     return C;
 }
 
-Csr transpose(const Csr& P)
+template <typename Real>
+CsrT<Real> transpose(const CsrT<Real>& P)
 {
-    Csr R;
+    CsrT<Real> R;
     R.rows = P.cols;
     R.cols = P.rows;
     R.rp.assign((size_t)P.cols + 1, 0);
@@ -92,11 +115,12 @@ Csr transpose(const Csr& P)
 
 // ---------------------------------------------------------------- smoothed aggregation
 // P of one level, false when no row has a strong connection
-bool sa_transfer(const Csr& A, float eps, Csr& P)
+template <typename Real>
+bool sa_transfer(const CsrT<Real>& A, float eps, CsrT<Real>& P)
 {
     const int64_t n = A.rows;
-    const double eps2 = (double)(eps * eps);  // the product of two floats, in float
-    std::vector<double> dia((size_t)n, 0.0);
+    const Real eps2 = (Real)(eps * eps);  // the product of two floats, in float
+    std::vector<Real> dia((size_t)n, Real(0));
     for (int64_t i = 0; i < n; ++i)
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e)
             if (A.ci[e] == i) dia[i] = A.v[e];
@@ -106,7 +130,7 @@ bool sa_transfer(const Csr& A, float eps, Csr& P)
         bool any = false;
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) {
             const int32_t c = A.ci[e];
-            const double v = A.v[e];
+            const Real v = A.v[e];
             strong[e] = c != i && (eps2 * dia[i]) * dia[c] < v * v;
             any = any || strong[e];
         }
@@ -142,25 +166,25 @@ bool sa_transfer(const Csr& A, float eps, Csr& P)
     count = used;
     // P(i, :) = sum over the strong and diagonal entries of row i, in order, of
     // ((1 - omega) on the diagonal, -omega a_ij / d_F(i) elsewhere) P0(j, :)
-    const double omega = 1.0 * (2.0 / 3.0);
-    P = Csr();
+    const Real omega = Real(1) * Real(2.0 / 3.0);
+    P = CsrT<Real>();
     P.rows = n;
     P.cols = count;
     P.rp.assign((size_t)n + 1, 0);
-    std::vector<std::pair<int32_t, double>> acc;
+    std::vector<std::pair<int32_t, Real>> acc;
     for (int64_t i = 0; i < n; ++i) {
-        double df = 0.0;  // filtered diagonal: the diagonal plus the weak entries
+        Real df = Real(0);  // filtered diagonal: the diagonal plus the weak entries
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e)
             if (!strong[e]) df += A.v[e];
-        const double scale = df != 0.0 ? -omega * (1.0 / df) : 0.0;
+        const Real scale = df != Real(0) ? -omega * (Real(1) / df) : Real(0);
         acc.clear();
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) {
             const int32_t c = A.ci[e];
             const bool diag = c == i;
             if (!(diag || strong[e]) || aid[c] < 0) continue;
-            const double val = diag ? 1.0 - omega : scale * A.v[e];
+            const Real val = diag ? Real(1) - omega : scale * A.v[e];
             const int32_t t = aid[c];
-            auto it = std::find_if(acc.begin(), acc.end(), [t](const std::pair<int32_t, double>& p) { return p.first == t; });
+            auto it = std::find_if(acc.begin(), acc.end(), [t](const std::pair<int32_t, Real>& p) { return p.first == t; });
             if (it == acc.end()) acc.emplace_back(t, val);
             else it->second = it->second + val;
         }
@@ -177,20 +201,22 @@ bool sa_transfer(const Csr& A, float eps, Csr& P)
 // ---------------------------------------------------------------- Ruge-Stuben
 enum : char { kU = 0, kF = 1, kC = 2 };
 
-bool rs_transfer(const Csr& A, Csr& P)
+template <typename Real>
+bool rs_transfer(const CsrT<Real>& A, CsrT<Real>& P)
 {
     const int64_t n = A.rows;
-    const double eps_str = (double)0.25f, eps_tr = (double)0.2f;
+    const Real eps_str = (Real)0.25f, eps_tr = (Real)0.2f;
+    const Real kTiny = tiny<Real>();
     std::vector<char> strong(A.ci.size(), 0), cf((size_t)n, kU);
     for (int64_t i = 0; i < n; ++i) {
-        double amin = 0.0;
+        Real amin = Real(0);
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e)
             if (A.ci[e] != i) amin = std::min(amin, A.v[e]);
         if (std::fabs(amin) < kTiny) {
             cf[i] = kF;
             continue;
         }
-        const double thr = amin * eps_str;
+        const Real thr = amin * eps_str;
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) strong[e] = A.ci[e] != i && A.v[e] < thr;
     }
     // transposed strength graph: for column c, the rows depending strongly on it, by row
@@ -273,18 +299,18 @@ bool rs_transfer(const Csr& A, Csr& P)
         if (cf[i] == kC) cidx[i] = nc++;
     if (nc == 0) return false;
     // direct interpolation with truncation
-    P = Csr();
+    P = CsrT<Real>();
     P.rows = n;
     P.cols = nc;
     P.rp.assign((size_t)n + 1, 0);
     for (int64_t i = 0; i < n; ++i) {
         if (cf[i] == kC) {
             P.ci.push_back(cidx[i]);
-            P.v.push_back(1.0);
+            P.v.push_back(Real(1));
             P.rp[i + 1] = (int64_t)P.ci.size();
             continue;
         }
-        double lo = 0.0, hi = 0.0;
+        Real lo = Real(0), hi = Real(0);
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e)
             if (strong[e] && cf[A.ci[e]] == kC) {
                 lo = std::min(lo, A.v[e]);
@@ -292,16 +318,16 @@ bool rs_transfer(const Csr& A, Csr& P)
             }
         lo *= eps_tr;
         hi *= eps_tr;
-        double dia = 0.0, a_num = 0.0, a_den = 0.0, b_num = 0.0, b_den = 0.0, d_neg = 0.0, d_pos = 0.0;
+        Real dia = 0, a_num = 0, a_den = 0, b_num = 0, b_den = 0, d_neg = 0, d_pos = 0;
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) {
             const int32_t c = A.ci[e];
-            const double v = A.v[e];
+            const Real v = A.v[e];
             if (c == i) {
                 dia = v;
                 continue;
             }
             const bool sc = strong[e] && cf[c] == kC;
-            if (v < 0.0) {
+            if (v < Real(0)) {
                 a_num += v;
                 if (sc) {
                     a_den += v;
@@ -315,19 +341,19 @@ bool rs_transfer(const Csr& A, Csr& P)
                 }
             }
         }
-        const double cf_neg = std::fabs(a_den - d_neg) > kTiny ? std::fabs(a_den) / std::fabs(a_den - d_neg) : 1.0;
-        const double cf_pos = std::fabs(b_den - d_pos) > kTiny ? std::fabs(b_den) / std::fabs(b_den - d_pos) : 1.0;
-        if (0.0 < b_num && std::fabs(b_den) < kTiny) dia += b_num;
-        const double alpha =
-            std::fabs(a_den) > kTiny ? -cf_neg * std::fabs(a_num) / (std::fabs(dia) * std::fabs(a_den)) : 0.0;
-        const double beta =
-            std::fabs(b_den) > kTiny ? -cf_pos * std::fabs(b_num) / (std::fabs(dia) * std::fabs(b_den)) : 0.0;
+        const Real cf_neg = std::fabs(a_den - d_neg) > kTiny ? std::fabs(a_den) / std::fabs(a_den - d_neg) : Real(1);
+        const Real cf_pos = std::fabs(b_den - d_pos) > kTiny ? std::fabs(b_den) / std::fabs(b_den - d_pos) : Real(1);
+        if (Real(0) < b_num && std::fabs(b_den) < kTiny) dia += b_num;
+        const Real alpha =
+            std::fabs(a_den) > kTiny ? -cf_neg * std::fabs(a_num) / (std::fabs(dia) * std::fabs(a_den)) : Real(0);
+        const Real beta =
+            std::fabs(b_den) > kTiny ? -cf_pos * std::fabs(b_num) / (std::fabs(dia) * std::fabs(b_den)) : Real(0);
         for (int64_t e = A.rp[i]; e < A.rp[i + 1]; ++e) {
             const int32_t c = A.ci[e];
-            const double v = A.v[e];
+            const Real v = A.v[e];
             if (!(strong[e] && cf[c] == kC) || (lo <= v && v <= hi)) continue;
             P.ci.push_back(cidx[c]);
-            P.v.push_back((v < 0.0 ? alpha : beta) * v);
+            P.v.push_back((v < Real(0) ? alpha : beta) * v);
         }
         P.rp[i + 1] = (int64_t)P.ci.size();
     }
@@ -356,16 +382,63 @@ struct s2l_amg {
     std::vector<Csr> A, P, R;  // P[l].rows == 0: a last level without a coarser one
     int64_t n_coarse = 0;
     std::vector<double> coarse;  // row-major
+    bool single = false;         // computed in float (every value exactly a float)
 };
 
 namespace {
 
-void finish_coarse(s2l_amg& h, const Csr& C)
+template <typename Real>
+void finish_coarse(s2l_amg& h, const CsrT<Real>& C)
 {
     h.n_coarse = C.rows;
     h.coarse.assign((size_t)(C.rows * C.rows), 0.0);
     for (int64_t i = 0; i < C.rows; ++i)
-        for (int64_t e = C.rp[i]; e < C.rp[i + 1]; ++e) h.coarse[(size_t)(i * C.rows + C.ci[e])] = C.v[e];
+        for (int64_t e = C.rp[i]; e < C.rp[i + 1]; ++e) h.coarse[(size_t)(i * C.rows + C.ci[e])] = (double)C.v[e];
+}
+
+// the levels of A in precision Real (AMGCL's amg constructor): transfer operators while a level
+// has more than coarse_enough rows, the last level kept dense
+template <typename Real>
+void build_levels(CsrT<Real> A, int coarse_enough, int coarsening, s2l_amg& h)
+{
+    float eps = 0.08f;
+    bool have = true, direct = true;
+    while (have && A.rows > coarse_enough) {
+        CsrT<Real> P;
+        const bool ok = coarsening == S2L_AMG_RS ? rs_transfer(A, P) : sa_transfer(A, eps, P);
+        eps = eps * 0.5f;
+        h.A.push_back(convert<double>(A));
+        if (!ok) {  // nothing to coarsen: the last level is smoothed only
+            h.P.emplace_back();
+            h.R.emplace_back();
+            have = false;
+            direct = false;
+            break;
+        }
+        CsrT<Real> R = transpose(P);
+        A = product(R, product(A, P));
+        h.P.push_back(convert<double>(P));
+        h.R.push_back(convert<double>(R));
+    }
+    if (direct) finish_coarse(h, A);
+}
+
+// new values on the kept transfer operators of `old` (AMGCL's rebuild), in old's precision
+template <typename Real>
+void rebuild_levels(const s2l_amg& old, CsrT<Real> A, s2l_amg& h)
+{
+    bool direct = true;
+    for (size_t l = 0; l < old.A.size(); ++l) {
+        h.A.push_back(convert<double>(A));
+        h.P.push_back(old.P[l]);
+        h.R.push_back(old.R[l]);
+        if (old.P[l].rows == 0) {
+            direct = false;
+            break;
+        }
+        A = product(convert<Real>(old.R[l]), product(A, convert<Real>(old.P[l])));
+    }
+    if (direct && old.n_coarse > 0) finish_coarse(h, A);
 }
 
 }  // namespace
@@ -377,33 +450,18 @@ int s2l_amg_build(int64_t n, const int64_t* rowptr, const int32_t* col, const do
 {
     if (!out) return S2L_ERR_BADARG;
     *out = nullptr;
+    const bool single = (coarsening & S2L_AMG_SINGLE) != 0;
+    coarsening &= ~S2L_AMG_SINGLE;
     if (coarse_enough < 1 || (coarsening != S2L_AMG_SA && coarsening != S2L_AMG_RS)) return S2L_ERR_BADARG;
     Csr A;
     const int rc = read_csr(n, rowptr, col, val, A);
     if (rc != S2L_OK) return rc;
     std::unique_ptr<s2l_amg> h(new (std::nothrow) s2l_amg());
     if (!h) return S2L_ERR_OOM;
+    h->single = single;
     try {
-        float eps = 0.08f;
-        bool have = true, direct = true;
-        while (have && A.rows > coarse_enough) {
-            Csr P;
-            const bool ok = coarsening == S2L_AMG_RS ? rs_transfer(A, P) : sa_transfer(A, eps, P);
-            eps = eps * 0.5f;
-            h->A.push_back(A);
-            if (!ok) {  // nothing to coarsen: the last level is smoothed only
-                h->P.emplace_back();
-                h->R.emplace_back();
-                have = false;
-                direct = false;
-                break;
-            }
-            Csr R = transpose(P);
-            A = product(R, product(A, P));
-            h->P.push_back(std::move(P));
-            h->R.push_back(std::move(R));
-        }
-        if (direct) finish_coarse(*h, A);
+        if (single) build_levels(convert<float>(A), coarse_enough, coarsening, *h);
+        else build_levels(A, coarse_enough, coarsening, *h);
     } catch (const std::bad_alloc&) {
         return S2L_ERR_OOM;
     }
@@ -424,19 +482,10 @@ int s2l_amg_rebuild(const s2l_amg* old, const int64_t* rowptr, const int32_t* co
     }
     std::unique_ptr<s2l_amg> h(new (std::nothrow) s2l_amg());
     if (!h) return S2L_ERR_OOM;
+    h->single = old->single;
     try {
-        bool direct = true;
-        for (size_t l = 0; l < old->A.size(); ++l) {
-            h->A.push_back(A);
-            h->P.push_back(old->P[l]);
-            h->R.push_back(old->R[l]);
-            if (old->P[l].rows == 0) {
-                direct = false;
-                break;
-            }
-            A = product(old->R[l], product(A, old->P[l]));
-        }
-        if (direct && old->n_coarse > 0) finish_coarse(*h, A);
+        if (old->single) rebuild_levels(*old, convert<float>(A), *h);
+        else rebuild_levels(*old, A, *h);
     } catch (const std::bad_alloc&) {
         return S2L_ERR_OOM;
     }

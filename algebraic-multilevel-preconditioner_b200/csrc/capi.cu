@@ -200,6 +200,7 @@ struct s2l_setup {
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     std::atomic<int> opt_spin_limit{S2L_SPIN_LIMIT};  // polls of a sweep wait before it gives up
     double opt_pivot_tol = 1e-6;  // refactorization of LU factors: largest multiplier 1 / pivot_tol
+    int opt_amg_single = 0;       // AMG local solvers in single precision (--local-precision single)
     // statistics
     int64_t st_sparse_nnz = 0, st_coupling_nnz = 0, st_dense_entries = 0, st_tail_rows = 0;
     int64_t st_levels_max = 0, st_levels_sum = 0;  // sweep dependency levels (both factors)
@@ -242,7 +243,8 @@ struct s2l_setup {
         int64_t vtotal = 0;                 // doubles of one of the three work vectors (f, x, t)
         std::vector<int64_t*> Arp, Rrp, Prp;
         std::vector<int32_t*> Aci, Rci, Pci;
-        std::vector<double*> Av, Rv, Pv;
+        std::vector<double*> Av, Rv, Pv;    // values (float arrays when `single`, cast at use)
+        bool single = false;                // setup option "amg_single": hierarchy and V-cycle in float
         std::vector<int> nsmooth;           // per level: subdomains smoothed on it (CTAs of a sweep)
         std::vector<int32_t*> fsched, bsched, fsub, bsub;
         std::vector<int64_t*> fwf, bwf;
@@ -1144,55 +1146,64 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
 // (mode 1) ylocal, (mode 2: local input/output of subdomain only_sub) out.
 // The AMG local solves of every subdomain: one V-cycle from x = 0 (the reference's
 // --local-approx amg), with the outputs of run_local_solve's modes.
-int amg_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
-                    const double* local_in)
+template <typename Real>
+int amg_local_solve_t(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
+                      const double* local_in)
 {
     s2l_setup* s = w->s;
     const auto& G = s->amgd;
     cudaStream_t st = w->stream;
     const int L = G.nlev;
-    double* f = w->d_amg;
-    double* x = w->d_amg + G.vtotal;
-    double* t = w->d_amg + 2 * G.vtotal;
+    Real* f = reinterpret_cast<Real*>(w->d_amg);
+    Real* x = f + G.vtotal;
+    Real* t = f + 2 * G.vtotal;
+    auto V = [](double* p) { return reinterpret_cast<const Real*>(p); };
     int64_t lo = 0, hi = 0;
     if (only_sub >= 0) {
         lo = s->h_subs[only_sub].loc_off;
         hi = lo + s->h_subs[only_sub].n_local;
     }
-    launch_amg_gather(st, G.nspace[0], s->d_l2g, in, mode == 2 ? local_in : nullptr, lo, hi, f);
-    CUDA_OK(w, cudaMemsetAsync(x, 0, (size_t)G.vtotal * sizeof(double), st));
+    launch_amg_gather<Real>(st, G.nspace[0], s->d_l2g, in, mode == 2 ? local_in : nullptr, lo, hi, f);
+    CUDA_OK(w, cudaMemsetAsync(x, 0, (size_t)G.vtotal * sizeof(Real), st));
     int launched = 2;
     for (int l = 0; l < L; ++l) {
-        double *fl = f + G.voff[l], *xl = x + G.voff[l], *tl = t + G.voff[l];
+        Real *fl = f + G.voff[l], *xl = x + G.voff[l], *tl = t + G.voff[l];
         for (int k = 0; k < G.sweeps; ++k)
-            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.fsched[l], G.fwf[l], G.fsub[l],
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], V(G.Av[l]), fl, xl, G.fsched[l], G.fwf[l], G.fsub[l],
                             G.soff[l], G.sn[l], G.smax[l], G.lanes[l]);
-        launch_coarse_inverse(st, G.ncoarse[l], G.c_off[l], G.c_n[l], G.c_inv[l], G.Cinv, f + G.voff[l], xl);
+        launch_coarse_inverse(st, G.ncoarse[l], G.c_off[l], G.c_n[l], G.c_inv[l], V(G.Cinv), f + G.voff[l], xl);
         launched += G.sweeps + 1;
         if (l + 1 < L) {
-            launch_csr_residual(st, G.nspace[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, tl);
-            launch_csr_mv(st, G.nspace[l + 1], G.Rrp[l], G.Rci[l], G.Rv[l], tl, f + G.voff[l + 1], 0);
+            launch_csr_residual(st, G.nspace[l], G.Arp[l], G.Aci[l], V(G.Av[l]), fl, xl, tl);
+            launch_csr_mv(st, G.nspace[l + 1], G.Rrp[l], G.Rci[l], V(G.Rv[l]), tl, f + G.voff[l + 1], 0);
             launched += 2;
         }
     }
     // the deepest level space: its smoothed subdomains have no coarser level (backward sweeps now)
     for (int k = 0; k < G.sweeps; ++k)
-        launch_gs_sweep(st, G.nsmooth[L - 1], G.Arp[L - 1], G.Aci[L - 1], G.Av[L - 1], f + G.voff[L - 1],
+        launch_gs_sweep(st, G.nsmooth[L - 1], G.Arp[L - 1], G.Aci[L - 1], V(G.Av[L - 1]), f + G.voff[L - 1],
                         x + G.voff[L - 1], G.bsched[L - 1], G.bwf[L - 1], G.bsub[L - 1], G.soff[L - 1], G.sn[L - 1],
                         G.smax[L - 1], G.lanes[L - 1]);
     for (int l = L - 2; l >= 0; --l) {
-        double *fl = f + G.voff[l], *xl = x + G.voff[l];
-        launch_csr_mv(st, G.nspace[l], G.Prp[l], G.Pci[l], G.Pv[l], x + G.voff[l + 1], xl, 1);
+        Real *fl = f + G.voff[l], *xl = x + G.voff[l];
+        launch_csr_mv(st, G.nspace[l], G.Prp[l], G.Pci[l], V(G.Pv[l]), x + G.voff[l + 1], xl, 1);
         for (int k = 0; k < G.sweeps; ++k)
-            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], G.Av[l], fl, xl, G.bsched[l], G.bwf[l], G.bsub[l],
+            launch_gs_sweep(st, G.nsmooth[l], G.Arp[l], G.Aci[l], V(G.Av[l]), fl, xl, G.bsched[l], G.bwf[l], G.bsub[l],
                             G.soff[l], G.sn[l], G.smax[l], G.lanes[l]);
         launched += G.sweeps + 1;
     }
-    launch_amg_scatter(st, G.nspace[0], G.out_idx, x, base, mode == 1 ? w->d_ylocal : out, mode, lo, hi);
+    launch_amg_scatter<Real>(st, G.nspace[0], G.out_idx, x, base, mode == 1 ? w->d_ylocal : out, mode, lo, hi);
     w->launches += launched + 1;
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("AMG local solve launch: ") + cudaGetErrorString(e));
     return S2L_OK;
+}
+
+int amg_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
+                    const double* local_in)
+{
+    return w->s->amgd.single ? amg_local_solve_t<float>(w, in, base, out, mode, only_sub, local_in)
+                             : amg_local_solve_t<double>(w, in, base, out, mode, only_sub, local_in);
 }
 
 int run_local_solve(s2l_work* w, const double* in, const double* base, double* out, int mode, int only_sub,
@@ -2121,6 +2132,17 @@ int amg_build(s2l_setup* s)
     for (int i = 0; i < nsub; ++i)
         if (s->hs[i].amg_sweeps != G.sweeps) return s->fail(S2L_ERR_BADARG, "all AMG hierarchies need the same sweeps");
     G.nlev = L;
+    G.single = s->opt_amg_single != 0;
+    const double vb = G.single ? 4.0 : 8.0;  // bytes of a value
+    // values in the hierarchy's precision (float arrays behind the double pointers when single)
+    auto upload_vals = [&](double** dst, const std::vector<double>& src) -> int {
+        if (!G.single) return upload(s, dst, src);
+        std::vector<float> f(src.begin(), src.end());
+        float* p = nullptr;
+        RET_IF(upload(s, &p, f));
+        *dst = reinterpret_cast<double*>(p);
+        return S2L_OK;
+    };
     auto rows_at = [&](const HostSub& h, int l) -> int64_t {
         const int nl = (int)h.amgA.size();
         if (l < nl) return (int64_t)h.amgA[l].rp.size() - 1;
@@ -2187,7 +2209,7 @@ int amg_build(s2l_setup* s)
                         }
                         rrp.push_back((int64_t)rci.size());
                     }
-                    bytes += (double)(h.amgP[l].ci.size() + h.amgR[l].ci.size()) * 12.0;
+                    bytes += (double)(h.amgP[l].ci.size() + h.amgR[l].ci.size()) * (4.0 + vb);
                 }
                 // sweeps' wavefronts (rows as level-space indices)
                 for (int f = 0; f < 2; ++f) {
@@ -2212,7 +2234,7 @@ int amg_build(s2l_setup* s)
                 soff.push_back(o);
                 sn.push_back(n);
                 G.smax[l] = std::max(G.smax[l], n);
-                bytes += (double)A.ci.size() * 12.0 * (2.0 * sw + 1.0) + (double)n * 8.0 * 6.0;
+                bytes += (double)A.ci.size() * (4.0 + vb) * (2.0 * sw + 1.0) + (double)n * vb * 6.0;
             } else {
                 const int64_t n = rows_at(h, l);  // a coarsest level: no rows of A_l, P_l
                 for (int64_t r = 0; r < n; ++r) {
@@ -2230,7 +2252,7 @@ int amg_build(s2l_setup* s)
                     for (int c = 0; c < nc; ++c)  // stored transposed (column by column)
                         for (int r = 0; r < nc; ++r) cinv_all.push_back(Ci[(size_t)r * nc + c]);
                     G.ncoarse[l] += 1;
-                    bytes += (double)nc * nc * 8.0;
+                    bytes += (double)nc * nc * vb;
                 }
             }
             // rows of space l + 1 that come from subdomains without a transfer at level l
@@ -2239,13 +2261,13 @@ int amg_build(s2l_setup* s)
         }
         RET_IF(upload(s, &G.Arp[l], arp));
         RET_IF(upload(s, &G.Aci[l], aci));
-        RET_IF(upload(s, &G.Av[l], av));
+        RET_IF(upload_vals(&G.Av[l], av));
         RET_IF(upload(s, &G.Prp[l], prp));
         RET_IF(upload(s, &G.Pci[l], pci));
-        RET_IF(upload(s, &G.Pv[l], pv));
+        RET_IF(upload_vals(&G.Pv[l], pv));
         RET_IF(upload(s, &G.Rrp[l], rrp));
         RET_IF(upload(s, &G.Rci[l], rci));
-        RET_IF(upload(s, &G.Rv[l], rv));
+        RET_IF(upload_vals(&G.Rv[l], rv));
         RET_IF(upload(s, &G.fsched[l], fs));
         RET_IF(upload(s, &G.bsched[l], bs));
         RET_IF(upload(s, &G.fwf[l], fwf));
@@ -2262,7 +2284,7 @@ int amg_build(s2l_setup* s)
         RET_IF(upload(s, &G.c_n[l], cn));
         RET_IF(upload(s, &G.c_inv[l], cinvoff));
     }
-    RET_IF(upload(s, &G.Cinv, cinv_all));
+    RET_IF(upload_vals(&G.Cinv, cinv_all));
     std::vector<int32_t> out_idx((size_t)s->nloc, -1);
     for (int i = 0; i < nsub; ++i) {
         const DevSub& d = s->h_subs[i];
@@ -3437,6 +3459,8 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         s->opt_chain = c;
     } else if (n == "refactor") {
         s->opt_refactor = value != 0.0;
+    } else if (n == "amg_single") {
+        s->opt_amg_single = value != 0.0;
     } else if (n == "pivot_tol") {
         if (!(value >= 0.0 && value < 1.0)) return s->fail(S2L_ERR_BADARG, "pivot_tol must be in [0, 1)");
         s->opt_pivot_tol = value;

@@ -238,22 +238,29 @@ void launch_coarse_prolong(cudaStream_t st, int ntiles, const int32_t* t_sub, co
                            const double* y, double* out, double* plocal);
 void launch_to_float(cudaStream_t st, const double* in, float* out, int64_t n);
 
-// AMG local solves (amg.cu)
+// AMG local solves (amg.cu), in the precision Real of the hierarchy (double, or float for the
+// reference's --local-precision single)
 // a Gauss-Seidel sweep of every smoothed subdomain of a level (CTA b: rows [sub_off[b], + sub_n[b])
-// of the level space, kept in shared memory when max_n doubles fit S2L_GS_SMEM_CAP), `lanes`
+// of the level space, kept in shared memory when max_n values fit S2L_GS_SMEM_CAP), `lanes`
 // (4, 8, 16 or 32) lanes per row
-void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const double* v,
-                     const double* f, double* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
+template <typename Real>
+void launch_gs_sweep(cudaStream_t st, int nsub_lvl, const int64_t* rp, const int32_t* ci, const Real* v, const Real* f,
+                     Real* x, const int32_t* sched, const int64_t* wf_ptr, const int32_t* sub_wf,
                      const int64_t* sub_off, const int32_t* sub_n, int max_n, int lanes);
-void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v, const double* x,
-                   double* y, int accumulate);
-void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const double* v,
-                         const double* f, const double* x, double* t);
+template <typename Real>
+void launch_csr_mv(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const Real* v, const Real* x,
+                   Real* y, int accumulate);
+template <typename Real>
+void launch_csr_residual(cudaStream_t st, int64_t n, const int64_t* rp, const int32_t* ci, const Real* v,
+                         const Real* f, const Real* x, Real* t);
+template <typename Real>
 void launch_coarse_inverse(cudaStream_t st, int ncoarse, const int32_t* c_sub_off, const int32_t* c_n,
-                           const int64_t* c_inv_off, const double* Cinv, const double* f, double* x);
+                           const int64_t* c_inv_off, const Real* Cinv, const Real* f, Real* x);
+template <typename Real>
 void launch_amg_gather(cudaStream_t st, int64_t n, const int32_t* l2g, const double* in, const double* local_in,
-                       int64_t lo, int64_t hi, double* f);
-void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const double* x, const double* base,
+                       int64_t lo, int64_t hi, Real* f);
+template <typename Real>
+void launch_amg_scatter(cudaStream_t st, int64_t n, const int32_t* out_idx, const Real* x, const double* base,
                         double* out, int mode, int64_t lo, int64_t hi);
 
 // refactorization (refactor.cu)

@@ -203,8 +203,6 @@ GpuSolvePhase::GpuSolvePhase(const part::Subdomain& sd, const prec::OneLevelSchw
     if (cfg.local_approx != "none" && cfg.local_approx != "amg")
         throw std::invalid_argument("unknown local approximation '" + cfg.local_approx + "' (none|amg)");
     amg_on_ = cfg.local_approx == "amg";
-    if (amg_on_ && cfg.local_precision == "single")
-        throw std::invalid_argument("the GPU AMG local solver runs in FP64 (--local-precision double)");
     coarse_ = two && two->coarse().dimension() > 0 && cfg.coarse != "none";
     if (two && two->coarse().dimension() > 0) {
         const core::Mat& V = two->coarse().basis();
@@ -229,8 +227,11 @@ void GpuSolvePhase::buildAmg(bool keep_transfer)
     if (keep_transfer && amg_) {
         st = s2l_amg_rebuild(amg_, rp.data(), ci.data(), R.valuePtr(), &h);
     } else {
+        // --local-precision single: the hierarchy built in float, as the reference's AMGCL<float>
         st = s2l_amg_build(n, rp.data(), ci.data(), R.valuePtr(), cfg_.amg_coarse_enough,
-                           cfg_.amg_coarsening == "rs" ? S2L_AMG_RS : S2L_AMG_SA, &h);
+                           (cfg_.amg_coarsening == "rs" ? S2L_AMG_RS : S2L_AMG_SA) |
+                               (cfg_.local_precision == "single" ? S2L_AMG_SINGLE : 0),
+                           &h);
     }
     int worst = st;
     MPI_Allreduce(&st, &worst, 1, MPI_INT, MPI_MAX, comm_);
@@ -460,6 +461,8 @@ void GpuSolvePhase::upload()
         }
         // factors are refactorized on the device; AMG hierarchies on the host, then uploaded again
         if (status == S2L_OK && refactorize_ && !amg_on_) status = s2l_gpu_setup_option(setup_, "refactor", 1.0);
+        if (status == S2L_OK && amg_on_ && cfg_.local_precision == "single")
+            status = s2l_gpu_setup_option(setup_, "amg_single", 1.0);  // V-cycle in float
         if (status == S2L_OK) status = s2l_gpu_setup_end(setup_);
         if (status != S2L_OK) msg = ctx_ ? s2l_gpu_last_error(ctx_) : "no CUDA device";
     }

@@ -370,7 +370,7 @@ def build_hierarchy(A, coarse_enough: int = 500, sweeps: int = 1, coarsening: st
     return H
 
 
-def rebuild_hierarchy(H: AmgHierarchy, A) -> AmgHierarchy:
+def rebuild_hierarchy(H: AmgHierarchy, A, single: bool = False) -> AmgHierarchy:
     """The hierarchy of new values of the same matrix with H's transfer operators kept: every
     coarser operator is recomputed as R (A P) and the coarsest is solved directly again
     (AMGCL's ``amg::rebuild``, ``amg.hpp:250-269``, ``level::rebuild``; the reference's
@@ -379,22 +379,34 @@ def rebuild_hierarchy(H: AmgHierarchy, A) -> AmgHierarchy:
     if H.n != A.shape[0]:
         raise ValueError(f"rebuild: {A.shape[0]} rows, the hierarchy has {H.n}")
     out = AmgHierarchy(sweeps=H.sweeps)
+    if single:  # the Galerkin products in float, as AMGCL<float> rebuilds them (values stored widened)
+        A = A.astype(np.float32).astype(np.float64)
     for lvl in H.levels:
         out.levels.append(AmgLevel(A, lvl.P, lvl.R))
-        A = _sorted_csr(lvl.R @ (A @ lvl.P)) if lvl.P is not None else None
+        if lvl.P is None:
+            A = None
+        elif single:
+            f = np.float32
+            A = _sorted_csr((lvl.R.astype(f) @ (A.astype(f) @ lvl.P.astype(f))).astype(np.float64))
+        else:
+            A = _sorted_csr(lvl.R @ (A @ lvl.P))
     if H.coarse is not None:
         out.coarse = A.toarray()
     return out
 
 
-def build_hierarchy_native(A, coarse_enough: int = 500, sweeps: int = 1, coarsening: str = "sa") -> AmgHierarchy:
+def build_hierarchy_native(A, coarse_enough: int = 500, sweeps: int = 1, coarsening: str = "sa",
+                           single: bool = False) -> AmgHierarchy:
     """build_hierarchy computed by the library's host setup (s2l_amg_build, the same algorithms in
     C++, bit-identical levels) when libs2l_gpu.so is built, else by the Python restatement; used by
-    the setup producer, where the Python loops would dominate the setup of large subdomains."""
+    the setup producer, where the Python loops would dominate the setup of large subdomains.
+    single: the setup in single precision (--local-precision single; the library's host setup only)."""
     try:
         from . import capi
-        N = capi.NativeAmg.build(A, coarse_enough, coarsening)
+        N = capi.NativeAmg.build(A, coarse_enough, coarsening, single=single)
     except FileNotFoundError:
+        if single:
+            raise
         return build_hierarchy(A, coarse_enough=coarse_enough, sweeps=sweeps, coarsening=coarsening)
     try:
         return N.hierarchy(sweeps=sweeps)

@@ -251,7 +251,10 @@ class GpuSetup:
                                                 COARSE[coarse or opts.coarse], POU[pou or opts.pou], C.byref(h)))
         self.h = h
         try:
-            for k, v in (options or {}).items():
+            options = dict(options or {})
+            if opts.local_approx == "amg" and opts.local_precision == "single":
+                options.setdefault("amg_single", 1)  # the hierarchy's values are floats: V-cycle in float
+            for k, v in options.items():
                 ctx.check(self.lib.s2l_gpu_setup_option(h, k.encode(), float(v)))
             self._upload(st, coarse or opts.coarse)
         except Exception:
@@ -576,8 +579,11 @@ class NativeAmg:
     def __init__(self, h, lib):
         self.h, self.lib = h, lib
 
+    SINGLE = 16  # S2L_AMG_SINGLE
+
     @classmethod
-    def build(cls, A, coarse_enough: int = 500, coarsening: str = "sa") -> "NativeAmg":
+    def build(cls, A, coarse_enough: int = 500, coarsening: str = "sa", single: bool = False) -> "NativeAmg":
+        """single: the setup in single precision (--local-precision single), every value a float."""
         import scipy.sparse as sp
         lib = load()
         A = sp.csr_matrix(A, dtype=np.float64)
@@ -586,8 +592,8 @@ class NativeAmg:
         ci = np.ascontiguousarray(A.indices, dtype=np.int32)
         v = np.ascontiguousarray(A.data, dtype=np.float64)
         h = C.c_void_p()
-        rc = lib.s2l_amg_build(A.shape[0], _vp(rp), _vp(ci), _vp(v), int(coarse_enough), cls.CODES[coarsening],
-                               C.byref(h))
+        code = cls.CODES[coarsening] | (cls.SINGLE if single else 0)
+        rc = lib.s2l_amg_build(A.shape[0], _vp(rp), _vp(ci), _vp(v), int(coarse_enough), code, C.byref(h))
         if rc != S2L_OK:
             raise S2LError(rc, "s2l_amg_build")
         return cls(h, lib)

@@ -338,7 +338,7 @@ def _subdomain_work(args):
     if opts.local_approx == "amg":
         from .amg import build_hierarchy_native
         fac = build_hierarchy_native(Aii, coarse_enough=opts.amg_coarse_enough, sweeps=opts.amg_sweeps,
-                                     coarsening=opts.amg_coarsening)
+                                     coarsening=opts.amg_coarsening, single=opts.local_precision == "single")
     else:
         fac = factorize_local(Aii, symmetric, opts.local_factorization, opts.local_precision)
     Z, info = (local_coarse_vectors(Aii, Atil, D, opts, symmetric) if want_coarse
@@ -559,11 +559,12 @@ def refactor_amg_setup(st: Setup, A_new: sp.csr_matrix) -> Setup:
         idx = sd.l2g()
         Aii = sp.csr_matrix(A_new[idx][:, idx])
         Aii.sort_indices()
+        single = o.local_precision == "single"
         if o.amg_reuse:
-            H = rebuild_hierarchy(sd.amg, Aii)
+            H = rebuild_hierarchy(sd.amg, Aii, single=single)
         else:
             H = build_hierarchy_native(Aii, coarse_enough=o.amg_coarse_enough, sweeps=o.amg_sweeps,
-                                       coarsening=o.amg_coarsening)
+                                       coarsening=o.amg_coarsening, single=single)
         ns = copy.copy(sd)
         ns.Aii = Aii
         ns.amg = H

@@ -506,7 +506,7 @@ def run_ours(a):
 
     log(f"serving done: {serving and round(serving['solves_per_s'], 1)} solves/s")
     # ---- AMG local solvers (the reference's --local-approx amg) on the same matrix and basis
-    amg_form = amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64) if a.amg else None
+    amg_form = amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64, mixed) if a.amg else None
 
     # roofline of the headline's dominant kernel group: the block local solve (factors read once,
     # every column's gather and owned write), and of the single-column forms and the SpMV
@@ -638,28 +638,41 @@ def run_ours(a):
     reps.close()
 
 
-def amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64):
-    """The same matrix, partition and coarse basis with each A_ii^-1 replaced by one AMG V-cycle."""
+def amg_local_solves(a, tm, ctx, st, b_dev, x_dev, stream, plain, x64, mixed=None):
+    """The same matrix, partition and coarse basis with each A_ii^-1 replaced by one AMG V-cycle:
+    FP64 (the hierarchy and the V-cycle in double, the reference's GMRES) and FP32 (the reference's
+    --local-precision single: the hierarchy built in float, the V-cycle in float, flexible GMRES in
+    FP64 converged at the FP64 true residual)."""
+    import copy
     import dataclasses
     import numpy as np
     from s2l_b200 import capi
     from s2l_b200.amg import build_hierarchy_native as build_hierarchy
-    t0 = time.time()
-    subs = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii)) for sd in st.subdomains]
-    st_amg = dataclasses.replace(st, subdomains=subs)
-    host_s = time.time() - t0
-    ga = capi.GpuSetup(ctx, st_amg)
-    ga.set_stream(stream.cuda_stream)
-    kw = dict(restart=50, rtol=1e-8, flexible=False, strict=False, maxit=2000)
-    f, xa = single_form(tm, ga, b_dev, x_dev, kw, x_ref=x64)
-    ga.close()
-    levels = sorted({len(sd.amg.levels) + (sd.amg.coarse is not None) for sd in subs})
-    return {"ms_per_solve": f["ms_per_solve"], "iterations": f["iterations"], "converged": f["converged"],
+    out = {}
+    for prec in ("double", "single"):
+        t0 = time.time()
+        subs = [dataclasses.replace(sd, factor=None, amg=build_hierarchy(sd.Aii, single=prec == "single"))
+                for sd in st.subdomains]
+        st_amg = dataclasses.replace(st, subdomains=subs, opts=copy.copy(st.opts))
+        st_amg.opts.local_approx = "amg"
+        st_amg.opts.local_precision = prec
+        host_s = time.time() - t0
+        ga = capi.GpuSetup(ctx, st_amg)
+        ga.set_stream(stream.cuda_stream)
+        flex = prec == "single"
+        kw = dict(restart=50, rtol=1e-8, flexible=flex, strict=flex, maxit=2000)
+        f, xa = single_form(tm, ga, b_dev, x_dev, kw, x_ref=x64)
+        ga.close()
+        levels = sorted({len(sd.amg.levels) + (sd.amg.coarse is not None) for sd in subs})
+        out["fp64" if prec == "double" else "fp32"] = {
+            "ms_per_solve": f["ms_per_solve"], "iterations": f["iterations"], "converged": f["converged"],
             "true_rel_residual_host_check": float(np.linalg.norm(st.b - st.A @ xa) / np.linalg.norm(st.b)),
             "rel_error_vs_fp64": f["rel_error_vs_fp64"],
             "v_cycle_ms": f["local_solve_ms_total"] / max(f["local_solve_launches"], 1), "levels": levels,
-            "operator_entries": int(sum(sd.amg.nnz() for sd in subs)), "host_setup_s": host_s,
-            "vs_plain_fp64_exact": {"ms_per_solve": plain["ms_per_solve"], "iterations": plain["iterations"]}}
+            "operator_entries": int(sum(sd.amg.nnz() for sd in subs)), "host_setup_s": host_s}
+    out["vs_exact_factors"] = {"plain_fp64_ms_per_solve": plain["ms_per_solve"], "plain_fp64_iterations": plain["iterations"],
+                               "mixed_fp32_ms_per_solve": mixed["ms_per_solve"] if mixed else None}
+    return out
 
 
 def three_forms(tm, ctx, st, w, stream, dev, k=16):

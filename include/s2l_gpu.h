@@ -159,7 +159,10 @@ int s2l_gpu_add_subdomain_amg(s2l_setup* s, int i, int64_t begin, int n_owned, i
  * without a coarser one) / s2l_amg_coarse (row-major, n_coarse^2) in the layout
  * s2l_gpu_add_subdomain_amg takes; the pointers stay valid until s2l_amg_free. */
 typedef struct s2l_amg s2l_amg;
-enum { S2L_AMG_SA = 0, S2L_AMG_RS = 1 };
+/* coarsening, optionally | S2L_AMG_SINGLE: the whole setup in single precision, as the reference's
+ * --local-precision single builds it (AMGCL's builtin<float> backend); every value returned is then a
+ * float widened to double.  s2l_amg_rebuild keeps the precision of `old`. */
+enum { S2L_AMG_SA = 0, S2L_AMG_RS = 1, S2L_AMG_SINGLE = 16 };
 int s2l_amg_build(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val, int coarse_enough,
                   int coarsening, s2l_amg** out);
 int s2l_amg_rebuild(const s2l_amg* old, const int64_t* rowptr, const int32_t* col, const double* val, s2l_amg** out);

@@ -9,6 +9,7 @@
 // next.bin: the same layout with nvec = 0: new values of A_ii; the solver is then refactorize()d
 //          with them (AmgOptions::reuse: keep the transfer operators, else a new hierarchy)
 // out.bin: double results[nvec][n]          (the solver's solve() of each vector)
+// S2L_AMG_SINGLE=1 in the environment: the solver in single precision (--local-precision single)
 #include "inexact_solver.hpp"
 
 #include <cstdio>
@@ -65,6 +66,8 @@ int s2l_rank_main(int argc, char** argv)
     spec.amg.sweeps = std::atoi(argv[4]);
     spec.amg.coarsening = argv[5];
     spec.amg.reuse = argc >= 8 && std::atoi(argv[7]) != 0;
+    const char* single = std::getenv("S2L_AMG_SINGLE");  // 1: --local-precision single (AMGCL in float)
+    spec.single = single && std::atoi(single) != 0;
     auto solver = linalg::makeInexactSolver(spec);
     if (!solver->factorize(A)) {
         std::cerr << "AMG setup failed: " << solver->lastError() << "\n";

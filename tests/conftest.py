@@ -35,6 +35,8 @@ def small_setup(name: str, **kw):
         w.opts.nev = kw.get("nev", 8)
     else:
         raise ValueError(name)
+    if "precision" in kw:
+        w.opts.local_precision = kw["precision"]
     for k in ("one_level", "coarse", "pou", "overlap", "local_approx", "amg_coarse_enough", "amg_sweeps",
               "amg_coarsening"):
         if k in kw:

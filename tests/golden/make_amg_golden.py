@@ -36,6 +36,15 @@ CASES = {  # name: (family, setup keywords, subdomain, coarse_enough, sweeps[, c
 }
 
 
+# single precision (--local-precision single: AMGCL's builtin<float>, setup and V-cycle in float)
+SINGLE_CASES = {  # name: (family, setup keywords, subdomain, coarse_enough, sweeps, coarsening)
+    "single_bubbles3d_3lev": ("bubbles3d", {}, 0, 50, 1, "sa"),
+    "single_poisson2d_3lev": ("poisson2d", {}, 0, 50, 1, "sa"),
+    "single_rs_convdiff3d": ("convdiff3d", {}, 0, 50, 1, "rs"),
+    "single_rs_bubbles3d_sweeps2": ("bubbles3d", {}, 5, 100, 2, "rs"),
+}
+
+
 # refactorization: the reference's solver set up on A_ii of the bubble sequence at time 0, then
 # refactorize()d with A_ii at a later time (bubbles moved), with and without --amg-reuse
 REFACTOR_CASES = {  # name: (subdomain, coarse_enough, sweeps, time of the new matrix, reuse)
@@ -55,7 +64,7 @@ def write_matrix(path, A, vecs=()):
             np.asarray(vecs, dtype=np.float64).tofile(f)
 
 
-def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0, coarsening="sa"):
+def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0, coarsening="sa", single=False):
     A = sp.csr_matrix(A)
     A.sort_indices()
     with tempfile.TemporaryDirectory() as d:
@@ -67,7 +76,8 @@ def reference_apply(A, vecs, coarse_enough, sweeps, A_next=None, reuse=0, coarse
             A_next.sort_indices()
             write_matrix(fnext, A_next)
             cmd += [fnext, str(int(reuse))]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        env = dict(os.environ, S2L_AMG_SINGLE="1" if single else "0")
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
         if r.returncode:
             raise RuntimeError(r.stderr)
         return np.fromfile(fout).reshape(len(vecs), -1), r.stderr.strip()
@@ -88,6 +98,18 @@ def main():
         extra = {"coarsening": coarsening} if coarsening != "sa" else {}
         np.savez_compressed(os.path.join(HERE, f"amg_{name}.npz"), indptr=A.indptr, indices=A.indices, data=A.data,
                             vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps, info=info, **extra)
+        print(name, A.shape[0], info)
+    for name, (fam, kw, i, ce, sweeps, coarsening) in SINGLE_CASES.items():
+        _, st = small_setup(fam, **kw)
+        s = st.subdomains[i]
+        idx = s.l2g()
+        A = sp.csr_matrix(st.A[idx][:, idx])
+        A.sort_indices()
+        vecs = np.random.default_rng(900 + i).uniform(-1.0, 1.0, (2, A.shape[0]))
+        out, info = reference_apply(A, vecs, ce, sweeps, coarsening=coarsening, single=True)
+        np.savez_compressed(os.path.join(HERE, f"amg_{name}.npz"), indptr=A.indptr, indices=A.indices, data=A.data,
+                            vecs=vecs, out=out, coarse_enough=ce, sweeps=sweeps, info=info, coarsening=coarsening,
+                            precision="single")
         print(name, A.shape[0], info)
     import dataclasses
     from s2l_b200 import sequence as seqmod

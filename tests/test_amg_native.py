@@ -78,7 +78,7 @@ def test_native_rebuild_equals_python(coarsening):
 
 
 @pytest.mark.parametrize("fixture", sorted(f for f in os.listdir(GOLDEN) if f.startswith("amg_")
-                                           and not f.startswith("amg_refactor_")))
+                                           and not f.startswith(("amg_refactor_", "amg_single_"))))
 def test_native_hierarchy_reproduces_the_reference(fixture):
     from oracle.oracle import amg_apply
     g = np.load(os.path.join(GOLDEN, fixture))

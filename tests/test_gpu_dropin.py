@@ -51,6 +51,11 @@ CASES = {
     "convdiff3d_amg_rs": (4, ["--generate", "convdiff3d", "--nx", "12", "--nev", "8", "--coarse", "deflated",
                               "--local-factorization", "lu", "--restart", "40", "--local-approx", "amg",
                               "--amg-coarsening", "rs", "--amg-coarse-enough", "50"]),
+    # AMG local solvers in single precision (the hierarchy in float, the V-cycle on the device in float)
+    "bubbles3d_amg_sa_single": (4, ["--generate", "bubbles3d", "--nx", "16", "--nbubbles", "8", "--radius", "0.12",
+                                    "--nev", "10", "--coarse", "deflated", "--local-factorization", "cholesky",
+                                    "--restart", "50", "--local-approx", "amg", "--amg-coarse-enough", "100",
+                                    "--local-precision", "single"]),
 }
 
 

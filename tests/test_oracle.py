@@ -175,7 +175,9 @@ def test_oracle_refactorization_reports_bad_pivots():
 
 
 AMG_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden"))
-                    if f.startswith("amg_") and not f.startswith("amg_refactor_"))
+                    if f.startswith("amg_") and not f.startswith(("amg_refactor_", "amg_single_")))
+AMG_SINGLE_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden"))
+                           if f.startswith("amg_single_"))
 AMG_REFACTOR_GOLDEN = sorted(f for f in os.listdir(os.path.join(os.path.dirname(__file__), "golden"))
                              if f.startswith("amg_refactor_"))
 
@@ -199,6 +201,32 @@ def test_amg_hierarchy_and_cycle_pinned_on_the_reference(fixture):
     for v, ref in zip(g["vecs"], g["out"]):
         x = amg_apply(H, v)
         assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("fixture", AMG_SINGLE_GOLDEN)
+def test_single_precision_amg_pinned_on_the_reference(fixture):
+    """--local-precision single with --local-approx amg: the library's host setup in float
+    (s2l_amg_build with S2L_AMG_SINGLE, AMGCL's builtin<float> restated) builds the reference's
+    hierarchy (same levels); the oracle's V-cycle on it (FP64 arithmetic on the float values)
+    reproduces the reference's float solve() to 1e-5, the tolerance of the FP32 paths."""
+    import scipy.sparse as sp
+    from oracle.oracle import amg_apply
+    from s2l_b200 import capi
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture))
+    n = g["indptr"].size - 1
+    A = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
+    N = capi.NativeAmg.build(A, int(g["coarse_enough"]), str(g["coarsening"]), single=True)
+    H = N.hierarchy(sweeps=int(g["sweeps"]))
+    N.close()
+    levels = str(g["info"]).split("[")[1].split(" levels")[0]
+    assert len(H.levels) + (H.coarse is not None) == int(levels)
+    for lv in H.levels:  # every stored value is a float
+        for M in (lv.A, lv.P, lv.R):
+            if M is not None:
+                assert np.array_equal(M.data, M.data.astype(np.float32).astype(np.float64))
+    for v, ref in zip(g["vecs"], g["out"]):
+        x = amg_apply(H, v)
+        assert np.linalg.norm(x - ref) <= 1e-5 * np.linalg.norm(ref), np.linalg.norm(x - ref) / np.linalg.norm(ref)
 
 
 @pytest.mark.parametrize("fixture", AMG_REFACTOR_GOLDEN)
