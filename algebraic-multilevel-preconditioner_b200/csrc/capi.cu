@@ -467,6 +467,23 @@ std::vector<std::vector<int32_t>> chain_blocks(const HostCsr& M, int T, bool low
 // which depend only on rows solved before the block, and the right-hand side of the block by
 // W^-1 b(B) (the sweep's prologue): the k-step chain becomes one level.  The replaced rows hold
 // the union of the block rows' patterns; a block stops before a row that would reach 65535 entries.
+// f(i) for i in [0, n) on up to hardware_concurrency host threads (each i independent)
+void parallel_for(int n, const std::function<void(int)>& f)
+{
+    const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&] {
+            for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) f(i);
+        });
+    for (auto& x : th) x.join();
+}
+
 void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, int gmax, int chain, Sweep& out,
                  std::string& err, const std::vector<int32_t>* mpos = nullptr)
 {
@@ -2379,13 +2396,14 @@ int s2l_gpu_setup_end(s2l_setup* s)
     tm.nsub = nsub;
     tm.real_bytes = (double)rs;
     tm.chain = s->opt_chain;
-    double sp_nnz_total = 0.0, sp_rows_total = 0.0;
-    for (int i = 0; i < nsub; ++i) {
+    // per subdomain and independent of the others: on several host threads
+    std::vector<char> ldlt_bad(nsub, 0);
+    parallel_for(nsub, [&](int i) {
         HostSub& h = s->hs[i];
         const int nl = h.n_local();
         if (h.amg) {  // no factors: the whole local space is "sparse part" without a tail
             Ts[i] = nl;
-            continue;
+            return;
         }
         if (h.kind == S2L_FACTOR_LU) {
             Us[i] = std::move(h.U);
@@ -2405,16 +2423,16 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     }
                     missing = missing || !f;
                 }
-                if (missing) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
+                if (missing) {
+                    ldlt_bad[i] = 1;
+                    return;
+                }
             }
         }
         Ts[i] = choose_tail(h.L, Us[i], nl, tm);
-        for (int r = 0; r < Ts[i]; ++r)
-            for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) sp_nnz_total += h.L.ci[e] < r ? 1.0 : 0.0;
-        sp_rows_total += Ts[i];
-    }
-    (void)sp_nnz_total;
-    (void)sp_rows_total;
+    });
+    for (int i = 0; i < nsub; ++i)
+        if (ldlt_bad[i]) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
     s->sweep_group = s->opt_group ? s->opt_group : 32;  // widest lane group of a sweep row
     const int nw = S2L_BS_SWEEP / 32;
     // pass 2: layouts
@@ -2450,11 +2468,56 @@ int s2l_gpu_setup_end(s2l_setup* s)
         s->rf.sz.assign(nsub, 0);
         s->rf.llt.assign(nsub, 0);
     }
+    // the sweep layouts of both factors and, with the refactorization plan, the combined pattern and
+    // the position of every factor entry in it: per subdomain, on several host threads
+    struct PreLayout {
+        Sweep sl, su;
+        FPat P;
+        std::vector<int32_t> mposL, mposU;
+        std::string err;
+        int code = S2L_OK;
+    };
+    std::vector<PreLayout> pre(nsub);
+    s->sweep_group = s->opt_group ? s->opt_group : 32;
+    parallel_for(nsub, [&](int i) {
+        HostSub& h = s->hs[i];
+        if (h.amg) return;
+        PreLayout& q = pre[i];
+        const HostCsr& U = Us[i];
+        const int nl = h.n_local();
+        const int T = Ts[i];
+        const bool unitL = h.kind != S2L_FACTOR_LLT;
+        const bool llt = h.kind == S2L_FACTOR_LLT;
+        if (rfon) {
+            if (!make_fpattern(h.L, U, nl, llt, q.P)) {
+                q.code = S2L_ERR_BADARG;
+                q.err = "a factor has no diagonal entry";
+                return;
+            }
+            q.mposL.assign(h.L.ci.size(), -1);
+            for (int r = 0; r < nl; ++r)
+                for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) {
+                    const int c = h.L.ci[e];
+                    if (llt ? c <= r : c < r) q.mposL[e] = q.P.find(r, c);
+                }
+            q.mposU.assign(U.ci.size(), -1);
+            for (int r = 0; r < nl; ++r)
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
+                    const int c = U.ci[e];
+                    q.mposU[e] = llt ? q.P.find(c, r) : q.P.find(r, c);
+                }
+        }
+        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, q.sl, q.err, rfon ? &q.mposL : nullptr);
+        if (q.err.empty())
+            build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, q.su, q.err, rfon ? &q.mposU : nullptr);
+        if (!q.err.empty()) q.code = S2L_ERR_NUMERIC;
+    });
     for (int i = 0; i < nsub; ++i) {
         HostSub& h = s->hs[i];
         const HostCsr& U = Us[i];
         const int nl = h.n_local();
         max_nl = std::max(max_nl, nl);
+        if (pre[i].code != S2L_OK) return s->fail(pre[i].code, "subdomain " + std::to_string(i) + ": " + pre[i].err);
         if (h.amg) {  // AMG local solver: the local space in natural order, no sweeps or tails
             s->tr_first_h[i] = (int)tr_sub.size();
             s->us_first_h[i] = (int)us_sub.size();
@@ -2489,15 +2552,14 @@ int s2l_gpu_setup_end(s2l_setup* s)
         const int T = Ts[i];
         const int sz = nl - T;
         max_T = std::max(max_T, T);
-        std::string err;
-        Sweep sl, su;
-        FPat P;
-        std::vector<int32_t> mposL, mposU;
+        Sweep& sl = pre[i].sl;
+        Sweep& su = pre[i].su;
+        const FPat& P = pre[i].P;
+        const std::vector<int32_t>& mposL = pre[i].mposL;
+        const std::vector<int32_t>& mposU = pre[i].mposU;
         const bool llt = h.kind == S2L_FACTOR_LLT;
         const int64_t fb = rf_fbase.back();
         if (rfon) {
-            if (!make_fpattern(h.L, U, nl, llt, P))
-                return s->fail(S2L_ERR_BADARG, "subdomain " + std::to_string(i) + ": a factor has no diagonal entry");
             // the column kernels address a column's tail rows through 16-bit offsets and keep one
             // row map of the tail per warp in shared memory
             for (int c = 0; c < nl; ++c) {
@@ -2506,20 +2568,9 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 s->rf.maxcol = std::max(s->rf.maxcol, (int)(P.cp[c + 1] - P.cp[c]));
             }
             if (nl > 100000) return s->fail(S2L_ERR_BADARG, "refactor: a subdomain of more than 100000 rows");
-            mposL.assign(h.L.ci.size(), -1);
-            for (int r = 0; r < nl; ++r)
-                for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e) {
-                    const int c = h.L.ci[e];
-                    if (llt ? c <= r : c < r) mposL[e] = P.find(r, c);
-                }
-            mposU.assign(U.ci.size(), -1);
             bool found = true;
             for (int r = 0; r < nl; ++r) {
-                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) {
-                    const int c = U.ci[e];
-                    mposU[e] = llt ? P.find(c, r) : P.find(r, c);
-                    found = found && mposU[e] >= 0;
-                }
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) found = found && mposU[e] >= 0;
                 for (int64_t e = h.L.rp[r]; e < h.L.rp[r + 1]; ++e)
                     if (llt ? h.L.ci[e] <= r : h.L.ci[e] < r) found = found && mposL[e] >= 0;
             }
@@ -2528,10 +2579,6 @@ int s2l_gpu_setup_end(s2l_setup* s)
             s->rf.sz[i] = sz;
             s->rf.llt[i] = llt;
         }
-        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, sl, err, rfon ? &mposL : nullptr);
-        if (err.empty())
-            build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, su, err, rfon ? &mposU : nullptr);
-        if (!err.empty()) return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": " + err);
         if (rfon) {
             // pattern, per-column data, L L^T row lists
             for (int c = 0; c < nl; ++c) {

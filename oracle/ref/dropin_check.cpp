@@ -76,6 +76,35 @@ int main(int argc, char** argv)
             return worst;
         };
         double worst = apply_diff();
+        // the two parts of the apply on their own (the drop-in's device setup through the C ABI on
+        // rank 0): the one-level apply (local solves, exact factors on both sides) and the coarse
+        // correction (E solved by the reference's factorization, by the explicit inverse on the GPU)
+        auto part_diff = [&](bool coarse_part) {
+            std::mt19937_64 g(777);
+            std::uniform_real_distribution<double> u(-1.0, 1.0);
+            std::vector<double> rg((size_t)sys.n_global);
+            for (auto& v : rg) v = u(g);
+            core::Vec r(sys.nOwned()), z1, z2;
+            for (int i = 0; i < sys.nOwned(); ++i) r[i] = rg[(size_t)(sys.rowBegin() + i)];
+            if (coarse_part) two->coarse().apply(r, z1);
+            else one->apply(r, z1);
+            std::vector<double> rgl, zgl;
+            phase->gather(r, rgl);
+            int st = 0;
+            if (rank == 0) {
+                zgl.assign(rgl.size(), 0.0);
+                st = coarse_part ? s2l_gpu_coarse_apply(phase->setup(), rgl.data(), zgl.data(), S2L_PTR_HOST)
+                                 : s2l_gpu_one_level_apply(phase->setup(), rgl.data(), zgl.data(), S2L_PTR_HOST);
+            }
+            phase->check(st, "component apply");
+            phase->scatter(zgl, z2);
+            double num = (z1 - z2).squaredNorm(), den = z1.squaredNorm(), gn = 0.0, gd = 0.0;
+            MPI_Allreduce(&num, &gn, 1, MPI_DOUBLE, MPI_SUM, comm);
+            MPI_Allreduce(&den, &gd, 1, MPI_DOUBLE, MPI_SUM, comm);
+            return std::sqrt(gn / gd);
+        };
+        const double one_diff = part_diff(false);
+        const double coarse_diff = (two && cfg.coarse != "none" && two->coarse().dimension() > 0) ? part_diff(true) : 0.0;
         std::string level_out;
         if (!update_level.empty()) {
             // new values D A D with d(g) = 1 + 0.1 sin(1 + 0.37 g) (same pattern, symmetric kept)
@@ -125,7 +154,8 @@ int main(int argc, char** argv)
               << ", \"gpu_true_rel_residual\": " << r2.true_rel_residual << ", \"ref_true_rel_residual\": "
               << r1.true_rel_residual << ", \"gpu_final_residual_of\": " << r2.final_residual_of
               << ", \"ref_final_residual_of\": " << r1.final_residual_of << ", \"x_rel_diff\": " << xdiff
-              << ", \"history_rel_diff\": " << hdiff
+              << ", \"history_rel_diff\": " << hdiff << ", \"one_level_rel_diff\": " << one_diff
+              << ", \"coarse_rel_diff\": " << coarse_diff
               << ", \"gpu_solver\": \"" << gk->name() << "\", \"update\": \"" << level_out
               << "\", \"ok\": " << (ok ? "true" : "false") << "}";
             std::cout << s.str() << std::endl;
