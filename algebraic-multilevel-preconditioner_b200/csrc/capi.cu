@@ -2741,7 +2741,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 bool any = false;
                 for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e)
                     if (U.ci[e] >= T) {
-                        ust_col.push_back(U.ci[e]);
+                        ust_col.push_back((int32_t)(loc + U.ci[e]));  // local-space index of the tail row
                         ust_val.push_back(U.v[e]);
                         if (rfon) rf_ust.push_back(fb + (llt ? P.find(U.ci[e], r) : P.find(r, U.ci[e])));
                         any = true;

@@ -339,6 +339,9 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     }
     volatile Real* x = xs;
     if (threadIdx.x == 0) abort_flag = 0;
+    // the right-hand side of every slot (scaled by 1/diag): iterations are independent, so four are
+    // unrolled to keep their gathers in flight together
+#pragma unroll 4
     for (int k = threadIdx.x; k < T; k += S2L_BS_SWEEP) {
         const Real d = F.dinv[lo + k];
         const int64_t src = FWD ? (int64_t)a.gather[lo + k] * K : (lo + a.u2l[lo + k]) * K;
@@ -660,17 +663,47 @@ __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Rea
 }
 
 // Backward coupling: y(r) -= U(r, T:n) x(T:n) for the sparse rows that have tail columns, K columns.
+// These rows are short (a sparse row's entries in the tail columns), so a warp takes 32 of them
+// (chunk mode): their entries are contiguous, loaded with coalesced loads, multiplied by the
+// gathered tail values (columns stored as local-space indices) and left in shared memory; lane j
+// then adds row j's products in entry order.
 template <typename Real, int K>
 __global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveArgs<Real> a, int q0, int count)
 {
-    const int q = q0 + blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (q >= q0 + count) return;
-    const DevSub sd = a.subs[a.us_sub[q]];
-    const int64_t lo = sd.loc_off;
-    Real acc[K];
-    warp_gather_dot<Real, K>(a.ust_val, a.ust_col, a.ust_ptr[q], a.ust_ptr[q + 1], a.ybuf + lo * K, lane, acc);
-    if (lane < K) a.ybuf[(lo + a.us_r[q]) * K + lane] -= pick<Real, K>(acc, lane);
+    constexpr int CAP = 512 / K;  // entries of a piece
+    __shared__ Real prod[8][CAP * K];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Real* wp = prod[warp];
+    const int nchunks = (count + 31) / 32;
+    for (int ch = blockIdx.x * 8 + warp; ch < nchunks; ch += gridDim.x * 8) {
+        const int qa = q0 + ch * 32, qb = min(qa + 32, q0 + count), q = qa + lane;
+        const int64_t e_lo = a.ust_ptr[qa], e_hi = a.ust_ptr[qb];
+        const int64_t my0 = q < qb ? a.ust_ptr[q] : e_hi, my1 = q < qb ? a.ust_ptr[q + 1] : e_hi;
+        Real acc[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) acc[r] = Real(0);
+        for (int64_t base = e_lo; base < e_hi; base += CAP) {
+            const int cnt = (int)(e_hi - base < CAP ? e_hi - base : CAP);
+            for (int e = lane; e < cnt; e += 32) {
+                const Real v = a.ust_val[base + e];
+                Real x[K];
+                load_k<Real, K>(a.ybuf + (int64_t)a.ust_col[base + e] * K, x);
+#pragma unroll
+                for (int r = 0; r < K; ++r) wp[e * K + r] = v * x[r];
+            }
+            __syncwarp();
+            const int64_t s0 = (my0 > base ? my0 : base) - base, s1 = (my1 < base + cnt ? my1 : base + cnt) - base;
+            for (int64_t e = s0; e < s1; ++e)
+#pragma unroll
+                for (int r = 0; r < K; ++r) acc[r] += wp[e * K + r];
+            __syncwarp();
+        }
+        if (q < qb) {
+            const int64_t o = (a.subs[a.us_sub[q]].loc_off + a.us_r[q]) * K;
+#pragma unroll
+            for (int r = 0; r < K; ++r) a.ybuf[o + r] -= acc[r];
+        }
+    }
 }
 
 __global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n)
@@ -1474,7 +1507,7 @@ cudaError_t launch_local_solve_k(cudaStream_t st, const LocalSolveArgs<Real>& a,
         nl += 3;
     }
     if (us_count > 0) {
-        sparse_coupling_kernel<Real, K><<<(us_count + 7) / 8, 256, 0, st>>>(a, us_first, us_count);
+        sparse_coupling_kernel<Real, K><<<(us_count + 255) / 256, 256, 0, st>>>(a, us_first, us_count);
         nl += 1;
     }
     if (smem > 0)

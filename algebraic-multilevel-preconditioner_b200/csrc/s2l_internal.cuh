@@ -89,7 +89,8 @@ struct LocalSolveArgs {
     const int64_t* lts_ptr;
     const int32_t* lts_col;
     const Real* lts_val;
-    // sparse rows with U(r, T:n) coupling: (sub, r) pairs and CSR
+    // sparse rows with U(r, T:n) coupling: (sub, r) pairs and CSR (columns as local-space indices,
+    // loc_off + tail row, so a warp can gather for rows of several subdomains)
     const int32_t* us_sub;
     const int32_t* us_r;
     const int64_t* ust_ptr;
