@@ -114,7 +114,7 @@ struct Sweep {
     std::vector<int32_t> pos;     // row -> slot
     std::vector<uint16_t> len;    // entries per slot
     std::vector<double> dinv;     // per slot
-    std::vector<int32_t> col;     // column slots (-1: padding), per warp, per task lane-interleaved
+    std::vector<int32_t> col;     // column slots (T, the sentinel slot: padding), per warp, per task lane-interleaved
     std::vector<double> val;      // values times 1/diag of their row
     std::vector<uint32_t> thdr;   // per task: chunks C (bits 0-15), log2 G (16-18), rows R - 1 (19-23)
     std::vector<int32_t> tslot;   // per task: its R slots
@@ -187,18 +187,19 @@ struct s2l_setup {
     int32_t *d_tr_sub = nullptr, *d_tr_i = nullptr, *d_lts_col = nullptr;
     int64_t* d_lts_ptr = nullptr;
     void* d_lts_val = nullptr;
-    int32_t *d_us_sub = nullptr, *d_us_r = nullptr, *d_ust_col = nullptr;
+    int32_t *d_us_sub = nullptr, *d_us_r = nullptr, *d_ust_col = nullptr, *d_uu = nullptr;
     int64_t* d_ust_ptr = nullptr;
     void* d_ust_val = nullptr;
     void *d_linv = nullptr, *d_uinv = nullptr;
     bool need_gflags = false;
-    std::vector<int> tr_first_h, us_first_h;  // per subdomain, nsub+1 entries
+    std::vector<int> tr_first_h, us_first_h, uu_first_h;  // per subdomain, nsub+1 entries
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
     int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0,
         opt_tpr = 0;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     std::atomic<int> opt_spin_limit{S2L_SPIN_LIMIT};  // polls of a sweep wait before it gives up
+    std::atomic<int> opt_spin_sleep{S2L_SPIN_SLEEP_NS};  // back-off of a sweep poll that found a column not ready
     double opt_pivot_tol = 1e-6;  // refactorization of LU factors: largest multiplier 1 / pivot_tol
     int opt_amg_single = 0;       // AMG local solvers in single precision (--local-precision single)
     // statistics
@@ -670,7 +671,8 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
     // about four entries per lane, at most gmax), sorted by width and length so a task's rows
     // are alike.  Each task goes to the warp with the least work so far; a warp's tasks stay in
     // level order.  Entries are stored lane-interleaved: chunk c of a task holds, for lane
-    // k * G + j, entry c * G + j of its row k (column -1 and value 0 past the row's end), with
+    // k * G + j, entry c * G + j of its row k (column T, the sentinel slot, and value 0 past the
+    // row's end), with
     // 1/diag folded into the values (the sweep scales the right-hand side by 1/diag too).
     auto width = [&](int len) {
         int g = 1;
@@ -721,7 +723,7 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
             for (int c = 0; c < C; ++c)
                 for (int lane = 0; lane < 32; ++lane) {
                     const int k = lane / G, j = lane % G, e = c * G + j;
-                    int32_t colv = -1, sv = -1;
+                    int32_t colv = T, sv = -1;
                     double v = 0.0;
                     if (k < R) {
                         const int p = items[i0 + k].second;
@@ -740,7 +742,7 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
                             }
                         }
                     }
-                    if (colv < 0) ++out.pad;
+                    if (colv == T) ++out.pad;
                     W.col.push_back(colv);
                     W.val.push_back(v);
                     if (track) W.src.push_back(sv);
@@ -811,6 +813,15 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
 // smaller rows only) and bytes what one local solve reads for this split: sparse entries of L and
 // U, coupling entries L(T:n, 0:T) and U(0:T, T:n), and the two dense triangles of the tail.  The
 // tail is at most tail_max rows; the sweep's shared memory must hold T rows.
+// Lanes of the U-coupling kernel for a row of `len` entries: about four entries per lane, a power
+// of two, 1 to 32 (a warp takes 32 / lanes rows of about that length)
+int coupling_lanes(int len)
+{
+    int g = 1;
+    while (g < 32 && 4 * g < len) g <<= 1;
+    return g;
+}
+
 int choose_tail(const HostCsr& L, const HostCsr& U, int n, const s2l_tail_model& tm)
 {
     if (tm.force_rows > 0) return std::max(1, n - std::min(tm.force_rows, n - 1));
@@ -1144,6 +1155,7 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
     a.ust_ptr = s->d_ust_ptr;
     a.ust_col = s->d_ust_col;
     a.ust_val = (const Real*)s->d_ust_val;
+    a.uu = s->d_uu;
     a.linv = (const Real*)s->d_linv;
     a.uinv = (const Real*)s->d_uinv;
     a.gout = s->d_gout;
@@ -1156,6 +1168,7 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
     a.KC = 1;
     a.nloc = s->nloc;
     a.spin_limit = s->opt_spin_limit.load();
+    a.spin_sleep_ns = s->opt_spin_sleep.load();
     return a;
 }
 
@@ -1231,15 +1244,15 @@ int run_local_solve(s2l_work* w, const double* in, const double* base, double* o
     if (s->amgd.on) return amg_local_solve(w, in, base, out, mode, only_sub, local_in);
     const int nb = only_sub >= 0 ? 1 : s->nsub;
     int32_t* sub_list = nullptr;
-    int tr0 = 0, trn = s->tr_first_h[s->nsub], us0 = 0, usn = s->us_first_h[s->nsub];
+    int tr0 = 0, trn = s->tr_first_h[s->nsub], us0 = 0, usn = s->uu_first_h[s->nsub];
     if (only_sub >= 0) {
         sub_list = reinterpret_cast<int32_t*>(w->d_red + 500);  // scratch slot for one index
         int32_t v = only_sub;
         CUDA_OK(w, cudaMemcpyAsync(sub_list, &v, sizeof(v), cudaMemcpyHostToDevice, w->stream));
         tr0 = s->tr_first_h[only_sub];
         trn = s->tr_first_h[only_sub + 1] - tr0;
-        us0 = s->us_first_h[only_sub];
-        usn = s->us_first_h[only_sub + 1] - us0;
+        us0 = s->uu_first_h[only_sub];
+        usn = s->uu_first_h[only_sub + 1] - us0;
     }
     cudaError_t e;
     int launched = 0;
@@ -1396,7 +1409,8 @@ int block_width_best(s2l_setup* s)
 size_t sweep_smem(const s2l_setup* s, int kc)
 {
     const size_t rs = s->real == S2L_REAL_F32 ? 4 : 8;
-    return ((((size_t)s->max_T * kc * rs) + 15) & ~(size_t)15) + (((size_t)s->max_T + 15) & ~(size_t)15);
+    const size_t slots = (size_t)s->max_T + 1;  // the sparse rows and the sentinel slot of the padding
+    return (((slots * kc * rs) + 15) & ~(size_t)15) + ((slots + 15) & ~(size_t)15);
 }
 
 // local solves of every subdomain for K columns: (mode 0) out[owned] (+ base), (mode 1) ylocal
@@ -1420,7 +1434,7 @@ int local_solve_block_t(s2l_work* w, int K, const double* in, const double* base
     const size_t smem = B.gflags ? 0 : sweep_smem(s, a.KC);
     int launched = 0;
     const cudaError_t e = launch_local_solve<Real>(w->stream, a, s->nsub, smem, 0, s->tr_first_h[s->nsub], 0,
-                                                   s->us_first_h[s->nsub], &launched);
+                                                   s->uu_first_h[s->nsub], &launched);
     w->launches += launched;
     if (e != cudaSuccess) return w->fail(S2L_ERR_CUDA, std::string("block local_solve launch: ") + cudaGetErrorString(e));
     return S2L_OK;
@@ -2446,13 +2460,14 @@ int s2l_gpu_setup_end(s2l_setup* s)
     std::vector<int32_t> sw_bfirst[2], sw_bslot[2];
     std::vector<int64_t> sw_boff[2] = {{0}, {0}}, sw_bioff[2] = {{0}, {0}};
     std::vector<double> sw_binv[2];
-    std::vector<int32_t> tr_sub, tr_i, lts_col, us_sub, us_r, ust_col;
+    std::vector<int32_t> tr_sub, tr_i, lts_col, us_sub, us_r, ust_col, uu;
     std::vector<int64_t> lts_ptr(1, 0), ust_ptr(1, 0);
     std::vector<double> lts_val, ust_val;
     std::vector<std::vector<double>> Ltt(nsub), Utt(nsub);
     std::vector<int64_t> d_off(nsub + 1, 0);
     s->tr_first_h.assign(nsub + 1, 0);
     s->us_first_h.assign(nsub + 1, 0);
+    s->uu_first_h.assign(nsub + 1, 0);
     double bytes = 0.0;
     int max_T = 0, max_nl = 0;
     int64_t sparse_nnz = 0;
@@ -2521,6 +2536,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
         if (h.amg) {  // AMG local solver: the local space in natural order, no sweeps or tails
             s->tr_first_h[i] = (int)tr_sub.size();
             s->us_first_h[i] = (int)us_sub.size();
+            s->uu_first_h[i] = (int)uu.size();
             d_off[i + 1] = d_off[i];
             DevSub d{};
             d.begin = h.begin;
@@ -2734,24 +2750,39 @@ int s2l_gpu_setup_end(s2l_setup* s)
                 if (Utt[i][(size_t)k * sz + k] == 0.0 || Ltt[i][(size_t)k * sz + k] == 0.0)
                     return s->fail(S2L_ERR_NUMERIC, "subdomain " + std::to_string(i) + ": zero pivot in the dense tail");
         }
-        // U coupling of the sparse rows: the target is the row's forward slot (ybuf keeps forward order)
+        // U coupling of the sparse rows: the target is the row's forward slot (ybuf keeps forward order).
+        // The rows are stored longest first and grouped into units of one warp: a unit holds rows of
+        // about the same length, each taken by the lanes its length needs (coupling_lanes)
         s->us_first_h[i] = (int)us_sub.size();
-        if (sz > 0)
+        s->uu_first_h[i] = (int)uu.size();
+        if (sz > 0) {
+            std::vector<std::pair<int, int>> rows;  // (tail entries, row)
             for (int r = 0; r < T; ++r) {
-                bool any = false;
+                int cnt = 0;
+                for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e) cnt += U.ci[e] >= T;
+                if (cnt) rows.emplace_back(cnt, r);
+            }
+            std::stable_sort(rows.begin(), rows.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+                return x.first > y.first;
+            });
+            const int q0 = (int)us_sub.size();
+            for (const auto& pr : rows) {
+                const int r = pr.second;
                 for (int64_t e = U.rp[r]; e < U.rp[r + 1]; ++e)
                     if (U.ci[e] >= T) {
                         ust_col.push_back((int32_t)(loc + U.ci[e]));  // local-space index of the tail row
                         ust_val.push_back(U.v[e]);
                         if (rfon) rf_ust.push_back(fb + (llt ? P.find(U.ci[e], r) : P.find(r, U.ci[e])));
-                        any = true;
                     }
-                if (any) {
-                    us_sub.push_back(i);
-                    us_r.push_back(sl.pos[r]);
-                    ust_ptr.push_back((int64_t)ust_col.size());
-                }
+                us_sub.push_back(i);
+                us_r.push_back(sl.pos[r]);
+                ust_ptr.push_back((int64_t)ust_col.size());
             }
+            for (size_t k = 0; k < rows.size();) {
+                uu.push_back(q0 + (int)k);
+                k += std::min(rows.size() - k, (size_t)(32 / coupling_lanes(rows[k].first)));
+            }
+        }
         d_off[i + 1] = d_off[i] + (int64_t)sz * sz;
         DevSub d{};
         d.begin = h.begin;
@@ -2788,6 +2819,8 @@ int s2l_gpu_setup_end(s2l_setup* s)
     }
     s->tr_first_h[nsub] = (int)tr_sub.size();
     s->us_first_h[nsub] = (int)us_sub.size();
+    s->uu_first_h[nsub] = (int)uu.size();
+    uu.push_back((int32_t)us_sub.size());  // the end of the last unit
     s->nloc = loc;
     s->st_sparse_nnz = sparse_nnz;
     s->st_coupling_nnz = (int64_t)lts_col.size() + (int64_t)ust_col.size();
@@ -2833,6 +2866,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
     RET_IF(upload(s, &s->d_us_r, us_r));
     RET_IF(upload(s, &s->d_ust_ptr, ust_ptr));
     RET_IF(upload(s, &s->d_ust_col, ust_col));
+    RET_IF(upload(s, &s->d_uu, uu));
     if (s->real == S2L_REAL_F32) {
         RET_IF(upload_real<float>(s, &s->d_lts_val, lts_val));
         RET_IF(upload_real<float>(s, &s->d_ust_val, ust_val));
@@ -3110,8 +3144,9 @@ int s2l_gpu_setup_end(s2l_setup* s)
         R.on = true;
     }
 
-    // sweep shared memory: x (T values) + one ready byte per row
-    const size_t smem = ((((size_t)max_T * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15);
+    // sweep shared memory: x (T values and the sentinel slot) + one ready byte per slot
+    const size_t slots = (size_t)max_T + 1;
+    const size_t smem = (((slots * rs) + 15) & ~(size_t)15) + ((slots + 15) & ~(size_t)15);
     const size_t smem_cap = S2L_SWEEP_SMEM_CAP;
     if (smem <= smem_cap) {
         s->smem_bytes = smem;
@@ -3124,7 +3159,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
     s->kc_max = 1;
     if (s->smem_bytes > 0)
         for (int kc = 2; kc <= 4; kc *= 2)
-            if (((((size_t)max_T * kc * rs) + 15) & ~(size_t)15) + (((size_t)max_T + 15) & ~(size_t)15) <= smem_cap)
+            if ((((slots * kc * rs) + 15) & ~(size_t)15) + ((slots + 15) & ~(size_t)15) <= smem_cap)
                 s->kc_max = kc;
     CUDA_OK(s, cudaStreamSynchronize(s->setup_stream));
     // host staging no longer needed
@@ -3478,6 +3513,11 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
     if (n == "spin_limit") {  // read at every launch: may change after setup_end
         if (!(value >= 1.0 && value <= 2147483647.0)) return s->fail(S2L_ERR_BADARG, "spin_limit must be in [1, 2^31)");
         s->opt_spin_limit.store((int)value);
+        return S2L_OK;
+    }
+    if (n == "spin_sleep_ns") {  // read at every launch, like spin_limit
+        if (!(value >= 0.0 && value <= 1000000.0)) return s->fail(S2L_ERR_BADARG, "spin_sleep_ns must be in [0, 1e6]");
+        s->opt_spin_sleep.store((int)value);
         return S2L_OK;
     }
     if (s->ended) return s->fail(S2L_ERR_STATE, "setup_option after setup_end");

@@ -69,7 +69,18 @@ __global__ void __launch_bounds__(S2L_BS_VEC) spmv_kernel(int64_t n, const int32
         double s = 0.0;
         if (row < n) {
             const int e1 = rp[row + 1];
-            for (int e = rp[row] + lane; e < e1; e += TPR) s += v[e] * __ldg(x + ci[e]);
+            int e = rp[row] + lane;
+            // four entries of the lane at once (loads, then gathers), added in entry order
+            for (; e + 3 * TPR < e1; e += 4 * TPR) {
+                const int c0 = ci[e], c1 = ci[e + TPR], c2 = ci[e + 2 * TPR], c3 = ci[e + 3 * TPR];
+                const double a0 = v[e], a1 = v[e + TPR], a2 = v[e + 2 * TPR], a3 = v[e + 3 * TPR];
+                const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+                s += a0 * x0;
+                s += a1 * x1;
+                s += a2 * x2;
+                s += a3 * x3;
+            }
+            for (; e < e1; e += TPR) s += v[e] * __ldg(x + ci[e]);
         }
 #pragma unroll
         for (int o = TPR / 2; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
@@ -304,6 +315,56 @@ __global__ void __launch_bounds__(256) bicg_x_kernel(int64_t n, double* __restri
 // so a row ends with x = b - sum, one write and its flag.  Every wait is bounded: after
 // a.spin_limit polls (the setup option "spin_limit", S2L_SPIN_LIMIT by default) the CTA raises
 // *err and all warps leave.
+// One batch of N chunks of a sweep task for one lane: its N entries (column slot, value) loaded
+// together, a wait until all N columns are ready (their flags polled together, one round trip
+// per poll), then the N products added in entry order.  With x in shared memory a padding entry
+// points at the sentinel slot T (ready, x = 0, value 0), so the batch has no branch per entry; in
+// the global-flag layout it is skipped (column >= T).  Returns true when the sweep gave up.
+template <typename Real, bool SMEM, int KC, int N>
+__device__ __forceinline__ bool sweep_batch(const int32_t* __restrict__ colp, const Real* __restrict__ valp,
+                                            volatile const uint8_t* flag, volatile const Real* x, int xstride,
+                                            int T, Real (&acc)[KC], volatile int& abort_flag, int* err,
+                                            int spin_limit, int sleep_ns)
+{
+    int lc[N];
+    Real lv[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        lc[q] = colp[q * 32];
+        lv[q] = valp[q * 32];
+    }
+    int spin = 0;
+    for (;;) {
+        int ready = 1;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            if (SMEM)
+                ready &= (int)flag[lc[q]];
+            else if (lc[q] < T)
+                ready &= (int)flag[lc[q]];
+        }
+        if (ready) break;
+        if ((++spin & 31) == 0) {  // the abort word and the limit, every 32 polls
+            if (abort_flag) return true;
+            if (spin > spin_limit) {
+                abort_flag = 1;
+                atomicExch(err, 1);
+                return true;
+            }
+        }
+        // a waiting lane pauses, leaving the issue slots to the warps that compute its columns
+        if (sleep_ns > 0) __nanosleep((unsigned)sleep_ns);
+    }
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        if (SMEM || lc[q] < T) {
+#pragma unroll
+            for (int r = 0; r < KC; ++r) acc[r] += lv[q] * x[lc[q] * xstride + r];
+        }
+    }
+    return false;
+}
+
 template <typename Real, bool SMEM, bool FWD, int KC>
 __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolveArgs<Real> a)
 {
@@ -328,7 +389,7 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     volatile uint8_t* flag;
     int xstride;  // x of slot k, column r: xs[k * xstride + r]
     if (SMEM) {
-        const size_t off1 = (((size_t)T * KC * sizeof(Real)) + 15) & ~(size_t)15;
+        const size_t off1 = (((size_t)(T + 1) * KC * sizeof(Real)) + 15) & ~(size_t)15;  // T slots + the sentinel
         xs = reinterpret_cast<Real*>(smem_raw);
         flag = reinterpret_cast<volatile uint8_t*>(smem_raw + off1);
         xstride = KC;
@@ -351,6 +412,11 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
             xs[k * xstride + r] = b * d;
         }
         flag[k] = 0;
+    }
+    if (SMEM && threadIdx.x == 0) {  // the sentinel slot T of the padding entries: ready, x = 0
+#pragma unroll
+        for (int r = 0; r < KC; ++r) xs[T * xstride + r] = Real(0);
+        flag[T] = 1;
     }
     __syncthreads();
     // chain blocks: right-hand side of block B becomes W^-1 b(B) (W^-1 packed lower, solve order);
@@ -403,19 +469,7 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
         Real acc[KC];
 #pragma unroll
         for (int r = 0; r < KC; ++r) acc[r] = Real(0);
-        for (int c0 = 0; c0 < C; c0 += Q) {  // C is the same for the whole warp
-            int lc[Q];
-            Real lv[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                lc[q] = -1;
-                lv[q] = Real(0);
-                if (c0 + q < C) {
-                    const int64_t e = eo + (int64_t)(c0 + q) * 32 + lane;
-                    lc[q] = F.col[e];
-                    lv[q] = F.val[e];
-                }
-            }
+        for (int c0 = 0; c0 < C && !dead; c0 += Q) {  // C is the same for the whole warp
             // hint the next batch into L2: lane q < Q takes chunk q of it (lines of 128 bytes)
             if (lane < Q && c0 + Q + lane < C) {
                 const int64_t e = eo + (int64_t)(c0 + Q + lane) * 32;
@@ -423,26 +477,27 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e));
                 if (sizeof(Real) == 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(F.val + e + 16));
             }
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int c = lc[q];
-                if (c >= 0 && !dead) {
-                    int spin = 0;
-                    while (flag[c] == 0) {  // the abort word and the limit are checked every 32 polls
-                        if ((++spin & 31) == 0) {
-                            if (abort_flag) { dead = true; break; }
-                            if (spin > a.spin_limit) {
-                                abort_flag = 1;
-                                atomicExch(a.err, 1);
-                                dead = true;
-                                break;
-                            }
-                        }
-                        if (S2L_SPIN_SLEEP_NS > 0 && spin > 8) __nanosleep(S2L_SPIN_SLEEP_NS);
-                    }
-#pragma unroll
-                    for (int r = 0; r < KC; ++r) acc[r] += lv[q] * x[c * xstride + r];
-                }
+            const int64_t e = eo + (int64_t)c0 * 32 + lane;
+            const int32_t* cp = F.col + e;
+            const Real* vp = F.val + e;
+            // a batch of exactly the chunks left (at most Q): no work for absent chunks
+            switch (min(C - c0, Q)) {
+#define S2L_SWEEP_BATCH(n_)                                                                                        \
+    case n_:                                                                                                   \
+        if constexpr (n_ <= Q)                                                                                 \
+            dead = sweep_batch<Real, SMEM, KC, n_>(cp, vp, flag, x, xstride, T, acc, abort_flag, a.err,         \
+                                                   a.spin_limit, a.spin_sleep_ns);                             \
+        break;
+                S2L_SWEEP_BATCH(1)
+                S2L_SWEEP_BATCH(2)
+                S2L_SWEEP_BATCH(3)
+                S2L_SWEEP_BATCH(4)
+                S2L_SWEEP_BATCH(5)
+                S2L_SWEEP_BATCH(6)
+                S2L_SWEEP_BATCH(7)
+                S2L_SWEEP_BATCH(8)
+#undef S2L_SWEEP_BATCH
+            default: break;
             }
         }
         eo += (int64_t)C * 32;
@@ -663,46 +718,51 @@ __global__ void __launch_bounds__(256) tail_gemv_kernel(const LocalSolveArgs<Rea
 }
 
 // Backward coupling: y(r) -= U(r, T:n) x(T:n) for the sparse rows that have tail columns, K columns.
-// These rows are short (a sparse row's entries in the tail columns), so a warp takes 32 of them
-// (chunk mode): their entries are contiguous, loaded with coalesced loads, multiplied by the
-// gathered tail values (columns stored as local-space indices) and left in shared memory; lane j
-// then adds row j's products in entry order.
+// One warp per unit of rows of about the same length (stored longest first): with n rows in the
+// unit, G = 32 / n lanes (a power of two) take each row, each lane with four entries in flight,
+// and the G partial sums of a row are added by a butterfly within its lane group.
 template <typename Real, int K>
-__global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveArgs<Real> a, int q0, int count)
+__global__ void __launch_bounds__(256) sparse_coupling_kernel(const LocalSolveArgs<Real> a, int u0, int ucount)
 {
-    constexpr int CAP = 512 / K;  // entries of a piece
-    __shared__ Real prod[8][CAP * K];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Real* wp = prod[warp];
-    const int nchunks = (count + 31) / 32;
-    for (int ch = blockIdx.x * 8 + warp; ch < nchunks; ch += gridDim.x * 8) {
-        const int qa = q0 + ch * 32, qb = min(qa + 32, q0 + count), q = qa + lane;
-        const int64_t e_lo = a.ust_ptr[qa], e_hi = a.ust_ptr[qb];
-        const int64_t my0 = q < qb ? a.ust_ptr[q] : e_hi, my1 = q < qb ? a.ust_ptr[q + 1] : e_hi;
-        Real acc[K];
+    const int u = u0 + blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (u >= u0 + ucount) return;
+    const int qa = a.uu[u], n = a.uu[u + 1] - qa;  // 1 <= n <= 32
+    int lg = 5;
+    while ((n << lg) > 32) --lg;  // G = 2^lg lanes per row, the largest with G n <= 32
+    const int G = 1 << lg, ri = lane >> lg, sl = lane & (G - 1);
+    const bool valid = ri < n;
+    const int q = qa + (valid ? ri : 0);
+    int64_t e = a.ust_ptr[q] + sl;
+    const int64_t e1 = valid ? a.ust_ptr[q + 1] : e;
+    Real acc[K];
 #pragma unroll
-        for (int r = 0; r < K; ++r) acc[r] = Real(0);
-        for (int64_t base = e_lo; base < e_hi; base += CAP) {
-            const int cnt = (int)(e_hi - base < CAP ? e_hi - base : CAP);
-            for (int e = lane; e < cnt; e += 32) {
-                const Real v = a.ust_val[base + e];
-                Real x[K];
-                load_k<Real, K>(a.ybuf + (int64_t)a.ust_col[base + e] * K, x);
+    for (int r = 0; r < K; ++r) acc[r] = Real(0);
+    for (; e + 3 * G < e1; e += 4 * G) {
+        const int c0 = a.ust_col[e], c1 = a.ust_col[e + G], c2 = a.ust_col[e + 2 * G], c3 = a.ust_col[e + 3 * G];
+        const Real v0 = a.ust_val[e], v1 = a.ust_val[e + G], v2 = a.ust_val[e + 2 * G], v3 = a.ust_val[e + 3 * G];
+        Real x0[K], x1[K], x2[K], x3[K];
+        load_k<Real, K>(a.ybuf + (int64_t)c0 * K, x0);
+        load_k<Real, K>(a.ybuf + (int64_t)c1 * K, x1);
+        load_k<Real, K>(a.ybuf + (int64_t)c2 * K, x2);
+        load_k<Real, K>(a.ybuf + (int64_t)c3 * K, x3);
 #pragma unroll
-                for (int r = 0; r < K; ++r) wp[e * K + r] = v * x[r];
-            }
-            __syncwarp();
-            const int64_t s0 = (my0 > base ? my0 : base) - base, s1 = (my1 < base + cnt ? my1 : base + cnt) - base;
-            for (int64_t e = s0; e < s1; ++e)
+        for (int r = 0; r < K; ++r) acc[r] += (v0 * x0[r] + v1 * x1[r]) + (v2 * x2[r] + v3 * x3[r]);
+    }
+    for (; e < e1; e += G) {
+        const Real v0 = a.ust_val[e];
+        Real x0[K];
+        load_k<Real, K>(a.ybuf + (int64_t)a.ust_col[e] * K, x0);
 #pragma unroll
-                for (int r = 0; r < K; ++r) acc[r] += wp[e * K + r];
-            __syncwarp();
-        }
-        if (q < qb) {
-            const int64_t o = (a.subs[a.us_sub[q]].loc_off + a.us_r[q]) * K;
+        for (int r = 0; r < K; ++r) acc[r] += v0 * x0[r];
+    }
 #pragma unroll
-            for (int r = 0; r < K; ++r) a.ybuf[o + r] -= acc[r];
-        }
+    for (int r = 0; r < K; ++r)
+        for (int o = G >> 1; o; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+    if (valid && sl == 0) {
+        const int64_t o = (a.subs[a.us_sub[q]].loc_off + a.us_r[q]) * K;
+#pragma unroll
+        for (int r = 0; r < K; ++r) a.ybuf[o + r] -= acc[r];
     }
 }
 
@@ -776,11 +836,25 @@ __global__ void __launch_bounds__(S2L_BS_VEC) spmv_block_kernel(int64_t n, const
         for (int r = 0; r < K; ++r) acc[r] = 0.0;
         if (row < n) {
             const int e1 = rp[row + 1];
-            for (int e = rp[row] + lane; e < e1; e += TPR) {
-                const double a = v[e];
-                const double* x = X + (int64_t)ci[e] * K;
+            int e = rp[row] + lane;
+            // two entries of the lane at once (loads, then gathers), added in entry order
+            for (; e + TPR < e1; e += 2 * TPR) {
+                const int c0 = ci[e], c1 = ci[e + TPR];
+                const double a0 = v[e], a1 = v[e + TPR];
+                double x0[K], x1[K];
+                load_k<double, K>(X + (int64_t)c0 * K, x0);
+                load_k<double, K>(X + (int64_t)c1 * K, x1);
 #pragma unroll
-                for (int r = 0; r < K; ++r) acc[r] += a * x[r];
+                for (int r = 0; r < K; ++r) acc[r] += a0 * x0[r];
+#pragma unroll
+                for (int r = 0; r < K; ++r) acc[r] += a1 * x1[r];
+            }
+            if (e < e1) {
+                const double a0 = v[e];
+                double x0[K];
+                load_k<double, K>(X + (int64_t)ci[e] * K, x0);
+#pragma unroll
+                for (int r = 0; r < K; ++r) acc[r] += a0 * x0[r];
             }
         }
 #pragma unroll
@@ -846,12 +920,27 @@ __global__ void __launch_bounds__(S2L_BS_VEC) spmv_chunk_kernel(int64_t n, const
         for (int r = 0; r < K; ++r) acc[r] = 0.0;
         for (int base = e_lo; base < e_hi; base += CAP) {
             const int cnt = e_hi - base < CAP ? e_hi - base : CAP;
-            for (int e = lane; e < cnt; e += 32) {
-                const double a = v[base + e];
-                double x[K];
-                load_k<double, K>(X + (int64_t)ci[base + e] * K, x);
+            // U entries per lane at once: all their loads, then all their gathers, are in flight together
+            constexpr int U = K == 1 ? 8 : 4;
+            for (int e0 = lane; e0 < cnt; e0 += 32 * U) {
+                int c[U];
+                double a[U];
 #pragma unroll
-                for (int r = 0; r < K; ++r) wp[e * K + r] = a * x[r];
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + 32 * u;
+                    c[u] = e < cnt ? ci[base + e] : 0;
+                    a[u] = e < cnt ? v[base + e] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + 32 * u;
+                    if (e < cnt) {
+                        double x[K];
+                        load_k<double, K>(X + (int64_t)c[u] * K, x);
+#pragma unroll
+                        for (int r = 0; r < K; ++r) wp[e * K + r] = a[u] * x[r];
+                    }
+                }
             }
             __syncwarp();
             const int s0 = (my0 > base ? my0 : base) - base, s1 = (my1 < base + cnt ? my1 : base + cnt) - base;
@@ -1480,7 +1569,7 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
 
 template <typename Real, int KC, int K>
 cudaError_t launch_local_solve_k(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
-                                 int tr_count, int us_first, int us_count, int* launches)
+                                 int tr_count, int uu_first, int uu_count, int* launches)
 {
     cudaError_t e;
     const int grid = nblocks * (K / KC);
@@ -1506,8 +1595,8 @@ cudaError_t launch_local_solve_k(cudaStream_t st, const LocalSolveArgs<Real>& a,
         tail_gemv_kernel<Real, false, K><<<g, 256, 0, st>>>(a, a.uinv, a.xbuf, a.ybuf, tr_first, tr_count);
         nl += 3;
     }
-    if (us_count > 0) {
-        sparse_coupling_kernel<Real, K><<<(us_count + 255) / 256, 256, 0, st>>>(a, us_first, us_count);
+    if (uu_count > 0) {
+        sparse_coupling_kernel<Real, K><<<(uu_count + 7) / 8, 256, 0, st>>>(a, uu_first, uu_count);
         nl += 1;
     }
     if (smem > 0)
@@ -1520,13 +1609,13 @@ cudaError_t launch_local_solve_k(cudaStream_t st, const LocalSolveArgs<Real>& a,
 
 template <typename Real>
 cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem, int tr_first,
-                               int tr_count, int us_first, int us_count, int* launches)
+                               int tr_count, int uu_first, int uu_count, int* launches)
 {
     // (KC, K): right-hand sides per sweep CTA and in all; the setup's shared memory fixes KC
     const int K = a.K, KC = smem > 0 ? a.KC : 1;
 #define S2L_LS(KC_, K_)                                                                                         \
     if (KC == KC_ && K == K_)                                                                                  \
-    return launch_local_solve_k<Real, KC_, K_>(st, a, nblocks, smem, tr_first, tr_count, us_first, us_count, \
+    return launch_local_solve_k<Real, KC_, K_>(st, a, nblocks, smem, tr_first, tr_count, uu_first, uu_count, \
                                                launches)
     S2L_LS(1, 1);
     S2L_LS(1, 2);

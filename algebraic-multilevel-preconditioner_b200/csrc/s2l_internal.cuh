@@ -32,10 +32,10 @@
 #define S2L_SWEEP_SMEM_CAP (227 * 1024 - 64)  // dynamic shared memory of a sweep CTA, at most
 #define S2L_ADMIT_WAIT_S 600   // longest wait of a call for a free workspace when the HBM budget is full
 #ifndef S2L_SPIN_SLEEP_NS
-#define S2L_SPIN_SLEEP_NS 0   // back-off of a sweep poll after its first 8 (ns; 0 = poll without pause)
+#define S2L_SPIN_SLEEP_NS 0   // pause of a sweep warp after a poll that found a column not ready (ns; 0 = none)
 #endif
-#define S2L_SPIN_LIMIT (1 << 24)
-#define S2L_GS_SMEM_CAP (224 * 1024)  // shared memory of a Gauss-Seidel sweep CTA (its subdomain's x)  // polls of one ready flag before a sweep gives up (error 1)
+#define S2L_SPIN_LIMIT (1 << 24)  // polls of one ready flag before a sweep gives up (error 1)
+#define S2L_GS_SMEM_CAP (224 * 1024)  // shared memory of a Gauss-Seidel sweep CTA (its subdomain's x)
 
 struct DevSub {
     int64_t begin;      // first owned global row
@@ -90,12 +90,14 @@ struct LocalSolveArgs {
     const int32_t* lts_col;
     const Real* lts_val;
     // sparse rows with U(r, T:n) coupling: (sub, r) pairs and CSR (columns as local-space indices,
-    // loc_off + tail row, so a warp can gather for rows of several subdomains)
+    // loc_off + tail row), longest rows first within a subdomain; unit u (one warp) holds the rows
+    // uu[u] .. uu[u + 1] - 1, 32 / (its row count) lanes per row
     const int32_t* us_sub;
     const int32_t* us_r;
     const int64_t* ust_ptr;
     const int32_t* ust_col;
     const Real* ust_val;
+    const int32_t* uu;
     const Real* linv;          // inverse tails, row-major per subdomain
     const Real* uinv;
     const int32_t* gather;     // slot k -> index into `in` (global gather, or perm_in for a local input)
@@ -116,6 +118,7 @@ struct LocalSolveArgs {
     int KC;
     int64_t nloc;              // local-space size (stride of the per-column-group ready flags)
     int spin_limit;            // polls of one ready flag before a sweep gives up (S2L_SPIN_LIMIT by default)
+    int spin_sleep_ns;         // pause of a warp after a poll that found a column not ready (0: none)
 };
 
 // Numeric refactorization of every subdomain's factors on their kept patterns (s2l_gpu_refactor).
@@ -224,7 +227,7 @@ void launch_bicg_x(cudaStream_t st, int64_t n, double* x, const double* y, const
 // kernels (first, count); `launches` receives the number of kernels issued.
 template <typename Real>
 cudaError_t launch_local_solve(cudaStream_t st, const LocalSolveArgs<Real>& a, int nblocks, size_t smem_bytes,
-                               int tr_first, int tr_count, int us_first, int us_count, int* launches);
+                               int tr_first, int tr_count, int uu_first, int uu_count, int* launches);
 
 void launch_combine(cudaStream_t st, int64_t n, const int64_t* cp_ptr, const int32_t* cp_pos, const double* cp_w,
                     const double* ylocal, const double* base, double* out);

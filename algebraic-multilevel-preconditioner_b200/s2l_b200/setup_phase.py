@@ -411,8 +411,33 @@ def build_subdomain_structure(A: sp.csr_matrix, ownership: np.ndarray, overlap: 
     return out
 
 
+_THREAD_LIMIT = None
+
+
+def _one_thread_worker():
+    """Initializer of a setup worker process: one BLAS / OpenMP thread (the pool's processes are
+    the parallelism; a worker may be started at any time, whatever the parent's environment)."""
+    global _THREAD_LIMIT
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    try:
+        from threadpoolctl import threadpool_limits
+        _THREAD_LIMIT = threadpool_limits(limits=1)  # kept: the limit holds while the object lives
+    except ImportError:
+        pass
+
+
+def worker_pool(workers: int | None = None) -> ProcessPoolExecutor:
+    """A pool of spawned worker processes for the per-subdomain setup work (factorization and
+    eigenproblem), one BLAS thread each; pass it to build_setup(pool=...) to set up several matrices
+    without starting new processes for each."""
+    return ProcessPoolExecutor(max_workers=workers or os.cpu_count() or 1, mp_context=mp.get_context("spawn"),
+                               initializer=_one_thread_worker)
+
+
 def build_setup(A_orig: sp.csr_matrix, b_orig: np.ndarray, part: np.ndarray, nsub: int, opts: SchwarzOptions,
-                symmetric: bool, workers: int | None = None, description: str = "") -> Setup:
+                symmetric: bool, workers: int | None = None, description: str = "",
+                pool: ProcessPoolExecutor | None = None) -> Setup:
     ownership, n2o, _ = partmod.renumber(part, nsub)
     A = partmod.permute(A_orig.tocsr(), n2o)
     b = np.asarray(b_orig, dtype=np.float64)[n2o]
@@ -429,7 +454,12 @@ def build_setup(A_orig: sp.csr_matrix, b_orig: np.ndarray, part: np.ndarray, nsu
         jobs.append((Aii, Atil, D, opts, symmetric, want_coarse))
     if workers is None:
         workers = min(len(jobs), os.cpu_count() or 1)
-    if workers > 1 and len(jobs) > 1:
+    if pool is not None and len(jobs) > 1:
+        # largest subdomains first, so the last jobs to finish are short ones
+        order = sorted(range(len(jobs)), key=lambda i: -jobs[i][0].nnz)
+        done = dict(zip(order, pool.map(_subdomain_work, [jobs[i] for i in order], chunksize=1)))
+        results = [done[i] for i in range(len(jobs))]
+    elif workers > 1 and len(jobs) > 1:
         saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
         for k in saved:
             os.environ[k] = "1"

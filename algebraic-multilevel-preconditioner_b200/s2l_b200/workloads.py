@@ -107,14 +107,15 @@ def make_partition(w: Workload, prob) -> np.ndarray:
     return np.repeat(part, per_cell) if per_cell > 1 else part
 
 
-def build(w: Workload, workers=None, use_cache=True):
-    """Problem + partition + setup (cached under $S2L_CACHE_DIR when set)."""
+def build(w: Workload, workers=None, use_cache=True, pool=None):
+    """Problem + partition + setup (cached under $S2L_CACHE_DIR when set); `pool`: a process pool of
+    setup_phase.worker_pool for the per-subdomain work."""
     def make():
         prob = make_problem(w)
         part = make_partition(w, prob)
         b = random_rhs(prob.n, w.seed)
         st = build_setup(prob.A, b, part, w.nsub, w.opts, prob.symmetric, workers=workers,
-                         description=prob.description)
+                         description=prob.description, pool=pool)
         st.stats["part"] = part
         return st
     if use_cache:

@@ -52,6 +52,7 @@ for _p in (REPO, PKG):
         sys.path.insert(0, _p)
 
 METRIC = "solve time to FP64 residual 1e-8 (mixed/batched vs plain FP64 GPU); p50/p99 latency"
+POOL = None  # the run's setup worker processes (setup_phase.worker_pool), on one GPU
 _T0 = time.time()
 
 
@@ -419,15 +420,19 @@ def serve_form(local, st, kw, n_req, rate, bpool, xpool, workers=8, options=None
 def run_ours(a):
     reps = Replicas()
     rank, world, local = reps.rank, reps.world, reps.local
-    os.environ.setdefault("S2L_CACHE_DIR", os.path.join(REPO, "_cache"))
+    if world > 1:  # rank 0 sets the main workload up, the other ranks load its pickled copy
+        os.environ.setdefault("S2L_CACHE_DIR", os.path.join(REPO, "_cache"))
     import numpy as np
     from s2l_b200 import workloads as W
-    from s2l_b200.setup_phase import with_factor_precision
+    from s2l_b200.setup_phase import with_factor_precision, worker_pool
 
+    # one pool of setup worker processes for every host setup of the run (spawned before any CUDA call)
+    global POOL
+    POOL = worker_pool() if world == 1 else None
     wl = main_workload(a)
     wdesc = workload_desc(wl, a.overlap)
     t0 = time.time()
-    st = reps.rank0_first(lambda: W.build(wl)) if world > 1 else W.build(wl)
+    st = reps.rank0_first(lambda: W.build(wl)) if world > 1 else W.build(wl, pool=POOL)
     setup_s = time.time() - t0
     log(f"main workload host setup {setup_s:.1f} s (n = {st.n})")
     # ---- device (no CUDA call before the setup's process pool is done)
@@ -559,15 +564,19 @@ def run_ours(a):
     del b_dev, x_dev, st, st32, B_host, X64, b_pin, x_pin
 
     # ---- the other configurations (each builds, times and frees its own setups)
+    # (on one GPU: with replicas the line reports the headline form only)
     log("main workload done")
-    c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if a.overlap2 and a.overlap != 2 else None
+    one = world == 1
+    c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if one and a.overlap2 and a.overlap != 2 else None
     log("c2 overlap 2 done")
-    sequence = sequence_form(a, tm, ctx, stream, dev) if a.seq > 0 else None
+    sequence = sequence_form(a, tm, ctx, stream, dev) if one and a.seq > 0 else None
     log("sequence done")
-    c3 = c3_form(a, tm, ctx, stream, dev) if a.c3 > 0 else None
+    c3 = c3_form(a, tm, ctx, stream, dev) if one and a.c3 > 0 else None
     log("c3 done")
-    serving_mix = serve_mix(a, local) if a.serve_mix > 0 and world == 1 else None
+    serving_mix = serve_mix(a, local) if one and a.serve_mix > 0 else None
     log("serving mix done")
+    if POOL is not None:
+        POOL.shutdown()
 
     out = {
         "metric": METRIC,
@@ -728,7 +737,7 @@ def c2_overlap2_form(a, tm, ctx, stream, dev):
     from s2l_b200 import workloads as W
     w = W.bubbles3d(a.nx, a.nsub, nbubbles=a.nbubbles, overlap=2)
     t0 = time.time()
-    st = W.build(w)
+    st = W.build(w, pool=POOL)
     setup_s = time.time() - t0
     out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
     out.update(workload=workload_desc(w, 2), setup_s=round(setup_s, 1))
@@ -741,7 +750,7 @@ def c3_form(a, tm, ctx, stream, dev):
     from s2l_b200 import workloads as W
     w = W.convdiff3d(a.c3, a.c3_nsub, precision="double")
     t0 = time.time()
-    st = W.build(w)
+    st = W.build(w, pool=POOL)
     setup_s = time.time() - t0
     out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
     out.update(workload=f"convdiff3d {w.nx}^3 upwind convection-diffusion, {w.nsub} subdomains, overlap 1, nev 24, "
@@ -784,8 +793,11 @@ def sequence_form(a, tm, ctx, stream, dev):
             level = UpdateLevel.REBUILD if g is None else policy.decide(True)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
+            host_ms = None
             if level == UpdateLevel.REBUILD:
-                st = with_factor_precision(build_setup(A, B[0], part, w.nsub, w.opts, prob0.symmetric), "single")
+                st = with_factor_precision(build_setup(A, B[0], part, w.nsub, w.opts, prob0.symmetric, pool=POOL),
+                                           "single")
+                host_ms = (time.perf_counter() - t0) * 1e3
                 st.stats["part"] = part  # the renumbering of later matrices' values (sequence.values_in_setup_order)
                 if g is not None:
                     g.close()
@@ -813,8 +825,9 @@ def sequence_form(a, tm, ctx, stream, dev):
             At = sp.csr_matrix((st.A.data if level == UpdateLevel.REBUILD else vals, st.A.indices, st.A.indptr),
                                shape=st.A.shape)
             chk = max(float(np.linalg.norm(Bh[j] - At @ Xh[j]) / np.linalg.norm(Bh[j])) for j in range(k))
-            log(f"sequence step {step}: {level.name.lower()} {t_update * 1e3:.0f} ms, solve {t_solve * 1e3:.0f} ms")
-            steps.append({"step": step, "level": level.name.lower(), "update_ms": t_update * 1e3,
+            log(f"sequence step {step}: {level.name.lower()} {t_update * 1e3:.0f} ms"
+                + (f" (host setup {host_ms:.0f} ms)" if host_ms else "") + f", solve {t_solve * 1e3:.0f} ms")
+            steps.append({"step": step, "level": level.name.lower(), "update_ms": t_update * 1e3, "host_setup_ms": host_ms,
                           "solve_ms": t_solve * 1e3, "iterations_max": max(r["iterations"] for r in rq),
                           "converged": all(r["converged"] for r in rq), "true_rel_residual_host_check": chk})
     finally:
@@ -864,15 +877,15 @@ def serve_mix(a, device: int) -> dict:
         flex = w.opts.local_precision == "single"
         kws.append(dict(restart=w.restart, rtol=w.rtol, flexible=flex, strict=flex, history_cap=0))
         t0 = time.time()
-        st = W.build(w)
+        st = W.build(w, pool=POOL)
         setup_s += time.time() - t0
         sizes.append(st.n)
-        t = eng.submit(q, (lambda w=w: W.build(w)), st.b, **kws[q])
+        t = eng.submit(q, (lambda w=w: W.build(w, pool=POOL)), st.b, **kws[q])
         t.wait(600.0)
         t.free()
         del st
     log(f"serving mix: 40 host setups in {setup_s:.1f} s")
-    makers = [(lambda w=w: W.build(w)) for _, w in cases]
+    makers = [(lambda w=w: W.build(w, pool=POOL)) for _, w in cases]
     rng = np.random.default_rng(2027)
     gaps = rng.exponential(1.0 / a.serve_mix_rate, a.serve_mix)
     picks = rng.integers(0, len(cases), a.serve_mix)

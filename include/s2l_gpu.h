@@ -203,7 +203,10 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "spin_limit" (default 2^24): polls of one ready flag after which a sparse sweep gives up and
  *   the call returns S2L_ERR_TIMEOUT (every wait of the sweeps is bounded).  Unlike the options
  *   above it may also be set after s2l_gpu_setup_end; it applies to the launches that follow and
- *   must not be changed while a solve-phase call runs on the setup.
+ *   must not be changed while a solve-phase call runs on the setup;
+ *   "spin_sleep_ns" (default 0, at most 1e6): a sparse-sweep warp whose poll found a column not
+ *   ready pauses this long (__nanosleep) before the next poll, leaving the issue slots to the warps
+ *   that compute the rows it waits for.  Like "spin_limit" it may be set after s2l_gpu_setup_end.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 

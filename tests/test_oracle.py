@@ -394,3 +394,23 @@ def test_reference_generator_workloads_solve(kind, extra):
     x, res = o.gmres(st.b, restart=w.restart, rtol=1e-8)
     assert res["converged"] and np.linalg.norm(st.b - st.A @ x) <= 1.1e-8 * np.linalg.norm(st.b)
     o.close()
+
+
+def test_setup_with_a_shared_worker_pool_is_the_same_setup():
+    """build_setup(pool=...) (one pool of spawned workers for several setups, largest subdomains
+    first) gives the setup of the serial path, entry for entry."""
+    from s2l_b200 import workloads as W
+    from s2l_b200.setup_phase import worker_pool
+    w = W.bubbles3d(14, 4, nbubbles=3, overlap=1)
+    serial = W.build(w, workers=1, use_cache=False)
+    pool = worker_pool(2)
+    try:
+        pooled = [W.build(w, use_cache=False, pool=pool) for _ in range(2)]
+    finally:
+        pool.shutdown()
+    for st in pooled:
+        assert np.array_equal(st.E, serial.E)
+        for a, b in zip(st.subdomains, serial.subdomains):
+            assert np.array_equal(a.V, b.V)
+            assert (a.factor.L != b.factor.L).nnz == 0
+            assert np.array_equal(a.factor.perm_in, b.factor.perm_in)
