@@ -200,6 +200,7 @@ struct s2l_setup {
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     std::atomic<int> opt_spin_limit{S2L_SPIN_LIMIT};  // polls of a sweep wait before it gives up
     std::atomic<int> opt_spin_sleep{S2L_SPIN_SLEEP_NS};  // back-off of a sweep poll that found a column not ready
+    std::atomic<int> opt_sweep_pf{S2L_BATCH_CHUNKS};     // chunks a sweep warp hints into L2 ahead of its task
     double opt_pivot_tol = 1e-6;  // refactorization of LU factors: largest multiplier 1 / pivot_tol
     int opt_amg_single = 0;       // AMG local solvers in single precision (--local-precision single)
     // statistics
@@ -1169,6 +1170,7 @@ LocalSolveArgs<Real> solve_args(s2l_work* w)
     a.nloc = s->nloc;
     a.spin_limit = s->opt_spin_limit.load();
     a.spin_sleep_ns = s->opt_spin_sleep.load();
+    a.sweep_pf = s->opt_sweep_pf.load();
     return a;
 }
 
@@ -2386,12 +2388,11 @@ int s2l_gpu_setup_end(s2l_setup* s)
             for (int64_t e = s->A.rp[r]; e < s->A.rp[r + 1]; ++e) rowsum[r] += s->A.v[e];
         RET_IF(upload(s, &s->d_rowsum, rowsum));
         const double avg = (double)s->nnz / (double)s->n;
-        // short rows (up to 16 entries on average): chunk mode, a warp per 32 rows with coalesced
-        // loads of their entries (spmv_tpr 1); longer rows: lanes per row for about four entries
-        // per lane, between 2 and 32
+        // lanes per row for about four entries per lane, between 2 and 32 (each lane with four
+        // entries in flight: on a 7-point matrix 2 lanes per row beat the chunk mode, a warp per 32
+        // rows with coalesced entry loads, spmv_tpr 1, by 1.3x for one column and 1.5x for four)
         int tpr = 2;
         while (tpr < 32 && tpr * 4 < avg) tpr *= 2;
-        if (avg <= 16.0) tpr = 1;
         s->tpr = s->opt_tpr ? s->opt_tpr : tpr;
     }
 
@@ -2447,7 +2448,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
     });
     for (int i = 0; i < nsub; ++i)
         if (ldlt_bad[i]) return s->fail(S2L_ERR_BADARG, "LDLT: L must store its unit diagonal");
-    s->sweep_group = s->opt_group ? s->opt_group : 32;  // widest lane group of a sweep row
+    s->sweep_group = s->opt_group ? s->opt_group : 16;  // widest lane group of a sweep row
     const int nw = S2L_BS_SWEEP / 32;
     // pass 2: layouts
     int64_t loc = 0;
@@ -2493,7 +2494,7 @@ int s2l_gpu_setup_end(s2l_setup* s)
         int code = S2L_OK;
     };
     std::vector<PreLayout> pre(nsub);
-    s->sweep_group = s->opt_group ? s->opt_group : 32;
+    s->sweep_group = s->opt_group ? s->opt_group : 16;
     parallel_for(nsub, [&](int i) {
         HostSub& h = s->hs[i];
         if (h.amg) return;
@@ -3513,6 +3514,11 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
     if (n == "spin_limit") {  // read at every launch: may change after setup_end
         if (!(value >= 1.0 && value <= 2147483647.0)) return s->fail(S2L_ERR_BADARG, "spin_limit must be in [1, 2^31)");
         s->opt_spin_limit.store((int)value);
+        return S2L_OK;
+    }
+    if (n == "sweep_prefetch") {  // read at every launch, like spin_limit
+        if (!(value >= 0.0 && value <= 32.0)) return s->fail(S2L_ERR_BADARG, "sweep_prefetch must be in [0, 32]");
+        s->opt_sweep_pf.store((int)value);
         return S2L_OK;
     }
     if (n == "spin_sleep_ns") {  // read at every launch, like spin_limit

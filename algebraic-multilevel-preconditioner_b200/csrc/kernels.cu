@@ -453,9 +453,9 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     for (int64_t t = F.wtask[wi]; t < t1; ++t) {
         const uint32_t h = F.thdr[t];
         const int C = (int)(h & 0xFFFFu), gl2 = (int)((h >> 16) & 7u), R = (int)((h >> 19) & 31u) + 1;
-        // the warp's entries are one contiguous stream: hint the first Q chunks after this task (the
-        // next tasks' loads) into L2 while this task waits on its ready flags
-        if (lane < Q) {
+        // the warp's entries are one contiguous stream: hint the first a.sweep_pf chunks after this
+        // task (the next tasks' loads) into L2 while this task waits on its ready flags
+        if (lane < a.sweep_pf) {
             const int64_t e = eo + (int64_t)(C + lane) * 32;
             if (e < e_end) {
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(F.col + e));

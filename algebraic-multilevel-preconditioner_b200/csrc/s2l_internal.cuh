@@ -119,6 +119,7 @@ struct LocalSolveArgs {
     int64_t nloc;              // local-space size (stride of the per-column-group ready flags)
     int spin_limit;            // polls of one ready flag before a sweep gives up (S2L_SPIN_LIMIT by default)
     int spin_sleep_ns;         // pause of a warp after a poll that found a column not ready (0: none)
+    int sweep_pf;              // chunks after a task that a sweep warp hints into L2 (0 .. 32)
 };
 
 // Numeric refactorization of every subdomain's factors on their kept patterns (s2l_gpu_refactor).

@@ -3,7 +3,8 @@
 The layout options of ``s2l_gpu_setup_option`` choose how the same factors and matrix are laid out
 on the device: where each factor is split between the sparse sweeps and the dense tail (the cost
 model's ``hop_us``), how long the chain blocks are (``chain_block``), how many lanes a sparse-sweep
-row may take (``sweep_group``) and how the product with A is spread (``spmv_tpr``).  Their best
+row may take (``sweep_group``), how the product with A is spread (``spmv_tpr``) and how far ahead a
+sweep warp hints its entries into L2 (``sweep_prefetch``, set on an uploaded setup).  Their best
 values depend on the matrix, the partition and the precision.  ``tune`` builds device setups of the
 same host setup with candidate values, times each with CUDA events on the device (the library's
 kernel timers around the local solve and the SpMV of ``s2l_gpu_apply_block`` / ``s2l_gpu_spmv``),
@@ -24,9 +25,12 @@ from . import capi
 SEARCH = (
     ("hop_us", (0.25, 0.1, 0.5, 1.0)),
     ("chain_block", (8, 4, 16)),
-    ("sweep_group", (32, 16, 8)),
+    ("sweep_group", (16, 32, 8)),
     ("spmv_tpr", (0, 1, 2, 4)),
+    ("sweep_prefetch", (8, 16, 24)),
 )
+# options a device setup takes after its upload: tried on the current best setup, not on a new one
+RUNTIME = ("sweep_prefetch", "spin_sleep_ns")
 
 
 def measure(g: capi.GpuSetup, k: int, reps: int, rng) -> dict:
@@ -74,13 +78,29 @@ def tune(ctx: capi.Context, st, k: int = 4, reps: int = 5, spmv_per_step: int = 
         g.close()
         return False
 
+    def runtime_trial(opts, name, v):
+        nonlocal best_t, best_m
+        best_g.set_option(name, v)
+        m = measure(best_g, k, reps, rng)
+        t = objective(m)
+        report["candidates"].append(dict(options=dict(opts), ms=t, **m))
+        if t < best_t:
+            best_t, best_m = t, m
+            return True
+        return False
+
     trial({})
     default_t = best_t
     for name, values in search:
         chosen = current.get(name)
         for v in values[1:]:
             opts = dict(current, **{name: v})
-            if trial(opts):
+            if name in RUNTIME:
+                if runtime_trial(opts, name, v):
+                    chosen = v
+                else:  # back to the value the best setup had
+                    best_g.set_option(name, chosen if chosen is not None else values[0])
+            elif trial(opts):
                 chosen = v
         if chosen is not None:
             current[name] = chosen

@@ -522,7 +522,8 @@ class GpuSetup:
         self.ctx.check(self.lib.s2l_gpu_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
 
     def set_option(self, name: str, value: float):
-        """A setup option that may change after the upload ("spin_limit", "spin_sleep_ns")."""
+        """A setup option that may change after the upload ("spin_limit", "spin_sleep_ns",
+        "sweep_prefetch")."""
         self.ctx.check(self.lib.s2l_gpu_setup_option(self.h, name.encode(), float(value)))
 
     PROF = {"spmv": 1, "local_solve": 2, "coarse": 4, "combine": 8, "krylov_vec": 16, "all": 31}

@@ -57,8 +57,17 @@ _T0 = time.time()
 
 
 def log(msg: str) -> None:
-    """Progress on stderr (the JSON line is the only stdout)."""
-    print(f"[bench {time.time() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+    """Progress on stderr (the JSON line is the only stdout), with the host memory in use: this
+    process (and its setup workers) and what the host has left."""
+    mem = ""
+    try:
+        import psutil
+        me = psutil.Process()
+        rss = me.memory_info().rss + sum(c.memory_info().rss for c in me.children(recursive=True))
+        mem = f" [rss {rss / 2**30:.1f} GB, host free {psutil.virtual_memory().available / 2**30:.0f} GB]"
+    except Exception:
+        pass
+    print(f"[bench {time.time() - _T0:7.1f} s] {msg}{mem}", file=sys.stderr, flush=True)
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "s2l_ref")
 
 
@@ -248,8 +257,8 @@ class Replicas:
 
 # the autotuner's search in the benchmark: a reduced set of candidates (every candidate is a device
 # setup of the 100^3 workload), the first value of each option the default
-TUNE_SEARCH = (("hop_us", (0.25, 0.1, 0.5)), ("chain_block", (8, 16)), ("sweep_group", (32, 16)),
-               ("spmv_tpr", (0, 2)))
+TUNE_SEARCH = (("hop_us", (0.25, 0.1, 0.5)), ("chain_block", (8, 16)), ("sweep_group", (16, 32)),
+               ("spmv_tpr", (0, 1)), ("sweep_prefetch", (8, 16, 24)))
 
 
 def workload_desc(w, overlap) -> str:
@@ -567,6 +576,9 @@ def run_ours(a):
     # (on one GPU: with replicas the line reports the headline form only)
     log("main workload done")
     one = world == 1
+    # the other configurations: 3 warm-up and at most 5 timed steps per form (their setups, not
+    # their solves, take the time)
+    tm = Timer(argparse.Namespace(**dict(vars(a), steps=min(a.steps, 5), warmup=3)), reps, stream)
     c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if one and a.overlap2 and a.overlap != 2 else None
     log("c2 overlap 2 done")
     sequence = sequence_form(a, tm, ctx, stream, dev) if one and a.seq > 0 else None
@@ -739,6 +751,7 @@ def c2_overlap2_form(a, tm, ctx, stream, dev):
     t0 = time.time()
     st = W.build(w, pool=POOL)
     setup_s = time.time() - t0
+    log(f"c2 overlap 2 host setup {setup_s:.1f} s")
     out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
     out.update(workload=workload_desc(w, 2), setup_s=round(setup_s, 1))
     return out
@@ -752,6 +765,7 @@ def c3_form(a, tm, ctx, stream, dev):
     t0 = time.time()
     st = W.build(w, pool=POOL)
     setup_s = time.time() - t0
+    log(f"c3 host setup {setup_s:.1f} s (n = {st.n})")
     out = three_forms(tm, ctx, st, w, stream, dev, k=a.head_k)
     out.update(workload=f"convdiff3d {w.nx}^3 upwind convection-diffusion, {w.nsub} subdomains, overlap 1, nev 24, "
                         f"deflated RAS, LU factors, FGMRES({w.restart}), rtol 1e-8",
@@ -880,10 +894,12 @@ def serve_mix(a, device: int) -> dict:
         st = W.build(w, pool=POOL)
         setup_s += time.time() - t0
         sizes.append(st.n)
-        t = eng.submit(q, (lambda w=w: W.build(w, pool=POOL)), st.b, **kws[q])
+        t = eng.submit(q, (lambda st=st: st), st.b, **kws[q])  # the setup just built, uploaded
         t.wait(600.0)
         t.free()
         del st
+        if q % 10 == 9:
+            log(f"serving mix: {q + 1} cases set up ({setup_s:.1f} s of host setup)")
     log(f"serving mix: 40 host setups in {setup_s:.1f} s")
     makers = [(lambda w=w: W.build(w, pool=POOL)) for _, w in cases]
     rng = np.random.default_rng(2027)

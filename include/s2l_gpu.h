@@ -183,11 +183,11 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "tail_min" (rows, default 64), "tail_max" (default 4096): bounds of a non-empty tail;
  *   "tail_rows" (default 0 = cost model): force every subdomain's tail to this many rows;
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
- *   "sweep_group" (0 = 32, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
+ *   "sweep_group" (0 = 16, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
  *   entries get G lanes, 32 / G rows of one dependency level share a warp);
  *   "spmv_tpr" (0 = automatic, 1, 2, 4, 8, 16 or 32): lanes per row of the products with A; 1 is
- *   chunk mode (a warp per 32 consecutive rows, their entries loaded together; automatic for rows of
- *   up to 16 entries on average), otherwise about four entries per lane from the mean row length;
+ *   chunk mode (a warp per 32 consecutive rows, their entries loaded together); automatic: about
+ *   four entries per lane from the mean row length, at least 2;
  *   "block_width" (0 = automatic, 1, 2, 4, 8 or 16): the most right-hand sides s2l_gpu_gmres_block
  *   puts in one block; larger k run as several blocks at once (automatic: the widest block whose
  *   sparse-sweep CTAs fit the SMs in one wave);
@@ -206,7 +206,9 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   must not be changed while a solve-phase call runs on the setup;
  *   "spin_sleep_ns" (default 0, at most 1e6): a sparse-sweep warp whose poll found a column not
  *   ready pauses this long (__nanosleep) before the next poll, leaving the issue slots to the warps
- *   that compute the rows it waits for.  Like "spin_limit" it may be set after s2l_gpu_setup_end.
+ *   that compute the rows it waits for.  Like "spin_limit" it may be set after s2l_gpu_setup_end;
+ *   "sweep_prefetch" (default 8, 0 to 32): chunks of 32 entries after its current task that a
+ *   sparse-sweep warp hints into L2; may be set after s2l_gpu_setup_end.
  */
 int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value);
 
