@@ -196,7 +196,7 @@ struct s2l_setup {
     int sweep_group = 32;
     // options (s2l_gpu_setup_option)
     int opt_tail_min = 64, opt_tail_max = 4096, opt_group = 0, opt_tail_rows = 0, opt_chain = S2L_CHAIN_DEFAULT, opt_block_width = 0,
-        opt_tpr = 0;
+        opt_tpr = 0, opt_epl = 4;
     double opt_hop_us = 0.25, opt_bw_gbs = 6000.0;
     std::atomic<int> opt_spin_limit{S2L_SPIN_LIMIT};  // polls of a sweep wait before it gives up
     std::atomic<int> opt_spin_sleep{S2L_SPIN_SLEEP_NS};  // back-off of a sweep poll that found a column not ready
@@ -486,7 +486,7 @@ void parallel_for(int n, const std::function<void(int)>& f)
     for (auto& x : th) x.join();
 }
 
-void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, int gmax, int chain, Sweep& out,
+void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, int gmax, int epl, int chain, Sweep& out,
                  std::string& err, const std::vector<int32_t>* mpos = nullptr)
 {
     const bool track = mpos != nullptr;
@@ -669,7 +669,7 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
         out.dinv[p] = 1.0 / diag[r];
     }
     // Tasks: the rows of one level, R = 32 / G of them with G lanes each (G from the row length,
-    // about four entries per lane, at most gmax), sorted by width and length so a task's rows
+    // about epl entries per lane, at most gmax), sorted by width and length so a task's rows
     // are alike.  Each task goes to the warp with the least work so far; a warp's tasks stay in
     // level order.  Entries are stored lane-interleaved: chunk c of a task holds, for lane
     // k * G + j, entry c * G + j of its row k (column T, the sentinel slot, and value 0 past the
@@ -677,7 +677,7 @@ void build_sweep(const HostCsr& M, int T, bool lower, bool unit_diag, int nw, in
     // 1/diag folded into the values (the sweep scales the right-hand side by 1/diag too).
     auto width = [&](int len) {
         int g = 1;
-        while (g < gmax && g * 4 < len) g <<= 1;
+        while (g < gmax && g * epl < len) g <<= 1;
         return g;
     };
     struct WarpOut {
@@ -2523,9 +2523,9 @@ int s2l_gpu_setup_end(s2l_setup* s)
                     q.mposU[e] = llt ? q.P.find(c, r) : q.P.find(r, c);
                 }
         }
-        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_chain, q.sl, q.err, rfon ? &q.mposL : nullptr);
+        build_sweep(h.L, T, true, unitL, nw, s->sweep_group, s->opt_epl, s->opt_chain, q.sl, q.err, rfon ? &q.mposL : nullptr);
         if (q.err.empty())
-            build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_chain, q.su, q.err, rfon ? &q.mposU : nullptr);
+            build_sweep(U, T, false, false, nw, s->sweep_group, s->opt_epl, s->opt_chain, q.su, q.err, rfon ? &q.mposU : nullptr);
         if (!q.err.empty()) q.code = S2L_ERR_NUMERIC;
     });
     for (int i = 0; i < nsub; ++i) {
@@ -3546,6 +3546,10 @@ int s2l_gpu_setup_option(s2l_setup* s, const char* name, double value)
         if (bw != 0 && bw != 1 && bw != 2 && bw != 4 && bw != 8 && bw != 16)
             return s->fail(S2L_ERR_BADARG, "block_width must be 0, 1, 2, 4, 8 or 16");
         s->opt_block_width = bw;
+    } else if (n == "sweep_epl") {
+        const int v = (int)value;
+        if (v != 2 && v != 4 && v != 8 && v != 16) return s->fail(S2L_ERR_BADARG, "sweep_epl must be 2, 4, 8 or 16");
+        s->opt_epl = v;
     } else if (n == "chain_block") {
         const int c = (int)value;
         if (c < 1 || c > S2L_CHAIN_MAX) return s->fail(S2L_ERR_BADARG, "chain_block must be in [1, 16]");

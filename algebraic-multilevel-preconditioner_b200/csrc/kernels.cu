@@ -329,9 +329,9 @@ __device__ __forceinline__ bool sweep_batch(const int32_t* __restrict__ colp, co
     int lc[N];
     Real lv[N];
 #pragma unroll
-    for (int q = 0; q < N; ++q) {
-        lc[q] = colp[q * 32];
-        lv[q] = valp[q * 32];
+    for (int q = 0; q < N; ++q) {  // read once: streaming loads, so they do not evict the warp's other lines
+        lc[q] = __ldcs(colp + q * 32);
+        lv[q] = __ldcs(valp + q * 32);
     }
     int spin = 0;
     for (;;) {
@@ -371,7 +371,8 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_word;
     volatile int& abort_flag = abort_word;
-    constexpr int Q = (sizeof(Real) == 8 && KC > 1) ? S2L_BATCH_CHUNKS / 2 : S2L_BATCH_CHUNKS;
+    // chunks per batch: 8 (FP32), 6 (FP64, one column: the registers of 1024 threads), 4 (FP64 blocks)
+    constexpr int Q = sizeof(Real) == 4 ? S2L_BATCH_CHUNKS : (KC > 1 ? S2L_BATCH_CHUNKS / 2 : S2L_BATCH_CHUNKS * 3 / 4);
     // KC right-hand sides per CTA: CTA b takes subdomain b / ngrp and columns grp * KC .. + KC of
     // the K interleaved columns (the CTAs of one subdomain are neighbours, so they share the
     // factor stream in L2)
@@ -432,6 +433,8 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
                 Real v[KC];
 #pragma unroll
                 for (int r = 0; r < KC; ++r) v[r] = Real(0);
+                // four entries' loads (slot, W) in flight together, added in entry order
+#pragma unroll 4
                 for (int j = 0; j <= i; ++j) {
                     const int sj = F.blk_slot[o + j];
 #pragma unroll
@@ -450,8 +453,16 @@ __global__ void __launch_bounds__(S2L_BS_SWEEP, 1) sweep_kernel(const LocalSolve
     int64_t so = F.wslot[wi], eo = F.went[wi];
     const int64_t e_end = F.went[wi + 1];  // the warp's entries are [went[wi], went[wi + 1])
     bool dead = false;
+    // task headers 32 at a time: lane j holds the header of task hbase + j (one coalesced load),
+    // each task takes its own by a shuffle instead of a load of its own
+    int64_t hbase = F.wtask[wi];
+    uint32_t hwin = hbase + lane < t1 ? F.thdr[hbase + lane] : 0u;
     for (int64_t t = F.wtask[wi]; t < t1; ++t) {
-        const uint32_t h = F.thdr[t];
+        if (t - hbase == 32) {  // the same for the whole warp
+            hbase = t;
+            hwin = hbase + lane < t1 ? F.thdr[hbase + lane] : 0u;
+        }
+        const uint32_t h = __shfl_sync(0xffffffffu, hwin, (int)(t - hbase));
         const int C = (int)(h & 0xFFFFu), gl2 = (int)((h >> 16) & 7u), R = (int)((h >> 19) & 31u) + 1;
         // the warp's entries are one contiguous stream: hint the first a.sweep_pf chunks after this
         // task (the next tasks' loads) into L2 while this task waits on its ready flags

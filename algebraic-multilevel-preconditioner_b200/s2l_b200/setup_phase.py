@@ -427,12 +427,13 @@ def _one_thread_worker():
         pass
 
 
-def worker_pool(workers: int | None = None) -> ProcessPoolExecutor:
+def worker_pool(workers: int | None = None, tasks_per_worker: int | None = 32) -> ProcessPoolExecutor:
     """A pool of spawned worker processes for the per-subdomain setup work (factorization and
     eigenproblem), one BLAS thread each; pass it to build_setup(pool=...) to set up several matrices
-    without starting new processes for each."""
+    without starting new processes for each.  A worker is replaced after `tasks_per_worker`
+    subdomains, so the memory a process keeps from large factorizations does not pile up."""
     return ProcessPoolExecutor(max_workers=workers or os.cpu_count() or 1, mp_context=mp.get_context("spawn"),
-                               initializer=_one_thread_worker)
+                               initializer=_one_thread_worker, max_tasks_per_child=tasks_per_worker)
 
 
 def build_setup(A_orig: sp.csr_matrix, b_orig: np.ndarray, part: np.ndarray, nsub: int, opts: SchwarzOptions,

@@ -63,8 +63,9 @@ def log(msg: str) -> None:
     try:
         import psutil
         me = psutil.Process()
-        rss = me.memory_info().rss + sum(c.memory_info().rss for c in me.children(recursive=True))
-        mem = f" [rss {rss / 2**30:.1f} GB, host free {psutil.virtual_memory().available / 2**30:.0f} GB]"
+        kids = sum(c.memory_info().rss for c in me.children(recursive=True))
+        mem = (f" [rss {me.memory_info().rss / 2**30:.1f} GB + workers {kids / 2**30:.1f} GB, "
+               f"host free {psutil.virtual_memory().available / 2**30:.0f} GB]")
     except Exception:
         pass
     print(f"[bench {time.time() - _T0:7.1f} s] {msg}{mem}", file=sys.stderr, flush=True)
@@ -579,11 +580,15 @@ def run_ours(a):
     # the other configurations: 3 warm-up and at most 5 timed steps per form (their setups, not
     # their solves, take the time)
     tm = Timer(argparse.Namespace(**dict(vars(a), steps=min(a.steps, 5), warmup=3)), reps, stream)
+    import gc
     c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if one and a.overlap2 and a.overlap != 2 else None
+    gc.collect()
     log("c2 overlap 2 done")
     sequence = sequence_form(a, tm, ctx, stream, dev) if one and a.seq > 0 else None
+    gc.collect()
     log("sequence done")
     c3 = c3_form(a, tm, ctx, stream, dev) if one and a.c3 > 0 else None
+    gc.collect()
     log("c3 done")
     serving_mix = serve_mix(a, local) if one and a.serve_mix > 0 else None
     log("serving mix done")

@@ -183,8 +183,12 @@ int s2l_gpu_set_coarse(s2l_setup* s, int64_t n0, const int64_t* offsets, const d
  *   "tail_min" (rows, default 64), "tail_max" (default 4096): bounds of a non-empty tail;
  *   "tail_rows" (default 0 = cost model): force every subdomain's tail to this many rows;
  *   "hop_us" (default 0.25), "bw_gbs" (default 6000): the cost model's parameters;
- *   "sweep_group" (0 = 16, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to 4G
- *   entries get G lanes, 32 / G rows of one dependency level share a warp);
+ *   "sweep_group" (0 = 16, 8, 16 or 32): most lanes a sparse-sweep row gets (rows of up to
+ *   sweep_epl G entries get G lanes, 32 / G rows of one dependency level share a warp);
+ *   "sweep_epl" (2, 4, 8 or 16, default 4): entries per lane a sparse-sweep row is sized for (a
+ *   row of len entries gets the fewest lanes G, a power of two up to sweep_group, with
+ *   G sweep_epl >= len): larger values pack more rows into one task, so a warp has fewer tasks,
+ *   each with more entries per lane;
  *   "spmv_tpr" (0 = automatic, 1, 2, 4, 8, 16 or 32): lanes per row of the products with A; 1 is
  *   chunk mode (a warp per 32 consecutive rows, their entries loaded together); automatic: about
  *   four entries per lane from the mean row length, at least 2;
