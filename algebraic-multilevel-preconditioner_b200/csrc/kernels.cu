@@ -1184,48 +1184,71 @@ __global__ void combine_block_kernel(int64_t n, const int64_t* __restrict__ cp_p
     }
 }
 
-// c_i(c, r) = V_i(:, c)^T R(:, r) per 256-row tile of one subdomain: partials[(tile * mmax + c) * K + r].
-// Warp w takes the tile rows w, w + 8, ...; lane c keeps the sums of coarse column c (32 columns at a
-// time) for the K right-hand sides, so a row of V (m contiguous doubles) is one coalesced load and
-// the K values of R at the row one broadcast load; no shuffle per row.  The warps' sums are added in
-// warp order after one barrier.
+// Coarse restriction of one tile (up to S2L_TILE_ROWS rows of one subdomain), K columns:
+// partials(tile, c, r) = sum_i V(row0 + i, c) R(g(row0 + i), r).  The tile's rows of R are staged
+// in shared memory first; the tile's block of V (nr x m, contiguous row-major) is then streamed by
+// all threads, with 16-byte loads when m is even: thread (g, p) takes the column pair p of rows
+// g, g + G, ... (G = threads / pairs, so all lanes load), and the G partial sums of each (c, r)
+// are added in order of g.  Every (c, r) sums in the same order whatever K is.
 template <int K>
 __global__ void __launch_bounds__(S2L_TILE_ROWS) coarse_restrict_block_kernel(
     const int32_t* __restrict__ t_sub, const int32_t* __restrict__ t_row0, const int32_t* __restrict__ t_nrow,
     const DevSub* __restrict__ subs, const double* __restrict__ V, const int32_t* __restrict__ l2g, int boolean_pou,
     const double* __restrict__ R, int mmax, double* __restrict__ partials)
 {
-    extern __shared__ double red[];  // [S2L_TILE_ROWS / 32][mmax * K]
+    extern __shared__ double sm[];  // Rs[S2L_TILE_ROWS * K], then red[G * m * K] (G m <= 2 S2L_TILE_ROWS)
     const int tile = blockIdx.x;
     const DevSub sd = subs[t_sub[tile]];
     const int m = sd.m, nr = t_nrow[tile], row0 = t_row0[tile];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const double* Vs = V + sd.v_off;
-    double* wred = red + (size_t)warp * mmax * K;
-    for (int c0 = 0; c0 < m; c0 += 32) {
-        const int c = c0 + lane;
-        double acc[K];
+    if (m == 0) return;  // the prolongation's zero tiles of subdomains without a coarse basis
+    double* Rs = sm;
+    double* red = sm + S2L_TILE_ROWS * K;
+    for (int e = threadIdx.x; e < nr * K; e += S2L_TILE_ROWS) {
+        const int i = e / K, r = e % K;
+        const int l = row0 + i;
+        const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
+        Rs[e] = R[g * K + r];
+    }
+    __syncthreads();
+    const double* Vt = V + sd.v_off + (int64_t)row0 * m;
+    const bool vec = (m & 1) == 0 && (reinterpret_cast<uintptr_t>(Vt) & 15) == 0;
+    const int W = vec ? 2 : 1;  // columns per thread
+    const int P = (m + W - 1) / W, G = S2L_TILE_ROWS / P;
+    const int p = threadIdx.x % P, g = threadIdx.x / P;
+    if (g < G) {
+        double a0[K], a1[K];
 #pragma unroll
-        for (int r = 0; r < K; ++r) acc[r] = 0.0;
+        for (int r = 0; r < K; ++r) a0[r] = a1[r] = 0.0;
+        if (vec) {
 #pragma unroll 4
-        for (int i = warp; i < nr; i += S2L_TILE_ROWS / 32) {
-            const int l = row0 + i;
-            const int64_t g = boolean_pou ? sd.begin + l : (int64_t)l2g[sd.loc_off + l];
-            double rv[K];
-            load_k<double, K>(R + g * K, rv);
-            const double vc = c < m ? Vs[(int64_t)l * m + c] : 0.0;
+            for (int i = g; i < nr; i += G) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(Vt + (int64_t)i * m) + p);
 #pragma unroll
-            for (int r = 0; r < K; ++r) acc[r] += vc * rv[r];
+                for (int r = 0; r < K; ++r) {
+                    const double x = Rs[i * K + r];
+                    a0[r] += v.x * x;
+                    a1[r] += v.y * x;
+                }
+            }
+        } else {
+#pragma unroll 4
+            for (int i = g; i < nr; i += G) {
+                const double v = __ldg(Vt + (int64_t)i * m + p);
+#pragma unroll
+                for (int r = 0; r < K; ++r) a0[r] += v * Rs[i * K + r];
+            }
         }
-        if (c < m)
+        const int c = p * W;
 #pragma unroll
-            for (int r = 0; r < K; ++r) wred[c * K + r] = acc[r];
+        for (int r = 0; r < K; ++r) red[((size_t)g * m + c) * K + r] = a0[r];
+        if (vec)
+#pragma unroll
+            for (int r = 0; r < K; ++r) red[((size_t)g * m + c + 1) * K + r] = a1[r];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < m * K; e += S2L_TILE_ROWS) {
         double t = 0.0;
-#pragma unroll
-        for (int w = 0; w < S2L_TILE_ROWS / 32; ++w) t += red[(size_t)w * mmax * K + e];
+        for (int q = 0; q < G; ++q) t += red[(size_t)q * m * K + e];
         partials[(int64_t)tile * mmax * K + e] = t;
     }
 }
@@ -1480,9 +1503,10 @@ static void restrict_tiles(cudaStream_t st, int K, int ntiles, const int32_t* t_
                            int boolean_pou, const double* R, int mmax, double* partials)
 {
     if (ntiles <= 0) return;
-    const size_t smem = (size_t)(S2L_TILE_ROWS / 32) * mmax * K * sizeof(double);  // <= 131 KB (mmax <= 128, K <= 16)
+    // staged R rows + the row groups' partial sums (G m <= 2 S2L_TILE_ROWS): <= 96 KB for K = 16
+    const size_t smem = (size_t)3 * S2L_TILE_ROWS * K * sizeof(double);
     S2L_KSWITCH(K, (cudaFuncSetAttribute(coarse_restrict_block_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)((size_t)(S2L_TILE_ROWS / 32) * S2L_MAX_RED_COLS * KK * sizeof(double))),
+                                         (int)((size_t)3 * S2L_TILE_ROWS * KK * sizeof(double))),
                     coarse_restrict_block_kernel<KK><<<ntiles, S2L_TILE_ROWS, smem, st>>>(
                         t_sub, t_row0, t_nrow, subs, V, l2g, boolean_pou, R, mmax, partials)));
 }

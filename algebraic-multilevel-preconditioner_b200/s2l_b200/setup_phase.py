@@ -427,11 +427,12 @@ def _one_thread_worker():
         pass
 
 
-def worker_pool(workers: int | None = None, tasks_per_worker: int | None = 32) -> ProcessPoolExecutor:
+def worker_pool(workers: int | None = None, tasks_per_worker: int | None = None) -> ProcessPoolExecutor:
     """A pool of spawned worker processes for the per-subdomain setup work (factorization and
     eigenproblem), one BLAS thread each; pass it to build_setup(pool=...) to set up several matrices
-    without starting new processes for each.  A worker is replaced after `tasks_per_worker`
-    subdomains, so the memory a process keeps from large factorizations does not pile up."""
+    without starting new processes for each.  With `tasks_per_worker` a worker is replaced after
+    that many subdomains (off by default: the workers' memory stays small, about 1.4 GB for 16
+    after the 2.1M-row convection-diffusion setup)."""
     return ProcessPoolExecutor(max_workers=workers or os.cpu_count() or 1, mp_context=mp.get_context("spawn"),
                                initializer=_one_thread_worker, max_tasks_per_child=tasks_per_worker)
 

@@ -97,6 +97,9 @@ def parse(argv=None):
     ap.add_argument("--amg", type=int, default=1, help="AMG form: AMG local solvers on the main matrix (0 = off)")
     ap.add_argument("--serve-mix", type=int, default=2000, help="serving-mix form: requests over 40 cases (0 = off)")
     ap.add_argument("--serve-mix-rate", type=float, default=50.0)
+    ap.add_argument("--serve-mix-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--budget-s", type=float, default=1500.0,
+                    help="wall-clock budget of the run: the secondary configurations that no longer fit are skipped")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune the mixed setup's device layout (s2l_b200.autotune) before the timed forms (0 = off)")
     ap.add_argument("--parity", type=int, default=1,
@@ -577,23 +580,45 @@ def run_ours(a):
     # (on one GPU: with replicas the line reports the headline form only)
     log("main workload done")
     one = world == 1
-    # the other configurations: 3 warm-up and at most 5 timed steps per form (their setups, not
-    # their solves, take the time)
-    tm = Timer(argparse.Namespace(**dict(vars(a), steps=min(a.steps, 5), warmup=3)), reps, stream)
     import gc
-    c2_overlap2 = c2_overlap2_form(a, tm, ctx, stream, dev) if one and a.overlap2 and a.overlap != 2 else None
     gc.collect()
-    log("c2 overlap 2 done")
-    sequence = sequence_form(a, tm, ctx, stream, dev) if one and a.seq > 0 else None
-    gc.collect()
-    log("sequence done")
-    c3 = c3_form(a, tm, ctx, stream, dev) if one and a.c3 > 0 else None
-    gc.collect()
-    log("c3 done")
-    serving_mix = serve_mix(a, local) if one and a.serve_mix > 0 else None
-    log("serving mix done")
+    torch.cuda.empty_cache()
+    # the reference's own run (the line's cpu_baseline and parity) before the other configurations
+    cb = parity = None
+    if rank == 0 and one and not a.no_cpu_baseline and a.overlap == 1:
+        try:
+            cb, parity = cpu_baseline_leg(a, wl)
+        except Exception as e:  # reported, not fatal to the line
+            parity = {"error": str(e)[-300:]}
+        log("cpu baseline and parity done")
+    # the other configurations, in order of the configurations they stand for, while the run's time
+    # budget allows (each form is skipped, not cut, when its usual time no longer fits): 3 warm-up
+    # and at most 5 timed steps per form (their setups, not their solves, take the time)
+    tm = Timer(argparse.Namespace(**dict(vars(a), steps=min(a.steps, 5), warmup=3)), reps, stream)
+
+    def form(name, on, est_s, fn):
+        if not (one and on):
+            return None
+        left = a.budget_s - (time.time() - _T0)
+        if left < est_s:
+            log(f"{name} skipped: {left:.0f} s of the {a.budget_s:.0f} s budget left, it takes about {est_s} s")
+            return {"skipped": f"time budget: {left:.0f} s of {a.budget_s:.0f} s left, the form takes about {est_s} s"}
+        try:
+            out = fn()
+        except Exception as e:  # reported in the line, not fatal to it
+            out = {"error": f"{type(e).__name__}: {str(e)[-300:]}"}
+        gc.collect()
+        torch.cuda.empty_cache()
+        log(f"{name} done")
+        return out
+
+    c3 = form("c3", a.c3 > 0, 300, lambda: c3_form(a, tm, ctx, stream, dev))
+    sequence = form("sequence", a.seq > 0, 330, lambda: sequence_form(a, tm, ctx, stream, dev))
+    c2_overlap2 = form("c2 overlap 2", a.overlap2 and a.overlap != 2, 90,
+                       lambda: c2_overlap2_form(a, tm, ctx, stream, dev))
     if POOL is not None:
         POOL.shutdown()
+    serving_mix = form("serving mix", a.serve_mix > 0, 240, lambda: serve_mix_child(a, local))
 
     out = {
         "metric": METRIC,
@@ -660,15 +685,12 @@ def run_ours(a):
         "gpu_launches": int(rf["launches"] * max(kh // bw, 1)),
         "clocks": head["clocks"],
     }
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cb, parity = cpu_baseline_leg(a, wl) if a.overlap == 1 else (None, None)
-        log("cpu baseline and parity done")
-        if cb is not None:
-            out["cpu_baseline"] = cb
-            out["forms"]["plain_fp64"]["speedup_vs_reference_same_config"] = cb["ms_per_solve"] / plain["ms_per_solve"]
-            out["forms"]["speedup_head_vs_reference_per_solve"] = cb["ms_per_solve"] / head["ms_per_solve"]
-        if parity is not None and a.parity:
-            out["parity"] = parity
+    if cb is not None:
+        out["cpu_baseline"] = cb
+        out["forms"]["plain_fp64"]["speedup_vs_reference_same_config"] = cb["ms_per_solve"] / plain["ms_per_solve"]
+        out["forms"]["speedup_head_vs_reference_per_solve"] = cb["ms_per_solve"] / head["ms_per_solve"]
+    if parity is not None and a.parity:
+        out["parity"] = parity
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -864,6 +886,28 @@ def sequence_form(a, tm, ctx, stream, dev):
             "all_converged": all(q["converged"] for q in steps), "steps": steps}
 
 
+def serve_mix_child(a, device: int) -> dict:
+    """serve_mix in a child process (its own CUDA context and setup workers), bounded by what is
+    left of the run's time budget: a child that fails or runs out of time costs the line this form
+    only."""
+    left = a.budget_s - (time.time() - _T0) - 30.0
+    cmd = [sys.executable, os.path.abspath(__file__), "--serve-mix-only", "--serve-mix", str(a.serve_mix),
+           "--serve-mix-rate", str(a.serve_mix_rate)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=max(left, 60.0),
+                           env=dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(device))))
+    except subprocess.TimeoutExpired as e:
+        tail = (e.stderr or b"")[-400:]
+        return {"error": f"did not finish within the {left:.0f} s left of the time budget", "stderr_tail":
+                tail.decode(errors="replace") if isinstance(tail, bytes) else str(tail)}
+    for line in r.stderr.splitlines()[-12:]:
+        log("  " + line)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"child exited with {r.returncode}", "stderr_tail": r.stderr[-400:]}
+    return json.loads(lines[-1])
+
+
 def serve_mix(a, device: int) -> dict:
     """Poisson arrivals (a.serve_mix_rate per second) of a.serve_mix solve requests, each on one of
     40 seeded cases of the three workload families at several sizes (2D Poisson with LU factors,
@@ -1055,7 +1099,12 @@ def run_reference(a):
 
 if __name__ == "__main__":
     args = parse()
-    if args.impl == "reference":
+    if args.serve_mix_only:  # the serving-mix form alone (run as a child of the bench)
+        from s2l_b200.setup_phase import worker_pool
+        POOL = worker_pool()
+        print(json.dumps(serve_mix(args, 0)), flush=True)
+        POOL.shutdown()
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
