@@ -56,6 +56,16 @@ POOL = None  # the run's setup worker processes (setup_phase.worker_pool), on on
 _T0 = time.time()
 
 
+def release_host_memory() -> None:
+    """Give the heap pages freed by a form's host setup back to the system (glibc malloc_trim): the
+    many tens-of-MB arrays of a large setup are freed into the heap, not unmapped."""
+    try:
+        import ctypes
+        ctypes.CDLL("libc.so.6").malloc_trim(0)
+    except Exception:
+        pass
+
+
 def log(msg: str) -> None:
     """Progress on stderr (the JSON line is the only stdout), with the host memory in use: this
     process (and its setup workers) and what the host has left."""
@@ -95,7 +105,8 @@ def parse(argv=None):
     ap.add_argument("--c3", type=int, default=128, help="convection-diffusion form: grid size (0 = off)")
     ap.add_argument("--c3-nsub", type=int, default=128)
     ap.add_argument("--amg", type=int, default=1, help="AMG form: AMG local solvers on the main matrix (0 = off)")
-    ap.add_argument("--serve-mix", type=int, default=2000, help="serving-mix form: requests over 40 cases (0 = off)")
+    ap.add_argument("--serve-mix", type=int, default=0,
+                    help="serving-mix form: requests over 40 cases, in a child process (0 = off; 2000 is the configuration)")
     ap.add_argument("--serve-mix-rate", type=float, default=50.0)
     ap.add_argument("--serve-mix-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--budget-s", type=float, default=1500.0,
@@ -583,6 +594,7 @@ def run_ours(a):
     import gc
     gc.collect()
     torch.cuda.empty_cache()
+    release_host_memory()
     # the reference's own run (the line's cpu_baseline and parity) before the other configurations
     cb = parity = None
     if rank == 0 and one and not a.no_cpu_baseline and a.overlap == 1:
@@ -609,6 +621,7 @@ def run_ours(a):
             out = {"error": f"{type(e).__name__}: {str(e)[-300:]}"}
         gc.collect()
         torch.cuda.empty_cache()
+        release_host_memory()
         log(f"{name} done")
         return out
 
