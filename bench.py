@@ -56,6 +56,20 @@ POOL = None  # the run's setup worker processes (setup_phase.worker_pool), on on
 _T0 = time.time()
 
 
+def budgeted(name: str, est_s: float, fn, left_s: float, budget_s: float):
+    """fn() when its usual time est_s fits in what is left of the run's budget, else a "skipped"
+    record; an exception in fn becomes an "error" record (reported in the line, not fatal to it)."""
+    if left_s < est_s:
+        log(f"{name} skipped: {left_s:.0f} s of the {budget_s:.0f} s budget left, it takes about {est_s} s")
+        return {"skipped": f"time budget: {left_s:.0f} s of {budget_s:.0f} s left, the form takes about {est_s} s"}
+    try:
+        out = fn()
+    except Exception as e:
+        out = {"error": f"{type(e).__name__}: {str(e)[-300:]}"}
+    log(f"{name} done")
+    return out
+
+
 def release_host_memory() -> None:
     """Give the heap pages freed by a form's host setup back to the system (glibc malloc_trim): the
     many tens-of-MB arrays of a large setup are freed into the heap, not unmapped."""
@@ -611,18 +625,10 @@ def run_ours(a):
     def form(name, on, est_s, fn):
         if not (one and on):
             return None
-        left = a.budget_s - (time.time() - _T0)
-        if left < est_s:
-            log(f"{name} skipped: {left:.0f} s of the {a.budget_s:.0f} s budget left, it takes about {est_s} s")
-            return {"skipped": f"time budget: {left:.0f} s of {a.budget_s:.0f} s left, the form takes about {est_s} s"}
-        try:
-            out = fn()
-        except Exception as e:  # reported in the line, not fatal to it
-            out = {"error": f"{type(e).__name__}: {str(e)[-300:]}"}
+        out = budgeted(name, est_s, fn, a.budget_s - (time.time() - _T0), a.budget_s)
         gc.collect()
         torch.cuda.empty_cache()
         release_host_memory()
-        log(f"{name} done")
         return out
 
     c3 = form("c3", a.c3 > 0, 300, lambda: c3_form(a, tm, ctx, stream, dev))

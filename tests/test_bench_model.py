@@ -47,3 +47,25 @@ def test_gmres_solve_bytes_one_level(bench):
     got = bench.gmres_solve_bytes(st, [1], 30, 5.0e5, 1.0e4)
     want = (5.0e5 - 1.0e4) + st.A.nnz * 12 + (n + 1) * 4 + 1.0e4 + 16 * n + 24 * n + 2 * (16 * n + 16 * n)
     assert got == pytest.approx(want)
+
+
+def test_secondary_forms_run_within_the_budget(bench):
+    """A form runs when its usual time fits in what is left of the run's budget, is skipped (with a
+    record) when it does not, and an exception becomes an error record instead of ending the run."""
+    assert bench.budgeted("f", 100, lambda: {"x": 1}, 500, 1500) == {"x": 1}
+    assert "skipped" in bench.budgeted("f", 100, lambda: {"x": 1}, 50, 1500)
+
+    def boom():
+        raise RuntimeError("no room")
+    assert bench.budgeted("f", 100, boom, 500, 1500)["error"].startswith("RuntimeError: no room")
+
+
+def test_serving_mix_child_failure_is_a_record(bench):
+    """The serving mix runs in a child process: a child that fails (here: no CUDA device, or any
+    other error) gives an error record, the parent carries on."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU would run the whole serving mix")
+    a = bench.parse(["--serve-mix", "10", "--budget-s", "600"])
+    r = bench.serve_mix_child(a, 0)
+    assert "error" in r and "stderr_tail" in r
