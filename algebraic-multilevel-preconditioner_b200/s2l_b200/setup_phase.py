@@ -200,7 +200,9 @@ def kernel_complement(B: sp.spmatrix, Q: np.ndarray, thr: float) -> np.ndarray:
     if Q.shape[1] == 0:
         return np.zeros((Q.shape[0], 0))
     BQ = B @ Q
-    _, s, vh = np.linalg.svd(BQ, full_matrices=True)
+    # thin SVD: only the right singular vectors (k x k) are used; the full one would also build the
+    # n x n left factor (7 GB for a 30k-row subdomain)
+    _, s, vh = np.linalg.svd(BQ, full_matrices=False)
     r = int(np.sum(s > thr))
     return Q @ vh.T[:, :r]
 
