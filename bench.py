@@ -119,8 +119,8 @@ def parse(argv=None):
     ap.add_argument("--c3", type=int, default=128, help="convection-diffusion form: grid size (0 = off)")
     ap.add_argument("--c3-nsub", type=int, default=128)
     ap.add_argument("--amg", type=int, default=1, help="AMG form: AMG local solvers on the main matrix (0 = off)")
-    ap.add_argument("--serve-mix", type=int, default=0,
-                    help="serving-mix form: requests over 40 cases, in a child process (0 = off; 2000 is the configuration)")
+    ap.add_argument("--serve-mix", type=int, default=2000,
+                    help="serving-mix form: requests over 40 cases, in a child process bounded by the budget (0 = off)")
     ap.add_argument("--serve-mix-rate", type=float, default=50.0)
     ap.add_argument("--serve-mix-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--budget-s", type=float, default=1500.0,
